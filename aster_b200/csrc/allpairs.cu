@@ -1,0 +1,343 @@
+// All-pairs force kernels: the replacement for Parallelized::compute_forces
+// (src/utils/builder_endpoint.cpp:729-757), SimpleGPU::compute_forces +
+// cl3d_newton (src/solvers/SimpleGPU.cpp:17-71,
+// include/Aster/kernels/newton_update3d.cl.h:28-72) and the PN pair law of
+// compute_gravitational/get_pn1 (src/physics/tool_chain_impl.cpp:110-137).
+//
+// Pair law (acceleration on i from j, d = x_j - x_i, r^2 = d.d + eps2):
+//   a_i += G m_j d / r^3
+//   PN1:  + G m_j / (c^2 r^2) [ n A + (v_i - v_j) B ],  n = -d/r,
+//         A = -v_i^2 - 2 v_j^2 + 4 v_i.v_j + 1.5 (n.v_j)^2 + 5 G m_i/r + 4 G m_j/r,
+//         B = 4 n.v_i - 3 n.v_j                  (tool_chain_impl.cpp:110-118)
+//
+// Two arithmetic paths, one tiling:
+//  * FP64: double4 (x,y,z,m) j-tiles in shared memory, FP64 throughout; the
+//    "plain FP64 GPU path" the mixed path is measured against.
+//  * MIXED: positions as double-single float pairs (hi = rn(x), lo = rn(x-hi)),
+//    d = (x_j,hi - x_i,hi) + (x_j,lo - x_i,lo) in FP32 (accurate to FP32
+//    relative precision of d even for close pairs far from the origin),
+//    rsqrt on the SFU, per-thread FP32 partial sums over 64 j folded into a
+//    two-sum compensated accumulator (hi, lo), final value in FP64.
+// Each thread owns IPT targets; a block of BLOCK threads owns BLOCK*IPT targets
+// and walks one j-slice; small n use several j-slices whose partial sums are
+// added by k_reduce_slices (scratch memory).
+#include "aster_internal.cuh"
+
+namespace {
+
+constexpr int BLOCK = 128;   // threads per block == j-tile length
+constexpr int IPT = 2;       // targets per thread
+constexpr int FOLD = 64;     // FP32 terms summed before a compensated fold
+constexpr float PAD_POS = 1.0e30f;
+
+struct KickArgs {
+    bool on;
+    double half_dt;
+    double4* vel;
+};
+
+// Epilogue shared by both paths: write acceleration (scaled by G) either to
+// ctx->acc (+ optional closing kick v += a dt/2) or to an explicit output, or
+// as a partial sum of slice s to scratch.
+__device__ __forceinline__ void store_result(int64_t t, int64_t body, double ax, double ay, double az,
+                                             double G, int nslices, int slice, int64_t nt,
+                                             double4* __restrict__ partial, double4* __restrict__ acc,
+                                             double* __restrict__ out3, KickArgs kick) {
+    if (nslices > 1) {
+        partial[(int64_t)slice * nt + t] = make_double4(ax, ay, az, 0.0);
+        return;
+    }
+    ax *= G; ay *= G; az *= G;
+    if (out3) {
+        out3[3 * t] = ax; out3[3 * t + 1] = ay; out3[3 * t + 2] = az;
+        return;
+    }
+    acc[body] = make_double4(ax, ay, az, 0.0);
+    if (kick.on) {
+        double4 v = kick.vel[body];
+        v.x += ax * kick.half_dt; v.y += ay * kick.half_dt; v.z += az * kick.half_dt;
+        kick.vel[body] = v;
+    }
+}
+
+// ---------------------------------------------------------------- FP64 path
+template <bool PN, bool GUARD>
+__global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
+    int64_t n, int64_t nt, const int32_t* __restrict__ targets, const double4* __restrict__ pm,
+    const double4* __restrict__ vel, double G, double eps2, double inv_c2, int64_t slice_len, int nslices,
+    double4* __restrict__ partial, double4* __restrict__ acc, double* __restrict__ out3, KickArgs kick) {
+    __shared__ double4 sp[BLOCK];
+    __shared__ double4 sv[PN ? BLOCK : 1];
+    const int slice = blockIdx.y;
+    const int64_t j0 = (int64_t)slice * slice_len;
+    const int64_t j1 = min(n, j0 + slice_len);
+    int64_t tt[IPT], bi[IPT];
+    double xi[IPT], yi[IPT], zi[IPT], mi[IPT], vxi[IPT], vyi[IPT], vzi[IPT];
+    double ax[IPT], ay[IPT], az[IPT];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        tt[k] = (int64_t)blockIdx.x * BLOCK * IPT + k * BLOCK + threadIdx.x;
+        bi[k] = tt[k] < nt ? (targets ? (int64_t)targets[tt[k]] : tt[k]) : 0;
+        double4 p = pm[bi[k]];
+        xi[k] = p.x; yi[k] = p.y; zi[k] = p.z; mi[k] = p.w;
+        if (PN) { double4 v = vel[bi[k]]; vxi[k] = v.x; vyi[k] = v.y; vzi[k] = v.z; }
+        ax[k] = ay[k] = az[k] = 0.0;
+    }
+    for (int64_t base = j0; base < j1; base += BLOCK) {
+        const int64_t j = base + threadIdx.x;
+        __syncthreads();
+        sp[threadIdx.x] = j < j1 ? pm[j] : make_double4(1e300, 1e300, 1e300, 0.0);
+        if (PN) sv[threadIdx.x] = j < j1 ? vel[j] : make_double4(0, 0, 0, 0);
+        __syncthreads();
+#pragma unroll 4
+        for (int q = 0; q < BLOCK; ++q) {
+            const double4 pj = sp[q];
+#pragma unroll
+            for (int k = 0; k < IPT; ++k) {
+                double dx = pj.x - xi[k], dy = pj.y - yi[k], dz = pj.z - zi[k];
+                double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+                double inv = rsqrt(r2);
+                if (GUARD) inv = r2 > 0.0 ? inv : 0.0;
+                double inv2 = inv * inv;
+                double s = pj.w * inv * inv2;
+                ax[k] = fma(dx, s, ax[k]); ay[k] = fma(dy, s, ay[k]); az[k] = fma(dz, s, az[k]);
+                if (PN) {
+                    const double4 vj = sv[q];
+                    double nx = -dx * inv, ny = -dy * inv, nz = -dz * inv;
+                    double v1sq = vxi[k] * vxi[k] + vyi[k] * vyi[k] + vzi[k] * vzi[k];
+                    double v2sq = vj.x * vj.x + vj.y * vj.y + vj.z * vj.z;
+                    double v12 = vxi[k] * vj.x + vyi[k] * vj.y + vzi[k] * vj.z;
+                    double nv1 = nx * vxi[k] + ny * vyi[k] + nz * vzi[k];
+                    double nv2 = nx * vj.x + ny * vj.y + nz * vj.z;
+                    double A = -v1sq - 2.0 * v2sq + 4.0 * v12 + 1.5 * nv2 * nv2 + 5.0 * G * mi[k] * inv +
+                               4.0 * G * pj.w * inv;
+                    double B = 4.0 * nv1 - 3.0 * nv2;
+                    double f = pj.w * inv2 * inv_c2;  // G applied in store_result
+                    ax[k] += (nx * A + (vxi[k] - vj.x) * B) * f;
+                    ay[k] += (ny * A + (vyi[k] - vj.y) * B) * f;
+                    az[k] += (nz * A + (vzi[k] - vj.z) * B) * f;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < IPT; ++k)
+        if (tt[k] < nt) store_result(tt[k], bi[k], ax[k], ay[k], az[k], G, nslices, slice, nt, partial, acc, out3, kick);
+}
+
+// --------------------------------------------------------------- mixed path
+template <bool PN, bool GUARD>
+__global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
+    int64_t n, int64_t nt, const int32_t* __restrict__ targets, const float4* __restrict__ phi,
+    const float4* __restrict__ plo, const float4* __restrict__ vf, float G, float eps2, float inv_c2,
+    double Gd, int64_t slice_len, int nslices, double4* __restrict__ partial, double4* __restrict__ acc,
+    double* __restrict__ out3, KickArgs kick) {
+    __shared__ float4 sh[BLOCK];
+    __shared__ float4 sl[BLOCK];
+    __shared__ float4 sv[PN ? BLOCK : 1];
+    const int slice = blockIdx.y;
+    const int64_t j0 = (int64_t)slice * slice_len;
+    const int64_t j1 = min(n, j0 + slice_len);
+    int64_t tt[IPT], bi[IPT];
+    float xh[IPT], yh[IPT], zh[IPT], xl[IPT], yl[IPT], zl[IPT], mi[IPT];
+    float vxi[IPT], vyi[IPT], vzi[IPT], v1sq[IPT];
+    float ax[IPT], ay[IPT], az[IPT];
+    float px[IPT], py[IPT], pz[IPT];
+    CompSum cx[IPT], cy[IPT], cz[IPT];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        tt[k] = (int64_t)blockIdx.x * BLOCK * IPT + k * BLOCK + threadIdx.x;
+        bi[k] = tt[k] < nt ? (targets ? (int64_t)targets[tt[k]] : tt[k]) : 0;
+        float4 h = phi[bi[k]], l = plo[bi[k]];
+        xh[k] = h.x; yh[k] = h.y; zh[k] = h.z; mi[k] = h.w;
+        xl[k] = l.x; yl[k] = l.y; zl[k] = l.z;
+        if (PN) {
+            float4 v = vf[bi[k]];
+            vxi[k] = v.x; vyi[k] = v.y; vzi[k] = v.z;
+            v1sq[k] = v.x * v.x + v.y * v.y + v.z * v.z;
+        }
+        ax[k] = ay[k] = az[k] = 0.f;
+        px[k] = py[k] = pz[k] = 0.f;
+    }
+    for (int64_t base = j0; base < j1; base += BLOCK) {
+        const int64_t j = base + threadIdx.x;
+        __syncthreads();
+        if (j < j1) {
+            sh[threadIdx.x] = phi[j];
+            sl[threadIdx.x] = plo[j];
+            if (PN) sv[threadIdx.x] = vf[j];
+        } else {
+            sh[threadIdx.x] = make_float4(PAD_POS, PAD_POS, PAD_POS, 0.f);
+            sl[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (PN) sv[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int c0 = 0; c0 < BLOCK; c0 += FOLD) {
+#pragma unroll 8
+            for (int q = c0; q < c0 + FOLD; ++q) {
+                const float4 h = sh[q];
+                const float4 l = sl[q];
+#pragma unroll
+                for (int k = 0; k < IPT; ++k) {
+                    float dx = (h.x - xh[k]) + (l.x - xl[k]);
+                    float dy = (h.y - yh[k]) + (l.y - yl[k]);
+                    float dz = (h.z - zh[k]) + (l.z - zl[k]);
+                    float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+                    float inv = rsqrt_approx(r2);
+                    if (GUARD) inv = r2 > 0.f ? inv : 0.f;
+                    float inv2 = inv * inv;
+                    float s = h.w * inv * inv2;
+                    ax[k] = fmaf(dx, s, ax[k]); ay[k] = fmaf(dy, s, ay[k]); az[k] = fmaf(dz, s, az[k]);
+                    if (PN) {
+                        const float4 vj = sv[q];
+                        float nx = -dx * inv, ny = -dy * inv, nz = -dz * inv;
+                        float v2sq = vj.x * vj.x + vj.y * vj.y + vj.z * vj.z;
+                        float v12 = vxi[k] * vj.x + vyi[k] * vj.y + vzi[k] * vj.z;
+                        float nv1 = nx * vxi[k] + ny * vyi[k] + nz * vzi[k];
+                        float nv2 = nx * vj.x + ny * vj.y + nz * vj.z;
+                        float A = -v1sq[k] - 2.f * v2sq + 4.f * v12 + 1.5f * nv2 * nv2 +
+                                  (5.f * mi[k] + 4.f * h.w) * G * inv;
+                        float B = 4.f * nv1 - 3.f * nv2;
+                        float f = h.w * inv2 * inv_c2;
+                        px[k] = fmaf(nx * A + (vxi[k] - vj.x) * B, f, px[k]);
+                        py[k] = fmaf(ny * A + (vyi[k] - vj.y) * B, f, py[k]);
+                        pz[k] = fmaf(nz * A + (vzi[k] - vj.z) * B, f, pz[k]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < IPT; ++k) {
+                cx[k].add(ax[k]); cy[k].add(ay[k]); cz[k].add(az[k]);
+                ax[k] = ay[k] = az[k] = 0.f;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < IPT; ++k)
+        if (tt[k] < nt)
+            store_result(tt[k], bi[k], cx[k].value() + (double)px[k], cy[k].value() + (double)py[k],
+                         cz[k].value() + (double)pz[k], Gd, nslices, slice, nt, partial, acc, out3, kick);
+}
+
+__global__ void k_reduce_slices(int64_t nt, int nslices, const double4* __restrict__ partial,
+                                const int32_t* __restrict__ targets, double G, double4* __restrict__ acc,
+                                double* __restrict__ out3, KickArgs kick) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nt; t += (int64_t)gridDim.x * blockDim.x) {
+        double ax = 0, ay = 0, az = 0;
+        for (int s = 0; s < nslices; ++s) {
+            double4 p = partial[(int64_t)s * nt + t];
+            ax += p.x; ay += p.y; az += p.z;
+        }
+        int64_t body = targets ? (int64_t)targets[t] : t;
+        store_result(t, body, ax, ay, az, G, 1, 0, nt, nullptr, acc, out3, kick);
+    }
+}
+
+template <bool PN, bool GUARD>
+void launch_fp64(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32_t* tg, aster_ctx* c,
+                 const aster_params* p, int64_t slice_len, int ns, double4* partial, double* out3, KickArgs kick) {
+    const double inv_c2 = PN ? 1.0 / (p->c * p->c) : 0.0;
+    k_allpairs_fp64<PN, GUARD><<<grid, BLOCK, 0, st>>>(n, nt, tg, c->pm.as<double4>(), c->vel.as<double4>(), p->G,
+                                                        p->eps2, inv_c2, slice_len, ns, partial,
+                                                        c->acc.as<double4>(), out3, kick);
+}
+
+template <bool PN, bool GUARD>
+void launch_mixed(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32_t* tg, aster_ctx* c,
+                  const aster_params* p, int64_t slice_len, int ns, double4* partial, double* out3, KickArgs kick) {
+    const float inv_c2 = PN ? (float)(1.0 / (p->c * p->c)) : 0.f;
+    k_allpairs_mixed<PN, GUARD><<<grid, BLOCK, 0, st>>>(
+        n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), (float)p->G, (float)p->eps2,
+        inv_c2, p->G, slice_len, ns, partial, c->acc.as<double4>(), out3, kick);
+}
+
+}  // namespace
+
+// Launch one all-pairs evaluation. Targets: every body (targets_dev == null,
+// nt == n) or an explicit list. Output: ctx->acc (out_dev == null) with an
+// optional closing kick, or out_dev[nt*3].
+int aster_allpairs_launch(aster_ctx* c, const aster_params* p, int precision, bool closing_kick, int64_t nt,
+                          const int32_t* targets_dev, double* out_dev) {
+    const int64_t n = c->n;
+    const int64_t per_block = (int64_t)BLOCK * IPT;
+    const int64_t iblocks = (nt + per_block - 1) / per_block;
+    // j-slices so that small n still fill the GPU (>= 2 blocks per SM).
+    int64_t want = 2 * (int64_t)c->sm_count;
+    int64_t ns = iblocks >= want ? 1 : (want + iblocks - 1) / iblocks;
+    int64_t max_ns = (n + BLOCK - 1) / BLOCK;
+    if (ns > max_ns) ns = max_ns;
+    if (ns > 64) ns = 64;
+    if (ns < 1) ns = 1;
+    int64_t slice_len = ((n + ns - 1) / ns + BLOCK - 1) / BLOCK * BLOCK;
+    ns = (n + slice_len - 1) / slice_len;
+    double4* partial = nullptr;
+    if (ns > 1) {
+        ASTER_TRY(c->scratch.ensure((size_t)ns * nt * sizeof(double4)));
+        partial = c->scratch.as<double4>();
+    }
+    KickArgs kick{closing_kick && !out_dev, 0.5 * p->dt, c->vel.as<double4>()};
+    dim3 grid((unsigned)iblocks, (unsigned)ns);
+    const bool pn = (p->force_law & ASTER_PN1) != 0;
+    const bool guard = !(p->eps2 > 0.0);
+    if (precision == ASTER_FP64) {
+        if (pn) { if (guard) launch_fp64<true, true>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
+                  else launch_fp64<true, false>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick); }
+        else    { if (guard) launch_fp64<false, true>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
+                  else launch_fp64<false, false>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick); }
+    } else if (precision == ASTER_MIXED) {
+        if (pn) { if (guard) launch_mixed<true, true>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
+                  else launch_mixed<true, false>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick); }
+        else    { if (guard) launch_mixed<false, true>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
+                  else launch_mixed<false, false>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick); }
+    } else {
+        return ASTER_ERR_INVALID_ARG;
+    }
+    ASTER_CUDA(cudaGetLastError());
+    c->stats.kernels += 1;
+    if (ns > 1) {
+        int g = (int)((nt + 255) / 256);
+        k_reduce_slices<<<g, 256, 0, c->stream>>>(nt, (int)ns, partial, targets_dev, p->G, c->acc.as<double4>(),
+                                                  out_dev, kick);
+        ASTER_CUDA(cudaGetLastError());
+        c->stats.kernels += 1;
+    }
+    c->stats.interactions += (double)nt * (double)n;
+    return ASTER_OK;
+}
+
+extern "C" int aster_allpairs(aster_ctx* c, const aster_params* p, int precision, double* acc_out) {
+    if (!c) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (c->n <= 0) return ASTER_ERR_NO_STATE;
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    cudaEventRecord(c->ev[0], c->stream);
+    ASTER_TRY(aster_allpairs_launch(c, p, precision, false, c->n, nullptr, nullptr));
+    cudaEventRecord(c->ev[1], c->stream);
+    ASTER_TRY(aster_finish(c));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = c->stats.ms_force = ms;
+    c->acc_valid = true;
+    return aster_copy_acc_out(c, acc_out);
+}
+
+extern "C" int aster_allpairs_targets(aster_ctx* c, const aster_params* p, int precision, int64_t nt,
+                                      const int32_t* targets, double* acc_out) {
+    if (!c || !targets || !acc_out || nt <= 0) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (c->n <= 0) return ASTER_ERR_NO_STATE;
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    for (int64_t t = 0; t < nt; ++t)
+        if (targets[t] < 0 || targets[t] >= c->n) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_begin(c));
+    ASTER_TRY(c->targets.ensure((size_t)nt * sizeof(int32_t) + (size_t)nt * 3 * sizeof(double) + 256));
+    int32_t* tg = c->targets.as<int32_t>();
+    double* out = reinterpret_cast<double*>(c->targets.as<char>() + ((nt * sizeof(int32_t) + 255) / 256) * 256);
+    ASTER_CUDA(cudaMemcpyAsync(tg, targets, (size_t)nt * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    ASTER_TRY(aster_allpairs_launch(c, p, precision, false, nt, tg, out));
+    ASTER_CUDA(cudaMemcpyAsync(acc_out, out, (size_t)nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return aster_finish(c);
+}

@@ -1,0 +1,129 @@
+// Internal declarations shared by the CUDA translation units of
+// libaster_cuda.so. Not part of the C ABI (include/aster_cuda.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+
+#include "../../include/aster_cuda.h"
+
+// Device error flag bits (ctx->err_dev). Kernels OR a bit in and stop the
+// affected work; the host turns the first bit found into a status code.
+#define ASTER_DEVERR_STACK 0x1
+#define ASTER_DEVERR_TREE 0x2
+#define ASTER_DEVERR_NONFINITE 0x4
+#define ASTER_DEVERR_CANCEL 0x8
+#define ASTER_DEVERR_LIST 0x10
+
+#define ASTER_TRY(expr)                                   \
+    do {                                                  \
+        int _st = (expr);                                 \
+        if (_st != ASTER_OK) return _st;                  \
+    } while (0)
+
+#define ASTER_CUDA(expr)                                  \
+    do {                                                  \
+        cudaError_t _e = (expr);                          \
+        if (_e != cudaSuccess) return aster_cuda_fail(_e, #expr, __FILE__, __LINE__); \
+    } while (0)
+
+int aster_cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// LBVH device arrays (sized for n bodies, 2n-1 nodes).
+struct LbvhBufs {
+    DevBuf codes, codes_alt, sorted_codes, perm, perm_alt, hist, digit_off;
+    DevBuf left, right, parent, rlo, rhi, counters;
+    DevBuf node_cm, bmin, bmax;  // node_cm: double4 (com x, y, z, mass)
+    DevBuf node_hi, node_lo, child;
+    int64_t n = 0;
+    bool built = false;
+    double box = 0.0;
+};
+
+struct aster_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int64_t n = 0;
+    DevBuf pm;    // double4 (x, y, z, m), input order
+    DevBuf vel;   // double4 (vx, vy, vz, 0)
+    DevBuf acc;   // double4 (ax, ay, az, 0): cached acceleration
+    DevBuf phi;   // float4 (x_hi, y_hi, z_hi, m): round-to-nearest of x
+    DevBuf plo;   // float4 (x - x_hi, ..., 0): double-single low parts
+    DevBuf vf;    // float4 (vx, vy, vz, 0) for PN terms in FP32
+    DevBuf scratch;   // j-split partial accumulators, reductions
+    DevBuf targets;   // target list for aster_allpairs_targets
+    DevBuf stage;     // device staging for AoS <-> SoA-4 conversion
+    DevBuf red;       // small reduction buffers (box, energy)
+    bool acc_valid = false;
+    int* err_dev = nullptr;     // device error flags
+    int* err_host = nullptr;    // pinned copy
+    int* stack_hw_dev = nullptr;  // tree-walk stack high-water mark
+    LbvhBufs tree;
+    aster_stats stats{};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+// ---- shared host helpers (context.cu) -------------------------------------
+int aster_check_params(const aster_params* p);
+int aster_begin(aster_ctx* ctx);                // clears the device error flag
+int aster_finish(aster_ctx* ctx);               // syncs, turns flags into status
+int aster_refresh_mixed(aster_ctx* ctx);        // rebuild phi/plo/vf from pm/vel
+int aster_copy_acc_out(aster_ctx* ctx, double* acc_out);
+
+// ---- kernels exposed across translation units ------------------------------
+// allpairs.cu
+int aster_allpairs_launch(aster_ctx* ctx, const aster_params* p, int precision,
+                          bool closing_kick, int64_t nt, const int32_t* targets_dev,
+                          double* out_dev /* nt*3 or null: write ctx->acc */);
+// integrate.cu
+int aster_kick_drift_launch(aster_ctx* ctx, const aster_params* p, bool want_box, bool want_mixed);
+// lbvh.cu
+int aster_lbvh_build_dev(aster_ctx* ctx, const aster_params* p, bool box_ready);
+int aster_lbvh_walk_launch(aster_ctx* ctx, const aster_params* p, int precision,
+                           bool closing_kick, int32_t* group_counts_dev);
+
+// ---- device helpers --------------------------------------------------------
+__device__ __forceinline__ void ds_split(double x, float& hi, float& lo) {
+    hi = __double2float_rn(x);
+    lo = __double2float_rn(__dsub_rn(x, (double)hi));
+}
+
+// Error-free transformation a + b = s + e (Knuth two-sum, FP32), written with
+// explicitly rounded intrinsics so that no FMA contraction can cancel it.
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    float bp = __fsub_rn(s, a);
+    float ap = __fsub_rn(s, bp);
+    e = __fadd_rn(__fsub_rn(a, ap), __fsub_rn(b, bp));
+}
+
+// Compensated accumulator: value = hi + lo. add() folds one FP32 partial in.
+struct CompSum {
+    float hi = 0.f, lo = 0.f;
+    __device__ __forceinline__ void add(float x) {
+        float s, e;
+        two_sum(hi, x, s, e);
+        hi = s;
+        lo = __fadd_rn(lo, e);
+    }
+    __device__ __forceinline__ double value() const { return (double)hi + (double)lo; }
+};
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}

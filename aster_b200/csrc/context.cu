@@ -1,0 +1,279 @@
+// Context, state transfer, error handling and the shared host helpers of the
+// C ABI (include/aster_cuda.h). The state upload/download replace the
+// reference's Simulation::load_gpu_buffers / read_bodies_gpu
+// (src/utils/builder_endpoint.cpp:102-119, 424-434): the reference copies
+// std::vector<vec3> (AoS FP64) into OpenCL buffers; here AoS FP64 host arrays
+// are packed into 32-byte double4 records (x, y, z, m) and (vx, vy, vz, 0) so
+// that every body is one aligned 32-byte load.
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "aster_internal.cuh"
+
+static thread_local char g_last_error[256] = "";
+
+int aster_cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+    snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    return e == cudaErrorMemoryAllocation ? ASTER_ERR_OOM : ASTER_ERR_CUDA;
+}
+
+int DevBuf::ensure(size_t want) {
+    if (want <= bytes && ptr) return ASTER_OK;
+    release();
+    size_t b = want < 256 ? 256 : want;
+    cudaError_t e = cudaMalloc(&ptr, b);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        bytes = 0;
+        cudaGetLastError();
+        return aster_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+    }
+    bytes = b;
+    return ASTER_OK;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+extern "C" const char* aster_strerror(int s) {
+    switch (s) {
+        case ASTER_OK: return "ok";
+        case ASTER_ERR_INVALID_ARG: return "invalid argument";
+        case ASTER_ERR_CUDA: return g_last_error[0] ? g_last_error : "CUDA runtime error";
+        case ASTER_ERR_OOM: return "device out of memory";
+        case ASTER_ERR_NO_STATE: return "no body state uploaded";
+        case ASTER_ERR_STACK: return "tree-walk stack overflow";
+        case ASTER_ERR_TREE: return "bottom-up climb exceeded level cap";
+        case ASTER_ERR_NONFINITE: return "non-finite value in state or result";
+        case ASTER_ERR_CANCELLED: return "cancelled";
+        case ASTER_ERR_UNSUPPORTED: return "unsupported option";
+        case ASTER_ERR_TOO_LARGE: return "size beyond fixed capacity";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int aster_version(void) { return 10000; }
+
+int aster_check_params(const aster_params* p) {
+    if (!p) return ASTER_ERR_INVALID_ARG;
+    if (!std::isfinite(p->G) || !std::isfinite(p->eps2) || p->eps2 < 0.0) return ASTER_ERR_INVALID_ARG;
+    if (!std::isfinite(p->dt) || !std::isfinite(p->theta) || p->theta < 0.0) return ASTER_ERR_INVALID_ARG;
+    if ((p->force_law & ASTER_PN1) && !(std::isfinite(p->c) && p->c > 0.0)) return ASTER_ERR_INVALID_ARG;
+    if (p->force_law & ~(ASTER_NEWTON | ASTER_PN1)) return ASTER_ERR_UNSUPPORTED;
+    if (p->morton_bits != 30 && p->morton_bits != 63) return ASTER_ERR_INVALID_ARG;
+    if (p->compat_mode != 0 && p->compat_mode != 1) return ASTER_ERR_INVALID_ARG;
+    if (p->compat_mode == 1 && p->morton_bits != 30) return ASTER_ERR_UNSUPPORTED;
+    if (p->reserved != 0) return ASTER_ERR_INVALID_ARG;
+    return ASTER_OK;
+}
+
+extern "C" int aster_ctx_create(aster_ctx** out, int device, void* stream) {
+    if (!out) return ASTER_ERR_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    ASTER_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return ASTER_ERR_INVALID_ARG;
+    ASTER_CUDA(cudaSetDevice(device));
+    aster_ctx* c = new (std::nothrow) aster_ctx();
+    if (!c) return ASTER_ERR_OOM;
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete c; return aster_cuda_fail(e, "cudaStreamCreate", __FILE__, __LINE__); }
+        c->own_stream = true;
+    }
+    cudaError_t e = cudaMalloc(&c->err_dev, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaHostAlloc(&c->err_host, 2 * sizeof(int), cudaHostAllocDefault);
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    if (e != cudaSuccess) {
+        aster_ctx_destroy(c);
+        return aster_cuda_fail(e, "aster_ctx_create", __FILE__, __LINE__);
+    }
+    c->stack_hw_dev = c->err_dev + 1;
+    cudaMemset(c->err_dev, 0, 2 * sizeof(int));
+    *out = c;
+    return ASTER_OK;
+}
+
+extern "C" int aster_ctx_destroy(aster_ctx* c) {
+    if (!c) return ASTER_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DevBuf* bufs[] = {&c->pm, &c->vel, &c->acc, &c->phi, &c->plo, &c->vf, &c->scratch, &c->targets,
+                      &c->stage, &c->red,
+                      &c->tree.codes, &c->tree.codes_alt, &c->tree.sorted_codes, &c->tree.perm,
+                      &c->tree.perm_alt, &c->tree.hist, &c->tree.digit_off, &c->tree.left, &c->tree.right,
+                      &c->tree.parent, &c->tree.rlo, &c->tree.rhi, &c->tree.counters, &c->tree.node_cm,
+                      &c->tree.bmin, &c->tree.bmax, &c->tree.node_hi,
+                      &c->tree.node_lo, &c->tree.child};
+    for (DevBuf* b : bufs) b->release();
+    for (int i = 0; i < 4; ++i)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->err_dev) cudaFree(c->err_dev);
+    if (c->err_host) cudaFreeHost(c->err_host);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ASTER_OK;
+}
+
+int aster_begin(aster_ctx* c) {
+    ASTER_CUDA(cudaSetDevice(c->device));
+    ASTER_CUDA(cudaMemsetAsync(c->err_dev, 0, 2 * sizeof(int), c->stream));
+    return ASTER_OK;
+}
+
+int aster_finish(aster_ctx* c) {
+    ASTER_CUDA(cudaMemcpyAsync(c->err_host, c->err_dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    ASTER_CUDA(cudaStreamSynchronize(c->stream));
+    ASTER_CUDA(cudaGetLastError());
+    int f = c->err_host[0];
+    c->stats.max_stack = c->err_host[1];
+    if (f & ASTER_DEVERR_STACK) return ASTER_ERR_STACK;
+    if (f & ASTER_DEVERR_LIST) return ASTER_ERR_STACK;
+    if (f & ASTER_DEVERR_TREE) return ASTER_ERR_TREE;
+    if (f & ASTER_DEVERR_CANCEL) return ASTER_ERR_CANCELLED;
+    if (f & ASTER_DEVERR_NONFINITE) return ASTER_ERR_NONFINITE;
+    return ASTER_OK;
+}
+
+// ---- packing kernels --------------------------------------------------------
+__global__ void k_pack_state(int64_t n, const double* __restrict__ pos, const double* __restrict__ vel,
+                             const double* __restrict__ mass, double4* __restrict__ pm,
+                             double4* __restrict__ v4, float4* __restrict__ phi,
+                             float4* __restrict__ plo, float4* __restrict__ vf, int* err) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2], m = mass[i];
+        double vx = 0, vy = 0, vz = 0;
+        if (vel) { vx = vel[3 * i]; vy = vel[3 * i + 1]; vz = vel[3 * i + 2]; }
+        if (!(isfinite(x) && isfinite(y) && isfinite(z) && isfinite(m) && isfinite(vx) && isfinite(vy) &&
+              isfinite(vz)))
+            atomicOr(err, ASTER_DEVERR_NONFINITE);
+        pm[i] = make_double4(x, y, z, m);
+        v4[i] = make_double4(vx, vy, vz, 0.0);
+        float4 h, l;
+        ds_split(x, h.x, l.x);
+        ds_split(y, h.y, l.y);
+        ds_split(z, h.z, l.z);
+        h.w = __double2float_rn(m);
+        l.w = 0.f;
+        phi[i] = h;
+        plo[i] = l;
+        vf[i] = make_float4((float)vx, (float)vy, (float)vz, 0.f);
+    }
+}
+
+__global__ void k_refresh_mixed(int64_t n, const double4* __restrict__ pm, const double4* __restrict__ v4,
+                                float4* __restrict__ phi, float4* __restrict__ plo, float4* __restrict__ vf) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double4 p = pm[i];
+        double4 v = v4[i];
+        float4 h, l;
+        ds_split(p.x, h.x, l.x);
+        ds_split(p.y, h.y, l.y);
+        ds_split(p.z, h.z, l.z);
+        h.w = __double2float_rn(p.w);
+        l.w = 0.f;
+        phi[i] = h;
+        plo[i] = l;
+        vf[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+    }
+}
+
+__global__ void k_unpack3(int64_t n, const double4* __restrict__ src, double* __restrict__ dst) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double4 v = src[i];
+        dst[3 * i] = v.x;
+        dst[3 * i + 1] = v.y;
+        dst[3 * i + 2] = v.z;
+    }
+}
+
+static int grid_for(aster_ctx* c, int64_t n, int block) {
+    int64_t g = (n + block - 1) / block;
+    int64_t cap = (int64_t)c->sm_count * 16;
+    return (int)(g < cap ? (g > 0 ? g : 1) : cap);
+}
+
+int aster_refresh_mixed(aster_ctx* c) {
+    k_refresh_mixed<<<grid_for(c, c->n, 256), 256, 0, c->stream>>>(
+        c->n, c->pm.as<double4>(), c->vel.as<double4>(), c->phi.as<float4>(), c->plo.as<float4>(),
+        c->vf.as<float4>());
+    ASTER_CUDA(cudaGetLastError());
+    return ASTER_OK;
+}
+
+extern "C" int aster_state_upload(aster_ctx* c, int64_t n, const double* pos, const double* vel,
+                                  const double* mass) {
+    if (!c || !pos || !mass || n <= 0 || n > (int64_t)1 << 30) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_begin(c));
+    const size_t n4d = (size_t)n * sizeof(double4), n4f = (size_t)n * sizeof(float4);
+    ASTER_TRY(c->pm.ensure(n4d));
+    ASTER_TRY(c->vel.ensure(n4d));
+    ASTER_TRY(c->acc.ensure(n4d));
+    ASTER_TRY(c->phi.ensure(n4f));
+    ASTER_TRY(c->plo.ensure(n4f));
+    ASTER_TRY(c->vf.ensure(n4f));
+    const size_t v3 = (size_t)n * 3 * sizeof(double);
+    ASTER_TRY(c->stage.ensure(2 * v3 + (size_t)n * sizeof(double)));
+    double* sp = c->stage.as<double>();
+    double* sv = sp + 3 * n;
+    double* sm = sv + 3 * n;
+    ASTER_CUDA(cudaMemcpyAsync(sp, pos, v3, cudaMemcpyHostToDevice, c->stream));
+    if (vel) ASTER_CUDA(cudaMemcpyAsync(sv, vel, v3, cudaMemcpyHostToDevice, c->stream));
+    ASTER_CUDA(cudaMemcpyAsync(sm, mass, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    k_pack_state<<<grid_for(c, n, 256), 256, 0, c->stream>>>(n, sp, vel ? sv : nullptr, sm, c->pm.as<double4>(),
+                                                             c->vel.as<double4>(), c->phi.as<float4>(),
+                                                             c->plo.as<float4>(), c->vf.as<float4>(), c->err_dev);
+    ASTER_CUDA(cudaGetLastError());
+    ASTER_CUDA(cudaMemsetAsync(c->acc.ptr, 0, n4d, c->stream));
+    c->n = n;
+    c->acc_valid = false;
+    c->tree.built = false;
+    int st = aster_finish(c);
+    if (st != ASTER_OK) c->n = 0;
+    return st;
+}
+
+extern "C" int aster_state_download(aster_ctx* c, double* pos, double* vel, double* acc) {
+    if (!c) return ASTER_ERR_INVALID_ARG;
+    if (c->n <= 0) return ASTER_ERR_NO_STATE;
+    ASTER_CUDA(cudaSetDevice(c->device));
+    const int64_t n = c->n;
+    const size_t v3 = (size_t)n * 3 * sizeof(double);
+    ASTER_TRY(c->stage.ensure(3 * v3));
+    double* st = c->stage.as<double>();
+    const DevBuf* srcs[3] = {&c->pm, &c->vel, &c->acc};
+    double* dsts[3] = {pos, vel, acc};
+    for (int k = 0; k < 3; ++k) {
+        if (!dsts[k]) continue;
+        k_unpack3<<<grid_for(c, n, 256), 256, 0, c->stream>>>(n, srcs[k]->as<double4>(), st + 3 * n * k);
+        ASTER_CUDA(cudaGetLastError());
+        ASTER_CUDA(cudaMemcpyAsync(dsts[k], st + 3 * n * k, v3, cudaMemcpyDeviceToHost, c->stream));
+    }
+    ASTER_CUDA(cudaStreamSynchronize(c->stream));
+    return ASTER_OK;
+}
+
+extern "C" int aster_state_size(aster_ctx* c, int64_t* n) {
+    if (!c || !n) return ASTER_ERR_INVALID_ARG;
+    *n = c->n;
+    return ASTER_OK;
+}
+
+int aster_copy_acc_out(aster_ctx* c, double* acc_out) {
+    if (!acc_out) return ASTER_OK;
+    return aster_state_download(c, nullptr, nullptr, acc_out);
+}
+
+extern "C" int aster_get_stats(aster_ctx* c, aster_stats* out) {
+    if (!c || !out) return ASTER_ERR_INVALID_ARG;
+    *out = c->stats;
+    return ASTER_OK;
+}

@@ -1,0 +1,271 @@
+// Kick-drift-kick leapfrog driver and FP64 diagnostics.
+//
+// Replaces update_leapfrog / update_leapfrog_gpu_3d + the `leapfrog` OpenCL
+// kernel (src/physics/tool_chain_impl.cpp:169-185, src/utils/updater.cpp:53-87,
+// include/Aster/kernels/leapfrog.cl.h:9-29). The reference evaluates the force
+// twice per step (before and after the drift); the map it implements is
+//   x' = x + v dt + a(x) dt^2/2,  v' = v + (a(x) + a(x')) dt/2,
+// which is kick-drift-kick with a(x) reused from the previous step. Here one
+// step is two launches:
+//   k_kick_drift : v += a dt/2; x += v dt; (mixed: refresh the double-single
+//                  copies; LBVH: max |coordinate| for the Morton cube)
+//   force kernel : a = A(x) and, fused in its epilogue, v += a dt/2.
+// Positions and velocities stay FP64.
+//
+// Energy replaces Graphs::get_total_energy (src/utils/collectors.cpp:19-53).
+#include <algorithm>
+#include <cmath>
+
+#include "aster_internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template <bool MIXED, bool BOX>
+__global__ void __launch_bounds__(256) k_kick_drift(int64_t n, double half_dt, double dt,
+                                                    double4* __restrict__ pm, double4* __restrict__ vel,
+                                                    const double4* __restrict__ acc, float4* __restrict__ phi,
+                                                    float4* __restrict__ plo, float4* __restrict__ vf,
+                                                    unsigned long long* __restrict__ box_bits) {
+    double bmax = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double4 p = pm[i], v = vel[i];
+        const double4 a = acc[i];
+        v.x += a.x * half_dt; v.y += a.y * half_dt; v.z += a.z * half_dt;
+        p.x += v.x * dt; p.y += v.y * dt; p.z += v.z * dt;
+        pm[i] = p;
+        vel[i] = v;
+        if (MIXED) {
+            float4 h, l;
+            ds_split(p.x, h.x, l.x);
+            ds_split(p.y, h.y, l.y);
+            ds_split(p.z, h.z, l.z);
+            h.w = __double2float_rn(p.w);
+            l.w = 0.f;
+            phi[i] = h;
+            plo[i] = l;
+            vf[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+        }
+        if (BOX) bmax = fmax(bmax, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))));
+    }
+    if (BOX) {
+        __shared__ double red[8];
+        bmax = warp_max(bmax);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bmax;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+            v = warp_max(v);
+            // non-negative doubles order like their bit patterns
+            if (threadIdx.x == 0) atomicMax(box_bits, (unsigned long long)__double_as_longlong(v));
+        }
+    }
+}
+
+// FP64 energy/momentum: per-block partials (ke, pe, px, py, pz), then one
+// block adds them in a fixed order (deterministic).
+template <bool REF_FORM>
+__global__ void __launch_bounds__(256) k_energy_partial(int64_t n, const double4* __restrict__ pm,
+                                                        const double4* __restrict__ vel, double eps2,
+                                                        double* __restrict__ part) {
+    __shared__ double4 sp[256];
+    __shared__ double red[5][8];
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double4 pi = i < n ? pm[i] : make_double4(0, 0, 0, 0);
+    double pot = 0.0;
+    for (int64_t base = 0; base < n; base += 256) {
+        __syncthreads();
+        const int64_t j = base + threadIdx.x;
+        sp[threadIdx.x] = j < n ? pm[j] : make_double4(0, 0, 0, 0);
+        __syncthreads();
+        const int lim = (int)min((int64_t)256, n - base);
+        for (int q = 0; q < lim; ++q) {
+            if (base + q == i) continue;
+            const double4 pj = sp[q];
+            double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+            double r2 = dx * dx + dy * dy + dz * dz;
+            double inv = REF_FORM ? 1.0 / (sqrt(r2) + eps2) : 1.0 / sqrt(r2 + eps2);
+            pot += pj.w * inv;
+        }
+    }
+    double v[5] = {0, 0, 0, 0, 0};
+    if (i < n) {
+        const double4 vi = vel[i];
+        v[0] = 0.5 * pi.w * (vi.x * vi.x + vi.y * vi.y + vi.z * vi.z);
+        v[1] = -0.5 * pi.w * pot;
+        v[2] = pi.w * vi.x; v[3] = pi.w * vi.y; v[4] = pi.w * vi.z;
+    }
+    for (int k = 0; k < 5; ++k) {
+        double x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double s = 0;
+        for (int w = 0; w < 8; ++w) s += red[threadIdx.x][w];
+        part[blockIdx.x * 5 + threadIdx.x] = s;
+    }
+}
+
+__global__ void k_energy_final(int nblocks, const double* __restrict__ part, double G, double* __restrict__ out) {
+    // out[0] = energy, out[1..3] = momentum; 5 threads, fixed order
+    __shared__ double s[5];
+    if (threadIdx.x < 5) {
+        double a = 0;
+        for (int b = 0; b < nblocks; ++b) a += part[b * 5 + threadIdx.x];
+        s[threadIdx.x] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        out[0] = s[0] + G * s[1];
+        out[1] = s[2]; out[2] = s[3]; out[3] = s[4];
+    }
+}
+
+}  // namespace
+
+int aster_kick_drift_launch(aster_ctx* c, const aster_params* p, bool want_box, bool want_mixed) {
+    const int64_t n = c->n;
+    int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 8);
+    if (grid < 1) grid = 1;
+    unsigned long long* box = nullptr;
+    if (want_box) {
+        ASTER_TRY(c->red.ensure(4096));
+        box = c->red.as<unsigned long long>();
+        ASTER_CUDA(cudaMemsetAsync(box, 0, sizeof(unsigned long long), c->stream));
+    }
+    auto* pm = c->pm.as<double4>();
+    auto* v = c->vel.as<double4>();
+    auto* a = c->acc.as<double4>();
+    const double h = 0.5 * p->dt, dt = p->dt;
+    if (want_mixed && want_box)
+        k_kick_drift<true, true><<<grid, 256, 0, c->stream>>>(n, h, dt, pm, v, a, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), box);
+    else if (want_mixed)
+        k_kick_drift<true, false><<<grid, 256, 0, c->stream>>>(n, h, dt, pm, v, a, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), box);
+    else if (want_box)
+        k_kick_drift<false, true><<<grid, 256, 0, c->stream>>>(n, h, dt, pm, v, a, nullptr, nullptr, nullptr, box);
+    else
+        k_kick_drift<false, false><<<grid, 256, 0, c->stream>>>(n, h, dt, pm, v, a, nullptr, nullptr, nullptr, box);
+    ASTER_CUDA(cudaGetLastError());
+    c->stats.kernels += 1;
+    return ASTER_OK;
+}
+
+// Per-phase device timing of a time-stepping call: an event pair around every
+// build and every force launch, summed after the final synchronisation.
+struct PhaseTimer {
+    static constexpr int kMax = 2048;
+    cudaEvent_t ev[2 * kMax];
+    int used = 0;
+    bool ok = true;
+    ~PhaseTimer() {
+        for (int i = 0; i < used; ++i) cudaEventDestroy(ev[i]);
+    }
+    int mark(cudaStream_t s) {  // returns the event index, -1 if out of slots
+        if (used >= 2 * kMax || cudaEventCreate(&ev[used]) != cudaSuccess) return -1;
+        cudaEventRecord(ev[used], s);
+        return used++;
+    }
+    double span(int a, int b) const {
+        float ms = 0.f;
+        if (a < 0 || b < 0 || cudaEventElapsedTime(&ms, ev[a], ev[b]) != cudaSuccess) return 0.0;
+        return ms;
+    }
+};
+
+static int force_eval(aster_ctx* c, const aster_params* p, int solver, int precision, bool closing_kick,
+                      bool box_ready, PhaseTimer* tm, double* ms_build, double* ms_force, int* pairs) {
+    int e0 = tm ? tm->mark(c->stream) : -1;
+    if (solver == ASTER_SOLVER_ALLPAIRS) {
+        ASTER_TRY(aster_allpairs_launch(c, p, precision, closing_kick, c->n, nullptr, nullptr));
+        if (tm) pairs[0] = e0, pairs[1] = e0, pairs[2] = tm->mark(c->stream);
+        return ASTER_OK;
+    }
+    ASTER_TRY(aster_lbvh_build_dev(c, p, box_ready));
+    int e1 = tm ? tm->mark(c->stream) : -1;
+    ASTER_TRY(aster_lbvh_walk_launch(c, p, precision, closing_kick, nullptr));
+    if (tm) pairs[0] = e0, pairs[1] = e1, pairs[2] = tm->mark(c->stream);
+    (void)ms_build;
+    (void)ms_force;
+    return ASTER_OK;
+}
+
+extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps) {
+    if (!c || nsteps < 0) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (c->n <= 0) return ASTER_ERR_NO_STATE;
+    if (solver != ASTER_SOLVER_ALLPAIRS && solver != ASTER_SOLVER_LBVH) return ASTER_ERR_INVALID_ARG;
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    if (solver == ASTER_SOLVER_LBVH && (p->force_law & ASTER_PN1)) return ASTER_ERR_UNSUPPORTED;
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    const bool mixed_ap = solver == ASTER_SOLVER_ALLPAIRS && precision == ASTER_MIXED;
+    // phase timing only when the event budget covers every step
+    PhaseTimer* tm = (nsteps + 1) * 3 <= 2 * PhaseTimer::kMax ? new PhaseTimer() : nullptr;
+    int marks[3 * (PhaseTimer::kMax / 3 + 2)][3];
+    int nm = 0;
+    ASTER_TRY(c->red.ensure(4096));
+    unsigned long long* inter = c->red.as<unsigned long long>() + 64;  // walk interaction counter
+    ASTER_CUDA(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), c->stream));
+    cudaEventRecord(c->ev[0], c->stream);
+    if (!c->acc_valid) {
+        if (mixed_ap) ASTER_TRY(aster_refresh_mixed(c));
+        ASTER_TRY(force_eval(c, p, solver, precision, false, false, tm, nullptr, nullptr, marks[nm]));
+        if (tm) ++nm;
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        ASTER_TRY(aster_kick_drift_launch(c, p, solver == ASTER_SOLVER_LBVH, mixed_ap));
+        ASTER_TRY(force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, marks[nm]));
+        if (tm) ++nm;
+    }
+    cudaEventRecord(c->ev[1], c->stream);
+    unsigned long long ic = 0;
+    if (solver == ASTER_SOLVER_LBVH)
+        ASTER_CUDA(cudaMemcpyAsync(&ic, inter, sizeof(ic), cudaMemcpyDeviceToHost, c->stream));
+    int st = aster_finish(c);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    if (solver == ASTER_SOLVER_LBVH) c->stats.interactions = (double)ic;
+    if (tm) {
+        for (int k = 0; k < nm; ++k) {
+            c->stats.ms_build += tm->span(marks[k][0], marks[k][1]);
+            c->stats.ms_force += tm->span(marks[k][1], marks[k][2]);
+        }
+        delete tm;
+    }
+    c->acc_valid = st == ASTER_OK;
+    c->tree.built = false;
+    return st;
+}
+
+extern "C" int aster_energy(aster_ctx* c, const aster_params* p, int ref_form, double* energy, double* momentum3) {
+    if (!c || !energy) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (c->n <= 0) return ASTER_ERR_NO_STATE;
+    ASTER_TRY(aster_begin(c));
+    const int64_t n = c->n;
+    const int nb = (int)((n + 255) / 256);
+    ASTER_TRY(c->scratch.ensure((size_t)nb * 5 * sizeof(double) + 64));
+    ASTER_TRY(c->red.ensure(4096));
+    double* part = c->scratch.as<double>();
+    double* out = c->red.as<double>() + 8;
+    if (ref_form)
+        k_energy_partial<true><<<nb, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2, part);
+    else
+        k_energy_partial<false><<<nb, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2, part);
+    ASTER_CUDA(cudaGetLastError());
+    k_energy_final<<<1, 32, 0, c->stream>>>(nb, part, p->G, out);
+    ASTER_CUDA(cudaGetLastError());
+    double host[4];
+    ASTER_CUDA(cudaMemcpyAsync(host, out, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ASTER_TRY(aster_finish(c));
+    *energy = host[0];
+    if (momentum3) { momentum3[0] = host[1]; momentum3[1] = host[2]; momentum3[2] = host[3]; }
+    return ASTER_OK;
+}

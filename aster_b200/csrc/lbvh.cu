@@ -1,0 +1,863 @@
+// LBVH Barnes-Hut: the replacement for Barnes_Hut::make_tree/compute_forces
+// (src/solvers/barnes_hut.cpp:309-418, bh_specialization.cpp:30-46) and the
+// OpenCL BH_hyper pipeline (src/solvers/full_GPU.cpp:54-339,519-527 with
+// include/Aster/kernels/{morton_writer,radix,BHH_specific}.cl.h).
+//
+// Pipeline per force evaluation (all on one stream, no host sync):
+//   box      max |coordinate| of the FP64 state (fused into the drift kernel
+//            during time stepping, a separate reduction otherwise)
+//   morton   30-bit code as the reference get_morton: x' = (x+B)/(2B),
+//            q = min(trunc(x' * 1024), 1023), interleave z|y|x (63-bit: 21
+//            bits per axis). IEEE FP64 add/div, no contraction: bit-exact.
+//   sort     stable LSD radix sort of (code, body index), 8-bit digits:
+//            per pass a tile histogram, one exclusive scan, a stable scatter
+//            (warp match-any ranking). Ties keep body-index order.
+//   karras   Karras (2012) node split exactly as barnes_hut.cpp:338-396
+//            (tie-break 32 + clz(i ^ j) on sorted positions), children,
+//            parents and leaf ranges; the same kernel gathers the leaves.
+//   bottomup one thread per leaf climbs with an atomic arrival counter per
+//            node; the second arrival merges the children: FP64 mass and
+//            centre of mass in NodesArray::unite order (barnes_hut.cpp:137-152,
+//            bit-exact), FP32 AABB, squared opening radius
+//            r_crit = l/theta + |com - box centre| (rounded up to FP32).
+//   walk     one warp per 32 consecutive sorted bodies: a shared-memory stack
+//            walk that opens a node for the whole group unless its FP32 centre
+//            of mass lies farther than r_crit from the group's FP32 box;
+//            accepted nodes are appended to a shared interaction list and
+//            evaluated 32 at a time by every lane (FP32 double-single or FP64).
+// Node numbering is the reference's: leaves 0..n-1 (sorted order), internal
+// n..2n-2, root n, -1 = no child.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "aster_internal.cuh"
+
+namespace {
+
+constexpr int SORT_THREADS = 256;
+constexpr int SORT_ITEMS = 8;
+constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // 2048 keys per block
+constexpr int SORT_WARPS = SORT_THREADS / 32;
+constexpr int RADIX = 256;
+constexpr int MAX_CLIMB = 160;     // bottom-up level cap (tree depth <= 97 for 63-bit codes)
+constexpr int WALK_WARPS = 4;
+constexpr int WALK_STACK = 2048;   // nodes per warp
+constexpr int WALK_LIST = 64;      // interaction-list capacity per warp
+
+// ----------------------------------------------------------------- box
+__device__ __forceinline__ double warp_max_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__global__ void __launch_bounds__(256) k_box(int64_t n, const double4* __restrict__ pm,
+                                             unsigned long long* __restrict__ box_bits) {
+    __shared__ double red[8];
+    double b = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double4 p = pm[i];
+        b = fmax(b, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))));
+    }
+    b = warp_max_d(b);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        v = warp_max_d(v);
+        if (threadIdx.x == 0) atomicMax(box_bits, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// -------------------------------------------------------------- morton
+__device__ __forceinline__ uint32_t part1by2_32(uint32_t n) {
+    n = (n | (n << 16)) & 0x030000FFu;
+    n = (n | (n << 8)) & 0x0300F00Fu;
+    n = (n | (n << 4)) & 0x030C30C3u;
+    n = (n | (n << 2)) & 0x09249249u;
+    return n;
+}
+
+__device__ __forceinline__ uint64_t part1by2_64(uint64_t n) {
+    n &= 0x1FFFFFull;
+    n = (n | (n << 32)) & 0x001F00000000FFFFull;
+    n = (n | (n << 16)) & 0x001F0000FF0000FFull;
+    n = (n | (n << 8)) & 0x100F00F00F00F00Full;
+    n = (n | (n << 4)) & 0x10C30C30C30C30C3ull;
+    n = (n | (n << 2)) & 0x1249249249249249ull;
+    return n;
+}
+
+// (x + B) / (2B) * scale truncated and clamped to maxv; NaN / negative -> 0.
+__device__ __forceinline__ uint32_t quantize(double x, double B, double scale, uint32_t maxv) {
+    double t = __ddiv_rn(__dadd_rn(x, B), __dmul_rn(2.0, B));
+    double s = __dmul_rn(t, scale);
+    if (!(s > 0.0)) return 0u;
+    if (s >= 4294967296.0) return maxv;
+    uint32_t q = (uint32_t)s;
+    return q < maxv ? q : maxv;
+}
+
+// OpenCL gen_mortons (morton_writer.cl.h:72-122): clamp to [0,1], 1024 max,
+// (ushort), so +B wraps to 0 through the 10-bit expansion mask.
+__device__ __forceinline__ uint32_t quantize_compat(double x, double B) {
+    double t = __ddiv_rn(__dadd_rn(x, B), __dmul_rn(2.0, B));
+    t = fmin(fmax(t, 0.0), 1.0);
+    uint32_t v = (uint32_t)__dmul_rn(t, 1024.0);
+    v = v < 1024u ? v : 1024u;
+    return (uint32_t)(uint16_t)v;
+}
+
+template <class KeyT, int MODE>  // MODE 0: 30-bit, 1: 63-bit, 2: 30-bit compat
+__global__ void __launch_bounds__(256) k_morton(int64_t n, const double4* __restrict__ pm,
+                                                const unsigned long long* __restrict__ box_bits,
+                                                KeyT* __restrict__ codes) {
+    const double B = __longlong_as_double((long long)*box_bits);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double4 p = pm[i];
+        if (MODE == 0) {
+            uint32_t ix = quantize(p.x, B, 1024.0, 1023u), iy = quantize(p.y, B, 1024.0, 1023u),
+                     iz = quantize(p.z, B, 1024.0, 1023u);
+            codes[i] = (KeyT)((part1by2_32(iz) << 2) | (part1by2_32(iy) << 1) | part1by2_32(ix));
+        } else if (MODE == 1) {
+            uint64_t ix = quantize(p.x, B, 2097152.0, 2097151u), iy = quantize(p.y, B, 2097152.0, 2097151u),
+                     iz = quantize(p.z, B, 2097152.0, 2097151u);
+            codes[i] = (KeyT)((part1by2_64(iz) << 2) | (part1by2_64(iy) << 1) | part1by2_64(ix));
+        } else {
+            uint32_t ix = quantize_compat(p.x, B), iy = quantize_compat(p.y, B), iz = quantize_compat(p.z, B);
+            codes[i] = (KeyT)(part1by2_32(ix) | (part1by2_32(iy) << 1) | (part1by2_32(iz) << 2));
+        }
+    }
+}
+
+// ---------------------------------------------------------------- sort
+template <class KeyT>
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(int64_t n, const KeyT* __restrict__ keys, int shift,
+                                                            int nblocks, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[SORT_WARPS][RADIX];
+    const int warp = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < SORT_WARPS * RADIX; d += SORT_THREADS) (&h[0][0])[d] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * SORT_TILE;
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        int64_t i = base + (int64_t)r * SORT_THREADS + threadIdx.x;
+        if (i < n) atomicAdd(&h[warp][(uint32_t)(keys[i] >> shift) & (RADIX - 1)], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
+        uint32_t s = 0;
+        for (int w = 0; w < SORT_WARPS; ++w) s += h[w][d];
+        hist[(int64_t)d * nblocks + blockIdx.x] = s;
+    }
+}
+
+// Exclusive scan of `count` uint32 in place, one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ data, int64_t count) {
+    __shared__ uint32_t sums[1024];
+    const int64_t per = (count + 1023) / 1024;
+    const int64_t b = threadIdx.x * per, e = min(count, b + per);
+    uint32_t s = 0;
+    for (int64_t i = b; i < e; ++i) s += data[i];
+    sums[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        uint32_t v = threadIdx.x >= off ? sums[threadIdx.x - off] : 0u;
+        __syncthreads();
+        sums[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = threadIdx.x ? sums[threadIdx.x - 1] : 0u;
+    for (int64_t i = b; i < e; ++i) {
+        uint32_t v = data[i];
+        data[i] = run;
+        run += v;
+    }
+}
+
+// Stable scatter of one 8-bit digit. Warp w of the block owns the 256 keys
+// [w*256, w*256+256) of the tile and ranks them round by round (32 consecutive
+// keys per round) with __match_any_sync, so ranks follow input order.
+template <class KeyT, bool IDENTITY_VALS>
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(int64_t n, const KeyT* __restrict__ kin,
+                                                               const int32_t* __restrict__ vin, KeyT* __restrict__ kout,
+                                                               int32_t* __restrict__ vout, int shift, int nblocks,
+                                                               const uint32_t* __restrict__ offsets) {
+    __shared__ uint32_t wh[SORT_WARPS][RADIX];
+    __shared__ uint32_t dstart[RADIX];
+    __shared__ KeyT sk[SORT_TILE];
+    __shared__ int32_t sv[SORT_TILE];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = threadIdx.x; d < SORT_WARPS * RADIX; d += SORT_THREADS) (&wh[0][0])[d] = 0;
+    __syncthreads();
+    const int64_t tile0 = (int64_t)blockIdx.x * SORT_TILE;
+    const uint32_t lt = (1u << lane) - 1u;
+    KeyT key[SORT_ITEMS];
+    int32_t val[SORT_ITEMS];
+    uint32_t rank[SORT_ITEMS];
+    uint32_t dig[SORT_ITEMS];
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        const int64_t i = tile0 + warp * (32 * SORT_ITEMS) + r * 32 + lane;
+        const bool ok = i < n;
+        key[r] = ok ? kin[i] : (KeyT)0;
+        val[r] = ok ? (IDENTITY_VALS ? (int32_t)i : vin[i]) : 0;
+        const uint32_t d = ok ? ((uint32_t)(key[r] >> shift) & (RADIX - 1)) : 0xFFFFu;
+        dig[r] = d;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t before = 0;
+        if (ok) before = wh[warp][d];
+        __syncwarp();
+        rank[r] = before + __popc(peers & lt);
+        if (ok && (peers & lt) == 0) wh[warp][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over warps, then over digits (block-local start)
+    uint32_t tot = 0;
+    if (threadIdx.x < RADIX) {
+        for (int w = 0; w < SORT_WARPS; ++w) {
+            uint32_t t = wh[w][threadIdx.x];
+            wh[w][threadIdx.x] = tot;
+            tot += t;
+        }
+        dstart[threadIdx.x] = tot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int d = 0; d < RADIX; ++d) {
+            uint32_t t = dstart[d];
+            dstart[d] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        if (dig[r] < RADIX) {
+            const uint32_t pos = dstart[dig[r]] + wh[warp][dig[r]] + rank[r];
+            sk[pos] = key[r];
+            sv[pos] = val[r];
+        }
+    }
+    __syncthreads();
+    const int64_t valid = min((int64_t)SORT_TILE, n - tile0);
+    for (int p = threadIdx.x; p < valid; p += SORT_THREADS) {
+        const KeyT k = sk[p];
+        const uint32_t d = (uint32_t)(k >> shift) & (RADIX - 1);
+        const int64_t g = (int64_t)offsets[(int64_t)d * nblocks + blockIdx.x] + (p - dstart[d]);
+        kout[g] = k;
+        vout[g] = sv[p];
+    }
+}
+
+template <class KeyT>
+__global__ void k_reverse(int64_t n, const KeyT* __restrict__ kin, const int32_t* __restrict__ vin,
+                          KeyT* __restrict__ kout, int32_t* __restrict__ vout) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        kout[i] = kin[n - 1 - i];
+        vout[i] = vin[n - 1 - i];
+    }
+}
+
+// -------------------------------------------------------------- karras
+template <class KeyT, bool COMPAT>
+__device__ __forceinline__ int kdelta(const KeyT* __restrict__ codes, const int32_t* __restrict__ perm,
+                                      int64_t n, int64_t i, int64_t j) {
+    if (j < 0 || j >= n) return -1;
+    const KeyT a = codes[i], b = codes[j];
+    if (a == b) {
+        const uint32_t t = COMPAT ? (uint32_t)(perm[i] ^ perm[j]) : (uint32_t)(i ^ j);
+        return (sizeof(KeyT) == 8 ? 64 : 32) + __clz((int)t);
+    }
+    return sizeof(KeyT) == 8 ? __clzll((long long)(a ^ b)) : __clz((int)(uint32_t)(a ^ b));
+}
+
+template <class KeyT, bool COMPAT>
+__global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restrict__ codes, const int32_t* __restrict__ perm,
+                                                const double4* __restrict__ pm, int32_t* __restrict__ left,
+                                                int32_t* __restrict__ right, int32_t* __restrict__ parent,
+                                                int32_t* __restrict__ rlo, int32_t* __restrict__ rhi,
+                                                int2* __restrict__ child, uint32_t* __restrict__ counters,
+                                                double4* __restrict__ node_cm, float4* __restrict__ bmin,
+                                                float4* __restrict__ bmax, float4* __restrict__ node_hi,
+                                                float4* __restrict__ node_lo) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        // leaf i: gather body perm[i]
+        {
+            const double4 p = pm[perm[i]];
+            node_cm[i] = p;
+            bmin[i] = make_float4(__double2float_rd(p.x), __double2float_rd(p.y), __double2float_rd(p.z), 0.f);
+            bmax[i] = make_float4(__double2float_ru(p.x), __double2float_ru(p.y), __double2float_ru(p.z), 0.f);
+            float4 h, l;
+            ds_split(p.x, h.x, l.x);
+            ds_split(p.y, h.y, l.y);
+            ds_split(p.z, h.z, l.z);
+            h.w = __double2float_rn(p.w);
+            l.w = 0.f;
+            node_hi[i] = h;
+            node_lo[i] = l;
+            left[i] = -1;
+            right[i] = -1;
+            rlo[i] = (int32_t)i;
+            rhi[i] = (int32_t)i;
+            child[i] = make_int2(-1, -1);
+            if (n == 1) parent[0] = -1;
+        }
+        if (i == n - 1) {
+            parent[n] = -1;  // root (n >= 2) or unused slot
+            continue;
+        }
+        const int dl = i == 0 ? -1 : kdelta<KeyT, COMPAT>(codes, perm, n, i, i - 1);
+        const int dr = kdelta<KeyT, COMPAT>(codes, perm, n, i, i + 1);
+        const int64_t d = dr > dl ? 1 : -1;
+        const int dmin = d == 1 ? dl : dr;
+        int64_t lmax = 2;
+        while (kdelta<KeyT, COMPAT>(codes, perm, n, i, i + lmax * d) > dmin) lmax *= 2;
+        int64_t l = 0;
+        for (int64_t t = lmax / 2; t >= 1; t /= 2)
+            if (kdelta<KeyT, COMPAT>(codes, perm, n, i, i + (l + t) * d) > dmin) l += t;
+        const int64_t j = i + l * d;
+        const int dnode = kdelta<KeyT, COMPAT>(codes, perm, n, i, j);
+        int64_t s = 0;
+        const int64_t range = j > i ? j - i : i - j;
+        for (int64_t t = (range + 1) / 2; t >= 1; t = (t + 1) / 2) {
+            if (kdelta<KeyT, COMPAT>(codes, perm, n, i, i + (s + t) * d) > dnode) s += t;
+            if (t == 1) break;
+        }
+        const int64_t gamma = i + s * d + (d < 0 ? d : 0);
+        const int64_t lo = i < j ? i : j, hi = i < j ? j : i;
+        const int64_t node = n + i;
+        const int32_t L = (int32_t)(lo == gamma ? gamma : n + gamma);
+        const int32_t R = (int32_t)(hi == gamma + 1 ? gamma + 1 : n + gamma + 1);
+        left[node] = L;
+        right[node] = R;
+        child[node] = make_int2(L, R);
+        parent[L] = (int32_t)node;
+        parent[R] = (int32_t)node;
+        rlo[node] = (int32_t)lo;
+        rhi[node] = (int32_t)hi;
+        counters[i] = 0u;
+    }
+}
+
+// ------------------------------------------------------------ bottom-up
+__device__ __forceinline__ double4 ld_cg(const double4* p) {
+    const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 ld_cg(const float4* p) { return __ldcg(p); }
+
+__global__ void __launch_bounds__(256) k_bottom_up(int64_t n, double theta, const int32_t* __restrict__ parent,
+                                                   const int2* __restrict__ child, uint32_t* __restrict__ counters,
+                                                   double4* __restrict__ node_cm, float4* __restrict__ bmin,
+                                                   float4* __restrict__ bmax, float4* __restrict__ node_hi,
+                                                   float4* __restrict__ node_lo, int* __restrict__ err) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t cur = k;
+        int level = 0;
+        for (;;) {
+            const int32_t par = parent[cur];
+            if (par < 0) break;
+            if (++level > MAX_CLIMB) {
+                atomicOr(err, ASTER_DEVERR_TREE);
+                break;
+            }
+            __threadfence();
+            const uint32_t old = atomicAdd(&counters[par - n], 1u);
+            if (old == 0u) break;  // first arrival: the sibling finishes the node
+            __threadfence();
+            const int2 ch = child[par];
+            const double4 cl = ld_cg(node_cm + ch.x), cr = ld_cg(node_cm + ch.y);
+            // NodesArray::unite order: M = m_R + m_L; c = (c_R m_R + c_L m_L) / M
+            const double M = __dadd_rn(cr.w, cl.w);
+            double4 c;
+            c.x = __ddiv_rn(__dadd_rn(__dmul_rn(cr.x, cr.w), __dmul_rn(cl.x, cl.w)), M);
+            c.y = __ddiv_rn(__dadd_rn(__dmul_rn(cr.y, cr.w), __dmul_rn(cl.y, cl.w)), M);
+            c.z = __ddiv_rn(__dadd_rn(__dmul_rn(cr.z, cr.w), __dmul_rn(cl.z, cl.w)), M);
+            c.w = M;
+            const float4 l0 = ld_cg(bmin + ch.x), l1 = ld_cg(bmin + ch.y);
+            const float4 h0 = ld_cg(bmax + ch.x), h1 = ld_cg(bmax + ch.y);
+            const float4 lo = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
+            const float4 hi = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
+            const double ex = __dsub_rn((double)hi.x, (double)lo.x), ey = __dsub_rn((double)hi.y, (double)lo.y),
+                         ez = __dsub_rn((double)hi.z, (double)lo.z);
+            double lmax = 0.0;
+            lmax = ex > lmax ? ex : lmax;
+            lmax = ey > lmax ? ey : lmax;
+            lmax = ez > lmax ? ez : lmax;
+            const double cx = __dmul_rn(0.5, __dadd_rn((double)lo.x, (double)hi.x));
+            const double cy = __dmul_rn(0.5, __dadd_rn((double)lo.y, (double)hi.y));
+            const double cz = __dmul_rn(0.5, __dadd_rn((double)lo.z, (double)hi.z));
+            const double dx = __dsub_rn(c.x, cx), dy = __dsub_rn(c.y, cy), dz = __dsub_rn(c.z, cz);
+            const double delta = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+            const double rc = __dadd_rn(__ddiv_rn(lmax, theta), delta);
+            float4 h, l;
+            ds_split(c.x, h.x, l.x);
+            ds_split(c.y, h.y, l.y);
+            ds_split(c.z, h.z, l.z);
+            h.w = __double2float_rn(M);
+            l.w = __double2float_ru(__dmul_rn(rc, rc));
+            node_cm[par] = c;
+            bmin[par] = lo;
+            bmax[par] = hi;
+            node_hi[par] = h;
+            node_lo[par] = l;
+            cur = par;
+        }
+    }
+}
+
+// ----------------------------------------------------------------- walk
+template <bool MIXED>
+struct WalkShared {
+    int stack[WALK_WARPS][WALK_STACK];
+    float4 lhi[WALK_WARPS][MIXED ? WALK_LIST : 1];
+    float4 llo[WALK_WARPS][MIXED ? WALK_LIST : 1];
+    double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST];
+};
+
+__device__ __forceinline__ float warp_min_f(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_max_f(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template <bool MIXED, bool GUARD, bool KICK>
+__global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
+    int64_t n, int64_t ngroups, const float4* __restrict__ node_hi, const float4* __restrict__ node_lo,
+    const double4* __restrict__ node_cm, const int2* __restrict__ child, const int32_t* __restrict__ perm,
+    double G, double eps2, double half_dt, double4* __restrict__ acc, double4* __restrict__ vel,
+    int* __restrict__ err, int* __restrict__ stack_hw, int32_t* __restrict__ group_counts,
+    unsigned long long* __restrict__ inter_count) {
+    __shared__ WalkShared<MIXED> sm;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t g = (int64_t)blockIdx.x * WALK_WARPS + warp;
+    if (g >= ngroups) return;
+    const uint32_t lt = (1u << lane) - 1u;
+    const int64_t k = g * 32 + lane;
+    const bool valid = k < n;
+    const int64_t kk = valid ? k : g * 32;  // inactive lanes mirror lane 0
+    int* stack = sm.stack[warp];
+
+    // this lane's body (leaf record) and the group box
+    float4 bh = node_hi[kk], bl = node_lo[kk];
+    double4 bc = MIXED ? make_double4(0, 0, 0, 0) : node_cm[kk];
+    const float glox = warp_min_f(valid ? bh.x : INFINITY), ghix = warp_max_f(valid ? bh.x : -INFINITY);
+    const float gloy = warp_min_f(valid ? bh.y : INFINITY), ghiy = warp_max_f(valid ? bh.y : -INFINITY);
+    const float gloz = warp_min_f(valid ? bh.z : INFINITY), ghiz = warp_max_f(valid ? bh.z : -INFINITY);
+
+    CompSum sx, sy, sz;
+    double dax = 0, day = 0, daz = 0;
+    const float epsf = (float)eps2;
+    int top = 1, lc = 0, hw = 1;
+    long long total = 0;
+    if (lane == 0) stack[0] = n >= 2 ? (int)n : 0;
+    __syncwarp();
+    bool overflow = false;
+
+    auto evaluate = [&](int cnt) {
+        if (MIXED) {
+            float ax = 0.f, ay = 0.f, az = 0.f;
+            for (int e = 0; e < cnt; ++e) {
+                const float4 h = sm.lhi[warp][e], l = sm.llo[warp][e];
+                float dx = (h.x - bh.x) + (l.x - bl.x);
+                float dy = (h.y - bh.y) + (l.y - bl.y);
+                float dz = (h.z - bh.z) + (l.z - bl.z);
+                float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, epsf)));
+                float inv = rsqrt_approx(r2);
+                if (GUARD) inv = r2 > 0.f ? inv : 0.f;
+                float s = h.w * inv * inv * inv;
+                ax = fmaf(dx, s, ax); ay = fmaf(dy, s, ay); az = fmaf(dz, s, az);
+            }
+            sx.add(ax); sy.add(ay); sz.add(az);
+        } else {
+            for (int e = 0; e < cnt; ++e) {
+                const double4 c = sm.lcm[warp][e];
+                double dx = c.x - bc.x, dy = c.y - bc.y, dz = c.z - bc.z;
+                double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+                double inv = rsqrt(r2);
+                if (GUARD) inv = r2 > 0.0 ? inv : 0.0;
+                double s = c.w * inv * inv * inv;
+                dax = fma(dx, s, dax); day = fma(dy, s, day); daz = fma(dz, s, daz);
+            }
+        }
+        total += cnt;
+    };
+
+    while (top > 0) {
+        const int cnt = top < 32 ? top : 32;
+        int node = -1;
+        if (lane < cnt) node = stack[top - 1 - lane];
+        __syncwarp();
+        top -= cnt;
+        bool accept = false, open = false;
+        float4 nh = make_float4(0, 0, 0, 0), nl = make_float4(0, 0, 0, 0);
+        if (lane < cnt) {
+            nh = node_hi[node];
+            nl = node_lo[node];
+            if (node < n) {
+                accept = true;
+            } else {
+                // FP32, round-to-nearest, no FMA (matches the CPU restatement)
+                float ux = __fsub_rn(glox, nh.x), wx = __fsub_rn(nh.x, ghix);
+                float uy = __fsub_rn(gloy, nh.y), wy = __fsub_rn(nh.y, ghiy);
+                float uz = __fsub_rn(gloz, nh.z), wz = __fsub_rn(nh.z, ghiz);
+                float tx = ux > wx ? ux : wx, ty = uy > wy ? uy : wy, tz = uz > wz ? uz : wz;
+                tx = tx > 0.f ? tx : 0.f;
+                ty = ty > 0.f ? ty : 0.f;
+                tz = tz > 0.f ? tz : 0.f;
+                const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), __fmul_rn(ty, ty)), __fmul_rn(tz, tz));
+                accept = d2 > nl.w;
+                open = !accept;
+            }
+        }
+        const uint32_t amask = __ballot_sync(0xffffffffu, accept);
+        const uint32_t omask = __ballot_sync(0xffffffffu, open);
+        const int nopen = __popc(omask);
+        if (top + 2 * nopen > WALK_STACK) {
+            overflow = true;
+            break;
+        }
+        if (open) {
+            const int2 ch = child[node];
+            const int pos = top + 2 * __popc(omask & lt);
+            stack[pos] = ch.y;
+            stack[pos + 1] = ch.x;
+        }
+        top += 2 * nopen;
+        hw = top > hw ? top : hw;
+        if (accept) {
+            const int pos = lc + __popc(amask & lt);
+            if (MIXED) {
+                sm.lhi[warp][pos] = nh;
+                sm.llo[warp][pos] = make_float4(nl.x, nl.y, nl.z, 0.f);
+            } else {
+                sm.lcm[warp][pos] = node_cm[node];
+            }
+        }
+        lc += __popc(amask);
+        __syncwarp();
+        if (lc >= 32) {
+            evaluate(32);
+            __syncwarp();
+            const int rest = lc - 32;
+            if (lane < rest) {
+                if (MIXED) {
+                    const float4 h = sm.lhi[warp][32 + lane], l = sm.llo[warp][32 + lane];
+                    sm.lhi[warp][lane] = h;
+                    sm.llo[warp][lane] = l;
+                } else {
+                    sm.lcm[warp][lane] = sm.lcm[warp][32 + lane];
+                }
+            }
+            lc = rest;
+            __syncwarp();
+        }
+    }
+    if (overflow) {
+        if (lane == 0) atomicOr(err, ASTER_DEVERR_STACK);
+        return;
+    }
+    if (lc > 0) evaluate(lc);
+    if (lane == 0) {
+        atomicMax(stack_hw, hw);
+        if (group_counts) group_counts[g] = (int32_t)total;
+        const int nvalid = (int)min((int64_t)32, n - g * 32);
+        atomicAdd(inter_count, (unsigned long long)total * (unsigned long long)nvalid);
+    }
+    if (valid) {
+        double ax, ay, az;
+        if (MIXED) { ax = G * sx.value(); ay = G * sy.value(); az = G * sz.value(); }
+        else { ax = G * dax; ay = G * day; az = G * daz; }
+        const int32_t b = perm[k];
+        acc[b] = make_double4(ax, ay, az, 0.0);
+        if (KICK) {
+            double4 v = vel[b];
+            v.x += ax * half_dt; v.y += ay * half_dt; v.z += az * half_dt;
+            vel[b] = v;
+        }
+    }
+}
+
+template <bool MIXED, bool GUARD, bool KICK>
+void launch_walk(aster_ctx* c, const aster_params* p, int32_t* gc, unsigned long long* inter) {
+    const int64_t n = c->n, ng = (n + 31) / 32;
+    LbvhBufs& t = c->tree;
+    const int blocks = (int)((ng + WALK_WARPS - 1) / WALK_WARPS);
+    k_walk<MIXED, GUARD, KICK><<<blocks, WALK_WARPS * 32, 0, c->stream>>>(
+        n, ng, t.node_hi.as<float4>(), t.node_lo.as<float4>(), t.node_cm.as<double4>(), t.child.as<int2>(),
+        t.perm.as<int32_t>(), p->G, p->eps2, 0.5 * p->dt, c->acc.as<double4>(), c->vel.as<double4>(), c->err_dev,
+        c->stack_hw_dev, gc, inter);
+}
+
+template <class KeyT>
+int run_sort(aster_ctx* c, int bits) {
+    LbvhBufs& t = c->tree;
+    const int64_t n = c->n;
+    const int nblocks = (int)((n + SORT_TILE - 1) / SORT_TILE);
+    const int passes = (bits + 7) / 8;  // 30 -> 4, 63 -> 8 (even: result lands in sorted_codes)
+    uint32_t* hist = t.hist.as<uint32_t>();
+    const KeyT* kin = t.codes.as<KeyT>();
+    const int32_t* vin = nullptr;
+    for (int ps = 0; ps < passes; ++ps) {
+        KeyT* kout = (ps & 1) ? t.sorted_codes.as<KeyT>() : t.codes_alt.as<KeyT>();
+        int32_t* vout = (ps & 1) ? t.perm.as<int32_t>() : t.perm_alt.as<int32_t>();
+        const int shift = 8 * ps;
+        k_sort_hist<KeyT><<<nblocks, SORT_THREADS, 0, c->stream>>>(n, kin, shift, nblocks, hist);
+        k_scan_exclusive<<<1, 1024, 0, c->stream>>>(hist, (int64_t)RADIX * nblocks);
+        if (ps == 0)
+            k_sort_scatter<KeyT, true><<<nblocks, SORT_THREADS, 0, c->stream>>>(n, kin, nullptr, kout, vout, shift,
+                                                                             nblocks, hist);
+        else
+            k_sort_scatter<KeyT, false><<<nblocks, SORT_THREADS, 0, c->stream>>>(n, kin, vin, kout, vout, shift,
+                                                                              nblocks, hist);
+        ASTER_CUDA(cudaGetLastError());
+        c->stats.kernels += 3;
+        kin = kout;
+        vin = vout;
+    }
+    return ASTER_OK;
+}
+
+template <class KeyT>
+int run_build(aster_ctx* c, const aster_params* p) {
+    LbvhBufs& t = c->tree;
+    const int64_t n = c->n;
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 16);
+    const unsigned long long* box = c->red.as<unsigned long long>();
+    const int mode = p->compat_mode ? 2 : (p->morton_bits == 63 ? 1 : 0);
+    if (mode == 0) k_morton<KeyT, 0><<<grid, 256, 0, c->stream>>>(n, c->pm.as<double4>(), box, t.codes.as<KeyT>());
+    else if (mode == 1) k_morton<KeyT, 1><<<grid, 256, 0, c->stream>>>(n, c->pm.as<double4>(), box, t.codes.as<KeyT>());
+    else k_morton<KeyT, 2><<<grid, 256, 0, c->stream>>>(n, c->pm.as<double4>(), box, t.codes.as<KeyT>());
+    ASTER_CUDA(cudaGetLastError());
+    c->stats.kernels += 1;
+    ASTER_TRY(run_sort<KeyT>(c, p->morton_bits == 63 ? 64 : 32));
+    if (p->compat_mode) {
+        // OpenCL order is descending by (code, index): reverse the ascending sort
+        k_reverse<KeyT><<<grid, 256, 0, c->stream>>>(n, t.sorted_codes.as<KeyT>(), t.perm.as<int32_t>(),
+                                                     t.codes_alt.as<KeyT>(), t.perm_alt.as<int32_t>());
+        ASTER_CUDA(cudaMemcpyAsync(t.sorted_codes.ptr, t.codes_alt.ptr, (size_t)n * sizeof(KeyT),
+                                   cudaMemcpyDeviceToDevice, c->stream));
+        ASTER_CUDA(cudaMemcpyAsync(t.perm.ptr, t.perm_alt.ptr, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                                   c->stream));
+        c->stats.kernels += 1;
+    }
+    const KeyT* sc = t.sorted_codes.as<KeyT>();
+    if (p->compat_mode)
+        k_karras<KeyT, true><<<grid, 256, 0, c->stream>>>(
+            n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.left.as<int32_t>(), t.right.as<int32_t>(),
+            t.parent.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(),
+            t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
+            t.node_hi.as<float4>(), t.node_lo.as<float4>());
+    else
+        k_karras<KeyT, false><<<grid, 256, 0, c->stream>>>(
+            n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.left.as<int32_t>(), t.right.as<int32_t>(),
+            t.parent.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(),
+            t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
+            t.node_hi.as<float4>(), t.node_lo.as<float4>());
+    ASTER_CUDA(cudaGetLastError());
+    k_bottom_up<<<grid, 256, 0, c->stream>>>(n, p->theta, t.parent.as<int32_t>(), t.child.as<int2>(),
+                                             t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(),
+                                             t.bmax.as<float4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>(),
+                                             c->err_dev);
+    ASTER_CUDA(cudaGetLastError());
+    c->stats.kernels += 2;
+    return ASTER_OK;
+}
+
+int ensure_tree(aster_ctx* c) {
+    LbvhBufs& t = c->tree;
+    const int64_t n = c->n, m = 2 * n;  // 2n-1 nodes, +1 slot so parent[n] exists for n == 1
+    const int64_t nblocks = (n + SORT_TILE - 1) / SORT_TILE;
+    ASTER_TRY(t.codes.ensure((size_t)n * 8));
+    ASTER_TRY(t.codes_alt.ensure((size_t)n * 8));
+    ASTER_TRY(t.sorted_codes.ensure((size_t)n * 8));
+    ASTER_TRY(t.perm.ensure((size_t)n * 4));
+    ASTER_TRY(t.perm_alt.ensure((size_t)n * 4));
+    ASTER_TRY(t.hist.ensure((size_t)nblocks * RADIX * 4));
+    ASTER_TRY(t.left.ensure((size_t)m * 4));
+    ASTER_TRY(t.right.ensure((size_t)m * 4));
+    ASTER_TRY(t.parent.ensure((size_t)m * 4));
+    ASTER_TRY(t.rlo.ensure((size_t)m * 4));
+    ASTER_TRY(t.rhi.ensure((size_t)m * 4));
+    ASTER_TRY(t.counters.ensure((size_t)n * 4));
+    ASTER_TRY(t.node_cm.ensure((size_t)m * sizeof(double4)));
+    ASTER_TRY(t.bmin.ensure((size_t)m * sizeof(float4)));
+    ASTER_TRY(t.bmax.ensure((size_t)m * sizeof(float4)));
+    ASTER_TRY(t.node_hi.ensure((size_t)m * sizeof(float4)));
+    ASTER_TRY(t.node_lo.ensure((size_t)m * sizeof(float4)));
+    ASTER_TRY(t.child.ensure((size_t)m * sizeof(int2)));
+    ASTER_TRY(c->red.ensure(4096));
+    t.n = n;
+    return ASTER_OK;
+}
+
+}  // namespace
+
+int aster_lbvh_build_dev(aster_ctx* c, const aster_params* p, bool box_ready) {
+    ASTER_TRY(ensure_tree(c));
+    if (!box_ready) {
+        unsigned long long* box = c->red.as<unsigned long long>();
+        ASTER_CUDA(cudaMemsetAsync(box, 0, sizeof(unsigned long long), c->stream));
+        const int grid = (int)std::min<int64_t>((c->n + 255) / 256, (int64_t)c->sm_count * 8);
+        k_box<<<grid, 256, 0, c->stream>>>(c->n, c->pm.as<double4>(), box);
+        ASTER_CUDA(cudaGetLastError());
+        c->stats.kernels += 1;
+    }
+    if (p->morton_bits == 63) ASTER_TRY(run_build<uint64_t>(c, p));
+    else ASTER_TRY(run_build<uint32_t>(c, p));
+    c->tree.built = true;
+    return ASTER_OK;
+}
+
+int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, bool kick, int32_t* gc) {
+    unsigned long long* inter = c->red.as<unsigned long long>() + 64;
+    const bool guard = !(p->eps2 > 0.0);
+    if (precision == ASTER_MIXED) {
+        if (guard) { if (kick) launch_walk<true, true, true>(c, p, gc, inter); else launch_walk<true, true, false>(c, p, gc, inter); }
+        else       { if (kick) launch_walk<true, false, true>(c, p, gc, inter); else launch_walk<true, false, false>(c, p, gc, inter); }
+    } else if (precision == ASTER_FP64) {
+        if (guard) { if (kick) launch_walk<false, true, true>(c, p, gc, inter); else launch_walk<false, true, false>(c, p, gc, inter); }
+        else       { if (kick) launch_walk<false, false, true>(c, p, gc, inter); else launch_walk<false, false, false>(c, p, gc, inter); }
+    } else {
+        return ASTER_ERR_INVALID_ARG;
+    }
+    ASTER_CUDA(cudaGetLastError());
+    c->stats.kernels += 1;
+    return ASTER_OK;
+}
+
+// ---- tree export -------------------------------------------------------------
+namespace {
+__global__ void k_export_nodes(int64_t m, const double4* __restrict__ cm, const float4* __restrict__ bmin,
+                               const float4* __restrict__ bmax, const float4* __restrict__ lo,
+                               double* __restrict__ mass, double* __restrict__ com, float* __restrict__ fmin3,
+                               float* __restrict__ fmax3, float* __restrict__ rc2) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        const double4 c = cm[i];
+        mass[i] = c.w;
+        com[3 * i] = c.x; com[3 * i + 1] = c.y; com[3 * i + 2] = c.z;
+        const float4 a = bmin[i], b = bmax[i];
+        fmin3[3 * i] = a.x; fmin3[3 * i + 1] = a.y; fmin3[3 * i + 2] = a.z;
+        fmax3[3 * i] = b.x; fmax3[3 * i + 1] = b.y; fmax3[3 * i + 2] = b.z;
+        rc2[i] = lo[i].w;
+    }
+}
+template <class KeyT>
+__global__ void k_widen(int64_t n, const KeyT* __restrict__ in, uint64_t* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (uint64_t)in[i];
+}
+}  // namespace
+
+static int export_tree(aster_ctx* c, const aster_params* p, aster_tree_view* v) {
+    LbvhBufs& t = c->tree;
+    const int64_t n = c->n, m = 2 * n - 1;
+    cudaStream_t st = c->stream;
+    const size_t need = (size_t)m * (8 + 24 + 12 + 12 + 4) + (size_t)n * 16 + 1024;
+    ASTER_TRY(c->stage.ensure(need));
+    char* base = c->stage.as<char>();
+    double* mass = (double*)base;
+    double* com = mass + m;
+    float* fmin3 = (float*)(com + 3 * m);
+    float* fmax3 = fmin3 + 3 * m;
+    float* rc2 = fmax3 + 3 * m;
+    uint64_t* wide = (uint64_t*)(((uintptr_t)(rc2 + m) + 15) & ~(uintptr_t)15);
+    uint64_t* wide2 = wide + n;
+    const int grid = (int)std::min<int64_t>((m + 255) / 256, (int64_t)c->sm_count * 16);
+    k_export_nodes<<<grid, 256, 0, st>>>(m, t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
+                                         t.node_lo.as<float4>(), mass, com, fmin3, fmax3, rc2);
+    if (p->morton_bits == 63) {
+        k_widen<uint64_t><<<grid, 256, 0, st>>>(n, t.codes.as<uint64_t>(), wide);
+        k_widen<uint64_t><<<grid, 256, 0, st>>>(n, t.sorted_codes.as<uint64_t>(), wide2);
+    } else {
+        k_widen<uint32_t><<<grid, 256, 0, st>>>(n, t.codes.as<uint32_t>(), wide);
+        k_widen<uint32_t><<<grid, 256, 0, st>>>(n, t.sorted_codes.as<uint32_t>(), wide2);
+    }
+    ASTER_CUDA(cudaGetLastError());
+    auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
+        if (dst) ASTER_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        return ASTER_OK;
+    };
+    ASTER_TRY(cp(v->codes, wide, (size_t)n * 8));
+    ASTER_TRY(cp(v->sorted_codes, wide2, (size_t)n * 8));
+    ASTER_TRY(cp(v->perm, t.perm.ptr, (size_t)n * 4));
+    ASTER_TRY(cp(v->left, t.left.ptr, (size_t)m * 4));
+    ASTER_TRY(cp(v->right, t.right.ptr, (size_t)m * 4));
+    ASTER_TRY(cp(v->parent, t.parent.ptr, (size_t)m * 4));
+    ASTER_TRY(cp(v->range_lo, t.rlo.ptr, (size_t)m * 4));
+    ASTER_TRY(cp(v->range_hi, t.rhi.ptr, (size_t)m * 4));
+    ASTER_TRY(cp(v->node_mass, mass, (size_t)m * 8));
+    ASTER_TRY(cp(v->node_com, com, (size_t)m * 24));
+    ASTER_TRY(cp(v->node_bmin, fmin3, (size_t)m * 12));
+    ASTER_TRY(cp(v->node_bmax, fmax3, (size_t)m * 12));
+    ASTER_TRY(cp(v->node_rcrit2, rc2, (size_t)m * 4));
+    unsigned long long bits = 0;
+    ASTER_CUDA(cudaMemcpyAsync(&bits, c->red.ptr, 8, cudaMemcpyDeviceToHost, st));
+    ASTER_CUDA(cudaStreamSynchronize(st));
+    double box;
+    memcpy(&box, &bits, 8);
+    v->box = box;
+    return ASTER_OK;
+}
+
+extern "C" int aster_lbvh_build(aster_ctx* c, const aster_params* p, aster_tree_view* view) {
+    if (!c) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (c->n <= 0) return ASTER_ERR_NO_STATE;
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    cudaEventRecord(c->ev[0], c->stream);
+    ASTER_TRY(aster_lbvh_build_dev(c, p, false));
+    cudaEventRecord(c->ev[1], c->stream);
+    ASTER_TRY(aster_finish(c));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_build = c->stats.ms_total = ms;
+    if (view) ASTER_TRY(export_tree(c, p, view));
+    return ASTER_OK;
+}
+
+extern "C" int aster_lbvh_forces(aster_ctx* c, const aster_params* p, int precision, double* acc_out,
+                                 int32_t* group_counts) {
+    if (!c) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (c->n <= 0) return ASTER_ERR_NO_STATE;
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    if (p->force_law & ASTER_PN1) return ASTER_ERR_UNSUPPORTED;
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    const int64_t ng = (c->n + 31) / 32;
+    int32_t* gc = nullptr;
+    if (group_counts) {
+        ASTER_TRY(c->targets.ensure((size_t)ng * 4));
+        gc = c->targets.as<int32_t>();
+    }
+    ASTER_TRY(ensure_tree(c));
+    unsigned long long* inter = c->red.as<unsigned long long>() + 64;
+    ASTER_CUDA(cudaMemsetAsync(inter, 0, 8, c->stream));
+    cudaEventRecord(c->ev[0], c->stream);
+    ASTER_TRY(aster_lbvh_build_dev(c, p, false));
+    cudaEventRecord(c->ev[1], c->stream);
+    ASTER_TRY(aster_lbvh_walk_launch(c, p, precision, false, gc));
+    cudaEventRecord(c->ev[2], c->stream);
+    unsigned long long ic = 0;
+    ASTER_CUDA(cudaMemcpyAsync(&ic, inter, 8, cudaMemcpyDeviceToHost, c->stream));
+    if (group_counts)
+        ASTER_CUDA(cudaMemcpyAsync(group_counts, gc, (size_t)ng * 4, cudaMemcpyDeviceToHost, c->stream));
+    ASTER_TRY(aster_finish(c));
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+    c->stats.ms_build = a;
+    c->stats.ms_force = b;
+    c->stats.ms_total = a + b;
+    c->stats.interactions = (double)ic;
+    c->acc_valid = true;
+    return aster_copy_acc_out(c, acc_out);
+}

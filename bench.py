@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the force/integration hot path on B200.
+
+Headline workload (one "step" = one kick-drift-kick leapfrog step):
+  LBVH Barnes-Hut, N = 2^20 Plummer sphere (lognormal masses mu=0 sigma=0.5,
+  renormalised to 1), 30-bit Morton codes on the bounding cube, stable radix
+  sort, Karras tree, monopole cells at theta = 0.5, eps = 0.005, FP32
+  interactions on double-single positions, FP64 state, dt = 5e-4.
+metric: LBVH-BH steps/s at N = 2^20 (higher is better).
+
+Also reported on the same JSON line: the all-pairs pair-interaction rates of
+the FP64 and mixed kernels on the cold-disk workload (N = 262144) and the
+mixed-vs-FP64 force error, the FP64-walk LBVH step rate at the same theta
+(equal approximation error), the roofline of the dominant kernel (the tree
+walk), a CPU baseline (the reference's own Barnes_Hut + update_leapfrog,
+compiled from its sources) and SM clocks sampled during the timed region.
+
+`--impl reference` times the reference CPU implementation of the same
+workload on the host cores (the reference has no usable GPU path here).
+
+Multi-GPU: the LBVH path does not shard (the tree is global), so N GPUs run N
+independent replicas of the workload ("replicas only"); value = total steps/s.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_C2 = 1 << 20
+THETA, EPS, DT = 0.5, 0.005, 5e-4
+SEED_C2 = 1002
+N_C3, EPS_C3, SEED_C3 = 262144, 0.002, 1003
+FLOP_PER_PAIR = 20  # Newtonian pair, Nyland et al. GPU Gems 3 ch. 31 convention
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        loaded = [s for s in sm if smax and s > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def cpu_baseline_c2(pos, vel, m, steps: int = 1):
+    """The reference's Barnes_Hut + update_leapfrog on the host cores, one
+    step at full N (2 tree builds + walks)."""
+    from oracle.oracle import Ref
+    if not Ref.available():
+        return None
+    ref = Ref()
+    ref.setup(pos, vel, m, G=1.0, dt=DT, eps2=EPS * EPS, theta=THETA, box=float(np.abs(pos).max()), solver="bh")
+    t0 = time.perf_counter()
+    ref.leapfrog(steps)
+    dt = time.perf_counter() - t0
+    return {"value": steps / dt, "unit": "steps/s", "cores": ref.threads(), "kind": "reference",
+            "sample": f"{steps} update_leapfrog step(s) of Barnes_Hut at N={len(m)} (full workload), "
+                      f"reference sources compiled unmodified with a std::thread TBB stand-in"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from aster_b200 import gen
+    from oracle.oracle import Ref
+    if not Ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref missing"}))
+        return 0
+    pos, vel, m = gen.plummer(N_C2, SEED_C2, masses="lognormal")
+    ref = Ref()
+    ref.setup(pos, vel, m, G=1.0, dt=DT, eps2=EPS * EPS, theta=THETA, box=float(np.abs(pos).max()), solver="bh")
+    for _ in range(args.warmup):
+        ref.leapfrog(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.leapfrog(1)
+    el = time.perf_counter() - t0
+    v = args.steps / el
+    line = {
+        "impl": "reference", "metric": "LBVH-BH steps/s @N=1M", "value": v, "unit": "steps/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "C2 LBVH Barnes-Hut KDK step, Plummer N=1048576 lognormal masses, theta=0.5, "
+                               "eps=0.005, dt=5e-4", "n": N_C2},
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": ref.threads(), "kind": "reference",
+                         "sample": f"full N={N_C2} update_leapfrog steps with Barnes_Hut (2 tree builds + walks "
+                                   f"each), reference sources compiled unmodified, std::thread TBB stand-in"},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from aster_b200 import gen
+    from aster_b200.api import FP64, MIXED, SOLVER_LBVH, Context, Params
+
+    device = local if world > 1 else 0
+    pos, vel, m = gen.plummer(N_C2, SEED_C2, masses="lognormal")
+    p = Params(G=1.0, eps2=EPS * EPS, theta=THETA, dt=DT)
+    ctx = Context(device)
+    ctx.upload(pos, vel, m)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    # warm-up (also primes the cached acceleration)
+    ctx.kdk_steps(p, args.warmup, SOLVER_LBVH, MIXED)
+    barrier()
+    clocks = ClockSampler(device)
+    clocks.start()
+    ctx.kdk_steps(p, args.steps, SOLVER_LBVH, MIXED)   # device-timed inside (CUDA events)
+    st = ctx.stats()
+    barrier()
+    clk = clocks.stop()
+    ms = st["ms_total"]
+    if dist:
+        import torch
+        t = torch.tensor([ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps / (ms / 1e3)
+    walk_ms = st["ms_force"] / max(args.steps, 1)
+    build_ms = st["ms_build"] / max(args.steps, 1)
+    inter_per_step = st["interactions"] / max(args.steps, 1)
+    kernels = st["kernels"]
+
+    # e2e through the C ABI with pinned host buffers: H2D state, one step, D2H state
+    e2e = e2e_c2(ctx, p, pos, vel, m, args)
+    line = {}
+    if rank == 0:
+        peaks, src = measured_peaks()
+        f_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+        sms = 148
+        fp32_peak = sms * 128 * 2 * f_mhz * 1e6 / 1e12
+        achieved = inter_per_step * FLOP_PER_PAIR / (walk_ms / 1e3) / 1e12
+        extra = secondary(ctx, args) if not args.quick else {}
+        line = {
+            "metric": "LBVH-BH steps/s @N=1M", "value": value, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 pairs / f64 state", "data": "synthetic",
+            "config": {"workload": "C2 LBVH Barnes-Hut KDK step, Plummer N=1048576 lognormal(0,0.5) masses, "
+                                   "30-bit Morton on the bounding cube, theta=0.5, eps=0.005, dt=5e-4, mixed",
+                       "n": N_C2, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "per-step working set > L2: the tree rebuild writes ~0.4 GB every step"},
+            "phases_ms": {"build": build_ms, "walk": walk_ms, "other": ms / args.steps - build_ms - walk_ms},
+            "interactions_per_step": inter_per_step,
+            "roofline": {"bound": "fp32", "kernel": "k_walk (tree walk + interactions)",
+                         "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                         "traffic": args.walk_traffic,
+                         "peak_source": f"148 SMs x 128 FP32 lanes x 2 x median SM clock {f_mhz:.0f} MHz sampled "
+                                        f"during the run (no FP32 figure in MEASURED_PEAKS.json)",
+                         "flop_per_interaction": FLOP_PER_PAIR},
+            "e2e": e2e,
+            "gpu_launches": kernels,
+            "clocks": clk,
+        }
+        line.update(extra)
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline_c2(pos, vel, m)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def e2e_c2(ctx, p, pos, vel, m, args):
+    """Same metric through the public C ABI with host buffers: each step
+    copies the state host->device from pinned memory, runs one KDK step
+    (the upload invalidates the cached acceleration, so the step evaluates the
+    force twice, as the reference's update_leapfrog does) and copies the new
+    positions and velocities back."""
+    import ctypes
+    from aster_b200.api import MIXED, SOLVER_LBVH
+    n = len(m)
+    lib = ctx.lib
+    # page-locked host buffers (torch's pinned allocator; same primary context)
+    pinned = []
+    try:
+        import torch
+        hp = torch.from_numpy(np.ascontiguousarray(pos)).pin_memory()
+        hv = torch.from_numpy(np.ascontiguousarray(vel)).pin_memory()
+        hm = torch.from_numpy(np.ascontiguousarray(m)).pin_memory()
+        op = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+        ov = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+        arrs = [t.numpy() for t in (hp, hv, hm, op, ov)]
+        pinned = [hp, hv, hm, op, ov]
+    except Exception:
+        arrs = [np.ascontiguousarray(pos), np.ascontiguousarray(vel), np.ascontiguousarray(m),
+                np.empty((n, 3)), np.empty((n, 3))]
+    hp, hv, hm, op, ov = arrs
+    vp = ctypes.c_void_p
+    cp = p.c_struct()
+
+    def one():
+        st = lib.aster_state_upload(ctx.h, n, vp(hp.ctypes.data), vp(hv.ctypes.data), vp(hm.ctypes.data))
+        st = st or lib.aster_kdk_steps(ctx.h, ctypes.byref(cp), SOLVER_LBVH, MIXED, 1)
+        st = st or lib.aster_state_download(ctx.h, vp(op.ctypes.data), vp(ov.ctypes.data), None)
+        if st:
+            raise RuntimeError(f"e2e step failed: {st}")
+
+    for _ in range(2):
+        one()
+    k = max(2, min(args.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        one()
+    el = time.perf_counter() - t0
+    del pinned
+    return {"value": k / el, "unit": "steps/s", "h2d_bytes_per_step": n * (24 + 24 + 8),
+            "d2h_bytes_per_step": n * (24 + 24), "steps": k,
+            "note": "host wall clock around synchronous C-ABI calls (each call ends with a stream sync)"}
+
+
+def secondary(ctx, args):
+    """All-pairs rates (C3 disk) and the FP64-walk LBVH rate (same theta)."""
+    from aster_b200 import gen
+    from aster_b200.api import FP64, MIXED, SOLVER_LBVH, Params
+    out = {}
+    # FP64 LBVH at the same theta: same tree, same interaction lists
+    pos, vel, m = gen.plummer(N_C2, SEED_C2, masses="lognormal")
+    p = Params(G=1.0, eps2=EPS * EPS, theta=THETA, dt=DT)
+    ctx.upload(pos, vel, m)
+    a32 = ctx.lbvh_forces(p, MIXED)
+    a64 = ctx.lbvh_forces(p, FP64)
+    ctx.kdk_steps(p, 1, SOLVER_LBVH, FP64)
+    ctx.kdk_steps(p, 3, SOLVER_LBVH, FP64)
+    s64 = ctx.stats()
+    tg = np.random.default_rng(4096).choice(N_C2, 4096, replace=False)
+    exact = ctx.allpairs_targets(p, tg, FP64)
+    err_bh = float(np.linalg.norm(a32[tg] - exact) / np.linalg.norm(exact))
+    out["lbvh_precision"] = {
+        "fp64_walk_steps_per_s": 3 / (s64["ms_total"] / 1e3),
+        "mixed_vs_fp64_walk_rel_l2": float(np.linalg.norm(a32 - a64) / np.linalg.norm(a64)),
+        "approx_rel_l2_vs_fp64_allpairs_4096_sample": err_bh,
+    }
+    # all-pairs on the C3 cold disk
+    pos, vel, m = gen.exponential_disk(N_C3, SEED_C3)
+    p3 = Params(G=1.0, eps2=EPS_C3 ** 2, dt=1e-4)
+    ctx.upload(pos, vel, m)
+    res = {}
+    accs = {}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        accs[name] = ctx.allpairs(p3, prec)
+        times = []
+        for _ in range(3):
+            ctx.allpairs(p3, prec)
+            times.append(ctx.stats()["ms_force"])
+        t = min(times)
+        res[name] = {"ms_per_eval": t, "pairs_per_s": N_C3 * (N_C3 - 1) / (t / 1e3)}
+    res["mixed_vs_fp64_rel_l2"] = float(np.linalg.norm(accs["mixed"] - accs["fp64"]) / np.linalg.norm(accs["fp64"]))
+    res["workload"] = "C3 cold exponential disk N=262144 (+central mass 0.1), eps=0.002, one force evaluation"
+    out["allpairs"] = res
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quick", action="store_true", help="skip the secondary measurements")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--walk-traffic", type=float, default=None,
+                    help="DRAM bytes per walk launch from an ncu capture (reported as roofline.traffic)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warm-up raised to 3 steps (timing rule)")
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

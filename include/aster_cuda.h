@@ -1,0 +1,168 @@
+/*
+ * aster_cuda.h -- C ABI of the B200 (sm_100a) force-evaluation and integration
+ * hot path for Aster. Plain C types only: no CUDA, torch or C++ types cross
+ * this boundary. Every function returns an int status (ASTER_OK or an
+ * ASTER_ERR_* code) and never exits the process.
+ *
+ * Pointer convention: every pointer is HOST memory unless its name ends in
+ * `_dev`. Vectors are array-of-structs FP64 triples (x,y,z per body), which is
+ * the reference's BodyArray layout (include/Aster/physics/body.h:9-24,
+ * std::vector<vec3> of doubles, include/Aster/physics/vectors.h:44-75).
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *   Solver::compute_forces          include/Aster/simulations/sim_obj.h:34-61
+ *   Parallelized::compute_forces    src/utils/builder_endpoint.cpp:729-757
+ *   SimpleGPU::compute_forces       src/solvers/SimpleGPU.cpp:17-71
+ *   Barnes_Hut::make_tree/compute_forces  src/solvers/barnes_hut.cpp:309-418
+ *   BH_hyper::compute_forces        src/solvers/full_GPU.cpp:519-527
+ *   update_leapfrog(_gpu_3d)        src/physics/tool_chain_impl.cpp:169-185,
+ *                                   src/utils/updater.cpp:53-87
+ *   Simulation::load_gpu_buffers / read_bodies_gpu
+ *                                   src/utils/builder_endpoint.cpp:102-119,424-434
+ *   Graphs::get_total_energy        src/utils/collectors.cpp:19-53
+ */
+#ifndef ASTER_CUDA_H
+#define ASTER_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define ASTER_OK 0
+#define ASTER_ERR_INVALID_ARG 1    /* null pointer, bad enum, n out of range   */
+#define ASTER_ERR_CUDA 2           /* a CUDA runtime call failed               */
+#define ASTER_ERR_OOM 3            /* device allocation failed                 */
+#define ASTER_ERR_NO_STATE 4       /* no bodies uploaded yet                   */
+#define ASTER_ERR_STACK 5          /* tree-walk stack overflow (walk stopped)  */
+#define ASTER_ERR_TREE 6           /* bottom-up climb exceeded its level cap   */
+#define ASTER_ERR_NONFINITE 7      /* NaN/Inf found in inputs or results       */
+#define ASTER_ERR_CANCELLED 8      /* persistent kernel stopped by cancel flag */
+#define ASTER_ERR_UNSUPPORTED 9    /* option combination not implemented       */
+#define ASTER_ERR_TOO_LARGE 10     /* size beyond a fixed capacity             */
+
+/* ---- force law bits: the reference PN_expansion_type bitmask
+ *      (include/Aster/simulations/basic.h:39-53) ------------------------- */
+#define ASTER_NEWTON 0x0001
+#define ASTER_PN1 0x0010
+
+/* ---- enums ------------------------------------------------------------- */
+#define ASTER_FP64 0   /* plain FP64 pair arithmetic                          */
+#define ASTER_MIXED 1  /* FP32 pair arithmetic on double-single relative
+                          positions, compensated accumulation, FP64 results   */
+
+#define ASTER_SOLVER_ALLPAIRS 0 /* replaces Parallelized / SimpleGPU          */
+#define ASTER_SOLVER_LBVH 1     /* replaces Barnes_Hut / BH_hyper             */
+
+typedef struct aster_ctx aster_ctx; /* opaque: device state + scratch        */
+
+/* Physical and algorithmic parameters. The reference reads these from the
+ * Simulation (sim_obj.h:165-180, sim_meta.h:8-60); here they are explicit. */
+typedef struct aster_params {
+    double G;           /* gravitational constant (Simulation::get_G)          */
+    double c;           /* speed of light, used by PN terms (get_c)            */
+    double eps2;        /* softening added to r^2 (Simulation::softening)      */
+    double theta;       /* opening angle (Simulation::theta)                   */
+    double dt;          /* time step (get_dt)                                  */
+    int32_t force_law;  /* ASTER_NEWTON | ASTER_PN1                            */
+    int32_t morton_bits;/* 30 (reference) or 63                                */
+    int32_t compat_mode;/* 1: OpenCL BH_hyper tree semantics (descending order,
+                           body-index tie-break, 1024->0 Morton wrap)         */
+    int32_t reserved;   /* must be 0                                           */
+} aster_params;
+
+/* Tree arrays in the reference's layout (barnes_hut.cpp:338-396): leaves
+ * 0..n-1 in sorted order, internal nodes n..2n-2, root = n, -1 = no child.
+ * Every pointer is host memory of the stated length, or NULL to skip. */
+typedef struct aster_tree_view {
+    uint64_t* codes;        /* [n]  Morton code per body, input order        */
+    uint64_t* sorted_codes; /* [n]  codes in sorted order                    */
+    int32_t* perm;          /* [n]  body index of each sorted leaf           */
+    int32_t* left;          /* [2n-1]                                        */
+    int32_t* right;         /* [2n-1]                                        */
+    int32_t* parent;        /* [2n-1] (parent[root] = -1)                    */
+    int32_t* range_lo;      /* [2n-1] first sorted leaf under the node       */
+    int32_t* range_hi;      /* [2n-1] last sorted leaf under the node        */
+    double* node_mass;      /* [2n-1] FP64 (NodesArray::masses)              */
+    double* node_com;       /* [(2n-1)*3] FP64 (NodesArray::centers_of_mass) */
+    float* node_bmin;       /* [(2n-1)*3] FP32 AABB, rounded outwards        */
+    float* node_bmax;       /* [(2n-1)*3]                                    */
+    float* node_rcrit2;     /* [2n-1] squared opening radius (leaves 0)      */
+    double box;             /* out: Morton cube half-width used              */
+} aster_tree_view;
+
+/* Timing and work counters of the last call that filled them. */
+typedef struct aster_stats {
+    double ms_total;          /* device time of the call (CUDA events)        */
+    double ms_force;          /* of which the force kernel                    */
+    double ms_build;          /* of which the LBVH build                      */
+    double interactions;      /* pair interactions evaluated                  */
+    int32_t max_stack;        /* tree-walk stack high-water mark              */
+    int32_t kernels;          /* kernel launches issued                       */
+} aster_stats;
+
+const char* aster_strerror(int status);
+int aster_version(void);
+
+/* Create a context on CUDA device `device`. `stream` is a cudaStream_t cast
+ * to void*, or NULL for a stream owned by the context. */
+int aster_ctx_create(aster_ctx** out, int device, void* stream);
+int aster_ctx_destroy(aster_ctx* ctx);
+
+/* Host -> device copy of the body state (Simulation::load_gpu_buffers,
+ * builder_endpoint.cpp:102-119). vel may be NULL (zero velocities).
+ * Invalidates the cached acceleration. */
+int aster_state_upload(aster_ctx* ctx, int64_t n, const double* pos,
+                       const double* vel, const double* mass);
+/* Device -> host copy (read_bodies_gpu, builder_endpoint.cpp:424-434); any
+ * pointer may be NULL. acc is the cached acceleration of the current state. */
+int aster_state_download(aster_ctx* ctx, double* pos, double* vel, double* acc);
+int aster_state_size(aster_ctx* ctx, int64_t* n);
+
+/* One all-pairs force evaluation of the current state (skips j == i), the
+ * Parallelized / SimpleGPU replacement. Accelerations are cached on the device
+ * and copied to acc_out (host, n*3) when it is not NULL. */
+int aster_allpairs(aster_ctx* ctx, const aster_params* p, int precision, double* acc_out);
+
+/* All-pairs accelerations for an explicit target list against every body:
+ * targets[nt] body indices, acc_out[nt*3] host. FP64 or mixed. Used for the
+ * sampled accuracy check of the tree code at large n. */
+int aster_allpairs_targets(aster_ctx* ctx, const aster_params* p, int precision,
+                           int64_t nt, const int32_t* targets, double* acc_out);
+
+/* Build the LBVH of the current state (Morton -> stable radix sort ->
+ * Karras tree -> bottom-up moments/bounds). view may be NULL; its non-NULL
+ * arrays are filled. */
+int aster_lbvh_build(aster_ctx* ctx, const aster_params* p, aster_tree_view* view);
+
+/* Build + warp-group traversal (Barnes_Hut / BH_hyper compute_forces
+ * replacement). precision: ASTER_MIXED (FP32 interactions) or ASTER_FP64
+ * (same tree, same interaction lists, FP64 arithmetic). acc_out may be NULL.
+ * group_counts (host, ceil(n/32)) receives the interaction-list length of each
+ * 32-body group when not NULL. */
+int aster_lbvh_forces(aster_ctx* ctx, const aster_params* p, int precision,
+                      double* acc_out, int32_t* group_counts);
+
+/* nsteps kick-drift-kick leapfrog steps of the resident state with one force
+ * evaluation per step (the acceleration is cached across steps; the reference
+ * update_leapfrog evaluates twice per step). solver: ASTER_SOLVER_*. */
+int aster_kdk_steps(aster_ctx* ctx, const aster_params* p, int solver, int precision,
+                    int nsteps);
+
+/* FP64 diagnostics of the current state: total energy with the Plummer
+ * potential -G m_i m_j / sqrt(r^2 + eps2) (consistent with the force), total
+ * momentum p[3]. ref_form = 1 uses the reference formula
+ * -G m_i m_j / (r + eps2) of collectors.cpp:43 instead. */
+int aster_energy(aster_ctx* ctx, const aster_params* p, int ref_form, double* energy,
+                 double* momentum3);
+
+/* Counters of the last force/step call on this context. */
+int aster_get_stats(aster_ctx* ctx, aster_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ASTER_CUDA_H */

@@ -1,0 +1,522 @@
+/*
+ * aster_oracle.c -- CPU restatement of the reference Aster force/integration
+ * hot path, plus FP64 CPU references for the forms the reference lacks.
+ *
+ * TEST INFRASTRUCTURE ONLY. Used by tests/, the golden-fixture script and the
+ * CPU-baseline leg of bench.py as the checker; never linked by the product.
+ * Compiled with -ffp-contract=off (no FMA) so that every FP64/FP32 expression
+ * rounds exactly as written; where the GPU must reproduce an integer or a
+ * decision bit-exactly, the GPU code uses the same operation order with
+ * explicitly rounded intrinsics.
+ *
+ * Pinned against the reference itself: tests/test_oracle.py compares each
+ * function here with the reference CPU code compiled from its own sources
+ * (oracle/_ref/libaster_ref.so) and with the committed golden fixtures.
+ *
+ * Functions and the reference code they restate:
+ *   orc_pair_acc        src/physics/tool_chain_impl.cpp:110-137 (Newton + 1PN, CPU form)
+ *   orc_allpairs        src/utils/builder_endpoint.cpp:729-757 (Parallelized)
+ *   orc_morton30        src/solvers/bh_specialization.cpp:30-46 (get_morton, part1by2)
+ *   orc_morton30_compat include/Aster/kernels/morton_writer.cl.h:72-122 (gen_mortons 3-D)
+ *   orc_sort_codes      src/solvers/barnes_hut.cpp:324 with a stable sort (ties by index)
+ *   orc_karras          src/solvers/barnes_hut.cpp:338-396 (CPU, tie-break on sorted position)
+ *                       include/Aster/kernels/BHH_specific.cl.h:171-272 (compat: body index)
+ *   orc_bottom_up       src/solvers/barnes_hut.cpp:137-152 (NodesArray::unite) + new AABB/opening radius
+ *   orc_lbvh_forces     new group-based traversal (same decisions as the GPU kernel)
+ *   orc_kdk             src/physics/tool_chain_impl.cpp:169-185 restated as kick-drift-kick
+ *                       with the acceleration cached across steps
+ *   orc_energy          Plummer-softened energy (the reference's collectors.cpp:19-53
+ *                       uses -Gm_im_j/(r+softening); orc_energy_ref restates that too)
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#define PN1_FLAG 0x10
+
+/* ------------------------------------------------------------------------ */
+/* threading helper                                                          */
+/* ------------------------------------------------------------------------ */
+typedef void (*orc_range_fn)(void* ctx, long lo, long hi);
+typedef struct { orc_range_fn fn; void* ctx; long n, chunk; long* next; pthread_mutex_t* mu; } orc_job;
+
+static int g_threads = 0;
+void orc_set_threads(int t) { g_threads = t; }
+static int orc_threads(void) {
+    if (g_threads > 0) return g_threads;
+    const char* e = getenv("ASTER_ORACLE_THREADS");
+    int v = e ? atoi(e) : 0;
+    if (v <= 0) v = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    return v > 0 ? v : 1;
+}
+
+static void* orc_worker(void* arg) {
+    orc_job* j = (orc_job*)arg;
+    for (;;) {
+        pthread_mutex_lock(j->mu);
+        long lo = *j->next;
+        *j->next += j->chunk;
+        pthread_mutex_unlock(j->mu);
+        if (lo >= j->n) break;
+        long hi = lo + j->chunk < j->n ? lo + j->chunk : j->n;
+        j->fn(j->ctx, lo, hi);
+    }
+    return NULL;
+}
+
+static void orc_parallel(long n, orc_range_fn fn, void* ctx) {
+    int T = orc_threads();
+    if (T > 256) T = 256;
+    if (n <= 0) return;
+    if (T == 1 || n < 64) { fn(ctx, 0, n); return; }
+    long next = 0;
+    pthread_mutex_t mu;
+    pthread_mutex_init(&mu, NULL);
+    orc_job job = {fn, ctx, n, n / (T * 16) > 0 ? n / (T * 16) : 1, &next, &mu};
+    pthread_t th[256];
+    for (int t = 1; t < T; ++t) pthread_create(&th[t], NULL, orc_worker, &job);
+    orc_worker(&job);
+    for (int t = 1; t < T; ++t) pthread_join(th[t], NULL);
+    pthread_mutex_destroy(&mu);
+}
+
+/* ------------------------------------------------------------------------ */
+/* pair law                                                                  */
+/* ------------------------------------------------------------------------ */
+/* Acceleration on body 1 from body 2 (G, 1/c^2, softening = eps^2 added to r^2).
+ * Newton: G m2 d / r^3 with d = p2 - p1, r^2 = d.d + eps2 (tool_chain_impl.cpp:121-127,
+ * divided by m1 as Parallelized does). 1PN (tool_chain_impl.cpp:110-118) with
+ * n = -(d/r) = (p1-p2)/r:
+ *   a1 = G m2 / r^2 [ n(-v1^2 - 2 v2^2 + 4 v1.v2 + 1.5 (n.v2)^2 + 5 G m1/r + 4 G m2/r)
+ *                     + (v1 - v2)(4 n.v1 - 3 n.v2) ] / c^2
+ * (the reference multiplies by m1 to make a force and Parallelized divides it
+ * back out, so the acceleration is a1 itself). */
+void orc_pair_acc(double G, double inv_c2, double eps2, int pn,
+                  double m1, double m2, const double* v1, const double* v2,
+                  const double* p1, const double* p2, double* a) {
+    double d[3] = {p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]};
+    double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
+    double inv_r = 1.0 / sqrt(r2);
+    double inv_r2 = inv_r * inv_r;
+    double s = G * m2 * inv_r2 * inv_r;
+    a[0] = d[0] * s; a[1] = d[1] * s; a[2] = d[2] * s;
+    if (pn & PN1_FLAG) {
+        double n[3] = {-d[0] * inv_r, -d[1] * inv_r, -d[2] * inv_r};
+        double v1sq = v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2];
+        double v2sq = v2[0] * v2[0] + v2[1] * v2[1] + v2[2] * v2[2];
+        double v12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
+        double nv1 = n[0] * v1[0] + n[1] * v1[1] + n[2] * v1[2];
+        double nv2 = n[0] * v2[0] + n[1] * v2[1] + n[2] * v2[2];
+        double A = -v1sq - 2.0 * v2sq + 4.0 * v12 + 1.5 * nv2 * nv2 + 5.0 * G * m1 * inv_r + 4.0 * G * m2 * inv_r;
+        double Bc = 4.0 * nv1 - 3.0 * nv2;
+        double f = G * m2 * inv_r2 * inv_c2;
+        for (int k = 0; k < 3; ++k) a[k] += (n[k] * A + (v1[k] - v2[k]) * Bc) * f;
+    }
+}
+
+typedef struct {
+    long n, ns; const double *pos, *vel, *m; const long* targets;
+    double G, inv_c2, eps2; int pn; double* acc;
+} allpairs_ctx;
+
+static void allpairs_range(void* c_, long lo, long hi) {
+    allpairs_ctx* c = (allpairs_ctx*)c_;
+    for (long t = lo; t < hi; ++t) {
+        long i = c->targets ? c->targets[t] : t;
+        double ax = 0, ay = 0, az = 0, a[3];
+        for (long j = 0; j < c->n; ++j) {
+            if (j == i) continue;
+            orc_pair_acc(c->G, c->inv_c2, c->eps2, c->pn, c->m[i], c->m[j], c->vel + 3 * i, c->vel + 3 * j,
+                         c->pos + 3 * i, c->pos + 3 * j, a);
+            ax += a[0]; ay += a[1]; az += a[2];
+        }
+        c->acc[3 * t] = ax; c->acc[3 * t + 1] = ay; c->acc[3 * t + 2] = az;
+    }
+}
+
+/* All-pairs accelerations (skip j == i). targets == NULL: every body, else the
+ * nt listed bodies (acc has nt rows). vel may be NULL when pn has no PN bit. */
+void orc_allpairs(long n, const double* pos, const double* vel, const double* m,
+                  double G, double inv_c2, double eps2, int pn,
+                  long nt, const long* targets, double* acc) {
+    double* vtmp = NULL;
+    if (!vel) { vtmp = (double*)calloc((size_t)n * 3, sizeof(double)); vel = vtmp; }
+    allpairs_ctx c = {n, nt, pos, vel, m, targets, G, inv_c2, eps2, pn, acc};
+    orc_parallel(targets ? nt : n, allpairs_range, &c);
+    free(vtmp);
+}
+
+/* ------------------------------------------------------------------------ */
+/* energy / momentum                                                         */
+/* ------------------------------------------------------------------------ */
+typedef struct { long n; const double *pos, *vel, *m; double G, eps2; int ref_form; double* part; } energy_ctx;
+
+static void energy_range(void* c_, long lo, long hi) {
+    energy_ctx* c = (energy_ctx*)c_;
+    for (long i = lo; i < hi; ++i) {
+        const double* v = c->vel + 3 * i;
+        double e = 0.5 * c->m[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (long j = i + 1; j < c->n; ++j) {
+            double dx = c->pos[3 * j] - c->pos[3 * i], dy = c->pos[3 * j + 1] - c->pos[3 * i + 1],
+                   dz = c->pos[3 * j + 2] - c->pos[3 * i + 2];
+            double r2 = dx * dx + dy * dy + dz * dz;
+            double inv = c->ref_form ? 1.0 / (sqrt(r2) + c->eps2) : 1.0 / sqrt(r2 + c->eps2);
+            e -= c->G * c->m[i] * c->m[j] * inv;
+        }
+        c->part[i] = e;
+    }
+}
+
+/* Total energy. ref_form = 0: Plummer potential -G m_i m_j / sqrt(r^2 + eps2),
+ * consistent with the softened force. ref_form = 1: the reference's
+ * collectors.cpp:43 form -G m_i m_j / (r + softening) with softening = eps2. */
+double orc_energy(long n, const double* pos, const double* vel, const double* m,
+                  double G, double eps2, int ref_form) {
+    double* part = (double*)malloc((size_t)n * sizeof(double));
+    energy_ctx c = {n, pos, vel, m, G, eps2, ref_form, part};
+    orc_parallel(n, energy_range, &c);
+    double e = 0;
+    for (long i = 0; i < n; ++i) e += part[i];
+    free(part);
+    return e;
+}
+
+void orc_momentum(long n, const double* vel, const double* m, double* p) {
+    p[0] = p[1] = p[2] = 0;
+    for (long i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) p[k] += m[i] * vel[3 * i + k];
+}
+
+/* ------------------------------------------------------------------------ */
+/* integrators                                                               */
+/* ------------------------------------------------------------------------ */
+/* Kick-drift-kick leapfrog with the acceleration cached between steps:
+ *   v += a dt/2; x += v dt; a = A(x); v += a dt/2
+ * The reference's update_leapfrog (tool_chain_impl.cpp:169-185) is the same map
+ * written as x += v dt + a dt^2/2, v += a dt/2, A(x), v += a dt/2 and evaluates
+ * A twice per step; both produce the same trajectory up to rounding.
+ * acc (n*3) must hold A(x0) on entry (computed here if acc_valid == 0);
+ * acc_steps (nsteps*n*3, optional) receives A(x_{k+1}). */
+void orc_kdk(long n, double* pos, double* vel, const double* m, double G, double inv_c2,
+             double eps2, int pn, double dt, int nsteps, double* acc, int acc_valid,
+             double* acc_steps) {
+    if (!acc_valid) orc_allpairs(n, pos, vel, m, G, inv_c2, eps2, pn, 0, NULL, acc);
+    const double h = 0.5 * dt;
+    for (int k = 0; k < nsteps; ++k) {
+        for (long i = 0; i < 3 * n; ++i) { vel[i] += acc[i] * h; pos[i] += vel[i] * dt; }
+        orc_allpairs(n, pos, vel, m, G, inv_c2, eps2, pn, 0, NULL, acc);
+        for (long i = 0; i < 3 * n; ++i) vel[i] += acc[i] * h;
+        if (acc_steps) memcpy(acc_steps + (size_t)k * n * 3, acc, (size_t)n * 3 * sizeof(double));
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Morton codes                                                              */
+/* ------------------------------------------------------------------------ */
+static uint32_t part1by2_32(uint32_t n) {
+    n = (n | (n << 16)) & 0x030000FFu;
+    n = (n | (n << 8)) & 0x0300F00Fu;
+    n = (n | (n << 4)) & 0x030C30C3u;
+    n = (n | (n << 2)) & 0x09249249u;
+    return n;
+}
+
+static uint64_t part1by2_64(uint64_t n) {
+    n &= 0x1FFFFFull;
+    n = (n | (n << 32)) & 0x001F00000000FFFFull;
+    n = (n | (n << 16)) & 0x001F0000FF0000FFull;
+    n = (n | (n << 8)) & 0x100F00F00F00F00Full;
+    n = (n | (n << 4)) & 0x10C30C30C30C30C3ull;
+    n = (n | (n << 2)) & 0x1249249249249249ull;
+    return n;
+}
+
+/* Reference get_morton: x' = (x + B)/(2B), ix = min((uint32)(x' * 1024), 1023),
+ * code = part(iz)<<2 | part(iy)<<1 | part(ix). A negative x' is undefined
+ * behaviour in the reference; with B = max |coord| it cannot occur, and this
+ * restatement clamps it to 0. */
+static uint32_t quant(double x, double B, double scale, uint32_t maxv) {
+    double t = (x + B) / (2.0 * B);
+    double s = t * scale;
+    if (!(s > 0.0)) return 0;                 /* negative or NaN */
+    if (s >= 4294967296.0) return maxv;
+    uint32_t q = (uint32_t)s;
+    return q < maxv ? q : maxv;
+}
+
+void orc_morton30(long n, const double* pos, double B, uint32_t* codes) {
+    for (long i = 0; i < n; ++i) {
+        uint32_t ix = quant(pos[3 * i], B, 1024.0, 1023u);
+        uint32_t iy = quant(pos[3 * i + 1], B, 1024.0, 1023u);
+        uint32_t iz = quant(pos[3 * i + 2], B, 1024.0, 1023u);
+        codes[i] = (part1by2_32(iz) << 2) | (part1by2_32(iy) << 1) | part1by2_32(ix);
+    }
+}
+
+/* 63-bit variant: 21 bits per axis, x' * 2^21 clamped to 2^21 - 1. */
+void orc_morton63(long n, const double* pos, double B, uint64_t* codes) {
+    for (long i = 0; i < n; ++i) {
+        uint64_t ix = quant(pos[3 * i], B, 2097152.0, 2097151u);
+        uint64_t iy = quant(pos[3 * i + 1], B, 2097152.0, 2097151u);
+        uint64_t iz = quant(pos[3 * i + 2], B, 2097152.0, 2097151u);
+        codes[i] = (part1by2_64(iz) << 2) | (part1by2_64(iy) << 1) | part1by2_64(ix);
+    }
+}
+
+/* OpenCL gen_mortons (morton_writer.cl.h:72-122): clamp x' to [0,1], then
+ * min((uint)(x'*1024), 1024), truncate to 16 bits and expand with the 10-bit
+ * mask, so 1024 (a coordinate exactly at +B) becomes 0 on that axis. */
+void orc_morton30_compat(long n, const double* pos, double B, uint32_t* codes) {
+    for (long i = 0; i < n; ++i) {
+        uint32_t q[3];
+        for (int k = 0; k < 3; ++k) {
+            double t = (pos[3 * i + k] + B) / (2.0 * B);
+            t = fmin(fmax(t, 0.0), 1.0);
+            uint32_t v = (uint32_t)(t * 1024.0);
+            v = v < 1024u ? v : 1024u;
+            q[k] = (uint32_t)(uint16_t)v;
+        }
+        codes[i] = part1by2_32(q[0]) | (part1by2_32(q[1]) << 1) | (part1by2_32(q[2]) << 2);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* sort                                                                      */
+/* ------------------------------------------------------------------------ */
+/* Stable LSD radix sort of (code, index): sorted codes + permutation
+ * (perm[k] = input index of the k-th smallest). bits = 30 or 63.
+ * descending != 0 reproduces the OpenCL bitonic order (radix.cl.h:11-13,26-91):
+ * descending by (code, index). */
+void orc_sort_codes(long n, const uint64_t* codes, int bits, int descending,
+                    uint64_t* sorted, int32_t* perm) {
+    uint64_t* k0 = (uint64_t*)malloc((size_t)n * 8);
+    uint64_t* k1 = (uint64_t*)malloc((size_t)n * 8);
+    int32_t* p0 = (int32_t*)malloc((size_t)n * 4);
+    int32_t* p1 = (int32_t*)malloc((size_t)n * 4);
+    for (long i = 0; i < n; ++i) { k0[i] = codes[i]; p0[i] = (int32_t)i; }
+    for (int shift = 0; shift < bits; shift += 8) {
+        long cnt[257];
+        memset(cnt, 0, sizeof(cnt));
+        for (long i = 0; i < n; ++i) cnt[((k0[i] >> shift) & 0xFF) + 1]++;
+        for (int b = 0; b < 256; ++b) cnt[b + 1] += cnt[b];
+        for (long i = 0; i < n; ++i) {
+            long d = cnt[(k0[i] >> shift) & 0xFF]++;
+            k1[d] = k0[i]; p1[d] = p0[i];
+        }
+        uint64_t* tk = k0; k0 = k1; k1 = tk;
+        int32_t* tp = p0; p0 = p1; p1 = tp;
+    }
+    for (long i = 0; i < n; ++i) {
+        long s = descending ? n - 1 - i : i;
+        sorted[i] = k0[s]; perm[i] = p0[s];
+    }
+    free(k0); free(k1); free(p0); free(p1);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Karras radix tree                                                         */
+/* ------------------------------------------------------------------------ */
+static int clz64(uint64_t x) { return x ? __builtin_clzll(x) : 64; }
+static int clz32(uint32_t x) { return x ? __builtin_clz(x) : 32; }
+
+typedef struct { long n; const uint64_t* codes; const int32_t* perm; int bits; int compat; } karras_in;
+
+/* delta(i,j): common-prefix length of sorted keys i and j; equal codes fall
+ * back to key_bits + clz of the tie-break value: the sorted positions i^j (CPU,
+ * barnes_hut.cpp:333-338) or the body indices (compat, BHH_specific.cl.h:180-189).
+ * 30-bit codes use 32-bit clz as the reference does; 63-bit codes use 64-bit
+ * clz and 64 + clz32 of the tie-break. Out-of-range j gives -1. */
+static int kdelta(const karras_in* k, long i, long j) {
+    if (j < 0 || j >= k->n) return -1;
+    uint64_t a = k->codes[i], b = k->codes[j];
+    if (a == b) {
+        uint32_t t = k->compat ? (uint32_t)(k->perm[i] ^ k->perm[j]) : (uint32_t)(i ^ j);
+        return (k->bits > 32 ? 64 : 32) + clz32(t);
+    }
+    return k->bits > 32 ? clz64(a ^ b) : clz32((uint32_t)(a ^ b));
+}
+
+/* Karras (2012) build. Nodes 0..n-1 are leaves in sorted order, n..2n-2 are
+ * internal (internal i is node n+i), root = n, -1 = no child. Also emits
+ * parent[2n-1] (parent[root] = -1) and the sorted-leaf range [lo, hi] of each
+ * internal node (leaves: [k, k]). */
+void orc_karras(long n, const uint64_t* sorted_codes, const int32_t* perm, int bits, int compat,
+                int32_t* left, int32_t* right, int32_t* parent, int32_t* rlo, int32_t* rhi) {
+    karras_in k = {n, sorted_codes, perm, bits, compat};
+    for (long i = 0; i < 2 * n - 1; ++i) {
+        left[i] = -1; right[i] = -1; parent[i] = -1;
+        rlo[i] = (int32_t)(i < n ? i : -1); rhi[i] = (int32_t)(i < n ? i : -1);
+    }
+    for (long i = 0; i < n - 1; ++i) {
+        int dl = (i == 0) ? -1 : kdelta(&k, i, i - 1);
+        int dr = kdelta(&k, i, i + 1);
+        int d = dr > dl ? 1 : -1;
+        int dmin = d == 1 ? dl : dr;
+        long lmax = 2;
+        while (kdelta(&k, i, i + lmax * d) > dmin) lmax *= 2;
+        long l = 0;
+        for (long t = lmax / 2; t >= 1; t /= 2)
+            if (kdelta(&k, i, i + (l + t) * d) > dmin) l += t;
+        long j = i + l * d;
+        int dnode = kdelta(&k, i, j);
+        long s = 0;
+        long range = j > i ? j - i : i - j;
+        for (long t = (range + 1) / 2; t >= 1; t = (t + 1) / 2) {
+            if (kdelta(&k, i, i + (s + t) * d) > dnode) s += t;
+            if (t == 1) break;
+        }
+        long gamma = i + s * d + (d < 0 ? d : 0);
+        long lo = i < j ? i : j, hi = i < j ? j : i;
+        long node = n + i;
+        left[node] = (int32_t)(lo == gamma ? gamma : n + gamma);
+        right[node] = (int32_t)(hi == gamma + 1 ? gamma + 1 : n + gamma + 1);
+        parent[left[node]] = (int32_t)node;
+        parent[right[node]] = (int32_t)node;
+        rlo[node] = (int32_t)lo; rhi[node] = (int32_t)hi;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* bottom-up moments, bounds, opening radius                                 */
+/* ------------------------------------------------------------------------ */
+/* double -> float rounded down / up (exact emulation of the CUDA __double2float_rd/ru). */
+static float f_rd(double d) { float f = (float)d; if ((double)f > d) f = nextafterf(f, -INFINITY); return f; }
+static float f_ru(double d) { float f = (float)d; if ((double)f < d) f = nextafterf(f, INFINITY); return f; }
+
+/* Node moments in FP64 exactly as NodesArray::unite (barnes_hut.cpp:137-152):
+ *   M = m_R + m_L; c = (c_R m_R + c_L m_L) / M   (component-wise, this order)
+ * plus (new) the node AABB in FP32 (leaf: position rounded outwards; internal:
+ * union of the children) and the squared opening radius
+ *   r_crit = l/theta + |c - box_centre|, l = longest AABB side,
+ * all in FP64, stored as a float rounded up (leaves: 0). */
+void orc_bottom_up(long n, const int32_t* left, const int32_t* right, const int32_t* perm,
+                   const double* pos, const double* m, double theta,
+                   double* node_mass, double* node_com, float* bmin, float* bmax, float* rcrit2) {
+    for (long k = 0; k < n; ++k) {
+        long b = perm[k];
+        node_mass[k] = m[b];
+        for (int a = 0; a < 3; ++a) {
+            node_com[3 * k + a] = pos[3 * b + a];
+            bmin[3 * k + a] = f_rd(pos[3 * b + a]);
+            bmax[3 * k + a] = f_ru(pos[3 * b + a]);
+        }
+        rcrit2[k] = 0.0f;
+    }
+    if (n < 2) return;
+    /* post-order over internal nodes, iterative */
+    long total = 2 * n - 1;
+    int32_t* stack = (int32_t*)malloc((size_t)total * 4);
+    char* done = (char*)calloc((size_t)total, 1);
+    long sp = 0;
+    stack[sp++] = (int32_t)n;
+    while (sp > 0) {
+        int32_t v = stack[sp - 1];
+        int32_t L = left[v], R = right[v];
+        if (v >= n && (!done[L] && L >= n)) { stack[sp++] = L; continue; }
+        if (v >= n && (!done[R] && R >= n)) { stack[sp++] = R; continue; }
+        sp--;
+        if (v < n) { done[v] = 1; continue; }
+        double M = node_mass[R] + node_mass[L];
+        node_mass[v] = M;
+        double lmax = 0.0, ctr[3];
+        for (int a = 0; a < 3; ++a) {
+            node_com[3 * v + a] = (node_com[3 * R + a] * node_mass[R] + node_com[3 * L + a] * node_mass[L]) / M;
+            bmin[3 * v + a] = fminf(bmin[3 * L + a], bmin[3 * R + a]);
+            bmax[3 * v + a] = fmaxf(bmax[3 * L + a], bmax[3 * R + a]);
+            double ext = (double)bmax[3 * v + a] - (double)bmin[3 * v + a];
+            if (ext > lmax) lmax = ext;
+            ctr[a] = 0.5 * ((double)bmin[3 * v + a] + (double)bmax[3 * v + a]);
+        }
+        double dx = node_com[3 * v] - ctr[0], dy = node_com[3 * v + 1] - ctr[1], dz = node_com[3 * v + 2] - ctr[2];
+        double delta = sqrt(dx * dx + dy * dy + dz * dz);
+        double rc = lmax / theta + delta;
+        rcrit2[v] = f_ru(rc * rc);
+        done[v] = 1;
+    }
+    free(stack);
+    free(done);
+}
+
+/* ------------------------------------------------------------------------ */
+/* group-based traversal                                                     */
+/* ------------------------------------------------------------------------ */
+/* The GPU walks the tree once per group of GROUP consecutive sorted bodies
+ * (one warp). A node is opened for the whole group unless it is a leaf or the
+ * squared distance from its FP32 centre of mass to the group's FP32 box exceeds
+ * rcrit2; accepted nodes go to the group's interaction list. Decision
+ * arithmetic is FP32, round-to-nearest, no FMA, in this exact order:
+ *   d_a = max(0, max(glo_a - c_a, c_a - ghi_a)); d2 = (dx*dx + dy*dy) + dz*dz
+ * where c = (float)com and the group box is the min/max of (float)pos.
+ * Every body of the group then sums the list in FP64 (G m d / (d.d+eps2)^1.5,
+ * zero when d.d+eps2 == 0). out_count[g] = list length of group g (optional). */
+#define ORC_GROUP 32
+
+typedef struct {
+    long n; int group; const int32_t *left, *right, *perm; const double *pos, *node_mass, *node_com;
+    const float* rcrit2; double G, eps2; double* acc; int32_t* count; long* list_buf_unused;
+} trav_ctx;
+
+static void trav_range(void* c_, long glo, long ghi) {
+    trav_ctx* c = (trav_ctx*)c_;
+    long total = 2 * c->n - 1;
+    int32_t* stack = (int32_t*)malloc((size_t)(total + 2) * 4);
+    int32_t* list = (int32_t*)malloc((size_t)(total + 2) * 4);
+    for (long g = glo; g < ghi; ++g) {
+        long b0 = g * c->group, b1 = b0 + c->group < c->n ? b0 + c->group : c->n;
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (long k = b0; k < b1; ++k)
+            for (int a = 0; a < 3; ++a) {
+                float p = (float)c->pos[3 * c->perm[k] + a];
+                lo[a] = fminf(lo[a], p); hi[a] = fmaxf(hi[a], p);
+            }
+        long sp = 0, nl = 0;
+        stack[sp++] = c->n >= 2 ? (int32_t)c->n : 0;
+        while (sp > 0) {
+            int32_t v = stack[--sp];
+            if (v < c->n) { list[nl++] = v; continue; }
+            float d[3];
+            for (int a = 0; a < 3; ++a) {
+                float cf = (float)c->node_com[3 * v + a];
+                float u = lo[a] - cf, w = cf - hi[a];
+                float t = u > w ? u : w;
+                d[a] = t > 0.0f ? t : 0.0f;
+            }
+            float d2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
+            if (d2 > c->rcrit2[v]) { list[nl++] = v; continue; }
+            stack[sp++] = c->right[v];
+            stack[sp++] = c->left[v];
+        }
+        if (c->count) c->count[g] = (int32_t)nl;
+        for (long k = b0; k < b1; ++k) {
+            long b = c->perm[k];
+            const double* x = c->pos + 3 * b;
+            double ax = 0, ay = 0, az = 0;
+            for (long e = 0; e < nl; ++e) {
+                int32_t v = list[e];
+                const double* y = c->node_com + 3 * v;
+                double dx = y[0] - x[0], dy = y[1] - x[1], dz = y[2] - x[2];
+                double r2 = dx * dx + dy * dy + dz * dz + c->eps2;
+                if (r2 == 0.0) continue;
+                double inv = 1.0 / sqrt(r2);
+                double s = c->node_mass[v] * inv * inv * inv;
+                ax += dx * s; ay += dy * s; az += dz * s;
+            }
+            c->acc[3 * b] = c->G * ax; c->acc[3 * b + 1] = c->G * ay; c->acc[3 * b + 2] = c->G * az;
+        }
+    }
+    free(stack);
+    free(list);
+}
+
+/* acc is indexed by body (input order). group_count (optional) has
+ * ceil(n/group) entries. */
+void orc_lbvh_forces(long n, int group, const int32_t* left, const int32_t* right, const int32_t* perm,
+                     const double* pos, const double* node_mass, const double* node_com,
+                     const float* rcrit2, double G, double eps2, double* acc, int32_t* group_count) {
+    if (group <= 0) group = ORC_GROUP;
+    trav_ctx c = {n, group, left, right, perm, pos, node_mass, node_com, rcrit2, G, eps2, acc, group_count, NULL};
+    orc_parallel((n + group - 1) / group, trav_range, &c);
+}

@@ -1,0 +1,256 @@
+"""ctypes front end for the two CPU checkers. TEST INFRASTRUCTURE ONLY.
+
+* ``Ref``: the reference Aster CPU code compiled unmodified from its sources
+  (oracle/Makefile -> oracle/_ref/libaster_ref.so). Exists where the reference
+  sources were available at build time; the library travels prebuilt.
+* ``Orc``: the CPU restatement in oracle/aster_oracle.c
+  (oracle/build_oracle.sh -> oracle/_build/libaster_oracle.so).
+
+Only tests/, the golden-fixture script, ``__graft_entry__.smoke`` and the
+CPU-baseline leg of bench.py may use this module, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_LIB = HERE / "_ref" / "libaster_ref.so"
+ORC_LIB = HERE / "_build" / "libaster_oracle.so"
+
+_D = ctypes.POINTER(ctypes.c_double)
+_F = ctypes.POINTER(ctypes.c_float)
+_I32 = ctypes.POINTER(ctypes.c_int32)
+_U32 = ctypes.POINTER(ctypes.c_uint32)
+_U64 = ctypes.POINTER(ctypes.c_uint64)
+_L = ctypes.POINTER(ctypes.c_long)
+
+NEWTON = 0x1
+PN1 = 0x10
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Ref:
+    """The reference CPU implementation (one Simulation per process)."""
+
+    _lib = None
+
+    def __init__(self):
+        if Ref._lib is None:
+            if not REF_LIB.exists():
+                raise FileNotFoundError(f"{REF_LIB} missing: run `make -C oracle`")
+            lib = ctypes.CDLL(str(REF_LIB))
+            lib.ref_setup.argtypes = [ctypes.c_int, _D, _D, _D] + [ctypes.c_double] * 6 + [ctypes.c_int, ctypes.c_int]
+            lib.ref_get_state.argtypes = [_D, _D, _D]
+            lib.ref_compute_forces.argtypes = [_D]
+            lib.ref_leapfrog.argtypes = [ctypes.c_int, _D]
+            lib.ref_energy.restype = ctypes.c_double
+            lib.ref_bh_tree.argtypes = [_U32, _I32, _I32, _D, _D]
+            lib.ref_pair_force.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D, _D, _D, _D]
+            Ref._lib = lib
+        self.lib = Ref._lib
+        self.n = 0
+
+    @staticmethod
+    def available() -> bool:
+        return REF_LIB.exists()
+
+    def threads(self) -> int:
+        return self.lib.ref_threads()
+
+    def setup(self, pos, vel, m, G=1.0, c=299792458.0, dt=1e-3, eps2=0.0, theta=0.5,
+              box=None, force_law=NEWTON, solver="allpairs"):
+        pos, vel, m = _c64(pos), _c64(vel), _c64(m)
+        if box is None:
+            box = float(np.abs(pos).max())
+        kind = {"allpairs": 1, "bh": 2}[solver]
+        self.n = len(m)
+        rc = self.lib.ref_setup(self.n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, c, dt, eps2, theta,
+                                box, force_law, kind)
+        if rc != 0:
+            raise RuntimeError(f"ref_setup failed: {rc}")
+        return self
+
+    def forces(self):
+        acc = np.zeros((self.n, 3))
+        self.lib.ref_compute_forces(_p(acc, _D))
+        return acc
+
+    def leapfrog(self, nsteps, record_acc=False):
+        acc = np.zeros((nsteps, self.n, 3)) if record_acc else None
+        self.lib.ref_leapfrog(nsteps, _p(acc, _D))
+        return acc
+
+    def state(self):
+        pos, vel, acc = (np.zeros((self.n, 3)) for _ in range(3))
+        self.lib.ref_get_state(_p(pos, _D), _p(vel, _D), _p(acc, _D))
+        return pos, vel, acc
+
+    def energy(self) -> float:
+        return self.lib.ref_energy()
+
+    def bh_tree(self):
+        n = self.n
+        codes = np.zeros(n, np.uint32)
+        left = np.zeros(2 * n - 1, np.int32)
+        right = np.zeros(2 * n - 1, np.int32)
+        nm = np.zeros(2 * n - 1)
+        nc = np.zeros((2 * n - 1, 3))
+        rc = self.lib.ref_bh_tree(_p(codes, _U32), _p(left, _I32), _p(right, _I32), _p(nm, _D), _p(nc, _D))
+        if rc != 0:
+            raise RuntimeError(f"ref_bh_tree failed: {rc}")
+        return dict(codes=codes, left=left, right=right, node_mass=nm, node_com=nc)
+
+    def pair_force(self, m1, m2, v1, v2, p1, p2):
+        f = np.zeros(3)
+        args = [_c64(v1), _c64(v2), _c64(p1), _c64(p2)]
+        self.lib.ref_pair_force(m1, m2, *[_p(a, _D) for a in args], _p(f, _D))
+        return f
+
+
+class Orc:
+    """The CPU restatement (oracle/aster_oracle.c)."""
+
+    _lib = None
+
+    def __init__(self):
+        if Orc._lib is None:
+            if not ORC_LIB.exists():
+                raise FileNotFoundError(f"{ORC_LIB} missing: run oracle/build_oracle.sh")
+            lib = ctypes.CDLL(str(ORC_LIB))
+            lib.orc_pair_acc.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                                 _D, _D, _D, _D, _D]
+            lib.orc_allpairs.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_int, ctypes.c_long, _L, _D]
+            lib.orc_energy.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+            lib.orc_energy.restype = ctypes.c_double
+            lib.orc_momentum.argtypes = [ctypes.c_long, _D, _D, _D]
+            lib.orc_kdk.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_double, ctypes.c_int, _D, ctypes.c_int, _D]
+            lib.orc_morton30.argtypes = [ctypes.c_long, _D, ctypes.c_double, _U32]
+            lib.orc_morton30_compat.argtypes = [ctypes.c_long, _D, ctypes.c_double, _U32]
+            lib.orc_morton63.argtypes = [ctypes.c_long, _D, ctypes.c_double, _U64]
+            lib.orc_sort_codes.argtypes = [ctypes.c_long, _U64, ctypes.c_int, ctypes.c_int, _U64, _I32]
+            lib.orc_karras.argtypes = [ctypes.c_long, _U64, _I32, ctypes.c_int, ctypes.c_int,
+                                       _I32, _I32, _I32, _I32, _I32]
+            lib.orc_bottom_up.argtypes = [ctypes.c_long, _I32, _I32, _I32, _D, _D, ctypes.c_double,
+                                          _D, _D, _F, _F, _F]
+            lib.orc_lbvh_forces.argtypes = [ctypes.c_long, ctypes.c_int, _I32, _I32, _I32, _D, _D, _D, _F,
+                                            ctypes.c_double, ctypes.c_double, _D, _I32]
+            lib.orc_set_threads.argtypes = [ctypes.c_int]
+            Orc._lib = lib
+        self.lib = Orc._lib
+
+    def set_threads(self, t: int):
+        self.lib.orc_set_threads(int(t))
+
+    def pair_acc(self, G, inv_c2, eps2, pn, m1, m2, v1, v2, p1, p2):
+        a = np.zeros(3)
+        args = [_c64(v1), _c64(v2), _c64(p1), _c64(p2)]
+        self.lib.orc_pair_acc(G, inv_c2, eps2, pn, m1, m2, *[_p(x, _D) for x in args], _p(a, _D))
+        return a
+
+    def allpairs(self, pos, m, G=1.0, eps2=0.0, vel=None, inv_c2=0.0, pn=NEWTON, targets=None):
+        pos, m = _c64(pos), _c64(m)
+        vel = _c64(vel) if vel is not None else None
+        n = len(m)
+        tg = None if targets is None else np.ascontiguousarray(targets, dtype=np.int64)
+        nt = n if tg is None else len(tg)
+        acc = np.zeros((nt, 3))
+        self.lib.orc_allpairs(n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, inv_c2, eps2, pn, nt,
+                              _p(tg, _L) if tg is not None else None, _p(acc, _D))
+        return acc
+
+    def energy(self, pos, vel, m, G=1.0, eps2=0.0, ref_form=False):
+        pos, vel, m = _c64(pos), _c64(vel), _c64(m)
+        return self.lib.orc_energy(len(m), _p(pos, _D), _p(vel, _D), _p(m, _D), G, eps2, int(ref_form))
+
+    def momentum(self, vel, m):
+        vel, m = _c64(vel), _c64(m)
+        p = np.zeros(3)
+        self.lib.orc_momentum(len(m), _p(vel, _D), _p(m, _D), _p(p, _D))
+        return p
+
+    def kdk(self, pos, vel, m, dt, nsteps, G=1.0, eps2=0.0, inv_c2=0.0, pn=NEWTON, record_acc=False):
+        pos, vel, m = _c64(pos).copy(), _c64(vel).copy(), _c64(m)
+        n = len(m)
+        acc = np.zeros((n, 3))
+        accs = np.zeros((nsteps, n, 3)) if record_acc else None
+        self.lib.orc_kdk(n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, inv_c2, eps2, pn, dt, nsteps,
+                         _p(acc, _D), 0, _p(accs, _D))
+        return pos, vel, acc, accs
+
+    def morton30(self, pos, B, compat=False):
+        pos = _c64(pos)
+        codes = np.zeros(len(pos), np.uint32)
+        fn = self.lib.orc_morton30_compat if compat else self.lib.orc_morton30
+        fn(len(pos), _p(pos, _D), B, _p(codes, _U32))
+        return codes
+
+    def morton63(self, pos, B):
+        pos = _c64(pos)
+        codes = np.zeros(len(pos), np.uint64)
+        self.lib.orc_morton63(len(pos), _p(pos, _D), B, _p(codes, _U64))
+        return codes
+
+    def sort_codes(self, codes, bits=30, descending=False):
+        c = np.ascontiguousarray(codes, dtype=np.uint64)
+        n = len(c)
+        s = np.zeros(n, np.uint64)
+        perm = np.zeros(n, np.int32)
+        self.lib.orc_sort_codes(n, _p(c, _U64), bits, int(descending), _p(s, _U64), _p(perm, _I32))
+        return s, perm
+
+    def karras(self, sorted_codes, perm, bits=30, compat=False):
+        sc = np.ascontiguousarray(sorted_codes, dtype=np.uint64)
+        perm = np.ascontiguousarray(perm, dtype=np.int32)
+        n = len(sc)
+        out = {k: np.zeros(2 * n - 1, np.int32) for k in ("left", "right", "parent", "range_lo", "range_hi")}
+        self.lib.orc_karras(n, _p(sc, _U64), _p(perm, _I32), bits, int(compat),
+                            *[_p(out[k], _I32) for k in ("left", "right", "parent", "range_lo", "range_hi")])
+        return out
+
+    def bottom_up(self, left, right, perm, pos, m, theta):
+        n = len(m)
+        pos, m = _c64(pos), _c64(m)
+        nm = np.zeros(2 * n - 1)
+        nc = np.zeros((2 * n - 1, 3))
+        bmin = np.zeros((2 * n - 1, 3), np.float32)
+        bmax = np.zeros((2 * n - 1, 3), np.float32)
+        rc2 = np.zeros(2 * n - 1, np.float32)
+        args = [np.ascontiguousarray(a, dtype=np.int32) for a in (left, right, perm)]
+        self.lib.orc_bottom_up(n, *[_p(a, _I32) for a in args], _p(pos, _D), _p(m, _D), theta,
+                               _p(nm, _D), _p(nc, _D), _p(bmin, _F), _p(bmax, _F), _p(rc2, _F))
+        return dict(node_mass=nm, node_com=nc, bmin=bmin, bmax=bmax, rcrit2=rc2)
+
+    def lbvh_forces(self, tree, perm, pos, G, eps2, group=32):
+        n = len(perm)
+        pos = _c64(pos)
+        acc = np.zeros((n, 3))
+        cnt = np.zeros((n + group - 1) // group, np.int32)
+        args = [np.ascontiguousarray(a, dtype=np.int32) for a in (tree["left"], tree["right"], perm)]
+        self.lib.orc_lbvh_forces(n, group, *[_p(a, _I32) for a in args], _p(pos, _D),
+                                 _p(tree["node_mass"], _D), _p(tree["node_com"], _D), _p(tree["rcrit2"], _F),
+                                 G, eps2, _p(acc, _D), _p(cnt, _I32))
+        return acc, cnt
+
+    def lbvh(self, pos, m, theta, B=None, bits=30):
+        """Full CPU LBVH build (Morton -> stable sort -> Karras -> bottom-up)."""
+        if B is None:
+            B = float(np.abs(pos).max())
+        codes = self.morton30(pos, B).astype(np.uint64) if bits == 30 else self.morton63(pos, B)
+        sc, perm = self.sort_codes(codes, bits=bits)
+        t = self.karras(sc, perm, bits=bits)
+        t.update(self.bottom_up(t["left"], t["right"], perm, pos, m, theta))
+        t.update(codes=codes, sorted_codes=sc, perm=perm, box=B)
+        return t

@@ -1,0 +1,109 @@
+"""Generate the golden fixtures in this directory from the REFERENCE Aster CPU
+code, compiled unmodified from its sources (oracle/Makefile ->
+oracle/_ref/libaster_ref.so). Run here, where the reference sources exist:
+
+    make -C oracle && python tests/golden/make_golden.py
+
+The fixtures are committed; the tests read them on machines without the
+reference. Inputs come from the seeded generators in aster_b200/gen.py.
+
+Fixtures:
+  allpairs_plummer512.npz   Parallelized::compute_forces (Newton, and Newton+PN1
+                            with c=100 and boosted velocities), eps2=1e-4,
+                            reference get_total_energy.
+  leapfrog_plummer4096.npz  C1 setup (N=4096 Plummer, eps=0.01, dt=1e-3):
+                            update_leapfrog x 100 with Parallelized; accelerations
+                            after steps 1, 10, 50, 100; final x, v; energies.
+  tree_plummer4096.npz      Barnes_Hut::make_tree + unite on a lognormal-mass
+                            Plummer sphere with 64 duplicated positions (forces
+                            Morton ties): codes, left, right, node masses/COMs.
+  tree_small.npz            the same for n = 2, 3, 5, 33 and an all-equal set.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from aster_b200 import gen  # noqa: E402
+from oracle.oracle import NEWTON, PN1, Ref  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def allpairs_fixture(ref: Ref):
+    pos, vel, m = gen.plummer(512, 1001)
+    B = gen.bounding_cube(pos)
+    ref.setup(pos, vel, m, G=1.0, eps2=1e-4, box=B)
+    acc = ref.forces()
+    e_ref = ref.energy()
+    vb = vel * 30.0
+    ref.setup(pos, vb, m, G=1.0, c=100.0, eps2=1e-4, box=B, force_law=NEWTON | PN1)
+    acc_pn = ref.forces()
+    np.savez_compressed(OUT / "allpairs_plummer512.npz", pos=pos, vel=vel, m=m, eps2=1e-4, acc=acc,
+                        energy_ref_form=e_ref, vel_pn=vb, c_pn=100.0, acc_pn1=acc_pn)
+
+
+def leapfrog_fixture(ref: Ref):
+    pos, vel, m = gen.plummer(4096, 1001)
+    B = gen.bounding_cube(pos)
+    eps2, dt = 1e-4, 1e-3
+    ref.setup(pos, vel, m, G=1.0, dt=dt, eps2=eps2, box=B)
+    e0 = ref.energy()
+    keep = [0, 9, 49, 99]
+    accs = []
+    for k in range(100):
+        a = ref.leapfrog(1, record_acc=True)[0]
+        if k in keep:
+            accs.append(a)
+    p1, v1, _ = ref.state()
+    e1 = ref.energy()
+    np.savez_compressed(OUT / "leapfrog_plummer4096.npz", pos=pos, vel=vel, m=m, eps2=eps2, dt=dt, steps=100,
+                        acc_steps=np.array(keep) + 1, acc=np.stack(accs), pos_final=p1, vel_final=v1,
+                        energy0_ref_form=e0, energy1_ref_form=e1)
+
+
+def tree_case(ref: Ref, pos, m):
+    vel = np.zeros_like(pos)
+    B = gen.bounding_cube(pos)
+    ref.setup(pos, vel, m, G=1.0, eps2=2.5e-5, theta=0.5, box=B, solver="bh")
+    t = ref.bh_tree()
+    return dict(pos=pos, m=m, box=B, codes=t["codes"], left=t["left"], right=t["right"],
+                node_mass=t["node_mass"], node_com=t["node_com"])
+
+
+def tree_fixture(ref: Ref):
+    pos, _, m = gen.plummer(4096, 1002, masses="lognormal")
+    rng = np.random.default_rng(7)
+    src = rng.choice(4096, 64, replace=False)
+    dst = rng.choice(np.setdiff1d(np.arange(4096), src), 64, replace=False)
+    pos[dst] = pos[src]  # exact duplicates: equal codes, tie-break exercised
+    d = tree_case(ref, pos, m)
+    np.savez_compressed(OUT / "tree_plummer4096.npz", **d)
+    small = {}
+    for n in (2, 3, 5, 33):
+        p, _, mm = gen.plummer(n, 2000 + n)
+        for k, v in tree_case(ref, p, mm).items():
+            small[f"n{n}_{k}"] = v
+    p = np.tile(np.array([[0.25, -0.5, 0.125]]), (9, 1))
+    p[0] = [1.0, 1.0, 1.0]  # one distinct body so the cube is not degenerate
+    for k, v in tree_case(ref, p, np.full(9, 1.0 / 9)).items():
+        small[f"eq9_{k}"] = v
+    np.savez_compressed(OUT / "tree_small.npz", **small)
+
+
+def main():
+    ref = Ref()
+    allpairs_fixture(ref)
+    leapfrog_fixture(ref)
+    tree_fixture(ref)
+    for f in sorted(OUT.glob("*.npz")):
+        print(f.name, f.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,124 @@
+"""All-pairs force kernels (FP64 and mixed) against the reference's own
+accelerations (golden fixtures) and the CPU oracle, through the C ABI.
+
+Tolerances (relative L2 over all components, stated per test):
+  FP64 vs reference/oracle       1e-12
+  mixed (FP32 pairs, compensated) vs FP64 oracle   1e-6
+"""
+import numpy as np
+import pytest
+
+from aster_b200 import gen
+from aster_b200.api import FP64, MIXED, NEWTON, PN1, Params
+from conftest import golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-12
+TOL_MIXED = 1e-6
+
+
+def test_fp64_matches_reference_golden(ctx):
+    g = golden("allpairs_plummer512.npz")
+    ctx.upload(g["pos"], g["vel"], g["m"])
+    a = ctx.allpairs(Params(eps2=float(g["eps2"])), FP64)
+    assert rel_l2(a, g["acc"]) < TOL_FP64
+
+
+def test_mixed_matches_reference_golden(ctx):
+    g = golden("allpairs_plummer512.npz")
+    ctx.upload(g["pos"], g["vel"], g["m"])
+    a = ctx.allpairs(Params(eps2=float(g["eps2"])), MIXED)
+    assert rel_l2(a, g["acc"]) < TOL_MIXED
+
+
+@pytest.mark.parametrize("prec,tol", [(FP64, TOL_FP64), (MIXED, TOL_MIXED)])
+def test_pn1_matches_reference_golden(ctx, prec, tol):
+    g = golden("allpairs_plummer512.npz")
+    ctx.upload(g["pos"], g["vel_pn"], g["m"])
+    p = Params(eps2=float(g["eps2"]), c=float(g["c_pn"]), force_law=NEWTON | PN1)
+    a = ctx.allpairs(p, prec)
+    assert rel_l2(a, g["acc_pn1"]) < tol
+    # the PN part alone (acc_pn1 - newton) to 1e-4 relative in mixed precision
+    newton = golden("allpairs_plummer512.npz")["acc"]
+    assert rel_l2(a - newton, g["acc_pn1"] - newton) < (1e-10 if prec == FP64 else 1e-3)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 31, 33, 127, 129, 1000, 4097])
+def test_ragged_sizes_vs_oracle(ctx, orc, n):
+    pos, vel, m = gen.plummer(n, 500 + n) if n > 1 else (np.array([[0.3, -0.2, 0.1]]), np.zeros((1, 3)), np.ones(1))
+    ctx.upload(pos, vel, m)
+    p = Params(eps2=1e-4)
+    ref = orc.allpairs(pos, m, 1.0, 1e-4)
+    a64 = ctx.allpairs(p, FP64)
+    a32 = ctx.allpairs(p, MIXED)
+    if n == 1:
+        assert np.all(a64 == 0) and np.all(a32 == 0)
+        return
+    assert rel_l2(a64, ref) < TOL_FP64
+    assert rel_l2(a32, ref) < TOL_MIXED
+
+
+def test_zero_softening_coincident_bodies(ctx):
+    """eps2 = 0 with exact duplicates: zero-distance pairs are skipped (the
+    reference would divide by zero); every other pair is exact."""
+    pos, vel, m = gen.plummer(300, 9)
+    pos[10] = pos[20]
+    pos[11] = pos[20]
+    ctx.upload(pos, vel, m)
+    d = pos[None, :, :] - pos[:, None, :]
+    r2 = (d ** 2).sum(-1)
+    with np.errstate(divide="ignore"):
+        w = np.where(r2 > 0, r2 ** -1.5, 0.0)
+    ref = (d * (m[None, :, None] * w[:, :, None])).sum(1)
+    for prec, tol in ((FP64, TOL_FP64), (MIXED, TOL_MIXED)):
+        a = ctx.allpairs(Params(eps2=0.0), prec)
+        assert np.isfinite(a).all()
+        assert rel_l2(a, ref) < tol
+
+
+def test_targets_api(ctx, orc):
+    pos, vel, m = gen.plummer(20000, 31, masses="lognormal")
+    ctx.upload(pos, vel, m)
+    tg = np.random.default_rng(1).choice(20000, 300, replace=False).astype(np.int32)
+    ref = orc.allpairs(pos, m, 1.0, 2.5e-5, targets=tg)
+    p = Params(eps2=2.5e-5)
+    assert rel_l2(ctx.allpairs_targets(p, tg, FP64), ref) < TOL_FP64
+    assert rel_l2(ctx.allpairs_targets(p, tg, MIXED), ref) < TOL_MIXED
+
+
+def test_disk_mixed_precision_small(ctx, orc):
+    """Cold disk with eps = 0.002 (C3 setup at n = 16384): close pairs far
+    from the origin are where plain FP32 positions would fail."""
+    pos, vel, m = gen.exponential_disk(16384, 1003)
+    ctx.upload(pos, vel, m)
+    p = Params(eps2=0.002 ** 2)
+    ref = orc.allpairs(pos, m, 1.0, p.eps2)
+    assert rel_l2(ctx.allpairs(p, FP64), ref) < TOL_FP64
+    assert rel_l2(ctx.allpairs(p, MIXED), ref) < TOL_MIXED
+
+
+def test_disk_full_size_sampled(ctx, orc):
+    """C3 at full size (n = 262144): mixed vs FP64 on every body, and both
+    against the CPU oracle on 256 sampled targets."""
+    pos, vel, m = gen.exponential_disk(262144, 1003)
+    ctx.upload(pos, vel, m)
+    p = Params(eps2=0.002 ** 2)
+    a64 = ctx.allpairs(p, FP64)
+    a32 = ctx.allpairs(p, MIXED)
+    assert rel_l2(a32, a64) < TOL_MIXED
+    tg = np.random.default_rng(3).choice(262144, 256, replace=False)
+    ref = orc.allpairs(pos, m, 1.0, p.eps2, targets=tg)
+    assert rel_l2(a64[tg], ref) < TOL_FP64
+    assert rel_l2(a32[tg], ref) < TOL_MIXED
+
+
+def test_invalid_arguments(ctx):
+    from aster_b200.api import AsterError
+    ctx.upload(*gen.plummer(64, 1))
+    with pytest.raises(AsterError):
+        ctx.allpairs(Params(eps2=-1.0), FP64)
+    with pytest.raises(AsterError):
+        ctx.allpairs(Params(), 7)
+    with pytest.raises(AsterError):
+        ctx.upload(np.array([[np.nan, 0, 0]]), None, np.ones(1))

@@ -1,0 +1,77 @@
+"""Fused kick-drift-kick leapfrog (C1: N=4096 Plummer, eps=0.01, dt=1e-3,
+100 steps) against the reference's own update_leapfrog trajectory (golden
+fixture) and the CPU oracle.
+
+Tolerances: FP64 accelerations/positions 1e-10 relative L2 after up to 100
+steps (only rounding differs); mixed 1e-6. Energy drift over 100 steps
+|dE/E0| < 1e-6 for both; total momentum stays below 1e-12 (FP64) / 1e-8 (mixed).
+"""
+import numpy as np
+import pytest
+
+from aster_b200.api import FP64, MIXED, SOLVER_ALLPAIRS, Params
+from conftest import golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("prec,tol", [(FP64, 1e-10), (MIXED, 1e-6)])
+def test_c1_trajectory_matches_reference(ctx, prec, tol):
+    g = golden("leapfrog_plummer4096.npz")
+    p = Params(eps2=float(g["eps2"]), dt=float(g["dt"]))
+    ctx.upload(g["pos"], g["vel"], g["m"])
+    e0, mom0 = ctx.energy(p)
+    done = 0
+    for k, step in enumerate(g["acc_steps"]):
+        ctx.kdk_steps(p, int(step) - done, SOLVER_ALLPAIRS, prec)
+        done = int(step)
+        _, _, acc = ctx.download()
+        assert rel_l2(acc, g["acc"][k]) < tol, (step, rel_l2(acc, g["acc"][k]))
+    pos, vel, _ = ctx.download()
+    assert rel_l2(pos, g["pos_final"]) < tol
+    assert rel_l2(vel, g["vel_final"]) < tol
+    e1, mom1 = ctx.energy(p)
+    assert abs(e1 - e0) / abs(e0) < 1e-6
+    assert np.abs(mom1).max() < (1e-12 if prec == FP64 else 1e-8)
+    # the reference's own energy formula, for its own drift number
+    er0, _ = ctx.energy(p, ref_form=True)
+    assert abs(er0 - float(g["energy0_ref_form"])) < 1e-12 * abs(er0)
+
+
+def test_kdk_matches_oracle_kdk(ctx, orc):
+    g = golden("leapfrog_plummer4096.npz")
+    p = Params(eps2=float(g["eps2"]), dt=float(g["dt"]))
+    ctx.upload(g["pos"], g["vel"], g["m"])
+    ctx.kdk_steps(p, 5, SOLVER_ALLPAIRS, FP64)
+    pos, vel, acc = ctx.download()
+    op, ov, oa, _ = orc.kdk(g["pos"], g["vel"], g["m"], p.dt, 5, eps2=p.eps2)
+    assert rel_l2(pos, op) < 1e-13
+    assert rel_l2(vel, ov) < 1e-12
+    assert rel_l2(acc, oa) < 1e-12
+
+
+def test_energy_matches_oracle(ctx, orc):
+    g = golden("leapfrog_plummer4096.npz")
+    ctx.upload(g["pos"], g["vel"], g["m"])
+    e, mom = ctx.energy(Params(eps2=float(g["eps2"])))
+    eo = orc.energy(g["pos"], g["vel"], g["m"], 1.0, float(g["eps2"]))
+    assert abs(e - eo) < 1e-12 * abs(eo)
+    np.testing.assert_allclose(mom, orc.momentum(g["vel"], g["m"]), atol=1e-15)
+
+
+def test_simulation_interface(orc):
+    """Reference-shaped driver: Simulation + CudaAllPairs + CudaKDK."""
+    from aster_b200 import api
+    g = golden("leapfrog_plummer4096.npz")
+    sim = api.Simulation(g["pos"], g["vel"], g["m"], dt=float(g["dt"]), softening=float(g["eps2"]))
+    sim.solver = api.CudaAllPairs(sim)
+    sim.updater = api.CudaKDK(sim)
+    sim.load()
+    sim.solver.compute_forces()
+    assert rel_l2(sim.bodies.accs, orc.allpairs(g["pos"], g["m"], 1.0, float(g["eps2"]))) < 1e-12
+    sim.step()
+    rep = sim.integrate(9, precision_test=True)
+    assert rep["precision"] < 1e-7
+    assert sim.time_passed == 10
+    op, ov, _, _ = orc.kdk(g["pos"], g["vel"], g["m"], float(g["dt"]), 10, eps2=float(g["eps2"]))
+    assert rel_l2(sim.bodies.positions, op) < 1e-12

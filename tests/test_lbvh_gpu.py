@@ -1,0 +1,157 @@
+"""LBVH Barnes-Hut on the GPU against the reference's own tree (golden
+fixtures from Barnes_Hut::make_tree) and the CPU oracle.
+
+Bit-exact: Morton codes, sorted order (ties by body index), children,
+parents, node ranges, FP64 node masses and centres of mass (NodesArray::unite
+order), FP32 bounds and opening radii, per-group interaction-list lengths.
+Forces: FP64 walk vs the oracle's FP64 sum over the same lists 1e-12;
+mixed walk 1e-6 (relative L2). Approximation error vs FP64 all-pairs is
+reported and bounded (theta = 0.5: < 5e-3; theta = 0: < 1e-12).
+"""
+import numpy as np
+import pytest
+
+from aster_b200 import gen
+from aster_b200.api import FP64, MIXED, SOLVER_LBVH, Params
+from conftest import golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _tree_vs_golden(ctx, d):
+    ctx.upload(d["pos"], np.zeros_like(d["pos"]), d["m"])
+    t = ctx.lbvh_build(Params(theta=0.5))
+    assert t["box"] == float(d["box"])
+    np.testing.assert_array_equal(t["codes"], d["codes"].astype(np.uint64))
+    np.testing.assert_array_equal(t["left"], d["left"])
+    np.testing.assert_array_equal(t["right"], d["right"])
+    np.testing.assert_array_equal(t["node_mass"], d["node_mass"])
+    np.testing.assert_array_equal(t["node_com"], d["node_com"])
+    return t
+
+
+def test_tree_bit_exact_vs_reference(ctx, orc):
+    d = golden("tree_plummer4096.npz")
+    t = _tree_vs_golden(ctx, d)
+    o = orc.lbvh(d["pos"], d["m"], 0.5, B=float(d["box"]))
+    for k in ("sorted_codes", "perm", "parent", "range_lo", "range_hi"):
+        np.testing.assert_array_equal(t[k], o[k], err_msg=k)
+    np.testing.assert_array_equal(t["node_bmin"], o["bmin"])
+    np.testing.assert_array_equal(t["node_bmax"], o["bmax"])
+    np.testing.assert_array_equal(t["node_rcrit2"], o["rcrit2"])
+
+
+@pytest.mark.parametrize("case", ["n2", "n3", "n5", "n33", "eq9"])
+def test_small_trees_vs_reference(ctx, case):
+    d = golden("tree_small.npz")
+    _tree_vs_golden(ctx, {k[len(case) + 1:]: d[k] for k in d.files if k.startswith(case + "_")})
+
+
+def test_single_body(ctx):
+    ctx.upload(np.array([[0.5, 0.25, -1.0]]), None, np.array([2.0]))
+    acc = ctx.lbvh_forces(Params(eps2=1e-4), MIXED)
+    assert np.all(acc == 0)
+
+
+@pytest.mark.parametrize("bits", [30, 63])
+def test_tree_vs_oracle_ragged(ctx, orc, bits):
+    for n in (64, 1000, 4097, 70001):
+        pos, _, m = gen.plummer(n, 300 + n, masses="lognormal")
+        pos[n // 3] = pos[n // 2]
+        ctx.upload(pos, None, m)
+        t = ctx.lbvh_build(Params(theta=0.5, morton_bits=bits))
+        o = orc.lbvh(pos, m, 0.5, bits=bits)
+        for k in ("codes", "sorted_codes", "perm", "left", "right", "parent", "range_lo", "range_hi"):
+            np.testing.assert_array_equal(t[k], o[k], err_msg=f"{k} n={n}")
+        np.testing.assert_array_equal(t["node_com"], o["node_com"])
+        np.testing.assert_array_equal(t["node_rcrit2"], o["rcrit2"])
+
+
+def test_compat_mode_matches_opencl_semantics(ctx, orc):
+    """compat_mode = 1: OpenCL gen_mortons (1024 wraps to 0), descending
+    (code, index) order, Karras tie-break on body indices."""
+    pos, _, m = gen.plummer(5000, 88)
+    pos[7] = pos[9]
+    B = float(np.abs(pos).max())
+    ctx.upload(pos, None, m)
+    t = ctx.lbvh_build(Params(compat_mode=1))
+    codes = orc.morton30(pos, B, compat=True).astype(np.uint64)
+    sc, perm = orc.sort_codes(codes, bits=30, descending=True)
+    k = orc.karras(sc, perm, bits=30, compat=True)
+    np.testing.assert_array_equal(t["codes"], codes)
+    np.testing.assert_array_equal(t["perm"], perm)
+    np.testing.assert_array_equal(t["left"], k["left"])
+    np.testing.assert_array_equal(t["right"], k["right"])
+
+
+@pytest.mark.parametrize("theta", [0.0, 0.3, 0.5, 0.8])
+def test_walk_matches_oracle_lists(ctx, orc, theta):
+    pos, vel, m = gen.plummer(30000, 1002, masses="lognormal")
+    eps2 = 0.005 ** 2
+    ctx.upload(pos, vel, m)
+    p = Params(eps2=eps2, theta=theta)
+    o = orc.lbvh(pos, m, theta)
+    oacc, ocnt = orc.lbvh_forces(o, o["perm"], pos, 1.0, eps2)
+    a64, c64 = ctx.lbvh_forces(p, FP64, group_counts=True)
+    a32, c32 = ctx.lbvh_forces(p, MIXED, group_counts=True)
+    np.testing.assert_array_equal(c64, ocnt)
+    np.testing.assert_array_equal(c32, ocnt)
+    assert rel_l2(a64, oacc) < 1e-12
+    assert rel_l2(a32, oacc) < 1e-6
+    exact = orc.allpairs(pos, m, 1.0, eps2)
+    err = rel_l2(a64, exact)
+    assert err < (1e-12 if theta == 0 else 5e-3), err
+
+
+def test_zero_softening_walk_is_finite(ctx):
+    pos, vel, m = gen.plummer(5000, 3)
+    pos[1] = pos[2]
+    ctx.upload(pos, vel, m)
+    for prec in (FP64, MIXED):
+        assert np.isfinite(ctx.lbvh_forces(Params(eps2=0.0), prec)).all()
+
+
+def test_c2_full_size_tree_bit_exact(ctx, orc):
+    """C2 at full size (n = 2^20, lognormal Plummer): the whole tree equals the
+    CPU restatement (itself pinned bit-exact to the reference above)."""
+    n = 1 << 20
+    pos, vel, m = gen.plummer(n, 1002, masses="lognormal")
+    ctx.upload(pos, vel, m)
+    t = ctx.lbvh_build(Params(theta=0.5, eps2=0.005 ** 2))
+    o = orc.lbvh(pos, m, 0.5)
+    for k in ("codes", "sorted_codes", "perm", "left", "right", "parent", "range_lo", "range_hi"):
+        np.testing.assert_array_equal(t[k], o[k], err_msg=k)
+    np.testing.assert_array_equal(t["node_mass"], o["node_mass"])
+    np.testing.assert_array_equal(t["node_com"], o["node_com"])
+    np.testing.assert_array_equal(t["node_rcrit2"], o["rcrit2"])
+    sc = t["sorted_codes"]
+    assert np.all(sc[1:] >= sc[:-1])
+    ties = sc[1:] == sc[:-1]
+    assert np.all(t["perm"][1:][ties] > t["perm"][:-1][ties])
+
+
+def test_c2_full_size_forces_sampled(ctx):
+    """C2 forces at full size: mixed vs FP64 walk on every body (same lists),
+    approximation error vs FP64 all-pairs on a fixed 4096-body sample."""
+    n = 1 << 20
+    pos, vel, m = gen.plummer(n, 1002, masses="lognormal")
+    ctx.upload(pos, vel, m)
+    p = Params(theta=0.5, eps2=0.005 ** 2)
+    a32 = ctx.lbvh_forces(p, MIXED)
+    a64 = ctx.lbvh_forces(p, FP64)
+    assert rel_l2(a32, a64) < 1e-6
+    tg = np.random.default_rng(4096).choice(n, 4096, replace=False)
+    exact = ctx.allpairs_targets(p, tg, FP64)
+    err = rel_l2(a32[tg], exact)
+    assert err < 5e-3, err
+
+
+def test_lbvh_kdk_conserves(ctx):
+    pos, vel, m = gen.plummer(50000, 1002, masses="lognormal")
+    ctx.upload(pos, vel, m)
+    p = Params(theta=0.5, eps2=0.005 ** 2, dt=5e-4)
+    e0, _ = ctx.energy(p)
+    ctx.kdk_steps(p, 10, SOLVER_LBVH, MIXED)
+    e1, mom = ctx.energy(p)
+    assert abs(e1 - e0) / abs(e0) < 1e-4
+    assert np.abs(mom).max() < 1e-6
