@@ -203,13 +203,15 @@ class Context:
         out["box"] = v.box
         return out
 
-    def lbvh_forces(self, p: Params, precision: int = MIXED, group_counts: bool = False):
+    def lbvh_forces(self, p: Params, precision: int = MIXED, list_counts: bool = False):
+        """Accelerations (n,3); with list_counts also the interaction-list
+        length of each body's group (n,), input order."""
         acc = np.empty((self.n, 3))
-        gc = np.empty((self.n + 31) // 32, np.int32) if group_counts else None
+        gc = np.empty(self.n, np.int32) if list_counts else None
         cp = p.c_struct()
         self._check(self.lib.aster_lbvh_forces(self.h, ctypes.byref(cp), precision, _ptr(acc), _ptr(gc)),
                     "aster_lbvh_forces")
-        return (acc, gc) if group_counts else acc
+        return (acc, gc) if list_counts else acc
 
     def kdk_steps(self, p: Params, nsteps: int, solver: int = SOLVER_ALLPAIRS, precision: int = FP64):
         cp = p.c_struct()

@@ -17,9 +17,9 @@
 #define ASTER_DEVERR_CANCEL 0x8
 #define ASTER_DEVERR_LIST 0x10
 
-#define ASTER_TRY(expr)                                   \
+#define ASTER_TRY(...)                                    \
     do {                                                  \
-        int _st = (expr);                                 \
+        int _st = (__VA_ARGS__);                          \
         if (_st != ASTER_OK) return _st;                  \
     } while (0)
 
@@ -45,7 +45,7 @@ struct LbvhBufs {
     DevBuf codes, codes_alt, sorted_codes, perm, perm_alt, hist, digit_off;
     DevBuf left, right, parent, rlo, rhi, counters;
     DevBuf node_cm, bmin, bmax;  // node_cm: double4 (com x, y, z, mass)
-    DevBuf node_hi, node_lo, child;
+    DevBuf node_hi, node_lo, child, groups;
     int64_t n = 0;
     bool built = false;
     double box = 0.0;
@@ -76,6 +76,14 @@ struct aster_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
+// Layout of ctx->red (4 KB of small device scalars).
+inline unsigned long long* red_box(aster_ctx* c) { return c->red.as<unsigned long long>(); }         // byte 0
+inline double* red_energy(aster_ctx* c) { return c->red.as<double>() + 8; }                         // byte 64
+inline unsigned long long* red_inter(aster_ctx* c) { return c->red.as<unsigned long long>() + 64; } // byte 512
+inline unsigned int* red_groups(aster_ctx* c) {  // [0] group count, [1] walk work counter
+    return reinterpret_cast<unsigned int*>(c->red.as<char>() + 1024);
+}
+
 // ---- shared host helpers (context.cu) -------------------------------------
 int aster_check_params(const aster_params* p);
 int aster_begin(aster_ctx* ctx);                // clears the device error flag
@@ -93,7 +101,7 @@ int aster_kick_drift_launch(aster_ctx* ctx, const aster_params* p, bool want_box
 // lbvh.cu
 int aster_lbvh_build_dev(aster_ctx* ctx, const aster_params* p, bool box_ready);
 int aster_lbvh_walk_launch(aster_ctx* ctx, const aster_params* p, int precision,
-                           bool closing_kick, int32_t* group_counts_dev);
+                           bool closing_kick, int32_t* list_counts_dev);
 
 // ---- device helpers --------------------------------------------------------
 __device__ __forceinline__ void ds_split(double x, float& hi, float& lo) {

@@ -112,7 +112,7 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
                       &c->tree.perm_alt, &c->tree.hist, &c->tree.digit_off, &c->tree.left, &c->tree.right,
                       &c->tree.parent, &c->tree.rlo, &c->tree.rhi, &c->tree.counters, &c->tree.node_cm,
                       &c->tree.bmin, &c->tree.bmax, &c->tree.node_hi,
-                      &c->tree.node_lo, &c->tree.child};
+                      &c->tree.node_lo, &c->tree.child, &c->tree.groups};
     for (DevBuf* b : bufs) b->release();
     for (int i = 0; i < 4; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);

@@ -136,7 +136,7 @@ int aster_kick_drift_launch(aster_ctx* c, const aster_params* p, bool want_box, 
     unsigned long long* box = nullptr;
     if (want_box) {
         ASTER_TRY(c->red.ensure(4096));
-        box = c->red.as<unsigned long long>();
+        box = red_box(c);
         ASTER_CUDA(cudaMemsetAsync(box, 0, sizeof(unsigned long long), c->stream));
     }
     auto* pm = c->pm.as<double4>();
@@ -210,7 +210,7 @@ extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, 
     int marks[3 * (PhaseTimer::kMax / 3 + 2)][3];
     int nm = 0;
     ASTER_TRY(c->red.ensure(4096));
-    unsigned long long* inter = c->red.as<unsigned long long>() + 64;  // walk interaction counter
+    unsigned long long* inter = red_inter(c);  // walk interaction counter
     ASTER_CUDA(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), c->stream));
     cudaEventRecord(c->ev[0], c->stream);
     if (!c->acc_valid) {
@@ -254,7 +254,7 @@ extern "C" int aster_energy(aster_ctx* c, const aster_params* p, int ref_form, d
     ASTER_TRY(c->scratch.ensure((size_t)nb * 5 * sizeof(double) + 64));
     ASTER_TRY(c->red.ensure(4096));
     double* part = c->scratch.as<double>();
-    double* out = c->red.as<double>() + 8;
+    double* out = red_energy(c);
     if (ref_form)
         k_energy_partial<true><<<nb, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2, part);
     else

@@ -410,6 +410,25 @@ __global__ void __launch_bounds__(256) k_bottom_up(int64_t n, double theta, cons
 }
 
 // ----------------------------------------------------------------- walk
+// Groups: a node whose subtree holds at most 32 leaves while its parent's holds
+// more (the root when n <= 32). Its leaves are a contiguous sorted run sharing
+// a Morton prefix, so the group is spatially compact (32 consecutive sorted
+// bodies are not: they can straddle a Morton jump and span the whole system).
+__global__ void __launch_bounds__(256) k_make_groups(int64_t n, const int32_t* __restrict__ parent,
+                                                     const int32_t* __restrict__ rlo,
+                                                     const int32_t* __restrict__ rhi, int2* __restrict__ groups,
+                                                     unsigned int* __restrict__ ngroups) {
+    const int64_t m = 2 * n - 1;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < m; v += (int64_t)gridDim.x * blockDim.x) {
+        const int sz = rhi[v] - rlo[v] + 1;
+        if (sz > 32) continue;
+        const int32_t p = n == 1 ? -1 : parent[v];
+        if (p >= 0 && rhi[p] - rlo[p] + 1 <= 32) continue;
+        const unsigned slot = atomicAdd(ngroups, 1u);
+        groups[slot] = make_int2(rlo[v], sz);
+    }
+}
+
 template <bool MIXED>
 struct WalkShared {
     int stack[WALK_WARPS][WALK_STACK];
@@ -427,172 +446,200 @@ __device__ __forceinline__ float warp_max_f(float v) {
     return v;
 }
 
+// Persistent walk: each warp takes groups from a global work counter until
+// none are left. Per group: the lanes hold the group's bodies (sorted leaves),
+// the warp pops up to 32 nodes per round from its shared stack, each lane
+// loads its node's record (centre of mass, mass, opening radius, children:
+// independent loads, one latency), decides open/accept, children of opened
+// nodes are pushed, accepted nodes appended to the shared list, which is
+// evaluated 32 entries at a time by every lane.
 template <bool MIXED, bool GUARD, bool KICK>
 __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
-    int64_t n, int64_t ngroups, const float4* __restrict__ node_hi, const float4* __restrict__ node_lo,
+    int64_t n, const int2* __restrict__ groups, const unsigned int* __restrict__ ngroups_p,
+    unsigned int* __restrict__ work, const float4* __restrict__ node_hi, const float4* __restrict__ node_lo,
     const double4* __restrict__ node_cm, const int2* __restrict__ child, const int32_t* __restrict__ perm,
     double G, double eps2, double half_dt, double4* __restrict__ acc, double4* __restrict__ vel,
-    int* __restrict__ err, int* __restrict__ stack_hw, int32_t* __restrict__ group_counts,
+    int* __restrict__ err, int* __restrict__ stack_hw, int32_t* __restrict__ body_counts,
     unsigned long long* __restrict__ inter_count) {
     __shared__ WalkShared<MIXED> sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t g = (int64_t)blockIdx.x * WALK_WARPS + warp;
-    if (g >= ngroups) return;
     const uint32_t lt = (1u << lane) - 1u;
-    const int64_t k = g * 32 + lane;
-    const bool valid = k < n;
-    const int64_t kk = valid ? k : g * 32;  // inactive lanes mirror lane 0
+    const unsigned int ngroups = *ngroups_p;
     int* stack = sm.stack[warp];
-
-    // this lane's body (leaf record) and the group box
-    float4 bh = node_hi[kk], bl = node_lo[kk];
-    double4 bc = MIXED ? make_double4(0, 0, 0, 0) : node_cm[kk];
-    const float glox = warp_min_f(valid ? bh.x : INFINITY), ghix = warp_max_f(valid ? bh.x : -INFINITY);
-    const float gloy = warp_min_f(valid ? bh.y : INFINITY), ghiy = warp_max_f(valid ? bh.y : -INFINITY);
-    const float gloz = warp_min_f(valid ? bh.z : INFINITY), ghiz = warp_max_f(valid ? bh.z : -INFINITY);
-
-    CompSum sx, sy, sz;
-    double dax = 0, day = 0, daz = 0;
     const float epsf = (float)eps2;
-    int top = 1, lc = 0, hw = 1;
-    long long total = 0;
-    if (lane == 0) stack[0] = n >= 2 ? (int)n : 0;
-    __syncwarp();
-    bool overflow = false;
+    int hw = 1;
+    unsigned long long wtotal = 0;
 
-    auto evaluate = [&](int cnt) {
-        if (MIXED) {
-            float ax = 0.f, ay = 0.f, az = 0.f;
-            for (int e = 0; e < cnt; ++e) {
-                const float4 h = sm.lhi[warp][e], l = sm.llo[warp][e];
-                float dx = (h.x - bh.x) + (l.x - bl.x);
-                float dy = (h.y - bh.y) + (l.y - bl.y);
-                float dz = (h.z - bh.z) + (l.z - bl.z);
-                float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, epsf)));
-                float inv = rsqrt_approx(r2);
-                if (GUARD) inv = r2 > 0.f ? inv : 0.f;
-                float s = h.w * inv * inv * inv;
-                ax = fmaf(dx, s, ax); ay = fmaf(dy, s, ay); az = fmaf(dz, s, az);
-            }
-            sx.add(ax); sy.add(ay); sz.add(az);
-        } else {
-            for (int e = 0; e < cnt; ++e) {
-                const double4 c = sm.lcm[warp][e];
-                double dx = c.x - bc.x, dy = c.y - bc.y, dz = c.z - bc.z;
-                double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-                double inv = rsqrt(r2);
-                if (GUARD) inv = r2 > 0.0 ? inv : 0.0;
-                double s = c.w * inv * inv * inv;
-                dax = fma(dx, s, dax); day = fma(dy, s, day); daz = fma(dz, s, daz);
-            }
-        }
-        total += cnt;
-    };
+    for (;;) {
+        unsigned int g = 0;
+        if (lane == 0) g = atomicAdd(work, 1u);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        if (g >= ngroups) break;
+        const int2 gr = groups[g];
+        const bool valid = lane < gr.y;
+        const int64_t k = (int64_t)gr.x + (valid ? lane : 0);
 
-    while (top > 0) {
-        const int cnt = top < 32 ? top : 32;
-        int node = -1;
-        if (lane < cnt) node = stack[top - 1 - lane];
+        const float4 bh = node_hi[k], bl = node_lo[k];
+        const double4 bc = MIXED ? make_double4(0, 0, 0, 0) : node_cm[k];
+        const float glox = warp_min_f(valid ? bh.x : INFINITY), ghix = warp_max_f(valid ? bh.x : -INFINITY);
+        const float gloy = warp_min_f(valid ? bh.y : INFINITY), ghiy = warp_max_f(valid ? bh.y : -INFINITY);
+        const float gloz = warp_min_f(valid ? bh.z : INFINITY), ghiz = warp_max_f(valid ? bh.z : -INFINITY);
+
+        CompSum sx, sy, sz;
+        double dax = 0, day = 0, daz = 0;
+        int top = 1, lc = 0;
+        int total = 0;
+        if (lane == 0) stack[0] = n >= 2 ? (int)n : 0;
         __syncwarp();
-        top -= cnt;
-        bool accept = false, open = false;
-        float4 nh = make_float4(0, 0, 0, 0), nl = make_float4(0, 0, 0, 0);
-        if (lane < cnt) {
-            nh = node_hi[node];
-            nl = node_lo[node];
-            if (node < n) {
-                accept = true;
-            } else {
-                // FP32, round-to-nearest, no FMA (matches the CPU restatement)
-                float ux = __fsub_rn(glox, nh.x), wx = __fsub_rn(nh.x, ghix);
-                float uy = __fsub_rn(gloy, nh.y), wy = __fsub_rn(nh.y, ghiy);
-                float uz = __fsub_rn(gloz, nh.z), wz = __fsub_rn(nh.z, ghiz);
-                float tx = ux > wx ? ux : wx, ty = uy > wy ? uy : wy, tz = uz > wz ? uz : wz;
-                tx = tx > 0.f ? tx : 0.f;
-                ty = ty > 0.f ? ty : 0.f;
-                tz = tz > 0.f ? tz : 0.f;
-                const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), __fmul_rn(ty, ty)), __fmul_rn(tz, tz));
-                accept = d2 > nl.w;
-                open = !accept;
-            }
-        }
-        const uint32_t amask = __ballot_sync(0xffffffffu, accept);
-        const uint32_t omask = __ballot_sync(0xffffffffu, open);
-        const int nopen = __popc(omask);
-        if (top + 2 * nopen > WALK_STACK) {
-            overflow = true;
-            break;
-        }
-        if (open) {
-            const int2 ch = child[node];
-            const int pos = top + 2 * __popc(omask & lt);
-            stack[pos] = ch.y;
-            stack[pos + 1] = ch.x;
-        }
-        top += 2 * nopen;
-        hw = top > hw ? top : hw;
-        if (accept) {
-            const int pos = lc + __popc(amask & lt);
+        bool overflow = false;
+
+        auto evaluate = [&](int cnt) {
             if (MIXED) {
-                sm.lhi[warp][pos] = nh;
-                sm.llo[warp][pos] = make_float4(nl.x, nl.y, nl.z, 0.f);
+                float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll 4
+                for (int e = 0; e < cnt; ++e) {
+                    const float4 h = sm.lhi[warp][e], l = sm.llo[warp][e];
+                    float dx = (h.x - bh.x) + (l.x - bl.x);
+                    float dy = (h.y - bh.y) + (l.y - bl.y);
+                    float dz = (h.z - bh.z) + (l.z - bl.z);
+                    float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, epsf)));
+                    float inv = rsqrt_approx(r2);
+                    if (GUARD) inv = r2 > 0.f ? inv : 0.f;
+                    float s = h.w * inv * inv * inv;
+                    ax = fmaf(dx, s, ax); ay = fmaf(dy, s, ay); az = fmaf(dz, s, az);
+                }
+                sx.add(ax); sy.add(ay); sz.add(az);
             } else {
-                sm.lcm[warp][pos] = node_cm[node];
-            }
-        }
-        lc += __popc(amask);
-        __syncwarp();
-        if (lc >= 32) {
-            evaluate(32);
-            __syncwarp();
-            const int rest = lc - 32;
-            if (lane < rest) {
-                if (MIXED) {
-                    const float4 h = sm.lhi[warp][32 + lane], l = sm.llo[warp][32 + lane];
-                    sm.lhi[warp][lane] = h;
-                    sm.llo[warp][lane] = l;
-                } else {
-                    sm.lcm[warp][lane] = sm.lcm[warp][32 + lane];
+#pragma unroll 2
+                for (int e = 0; e < cnt; ++e) {
+                    const double4 c = sm.lcm[warp][e];
+                    double dx = c.x - bc.x, dy = c.y - bc.y, dz = c.z - bc.z;
+                    double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+                    double inv = rsqrt(r2);
+                    if (GUARD) inv = r2 > 0.0 ? inv : 0.0;
+                    double s = c.w * inv * inv * inv;
+                    dax = fma(dx, s, dax); day = fma(dy, s, day); daz = fma(dz, s, daz);
                 }
             }
-            lc = rest;
+            total += cnt;
+        };
+
+        while (top > 0) {
+            const int cnt = top < 32 ? top : 32;
+            int node = 0;
+            if (lane < cnt) node = stack[top - 1 - lane];
             __syncwarp();
+            top -= cnt;
+            bool accept = false, open = false;
+            float4 nh = make_float4(0, 0, 0, 0), nl = make_float4(0, 0, 0, 0);
+            int2 ch = make_int2(0, 0);
+            if (lane < cnt) {
+                nh = node_hi[node];
+                nl = node_lo[node];
+                if (node >= n) ch = child[node];
+                if (node < n) {
+                    accept = true;
+                } else {
+                    // FP32, round-to-nearest, no FMA (matches the CPU restatement)
+                    float ux = __fsub_rn(glox, nh.x), wx = __fsub_rn(nh.x, ghix);
+                    float uy = __fsub_rn(gloy, nh.y), wy = __fsub_rn(nh.y, ghiy);
+                    float uz = __fsub_rn(gloz, nh.z), wz = __fsub_rn(nh.z, ghiz);
+                    float tx = ux > wx ? ux : wx, ty = uy > wy ? uy : wy, tz = uz > wz ? uz : wz;
+                    tx = tx > 0.f ? tx : 0.f;
+                    ty = ty > 0.f ? ty : 0.f;
+                    tz = tz > 0.f ? tz : 0.f;
+                    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), __fmul_rn(ty, ty)), __fmul_rn(tz, tz));
+                    accept = d2 > nl.w;
+                    open = !accept;
+                }
+            }
+            const uint32_t amask = __ballot_sync(0xffffffffu, accept);
+            const uint32_t omask = __ballot_sync(0xffffffffu, open);
+            const int nopen = __popc(omask);
+            if (top + 2 * nopen > WALK_STACK) {
+                overflow = true;
+                break;
+            }
+            if (open) {
+                const int pos = top + 2 * __popc(omask & lt);
+                stack[pos] = ch.y;
+                stack[pos + 1] = ch.x;
+            }
+            top += 2 * nopen;
+            hw = top > hw ? top : hw;
+            if (accept) {
+                const int pos = lc + __popc(amask & lt);
+                if (MIXED) {
+                    sm.lhi[warp][pos] = nh;
+                    sm.llo[warp][pos] = make_float4(nl.x, nl.y, nl.z, 0.f);
+                } else {
+                    sm.lcm[warp][pos] = node_cm[node];
+                }
+            }
+            lc += __popc(amask);
+            __syncwarp();
+            if (lc >= 32) {
+                evaluate(32);
+                __syncwarp();
+                const int rest = lc - 32;
+                if (lane < rest) {
+                    if (MIXED) {
+                        const float4 h = sm.lhi[warp][32 + lane], l = sm.llo[warp][32 + lane];
+                        sm.lhi[warp][lane] = h;
+                        sm.llo[warp][lane] = l;
+                    } else {
+                        sm.lcm[warp][lane] = sm.lcm[warp][32 + lane];
+                    }
+                }
+                lc = rest;
+                __syncwarp();
+            }
+        }
+        if (overflow) {
+            if (lane == 0) atomicOr(err, ASTER_DEVERR_STACK);
+            break;
+        }
+        if (lc > 0) evaluate(lc);
+        __syncwarp();
+        wtotal += (unsigned long long)total * (unsigned long long)gr.y;
+        if (valid) {
+            double ax, ay, az;
+            if (MIXED) { ax = G * sx.value(); ay = G * sy.value(); az = G * sz.value(); }
+            else { ax = G * dax; ay = G * day; az = G * daz; }
+            const int32_t b = perm[k];
+            acc[b] = make_double4(ax, ay, az, 0.0);
+            if (body_counts) body_counts[b] = total;
+            if (KICK) {
+                double4 v = vel[b];
+                v.x += ax * half_dt; v.y += ay * half_dt; v.z += az * half_dt;
+                vel[b] = v;
+            }
         }
     }
-    if (overflow) {
-        if (lane == 0) atomicOr(err, ASTER_DEVERR_STACK);
-        return;
-    }
-    if (lc > 0) evaluate(lc);
     if (lane == 0) {
         atomicMax(stack_hw, hw);
-        if (group_counts) group_counts[g] = (int32_t)total;
-        const int nvalid = (int)min((int64_t)32, n - g * 32);
-        atomicAdd(inter_count, (unsigned long long)total * (unsigned long long)nvalid);
-    }
-    if (valid) {
-        double ax, ay, az;
-        if (MIXED) { ax = G * sx.value(); ay = G * sy.value(); az = G * sz.value(); }
-        else { ax = G * dax; ay = G * day; az = G * daz; }
-        const int32_t b = perm[k];
-        acc[b] = make_double4(ax, ay, az, 0.0);
-        if (KICK) {
-            double4 v = vel[b];
-            v.x += ax * half_dt; v.y += ay * half_dt; v.z += az * half_dt;
-            vel[b] = v;
-        }
+        atomicAdd(inter_count, wtotal);
     }
 }
 
 template <bool MIXED, bool GUARD, bool KICK>
-void launch_walk(aster_ctx* c, const aster_params* p, int32_t* gc, unsigned long long* inter) {
-    const int64_t n = c->n, ng = (n + 31) / 32;
+int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts) {
     LbvhBufs& t = c->tree;
-    const int blocks = (int)((ng + WALK_WARPS - 1) / WALK_WARPS);
-    k_walk<MIXED, GUARD, KICK><<<blocks, WALK_WARPS * 32, 0, c->stream>>>(
-        n, ng, t.node_hi.as<float4>(), t.node_lo.as<float4>(), t.node_cm.as<double4>(), t.child.as<int2>(),
-        t.perm.as<int32_t>(), p->G, p->eps2, 0.5 * p->dt, c->acc.as<double4>(), c->vel.as<double4>(), c->err_dev,
-        c->stack_hw_dev, gc, inter);
+    auto kern = k_walk<MIXED, GUARD, KICK>;
+    int per_sm = 0;
+    ASTER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WALK_WARPS * 32, 0));
+    if (per_sm < 1) per_sm = 1;
+    const int64_t max_groups = (c->n + 0);  // every group holds >= 1 body
+    int64_t blocks = (int64_t)c->sm_count * per_sm;
+    const int64_t need = (max_groups + WALK_WARPS - 1) / WALK_WARPS;
+    if (blocks > need) blocks = need;
+    unsigned int* gcount = red_groups(c);
+    kern<<<(unsigned)blocks, WALK_WARPS * 32, 0, c->stream>>>(
+        c->n, t.groups.as<int2>(), gcount, gcount + 1, t.node_hi.as<float4>(), t.node_lo.as<float4>(),
+        t.node_cm.as<double4>(), t.child.as<int2>(), t.perm.as<int32_t>(), p->G, p->eps2, 0.5 * p->dt,
+        c->acc.as<double4>(), c->vel.as<double4>(), c->err_dev, c->stack_hw_dev, counts, red_inter(c));
+    ASTER_CUDA(cudaGetLastError());
+    return ASTER_OK;
 }
 
 template <class KeyT>
@@ -629,7 +676,7 @@ int run_build(aster_ctx* c, const aster_params* p) {
     LbvhBufs& t = c->tree;
     const int64_t n = c->n;
     const int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 16);
-    const unsigned long long* box = c->red.as<unsigned long long>();
+    const unsigned long long* box = red_box(c);
     const int mode = p->compat_mode ? 2 : (p->morton_bits == 63 ? 1 : 0);
     if (mode == 0) k_morton<KeyT, 0><<<grid, 256, 0, c->stream>>>(n, c->pm.as<double4>(), box, t.codes.as<KeyT>());
     else if (mode == 1) k_morton<KeyT, 1><<<grid, 256, 0, c->stream>>>(n, c->pm.as<double4>(), box, t.codes.as<KeyT>());
@@ -666,7 +713,12 @@ int run_build(aster_ctx* c, const aster_params* p) {
                                              t.bmax.as<float4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>(),
                                              c->err_dev);
     ASTER_CUDA(cudaGetLastError());
-    c->stats.kernels += 2;
+    unsigned int* gcount = red_groups(c);
+    ASTER_CUDA(cudaMemsetAsync(gcount, 0, 2 * sizeof(unsigned int), c->stream));
+    k_make_groups<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(),
+                                               t.groups.as<int2>(), gcount);
+    ASTER_CUDA(cudaGetLastError());
+    c->stats.kernels += 3;
     return ASTER_OK;
 }
 
@@ -692,6 +744,7 @@ int ensure_tree(aster_ctx* c) {
     ASTER_TRY(t.node_hi.ensure((size_t)m * sizeof(float4)));
     ASTER_TRY(t.node_lo.ensure((size_t)m * sizeof(float4)));
     ASTER_TRY(t.child.ensure((size_t)m * sizeof(int2)));
+    ASTER_TRY(t.groups.ensure((size_t)n * sizeof(int2)));
     ASTER_TRY(c->red.ensure(4096));
     t.n = n;
     return ASTER_OK;
@@ -702,7 +755,7 @@ int ensure_tree(aster_ctx* c) {
 int aster_lbvh_build_dev(aster_ctx* c, const aster_params* p, bool box_ready) {
     ASTER_TRY(ensure_tree(c));
     if (!box_ready) {
-        unsigned long long* box = c->red.as<unsigned long long>();
+        unsigned long long* box = red_box(c);
         ASTER_CUDA(cudaMemsetAsync(box, 0, sizeof(unsigned long long), c->stream));
         const int grid = (int)std::min<int64_t>((c->n + 255) / 256, (int64_t)c->sm_count * 8);
         k_box<<<grid, 256, 0, c->stream>>>(c->n, c->pm.as<double4>(), box);
@@ -715,19 +768,18 @@ int aster_lbvh_build_dev(aster_ctx* c, const aster_params* p, bool box_ready) {
     return ASTER_OK;
 }
 
-int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, bool kick, int32_t* gc) {
-    unsigned long long* inter = c->red.as<unsigned long long>() + 64;
+int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, bool kick, int32_t* counts) {
+    ASTER_CUDA(cudaMemsetAsync(red_groups(c) + 1, 0, sizeof(unsigned int), c->stream));  // work counter
     const bool guard = !(p->eps2 > 0.0);
     if (precision == ASTER_MIXED) {
-        if (guard) { if (kick) launch_walk<true, true, true>(c, p, gc, inter); else launch_walk<true, true, false>(c, p, gc, inter); }
-        else       { if (kick) launch_walk<true, false, true>(c, p, gc, inter); else launch_walk<true, false, false>(c, p, gc, inter); }
+        if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true>(c, p, counts) : launch_walk<true, true, false>(c, p, counts)); }
+        else       { ASTER_TRY(kick ? launch_walk<true, false, true>(c, p, counts) : launch_walk<true, false, false>(c, p, counts)); }
     } else if (precision == ASTER_FP64) {
-        if (guard) { if (kick) launch_walk<false, true, true>(c, p, gc, inter); else launch_walk<false, true, false>(c, p, gc, inter); }
-        else       { if (kick) launch_walk<false, false, true>(c, p, gc, inter); else launch_walk<false, false, false>(c, p, gc, inter); }
+        if (guard) { ASTER_TRY(kick ? launch_walk<false, true, true>(c, p, counts) : launch_walk<false, true, false>(c, p, counts)); }
+        else       { ASTER_TRY(kick ? launch_walk<false, false, true>(c, p, counts) : launch_walk<false, false, false>(c, p, counts)); }
     } else {
         return ASTER_ERR_INVALID_ARG;
     }
-    ASTER_CUDA(cudaGetLastError());
     c->stats.kernels += 1;
     return ASTER_OK;
 }
@@ -798,7 +850,7 @@ static int export_tree(aster_ctx* c, const aster_params* p, aster_tree_view* v) 
     ASTER_TRY(cp(v->node_bmax, fmax3, (size_t)m * 12));
     ASTER_TRY(cp(v->node_rcrit2, rc2, (size_t)m * 4));
     unsigned long long bits = 0;
-    ASTER_CUDA(cudaMemcpyAsync(&bits, c->red.ptr, 8, cudaMemcpyDeviceToHost, st));
+    ASTER_CUDA(cudaMemcpyAsync(&bits, red_box(c), 8, cudaMemcpyDeviceToHost, st));
     ASTER_CUDA(cudaStreamSynchronize(st));
     double box;
     memcpy(&box, &bits, 8);
@@ -824,7 +876,7 @@ extern "C" int aster_lbvh_build(aster_ctx* c, const aster_params* p, aster_tree_
 }
 
 extern "C" int aster_lbvh_forces(aster_ctx* c, const aster_params* p, int precision, double* acc_out,
-                                 int32_t* group_counts) {
+                                 int32_t* list_counts) {
     if (!c) return ASTER_ERR_INVALID_ARG;
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
@@ -832,24 +884,23 @@ extern "C" int aster_lbvh_forces(aster_ctx* c, const aster_params* p, int precis
     if (p->force_law & ASTER_PN1) return ASTER_ERR_UNSUPPORTED;
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
-    const int64_t ng = (c->n + 31) / 32;
-    int32_t* gc = nullptr;
-    if (group_counts) {
-        ASTER_TRY(c->targets.ensure((size_t)ng * 4));
-        gc = c->targets.as<int32_t>();
+    int32_t* cnt = nullptr;
+    if (list_counts) {
+        ASTER_TRY(c->targets.ensure((size_t)c->n * 4));
+        cnt = c->targets.as<int32_t>();
     }
     ASTER_TRY(ensure_tree(c));
-    unsigned long long* inter = c->red.as<unsigned long long>() + 64;
+    unsigned long long* inter = red_inter(c);
     ASTER_CUDA(cudaMemsetAsync(inter, 0, 8, c->stream));
     cudaEventRecord(c->ev[0], c->stream);
     ASTER_TRY(aster_lbvh_build_dev(c, p, false));
     cudaEventRecord(c->ev[1], c->stream);
-    ASTER_TRY(aster_lbvh_walk_launch(c, p, precision, false, gc));
+    ASTER_TRY(aster_lbvh_walk_launch(c, p, precision, false, cnt));
     cudaEventRecord(c->ev[2], c->stream);
     unsigned long long ic = 0;
     ASTER_CUDA(cudaMemcpyAsync(&ic, inter, 8, cudaMemcpyDeviceToHost, c->stream));
-    if (group_counts)
-        ASTER_CUDA(cudaMemcpyAsync(group_counts, gc, (size_t)ng * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (list_counts)
+        ASTER_CUDA(cudaMemcpyAsync(list_counts, cnt, (size_t)c->n * 4, cudaMemcpyDeviceToHost, c->stream));
     ASTER_TRY(aster_finish(c));
     float a = 0.f, b = 0.f;
     cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);

@@ -176,7 +176,7 @@ def run_ours(args):
     from aster_b200.api import FP64, MIXED, SOLVER_LBVH, Context, Params
 
     device = local if world > 1 else 0
-    pos, vel, m = gen.plummer(N_C2, SEED_C2, masses="lognormal")
+    pos, vel, m = gen.plummer(args.n, SEED_C2, masses="lognormal")
     p = Params(G=1.0, eps2=EPS * EPS, theta=THETA, dt=DT)
     ctx = Context(device)
     ctx.upload(pos, vel, m)
@@ -207,7 +207,7 @@ def run_ours(args):
     kernels = st["kernels"]
 
     # e2e through the C ABI with pinned host buffers: H2D state, one step, D2H state
-    e2e = e2e_c2(ctx, p, pos, vel, m, args)
+    e2e = None if args.no_e2e else e2e_c2(ctx, p, pos, vel, m, args)
     line = {}
     if rank == 0:
         peaks, src = measured_peaks()
@@ -222,7 +222,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 pairs / f64 state", "data": "synthetic",
             "config": {"workload": "C2 LBVH Barnes-Hut KDK step, Plummer N=1048576 lognormal(0,0.5) masses, "
                                    "30-bit Morton on the bounding cube, theta=0.5, eps=0.005, dt=5e-4, mixed",
-                       "n": N_C2, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "n": args.n, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "per-step working set > L2: the tree rebuild writes ~0.4 GB every step"},
             "phases_ms": {"build": build_ms, "walk": walk_ms, "other": ms / args.steps - build_ms - walk_ms},
             "interactions_per_step": inter_per_step,
@@ -306,11 +306,11 @@ def secondary(ctx, args):
     ctx.upload(pos, vel, m)
     a32 = ctx.lbvh_forces(p, MIXED)
     a64 = ctx.lbvh_forces(p, FP64)
+    tg = np.random.default_rng(4096).choice(N_C2, 4096, replace=False)
+    exact = ctx.allpairs_targets(p, tg, FP64)
     ctx.kdk_steps(p, 1, SOLVER_LBVH, FP64)
     ctx.kdk_steps(p, 3, SOLVER_LBVH, FP64)
     s64 = ctx.stats()
-    tg = np.random.default_rng(4096).choice(N_C2, 4096, replace=False)
-    exact = ctx.allpairs_targets(p, tg, FP64)
     err_bh = float(np.linalg.norm(a32[tg] - exact) / np.linalg.norm(exact))
     out["lbvh_precision"] = {
         "fp64_walk_steps_per_s": 3 / (s64["ms_total"] / 1e3),
@@ -345,6 +345,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quick", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
+    ap.add_argument("--n", type=int, default=N_C2,
+                    help="bodies in the headline workload (default 2^20; smaller only for profiling captures)")
     ap.add_argument("--walk-traffic", type=float, default=None,
                     help="DRAM bytes per walk launch from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()

@@ -138,12 +138,13 @@ int aster_allpairs_targets(aster_ctx* ctx, const aster_params* p, int precision,
 int aster_lbvh_build(aster_ctx* ctx, const aster_params* p, aster_tree_view* view);
 
 /* Build + warp-group traversal (Barnes_Hut / BH_hyper compute_forces
- * replacement). precision: ASTER_MIXED (FP32 interactions) or ASTER_FP64
- * (same tree, same interaction lists, FP64 arithmetic). acc_out may be NULL.
- * group_counts (host, ceil(n/32)) receives the interaction-list length of each
- * 32-body group when not NULL. */
+ * replacement). A group is a subtree of at most 32 leaves whose parent holds
+ * more; one warp walks the tree once per group. precision: ASTER_MIXED (FP32
+ * interactions) or ASTER_FP64 (same tree, same interaction lists, FP64
+ * arithmetic). acc_out may be NULL. list_counts (host, n, input order)
+ * receives the interaction-list length of each body's group when not NULL. */
 int aster_lbvh_forces(aster_ctx* ctx, const aster_params* p, int precision,
-                      double* acc_out, int32_t* group_counts);
+                      double* acc_out, int32_t* list_counts);
 
 /* nsteps kick-drift-kick leapfrog steps of the resident state with one force
  * evaluation per step (the acceleration is cached across steps; the reference

@@ -443,20 +443,44 @@ void orc_bottom_up(long n, const int32_t* left, const int32_t* right, const int3
 /* ------------------------------------------------------------------------ */
 /* group-based traversal                                                     */
 /* ------------------------------------------------------------------------ */
-/* The GPU walks the tree once per group of GROUP consecutive sorted bodies
- * (one warp). A node is opened for the whole group unless it is a leaf or the
+/* Groups: the GPU walks the tree once per group (one warp). A group is a tree
+ * node whose subtree holds at most GROUP leaves while its parent's holds more
+ * (the root when n <= GROUP): a contiguous run of sorted leaves sharing a Morton
+ * prefix, hence spatially compact. orc_groups lists them as (first sorted
+ * leaf, count), ordered by first leaf.
+ *
+ * Walk: a node is opened for the whole group unless it is a leaf or the
  * squared distance from its FP32 centre of mass to the group's FP32 box exceeds
  * rcrit2; accepted nodes go to the group's interaction list. Decision
  * arithmetic is FP32, round-to-nearest, no FMA, in this exact order:
  *   d_a = max(0, max(glo_a - c_a, c_a - ghi_a)); d2 = (dx*dx + dy*dy) + dz*dz
  * where c = (float)com and the group box is the min/max of (float)pos.
  * Every body of the group then sums the list in FP64 (G m d / (d.d+eps2)^1.5,
- * zero when d.d+eps2 == 0). out_count[g] = list length of group g (optional). */
+ * zero when d.d+eps2 == 0). count[b] = list length of body b's group. */
 #define ORC_GROUP 32
 
+long orc_groups(long n, int group, const int32_t* parent, const int32_t* rlo, const int32_t* rhi,
+                int32_t* start, int32_t* count) {
+    if (n == 1) { start[0] = 0; count[0] = 1; return 1; }
+    int32_t* at = (int32_t*)calloc((size_t)n, 4);  /* group size by first leaf */
+    for (long v = 0; v < 2 * n - 1; ++v) {
+        long sz = rhi[v] - rlo[v] + 1;
+        if (sz > group) continue;
+        long p = parent[v];
+        if (p >= 0 && rhi[p] - rlo[p] + 1 <= group) continue;
+        at[rlo[v]] = (int32_t)sz;
+    }
+    long ng = 0;
+    for (long k = 0; k < n; ++k)
+        if (at[k]) { start[ng] = (int32_t)k; count[ng] = at[k]; ++ng; }
+    free(at);
+    return ng;
+}
+
 typedef struct {
-    long n; int group; const int32_t *left, *right, *perm; const double *pos, *node_mass, *node_com;
-    const float* rcrit2; double G, eps2; double* acc; int32_t* count; long* list_buf_unused;
+    long n; const int32_t *gstart, *gcount; const int32_t *left, *right, *perm; const double *pos, *node_mass,
+        *node_com;
+    const float* rcrit2; double G, eps2; double* acc; int32_t* count;
 } trav_ctx;
 
 static void trav_range(void* c_, long glo, long ghi) {
@@ -465,7 +489,7 @@ static void trav_range(void* c_, long glo, long ghi) {
     int32_t* stack = (int32_t*)malloc((size_t)(total + 2) * 4);
     int32_t* list = (int32_t*)malloc((size_t)(total + 2) * 4);
     for (long g = glo; g < ghi; ++g) {
-        long b0 = g * c->group, b1 = b0 + c->group < c->n ? b0 + c->group : c->n;
+        long b0 = c->gstart[g], b1 = b0 + c->gcount[g];
         float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (long k = b0; k < b1; ++k)
             for (int a = 0; a < 3; ++a) {
@@ -489,9 +513,9 @@ static void trav_range(void* c_, long glo, long ghi) {
             stack[sp++] = c->right[v];
             stack[sp++] = c->left[v];
         }
-        if (c->count) c->count[g] = (int32_t)nl;
         for (long k = b0; k < b1; ++k) {
             long b = c->perm[k];
+            if (c->count) c->count[b] = (int32_t)nl;
             const double* x = c->pos + 3 * b;
             double ax = 0, ay = 0, az = 0;
             for (long e = 0; e < nl; ++e) {
@@ -511,12 +535,17 @@ static void trav_range(void* c_, long glo, long ghi) {
     free(list);
 }
 
-/* acc is indexed by body (input order). group_count (optional) has
- * ceil(n/group) entries. */
-void orc_lbvh_forces(long n, int group, const int32_t* left, const int32_t* right, const int32_t* perm,
+/* acc and body_count (optional) are indexed by body (input order). */
+void orc_lbvh_forces(long n, int group, const int32_t* left, const int32_t* right, const int32_t* parent,
+                     const int32_t* rlo, const int32_t* rhi, const int32_t* perm,
                      const double* pos, const double* node_mass, const double* node_com,
-                     const float* rcrit2, double G, double eps2, double* acc, int32_t* group_count) {
+                     const float* rcrit2, double G, double eps2, double* acc, int32_t* body_count) {
     if (group <= 0) group = ORC_GROUP;
-    trav_ctx c = {n, group, left, right, perm, pos, node_mass, node_com, rcrit2, G, eps2, acc, group_count, NULL};
-    orc_parallel((n + group - 1) / group, trav_range, &c);
+    int32_t* gs = (int32_t*)malloc((size_t)n * 4);
+    int32_t* gc = (int32_t*)malloc((size_t)n * 4);
+    long ng = orc_groups(n, group, parent, rlo, rhi, gs, gc);
+    trav_ctx c = {n, gs, gc, left, right, perm, pos, node_mass, node_com, rcrit2, G, eps2, acc, body_count};
+    orc_parallel(ng, trav_range, &c);
+    free(gs);
+    free(gc);
 }

@@ -145,8 +145,10 @@ class Orc:
                                        _I32, _I32, _I32, _I32, _I32]
             lib.orc_bottom_up.argtypes = [ctypes.c_long, _I32, _I32, _I32, _D, _D, ctypes.c_double,
                                           _D, _D, _F, _F, _F]
-            lib.orc_lbvh_forces.argtypes = [ctypes.c_long, ctypes.c_int, _I32, _I32, _I32, _D, _D, _D, _F,
-                                            ctypes.c_double, ctypes.c_double, _D, _I32]
+            lib.orc_lbvh_forces.argtypes = [ctypes.c_long, ctypes.c_int, _I32, _I32, _I32, _I32, _I32, _I32,
+                                            _D, _D, _D, _F, ctypes.c_double, ctypes.c_double, _D, _I32]
+            lib.orc_groups.argtypes = [ctypes.c_long, ctypes.c_int, _I32, _I32, _I32, _I32, _I32]
+            lib.orc_groups.restype = ctypes.c_long
             lib.orc_set_threads.argtypes = [ctypes.c_int]
             Orc._lib = lib
         self.lib = Orc._lib
@@ -234,15 +236,25 @@ class Orc:
         return dict(node_mass=nm, node_com=nc, bmin=bmin, bmax=bmax, rcrit2=rc2)
 
     def lbvh_forces(self, tree, perm, pos, G, eps2, group=32):
+        """Group walk; returns (acc per body, list length per body), input order."""
         n = len(perm)
         pos = _c64(pos)
         acc = np.zeros((n, 3))
-        cnt = np.zeros((n + group - 1) // group, np.int32)
-        args = [np.ascontiguousarray(a, dtype=np.int32) for a in (tree["left"], tree["right"], perm)]
+        cnt = np.zeros(n, np.int32)
+        args = [np.ascontiguousarray(a, dtype=np.int32)
+                for a in (tree["left"], tree["right"], tree["parent"], tree["range_lo"], tree["range_hi"], perm)]
         self.lib.orc_lbvh_forces(n, group, *[_p(a, _I32) for a in args], _p(pos, _D),
                                  _p(tree["node_mass"], _D), _p(tree["node_com"], _D), _p(tree["rcrit2"], _F),
                                  G, eps2, _p(acc, _D), _p(cnt, _I32))
         return acc, cnt
+
+    def groups(self, tree, group=32):
+        n = (len(tree["left"]) + 1) // 2
+        start = np.zeros(n, np.int32)
+        count = np.zeros(n, np.int32)
+        args = [np.ascontiguousarray(tree[k], dtype=np.int32) for k in ("parent", "range_lo", "range_hi")]
+        ng = self.lib.orc_groups(n, group, *[_p(a, _I32) for a in args], _p(start, _I32), _p(count, _I32))
+        return start[:ng], count[:ng]
 
     def lbvh(self, pos, m, theta, B=None, bits=30):
         """Full CPU LBVH build (Morton -> stable sort -> Karras -> bottom-up)."""

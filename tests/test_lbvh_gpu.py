@@ -3,7 +3,7 @@ fixtures from Barnes_Hut::make_tree) and the CPU oracle.
 
 Bit-exact: Morton codes, sorted order (ties by body index), children,
 parents, node ranges, FP64 node masses and centres of mass (NodesArray::unite
-order), FP32 bounds and opening radii, per-group interaction-list lengths.
+order), FP32 bounds and opening radii, per-body interaction-list lengths (groups = subtrees of <= 32 leaves).
 Forces: FP64 walk vs the oracle's FP64 sum over the same lists 1e-12;
 mixed walk 1e-6 (relative L2). Approximation error vs FP64 all-pairs is
 reported and bounded (theta = 0.5: < 5e-3; theta = 0: < 1e-12).
@@ -92,8 +92,8 @@ def test_walk_matches_oracle_lists(ctx, orc, theta):
     p = Params(eps2=eps2, theta=theta)
     o = orc.lbvh(pos, m, theta)
     oacc, ocnt = orc.lbvh_forces(o, o["perm"], pos, 1.0, eps2)
-    a64, c64 = ctx.lbvh_forces(p, FP64, group_counts=True)
-    a32, c32 = ctx.lbvh_forces(p, MIXED, group_counts=True)
+    a64, c64 = ctx.lbvh_forces(p, FP64, list_counts=True)
+    a32, c32 = ctx.lbvh_forces(p, MIXED, list_counts=True)
     np.testing.assert_array_equal(c64, ocnt)
     np.testing.assert_array_equal(c32, ocnt)
     assert rel_l2(a64, oacc) < 1e-12
