@@ -10,8 +10,8 @@
 //            q = min(trunc(x' * 1024), 1023), interleave z|y|x (63-bit: 21
 //            bits per axis). IEEE FP64 add/div, no contraction: bit-exact.
 //   sort     stable LSD radix sort of (code, body index), 8-bit digits:
-//            per pass a tile histogram, one exclusive scan, a stable scatter
-//            (warp match-any ranking). Ties keep body-index order.
+//            per pass a tile histogram, a per-digit scan over tiles, a stable
+//            scatter (warp match-any ranking). Ties keep body-index order.
 //   karras   Karras (2012) node split exactly as barnes_hut.cpp:338-396
 //            (tie-break 32 + clz(i ^ j) on sorted positions), children,
 //            parents and leaf ranges; the same kernel gathers the leaves.
@@ -20,11 +20,12 @@
 //            centre of mass in NodesArray::unite order (barnes_hut.cpp:137-152,
 //            bit-exact), FP32 AABB, squared opening radius
 //            r_crit = l/theta + |com - box centre| (rounded up to FP32).
-//   walk     one warp per 32 consecutive sorted bodies: a shared-memory stack
-//            walk that opens a node for the whole group unless its FP32 centre
-//            of mass lies farther than r_crit from the group's FP32 box;
-//            accepted nodes are appended to a shared interaction list and
-//            evaluated 32 at a time by every lane (FP32 double-single or FP64).
+//   walk     one warp per group (a subtree of <= 64 leaves whose parent holds
+//            more): a shared-memory stack walk that opens a node for the whole
+//            group unless its FP32 centre of mass lies farther than r_crit
+//            from the group's FP32 box; accepted nodes are appended to a
+//            shared interaction list and evaluated 32 at a time by every lane
+//            (FP32 on group-relative double-single coordinates, or FP64).
 // Node numbering is the reference's: leaves 0..n-1 (sorted order), internal
 // n..2n-2, root n, -1 = no child.
 #include <algorithm>
@@ -42,7 +43,8 @@ constexpr int SORT_WARPS = SORT_THREADS / 32;
 constexpr int RADIX = 256;
 constexpr int MAX_CLIMB = 160;     // bottom-up level cap (tree depth <= 97 for 63-bit codes)
 constexpr int WALK_WARPS = 4;
-constexpr int WALK_STACK = 2048;   // nodes per warp
+constexpr int WALK_STACK = 1024;   // nodes per warp
+constexpr int GROUP_MAX = 64;      // leaves per walk group (1 or 2 per lane)
 constexpr int WALK_LIST = 64;      // interaction-list capacity per warp
 
 // ----------------------------------------------------------------- box
@@ -151,43 +153,71 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(int64_t n, const Key
     }
 }
 
-// Exclusive scan of `count` uint32 in place, one block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ data, int64_t count) {
-    __shared__ uint32_t sums[1024];
-    const int64_t per = (count + 1023) / 1024;
-    const int64_t b = threadIdx.x * per, e = min(count, b + per);
-    uint32_t s = 0;
-    for (int64_t i = b; i < e; ++i) s += data[i];
-    sums[threadIdx.x] = s;
+// Block-wide exclusive scan of one uint32 per thread (blockDim.x <= 1024,
+// multiple of 32); returns the exclusive prefix, *total gets the block sum.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem32, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) smem32[warp] = x;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        uint32_t v = threadIdx.x >= off ? sums[threadIdx.x - off] : 0u;
-        __syncthreads();
-        sums[threadIdx.x] += v;
-        __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? smem32[lane] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < nw) smem32[lane] = w;  // inclusive warp sums
     }
-    uint32_t run = threadIdx.x ? sums[threadIdx.x - 1] : 0u;
-    for (int64_t i = b; i < e; ++i) {
-        uint32_t v = data[i];
-        data[i] = run;
-        run += v;
+    __syncthreads();
+    const uint32_t before = warp ? smem32[warp - 1] : 0u;
+    if (total) *total = smem32[nw - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+// Per digit d (one block each): exclusive scan of the per-tile counts
+// hist[d*nblocks + b] over b, in place; digit_tot[d] = the digit's total.
+__global__ void __launch_bounds__(1024) k_scan_digits(uint32_t* __restrict__ hist, int nblocks,
+                                                      uint32_t* __restrict__ digit_tot) {
+    __shared__ uint32_t s32[32];
+    uint32_t* row = hist + (int64_t)blockIdx.x * nblocks;
+    uint32_t carry = 0;
+    for (int base = 0; base < nblocks; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const uint32_t v = i < nblocks ? row[i] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan(v, s32, &tot);
+        if (i < nblocks) row[i] = carry + ex;
+        carry += tot;
     }
+    if (threadIdx.x == 0) digit_tot[blockIdx.x] = carry;
 }
 
 // Stable scatter of one 8-bit digit. Warp w of the block owns the 256 keys
 // [w*256, w*256+256) of the tile and ranks them round by round (32 consecutive
 // keys per round) with __match_any_sync, so ranks follow input order.
+// Global position = (keys of smaller digits) + (same digit in earlier tiles)
+// + (same digit earlier in this tile).
 template <class KeyT, bool IDENTITY_VALS>
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(int64_t n, const KeyT* __restrict__ kin,
                                                                const int32_t* __restrict__ vin, KeyT* __restrict__ kout,
                                                                int32_t* __restrict__ vout, int shift, int nblocks,
-                                                               const uint32_t* __restrict__ offsets) {
+                                                               const uint32_t* __restrict__ tile_off,
+                                                               const uint32_t* __restrict__ digit_tot) {
     __shared__ uint32_t wh[SORT_WARPS][RADIX];
     __shared__ uint32_t dstart[RADIX];
+    __shared__ uint32_t gbase[RADIX];
+    __shared__ uint32_t s32[32];
     __shared__ KeyT sk[SORT_TILE];
     __shared__ int32_t sv[SORT_TILE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int d = threadIdx.x; d < SORT_WARPS * RADIX; d += SORT_THREADS) (&wh[0][0])[d] = 0;
+    // global base of each digit: exclusive scan of the digit totals
+    gbase[threadIdx.x] = block_exclusive_scan(digit_tot[threadIdx.x], s32, nullptr);
     __syncthreads();
     const int64_t tile0 = (int64_t)blockIdx.x * SORT_TILE;
     const uint32_t lt = (1u << lane) - 1u;
@@ -214,23 +244,13 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(int64_t n, const 
     __syncthreads();
     // per digit: exclusive prefix over warps, then over digits (block-local start)
     uint32_t tot = 0;
-    if (threadIdx.x < RADIX) {
-        for (int w = 0; w < SORT_WARPS; ++w) {
-            uint32_t t = wh[w][threadIdx.x];
-            wh[w][threadIdx.x] = tot;
-            tot += t;
-        }
-        dstart[threadIdx.x] = tot;
+    for (int w = 0; w < SORT_WARPS; ++w) {
+        const uint32_t t = wh[w][threadIdx.x];
+        wh[w][threadIdx.x] = tot;
+        tot += t;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int d = 0; d < RADIX; ++d) {
-            uint32_t t = dstart[d];
-            dstart[d] = run;
-            run += t;
-        }
-    }
+    const uint32_t ds = block_exclusive_scan(tot, s32, nullptr);
+    dstart[threadIdx.x] = ds;
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < SORT_ITEMS; ++r) {
@@ -245,7 +265,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(int64_t n, const 
     for (int p = threadIdx.x; p < valid; p += SORT_THREADS) {
         const KeyT k = sk[p];
         const uint32_t d = (uint32_t)(k >> shift) & (RADIX - 1);
-        const int64_t g = (int64_t)offsets[(int64_t)d * nblocks + blockIdx.x] + (p - dstart[d]);
+        const int64_t g = (int64_t)gbase[d] + tile_off[(int64_t)d * nblocks + blockIdx.x] + (p - dstart[d]);
         kout[g] = k;
         vout[g] = sv[p];
     }
@@ -349,11 +369,10 @@ __device__ __forceinline__ double4 ld_cg(const double4* p) {
 }
 __device__ __forceinline__ float4 ld_cg(const float4* p) { return __ldcg(p); }
 
-__global__ void __launch_bounds__(256) k_bottom_up(int64_t n, double theta, const int32_t* __restrict__ parent,
+__global__ void __launch_bounds__(256) k_bottom_up(int64_t n, const int32_t* __restrict__ parent,
                                                    const int2* __restrict__ child, uint32_t* __restrict__ counters,
                                                    double4* __restrict__ node_cm, float4* __restrict__ bmin,
-                                                   float4* __restrict__ bmax, float4* __restrict__ node_hi,
-                                                   float4* __restrict__ node_lo, int* __restrict__ err) {
+                                                   float4* __restrict__ bmax, int* __restrict__ err) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         int64_t cur = k;
         int level = 0;
@@ -379,41 +398,56 @@ __global__ void __launch_bounds__(256) k_bottom_up(int64_t n, double theta, cons
             c.w = M;
             const float4 l0 = ld_cg(bmin + ch.x), l1 = ld_cg(bmin + ch.y);
             const float4 h0 = ld_cg(bmax + ch.x), h1 = ld_cg(bmax + ch.y);
-            const float4 lo = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
-            const float4 hi = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
-            const double ex = __dsub_rn((double)hi.x, (double)lo.x), ey = __dsub_rn((double)hi.y, (double)lo.y),
-                         ez = __dsub_rn((double)hi.z, (double)lo.z);
-            double lmax = 0.0;
-            lmax = ex > lmax ? ex : lmax;
-            lmax = ey > lmax ? ey : lmax;
-            lmax = ez > lmax ? ez : lmax;
-            const double cx = __dmul_rn(0.5, __dadd_rn((double)lo.x, (double)hi.x));
-            const double cy = __dmul_rn(0.5, __dadd_rn((double)lo.y, (double)hi.y));
-            const double cz = __dmul_rn(0.5, __dadd_rn((double)lo.z, (double)hi.z));
-            const double dx = __dsub_rn(c.x, cx), dy = __dsub_rn(c.y, cy), dz = __dsub_rn(c.z, cz);
-            const double delta = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-            const double rc = __dadd_rn(__ddiv_rn(lmax, theta), delta);
-            float4 h, l;
-            ds_split(c.x, h.x, l.x);
-            ds_split(c.y, h.y, l.y);
-            ds_split(c.z, h.z, l.z);
-            h.w = __double2float_rn(M);
-            l.w = __double2float_ru(__dmul_rn(rc, rc));
             node_cm[par] = c;
-            bmin[par] = lo;
-            bmax[par] = hi;
-            node_hi[par] = h;
-            node_lo[par] = l;
+            bmin[par] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
+            bmax[par] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
             cur = par;
         }
     }
 }
 
+
+// Per internal node, after the climb (no dependencies, fully parallel): the
+// squared opening radius r_crit = l/theta + |com - box centre| (l = longest
+// AABB side; FP64, rounded up to FP32) and the traversal records
+// node_hi = (rn(com), rn(mass)), node_lo = (com - rn(com), rcrit2).
+__global__ void __launch_bounds__(256) k_node_finalize(int64_t n, double theta, const double4* __restrict__ node_cm,
+                                                       const float4* __restrict__ bmin,
+                                                       const float4* __restrict__ bmax, float4* __restrict__ node_hi,
+                                                       float4* __restrict__ node_lo) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n - 1; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = n + i;
+        const double4 c = node_cm[v];
+        const float4 lo = bmin[v], hi = bmax[v];
+        const double ex = __dsub_rn((double)hi.x, (double)lo.x), ey = __dsub_rn((double)hi.y, (double)lo.y),
+                     ez = __dsub_rn((double)hi.z, (double)lo.z);
+        double lmax = 0.0;
+        lmax = ex > lmax ? ex : lmax;
+        lmax = ey > lmax ? ey : lmax;
+        lmax = ez > lmax ? ez : lmax;
+        const double cx = __dmul_rn(0.5, __dadd_rn((double)lo.x, (double)hi.x));
+        const double cy = __dmul_rn(0.5, __dadd_rn((double)lo.y, (double)hi.y));
+        const double cz = __dmul_rn(0.5, __dadd_rn((double)lo.z, (double)hi.z));
+        const double dx = __dsub_rn(c.x, cx), dy = __dsub_rn(c.y, cy), dz = __dsub_rn(c.z, cz);
+        const double delta = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+        const double rc = __dadd_rn(__ddiv_rn(lmax, theta), delta);
+        float4 h, l;
+        ds_split(c.x, h.x, l.x);
+        ds_split(c.y, h.y, l.y);
+        ds_split(c.z, h.z, l.z);
+        h.w = __double2float_rn(c.w);
+        l.w = __double2float_ru(__dmul_rn(rc, rc));
+        node_hi[v] = h;
+        node_lo[v] = l;
+    }
+}
+
 // ----------------------------------------------------------------- walk
-// Groups: a node whose subtree holds at most 32 leaves while its parent's holds
-// more (the root when n <= 32). Its leaves are a contiguous sorted run sharing
-// a Morton prefix, so the group is spatially compact (32 consecutive sorted
-// bodies are not: they can straddle a Morton jump and span the whole system).
+// Groups: a node whose subtree holds at most GROUP_MAX leaves while its
+// parent's holds more (the root when n <= GROUP_MAX). Its leaves are a
+// contiguous sorted run sharing a Morton prefix, so the group is spatially
+// compact (a fixed run of consecutive sorted bodies is not: it can straddle a
+// Morton jump and span the whole system).
 __global__ void __launch_bounds__(256) k_make_groups(int64_t n, const int32_t* __restrict__ parent,
                                                      const int32_t* __restrict__ rlo,
                                                      const int32_t* __restrict__ rhi, int2* __restrict__ groups,
@@ -421,9 +455,9 @@ __global__ void __launch_bounds__(256) k_make_groups(int64_t n, const int32_t* _
     const int64_t m = 2 * n - 1;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < m; v += (int64_t)gridDim.x * blockDim.x) {
         const int sz = rhi[v] - rlo[v] + 1;
-        if (sz > 32) continue;
+        if (sz > GROUP_MAX) continue;
         const int32_t p = n == 1 ? -1 : parent[v];
-        if (p >= 0 && rhi[p] - rlo[p] + 1 <= 32) continue;
+        if (p >= 0 && rhi[p] - rlo[p] + 1 <= GROUP_MAX) continue;
         const unsigned slot = atomicAdd(ngroups, 1u);
         groups[slot] = make_int2(rlo[v], sz);
     }
@@ -432,9 +466,8 @@ __global__ void __launch_bounds__(256) k_make_groups(int64_t n, const int32_t* _
 template <bool MIXED>
 struct WalkShared {
     int stack[WALK_WARPS][WALK_STACK];
-    float4 lhi[WALK_WARPS][MIXED ? WALK_LIST : 1];
-    float4 llo[WALK_WARPS][MIXED ? WALK_LIST : 1];
-    double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST];
+    float4 lrel[WALK_WARPS][MIXED ? WALK_LIST : 1];    // (x, y, z) relative to the group centre, mass
+    double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST];    // FP64 (com, mass)
 };
 
 __device__ __forceinline__ float warp_min_f(float v) {
@@ -446,13 +479,45 @@ __device__ __forceinline__ float warp_max_f(float v) {
     return v;
 }
 
+// Mixed-precision interaction of one body (rel. position b, compensated
+// accumulators) with list entry e: 12 FP32 operations + one SFU rsqrt.
+template <bool GUARD>
+__device__ __forceinline__ void interact_f32(const float4 e, const float3 b, float eps2, float& ax, float& ay,
+                                             float& az) {
+    const float dx = e.x - b.x, dy = e.y - b.y, dz = e.z - b.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+    float inv = rsqrt_approx(r2);
+    if (GUARD) inv = r2 > 0.f ? inv : 0.f;
+    const float s = e.w * inv * inv * inv;
+    ax = fmaf(dx, s, ax);
+    ay = fmaf(dy, s, ay);
+    az = fmaf(dz, s, az);
+}
+
+template <bool GUARD>
+__device__ __forceinline__ void interact_f64(const double4 e, const double4 b, double eps2, double& ax, double& ay,
+                                             double& az) {
+    const double dx = e.x - b.x, dy = e.y - b.y, dz = e.z - b.z;
+    const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+    double inv = rsqrt(r2);
+    if (GUARD) inv = r2 > 0.0 ? inv : 0.0;
+    const double s = e.w * inv * inv * inv;
+    ax = fma(dx, s, ax);
+    ay = fma(dy, s, ay);
+    az = fma(dz, s, az);
+}
+
 // Persistent walk: each warp takes groups from a global work counter until
-// none are left. Per group: the lanes hold the group's bodies (sorted leaves),
-// the warp pops up to 32 nodes per round from its shared stack, each lane
-// loads its node's record (centre of mass, mass, opening radius, children:
-// independent loads, one latency), decides open/accept, children of opened
-// nodes are pushed, accepted nodes appended to the shared list, which is
-// evaluated 32 entries at a time by every lane.
+// none are left. Per group: the lanes hold the group's bodies (one or two
+// sorted leaves per lane), the warp pops up to 32 nodes per round from its
+// shared stack, each lane loads its node's record (centre of mass, mass,
+// opening radius, children: independent loads, one latency), decides
+// open/accept, children of opened nodes are pushed, accepted nodes appended to
+// the shared list, which is evaluated 32 entries at a time by every lane.
+// Mixed precision: list entries and bodies are stored relative to the group
+// centre cg (FP32 of hi - cg plus the double-single low part), so an
+// interaction needs one subtraction per axis; the group is compact, so the
+// relative coordinates keep FP32 precision of the separation.
 template <bool MIXED, bool GUARD, bool KICK>
 __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
     int64_t n, const int2* __restrict__ groups, const unsigned int* __restrict__ ngroups_p,
@@ -476,17 +541,30 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= ngroups) break;
         const int2 gr = groups[g];
-        const bool valid = lane < gr.y;
-        const int64_t k = (int64_t)gr.x + (valid ? lane : 0);
+        const bool two = gr.y > 32;  // warp-uniform: two bodies per lane
+        const bool v0 = lane < gr.y, v1 = lane + 32 < gr.y;
+        const int64_t k0 = (int64_t)gr.x + (v0 ? lane : 0);
+        const int64_t k1 = (int64_t)gr.x + (v1 ? lane + 32 : 0);
 
-        const float4 bh = node_hi[k], bl = node_lo[k];
-        const double4 bc = MIXED ? make_double4(0, 0, 0, 0) : node_cm[k];
-        const float glox = warp_min_f(valid ? bh.x : INFINITY), ghix = warp_max_f(valid ? bh.x : -INFINITY);
-        const float gloy = warp_min_f(valid ? bh.y : INFINITY), ghiy = warp_max_f(valid ? bh.y : -INFINITY);
-        const float gloz = warp_min_f(valid ? bh.z : INFINITY), ghiz = warp_max_f(valid ? bh.z : -INFINITY);
+        const float4 h0 = node_hi[k0], l0 = node_lo[k0];
+        const float4 h1 = two ? node_hi[k1] : h0, l1 = two ? node_lo[k1] : l0;
+        const float glox = warp_min_f(fminf(v0 ? h0.x : INFINITY, v1 ? h1.x : INFINITY));
+        const float gloy = warp_min_f(fminf(v0 ? h0.y : INFINITY, v1 ? h1.y : INFINITY));
+        const float gloz = warp_min_f(fminf(v0 ? h0.z : INFINITY, v1 ? h1.z : INFINITY));
+        const float ghix = warp_max_f(fmaxf(v0 ? h0.x : -INFINITY, v1 ? h1.x : -INFINITY));
+        const float ghiy = warp_max_f(fmaxf(v0 ? h0.y : -INFINITY, v1 ? h1.y : -INFINITY));
+        const float ghiz = warp_max_f(fmaxf(v0 ? h0.z : -INFINITY, v1 ? h1.z : -INFINITY));
+        const float cgx = 0.5f * (glox + ghix), cgy = 0.5f * (gloy + ghiy), cgz = 0.5f * (gloz + ghiz);
+        const float3 b0 = make_float3((h0.x - cgx) + l0.x, (h0.y - cgy) + l0.y, (h0.z - cgz) + l0.z);
+        const float3 b1 = make_float3((h1.x - cgx) + l1.x, (h1.y - cgy) + l1.y, (h1.z - cgz) + l1.z);
+        double4 c0 = make_double4(0, 0, 0, 0), c1 = c0;
+        if (!MIXED) {
+            c0 = node_cm[k0];
+            c1 = two ? node_cm[k1] : c0;
+        }
 
-        CompSum sx, sy, sz;
-        double dax = 0, day = 0, daz = 0;
+        CompSum sx0, sy0, sz0, sx1, sy1, sz1;
+        double dx0 = 0, dy0 = 0, dz0 = 0, dx1 = 0, dy1 = 0, dz1 = 0;
         int top = 1, lc = 0;
         int total = 0;
         if (lane == 0) stack[0] = n >= 2 ? (int)n : 0;
@@ -495,30 +573,31 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
 
         auto evaluate = [&](int cnt) {
             if (MIXED) {
-                float ax = 0.f, ay = 0.f, az = 0.f;
+                float ax0 = 0.f, ay0 = 0.f, az0 = 0.f, ax1 = 0.f, ay1 = 0.f, az1 = 0.f;
+                if (two) {
 #pragma unroll 4
-                for (int e = 0; e < cnt; ++e) {
-                    const float4 h = sm.lhi[warp][e], l = sm.llo[warp][e];
-                    float dx = (h.x - bh.x) + (l.x - bl.x);
-                    float dy = (h.y - bh.y) + (l.y - bl.y);
-                    float dz = (h.z - bh.z) + (l.z - bl.z);
-                    float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, epsf)));
-                    float inv = rsqrt_approx(r2);
-                    if (GUARD) inv = r2 > 0.f ? inv : 0.f;
-                    float s = h.w * inv * inv * inv;
-                    ax = fmaf(dx, s, ax); ay = fmaf(dy, s, ay); az = fmaf(dz, s, az);
+                    for (int e = 0; e < cnt; ++e) {
+                        const float4 en = sm.lrel[warp][e];
+                        interact_f32<GUARD>(en, b0, epsf, ax0, ay0, az0);
+                        interact_f32<GUARD>(en, b1, epsf, ax1, ay1, az1);
+                    }
+                    sx1.add(ax1); sy1.add(ay1); sz1.add(az1);
+                } else {
+#pragma unroll 8
+                    for (int e = 0; e < cnt; ++e) interact_f32<GUARD>(sm.lrel[warp][e], b0, epsf, ax0, ay0, az0);
                 }
-                sx.add(ax); sy.add(ay); sz.add(az);
+                sx0.add(ax0); sy0.add(ay0); sz0.add(az0);
             } else {
+                if (two) {
 #pragma unroll 2
-                for (int e = 0; e < cnt; ++e) {
-                    const double4 c = sm.lcm[warp][e];
-                    double dx = c.x - bc.x, dy = c.y - bc.y, dz = c.z - bc.z;
-                    double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-                    double inv = rsqrt(r2);
-                    if (GUARD) inv = r2 > 0.0 ? inv : 0.0;
-                    double s = c.w * inv * inv * inv;
-                    dax = fma(dx, s, dax); day = fma(dy, s, day); daz = fma(dz, s, daz);
+                    for (int e = 0; e < cnt; ++e) {
+                        const double4 en = sm.lcm[warp][e];
+                        interact_f64<GUARD>(en, c0, eps2, dx0, dy0, dz0);
+                        interact_f64<GUARD>(en, c1, eps2, dx1, dy1, dz1);
+                    }
+                } else {
+#pragma unroll 4
+                    for (int e = 0; e < cnt; ++e) interact_f64<GUARD>(sm.lcm[warp][e], c0, eps2, dx0, dy0, dz0);
                 }
             }
             total += cnt;
@@ -569,12 +648,10 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
             hw = top > hw ? top : hw;
             if (accept) {
                 const int pos = lc + __popc(amask & lt);
-                if (MIXED) {
-                    sm.lhi[warp][pos] = nh;
-                    sm.llo[warp][pos] = make_float4(nl.x, nl.y, nl.z, 0.f);
-                } else {
+                if (MIXED)
+                    sm.lrel[warp][pos] = make_float4((nh.x - cgx) + nl.x, (nh.y - cgy) + nl.y, (nh.z - cgz) + nl.z, nh.w);
+                else
                     sm.lcm[warp][pos] = node_cm[node];
-                }
             }
             lc += __popc(amask);
             __syncwarp();
@@ -583,13 +660,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
                 __syncwarp();
                 const int rest = lc - 32;
                 if (lane < rest) {
-                    if (MIXED) {
-                        const float4 h = sm.lhi[warp][32 + lane], l = sm.llo[warp][32 + lane];
-                        sm.lhi[warp][lane] = h;
-                        sm.llo[warp][lane] = l;
-                    } else {
-                        sm.lcm[warp][lane] = sm.lcm[warp][32 + lane];
-                    }
+                    if (MIXED) sm.lrel[warp][lane] = sm.lrel[warp][32 + lane];
+                    else sm.lcm[warp][lane] = sm.lcm[warp][32 + lane];
                 }
                 lc = rest;
                 __syncwarp();
@@ -602,11 +674,17 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
         if (lc > 0) evaluate(lc);
         __syncwarp();
         wtotal += (unsigned long long)total * (unsigned long long)gr.y;
-        if (valid) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const bool vq = q ? v1 : v0;
+            if (!vq) continue;
             double ax, ay, az;
-            if (MIXED) { ax = G * sx.value(); ay = G * sy.value(); az = G * sz.value(); }
-            else { ax = G * dax; ay = G * day; az = G * daz; }
-            const int32_t b = perm[k];
+            if (MIXED) {
+                ax = G * (q ? sx1 : sx0).value(); ay = G * (q ? sy1 : sy0).value(); az = G * (q ? sz1 : sz0).value();
+            } else {
+                ax = G * (q ? dx1 : dx0); ay = G * (q ? dy1 : dy0); az = G * (q ? dz1 : dz0);
+            }
+            const int32_t b = perm[q ? k1 : k0];
             acc[b] = make_double4(ax, ay, az, 0.0);
             if (body_counts) body_counts[b] = total;
             if (KICK) {
@@ -629,9 +707,8 @@ int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts) {
     int per_sm = 0;
     ASTER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WALK_WARPS * 32, 0));
     if (per_sm < 1) per_sm = 1;
-    const int64_t max_groups = (c->n + 0);  // every group holds >= 1 body
     int64_t blocks = (int64_t)c->sm_count * per_sm;
-    const int64_t need = (max_groups + WALK_WARPS - 1) / WALK_WARPS;
+    const int64_t need = (c->n + WALK_WARPS - 1) / WALK_WARPS;  // groups <= n
     if (blocks > need) blocks = need;
     unsigned int* gcount = red_groups(c);
     kern<<<(unsigned)blocks, WALK_WARPS * 32, 0, c->stream>>>(
@@ -649,6 +726,7 @@ int run_sort(aster_ctx* c, int bits) {
     const int nblocks = (int)((n + SORT_TILE - 1) / SORT_TILE);
     const int passes = (bits + 7) / 8;  // 30 -> 4, 63 -> 8 (even: result lands in sorted_codes)
     uint32_t* hist = t.hist.as<uint32_t>();
+    uint32_t* dtot = t.digit_off.as<uint32_t>();
     const KeyT* kin = t.codes.as<KeyT>();
     const int32_t* vin = nullptr;
     for (int ps = 0; ps < passes; ++ps) {
@@ -656,13 +734,13 @@ int run_sort(aster_ctx* c, int bits) {
         int32_t* vout = (ps & 1) ? t.perm.as<int32_t>() : t.perm_alt.as<int32_t>();
         const int shift = 8 * ps;
         k_sort_hist<KeyT><<<nblocks, SORT_THREADS, 0, c->stream>>>(n, kin, shift, nblocks, hist);
-        k_scan_exclusive<<<1, 1024, 0, c->stream>>>(hist, (int64_t)RADIX * nblocks);
+        k_scan_digits<<<RADIX, 1024, 0, c->stream>>>(hist, nblocks, dtot);
         if (ps == 0)
             k_sort_scatter<KeyT, true><<<nblocks, SORT_THREADS, 0, c->stream>>>(n, kin, nullptr, kout, vout, shift,
-                                                                             nblocks, hist);
+                                                                             nblocks, hist, dtot);
         else
             k_sort_scatter<KeyT, false><<<nblocks, SORT_THREADS, 0, c->stream>>>(n, kin, vin, kout, vout, shift,
-                                                                              nblocks, hist);
+                                                                              nblocks, hist, dtot);
         ASTER_CUDA(cudaGetLastError());
         c->stats.kernels += 3;
         kin = kout;
@@ -708,17 +786,19 @@ int run_build(aster_ctx* c, const aster_params* p) {
             t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
             t.node_hi.as<float4>(), t.node_lo.as<float4>());
     ASTER_CUDA(cudaGetLastError());
-    k_bottom_up<<<grid, 256, 0, c->stream>>>(n, p->theta, t.parent.as<int32_t>(), t.child.as<int2>(),
+    k_bottom_up<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.child.as<int2>(),
                                              t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(),
-                                             t.bmax.as<float4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>(),
-                                             c->err_dev);
+                                             t.bmax.as<float4>(), c->err_dev);
+    ASTER_CUDA(cudaGetLastError());
+    k_node_finalize<<<grid, 256, 0, c->stream>>>(n, p->theta, t.node_cm.as<double4>(), t.bmin.as<float4>(),
+                                                 t.bmax.as<float4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>());
     ASTER_CUDA(cudaGetLastError());
     unsigned int* gcount = red_groups(c);
     ASTER_CUDA(cudaMemsetAsync(gcount, 0, 2 * sizeof(unsigned int), c->stream));
     k_make_groups<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(),
                                                t.groups.as<int2>(), gcount);
     ASTER_CUDA(cudaGetLastError());
-    c->stats.kernels += 3;
+    c->stats.kernels += 4;
     return ASTER_OK;
 }
 
@@ -732,6 +812,7 @@ int ensure_tree(aster_ctx* c) {
     ASTER_TRY(t.perm.ensure((size_t)n * 4));
     ASTER_TRY(t.perm_alt.ensure((size_t)n * 4));
     ASTER_TRY(t.hist.ensure((size_t)nblocks * RADIX * 4));
+    ASTER_TRY(t.digit_off.ensure((size_t)RADIX * 4));
     ASTER_TRY(t.left.ensure((size_t)m * 4));
     ASTER_TRY(t.right.ensure((size_t)m * 4));
     ASTER_TRY(t.parent.ensure((size_t)m * 4));

@@ -226,6 +226,7 @@ def run_ours(args):
                        "l2": "per-step working set > L2: the tree rebuild writes ~0.4 GB every step"},
             "phases_ms": {"build": build_ms, "walk": walk_ms, "other": ms / args.steps - build_ms - walk_ms},
             "interactions_per_step": inter_per_step,
+            "walk_stack_high_water": st["max_stack"],
             "roofline": {"bound": "fp32", "kernel": "k_walk (tree walk + interactions)",
                          "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                          "traffic": args.walk_traffic,

@@ -138,7 +138,7 @@ int aster_allpairs_targets(aster_ctx* ctx, const aster_params* p, int precision,
 int aster_lbvh_build(aster_ctx* ctx, const aster_params* p, aster_tree_view* view);
 
 /* Build + warp-group traversal (Barnes_Hut / BH_hyper compute_forces
- * replacement). A group is a subtree of at most 32 leaves whose parent holds
+ * replacement). A group is a subtree of at most 64 leaves whose parent holds
  * more; one warp walks the tree once per group. precision: ASTER_MIXED (FP32
  * interactions) or ASTER_FP64 (same tree, same interaction lists, FP64
  * arithmetic). acc_out may be NULL. list_counts (host, n, input order)

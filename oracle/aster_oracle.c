@@ -457,7 +457,7 @@ void orc_bottom_up(long n, const int32_t* left, const int32_t* right, const int3
  * where c = (float)com and the group box is the min/max of (float)pos.
  * Every body of the group then sums the list in FP64 (G m d / (d.d+eps2)^1.5,
  * zero when d.d+eps2 == 0). count[b] = list length of body b's group. */
-#define ORC_GROUP 32
+#define ORC_GROUP 64
 
 long orc_groups(long n, int group, const int32_t* parent, const int32_t* rlo, const int32_t* rhi,
                 int32_t* start, int32_t* count) {

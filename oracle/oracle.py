@@ -235,7 +235,7 @@ class Orc:
                                _p(nm, _D), _p(nc, _D), _p(bmin, _F), _p(bmax, _F), _p(rc2, _F))
         return dict(node_mass=nm, node_com=nc, bmin=bmin, bmax=bmax, rcrit2=rc2)
 
-    def lbvh_forces(self, tree, perm, pos, G, eps2, group=32):
+    def lbvh_forces(self, tree, perm, pos, G, eps2, group=64):
         """Group walk; returns (acc per body, list length per body), input order."""
         n = len(perm)
         pos = _c64(pos)
@@ -248,7 +248,7 @@ class Orc:
                                  G, eps2, _p(acc, _D), _p(cnt, _I32))
         return acc, cnt
 
-    def groups(self, tree, group=32):
+    def groups(self, tree, group=64):
         n = (len(tree["left"]) + 1) // 2
         start = np.zeros(n, np.int32)
         count = np.zeros(n, np.int32)

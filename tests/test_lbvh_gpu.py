@@ -3,7 +3,8 @@ fixtures from Barnes_Hut::make_tree) and the CPU oracle.
 
 Bit-exact: Morton codes, sorted order (ties by body index), children,
 parents, node ranges, FP64 node masses and centres of mass (NodesArray::unite
-order), FP32 bounds and opening radii, per-body interaction-list lengths (groups = subtrees of <= 32 leaves).
+order), FP32 bounds and opening radii, per-body interaction-list lengths
+(groups = subtrees of <= 64 leaves whose parent holds more).
 Forces: FP64 walk vs the oracle's FP64 sum over the same lists 1e-12;
 mixed walk 1e-6 (relative L2). Approximation error vs FP64 all-pairs is
 reported and bounded (theta = 0.5: < 5e-3; theta = 0: < 1e-12).
@@ -100,7 +101,8 @@ def test_walk_matches_oracle_lists(ctx, orc, theta):
     assert rel_l2(a32, oacc) < 1e-6
     exact = orc.allpairs(pos, m, 1.0, eps2)
     err = rel_l2(a64, exact)
-    assert err < (1e-12 if theta == 0 else 5e-3), err
+    bound = {0.0: 1e-12, 0.3: 1e-3, 0.5: 3e-3, 0.8: 1e-2}[theta]  # monopole approximation error
+    assert err < bound, err
 
 
 def test_zero_softening_walk_is_finite(ctx):
