@@ -43,6 +43,10 @@ THETA, EPS, DT = 0.5, 0.005, 5e-4
 SEED_C2 = 1002
 N_C3, EPS_C3, SEED_C3 = 262144, 0.002, 1003
 FLOP_PER_PAIR = 20  # Newtonian pair, Nyland et al. GPU Gems 3 ch. 31 convention
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_walk launch captured with
+# ncu at N = 2^19 (68.7 MB, profiles/k_walk_c2_plummer524288.md), scaled by the
+# number of bodies to N = 2^20 (the walk reads each tree node about once).
+WALK_TRAFFIC_BYTES = 68.7e6 * 2
 
 
 def log(*a):
@@ -349,7 +353,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
     ap.add_argument("--n", type=int, default=N_C2,
                     help="bodies in the headline workload (default 2^20; smaller only for profiling captures)")
-    ap.add_argument("--walk-traffic", type=float, default=None,
+    ap.add_argument("--walk-traffic", type=float, default=WALK_TRAFFIC_BYTES,
                     help="DRAM bytes per walk launch from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()
     if args.warmup < 3:
