@@ -15,6 +15,8 @@
 // Energy replaces Graphs::get_total_energy (src/utils/collectors.cpp:19-53).
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <mutex>
 
 #include "aster_internal.cuh"
 
@@ -267,5 +269,59 @@ extern "C" int aster_energy(aster_ctx* c, const aster_params* p, int ref_form, d
     ASTER_TRY(aster_finish(c));
     *energy = host[0];
     if (momentum3) { momentum3[0] = host[1]; momentum3[1] = host[2]; momentum3[2] = host[3]; }
+    return ASTER_OK;
+}
+
+// ---- allocation-free energy ------------------------------------------------
+// aster_energy_noalloc runs the same two kernels as aster_energy but keeps the
+// per-block partial sums (5 doubles per 256 bodies) in the file-scope device
+// array below instead of context memory, so the call allocates nothing. The
+// array is part of the module: every GPU that loads this library holds it
+// (ASTER_ENERGY_NOALLOC_MAX_N / 256 * 5 doubles = 2.5 MiB) until the process
+// exits. Device code could name the array directly; host code must not pass
+// &g_energy_partials to a kernel (on the host that name is only a stand-in),
+// so each device's address is fetched once with cudaGetSymbolAddress and kept.
+static constexpr int64_t kEnergyNoAllocMaxBlocks = ASTER_ENERGY_NOALLOC_MAX_N / 256;
+static constexpr int kEnergyNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_energy_partials[kEnergyNoAllocMaxBlocks * 5];
+static double* g_energy_partials_addr[kEnergyNoAllocMaxDevices];
+static std::mutex g_energy_partials_mu;
+
+// Address of g_energy_partials on the current device; the first call on a
+// device looks it up (with that device current) and caches it.
+static int energy_partials_on_current_device(double** out) {
+    int dev = -1;
+    ASTER_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kEnergyNoAllocMaxDevices) return ASTER_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_energy_partials_mu);
+    if (!g_energy_partials_addr[dev]) {
+        void* ptr = nullptr;
+        ASTER_CUDA(cudaGetSymbolAddress(&ptr, g_energy_partials));
+        g_energy_partials_addr[dev] = static_cast<double*>(ptr);
+    }
+    *out = g_energy_partials_addr[dev];
+    return ASTER_OK;
+}
+
+extern "C" int aster_energy_noalloc(int64_t n, const double* pm_dev, const double* vel_dev, const aster_params* p,
+                                    int ref_form, double* out_dev, void* stream) {
+    if (n <= 0 || !pm_dev || !vel_dev || !out_dev) return ASTER_ERR_INVALID_ARG;
+    if (((uintptr_t)pm_dev & 31) || ((uintptr_t)vel_dev & 31) || ((uintptr_t)out_dev & 7))
+        return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (n > ASTER_ENERGY_NOALLOC_MAX_N) return ASTER_ERR_TOO_LARGE;
+    const int nb = (int)((n + 255) / 256);
+    double* part = nullptr;
+    ASTER_TRY(energy_partials_on_current_device(&part));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const double4* pm = reinterpret_cast<const double4*>(pm_dev);
+    const double4* vel = reinterpret_cast<const double4*>(vel_dev);
+    if (ref_form)
+        k_energy_partial<true><<<nb, 256, 0, st>>>(n, pm, vel, p->eps2, part);
+    else
+        k_energy_partial<false><<<nb, 256, 0, st>>>(n, pm, vel, p->eps2, part);
+    ASTER_CUDA(cudaGetLastError());
+    k_energy_final<<<1, 32, 0, st>>>(nb, part, p->G, out_dev);
+    ASTER_CUDA(cudaGetLastError());
     return ASTER_OK;
 }

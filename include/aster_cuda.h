@@ -159,6 +159,31 @@ int aster_kdk_steps(aster_ctx* ctx, const aster_params* p, int solver, int preci
 int aster_energy(aster_ctx* ctx, const aster_params* p, int ref_form, double* energy,
                  double* momentum3);
 
+/* Allocation-free energy. No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory: codes that reserve all of
+ * the GPU's memory up front in their own pool (a cudaMalloc would fail or
+ * break their accounting), and time-stepping loops that must not allocate in
+ * the middle of a run because an allocation or free can stall the whole
+ * device. It computes what aster_energy computes, but takes device arrays from
+ * the caller and needs no context:
+ *   pm_dev   n records of 4 doubles (x, y, z, m), 32-byte aligned
+ *   vel_dev  n records of 4 doubles (vx, vy, vz, unused), 32-byte aligned
+ *   out_dev  4 doubles: total energy, then the momentum (px, py, pz)
+ * The per-block partial sums live in a fixed array inside the library (2.5 MiB
+ * on every GPU that loads it, held until the process exits), so n is limited
+ * to ASTER_ENERGY_NOALLOC_MAX_N; larger n returns ASTER_ERR_TOO_LARGE. The
+ * work is queued on `stream` (a cudaStream_t, NULL for the default stream) and
+ * the call returns without waiting; synchronise before reading out_dev.
+ * The first call on a device looks up that device's address of the array, so
+ * make that first call before any stream capture. All calls share the one
+ * array: calls that overlap on the GPU (on different streams) race and give
+ * wrong results. Each call fully rewrites the partials it reads, so nothing
+ * needs clearing between calls. */
+#define ASTER_ENERGY_NOALLOC_MAX_N (65536LL * 256)
+int aster_energy_noalloc(int64_t n, const double* pm_dev, const double* vel_dev, const aster_params* p,
+                         int ref_form, double* out_dev, void* stream);
+
 /* Counters of the last force/step call on this context. */
 int aster_get_stats(aster_ctx* ctx, aster_stats* out);
 
