@@ -31,11 +31,15 @@ FP64 = 0
 MIXED = 1
 SOLVER_ALLPAIRS = 0
 SOLVER_LBVH = 1
+LEAPFROG = 0
+YOSHIDA4 = 1
+ERR_CANCELLED = 8
 
 EXPORTS = [
     "aster_strerror", "aster_version", "aster_ctx_create", "aster_ctx_destroy", "aster_state_upload",
     "aster_state_download", "aster_state_size", "aster_allpairs", "aster_allpairs_targets", "aster_lbvh_build",
-    "aster_lbvh_forces", "aster_kdk_steps", "aster_energy", "aster_get_stats",
+    "aster_lbvh_forces", "aster_kdk_steps", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
+    "aster_ensemble_download", "aster_ensemble_run", "aster_ensemble_energy", "aster_ensemble_cancel",
 ]
 
 
@@ -57,6 +61,11 @@ class CTreeView(ctypes.Structure):
                 ("range_lo", ctypes.c_void_p), ("range_hi", ctypes.c_void_p), ("node_mass", ctypes.c_void_p),
                 ("node_com", ctypes.c_void_p), ("node_bmin", ctypes.c_void_p), ("node_bmax", ctypes.c_void_p),
                 ("node_rcrit2", ctypes.c_void_p), ("box", ctypes.c_double)]
+
+
+class CEnsembleConfig(ctypes.Structure):
+    _fields_ = [("warps_per_block", ctypes.c_int32), ("unroll", ctypes.c_int32), ("check_every", ctypes.c_int32),
+                ("use_graph", ctypes.c_int32)]
 
 
 class CStats(ctypes.Structure):
@@ -107,6 +116,12 @@ def load_library(path: Path | str | None = None) -> ctypes.CDLL:
     lib.aster_kdk_steps.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.aster_energy.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.POINTER(dbl), vp]
     lib.aster_get_stats.argtypes = [vp, ctypes.POINTER(CStats)]
+    lib.aster_ensemble_upload.argtypes = [vp, ctypes.c_int32, vp, vp, vp, vp]
+    lib.aster_ensemble_download.argtypes = [vp, vp, vp]
+    lib.aster_ensemble_run.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, i64,
+                                       ctypes.POINTER(CEnsembleConfig)]
+    lib.aster_ensemble_energy.argtypes = [vp, ctypes.POINTER(CParams), vp]
+    lib.aster_ensemble_cancel.argtypes = [vp]
     for name in EXPORTS:
         if not hasattr(lib, name):
             raise ImportError(f"{p} lacks {name}")
@@ -229,6 +244,44 @@ class Context:
         s = CStats()
         self._check(self.lib.aster_get_stats(self.h, ctypes.byref(s)), "aster_get_stats")
         return {k: getattr(s, k) for k, _ in CStats._fields_}
+
+    # -- batched ensembles ---------------------------------------------------
+    def ensemble_upload(self, offsets, pos, vel, mass):
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        nb = int(off[-1])
+        pos = _aos(pos, nb)
+        vel = None if vel is None else _aos(vel, nb)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        self._check(self.lib.aster_ensemble_upload(self.h, len(off) - 1, _ptr(off), _ptr(pos), _ptr(vel),
+                                                   _ptr(mass)), "aster_ensemble_upload")
+        self.ens_nsys, self.ens_nbodies = len(off) - 1, nb
+        self._ens_mass = mass.copy()
+        return self
+
+    def ensemble_download(self):
+        pos, vel = np.empty((self.ens_nbodies, 3)), np.empty((self.ens_nbodies, 3))
+        self._check(self.lib.aster_ensemble_download(self.h, _ptr(pos), _ptr(vel)), "aster_ensemble_download")
+        return pos, vel
+
+    def ensemble_run(self, p: Params, nsteps: int, integrator: int = YOSHIDA4, precision: int = MIXED,
+                     config: dict | None = None):
+        cp = p.c_struct()
+        cfg = None
+        if config is not None:
+            cfg = CEnsembleConfig(config.get("warps_per_block", 0), config.get("unroll", 0),
+                                  config.get("check_every", 0), int(config.get("use_graph", 1)))
+        self._check(self.lib.aster_ensemble_run(self.h, ctypes.byref(cp), integrator, precision, nsteps,
+                                                ctypes.byref(cfg) if cfg is not None else None),
+                    "aster_ensemble_run")
+
+    def ensemble_energy(self, p: Params):
+        e = np.empty(self.ens_nsys)
+        cp = p.c_struct()
+        self._check(self.lib.aster_ensemble_energy(self.h, ctypes.byref(cp), _ptr(e)), "aster_ensemble_energy")
+        return e
+
+    def ensemble_cancel(self):
+        self._check(self.lib.aster_ensemble_cancel(self.h), "aster_ensemble_cancel")
 
 
 # ---------------------------------------------------------------------------

@@ -1,0 +1,85 @@
+"""Autotuner for the batched-ensemble kernel.
+
+The tunables are the launch shape of the persistent kernel: warps (systems in
+flight) per block and the unroll factor of the inner pair loop. Each candidate
+is timed on the caller's own ensemble (the real size distribution) for a short
+run with CUDA events inside the library, after one untimed warm-up run; the
+state is saved before and restored after, so tuning leaves the ensemble
+untouched. Results are cached in a JSON file keyed by GPU name, precision,
+integrator, force law and a histogram of the system sizes, so later runs of
+the same configuration skip the search.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+
+from .api import MIXED, YOSHIDA4, Context, Params
+
+DEFAULT_SPACE = {"warps_per_block": (1, 2, 4, 8), "unroll": (1, 2, 4)}
+DEFAULT_CACHE = Path(os.environ.get("ASTER_TUNE_CACHE", Path.home() / ".cache" / "aster_b200" / "ensemble.json"))
+
+
+def _gpu_name() -> str:
+    try:
+        import subprocess
+        out = subprocess.run(["nvidia-smi", "--query-gpu=name", "--format=csv,noheader", "-i", "0"],
+                             capture_output=True, text=True, timeout=10).stdout.strip()
+        return out or "unknown"
+    except Exception:
+        return "unknown"
+
+
+def _key(offsets, precision, integrator, force_law) -> str:
+    sizes = np.diff(np.asarray(offsets, dtype=np.int64))
+    hist = np.bincount(sizes, minlength=65)[:65]
+    h = hashlib.sha1(hist.tobytes()).hexdigest()[:16]
+    return f"{_gpu_name()}|p{precision}|i{integrator}|f{force_law}|n{len(sizes)}|h{h}"
+
+
+def tune_ensemble(ctx: Context, offsets, p: Params, integrator: int = YOSHIDA4, precision: int = MIXED,
+                  steps: int = 40, space: dict | None = None, cache: Path | str | None = DEFAULT_CACHE,
+                  force: bool = False) -> dict:
+    """Return the fastest config for the ensemble currently uploaded to ctx
+    (offsets must be the ones uploaded). Adds "ms_per_step" and "timings"."""
+    space = space or DEFAULT_SPACE
+    key = _key(offsets, precision, integrator, p.force_law)
+    cache = Path(cache) if cache else None
+    if cache and cache.exists() and not force:
+        table = json.loads(cache.read_text())
+        if key in table:
+            return table[key]
+    pos0, vel0 = ctx.ensemble_download()
+    mass = None
+    timings = []
+    try:
+        for wpb in space["warps_per_block"]:
+            for unroll in space["unroll"]:
+                cfg = {"warps_per_block": wpb, "unroll": unroll, "check_every": 256, "use_graph": 1}
+                ctx.ensemble_run(p, max(2, steps // 8), integrator, precision, cfg)   # warm-up
+                ctx.ensemble_run(p, steps, integrator, precision, cfg)
+                ms = ctx.stats()["ms_total"] / steps
+                timings.append({**cfg, "ms_per_step": ms})
+    finally:
+        # restore the caller's state (masses are unchanged by a run)
+        mass = _masses_of(ctx)
+        ctx.ensemble_upload(offsets, pos0, vel0, mass)
+    best = min(timings, key=lambda t: t["ms_per_step"])
+    result = {**best, "timings": timings, "key": key}
+    if cache:
+        cache.parent.mkdir(parents=True, exist_ok=True)
+        table = json.loads(cache.read_text()) if cache.exists() else {}
+        table[key] = result
+        cache.write_text(json.dumps(table, indent=1))
+    return result
+
+
+def _masses_of(ctx: Context):
+    m = getattr(ctx, "_ens_mass", None)
+    if m is None:
+        raise RuntimeError("upload the ensemble with Context.ensemble_upload before tuning")
+    return m

@@ -51,6 +51,16 @@ struct LbvhBufs {
     double box = 0.0;
 };
 
+// Batched-ensemble device arrays.
+struct EnsBufs {
+    DevBuf pm, vel, off, order, counter;
+    int32_t nsys = 0;
+    int64_t nbodies = 0;
+    double pair_evals_per_stage = 0.0;   // sum over systems of n(n-1)
+    volatile int* cancel_host = nullptr;  // pinned, mapped
+    int* cancel_dev = nullptr;
+};
+
 struct aster_ctx {
     int device = 0;
     int sm_count = 148;
@@ -72,6 +82,7 @@ struct aster_ctx {
     int* err_host = nullptr;    // pinned copy
     int* stack_hw_dev = nullptr;  // tree-walk stack high-water mark
     LbvhBufs tree;
+    EnsBufs ens;
     aster_stats stats{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };

@@ -114,6 +114,9 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
                       &c->tree.bmin, &c->tree.bmax, &c->tree.node_hi,
                       &c->tree.node_lo, &c->tree.child, &c->tree.groups};
     for (DevBuf* b : bufs) b->release();
+    DevBuf* ens[] = {&c->ens.pm, &c->ens.vel, &c->ens.off, &c->ens.order, &c->ens.counter};
+    for (DevBuf* b : ens) b->release();
+    if (c->ens.cancel_host) cudaFreeHost((void*)c->ens.cancel_host);
     for (int i = 0; i < 4; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->err_dev) cudaFree(c->err_dev);

@@ -1,0 +1,480 @@
+// Batched ensembles of few-body systems: one persistent, graph-captured
+// launch integrates thousands of independent systems for many steps.
+//
+// The reference has no batched solver (a Simulation per system would also
+// share Parallelized's function-static pointer, builder_endpoint.cpp:731). The
+// pair law is the reference's compute_gravitational with the pairwise 1PN term
+// of get_pn1 (src/physics/tool_chain_impl.cpp:110-137); the integrators are
+// drift-kick-drift compositions: leapfrog (the map of update_leapfrog,
+// tool_chain_impl.cpp:169-185) and Yoshida's (1990) fourth-order triple jump.
+//
+// Mapping: one warp per system (at most 64 bodies: one body per lane, or two
+// when the system has more than 32), the whole state in registers for the
+// entire run; per force evaluation every lane publishes its bodies to the
+// warp's shared-memory slab and sums over the slab. Systems are taken largest
+// first from a global work counter (longest-processing-time order), so the
+// uneven sizes balance across warps. The kernel polls a host-written cancel
+// flag every check_every steps; it never waits on anything.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "aster_internal.cuh"
+
+namespace {
+
+struct Coeffs {
+    double cdt[4];  // drift coefficients x dt
+    double ddt[3];  // kick coefficients x dt
+    int nst;        // kicks per step
+};
+
+Coeffs make_coeffs(int integrator, double dt) {
+    Coeffs k{};
+    if (integrator == ASTER_INTEGRATOR_YOSHIDA4) {
+        const double cb = std::cbrt(2.0);
+        const double w1 = 1.0 / (2.0 - cb), w0 = -cb / (2.0 - cb);
+        const double c[4] = {0.5 * w1, 0.5 * (w0 + w1), 0.5 * (w0 + w1), 0.5 * w1};
+        const double d[3] = {w1, w0, w1};
+        for (int i = 0; i < 4; ++i) k.cdt[i] = c[i] * dt;
+        for (int i = 0; i < 3; ++i) k.ddt[i] = d[i] * dt;
+        k.nst = 3;
+    } else {
+        k.cdt[0] = k.cdt[1] = 0.5 * dt;
+        k.ddt[0] = dt;
+        k.nst = 1;
+    }
+    return k;
+}
+
+template <bool MIXED>
+struct EnsSlab;
+template <>
+struct EnsSlab<true> {
+    float4 hi[64];  // (x_hi, y_hi, z_hi, m)
+    float4 lo[64];  // (x_lo, y_lo, z_lo, 0)
+    float4 v[64];   // (vx, vy, vz, |v|^2)
+};
+template <>
+struct EnsSlab<false> {
+    double4 x[64];  // (x, y, z, m)
+    double4 v[64];  // (vx, vy, vz, |v|^2)
+};
+
+// Acceleration on body i from every body of the slab (j == i contributes 0:
+// zero separation is skipped), G applied by the caller.
+template <bool PN, int UNROLL>
+__device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int n, float4 hi, float4 lo, float4 vi, float eps2,
+                                          float G, float inv_c2, float& ax, float& ay, float& az) {
+    float px = 0.f, py = 0.f, pz = 0.f;
+    ax = ay = az = 0.f;
+#pragma unroll UNROLL
+    for (int j = 0; j < n; ++j) {
+        const float4 h = s.hi[j], l = s.lo[j];
+        const float dx = (h.x - hi.x) + (l.x - lo.x);
+        const float dy = (h.y - hi.y) + (l.y - lo.y);
+        const float dz = (h.z - hi.z) + (l.z - lo.z);
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+        float inv = rsqrt_approx(r2);
+        inv = r2 > 0.f ? inv : 0.f;
+        const float inv2 = inv * inv;
+        const float sN = h.w * inv * inv2;
+        ax = fmaf(dx, sN, ax); ay = fmaf(dy, sN, ay); az = fmaf(dz, sN, az);
+        if (PN) {
+            const float4 vj = s.v[j];
+            const float nx = -dx * inv, ny = -dy * inv, nz = -dz * inv;
+            const float v12 = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
+            const float nv1 = nx * vi.x + ny * vi.y + nz * vi.z;
+            const float nv2 = nx * vj.x + ny * vj.y + nz * vj.z;
+            const float A = -vi.w - 2.f * vj.w + 4.f * v12 + 1.5f * nv2 * nv2 + (5.f * hi.w + 4.f * h.w) * G * inv;
+            const float B = 4.f * nv1 - 3.f * nv2;
+            const float f = h.w * inv2 * inv_c2;
+            px = fmaf(nx * A + (vi.x - vj.x) * B, f, px);
+            py = fmaf(ny * A + (vi.y - vj.y) * B, f, py);
+            pz = fmaf(nz * A + (vi.z - vj.z) * B, f, pz);
+        }
+    }
+    ax += px; ay += py; az += pz;
+}
+
+template <bool PN, int UNROLL>
+__device__ __forceinline__ void accel_f64(const EnsSlab<false>& s, int n, double4 xi, double4 vi, double eps2,
+                                          double G, double inv_c2, double& ax, double& ay, double& az) {
+    ax = ay = az = 0.0;
+#pragma unroll UNROLL
+    for (int j = 0; j < n; ++j) {
+        const double4 xj = s.x[j];
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+        double inv = r2 > 0.0 ? rsqrt(r2) : 0.0;
+        const double inv2 = inv * inv;
+        const double sN = xj.w * inv * inv2;
+        ax = fma(dx, sN, ax); ay = fma(dy, sN, ay); az = fma(dz, sN, az);
+        if (PN) {
+            const double4 vj = s.v[j];
+            const double nx = -dx * inv, ny = -dy * inv, nz = -dz * inv;
+            const double v12 = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
+            const double nv1 = nx * vi.x + ny * vi.y + nz * vi.z;
+            const double nv2 = nx * vj.x + ny * vj.y + nz * vj.z;
+            const double A = -vi.w - 2.0 * vj.w + 4.0 * v12 + 1.5 * nv2 * nv2 + 5.0 * G * xi.w * inv +
+                             4.0 * G * xj.w * inv;
+            const double B = 4.0 * nv1 - 3.0 * nv2;
+            const double f = xj.w * inv2 * inv_c2;
+            ax += (nx * A + (vi.x - vj.x) * B) * f;
+            ay += (ny * A + (vi.y - vj.y) * B) * f;
+            az += (nz * A + (vi.z - vj.z) * B) * f;
+        }
+    }
+}
+
+template <bool MIXED, bool PN, int UNROLL>
+__global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, const int32_t* __restrict__ off,
+                           double4* __restrict__ pm, double4* __restrict__ vel, double G, double eps2, double inv_c2,
+                           Coeffs k, int64_t nsteps, int check_every, unsigned int* __restrict__ work,
+                           const volatile int* __restrict__ cancel, int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char ens_smem[];
+    EnsSlab<MIXED>& slab = reinterpret_cast<EnsSlab<MIXED>*>(ens_smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const float Gf = (float)G, epsf = (float)eps2, icf = (float)inv_c2;
+    for (;;) {
+        unsigned int w = 0;
+        if (lane == 0) w = atomicAdd(work, 1u);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (w >= (unsigned)nsys) break;
+        const int sys = order[w];
+        const int b0 = off[sys], n = off[sys + 1] - b0;
+        const bool two = n > 32;
+        const bool v0 = lane < n, v1 = lane + 32 < n;
+        double4 x[2], v[2];
+        x[0] = v0 ? pm[b0 + lane] : make_double4(0, 0, 0, 0);
+        v[0] = v0 ? vel[b0 + lane] : make_double4(0, 0, 0, 0);
+        x[1] = v1 ? pm[b0 + lane + 32] : make_double4(0, 0, 0, 0);
+        v[1] = v1 ? vel[b0 + lane + 32] : make_double4(0, 0, 0, 0);
+        bool stop = false;
+        for (int64_t step = 0; step < nsteps; ++step) {
+            if (step % check_every == 0) {
+                int cflag = 0;
+                if (lane == 0) cflag = *cancel;
+                cflag = __shfl_sync(0xffffffffu, cflag, 0);
+                if (cflag) {
+                    if (lane == 0) atomicOr(err, ASTER_DEVERR_CANCEL);
+                    stop = true;
+                    break;
+                }
+            }
+            for (int st = 0; st < k.nst; ++st) {
+                const double c = k.cdt[st], d = k.ddt[st];
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    x[q].x += c * v[q].x; x[q].y += c * v[q].y; x[q].z += c * v[q].z;
+                    const bool vq = q ? v1 : v0;
+                    if (!vq) continue;
+                    const int idx = lane + 32 * q;
+                    const double vsq = v[q].x * v[q].x + v[q].y * v[q].y + v[q].z * v[q].z;
+                    if (MIXED) {
+                        EnsSlab<true>& sl = reinterpret_cast<EnsSlab<true>&>(slab);
+                        float4 h, l;
+                        ds_split(x[q].x, h.x, l.x);
+                        ds_split(x[q].y, h.y, l.y);
+                        ds_split(x[q].z, h.z, l.z);
+                        h.w = (float)x[q].w;
+                        l.w = 0.f;
+                        sl.hi[idx] = h;
+                        sl.lo[idx] = l;
+                        sl.v[idx] = make_float4((float)v[q].x, (float)v[q].y, (float)v[q].z, (float)vsq);
+                    } else {
+                        EnsSlab<false>& sl = reinterpret_cast<EnsSlab<false>&>(slab);
+                        sl.x[idx] = x[q];
+                        sl.v[idx] = make_double4(v[q].x, v[q].y, v[q].z, vsq);
+                    }
+                }
+                __syncwarp();
+                double a[2][3];
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    if (q == 1 && !two) { a[1][0] = a[1][1] = a[1][2] = 0.0; continue; }
+                    const int idx = (q ? v1 : v0) ? lane + 32 * q : 0;  // idle slots read body 0
+                    if (MIXED) {
+                        const EnsSlab<true>& sl = reinterpret_cast<const EnsSlab<true>&>(slab);
+                        float ax, ay, az;
+                        accel_f32<PN, UNROLL>(sl, n, sl.hi[idx], sl.lo[idx], sl.v[idx], epsf, Gf, icf, ax, ay, az);
+                        a[q][0] = G * ax; a[q][1] = G * ay; a[q][2] = G * az;
+                    } else {
+                        const EnsSlab<false>& sl = reinterpret_cast<const EnsSlab<false>&>(slab);
+                        double ax, ay, az;
+                        accel_f64<PN, UNROLL>(sl, n, sl.x[idx], sl.v[idx], eps2, G, inv_c2, ax, ay, az);
+                        a[q][0] = G * ax; a[q][1] = G * ay; a[q][2] = G * az;
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    v[q].x += d * a[q][0]; v[q].y += d * a[q][1]; v[q].z += d * a[q][2];
+                }
+            }
+            const double c = k.cdt[k.nst];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                x[q].x += c * v[q].x; x[q].y += c * v[q].y; x[q].z += c * v[q].z;
+            }
+        }
+        if (v0) { pm[b0 + lane] = x[0]; vel[b0 + lane] = v[0]; }
+        if (v1) { pm[b0 + lane + 32] = x[1]; vel[b0 + lane + 32] = v[1]; }
+        if (stop) break;
+    }
+}
+
+// FP64 energy of one system per warp (Newtonian + pairwise 1PN energy).
+__global__ void k_ensemble_energy(int32_t nsys, const int32_t* __restrict__ off, const double4* __restrict__ pm,
+                                  const double4* __restrict__ vel, double G, double eps2, double inv_c2, int pn,
+                                  double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t sys = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (sys >= nsys) return;
+    const int b0 = off[sys], n = off[sys + 1] - b0;
+    double e = 0.0, e1 = 0.0;
+    for (int i = lane; i < n; i += 32) {
+        const double4 xi = pm[b0 + i], vi = vel[b0 + i];
+        const double v2 = vi.x * vi.x + vi.y * vi.y + vi.z * vi.z;
+        e += 0.5 * xi.w * v2;
+        e1 += 0.375 * xi.w * v2 * v2;
+        for (int j = i + 1; j < n; ++j) {
+            const double4 xj = pm[b0 + j], vj = vel[b0 + j];
+            const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            const double r = sqrt(dx * dx + dy * dy + dz * dz + eps2);
+            e -= G * xi.w * xj.w / r;
+            const double vj2 = vj.x * vj.x + vj.y * vj.y + vj.z * vj.z;
+            const double vij = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
+            const double nvi = (dx * vi.x + dy * vi.y + dz * vi.z) / r;
+            const double nvj = (dx * vj.x + dy * vj.y + dz * vj.z) / r;
+            e1 += G * xi.w * xj.w / (2.0 * r) * (3.0 * (v2 + vj2) - 7.0 * vij - nvi * nvj);
+            e1 += G * G * xi.w * xj.w * (xi.w + xj.w) / (2.0 * r * r);
+        }
+    }
+    double t = e + (pn ? inv_c2 * e1 : 0.0);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) out[sys] = t;
+}
+
+__global__ void k_pack_ens(int64_t n, const double* __restrict__ pos, const double* __restrict__ vel,
+                           const double* __restrict__ m, double4* __restrict__ pm, double4* __restrict__ v4,
+                           int* __restrict__ err) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2], mm = m[i];
+        const double vx = vel ? vel[3 * i] : 0.0, vy = vel ? vel[3 * i + 1] : 0.0, vz = vel ? vel[3 * i + 2] : 0.0;
+        if (!(isfinite(x) && isfinite(y) && isfinite(z) && isfinite(mm) && isfinite(vx) && isfinite(vy) &&
+              isfinite(vz)))
+            atomicOr(err, ASTER_DEVERR_NONFINITE);
+        pm[i] = make_double4(x, y, z, mm);
+        v4[i] = make_double4(vx, vy, vz, 0.0);
+    }
+}
+
+__global__ void k_unpack_ens(int64_t n, const double4* __restrict__ src, double* __restrict__ dst) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double4 v = src[i];
+        dst[3 * i] = v.x; dst[3 * i + 1] = v.y; dst[3 * i + 2] = v.z;
+    }
+}
+
+template <bool MIXED, bool PN, int UNROLL>
+int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_t nsteps, int wpb, int check_every,
+                    bool use_graph) {
+    EnsBufs& e = c->ens;
+    auto kern = k_ensemble<MIXED, PN, UNROLL>;
+    const size_t smem = (size_t)wpb * sizeof(EnsSlab<MIXED>);
+    if (smem > 48 * 1024) ASTER_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    ASTER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
+    if (per_sm < 1) return ASTER_ERR_UNSUPPORTED;
+    int64_t blocks = (int64_t)c->sm_count * per_sm;
+    const int64_t need = (e.nsys + wpb - 1) / wpb;
+    if (blocks > need) blocks = need;
+    const double inv_c2 = PN ? 1.0 / (p->c * p->c) : 0.0;
+    unsigned int* work = e.counter.as<unsigned int>();
+    auto enqueue = [&](cudaStream_t s) -> int {
+        ASTER_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned int), s));
+        kern<<<(unsigned)blocks, wpb * 32, smem, s>>>(e.nsys, e.order.as<int32_t>(), e.off.as<int32_t>(),
+                                                     e.pm.as<double4>(), e.vel.as<double4>(), p->G, p->eps2, inv_c2, k,
+                                                     nsteps, check_every, work, e.cancel_dev, c->err_dev);
+        ASTER_CUDA(cudaGetLastError());
+        return ASTER_OK;
+    };
+    if (!use_graph) return enqueue(c->stream);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ASTER_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int st = enqueue(c->stream);
+    cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    if (st != ASTER_OK) { if (graph) cudaGraphDestroy(graph); return st; }
+    if (ce != cudaSuccess) return aster_cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return aster_cuda_fail(ce, "cudaGraphInstantiate", __FILE__, __LINE__);
+    ce = cudaGraphLaunch(exec, c->stream);
+    // the executable graph may be destroyed once its launch is enqueued
+    cudaGraphExecDestroy(exec);
+    if (ce != cudaSuccess) return aster_cuda_fail(ce, "cudaGraphLaunch", __FILE__, __LINE__);
+    return ASTER_OK;
+}
+
+template <bool MIXED, bool PN>
+int dispatch_unroll(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_t nsteps, int wpb, int unroll,
+                    int check_every, bool g) {
+    switch (unroll) {
+        case 1: return launch_ensemble<MIXED, PN, 1>(c, p, k, nsteps, wpb, check_every, g);
+        case 4: return launch_ensemble<MIXED, PN, 4>(c, p, k, nsteps, wpb, check_every, g);
+        default: return launch_ensemble<MIXED, PN, 2>(c, p, k, nsteps, wpb, check_every, g);
+    }
+}
+
+}  // namespace
+
+extern "C" int aster_ensemble_upload(aster_ctx* c, int32_t nsys, const int64_t* offsets, const double* pos,
+                                     const double* vel, const double* mass) {
+    if (!c || nsys <= 0 || !offsets || !pos || !mass) return ASTER_ERR_INVALID_ARG;
+    if (offsets[0] != 0) return ASTER_ERR_INVALID_ARG;
+    std::vector<int32_t> off32(nsys + 1);
+    for (int32_t s = 0; s < nsys; ++s) {
+        const int64_t sz = offsets[s + 1] - offsets[s];
+        if (sz < 1) return ASTER_ERR_INVALID_ARG;
+        if (sz > ASTER_ENSEMBLE_MAX_BODIES) return ASTER_ERR_TOO_LARGE;
+    }
+    const int64_t nb = offsets[nsys];
+    if (nb > (int64_t)INT32_MAX) return ASTER_ERR_TOO_LARGE;
+    double pairs = 0.0;
+    for (int32_t s = 0; s <= nsys; ++s) off32[s] = (int32_t)offsets[s];
+    std::vector<int32_t> order(nsys);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        return off32[a + 1] - off32[a] > off32[b + 1] - off32[b];
+    });
+    for (int32_t s = 0; s < nsys; ++s) {
+        const double sz = (double)(off32[s + 1] - off32[s]);
+        pairs += sz * (sz - 1.0);
+    }
+    ASTER_TRY(aster_begin(c));
+    EnsBufs& e = c->ens;
+    ASTER_TRY(e.pm.ensure((size_t)nb * sizeof(double4)));
+    ASTER_TRY(e.vel.ensure((size_t)nb * sizeof(double4)));
+    ASTER_TRY(e.off.ensure((size_t)(nsys + 1) * 4));
+    ASTER_TRY(e.order.ensure((size_t)nsys * 4));
+    ASTER_TRY(e.counter.ensure(256));
+    if (!e.cancel_host) {
+        void* h = nullptr;
+        ASTER_CUDA(cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped));
+        e.cancel_host = static_cast<volatile int*>(h);
+        *e.cancel_host = 0;
+        void* d = nullptr;
+        ASTER_CUDA(cudaHostGetDevicePointer(&d, h, 0));
+        e.cancel_dev = static_cast<int*>(d);
+    }
+    const size_t v3 = (size_t)nb * 3 * sizeof(double);
+    ASTER_TRY(c->stage.ensure(2 * v3 + (size_t)nb * sizeof(double)));
+    double* sp = c->stage.as<double>();
+    double* sv = sp + 3 * nb;
+    double* sm = sv + 3 * nb;
+    ASTER_CUDA(cudaMemcpyAsync(sp, pos, v3, cudaMemcpyHostToDevice, c->stream));
+    if (vel) ASTER_CUDA(cudaMemcpyAsync(sv, vel, v3, cudaMemcpyHostToDevice, c->stream));
+    ASTER_CUDA(cudaMemcpyAsync(sm, mass, (size_t)nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    ASTER_CUDA(cudaMemcpyAsync(e.off.ptr, off32.data(), (size_t)(nsys + 1) * 4, cudaMemcpyHostToDevice, c->stream));
+    ASTER_CUDA(cudaMemcpyAsync(e.order.ptr, order.data(), (size_t)nsys * 4, cudaMemcpyHostToDevice, c->stream));
+    const int grid = (int)std::min<int64_t>((nb + 255) / 256, (int64_t)c->sm_count * 16);
+    k_pack_ens<<<grid, 256, 0, c->stream>>>(nb, sp, vel ? sv : nullptr, sm, e.pm.as<double4>(), e.vel.as<double4>(),
+                                            c->err_dev);
+    ASTER_CUDA(cudaGetLastError());
+    int st = aster_finish(c);  // host vectors must outlive the copies: synchronised here
+    if (st != ASTER_OK) return st;
+    e.nsys = nsys;
+    e.nbodies = nb;
+    e.pair_evals_per_stage = pairs;
+    return ASTER_OK;
+}
+
+extern "C" int aster_ensemble_download(aster_ctx* c, double* pos, double* vel) {
+    if (!c) return ASTER_ERR_INVALID_ARG;
+    EnsBufs& e = c->ens;
+    if (e.nsys <= 0) return ASTER_ERR_NO_STATE;
+    ASTER_CUDA(cudaSetDevice(c->device));
+    const int64_t nb = e.nbodies;
+    const size_t v3 = (size_t)nb * 3 * sizeof(double);
+    ASTER_TRY(c->stage.ensure(2 * v3));
+    double* st = c->stage.as<double>();
+    const int grid = (int)std::min<int64_t>((nb + 255) / 256, (int64_t)c->sm_count * 16);
+    if (pos) {
+        k_unpack_ens<<<grid, 256, 0, c->stream>>>(nb, e.pm.as<double4>(), st);
+        ASTER_CUDA(cudaGetLastError());
+        ASTER_CUDA(cudaMemcpyAsync(pos, st, v3, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (vel) {
+        k_unpack_ens<<<grid, 256, 0, c->stream>>>(nb, e.vel.as<double4>(), st + 3 * nb);
+        ASTER_CUDA(cudaGetLastError());
+        ASTER_CUDA(cudaMemcpyAsync(vel, st + 3 * nb, v3, cudaMemcpyDeviceToHost, c->stream));
+    }
+    ASTER_CUDA(cudaStreamSynchronize(c->stream));
+    return ASTER_OK;
+}
+
+extern "C" int aster_ensemble_run(aster_ctx* c, const aster_params* p, int integrator, int precision, int64_t nsteps,
+                                  const aster_ensemble_config* cfg) {
+    if (!c || nsteps < 0) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (c->ens.nsys <= 0) return ASTER_ERR_NO_STATE;
+    if (integrator != ASTER_INTEGRATOR_LEAPFROG && integrator != ASTER_INTEGRATOR_YOSHIDA4) return ASTER_ERR_INVALID_ARG;
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    int wpb = cfg && cfg->warps_per_block ? cfg->warps_per_block : 4;
+    int unroll = cfg && cfg->unroll ? cfg->unroll : 2;
+    int check = cfg && cfg->check_every ? cfg->check_every : 256;
+    // stream capture is not possible on the legacy default stream
+    bool graph = (cfg ? cfg->use_graph != 0 : true) && c->stream != nullptr;
+    if (wpb < 1 || wpb > 16 || (unroll != 1 && unroll != 2 && unroll != 4) || check < 1) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    *c->ens.cancel_host = 0;
+    const Coeffs k = make_coeffs(integrator, p->dt);
+    const bool pn = (p->force_law & ASTER_PN1) != 0;
+    cudaEventRecord(c->ev[0], c->stream);
+    int st;
+    if (precision == ASTER_MIXED)
+        st = pn ? dispatch_unroll<true, true>(c, p, k, nsteps, wpb, unroll, check, graph)
+                : dispatch_unroll<true, false>(c, p, k, nsteps, wpb, unroll, check, graph);
+    else
+        st = pn ? dispatch_unroll<false, true>(c, p, k, nsteps, wpb, unroll, check, graph)
+                : dispatch_unroll<false, false>(c, p, k, nsteps, wpb, unroll, check, graph);
+    if (st != ASTER_OK) return st;
+    cudaEventRecord(c->ev[1], c->stream);
+    st = aster_finish(c);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = c->stats.ms_force = ms;
+    c->stats.kernels = 1;
+    c->stats.interactions = c->ens.pair_evals_per_stage * k.nst * (double)nsteps;
+    return st;
+}
+
+extern "C" int aster_ensemble_energy(aster_ctx* c, const aster_params* p, double* energy) {
+    if (!c || !energy) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    EnsBufs& e = c->ens;
+    if (e.nsys <= 0) return ASTER_ERR_NO_STATE;
+    ASTER_TRY(aster_begin(c));
+    ASTER_TRY(c->scratch.ensure((size_t)e.nsys * sizeof(double)));
+    const int wpb = 4;
+    const int blocks = (e.nsys + wpb - 1) / wpb;
+    const bool pn = (p->force_law & ASTER_PN1) != 0;
+    k_ensemble_energy<<<blocks, wpb * 32, 0, c->stream>>>(e.nsys, e.off.as<int32_t>(), e.pm.as<double4>(),
+                                                           e.vel.as<double4>(), p->G, p->eps2,
+                                                           pn ? 1.0 / (p->c * p->c) : 0.0, pn ? 1 : 0,
+                                                           c->scratch.as<double>());
+    ASTER_CUDA(cudaGetLastError());
+    ASTER_CUDA(cudaMemcpyAsync(energy, c->scratch.ptr, (size_t)e.nsys * sizeof(double), cudaMemcpyDeviceToHost,
+                               c->stream));
+    return aster_finish(c);
+}
+
+extern "C" int aster_ensemble_cancel(aster_ctx* c) {
+    if (!c || !c->ens.cancel_host) return ASTER_ERR_INVALID_ARG;
+    *c->ens.cancel_host = 1;
+    return ASTER_OK;
+}

@@ -159,6 +159,47 @@ int aster_kdk_steps(aster_ctx* ctx, const aster_params* p, int solver, int preci
 int aster_energy(aster_ctx* ctx, const aster_params* p, int ref_form, double* energy,
                  double* momentum3);
 
+/* ---- batched ensembles of few-body systems ------------------------------
+ * Thousands of independent systems of 1..64 bodies integrated by one
+ * persistent kernel (one warp per system, systems taken largest first from a
+ * work counter), launched through a captured CUDA graph. The pair law is the
+ * reference's (compute_gravitational / get_pn1, tool_chain_impl.cpp:110-137,
+ * Newton + optional pairwise 1PN); the integrators are compositions of
+ * drift-kick-drift leapfrog steps: the reference's leapfrog
+ * (tool_chain_impl.cpp:169-185, same map) and Yoshida's (1990) fourth-order
+ * triple jump, which the reference lacks. The reference has no batched
+ * solver; per-system Simulations would also share Parallelized's cached
+ * pointer (builder_endpoint.cpp:731). */
+#define ASTER_INTEGRATOR_LEAPFROG 0
+#define ASTER_INTEGRATOR_YOSHIDA4 1
+#define ASTER_ENSEMBLE_MAX_BODIES 64
+
+typedef struct aster_ensemble_config {
+    int32_t warps_per_block; /* 1..16 (0: 4)                                  */
+    int32_t unroll;          /* inner-loop unroll 1, 2 or 4 (0: 2)            */
+    int32_t check_every;     /* steps between cancel-flag reads (0: 256)      */
+    int32_t use_graph;       /* 1: capture the launch in a CUDA graph         */
+} aster_ensemble_config;
+
+/* offsets[nsys+1]: system s owns bodies offsets[s] .. offsets[s+1]-1 of the
+ * AoS FP64 arrays (1 <= size <= 64). vel may be NULL. */
+int aster_ensemble_upload(aster_ctx* ctx, int32_t nsys, const int64_t* offsets, const double* pos,
+                          const double* vel, const double* mass);
+int aster_ensemble_download(aster_ctx* ctx, double* pos, double* vel);
+/* nsteps steps of every system in one launch. precision: ASTER_MIXED (FP64
+ * state, FP32 pair terms on double-single separations) or ASTER_FP64.
+ * cfg may be NULL (defaults). Returns ASTER_ERR_CANCELLED if
+ * aster_ensemble_cancel was called meanwhile (systems stop at a step
+ * boundary that is a multiple of check_every). */
+int aster_ensemble_run(aster_ctx* ctx, const aster_params* p, int integrator, int precision, int64_t nsteps,
+                       const aster_ensemble_config* cfg);
+/* FP64 energy per system (energy[nsys]): Newtonian with the softened
+ * potential, plus the two-body 1PN (EIH) energy of every pair when the
+ * force law has the PN1 bit. */
+int aster_ensemble_energy(aster_ctx* ctx, const aster_params* p, double* energy);
+/* Thread-safe request to stop a running aster_ensemble_run. */
+int aster_ensemble_cancel(aster_ctx* ctx);
+
 /* Allocation-free energy. No counterpart in the reference.
  *
  * For callers that cannot allocate device memory: codes that reserve all of

@@ -535,6 +535,115 @@ static void trav_range(void* c_, long glo, long ghi) {
     free(list);
 }
 
+/* ------------------------------------------------------------------------ */
+/* batched ensemble: drift-kick compositions with the pairwise 1PN pair law  */
+/* ------------------------------------------------------------------------ */
+/* Yoshida (1990) fourth-order triple jump of the drift-kick-drift leapfrog:
+ *   w1 = 1/(2 - 2^(1/3)), w0 = -2^(1/3)/(2 - 2^(1/3))
+ *   drifts c = {w1/2, (w0+w1)/2, (w0+w1)/2, w1/2}, kicks d = {w1, w0, w1}
+ * Leapfrog (integrator 0): c = {1/2, 1/2}, d = {1}. One step:
+ *   x += c0 v dt; v += d0 a(x, v) dt; x += c1 v dt; ... ; x += c_last v dt
+ * The acceleration is the reference pair law (orc_pair_acc, Newton + optional
+ * pairwise 1PN of tool_chain_impl.cpp:110-137) summed over the system,
+ * evaluated with the current (x, v). The reference has no Yoshida integrator
+ * and no batched systems; this is the FP64 CPU reference for both. */
+void orc_ens_coeffs(int integrator, double* c, double* d, int* nstages) {
+    if (integrator == 1) {
+        double cb = cbrt(2.0);
+        double w1 = 1.0 / (2.0 - cb), w0 = -cb / (2.0 - cb);
+        c[0] = c[3] = 0.5 * w1;
+        c[1] = c[2] = 0.5 * (w0 + w1);
+        d[0] = d[2] = w1;
+        d[1] = w0;
+        *nstages = 3;
+    } else {
+        c[0] = c[1] = 0.5;
+        d[0] = 1.0;
+        *nstages = 1;
+    }
+}
+
+typedef struct {
+    const int64_t* off; double *pos, *vel; const double* m; double G, inv_c2, eps2, dt; int pn, integrator;
+    long nsteps;
+} ens_ctx;
+
+static void ens_range(void* c_, long lo, long hi) {
+    ens_ctx* c = (ens_ctx*)c_;
+    double cc[4], dd[3];
+    int ns;
+    orc_ens_coeffs(c->integrator, cc, dd, &ns);
+    double acc[64 * 3], a[3];
+    for (long s = lo; s < hi; ++s) {
+        long b0 = c->off[s], n = c->off[s + 1] - b0;
+        double* x = c->pos + 3 * b0;
+        double* v = c->vel + 3 * b0;
+        const double* m = c->m + b0;
+        for (long step = 0; step < c->nsteps; ++step) {
+            for (int st = 0; st < ns; ++st) {
+                for (long i = 0; i < 3 * n; ++i) x[i] += cc[st] * c->dt * v[i];
+                for (long i = 0; i < n; ++i) {
+                    double ax = 0, ay = 0, az = 0;
+                    for (long j = 0; j < n; ++j) {
+                        if (j == i) continue;
+                        orc_pair_acc(c->G, c->inv_c2, c->eps2, c->pn, m[i], m[j], v + 3 * i, v + 3 * j, x + 3 * i,
+                                     x + 3 * j, a);
+                        ax += a[0]; ay += a[1]; az += a[2];
+                    }
+                    acc[3 * i] = ax; acc[3 * i + 1] = ay; acc[3 * i + 2] = az;
+                }
+                for (long i = 0; i < 3 * n; ++i) v[i] += dd[st] * c->dt * acc[i];
+            }
+            for (long i = 0; i < 3 * n; ++i) x[i] += cc[ns] * c->dt * v[i];
+        }
+    }
+}
+
+/* Advances every system (bodies off[s]..off[s+1]-1, at most 64) nsteps. */
+void orc_ens_run(long nsys, const int64_t* off, double* pos, double* vel, const double* m, double G, double inv_c2,
+                 double eps2, int pn, int integrator, double dt, long nsteps) {
+    ens_ctx c = {off, pos, vel, m, G, inv_c2, eps2, dt, pn, integrator, nsteps};
+    orc_parallel(nsys, ens_range, &c);
+}
+
+/* Per-system energy: Newtonian (Plummer-softened potential) plus, with the
+ * PN1 bit, the two-body 1PN energy summed over pairs (harmonic gauge,
+ * r = sqrt(d.d + eps2), n = d/r):
+ *   (1/c^2) [ sum_i 3/8 m_i v_i^4
+ *           + sum_{i<j} G m_i m_j/(2r) (3(v_i^2 + v_j^2) - 7 v_i.v_j - (n.v_i)(n.v_j))
+ *           + sum_{i<j} G^2 m_i m_j (m_i + m_j)/(2 r^2) ]
+ * (the energy of the two-body Einstein-Infeld-Hoffmann Lagrangian, whose
+ * equations of motion are the pairwise 1PN law). The kicks evaluate the
+ * velocity-dependent force at the current velocity, as the reference's
+ * integrators do, so the PN part is integrated to first order in dt. */
+void orc_ens_energy(long nsys, const int64_t* off, const double* pos, const double* vel, const double* m,
+                    double G, double inv_c2, double eps2, int pn, double* e_out) {
+    for (long s = 0; s < nsys; ++s) {
+        long b0 = off[s], n = off[s + 1] - b0;
+        const double* x = pos + 3 * b0;
+        const double* v = vel + 3 * b0;
+        const double* mm = m + b0;
+        double e = 0, e1 = 0;
+        for (long i = 0; i < n; ++i) {
+            double v2 = v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2];
+            e += 0.5 * mm[i] * v2;
+            e1 += 0.375 * mm[i] * v2 * v2;
+            for (long j = i + 1; j < n; ++j) {
+                double d[3] = {x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]};
+                double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2);
+                e -= G * mm[i] * mm[j] / r;
+                double vj2 = v[3 * j] * v[3 * j] + v[3 * j + 1] * v[3 * j + 1] + v[3 * j + 2] * v[3 * j + 2];
+                double vij = v[3 * i] * v[3 * j] + v[3 * i + 1] * v[3 * j + 1] + v[3 * i + 2] * v[3 * j + 2];
+                double nvi = (d[0] * v[3 * i] + d[1] * v[3 * i + 1] + d[2] * v[3 * i + 2]) / r;
+                double nvj = (d[0] * v[3 * j] + d[1] * v[3 * j + 1] + d[2] * v[3 * j + 2]) / r;
+                e1 += G * mm[i] * mm[j] / (2.0 * r) * (3.0 * (v2 + vj2) - 7.0 * vij - nvi * nvj);
+                e1 += G * G * mm[i] * mm[j] * (mm[i] + mm[j]) / (2.0 * r * r);
+            }
+        }
+        e_out[s] = e + ((pn & PN1_FLAG) ? inv_c2 * e1 : 0.0);
+    }
+}
+
 /* acc and body_count (optional) are indexed by body (input order). */
 void orc_lbvh_forces(long n, int group, const int32_t* left, const int32_t* right, const int32_t* parent,
                      const int32_t* rlo, const int32_t* rhi, const int32_t* perm,

@@ -150,6 +150,11 @@ class Orc:
             lib.orc_groups.argtypes = [ctypes.c_long, ctypes.c_int, _I32, _I32, _I32, _I32, _I32]
             lib.orc_groups.restype = ctypes.c_long
             lib.orc_set_threads.argtypes = [ctypes.c_int]
+            _I64 = ctypes.POINTER(ctypes.c_int64)
+            lib.orc_ens_run.argtypes = [ctypes.c_long, _I64, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_long]
+            lib.orc_ens_energy.argtypes = [ctypes.c_long, _I64, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_int, _D]
             Orc._lib = lib
         self.lib = Orc._lib
 
@@ -266,3 +271,25 @@ class Orc:
         t.update(self.bottom_up(t["left"], t["right"], perm, pos, m, theta))
         t.update(codes=codes, sorted_codes=sc, perm=perm, box=B)
         return t
+
+    # -- batched ensembles --------------------------------------------------
+    def ens_run(self, offsets, pos, vel, m, dt, nsteps, G=1.0, c=None, eps2=0.0, integrator=1):
+        """Advance every system nsteps (integrator 1 = Yoshida-4, 0 = leapfrog);
+        PN1 when c is given. Returns new (pos, vel)."""
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        pos, vel, m = _c64(pos).copy(), _c64(vel).copy(), _c64(m)
+        pn = NEWTON | (PN1 if c else 0)
+        inv_c2 = 1.0 / (c * c) if c else 0.0
+        self.lib.orc_ens_run(len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(pos, _D),
+                             _p(vel, _D), _p(m, _D), G, inv_c2, eps2, pn, integrator, dt, nsteps)
+        return pos, vel
+
+    def ens_energy(self, offsets, pos, vel, m, G=1.0, c=None, eps2=0.0):
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        pos, vel, m = _c64(pos), _c64(vel), _c64(m)
+        e = np.zeros(len(off) - 1)
+        pn = NEWTON | (PN1 if c else 0)
+        inv_c2 = 1.0 / (c * c) if c else 0.0
+        self.lib.orc_ens_energy(len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(pos, _D),
+                                _p(vel, _D), _p(m, _D), G, inv_c2, eps2, pn, _p(e, _D))
+        return e
