@@ -40,6 +40,7 @@ EXPORTS = [
     "aster_state_download", "aster_state_size", "aster_allpairs", "aster_allpairs_targets", "aster_lbvh_build",
     "aster_lbvh_forces", "aster_kdk_steps", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
     "aster_ensemble_download", "aster_ensemble_run", "aster_ensemble_energy", "aster_ensemble_cancel",
+    "aster_adjoint_leapfrog",
 ]
 
 
@@ -122,6 +123,8 @@ def load_library(path: Path | str | None = None) -> ctypes.CDLL:
                                        ctypes.POINTER(CEnsembleConfig)]
     lib.aster_ensemble_energy.argtypes = [vp, ctypes.POINTER(CParams), vp]
     lib.aster_ensemble_cancel.argtypes = [vp]
+    lib.aster_adjoint_leapfrog.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, i64, ctypes.c_int32, vp,
+                                           ctypes.POINTER(dbl), vp, vp, vp]
     for name in EXPORTS:
         if not hasattr(lib, name):
             raise ImportError(f"{p} lacks {name}")
@@ -282,6 +285,19 @@ class Context:
 
     def ensemble_cancel(self):
         self._check(self.lib.aster_ensemble_cancel(self.h), "aster_ensemble_cancel")
+
+    # -- adjoint ---------------------------------------------------------------
+    def adjoint(self, p: Params, nsteps: int, target, precision: int = MIXED, checkpoint_every: int = 32):
+        """Loss L = mean_i |x_T,i - target_i|^2 after nsteps KDK steps from the
+        uploaded state and (dL/dx0, dL/dv0, dL/dm). The state is unchanged."""
+        tg = _aos(target, self.n)
+        gx, gv, gm = np.empty((self.n, 3)), np.empty((self.n, 3)), np.empty(self.n)
+        loss = ctypes.c_double()
+        cp = p.c_struct()
+        self._check(self.lib.aster_adjoint_leapfrog(self.h, ctypes.byref(cp), precision, nsteps, checkpoint_every,
+                                                    _ptr(tg), ctypes.byref(loss), _ptr(gx), _ptr(gv), _ptr(gm)),
+                    "aster_adjoint_leapfrog")
+        return loss.value, gx, gv, gm
 
 
 # ---------------------------------------------------------------------------

@@ -61,6 +61,11 @@ struct EnsBufs {
     int* cancel_dev = nullptr;
 };
 
+// Adjoint (reverse-mode) buffers.
+struct AdjBufs {
+    DevBuf ckpt, segx, lx, lv, lm, w, target, part;
+};
+
 struct aster_ctx {
     int device = 0;
     int sm_count = 148;
@@ -83,6 +88,7 @@ struct aster_ctx {
     int* stack_hw_dev = nullptr;  // tree-walk stack high-water mark
     LbvhBufs tree;
     EnsBufs ens;
+    AdjBufs adj;
     aster_stats stats{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };

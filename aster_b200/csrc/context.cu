@@ -114,7 +114,9 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
                       &c->tree.bmin, &c->tree.bmax, &c->tree.node_hi,
                       &c->tree.node_lo, &c->tree.child, &c->tree.groups};
     for (DevBuf* b : bufs) b->release();
-    DevBuf* ens[] = {&c->ens.pm, &c->ens.vel, &c->ens.off, &c->ens.order, &c->ens.counter};
+    DevBuf* ens[] = {&c->ens.pm, &c->ens.vel, &c->ens.off, &c->ens.order, &c->ens.counter,
+                     &c->adj.ckpt, &c->adj.segx, &c->adj.lx, &c->adj.lv, &c->adj.lm, &c->adj.w,
+                     &c->adj.target, &c->adj.part};
     for (DevBuf* b : ens) b->release();
     if (c->ens.cancel_host) cudaFreeHost((void*)c->ens.cancel_host);
     for (int i = 0; i < 4; ++i)

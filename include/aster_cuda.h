@@ -200,6 +200,23 @@ int aster_ensemble_energy(aster_ctx* ctx, const aster_params* p, double* energy)
 /* Thread-safe request to stop a running aster_ensemble_run. */
 int aster_ensemble_cancel(aster_ctx* ctx);
 
+/* ---- adjoint of the kick-drift-kick leapfrog ----------------------------
+ * Loss L = (1/n) sum_i |x_T,i - target_i|^2 after nsteps KDK steps (the
+ * aster_kdk_steps map, Newtonian all-pairs forces) from the uploaded state,
+ * and its gradients dL/dx0, dL/dv0 (host, n*3) and dL/dm (host, n) by a
+ * hand-written reverse sweep: the forward pass stores (x, v, a) every
+ * checkpoint_every steps; the reverse pass recomputes each segment from its
+ * checkpoint and runs the adjoint recurrences
+ *   lv' = lv + dt lx;  w = c h lv';  lx += J(x_n)^T w;  lm += (dA/dm)^T w
+ * (h = dt/2, c = 2 except at n = 0) with one O(N^2) tidal-tensor/vector kernel
+ * per step. precision ASTER_MIXED: FP32 pair arithmetic (forces and adjoint),
+ * FP64 state and adjoint variables; ASTER_FP64: FP64 throughout. The uploaded
+ * state is unchanged on return. The reference has no adjoint. Any output
+ * pointer may be NULL. */
+int aster_adjoint_leapfrog(aster_ctx* ctx, const aster_params* p, int precision, int64_t nsteps,
+                           int32_t checkpoint_every, const double* target, double* loss, double* grad_x0,
+                           double* grad_v0, double* grad_m);
+
 /* Allocation-free energy. No counterpart in the reference.
  *
  * For callers that cannot allocate device memory: codes that reserve all of

@@ -644,6 +644,86 @@ void orc_ens_energy(long nsys, const int64_t* off, const double* pos, const doub
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* adjoint of the KDK leapfrog (FP64 reverse mode, no checkpointing)         */
+/* ------------------------------------------------------------------------ */
+/* Forward (h = dt/2, A = Newtonian softened acceleration, orc_kdk's map):
+ *   v' = v_n + h A(x_n);  x_{n+1} = x_n + dt v';  v_{n+1} = v' + h A(x_{n+1})
+ * Loss L = (1/N) sum_i |x_T,i - x*_i|^2. Reverse sweep, lx = dL/dx, lv = dL/dv:
+ *   seed lx = (2/N)(x_T - x*), lv = 0, lm = 0
+ *   for n = T-1 .. 0:  lv' = lv + dt lx;  w = c_n h lv'  (c_n = 2 for n >= 1,
+ *                      1 for n = 0: A(x_n) enters the closing kick of step n-1
+ *                      and the opening kick of step n with the same cotangent)
+ *                      lx += J(x_n)^T w;  lm += (dA/dm)^T w;  lv = lv'
+ * with d = x_j - x_k, s = (d.d + eps2)^(-1/2):
+ *   (J^T w)_k  = G sum_{j != k} [ s^3 u - 3 s^5 d (d.u) ],  u = m_k w_j - m_j w_k
+ *   (dA/dm)^T w at k = -G sum_{j != k} s^3 (w_j . d)
+ * The reference has no adjoint; this is the FP64 CPU reverse-mode reference. */
+void orc_adjoint_pair(long n, const double* x, const double* m, const double* w, double G, double eps2,
+                      double* jt, double* gm) {
+    for (long k = 0; k < n; ++k) {
+        double jx = 0, jy = 0, jz = 0, g = 0;
+        for (long j = 0; j < n; ++j) {
+            if (j == k) continue;
+            double d[3] = {x[3 * j] - x[3 * k], x[3 * j + 1] - x[3 * k + 1], x[3 * j + 2] - x[3 * k + 2]};
+            double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
+            double s = 1.0 / sqrt(r2);
+            double s3 = s * s * s, s5 = s3 * s * s;
+            double u[3] = {m[k] * w[3 * j] - m[j] * w[3 * k], m[k] * w[3 * j + 1] - m[j] * w[3 * k + 1],
+                           m[k] * w[3 * j + 2] - m[j] * w[3 * k + 2]};
+            double du = d[0] * u[0] + d[1] * u[1] + d[2] * u[2];
+            jx += s3 * u[0] - 3.0 * s5 * d[0] * du;
+            jy += s3 * u[1] - 3.0 * s5 * d[1] * du;
+            jz += s3 * u[2] - 3.0 * s5 * d[2] * du;
+            g -= s3 * (w[3 * j] * d[0] + w[3 * j + 1] * d[1] + w[3 * j + 2] * d[2]);
+        }
+        jt[3 * k] = G * jx; jt[3 * k + 1] = G * jy; jt[3 * k + 2] = G * jz;
+        gm[k] = G * g;
+    }
+}
+
+/* Loss and gradients dL/dx0, dL/dv0, dL/dm of the trajectory from (x0, v0, m).
+ * Keeps every position of the trajectory (small n and T only). */
+double orc_adjoint(long n, const double* x0, const double* v0, const double* m, const double* target, double G,
+                   double eps2, double dt, long T, double* gx, double* gv, double* gmass) {
+    double* xs = (double*)malloc((size_t)(T + 1) * n * 3 * sizeof(double));
+    double* v = (double*)malloc((size_t)n * 3 * sizeof(double));
+    double* a = (double*)malloc((size_t)n * 3 * sizeof(double));
+    double* w = (double*)malloc((size_t)n * 3 * sizeof(double));
+    double* jt = (double*)malloc((size_t)n * 3 * sizeof(double));
+    double* gm = (double*)malloc((size_t)n * sizeof(double));
+    const double h = 0.5 * dt;
+    memcpy(xs, x0, (size_t)n * 3 * sizeof(double));
+    memcpy(v, v0, (size_t)n * 3 * sizeof(double));
+    orc_allpairs(n, xs, NULL, m, G, 0.0, eps2, 1, 0, NULL, a);
+    for (long t = 0; t < T; ++t) {
+        double* xc = xs + (size_t)t * n * 3;
+        double* xn = xs + (size_t)(t + 1) * n * 3;
+        for (long i = 0; i < 3 * n; ++i) { v[i] += h * a[i]; xn[i] = xc[i] + dt * v[i]; }
+        orc_allpairs(n, xn, NULL, m, G, 0.0, eps2, 1, 0, NULL, a);
+        for (long i = 0; i < 3 * n; ++i) v[i] += h * a[i];
+    }
+    const double* xT = xs + (size_t)T * n * 3;
+    double loss = 0.0;
+    for (long i = 0; i < 3 * n; ++i) {
+        double d = xT[i] - target[i];
+        loss += d * d;
+        gx[i] = 2.0 * d / (double)n;
+        gv[i] = 0.0;
+    }
+    loss /= (double)n;
+    for (long k = 0; k < n; ++k) gmass[k] = 0.0;
+    for (long t = T - 1; t >= 0; --t) {
+        const double c = t >= 1 ? 2.0 : 1.0;
+        for (long i = 0; i < 3 * n; ++i) { gv[i] += dt * gx[i]; w[i] = c * h * gv[i]; }
+        orc_adjoint_pair(n, xs + (size_t)t * n * 3, m, w, G, eps2, jt, gm);
+        for (long i = 0; i < 3 * n; ++i) gx[i] += jt[i];
+        for (long k = 0; k < n; ++k) gmass[k] += gm[k];
+    }
+    free(xs); free(v); free(a); free(w); free(jt); free(gm);
+    return loss;
+}
+
 /* acc and body_count (optional) are indexed by body (input order). */
 void orc_lbvh_forces(long n, int group, const int32_t* left, const int32_t* right, const int32_t* parent,
                      const int32_t* rlo, const int32_t* rhi, const int32_t* perm,

@@ -293,3 +293,18 @@ class Orc:
         self.lib.orc_ens_energy(len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(pos, _D),
                                 _p(vel, _D), _p(m, _D), G, inv_c2, eps2, pn, _p(e, _D))
         return e
+
+    # -- adjoint -------------------------------------------------------------
+    def adjoint(self, x0, v0, m, target, dt, nsteps, G=1.0, eps2=0.0):
+        """FP64 reverse mode: (loss, dL/dx0, dL/dv0, dL/dm) of
+        L = mean_i |x_T,i - target_i|^2 after nsteps KDK steps."""
+        x0, v0, m, tg = _c64(x0), _c64(v0), _c64(m), _c64(target)
+        n = len(m)
+        gx, gv, gm = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n)
+        f = self.lib.orc_adjoint
+        f.restype = ctypes.c_double
+        f.argtypes = [ctypes.c_long, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                      ctypes.c_long, _D, _D, _D]
+        loss = f(n, _p(x0, _D), _p(v0, _D), _p(m, _D), _p(tg, _D), G, eps2, dt, nsteps, _p(gx, _D), _p(gv, _D),
+                 _p(gm, _D))
+        return loss, gx, gv, gm
