@@ -128,7 +128,7 @@ __device__ __forceinline__ void accel_f64(const EnsSlab<false>& s, int n, double
     }
 }
 
-template <bool MIXED, bool PN, int UNROLL>
+template <bool MIXED, bool PN, int UNROLL, int NST>
 __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, const int32_t* __restrict__ off,
                            double4* __restrict__ pm, double4* __restrict__ vel, double G, double eps2, double inv_c2,
                            Coeffs k, int64_t nsteps, int check_every, unsigned int* __restrict__ work,
@@ -163,7 +163,8 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
                     break;
                 }
             }
-            for (int st = 0; st < k.nst; ++st) {
+#pragma unroll
+            for (int st = 0; st < NST; ++st) {  // unrolled: coefficients stay in registers
                 const double c = k.cdt[st], d = k.ddt[st];
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
@@ -213,7 +214,7 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
                     v[q].x += d * a[q][0]; v[q].y += d * a[q][1]; v[q].z += d * a[q][2];
                 }
             }
-            const double c = k.cdt[k.nst];
+            const double c = k.cdt[NST];
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 x[q].x += c * v[q].x; x[q].y += c * v[q].y; x[q].z += c * v[q].z;
@@ -282,7 +283,7 @@ template <bool MIXED, bool PN, int UNROLL>
 int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_t nsteps, int wpb, int check_every,
                     bool use_graph) {
     EnsBufs& e = c->ens;
-    auto kern = k_ensemble<MIXED, PN, UNROLL>;
+    auto kern = k.nst == 3 ? k_ensemble<MIXED, PN, UNROLL, 3> : k_ensemble<MIXED, PN, UNROLL, 1>;
     const size_t smem = (size_t)wpb * sizeof(EnsSlab<MIXED>);
     if (smem > 48 * 1024) ASTER_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;

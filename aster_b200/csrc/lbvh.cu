@@ -508,8 +508,10 @@ __device__ __forceinline__ void interact_f64(const double4 e, const double4 b, d
 }
 
 // Persistent walk: each warp takes groups from a global work counter until
-// none are left. Per group: the lanes hold the group's bodies (one or two
-// sorted leaves per lane), the warp pops up to 32 nodes per round from its
+// none are left. Per group: lane l holds sorted leaf l of the group; the r
+// leaves beyond 32 are each shared by 32/r (rounded down to a power of two)
+// lanes that split the interaction list between them, so groups of 33..64
+// bodies keep every lane busy. The warp pops up to 32 nodes per round from its
 // shared stack, each lane loads its node's record (centre of mass, mass,
 // opening radius, children: independent loads, one latency), decides
 // open/accept, children of opened nodes are pushed, accepted nodes appended to
@@ -519,7 +521,7 @@ __device__ __forceinline__ void interact_f64(const double4 e, const double4 b, d
 // interaction needs one subtraction per axis; the group is compact, so the
 // relative coordinates keep FP32 precision of the separation.
 template <bool MIXED, bool GUARD, bool KICK>
-__global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
+__global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
     int64_t n, const int2* __restrict__ groups, const unsigned int* __restrict__ ngroups_p,
     unsigned int* __restrict__ work, const float4* __restrict__ node_hi, const float4* __restrict__ node_lo,
     const double4* __restrict__ node_cm, const int2* __restrict__ child, const int32_t* __restrict__ perm,
@@ -541,10 +543,16 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= ngroups) break;
         const int2 gr = groups[g];
-        const bool two = gr.y > 32;  // warp-uniform: two bodies per lane
-        const bool v0 = lane < gr.y, v1 = lane + 32 < gr.y;
+        // Bodies 0..31 of the group: one per lane (primary). Bodies 32.. (r of
+        // them, "secondary"): each shared by lps lanes that split the list.
+        const int r = gr.y > 32 ? gr.y - 32 : 0;
+        const bool two = r > 0;  // warp-uniform
+        int lps = 32;
+        while (lps > 1 && lps * r > 32) lps >>= 1;
+        const int sb = lane / lps, sub = lane & (lps - 1);
+        const bool v0 = lane < gr.y, v1 = two && sb < r;
         const int64_t k0 = (int64_t)gr.x + (v0 ? lane : 0);
-        const int64_t k1 = (int64_t)gr.x + (v1 ? lane + 32 : 0);
+        const int64_t k1 = (int64_t)gr.x + (v1 ? 32 + sb : 0);
 
         const float4 h0 = node_hi[k0], l0 = node_lo[k0];
         const float4 h1 = two ? node_hi[k1] : h0, l1 = two ? node_lo[k1] : l0;
@@ -574,30 +582,20 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
         auto evaluate = [&](int cnt) {
             if (MIXED) {
                 float ax0 = 0.f, ay0 = 0.f, az0 = 0.f, ax1 = 0.f, ay1 = 0.f, az1 = 0.f;
+#pragma unroll 8
+                for (int e = 0; e < cnt; ++e) interact_f32<GUARD>(sm.lrel[warp][e], b0, epsf, ax0, ay0, az0);
+                sx0.add(ax0); sy0.add(ay0); sz0.add(az0);
                 if (two) {
 #pragma unroll 4
-                    for (int e = 0; e < cnt; ++e) {
-                        const float4 en = sm.lrel[warp][e];
-                        interact_f32<GUARD>(en, b0, epsf, ax0, ay0, az0);
-                        interact_f32<GUARD>(en, b1, epsf, ax1, ay1, az1);
-                    }
+                    for (int e = sub; e < cnt; e += lps) interact_f32<GUARD>(sm.lrel[warp][e], b1, epsf, ax1, ay1, az1);
                     sx1.add(ax1); sy1.add(ay1); sz1.add(az1);
-                } else {
-#pragma unroll 8
-                    for (int e = 0; e < cnt; ++e) interact_f32<GUARD>(sm.lrel[warp][e], b0, epsf, ax0, ay0, az0);
                 }
-                sx0.add(ax0); sy0.add(ay0); sz0.add(az0);
             } else {
+#pragma unroll 4
+                for (int e = 0; e < cnt; ++e) interact_f64<GUARD>(sm.lcm[warp][e], c0, eps2, dx0, dy0, dz0);
                 if (two) {
 #pragma unroll 2
-                    for (int e = 0; e < cnt; ++e) {
-                        const double4 en = sm.lcm[warp][e];
-                        interact_f64<GUARD>(en, c0, eps2, dx0, dy0, dz0);
-                        interact_f64<GUARD>(en, c1, eps2, dx1, dy1, dz1);
-                    }
-                } else {
-#pragma unroll 4
-                    for (int e = 0; e < cnt; ++e) interact_f64<GUARD>(sm.lcm[warp][e], c0, eps2, dx0, dy0, dz0);
+                    for (int e = sub; e < cnt; e += lps) interact_f64<GUARD>(sm.lcm[warp][e], c1, eps2, dx1, dy1, dz1);
                 }
             }
             total += cnt;
@@ -674,15 +672,26 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_walk(
         if (lc > 0) evaluate(lc);
         __syncwarp();
         wtotal += (unsigned long long)total * (unsigned long long)gr.y;
+        // secondary bodies: add the lps partial sums (aligned lane groups)
+        double s1x = MIXED ? sx1.value() : dx1, s1y = MIXED ? sy1.value() : dy1, s1z = MIXED ? sz1.value() : dz1;
+        if (two) {
+            for (int o = lps >> 1; o >= 1; o >>= 1) {
+                s1x += __shfl_xor_sync(0xffffffffu, s1x, o);
+                s1y += __shfl_xor_sync(0xffffffffu, s1y, o);
+                s1z += __shfl_xor_sync(0xffffffffu, s1z, o);
+            }
+        }
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const bool vq = q ? v1 : v0;
+            const bool vq = q ? (v1 && sub == 0) : v0;
             if (!vq) continue;
             double ax, ay, az;
-            if (MIXED) {
-                ax = G * (q ? sx1 : sx0).value(); ay = G * (q ? sy1 : sy0).value(); az = G * (q ? sz1 : sz0).value();
+            if (q) {
+                ax = G * s1x; ay = G * s1y; az = G * s1z;
+            } else if (MIXED) {
+                ax = G * sx0.value(); ay = G * sy0.value(); az = G * sz0.value();
             } else {
-                ax = G * (q ? dx1 : dx0); ay = G * (q ? dy1 : dy0); az = G * (q ? dz1 : dz0);
+                ax = G * dx0; ay = G * dy0; az = G * dz0;
             }
             const int32_t b = perm[q ? k1 : k0];
             acc[b] = make_double4(ax, ay, az, 0.0);

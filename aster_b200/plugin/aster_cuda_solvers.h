@@ -1,0 +1,73 @@
+// Reference-side binding: Aster Solver/Updater classes backed by the B200
+// C ABI (include/aster_cuda.h). A maintainer adds this file and
+// aster_cuda_solvers.cpp to Aster's sources and links libaster_cuda.so.
+//
+//   Solver   include/Aster/simulations/sim_obj.h:34-61
+//   Updater  include/Aster/simulations/sim_obj.h:64-77
+//
+// Registration (bake_solver, src/utils/updater.cpp:155-170, is a closed
+// switch, so the objects are attached after Simulation::load()):
+//   sim->load();
+//   auto* s = new Aster::CudaLBVH(sim);           // or CudaAllPairs
+//   sim->solver = s; s->load();
+//   sim->update_with(new Aster::CudaKDK(sim, s)); // optional: device-resident steps
+#pragma once
+
+#include "Aster/simulations/sim_obj.h"
+#include "aster_cuda.h"
+
+namespace Aster {
+
+// Drop-in for Parallelized / SimpleGPU (src/utils/builder_endpoint.cpp:729-757,
+// src/solvers/SimpleGPU.cpp:17-71): compute_forces() uploads the bodies,
+// evaluates all pairs on the GPU and writes accelerations to bodies.accs,
+// honouring force_law (Newton, PN1), softening, G and c.
+class CudaAllPairs : public Solver {
+public:
+    explicit CudaAllPairs(Simulation* s, int precision = ASTER_MIXED, int device = 0);
+    ~CudaAllPairs() override;
+    void load() override;
+    void compute_forces() override;
+
+    aster_ctx* context() const { return ctx_; }
+    int precision() const { return precision_; }
+    virtual int solver_kind() const { return ASTER_SOLVER_ALLPAIRS; }
+    aster_params params() const;
+    // copies bodies (positions, velocities, masses) to the device
+    void upload();
+
+protected:
+    static void check(int status, const char* where);
+    aster_ctx* ctx_ = nullptr;
+    int precision_;
+    int device_;
+};
+
+// Drop-in for Barnes_Hut / BH_hyper (src/solvers/barnes_hut.cpp:402-418,
+// src/solvers/full_GPU.cpp:519-527): LBVH build + warp-group walk at
+// Simulation::theta (Newtonian force law only).
+class CudaLBVH : public CudaAllPairs {
+public:
+    explicit CudaLBVH(Simulation* s, int precision = ASTER_MIXED, int device = 0);
+    void compute_forces() override;
+    int solver_kind() const override { return ASTER_SOLVER_LBVH; }
+};
+
+// Drop-in for update_leapfrog (src/physics/tool_chain_impl.cpp:169-185):
+// one kick-drift-kick step per update_bodies() with the state kept on the
+// device (one force evaluation per step instead of two). bodies.positions /
+// velocities / accs are refreshed after every step, since the reference's
+// step() only reads GPU buffers back for its own OpenCL solvers.
+class CudaKDK : public Updater {
+public:
+    CudaKDK(Simulation* s, CudaAllPairs* solver);
+    void update_bodies() override;
+    // next update re-uploads bodies (call after changing them on the host)
+    void invalidate() { uploaded_ = false; }
+
+private:
+    CudaAllPairs* solver_;
+    bool uploaded_ = false;
+};
+
+}  // namespace Aster

@@ -339,7 +339,87 @@ def secondary(ctx, args):
     res["mixed_vs_fp64_rel_l2"] = float(np.linalg.norm(accs["mixed"] - accs["fp64"]) / np.linalg.norm(accs["fp64"]))
     res["workload"] = "C3 cold exponential disk N=262144 (+central mass 0.1), eps=0.002, one force evaluation"
     out["allpairs"] = res
+    out["ensemble"] = ensemble_c4(ctx)
+    out["adjoint"] = adjoint_c5(ctx)
     return out
+
+
+def ensemble_c4(ctx, nsteps: int = 10_000):
+    """C4: 16384 hierarchical systems (n in [3, 64]), pairwise 1PN (c = 100),
+    Yoshida-4, dt = 1e-4, nsteps in one persistent graph-captured launch with
+    the autotuned launch shape; FP32 pair terms, FP64 state."""
+    from aster_b200 import gen
+    from aster_b200.api import MIXED, NEWTON, PN1, YOSHIDA4, Params
+    from aster_b200.autotune import tune_ensemble
+    pos, vel, m, off = gen.hierarchical_ensemble(16384, 1004)
+    p = Params(G=1.0, c=100.0, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1)
+    ctx.ensemble_upload(off, pos, vel, m)
+    cfg = tune_ensemble(ctx, off, p, steps=40, cache=None)
+    cfg = {k: cfg[k] for k in ("warps_per_block", "unroll", "check_every", "use_graph")}
+    e0 = ctx.ensemble_energy(p)
+    ctx.ensemble_run(p, nsteps, YOSHIDA4, MIXED, cfg)
+    st = ctx.stats()
+    e1 = ctx.ensemble_energy(p)
+    de = np.abs((e1 - e0) / e0)
+    return {"workload": "C4 16384 systems n~U[3,64], 1PN c=100, Yoshida-4, dt=1e-4, one graph-captured launch",
+            "steps": nsteps, "ms": st["ms_total"], "steps_per_s": nsteps / (st["ms_total"] / 1e3),
+            "pair_terms_per_s": st["interactions"] / (st["ms_total"] / 1e3), "config": cfg,
+            "energy_drift_median": float(np.median(de)), "energy_drift_p90": float(np.percentile(de, 90))}
+
+
+def adjoint_c5(ctx):
+    """C5: N=16384 Plummer, eps=0.01, dt=1e-3, 1000 KDK steps, checkpoints
+    every 32; forward + reverse sweep time for dL/d(x0, v0, m)."""
+    from aster_b200 import gen
+    from aster_b200.api import FP64, MIXED, SOLVER_ALLPAIRS, Params
+    n, T = 16384, 1000
+    p = Params(eps2=1e-4, dt=1e-3)
+    x0, v0, m = gen.plummer(n, 1005)
+    rng = np.random.default_rng(1005)
+    ctx.upload(x0 + rng.normal(0, 1e-3, x0.shape), v0, m)
+    ctx.kdk_steps(p, T, SOLVER_ALLPAIRS, FP64)
+    target, _, _ = ctx.download()
+    ctx.upload(x0, v0, m)
+    out = {"workload": "C5 Plummer N=16384, eps=0.01, dt=1e-3, 1000 KDK steps, loss=mean|x_T-x*|^2, K=32"}
+    for name, prec in (("mixed", MIXED), ("fp64", FP64)):
+        loss, *_ = ctx.adjoint(p, T, target, prec, 32)
+        out[name] = {"ms_forward_plus_adjoint": ctx.stats()["ms_total"], "loss": loss}
+    return out
+
+
+def run_case(args):
+    """One secondary workload, briefly: C3 all-pairs (a warm-up then one
+    FP64 and one mixed evaluation), C4 ensemble (a 50-step launch), C5 adjoint
+    (8 steps, checkpoints every 4)."""
+    from aster_b200 import gen
+    from aster_b200.api import FP64, MIXED, NEWTON, PN1, YOSHIDA4, Context, Params
+    ctx = Context(0)
+    out = {"case": args.case}
+    if args.case == "allpairs":
+        pos, vel, m = gen.exponential_disk(N_C3, SEED_C3)
+        p3 = Params(G=1.0, eps2=EPS_C3 ** 2, dt=1e-4)
+        ctx.upload(pos, vel, m)
+        for prec in (FP64, MIXED):
+            ctx.allpairs(p3, prec)
+            ctx.allpairs(p3, prec)
+            out[f"ms_{prec}"] = ctx.stats()["ms_force"]
+    elif args.case == "ensemble":
+        pos, vel, m, off = gen.hierarchical_ensemble(16384, 1004)
+        p = Params(G=1.0, c=100.0, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1)
+        ctx.ensemble_upload(off, pos, vel, m)
+        cfg = {"warps_per_block": 8, "unroll": 2, "use_graph": 1}
+        ctx.ensemble_run(p, 5, YOSHIDA4, MIXED, cfg)
+        ctx.ensemble_run(p, 50, YOSHIDA4, MIXED, cfg)
+        out["ms_50_steps"] = ctx.stats()["ms_total"]
+    else:
+        x0, v0, m = gen.plummer(16384, 1005)
+        p = Params(eps2=1e-4, dt=1e-3)
+        ctx.upload(x0, v0, m)
+        ctx.adjoint(p, 8, x0 + 1e-3, MIXED, 4)
+        out["ms"] = ctx.stats()["ms_total"]
+    ctx.close()
+    print(json.dumps(out), flush=True)
+    return 0
 
 
 def main():
@@ -355,10 +435,14 @@ def main():
                     help="bodies in the headline workload (default 2^20; smaller only for profiling captures)")
     ap.add_argument("--walk-traffic", type=float, default=WALK_TRAFFIC_BYTES,
                     help="DRAM bytes per walk launch from an ncu capture (reported as roofline.traffic)")
+    ap.add_argument("--case", default=None, choices=["allpairs", "ensemble", "adjoint"],
+                    help="run one secondary workload briefly (used for profiling captures) and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warm-up raised to 3 steps (timing rule)")
         args.warmup = 3
+    if args.case:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -1,0 +1,65 @@
+// Test driver for the reference-side binding (aster_b200/plugin): builds a
+// reference Aster::Simulation (the reference library compiled from its own
+// sources, oracle/_ref), attaches CudaAllPairs / CudaLBVH and either the
+// reference's own leapfrog updater or CudaKDK, runs Simulation::step() and
+// exports the bodies. TEST INFRASTRUCTURE ONLY.
+#include <cstdint>
+#include <vector>
+
+#include "Aster/simulations/sim_obj.h"
+#include "aster_cuda_solvers.h"
+
+namespace {
+// the reference has no double setter for G/c/dt and `data` is protected
+struct PluginSim : public Aster::Simulation {
+    void set_consts(double G, double c, double dt) {
+        data.G = G;
+        data.c = c;
+        data.c_squared = c * c;
+        data.dt = dt;
+    }
+};
+}  // namespace
+
+extern "C" int plg_run(int n, const double* pos, const double* vel, const double* m, double G, double c, double dt,
+                       double eps2, double theta, int force_law, int solver_kind, int precision, int use_cuda_kdk,
+                       int nsteps, double* pos_out, double* vel_out, double* acc_out) {
+    if (n <= 0) return -1;
+    auto* s = new PluginSim();
+    s->bodies.positions.resize(n);
+    s->bodies.velocities.resize(n);
+    s->bodies.accs.assign(n, Aster::vec3(0.0));
+    s->bodies.masses.assign(m, m + n);
+    s->bodies.temps.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        s->bodies.positions[i] = Aster::vec3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        s->bodies.velocities[i] = Aster::vec3(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+    }
+    s->set_consts(G, c, dt);
+    s->softening = eps2;
+    s->theta = theta;
+    s->force_law = Aster::PN_expansion_type((short)force_law);
+    Aster::CudaAllPairs* solver = solver_kind == 1 ? new Aster::CudaLBVH(s, precision) : new Aster::CudaAllPairs(s, precision);
+    solver->force_law = Aster::PN_expansion_type((short)force_law);
+    s->solver = solver;
+    solver->load();
+    Aster::Updater* up = use_cuda_kdk ? static_cast<Aster::Updater*>(new Aster::CudaKDK(s, solver))
+                                      : new Aster::Updater(s, 0, Aster::LEAPFROG);
+    s->updater = up;
+    if (nsteps == 0) solver->compute_forces();
+    for (int k = 0; k < nsteps; ++k) s->step();
+    for (int i = 0; i < n; ++i) {
+        const auto& p = s->bodies.positions[i];
+        const auto& v = s->bodies.velocities[i];
+        const auto& a = s->bodies.accs[i];
+        pos_out[3 * i] = p.x; pos_out[3 * i + 1] = p.y; pos_out[3 * i + 2] = p.z;
+        vel_out[3 * i] = v.x; vel_out[3 * i + 1] = v.y; vel_out[3 * i + 2] = v.z;
+        acc_out[3 * i] = a.x; acc_out[3 * i + 1] = a.y; acc_out[3 * i + 2] = a.z;
+    }
+    s->solver = nullptr;
+    s->updater = nullptr;
+    delete up;
+    delete solver;
+    delete s;  // never load()ed: the destructor frees nothing else
+    return 0;
+}
