@@ -220,6 +220,90 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
                          cz[k].value() + (double)pz[k], Gd, nslices, slice, nt, partial, acc, out3, kick);
 }
 
+// Newtonian mixed path with the paired FP32 instructions of sm_100
+// (add/mul/fma .f32x2): two j bodies per instruction. The j-tile is staged
+// pair-interleaved so every paired operand is an aligned register pair:
+//   pa = (hx0, hx1, hy0, hy1)  pb = (hz0, hz1, m0, m1)
+//   pc = (lx0, lx1, ly0, ly1)  pd = (lz0, lz1, -, -)
+// Same arithmetic per pair as k_allpairs_mixed (double-single separation, SFU
+// rsqrt, FP32 partials folded into compensated sums every FOLD j).
+template <bool GUARD>
+__global__ void __launch_bounds__(BLOCK) k_allpairs_mixed2(
+    int64_t n, int64_t nt, const int32_t* __restrict__ targets, const float4* __restrict__ phi,
+    const float4* __restrict__ plo, float eps2, double Gd, int64_t slice_len, int nslices,
+    double4* __restrict__ partial, double4* __restrict__ acc, double* __restrict__ out3, KickArgs kick) {
+    __shared__ float4 pa[BLOCK / 2], pb[BLOCK / 2], pc[BLOCK / 2], pd[BLOCK / 2];
+    const int slice = blockIdx.y;
+    const int64_t j0 = (int64_t)slice * slice_len;
+    const int64_t j1 = min(n, j0 + slice_len);
+    int64_t tt[IPT], bi[IPT];
+    float2 nhx[IPT], nhy[IPT], nhz[IPT], nlx[IPT], nly[IPT], nlz[IPT];
+    float2 ax[IPT], ay[IPT], az[IPT];
+    CompSum cx[IPT], cy[IPT], cz[IPT];
+    const float2 e2 = make_float2(eps2, eps2);
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        tt[k] = (int64_t)blockIdx.x * BLOCK * IPT + k * BLOCK + threadIdx.x;
+        bi[k] = tt[k] < nt ? (targets ? (int64_t)targets[tt[k]] : tt[k]) : 0;
+        const float4 h = phi[bi[k]], l = plo[bi[k]];
+        nhx[k] = make_float2(-h.x, -h.x); nhy[k] = make_float2(-h.y, -h.y); nhz[k] = make_float2(-h.z, -h.z);
+        nlx[k] = make_float2(-l.x, -l.x); nly[k] = make_float2(-l.y, -l.y); nlz[k] = make_float2(-l.z, -l.z);
+        ax[k] = ay[k] = az[k] = make_float2(0.f, 0.f);
+    }
+    float* fa = reinterpret_cast<float*>(pa);
+    float* fb = reinterpret_cast<float*>(pb);
+    float* fc = reinterpret_cast<float*>(pc);
+    float* fd = reinterpret_cast<float*>(pd);
+    const int q = threadIdx.x >> 1, hh = threadIdx.x & 1;
+    for (int64_t base = j0; base < j1; base += BLOCK) {
+        const int64_t j = base + threadIdx.x;
+        __syncthreads();
+        float4 h = make_float4(PAD_POS, PAD_POS, PAD_POS, 0.f), l = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j < j1) { h = phi[j]; l = plo[j]; }
+        fa[4 * q + hh] = h.x; fa[4 * q + 2 + hh] = h.y;
+        fb[4 * q + hh] = h.z; fb[4 * q + 2 + hh] = h.w;
+        fc[4 * q + hh] = l.x; fc[4 * q + 2 + hh] = l.y;
+        fd[4 * q + hh] = l.z; fd[4 * q + 2 + hh] = 0.f;
+        __syncthreads();
+#pragma unroll 1
+        for (int c0 = 0; c0 < BLOCK / 2; c0 += FOLD / 2) {
+#pragma unroll 4
+            for (int pq = c0; pq < c0 + FOLD / 2; ++pq) {
+                const float4 A = pa[pq], B = pb[pq], C = pc[pq], D = pd[pq];
+#pragma unroll
+                for (int k = 0; k < IPT; ++k) {
+                    const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(A.x, A.y), nhx[k]), __fadd2_rn(make_float2(C.x, C.y), nlx[k]));
+                    const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(A.z, A.w), nhy[k]), __fadd2_rn(make_float2(C.z, C.w), nly[k]));
+                    const float2 dz = __fadd2_rn(__fadd2_rn(make_float2(B.x, B.y), nhz[k]), __fadd2_rn(make_float2(D.x, D.y), nlz[k]));
+                    float2 r2 = __ffma2_rn(dz, dz, e2);
+                    r2 = __ffma2_rn(dy, dy, r2);
+                    r2 = __ffma2_rn(dx, dx, r2);
+                    float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                    if (GUARD) {
+                        inv.x = r2.x > 0.f ? inv.x : 0.f;
+                        inv.y = r2.y > 0.f ? inv.y : 0.f;
+                    }
+                    const float2 inv2 = __fmul2_rn(inv, inv);
+                    const float2 s = __fmul2_rn(__fmul2_rn(make_float2(B.z, B.w), inv), inv2);
+                    ax[k] = __ffma2_rn(dx, s, ax[k]);
+                    ay[k] = __ffma2_rn(dy, s, ay[k]);
+                    az[k] = __ffma2_rn(dz, s, az[k]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < IPT; ++k) {
+                cx[k].add(ax[k].x + ax[k].y); cy[k].add(ay[k].x + ay[k].y); cz[k].add(az[k].x + az[k].y);
+                ax[k] = ay[k] = az[k] = make_float2(0.f, 0.f);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < IPT; ++k)
+        if (tt[k] < nt)
+            store_result(tt[k], bi[k], cx[k].value(), cy[k].value(), cz[k].value(), Gd, nslices, slice, nt, partial,
+                         acc, out3, kick);
+}
+
 __global__ void k_reduce_slices(int64_t nt, int nslices, const double4* __restrict__ partial,
                                 const int32_t* __restrict__ targets, double G, double4* __restrict__ acc,
                                 double* __restrict__ out3, KickArgs kick) {
@@ -247,6 +331,12 @@ template <bool PN, bool GUARD>
 void launch_mixed(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32_t* tg, aster_ctx* c,
                   const aster_params* p, int64_t slice_len, int ns, double4* partial, double* out3, KickArgs kick) {
     const float inv_c2 = PN ? (float)(1.0 / (p->c * p->c)) : 0.f;
+    if (!PN) {
+        k_allpairs_mixed2<GUARD><<<grid, BLOCK, 0, st>>>(n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(),
+                                                          (float)p->eps2, p->G, slice_len, ns, partial,
+                                                          c->acc.as<double4>(), out3, kick);
+        return;
+    }
     k_allpairs_mixed<PN, GUARD><<<grid, BLOCK, 0, st>>>(
         n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), (float)p->G, (float)p->eps2,
         inv_c2, p->G, slice_len, ns, partial, c->acc.as<double4>(), out3, kick);

@@ -86,6 +86,9 @@ struct aster_ctx {
     int* err_dev = nullptr;     // device error flags
     int* err_host = nullptr;    // pinned copy
     int* stack_hw_dev = nullptr;  // tree-walk stack high-water mark
+    // usable tree-walk stack entries per warp (<= the 1024 in shared memory);
+    // ASTER_WALK_STACK_LIMIT lowers it, e.g. to exercise the overflow path
+    int walk_stack_limit = 1024;
     LbvhBufs tree;
     EnsBufs ens;
     AdjBufs adj;

@@ -6,6 +6,7 @@
 // are packed into 32-byte double4 records (x, y, z, m) and (vx, vy, vz, 0) so
 // that every body is one aligned 32-byte load.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -97,6 +98,10 @@ extern "C" int aster_ctx_create(aster_ctx** out, int device, void* stream) {
         return aster_cuda_fail(e, "aster_ctx_create", __FILE__, __LINE__);
     }
     c->stack_hw_dev = c->err_dev + 1;
+    if (const char* lim = std::getenv("ASTER_WALK_STACK_LIMIT")) {
+        const int v = std::atoi(lim);
+        if (v >= 64 && v < c->walk_stack_limit) c->walk_stack_limit = v;
+    }
     cudaMemset(c->err_dev, 0, 2 * sizeof(int));
     *out = c;
     return ASTER_OK;

@@ -466,7 +466,11 @@ __global__ void __launch_bounds__(256) k_make_groups(int64_t n, const int32_t* _
 template <bool MIXED>
 struct WalkShared {
     int stack[WALK_WARPS][WALK_STACK];
-    float4 lrel[WALK_WARPS][MIXED ? WALK_LIST : 1];    // (x, y, z) relative to the group centre, mass
+    // mixed list, two entries per slot so that each paired FP32 operand is an
+    // aligned register pair: lpa = (x0, x1, y0, y1), lpb = (z0, z1, m0, m1),
+    // positions relative to the group centre
+    float4 lpa[WALK_WARPS][MIXED ? WALK_LIST / 2 : 1];
+    float4 lpb[WALK_WARPS][MIXED ? WALK_LIST / 2 : 1];
     double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST];    // FP64 (com, mass)
 };
 
@@ -492,6 +496,30 @@ __device__ __forceinline__ void interact_f32(const float4 e, const float3 b, flo
     ax = fmaf(dx, s, ax);
     ay = fmaf(dy, s, ay);
     az = fmaf(dz, s, az);
+}
+
+// Two interactions at once with the paired FP32 instructions of sm_100
+// (add/mul/fma .f32x2): list entries (A.x|A.y, A.z|A.w, B.x|B.y) positions,
+// B.z|B.w masses; nb = -(body position) broadcast to both halves.
+template <bool GUARD>
+__device__ __forceinline__ void interact2_f32(const float4 A, const float4 B, const float2 nbx, const float2 nby,
+                                              const float2 nbz, const float2 eps2, float2& ax, float2& ay, float2& az) {
+    const float2 dx = __fadd2_rn(make_float2(A.x, A.y), nbx);
+    const float2 dy = __fadd2_rn(make_float2(A.z, A.w), nby);
+    const float2 dz = __fadd2_rn(make_float2(B.x, B.y), nbz);
+    float2 r2 = __ffma2_rn(dz, dz, eps2);
+    r2 = __ffma2_rn(dy, dy, r2);
+    r2 = __ffma2_rn(dx, dx, r2);
+    float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    if (GUARD) {
+        inv.x = r2.x > 0.f ? inv.x : 0.f;
+        inv.y = r2.y > 0.f ? inv.y : 0.f;
+    }
+    const float2 inv2 = __fmul2_rn(inv, inv);
+    const float2 sN = __fmul2_rn(__fmul2_rn(make_float2(B.z, B.w), inv), inv2);
+    ax = __ffma2_rn(dx, sN, ax);
+    ay = __ffma2_rn(dy, sN, ay);
+    az = __ffma2_rn(dz, sN, az);
 }
 
 template <bool GUARD>
@@ -526,7 +554,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
     unsigned int* __restrict__ work, const float4* __restrict__ node_hi, const float4* __restrict__ node_lo,
     const double4* __restrict__ node_cm, const int2* __restrict__ child, const int32_t* __restrict__ perm,
     double G, double eps2, double half_dt, double4* __restrict__ acc, double4* __restrict__ vel,
-    int* __restrict__ err, int* __restrict__ stack_hw, int32_t* __restrict__ body_counts,
+    int* __restrict__ err, int* __restrict__ stack_hw, int stack_limit, int32_t* __restrict__ body_counts,
     unsigned long long* __restrict__ inter_count) {
     __shared__ WalkShared<MIXED> sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -565,6 +593,9 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
         const float cgx = 0.5f * (glox + ghix), cgy = 0.5f * (gloy + ghiy), cgz = 0.5f * (gloz + ghiz);
         const float3 b0 = make_float3((h0.x - cgx) + l0.x, (h0.y - cgy) + l0.y, (h0.z - cgz) + l0.z);
         const float3 b1 = make_float3((h1.x - cgx) + l1.x, (h1.y - cgy) + l1.y, (h1.z - cgz) + l1.z);
+        const float2 nb0x = make_float2(-b0.x, -b0.x), nb0y = make_float2(-b0.y, -b0.y), nb0z = make_float2(-b0.z, -b0.z);
+        const float2 nb1x = make_float2(-b1.x, -b1.x), nb1y = make_float2(-b1.y, -b1.y), nb1z = make_float2(-b1.z, -b1.z);
+        const float2 eps2f2 = make_float2((float)eps2, (float)eps2);
         double4 c0 = make_double4(0, 0, 0, 0), c1 = c0;
         if (!MIXED) {
             c0 = node_cm[k0];
@@ -581,14 +612,19 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
 
         auto evaluate = [&](int cnt) {
             if (MIXED) {
-                float ax0 = 0.f, ay0 = 0.f, az0 = 0.f, ax1 = 0.f, ay1 = 0.f, az1 = 0.f;
-#pragma unroll 8
-                for (int e = 0; e < cnt; ++e) interact_f32<GUARD>(sm.lrel[warp][e], b0, epsf, ax0, ay0, az0);
-                sx0.add(ax0); sy0.add(ay0); sz0.add(az0);
-                if (two) {
+                // an odd cnt has its last slot half zero-padded by the caller
+                const int np = (cnt + 1) >> 1;
+                float2 ax0 = make_float2(0.f, 0.f), ay0 = ax0, az0 = ax0;
 #pragma unroll 4
-                    for (int e = sub; e < cnt; e += lps) interact_f32<GUARD>(sm.lrel[warp][e], b1, epsf, ax1, ay1, az1);
-                    sx1.add(ax1); sy1.add(ay1); sz1.add(az1);
+                for (int q = 0; q < np; ++q)
+                    interact2_f32<GUARD>(sm.lpa[warp][q], sm.lpb[warp][q], nb0x, nb0y, nb0z, eps2f2, ax0, ay0, az0);
+                sx0.add(ax0.x + ax0.y); sy0.add(ay0.x + ay0.y); sz0.add(az0.x + az0.y);
+                if (two) {
+                    float2 ax1 = make_float2(0.f, 0.f), ay1 = ax1, az1 = ax1;
+#pragma unroll 2
+                    for (int q = sub; q < np; q += lps)
+                        interact2_f32<GUARD>(sm.lpa[warp][q], sm.lpb[warp][q], nb1x, nb1y, nb1z, eps2f2, ax1, ay1, az1);
+                    sx1.add(ax1.x + ax1.y); sy1.add(ay1.x + ay1.y); sz1.add(az1.x + az1.y);
                 }
             } else {
 #pragma unroll 4
@@ -633,7 +669,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
             const uint32_t amask = __ballot_sync(0xffffffffu, accept);
             const uint32_t omask = __ballot_sync(0xffffffffu, open);
             const int nopen = __popc(omask);
-            if (top + 2 * nopen > WALK_STACK) {
+            if (top + 2 * nopen > stack_limit) {
                 overflow = true;
                 break;
             }
@@ -646,9 +682,15 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
             hw = top > hw ? top : hw;
             if (accept) {
                 const int pos = lc + __popc(amask & lt);
-                if (MIXED)
-                    sm.lrel[warp][pos] = make_float4((nh.x - cgx) + nl.x, (nh.y - cgy) + nl.y, (nh.z - cgz) + nl.z, nh.w);
-                else
+                if (MIXED) {
+                    float* A = reinterpret_cast<float*>(&sm.lpa[warp][0]);
+                    float* B = reinterpret_cast<float*>(&sm.lpb[warp][0]);
+                    const int q = pos >> 1, h = pos & 1;
+                    A[4 * q + h] = (nh.x - cgx) + nl.x;
+                    A[4 * q + 2 + h] = (nh.y - cgy) + nl.y;
+                    B[4 * q + h] = (nh.z - cgz) + nl.z;
+                    B[4 * q + 2 + h] = nh.w;
+                } else
                     sm.lcm[warp][pos] = node_cm[node];
             }
             lc += __popc(amask);
@@ -657,9 +699,14 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
                 evaluate(32);
                 __syncwarp();
                 const int rest = lc - 32;
-                if (lane < rest) {
-                    if (MIXED) sm.lrel[warp][lane] = sm.lrel[warp][32 + lane];
-                    else sm.lcm[warp][lane] = sm.lcm[warp][32 + lane];
+                if (MIXED) {
+                    if (lane < ((rest + 1) >> 1)) {  // whole slots: 32 is even
+                        const float4 a = sm.lpa[warp][16 + lane], b = sm.lpb[warp][16 + lane];
+                        sm.lpa[warp][lane] = a;
+                        sm.lpb[warp][lane] = b;
+                    }
+                } else if (lane < rest) {
+                    sm.lcm[warp][lane] = sm.lcm[warp][32 + lane];
                 }
                 lc = rest;
                 __syncwarp();
@@ -669,6 +716,13 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
             if (lane == 0) atomicOr(err, ASTER_DEVERR_STACK);
             break;
         }
+        if (MIXED && (lc & 1) && lane == 0) {  // zero mass, zero offset: contributes nothing
+            float* A = reinterpret_cast<float*>(&sm.lpa[warp][0]);
+            float* B = reinterpret_cast<float*>(&sm.lpb[warp][0]);
+            const int q = lc >> 1;
+            A[4 * q + 1] = 0.f; A[4 * q + 3] = 0.f; B[4 * q + 1] = 0.f; B[4 * q + 3] = 0.f;
+        }
+        __syncwarp();
         if (lc > 0) evaluate(lc);
         __syncwarp();
         wtotal += (unsigned long long)total * (unsigned long long)gr.y;
@@ -723,7 +777,8 @@ int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts) {
     kern<<<(unsigned)blocks, WALK_WARPS * 32, 0, c->stream>>>(
         c->n, t.groups.as<int2>(), gcount, gcount + 1, t.node_hi.as<float4>(), t.node_lo.as<float4>(),
         t.node_cm.as<double4>(), t.child.as<int2>(), t.perm.as<int32_t>(), p->G, p->eps2, 0.5 * p->dt,
-        c->acc.as<double4>(), c->vel.as<double4>(), c->err_dev, c->stack_hw_dev, counts, red_inter(c));
+        c->acc.as<double4>(), c->vel.as<double4>(), c->err_dev, c->stack_hw_dev, c->walk_stack_limit, counts,
+        red_inter(c));
     ASTER_CUDA(cudaGetLastError());
     return ASTER_OK;
 }

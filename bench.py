@@ -110,6 +110,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(ms: float, dist=None, device: str = "cpu") -> float:
+    """Largest per-rank device time of the timed region (MAX all-reduce);
+    the rank's own value when not distributed."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, steps: int, ms_max: float) -> float:
+    """Steps per second of the whole job: every rank runs `steps` steps of its
+    own replica, the job lasts as long as the slowest rank."""
+    return world * steps / (ms_max / 1e3)
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -189,6 +206,7 @@ def run_ours(args):
         if dist:
             dist.barrier()
 
+    e_start = ctx.energy(p) if not args.quick else None
     # warm-up (also primes the cached acceleration)
     ctx.kdk_steps(p, args.warmup, SOLVER_LBVH, MIXED)
     barrier()
@@ -198,13 +216,14 @@ def run_ours(args):
     st = ctx.stats()
     barrier()
     clk = clocks.stop()
-    ms = st["ms_total"]
-    if dist:
-        import torch
-        t = torch.tensor([ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1e3)
+    ms = max_over_ranks(st["ms_total"], dist, f"cuda:{device}")
+    value = whole_job_rate(world, args.steps, ms)
+    drift = None
+    if e_start is not None:
+        e_end = ctx.energy(p)
+        drift = {"steps": args.warmup + args.steps, "energy_rel": abs(e_end[0] - e_start[0]) / abs(e_start[0]),
+                 "momentum_abs": float(np.abs(e_end[1] - e_start[1]).max()),
+                 "note": "FP64 O(N^2) energy with the Plummer potential, before warm-up and after the timed steps"}
     walk_ms = st["ms_force"] / max(args.steps, 1)
     build_ms = st["ms_build"] / max(args.steps, 1)
     inter_per_step = st["interactions"] / max(args.steps, 1)
@@ -230,6 +249,7 @@ def run_ours(args):
                        "l2": "per-step working set > L2: the tree rebuild writes ~0.4 GB every step"},
             "phases_ms": {"build": build_ms, "walk": walk_ms, "other": ms / args.steps - build_ms - walk_ms},
             "interactions_per_step": inter_per_step,
+            "drift": drift,
             "walk_stack_high_water": st["max_stack"],
             "roofline": {"bound": "fp32", "kernel": "k_walk (tree walk + interactions)",
                          "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
@@ -341,6 +361,48 @@ def secondary(ctx, args):
     out["allpairs"] = res
     out["ensemble"] = ensemble_c4(ctx)
     out["adjoint"] = adjoint_c5(ctx)
+    out["c1"] = kdk_c1(ctx)
+    return out
+
+
+def kdk_c1(ctx):
+    """C1: Plummer N=4096, eps=0.01, dt=1e-3, 100 KDK all-pairs steps, FP64
+    and mixed: device time per step, energy drift, momentum."""
+    from aster_b200 import gen
+    from aster_b200.api import FP64, MIXED, SOLVER_ALLPAIRS, Params
+    pos, vel, m = gen.plummer(4096, 1001)
+    p = Params(eps2=1e-4, dt=1e-3)
+    out = {"workload": "C1 Plummer N=4096, eps=0.01, dt=1e-3, 100 KDK steps (one force evaluation per step)"}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        ctx.upload(pos, vel, m)
+        e0, _ = ctx.energy(p)
+        ctx.kdk_steps(p, 100, SOLVER_ALLPAIRS, prec)
+        ms = ctx.stats()["ms_total"]
+        e1, mom = ctx.energy(p)
+        out[name] = {"ms_per_step": ms / 100, "pairs_per_s": 100 * 4096 * 4095 / (ms / 1e3),
+                     "energy_drift": abs(e1 - e0) / abs(e0), "momentum_abs": float(np.abs(mom).max())}
+    return out
+
+
+def c3_drift(ctx, nsteps: int = 1000):
+    """C3 long run: 1000 KDK steps (dt = 1e-4) of the N = 262144 cold disk
+    with FP64 and with mixed all-pairs forces; energy drift of each."""
+    from aster_b200 import gen
+    from aster_b200.api import FP64, MIXED, SOLVER_ALLPAIRS, Params
+    pos, vel, m = gen.exponential_disk(N_C3, SEED_C3)
+    p = Params(G=1.0, eps2=EPS_C3 ** 2, dt=1e-4)
+    out = {"workload": f"C3 disk N={N_C3}, eps=0.002, dt=1e-4, {nsteps} KDK steps"}
+    finals = {}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        ctx.upload(pos, vel, m)
+        e0, _ = ctx.energy(p)
+        ctx.kdk_steps(p, nsteps, SOLVER_ALLPAIRS, prec)
+        ms = ctx.stats()["ms_total"]
+        e1, mom = ctx.energy(p)
+        finals[name] = ctx.download()[0]
+        out[name] = {"s": ms / 1e3, "energy_drift": abs(e1 - e0) / abs(e0), "momentum_abs": float(np.abs(mom).max())}
+    out["final_pos_mixed_vs_fp64_rel_l2"] = float(np.linalg.norm(finals["mixed"] - finals["fp64"]) /
+                                                  np.linalg.norm(finals["fp64"]))
     return out
 
 
@@ -403,6 +465,8 @@ def run_case(args):
             ctx.allpairs(p3, prec)
             ctx.allpairs(p3, prec)
             out[f"ms_{prec}"] = ctx.stats()["ms_force"]
+    elif args.case == "c3drift":
+        out.update(c3_drift(ctx))
     elif args.case == "ensemble":
         pos, vel, m, off = gen.hierarchical_ensemble(16384, 1004)
         p = Params(G=1.0, c=100.0, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1)
@@ -435,7 +499,7 @@ def main():
                     help="bodies in the headline workload (default 2^20; smaller only for profiling captures)")
     ap.add_argument("--walk-traffic", type=float, default=WALK_TRAFFIC_BYTES,
                     help="DRAM bytes per walk launch from an ncu capture (reported as roofline.traffic)")
-    ap.add_argument("--case", default=None, choices=["allpairs", "ensemble", "adjoint"],
+    ap.add_argument("--case", default=None, choices=["allpairs", "ensemble", "adjoint", "c3drift"],
                     help="run one secondary workload briefly (used for profiling captures) and exit")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -148,6 +148,25 @@ def test_c2_full_size_forces_sampled(ctx):
     assert err < 5e-3, err
 
 
+def test_walk_stack_overflow_is_reported(monkeypatch):
+    """Failure path without a GPU fault: a tiny usable stack (host-side limit,
+    the shared-memory stack is unchanged) makes the walk stop early and the
+    call return ASTER_ERR_STACK; the context and the GPU stay usable."""
+    from aster_b200.api import AsterError, Context
+    pos, vel, m = gen.plummer(5000, 12)
+    monkeypatch.setenv("ASTER_WALK_STACK_LIMIT", "64")
+    with Context(0) as small:
+        small.upload(pos, vel, m)
+        with pytest.raises(AsterError) as ei:
+            small.lbvh_forces(Params(eps2=1e-4, theta=0.0), MIXED)
+        assert ei.value.status == 5  # ASTER_ERR_STACK
+        assert np.isfinite(small.allpairs(Params(eps2=1e-4), FP64)).all()
+    monkeypatch.delenv("ASTER_WALK_STACK_LIMIT")
+    with Context(0) as normal:
+        normal.upload(pos, vel, m)
+        assert np.isfinite(normal.lbvh_forces(Params(eps2=1e-4, theta=0.0), MIXED)).all()
+
+
 def test_lbvh_kdk_conserves(ctx):
     pos, vel, m = gen.plummer(50000, 1002, masses="lognormal")
     ctx.upload(pos, vel, m)
