@@ -45,7 +45,7 @@ struct LbvhBufs {
     DevBuf codes, codes_alt, sorted_codes, perm, perm_alt, hist, digit_off;
     DevBuf left, right, parent, rlo, rhi, counters;
     DevBuf node_cm, bmin, bmax;  // node_cm: double4 (com x, y, z, mass)
-    DevBuf node_hi, node_lo, child, groups;
+    DevBuf node_hi, node_lo, child, groups, crec;
     int64_t n = 0;
     bool built = false;
     double box = 0.0;

@@ -42,10 +42,20 @@ constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // 2048 keys per block
 constexpr int SORT_WARPS = SORT_THREADS / 32;
 constexpr int RADIX = 256;
 constexpr int MAX_CLIMB = 160;     // bottom-up level cap (tree depth <= 97 for 63-bit codes)
-constexpr int WALK_WARPS = 4;
+#ifndef ASTER_WALK_WARPS
+#define ASTER_WALK_WARPS 4
+#endif
+#ifndef ASTER_WALK_MINBLOCKS
+#define ASTER_WALK_MINBLOCKS 8
+#endif
+#ifndef ASTER_WALK_UNROLL
+#define ASTER_WALK_UNROLL 4
+#endif
+constexpr int WALK_WARPS = ASTER_WALK_WARPS;  // warps (groups in flight) per block
+constexpr int WALK_UNROLL = ASTER_WALK_UNROLL;
 constexpr int WALK_STACK = 1024;   // nodes per warp
 constexpr int GROUP_MAX = 64;      // leaves per walk group (1 or 2 per lane)
-constexpr int WALK_LIST = 64;      // interaction-list capacity per warp
+constexpr int WALK_LIST = 96;      // interaction-list capacity per warp (31 + 64 per round)
 
 // ----------------------------------------------------------------- box
 __device__ __forceinline__ double warp_max_d(double v) {
@@ -442,6 +452,25 @@ __global__ void __launch_bounds__(256) k_node_finalize(int64_t n, double theta, 
     }
 }
 
+// Child records for the walk: for internal node i (node n+i) the traversal
+// records of its two children, contiguous: crec[4i..4i+3] =
+// (hi_left, lo_left, hi_right, lo_right), so opening a node costs one 64-byte
+// load. Written by each non-root node into its parent's slot.
+__global__ void __launch_bounds__(256) k_child_records(int64_t n, const int32_t* __restrict__ parent,
+                                                       const int2* __restrict__ child,
+                                                       const float4* __restrict__ node_hi,
+                                                       const float4* __restrict__ node_lo, float4* __restrict__ crec) {
+    const int64_t m = 2 * n - 1;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < m; v += (int64_t)gridDim.x * blockDim.x) {
+        if (v == n) continue;  // the root has no parent
+        const int32_t p = parent[v];
+        const int side = child[p].x == (int32_t)v ? 0 : 1;
+        float4* dst = crec + 4 * (int64_t)(p - n) + 2 * side;
+        dst[0] = node_hi[v];
+        dst[1] = node_lo[v];
+    }
+}
+
 // ----------------------------------------------------------------- walk
 // Groups: a node whose subtree holds at most GROUP_MAX leaves while its
 // parent's holds more (the root when n <= GROUP_MAX). Its leaves are a
@@ -471,7 +500,7 @@ struct WalkShared {
     // positions relative to the group centre
     float4 lpa[WALK_WARPS][MIXED ? WALK_LIST / 2 : 1];
     float4 lpb[WALK_WARPS][MIXED ? WALK_LIST / 2 : 1];
-    double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST];    // FP64 (com, mass)
+    double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST];  // FP64 (com, mass)
 };
 
 __device__ __forceinline__ float warp_min_f(float v) {
@@ -481,21 +510,6 @@ __device__ __forceinline__ float warp_min_f(float v) {
 __device__ __forceinline__ float warp_max_f(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
-}
-
-// Mixed-precision interaction of one body (rel. position b, compensated
-// accumulators) with list entry e: 12 FP32 operations + one SFU rsqrt.
-template <bool GUARD>
-__device__ __forceinline__ void interact_f32(const float4 e, const float3 b, float eps2, float& ax, float& ay,
-                                             float& az) {
-    const float dx = e.x - b.x, dy = e.y - b.y, dz = e.z - b.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-    float inv = rsqrt_approx(r2);
-    if (GUARD) inv = r2 > 0.f ? inv : 0.f;
-    const float s = e.w * inv * inv * inv;
-    ax = fmaf(dx, s, ax);
-    ay = fmaf(dy, s, ay);
-    az = fmaf(dz, s, az);
 }
 
 // Two interactions at once with the paired FP32 instructions of sm_100
@@ -535,33 +549,50 @@ __device__ __forceinline__ void interact_f64(const double4 e, const double4 b, d
     az = fma(dz, s, az);
 }
 
+// Opening test of one node for the whole group, FP32 round-to-nearest without
+// FMA (the CPU restatement reproduces it bit for bit): accept when the squared
+// distance from the node's FP32 centre of mass to the group box exceeds rcrit2.
+__device__ __forceinline__ bool group_accepts(const float4 nh, float rcrit2, float glox, float gloy, float gloz,
+                                              float ghix, float ghiy, float ghiz) {
+    const float ux = __fsub_rn(glox, nh.x), wx = __fsub_rn(nh.x, ghix);
+    const float uy = __fsub_rn(gloy, nh.y), wy = __fsub_rn(nh.y, ghiy);
+    const float uz = __fsub_rn(gloz, nh.z), wz = __fsub_rn(nh.z, ghiz);
+    float tx = ux > wx ? ux : wx, ty = uy > wy ? uy : wy, tz = uz > wz ? uz : wz;
+    tx = tx > 0.f ? tx : 0.f;
+    ty = ty > 0.f ? ty : 0.f;
+    tz = tz > 0.f ? tz : 0.f;
+    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), __fmul_rn(ty, ty)), __fmul_rn(tz, tz));
+    return d2 > rcrit2;
+}
+
 // Persistent walk: each warp takes groups from a global work counter until
 // none are left. Per group: lane l holds sorted leaf l of the group; the r
 // leaves beyond 32 are each shared by 32/r (rounded down to a power of two)
 // lanes that split the interaction list between them, so groups of 33..64
-// bodies keep every lane busy. The warp pops up to 32 nodes per round from its
-// shared stack, each lane loads its node's record (centre of mass, mass,
-// opening radius, children: independent loads, one latency), decides
-// open/accept, children of opened nodes are pushed, accepted nodes appended to
-// the shared list, which is evaluated 32 entries at a time by every lane.
+// bodies keep every lane busy. The warp pops up to 32 opened internal nodes
+// per round from its shared stack; each lane loads the contiguous record of
+// its node's two children (centres of mass, masses, opening radii: one
+// 64-byte load, issued together with the child indices) and tests both:
+// leaves and accepted cells go to the shared interaction list, opened
+// internal children to the stack. The list is evaluated 32 entries at a
+// time by every lane.
 // Mixed precision: list entries and bodies are stored relative to the group
 // centre cg (FP32 of hi - cg plus the double-single low part), so an
 // interaction needs one subtraction per axis; the group is compact, so the
 // relative coordinates keep FP32 precision of the separation.
 template <bool MIXED, bool GUARD, bool KICK>
-__global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
+__global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS : 6) k_walk(
     int64_t n, const int2* __restrict__ groups, const unsigned int* __restrict__ ngroups_p,
     unsigned int* __restrict__ work, const float4* __restrict__ node_hi, const float4* __restrict__ node_lo,
-    const double4* __restrict__ node_cm, const int2* __restrict__ child, const int32_t* __restrict__ perm,
-    double G, double eps2, double half_dt, double4* __restrict__ acc, double4* __restrict__ vel,
-    int* __restrict__ err, int* __restrict__ stack_hw, int stack_limit, int32_t* __restrict__ body_counts,
-    unsigned long long* __restrict__ inter_count) {
+    const float4* __restrict__ crec, const double4* __restrict__ node_cm, const int2* __restrict__ child,
+    const int32_t* __restrict__ perm, double G, double eps2, double half_dt, double4* __restrict__ acc,
+    double4* __restrict__ vel, int* __restrict__ err, int* __restrict__ stack_hw, int stack_limit,
+    int32_t* __restrict__ body_counts, unsigned long long* __restrict__ inter_count) {
     __shared__ WalkShared<MIXED> sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     const unsigned int ngroups = *ngroups_p;
     int* stack = sm.stack[warp];
-    const float epsf = (float)eps2;
     int hw = 1;
     unsigned long long wtotal = 0;
 
@@ -604,18 +635,31 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
 
         CompSum sx0, sy0, sz0, sx1, sy1, sz1;
         double dx0 = 0, dy0 = 0, dz0 = 0, dx1 = 0, dy1 = 0, dz1 = 0;
-        int top = 1, lc = 0;
+        int top = 0, lc = 0;
         int total = 0;
-        if (lane == 0) stack[0] = n >= 2 ? (int)n : 0;
-        __syncwarp();
         bool overflow = false;
+
+        // append list entry `pos` (lane-private): node record (hi, lo) or FP64 record
+        auto append = [&](int pos, const float4 nh, const float4 nl, int node) {
+            if (MIXED) {
+                float* A = reinterpret_cast<float*>(&sm.lpa[warp][0]);
+                float* B = reinterpret_cast<float*>(&sm.lpb[warp][0]);
+                const int q = pos >> 1, h = pos & 1;
+                A[4 * q + h] = (nh.x - cgx) + nl.x;
+                A[4 * q + 2 + h] = (nh.y - cgy) + nl.y;
+                B[4 * q + h] = (nh.z - cgz) + nl.z;
+                B[4 * q + 2 + h] = nh.w;
+            } else {
+                sm.lcm[warp][pos] = node_cm[node];
+            }
+        };
 
         auto evaluate = [&](int cnt) {
             if (MIXED) {
                 // an odd cnt has its last slot half zero-padded by the caller
                 const int np = (cnt + 1) >> 1;
                 float2 ax0 = make_float2(0.f, 0.f), ay0 = ax0, az0 = ax0;
-#pragma unroll 4
+#pragma unroll WALK_UNROLL
                 for (int q = 0; q < np; ++q)
                     interact2_f32<GUARD>(sm.lpa[warp][q], sm.lpb[warp][q], nb0x, nb0y, nb0z, eps2f2, ax0, ay0, az0);
                 sx0.add(ax0.x + ax0.y); sy0.add(ay0.x + ay0.y); sz0.add(az0.x + az0.y);
@@ -637,76 +681,73 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
             total += cnt;
         };
 
+        if (n >= 2) {
+            if (lane == 0) stack[0] = (int)n;  // the root is internal: start by opening it
+            top = 1;
+        } else {
+            if (lane == 0) append(0, node_hi[0], node_lo[0], 0);  // a single body: its own leaf
+            lc = 1;
+        }
+        __syncwarp();
+
         while (top > 0) {
             const int cnt = top < 32 ? top : 32;
-            int node = 0;
-            if (lane < cnt) node = stack[top - 1 - lane];
+            int v = (int)n;
+            if (lane < cnt) v = stack[top - 1 - lane];
             __syncwarp();
             top -= cnt;
-            bool accept = false, open = false;
-            float4 nh = make_float4(0, 0, 0, 0), nl = make_float4(0, 0, 0, 0);
+            bool aL = false, aR = false, oL = false, oR = false;
+            float4 hL = make_float4(0, 0, 0, 0), lL = hL, hR = hL, lR = hL;
             int2 ch = make_int2(0, 0);
             if (lane < cnt) {
-                nh = node_hi[node];
-                nl = node_lo[node];
-                if (node >= n) ch = child[node];
-                if (node < n) {
-                    accept = true;
-                } else {
-                    // FP32, round-to-nearest, no FMA (matches the CPU restatement)
-                    float ux = __fsub_rn(glox, nh.x), wx = __fsub_rn(nh.x, ghix);
-                    float uy = __fsub_rn(gloy, nh.y), wy = __fsub_rn(nh.y, ghiy);
-                    float uz = __fsub_rn(gloz, nh.z), wz = __fsub_rn(nh.z, ghiz);
-                    float tx = ux > wx ? ux : wx, ty = uy > wy ? uy : wy, tz = uz > wz ? uz : wz;
-                    tx = tx > 0.f ? tx : 0.f;
-                    ty = ty > 0.f ? ty : 0.f;
-                    tz = tz > 0.f ? tz : 0.f;
-                    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), __fmul_rn(ty, ty)), __fmul_rn(tz, tz));
-                    accept = d2 > nl.w;
-                    open = !accept;
-                }
+                const float4* rec = crec + 4 * (int64_t)(v - n);
+                hL = rec[0]; lL = rec[1]; hR = rec[2]; lR = rec[3];
+                ch = child[v];
+                const bool leafL = ch.x < n, leafR = ch.y < n;
+                aL = leafL || group_accepts(hL, lL.w, glox, gloy, gloz, ghix, ghiy, ghiz);
+                aR = leafR || group_accepts(hR, lR.w, glox, gloy, gloz, ghix, ghiy, ghiz);
+                oL = !aL;
+                oR = !aR;
             }
-            const uint32_t amask = __ballot_sync(0xffffffffu, accept);
-            const uint32_t omask = __ballot_sync(0xffffffffu, open);
-            const int nopen = __popc(omask);
-            if (top + 2 * nopen > stack_limit) {
+            const uint32_t mAL = __ballot_sync(0xffffffffu, aL), mAR = __ballot_sync(0xffffffffu, aR);
+            const uint32_t mOL = __ballot_sync(0xffffffffu, oL), mOR = __ballot_sync(0xffffffffu, oR);
+            const int npush = __popc(mOL) + __popc(mOR);
+            if (top + npush > stack_limit) {
                 overflow = true;
                 break;
             }
-            if (open) {
-                const int pos = top + 2 * __popc(omask & lt);
-                stack[pos] = ch.y;
-                stack[pos + 1] = ch.x;
+            {
+                const int pos = top + __popc(mOL & lt) + __popc(mOR & lt);
+                if (oL) stack[pos] = ch.x;
+                if (oR) stack[pos + (oL ? 1 : 0)] = ch.y;
             }
-            top += 2 * nopen;
+            top += npush;
             hw = top > hw ? top : hw;
-            if (accept) {
-                const int pos = lc + __popc(amask & lt);
-                if (MIXED) {
-                    float* A = reinterpret_cast<float*>(&sm.lpa[warp][0]);
-                    float* B = reinterpret_cast<float*>(&sm.lpb[warp][0]);
-                    const int q = pos >> 1, h = pos & 1;
-                    A[4 * q + h] = (nh.x - cgx) + nl.x;
-                    A[4 * q + 2 + h] = (nh.y - cgy) + nl.y;
-                    B[4 * q + h] = (nh.z - cgz) + nl.z;
-                    B[4 * q + 2 + h] = nh.w;
-                } else
-                    sm.lcm[warp][pos] = node_cm[node];
+            {
+                const int pos = lc + __popc(mAL & lt) + __popc(mAR & lt);
+                if (aL) append(pos, hL, lL, ch.x);
+                if (aR) append(pos + (aL ? 1 : 0), hR, lR, ch.y);
             }
-            lc += __popc(amask);
+            lc += __popc(mAL) + __popc(mAR);
             __syncwarp();
-            if (lc >= 32) {
+            while (lc >= 32) {
                 evaluate(32);
                 __syncwarp();
                 const int rest = lc - 32;
-                if (MIXED) {
-                    if (lane < ((rest + 1) >> 1)) {  // whole slots: 32 is even
-                        const float4 a = sm.lpa[warp][16 + lane], b = sm.lpb[warp][16 + lane];
-                        sm.lpa[warp][lane] = a;
-                        sm.lpb[warp][lane] = b;
-                    }
-                } else if (lane < rest) {
-                    sm.lcm[warp][lane] = sm.lcm[warp][32 + lane];
+                if (MIXED) {  // whole slots (32 is even); read all, then write
+                    const int ns = (rest + 1) >> 1;
+                    float4 a = make_float4(0, 0, 0, 0), b = a;
+                    if (lane < ns) { a = sm.lpa[warp][16 + lane]; b = sm.lpb[warp][16 + lane]; }
+                    __syncwarp();
+                    if (lane < ns) { sm.lpa[warp][lane] = a; sm.lpb[warp][lane] = b; }
+                } else {
+                    const bool m0 = lane < rest, m1 = lane + 32 < rest;
+                    double4 x0 = make_double4(0, 0, 0, 0), x1 = x0;
+                    if (m0) x0 = sm.lcm[warp][32 + lane];
+                    if (m1) x1 = sm.lcm[warp][64 + lane];
+                    __syncwarp();
+                    if (m0) sm.lcm[warp][lane] = x0;
+                    if (m1) sm.lcm[warp][32 + lane] = x1;
                 }
                 lc = rest;
                 __syncwarp();
@@ -751,9 +792,9 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? 8 : 6) k_walk(
             acc[b] = make_double4(ax, ay, az, 0.0);
             if (body_counts) body_counts[b] = total;
             if (KICK) {
-                double4 v = vel[b];
-                v.x += ax * half_dt; v.y += ay * half_dt; v.z += az * half_dt;
-                vel[b] = v;
+                double4 vv = vel[b];
+                vv.x += ax * half_dt; vv.y += ay * half_dt; vv.z += az * half_dt;
+                vel[b] = vv;
             }
         }
     }
@@ -776,7 +817,7 @@ int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts) {
     unsigned int* gcount = red_groups(c);
     kern<<<(unsigned)blocks, WALK_WARPS * 32, 0, c->stream>>>(
         c->n, t.groups.as<int2>(), gcount, gcount + 1, t.node_hi.as<float4>(), t.node_lo.as<float4>(),
-        t.node_cm.as<double4>(), t.child.as<int2>(), t.perm.as<int32_t>(), p->G, p->eps2, 0.5 * p->dt,
+        t.crec.as<float4>(), t.node_cm.as<double4>(), t.child.as<int2>(), t.perm.as<int32_t>(), p->G, p->eps2, 0.5 * p->dt,
         c->acc.as<double4>(), c->vel.as<double4>(), c->err_dev, c->stack_hw_dev, c->walk_stack_limit, counts,
         red_inter(c));
     ASTER_CUDA(cudaGetLastError());
@@ -857,6 +898,12 @@ int run_build(aster_ctx* c, const aster_params* p) {
     k_node_finalize<<<grid, 256, 0, c->stream>>>(n, p->theta, t.node_cm.as<double4>(), t.bmin.as<float4>(),
                                                  t.bmax.as<float4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>());
     ASTER_CUDA(cudaGetLastError());
+    if (n >= 2) {
+        k_child_records<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.child.as<int2>(),
+                                                     t.node_hi.as<float4>(), t.node_lo.as<float4>(),
+                                                     t.crec.as<float4>());
+        ASTER_CUDA(cudaGetLastError());
+    }
     unsigned int* gcount = red_groups(c);
     ASTER_CUDA(cudaMemsetAsync(gcount, 0, 2 * sizeof(unsigned int), c->stream));
     k_make_groups<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(),
@@ -890,6 +937,7 @@ int ensure_tree(aster_ctx* c) {
     ASTER_TRY(t.node_lo.ensure((size_t)m * sizeof(float4)));
     ASTER_TRY(t.child.ensure((size_t)m * sizeof(int2)));
     ASTER_TRY(t.groups.ensure((size_t)n * sizeof(int2)));
+    ASTER_TRY(t.crec.ensure((size_t)4 * n * sizeof(float4)));
     ASTER_TRY(c->red.ensure(4096));
     t.n = n;
     return ASTER_OK;
