@@ -46,7 +46,7 @@ constexpr int MAX_CLIMB = 160;     // bottom-up level cap (tree depth <= 97 for 
 #define ASTER_WALK_WARPS 4
 #endif
 #ifndef ASTER_WALK_MINBLOCKS
-#define ASTER_WALK_MINBLOCKS 8
+#define ASTER_WALK_MINBLOCKS 6
 #endif
 #ifndef ASTER_WALK_UNROLL
 #define ASTER_WALK_UNROLL 4
@@ -55,7 +55,11 @@ constexpr int WALK_WARPS = ASTER_WALK_WARPS;  // warps (groups in flight) per bl
 constexpr int WALK_UNROLL = ASTER_WALK_UNROLL;
 constexpr int WALK_STACK = 1024;   // nodes per warp
 constexpr int GROUP_MAX = 64;      // leaves per walk group (1 or 2 per lane)
-constexpr int WALK_LIST = 96;      // interaction-list capacity per warp (31 + 64 per round)
+// Interaction list: evaluated (and its FP32 partial sums folded into the
+// compensated accumulators) every WALK_FLUSH entries; capacity = flush - 1 +
+// the 64 entries one round can append.
+constexpr int WALK_FLUSH_MIXED = 64, WALK_FLUSH_FP64 = 32;
+constexpr int WALK_LIST_MIXED = 128, WALK_LIST_FP64 = 96;
 
 // ----------------------------------------------------------------- box
 __device__ __forceinline__ double warp_max_d(double v) {
@@ -456,18 +460,21 @@ __global__ void __launch_bounds__(256) k_node_finalize(int64_t n, double theta, 
 // records of its two children, contiguous: crec[4i..4i+3] =
 // (hi_left, lo_left, hi_right, lo_right), so opening a node costs one 64-byte
 // load. Written by each non-root node into its parent's slot.
-__global__ void __launch_bounds__(256) k_child_records(int64_t n, const int32_t* __restrict__ parent,
-                                                       const int2* __restrict__ child,
+__global__ void __launch_bounds__(256) k_child_records(int64_t n, const int2* __restrict__ child,
                                                        const float4* __restrict__ node_hi,
                                                        const float4* __restrict__ node_lo, float4* __restrict__ crec) {
-    const int64_t m = 2 * n - 1;
-    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < m; v += (int64_t)gridDim.x * blockDim.x) {
-        if (v == n) continue;  // the root has no parent
-        const int32_t p = parent[v];
-        const int side = child[p].x == (int32_t)v ? 0 : 1;
-        float4* dst = crec + 4 * (int64_t)(p - n) + 2 * side;
-        dst[0] = node_hi[v];
-        dst[1] = node_lo[v];
+    // One 64-byte record per internal node holding both children, each field
+    // as a (left, right) pair so that the walk's paired FP32 opening test and
+    // list-entry arithmetic read aligned register pairs:
+    // (xL xR yL yR) (zL zR mL mR) (lxL lxR lyL lyR) (lzL lzR rcrit2L rcrit2R).
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n - 1; i += (int64_t)gridDim.x * blockDim.x) {
+        const int2 ch = child[n + i];
+        const float4 hL = node_hi[ch.x], lL = node_lo[ch.x], hR = node_hi[ch.y], lR = node_lo[ch.y];
+        float4* dst = crec + 4 * i;
+        dst[0] = make_float4(hL.x, hR.x, hL.y, hR.y);
+        dst[1] = make_float4(hL.z, hR.z, hL.w, hR.w);
+        dst[2] = make_float4(lL.x, lR.x, lL.y, lR.y);
+        dst[3] = make_float4(lL.z, lR.z, lL.w, lR.w);
     }
 }
 
@@ -498,9 +505,9 @@ struct WalkShared {
     // mixed list, two entries per slot so that each paired FP32 operand is an
     // aligned register pair: lpa = (x0, x1, y0, y1), lpb = (z0, z1, m0, m1),
     // positions relative to the group centre
-    float4 lpa[WALK_WARPS][MIXED ? WALK_LIST / 2 : 1];
-    float4 lpb[WALK_WARPS][MIXED ? WALK_LIST / 2 : 1];
-    double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST];  // FP64 (com, mass)
+    float4 lpa[WALK_WARPS][MIXED ? WALK_LIST_MIXED / 2 : 1];
+    float4 lpb[WALK_WARPS][MIXED ? WALK_LIST_MIXED / 2 : 1];
+    double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST_FP64];  // FP64 (com, mass)
 };
 
 __device__ __forceinline__ float warp_min_f(float v) {
@@ -549,20 +556,30 @@ __device__ __forceinline__ void interact_f64(const double4 e, const double4 b, d
     az = fma(dz, s, az);
 }
 
-// Opening test of one node for the whole group, FP32 round-to-nearest without
-// FMA (the CPU restatement reproduces it bit for bit): accept when the squared
-// distance from the node's FP32 centre of mass to the group box exceeds rcrit2.
-__device__ __forceinline__ bool group_accepts(const float4 nh, float rcrit2, float glox, float gloy, float gloz,
-                                              float ghix, float ghiy, float ghiz) {
-    const float ux = __fsub_rn(glox, nh.x), wx = __fsub_rn(nh.x, ghix);
-    const float uy = __fsub_rn(gloy, nh.y), wy = __fsub_rn(nh.y, ghiy);
-    const float uz = __fsub_rn(gloz, nh.z), wz = __fsub_rn(nh.z, ghiz);
-    float tx = ux > wx ? ux : wx, ty = uy > wy ? uy : wy, tz = uz > wz ? uz : wz;
-    tx = tx > 0.f ? tx : 0.f;
-    ty = ty > 0.f ? ty : 0.f;
-    tz = tz > 0.f ? tz : 0.f;
-    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), __fmul_rn(ty, ty)), __fmul_rn(tz, tz));
-    return d2 > rcrit2;
+__device__ __forceinline__ float max3_f32(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// Opening test of both children of a node for the whole group, FP32
+// round-to-nearest without FMA (the CPU restatement reproduces it bit for
+// bit), the two children in the halves of paired FP32 operations: the squared
+// distance from a child's FP32 centre of mass to the group box is
+// sum over axes of max(lo - c, c - hi, 0)^2; the child is accepted when it
+// exceeds the child's r_crit^2. lo - c is formed as fma(c, -1, lo), which is
+// the correctly rounded difference; nhi = -hi.
+__device__ __forceinline__ float2 box_dist2_pair(const float2 cx, const float2 cy, const float2 cz, const float2 lox,
+                                                 const float2 loy, const float2 loz, const float2 nhix,
+                                                 const float2 nhiy, const float2 nhiz) {
+    const float2 m1 = make_float2(-1.f, -1.f);
+    const float2 ux = __ffma2_rn(cx, m1, lox), wx = __fadd2_rn(cx, nhix);
+    const float2 uy = __ffma2_rn(cy, m1, loy), wy = __fadd2_rn(cy, nhiy);
+    const float2 uz = __ffma2_rn(cz, m1, loz), wz = __fadd2_rn(cz, nhiz);
+    const float2 tx = make_float2(max3_f32(ux.x, wx.x, 0.f), max3_f32(ux.y, wx.y, 0.f));
+    const float2 ty = make_float2(max3_f32(uy.x, wy.x, 0.f), max3_f32(uy.y, wy.y, 0.f));
+    const float2 tz = make_float2(max3_f32(uz.x, wz.x, 0.f), max3_f32(uz.y, wz.y, 0.f));
+    return __fadd2_rn(__fadd2_rn(__fmul2_rn(tx, tx), __fmul2_rn(ty, ty)), __fmul2_rn(tz, tz));
 }
 
 // Persistent walk: each warp takes groups from a global work counter until
@@ -639,19 +656,15 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
         int total = 0;
         bool overflow = false;
 
-        // append list entry `pos` (lane-private): node record (hi, lo) or FP64 record
-        auto append = [&](int pos, const float4 nh, const float4 nl, int node) {
-            if (MIXED) {
-                float* A = reinterpret_cast<float*>(&sm.lpa[warp][0]);
-                float* B = reinterpret_cast<float*>(&sm.lpb[warp][0]);
-                const int q = pos >> 1, h = pos & 1;
-                A[4 * q + h] = (nh.x - cgx) + nl.x;
-                A[4 * q + 2 + h] = (nh.y - cgy) + nl.y;
-                B[4 * q + h] = (nh.z - cgz) + nl.z;
-                B[4 * q + 2 + h] = nh.w;
-            } else {
-                sm.lcm[warp][pos] = node_cm[node];
-            }
+        // store list entry `pos` (lane-private): mixed = group-relative position and mass
+        auto put = [&](int pos, float x, float y, float z, float mass) {
+            float* A = reinterpret_cast<float*>(&sm.lpa[warp][0]);
+            float* B = reinterpret_cast<float*>(&sm.lpb[warp][0]);
+            const int o = ((pos >> 1) << 2) | (pos & 1);
+            A[o] = x;
+            A[o + 2] = y;
+            B[o] = z;
+            B[o + 2] = mass;
         };
 
         auto evaluate = [&](int cnt) {
@@ -659,6 +672,19 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
                 // an odd cnt has its last slot half zero-padded by the caller
                 const int np = (cnt + 1) >> 1;
                 float2 ax0 = make_float2(0.f, 0.f), ay0 = ax0, az0 = ax0;
+                if (two && lps == 1) {  // 49..64 bodies: both bodies of a lane share each list load
+                    float2 ax1 = make_float2(0.f, 0.f), ay1 = ax1, az1 = ax1;
+#pragma unroll 2
+                    for (int q = 0; q < np; ++q) {
+                        const float4 A = sm.lpa[warp][q], B = sm.lpb[warp][q];
+                        interact2_f32<GUARD>(A, B, nb0x, nb0y, nb0z, eps2f2, ax0, ay0, az0);
+                        interact2_f32<GUARD>(A, B, nb1x, nb1y, nb1z, eps2f2, ax1, ay1, az1);
+                    }
+                    sx0.add(ax0.x + ax0.y); sy0.add(ay0.x + ay0.y); sz0.add(az0.x + az0.y);
+                    sx1.add(ax1.x + ax1.y); sy1.add(ay1.x + ay1.y); sz1.add(az1.x + az1.y);
+                    total += cnt;
+                    return;
+                }
 #pragma unroll WALK_UNROLL
                 for (int q = 0; q < np; ++q)
                     interact2_f32<GUARD>(sm.lpa[warp][q], sm.lpb[warp][q], nb0x, nb0y, nb0z, eps2f2, ax0, ay0, az0);
@@ -681,34 +707,42 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
             total += cnt;
         };
 
+        const int nI = (int)n;  // node ids are int32: leaves < nI <= internal nodes
         if (n >= 2) {
-            if (lane == 0) stack[0] = (int)n;  // the root is internal: start by opening it
+            if (lane == 0) stack[0] = nI;  // the root is internal: start by opening it
             top = 1;
         } else {
-            if (lane == 0) append(0, node_hi[0], node_lo[0], 0);  // a single body: its own leaf
+            if (lane == 0) {  // a single body: its own leaf
+                if (MIXED) {
+                    const float4 h = node_hi[0], l = node_lo[0];
+                    put(0, (h.x - cgx) + l.x, (h.y - cgy) + l.y, (h.z - cgz) + l.z, h.w);
+                } else {
+                    sm.lcm[warp][0] = node_cm[0];
+                }
+            }
             lc = 1;
         }
         __syncwarp();
+        const float2 lox2 = make_float2(glox, glox), loy2 = make_float2(gloy, gloy), loz2 = make_float2(gloz, gloz);
+        const float2 nhix2 = make_float2(-ghix, -ghix), nhiy2 = make_float2(-ghiy, -ghiy),
+                     nhiz2 = make_float2(-ghiz, -ghiz);
+        const float2 ncgx2 = make_float2(-cgx, -cgx), ncgy2 = make_float2(-cgy, -cgy), ncgz2 = make_float2(-cgz, -cgz);
 
         while (top > 0) {
             const int cnt = top < 32 ? top : 32;
-            int v = (int)n;
-            if (lane < cnt) v = stack[top - 1 - lane];
+            const bool act = lane < cnt;
+            // inactive lanes read the root's record (valid memory) and are masked off
+            int v = nI;
+            if (act) v = stack[top - 1 - lane];
             __syncwarp();
             top -= cnt;
-            bool aL = false, aR = false, oL = false, oR = false;
-            float4 hL = make_float4(0, 0, 0, 0), lL = hL, hR = hL, lR = hL;
-            int2 ch = make_int2(0, 0);
-            if (lane < cnt) {
-                const float4* rec = crec + 4 * (int64_t)(v - n);
-                hL = rec[0]; lL = rec[1]; hR = rec[2]; lR = rec[3];
-                ch = child[v];
-                const bool leafL = ch.x < n, leafR = ch.y < n;
-                aL = leafL || group_accepts(hL, lL.w, glox, gloy, gloz, ghix, ghiy, ghiz);
-                aR = leafR || group_accepts(hR, lR.w, glox, gloy, gloz, ghix, ghiy, ghiz);
-                oL = !aL;
-                oR = !aR;
-            }
+            const float4* rec = crec + 4 * (int64_t)(v - nI);
+            const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3];
+            const int2 ch = child[v];
+            const float2 cx = make_float2(r0.x, r0.y), cy = make_float2(r0.z, r0.w), cz = make_float2(r1.x, r1.y);
+            const float2 d2 = box_dist2_pair(cx, cy, cz, lox2, loy2, loz2, nhix2, nhiy2, nhiz2);
+            const bool fL = ch.x < nI || d2.x > r3.z, fR = ch.y < nI || d2.y > r3.w;  // leaf or far enough
+            const bool aL = act && fL, aR = act && fR, oL = act && !fL, oR = act && !fR;
             const uint32_t mAL = __ballot_sync(0xffffffffu, aL), mAR = __ballot_sync(0xffffffffu, aR);
             const uint32_t mOL = __ballot_sync(0xffffffffu, oL), mOR = __ballot_sync(0xffffffffu, oR);
             const int npush = __popc(mOL) + __popc(mOR);
@@ -725,19 +759,29 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
             hw = top > hw ? top : hw;
             {
                 const int pos = lc + __popc(mAL & lt) + __popc(mAR & lt);
-                if (aL) append(pos, hL, lL, ch.x);
-                if (aR) append(pos + (aL ? 1 : 0), hR, lR, ch.y);
+                if (MIXED) {
+                    // both children's group-relative positions: (c - cg) + remainder
+                    const float2 ex = __fadd2_rn(__fadd2_rn(cx, ncgx2), make_float2(r2.x, r2.y));
+                    const float2 ey = __fadd2_rn(__fadd2_rn(cy, ncgy2), make_float2(r2.z, r2.w));
+                    const float2 ez = __fadd2_rn(__fadd2_rn(cz, ncgz2), make_float2(r3.x, r3.y));
+                    if (aL) put(pos, ex.x, ey.x, ez.x, r1.z);
+                    if (aR) put(pos + (aL ? 1 : 0), ex.y, ey.y, ez.y, r1.w);
+                } else {
+                    if (aL) sm.lcm[warp][pos] = node_cm[ch.x];
+                    if (aR) sm.lcm[warp][pos + (aL ? 1 : 0)] = node_cm[ch.y];
+                }
             }
             lc += __popc(mAL) + __popc(mAR);
             __syncwarp();
-            while (lc >= 32) {
-                evaluate(32);
+            constexpr int FL = MIXED ? WALK_FLUSH_MIXED : WALK_FLUSH_FP64;
+            while (lc >= FL) {
+                evaluate(FL);
                 __syncwarp();
-                const int rest = lc - 32;
-                if (MIXED) {  // whole slots (32 is even); read all, then write
+                const int rest = lc - FL;  // < 64
+                if (MIXED) {  // whole slots (FL is even), at most 32; read all, then write
                     const int ns = (rest + 1) >> 1;
                     float4 a = make_float4(0, 0, 0, 0), b = a;
-                    if (lane < ns) { a = sm.lpa[warp][16 + lane]; b = sm.lpb[warp][16 + lane]; }
+                    if (lane < ns) { a = sm.lpa[warp][FL / 2 + lane]; b = sm.lpb[warp][FL / 2 + lane]; }
                     __syncwarp();
                     if (lane < ns) { sm.lpa[warp][lane] = a; sm.lpb[warp][lane] = b; }
                 } else {
@@ -899,9 +943,8 @@ int run_build(aster_ctx* c, const aster_params* p) {
                                                  t.bmax.as<float4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>());
     ASTER_CUDA(cudaGetLastError());
     if (n >= 2) {
-        k_child_records<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.child.as<int2>(),
-                                                     t.node_hi.as<float4>(), t.node_lo.as<float4>(),
-                                                     t.crec.as<float4>());
+        k_child_records<<<grid, 256, 0, c->stream>>>(n, t.child.as<int2>(), t.node_hi.as<float4>(),
+                                                     t.node_lo.as<float4>(), t.crec.as<float4>());
         ASTER_CUDA(cudaGetLastError());
     }
     unsigned int* gcount = red_groups(c);
