@@ -43,9 +43,9 @@ struct DevBuf {
 // LBVH device arrays (sized for n bodies, 2n-1 nodes).
 struct LbvhBufs {
     DevBuf codes, codes_alt, sorted_codes, perm, perm_alt, hist, digit_off;
-    DevBuf left, right, parent, rlo, rhi, counters;
+    DevBuf left, right, parent, sib, rlo, rhi, counters;
     DevBuf node_cm, bmin, bmax;  // node_cm: double4 (com x, y, z, mass)
-    DevBuf node_hi, node_lo, child, groups, crec;
+    DevBuf node_hi, node_lo, child, groups, crec, front;
     int64_t n = 0;
     bool built = false;
     double box = 0.0;
@@ -100,7 +100,7 @@ struct aster_ctx {
 inline unsigned long long* red_box(aster_ctx* c) { return c->red.as<unsigned long long>(); }         // byte 0
 inline double* red_energy(aster_ctx* c) { return c->red.as<double>() + 8; }                         // byte 64
 inline unsigned long long* red_inter(aster_ctx* c) { return c->red.as<unsigned long long>() + 64; } // byte 512
-inline unsigned int* red_groups(aster_ctx* c) {  // [0] group count, [1] walk work counter
+inline unsigned int* red_groups(aster_ctx* c) {  // [0] group count, [1] walk work counter, [2] bottom-up frontier
     return reinterpret_cast<unsigned int*>(c->red.as<char>() + 1024);
 }
 

@@ -46,7 +46,7 @@ constexpr int MAX_CLIMB = 160;     // bottom-up level cap (tree depth <= 97 for 
 #define ASTER_WALK_WARPS 4
 #endif
 #ifndef ASTER_WALK_MINBLOCKS
-#define ASTER_WALK_MINBLOCKS 6
+#define ASTER_WALK_MINBLOCKS 5
 #endif
 #ifndef ASTER_WALK_UNROLL
 #define ASTER_WALK_UNROLL 4
@@ -311,7 +311,7 @@ template <class KeyT, bool COMPAT>
 __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restrict__ codes, const int32_t* __restrict__ perm,
                                                 const double4* __restrict__ pm, int32_t* __restrict__ left,
                                                 int32_t* __restrict__ right, int32_t* __restrict__ parent,
-                                                int32_t* __restrict__ rlo, int32_t* __restrict__ rhi,
+                                                int32_t* __restrict__ sib, int32_t* __restrict__ rlo, int32_t* __restrict__ rhi,
                                                 int2* __restrict__ child, uint32_t* __restrict__ counters,
                                                 double4* __restrict__ node_cm, float4* __restrict__ bmin,
                                                 float4* __restrict__ bmax, float4* __restrict__ node_hi,
@@ -369,6 +369,8 @@ __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restric
         child[node] = make_int2(L, R);
         parent[L] = (int32_t)node;
         parent[R] = (int32_t)node;
+        sib[L] = R;   // >= 0: the node is a left child
+        sib[R] = ~L;  // <  0: a right child, sibling ~sib
         rlo[node] = (int32_t)lo;
         rhi[node] = (int32_t)hi;
         counters[i] = 0u;
@@ -383,43 +385,154 @@ __device__ __forceinline__ double4 ld_cg(const double4* p) {
 }
 __device__ __forceinline__ float4 ld_cg(const float4* p) { return __ldcg(p); }
 
-__global__ void __launch_bounds__(256) k_bottom_up(int64_t n, const int32_t* __restrict__ parent,
-                                                   const int2* __restrict__ child, uint32_t* __restrict__ counters,
-                                                   double4* __restrict__ node_cm, float4* __restrict__ bmin,
-                                                   float4* __restrict__ bmax, int* __restrict__ err) {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        int64_t cur = k;
-        int level = 0;
-        for (;;) {
+// Bottom-up merge: every leaf climbs towards the root; at each internal node
+// the first arrival stops and the second merges the two children in
+// NodesArray::unite order. Two phases, so that the climbs through global
+// memory are short and all in flight at once:
+//  1. k_bottom_up_local: a block owns BU_LEAVES consecutive sorted leaves and
+//     completes every node whose leaf range lies inside them, with arrival
+//     counters and node data in shared memory (block-scope fences). A node
+//     whose parent's range leaves the block is a frontier node.
+//  2. k_bottom_up_front: one climb per frontier node through the remaining
+//     (boundary-crossing) nodes with global counters and device-scope fences.
+// sib[v] names v's sibling and side (>= 0: v is a left child), so a climb
+// reads both children without loading child[parent] first.
+constexpr int BU_LEAVES = 256;
+
+__device__ __forceinline__ void bu_merge(const double4 cl, const double4 cr, const float4 l0, const float4 l1,
+                                         const float4 h0, const float4 h1, double4& cm, float4& lo, float4& hi) {
+    // NodesArray::unite order: M = m_R + m_L; c = (c_R m_R + c_L m_L) / M
+    const double M = __dadd_rn(cr.w, cl.w);
+    cm.x = __ddiv_rn(__dadd_rn(__dmul_rn(cr.x, cr.w), __dmul_rn(cl.x, cl.w)), M);
+    cm.y = __ddiv_rn(__dadd_rn(__dmul_rn(cr.y, cr.w), __dmul_rn(cl.y, cl.w)), M);
+    cm.z = __ddiv_rn(__dadd_rn(__dmul_rn(cr.z, cr.w), __dmul_rn(cl.z, cl.w)), M);
+    cm.w = M;
+    lo = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
+    hi = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
+}
+
+__global__ void __launch_bounds__(BU_LEAVES) k_bottom_up_local(
+    int64_t n, const int32_t* __restrict__ parent, const int32_t* __restrict__ sib, const int32_t* __restrict__ rlo,
+    const int32_t* __restrict__ rhi, double4* __restrict__ node_cm, float4* __restrict__ bmin,
+    float4* __restrict__ bmax, int32_t* __restrict__ front, unsigned int* __restrict__ nfront, int* __restrict__ err) {
+    // [0][j]: leaf B0 + j; [1][j]: internal node n + B0 + j (Karras numbering:
+    // an internal node inside the block has its index inside the block too)
+    __shared__ double4 s_cm[2][BU_LEAVES];
+    __shared__ float4 s_lo[2][BU_LEAVES], s_hi[2][BU_LEAVES];
+    __shared__ int32_t s_par[2][BU_LEAVES], s_sib[2][BU_LEAVES];
+    __shared__ int32_t s_rlo[BU_LEAVES], s_rhi[BU_LEAVES];
+    __shared__ unsigned int s_cnt[BU_LEAVES];
+    __shared__ int32_t s_front[BU_LEAVES];  // frontier nodes are disjoint subtrees: at most one per leaf
+    __shared__ unsigned int s_nf, s_fbase;
+    const int j = threadIdx.x;
+    const int64_t B0 = (int64_t)blockIdx.x * BU_LEAVES;
+    const int64_t B1 = (B0 + BU_LEAVES < n ? B0 + BU_LEAVES : n) - 1;
+    const int64_t k = B0 + j;
+    s_cnt[j] = 0u;
+    if (j == 0) s_nf = 0u;
+    if (k < n) {
+        s_cm[0][j] = node_cm[k];
+        s_lo[0][j] = bmin[k];
+        s_hi[0][j] = bmax[k];
+        s_par[0][j] = parent[k];
+        s_sib[0][j] = sib[k];
+    }
+    if (k < n - 1) {
+        s_par[1][j] = parent[n + k];
+        s_sib[1][j] = sib[n + k];
+        s_rlo[j] = rlo[n + k];
+        s_rhi[j] = rhi[n + k];
+    }
+    __syncthreads();
+    int side = 0, slot = j;
+    int32_t cur = (int32_t)k;
+    double4 cm = make_double4(0, 0, 0, 0);
+    float4 lo = make_float4(0, 0, 0, 0), hi = lo;
+    if (k < n) {
+        cm = s_cm[0][j];
+        lo = s_lo[0][j];
+        hi = s_hi[0][j];
+    }
+    for (int level = 0; k < n; ++level) {
+        const int32_t par = s_par[side][slot];
+        if (par < 0) break;  // the root
+        const int64_t ip = (int64_t)par - n;
+        const bool local = ip >= B0 && ip <= B1 && s_rlo[ip - B0] >= B0 && s_rhi[ip - B0] <= B1;
+        if (!local) {
+            s_front[atomicAdd(&s_nf, 1u)] = cur;  // its data is in global memory already
+            break;
+        }
+        if (level >= MAX_CLIMB) {
+            atomicOr(err, ASTER_DEVERR_TREE);
+            break;
+        }
+        const int pslot = (int)(ip - B0);
+        __threadfence_block();  // own node data (shared) before the arrival count
+        if (atomicAdd(&s_cnt[pslot], 1u) == 0u) break;
+        __threadfence_block();
+        const int32_t sb = s_sib[side][slot];
+        const int32_t so = sb >= 0 ? sb : ~sb;
+        const int oside = so >= n ? 1 : 0;
+        const int oslot = (int)(oside ? (int64_t)so - n - B0 : (int64_t)so - B0);
+        const double4 oc = s_cm[oside][oslot];
+        const float4 ol = s_lo[oside][oslot], oh = s_hi[oside][oslot];
+        const bool right = sb < 0;  // cur is the right child
+        double4 pc;
+        float4 plo, phi;
+        bu_merge(right ? oc : cm, right ? cm : oc, right ? ol : lo, right ? lo : ol, right ? oh : hi, right ? hi : oh,
+                 pc, plo, phi);
+        node_cm[par] = pc;
+        bmin[par] = plo;
+        bmax[par] = phi;
+        s_cm[1][pslot] = pc;
+        s_lo[1][pslot] = plo;
+        s_hi[1][pslot] = phi;
+        cm = pc;
+        lo = plo;
+        hi = phi;
+        side = 1;
+        slot = pslot;
+        cur = par;
+    }
+    __syncthreads();  // one global reservation per block for its frontier nodes
+    if (j == 0) s_fbase = s_nf ? atomicAdd(nfront, s_nf) : 0u;
+    __syncthreads();
+    if ((unsigned)j < s_nf) front[s_fbase + j] = s_front[j];
+}
+
+__global__ void __launch_bounds__(256) k_bottom_up_front(int64_t n, const int32_t* __restrict__ front,
+                                                         const unsigned int* __restrict__ nfront,
+                                                         const int32_t* __restrict__ parent,
+                                                         const int32_t* __restrict__ sib,
+                                                         uint32_t* __restrict__ counters, double4* __restrict__ node_cm,
+                                                         float4* __restrict__ bmin, float4* __restrict__ bmax,
+                                                         int* __restrict__ err) {
+    const int64_t nf = *nfront;
+    for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nf; f += (int64_t)gridDim.x * blockDim.x) {
+        int32_t cur = front[f];
+        for (int level = 0;; ++level) {
             const int32_t par = parent[cur];
             if (par < 0) break;
-            if (++level > MAX_CLIMB) {
+            if (level >= MAX_CLIMB) {
                 atomicOr(err, ASTER_DEVERR_TREE);
                 break;
             }
+            const int32_t sb = sib[cur];
             __threadfence();
-            const uint32_t old = atomicAdd(&counters[par - n], 1u);
-            if (old == 0u) break;  // first arrival: the sibling finishes the node
+            if (atomicAdd(&counters[par - n], 1u) == 0u) break;  // first arrival: the sibling finishes it
             __threadfence();
-            const int2 ch = child[par];
-            const double4 cl = ld_cg(node_cm + ch.x), cr = ld_cg(node_cm + ch.y);
-            // NodesArray::unite order: M = m_R + m_L; c = (c_R m_R + c_L m_L) / M
-            const double M = __dadd_rn(cr.w, cl.w);
-            double4 c;
-            c.x = __ddiv_rn(__dadd_rn(__dmul_rn(cr.x, cr.w), __dmul_rn(cl.x, cl.w)), M);
-            c.y = __ddiv_rn(__dadd_rn(__dmul_rn(cr.y, cr.w), __dmul_rn(cl.y, cl.w)), M);
-            c.z = __ddiv_rn(__dadd_rn(__dmul_rn(cr.z, cr.w), __dmul_rn(cl.z, cl.w)), M);
-            c.w = M;
-            const float4 l0 = ld_cg(bmin + ch.x), l1 = ld_cg(bmin + ch.y);
-            const float4 h0 = ld_cg(bmax + ch.x), h1 = ld_cg(bmax + ch.y);
-            node_cm[par] = c;
-            bmin[par] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
-            bmax[par] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
+            const int32_t a = sb >= 0 ? cur : ~sb, b = sb >= 0 ? sb : cur;  // left, right
+            double4 pc;
+            float4 plo, phi;
+            bu_merge(ld_cg(node_cm + a), ld_cg(node_cm + b), ld_cg(bmin + a), ld_cg(bmin + b), ld_cg(bmax + a),
+                     ld_cg(bmax + b), pc, plo, phi);
+            node_cm[par] = pc;
+            bmin[par] = plo;
+            bmax[par] = phi;
             cur = par;
         }
     }
 }
-
 
 // Per internal node, after the climb (no dependencies, fully parallel): the
 // squared opening radius r_crit = l/theta + |com - box centre| (l = longest
@@ -457,9 +570,8 @@ __global__ void __launch_bounds__(256) k_node_finalize(int64_t n, double theta, 
 }
 
 // Child records for the walk: for internal node i (node n+i) the traversal
-// records of its two children, contiguous: crec[4i..4i+3] =
-// (hi_left, lo_left, hi_right, lo_right), so opening a node costs one 64-byte
-// load. Written by each non-root node into its parent's slot.
+// records of its two children in one contiguous 64-byte record, so opening a
+// node costs one load (layout below).
 __global__ void __launch_bounds__(256) k_child_records(int64_t n, const int2* __restrict__ child,
                                                        const float4* __restrict__ node_hi,
                                                        const float4* __restrict__ node_lo, float4* __restrict__ crec) {
@@ -898,6 +1010,24 @@ int run_sort(aster_ctx* c, int bits) {
     return ASTER_OK;
 }
 
+int launch_bottom_up(aster_ctx* c, int64_t n) {
+    LbvhBufs& t = c->tree;
+    unsigned int* nfront = red_groups(c) + 2;  // zeroed at the start of the build
+    const int64_t blocks = (n + BU_LEAVES - 1) / BU_LEAVES;
+    k_bottom_up_local<<<(unsigned)blocks, BU_LEAVES, 0, c->stream>>>(
+        n, t.parent.as<int32_t>(), t.sib.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(),
+        t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(), t.front.as<int32_t>(), nfront, c->err_dev);
+    ASTER_CUDA(cudaGetLastError());
+    const int64_t fb = std::min<int64_t>(blocks, (int64_t)c->sm_count * 8);
+    k_bottom_up_front<<<(unsigned)fb, 256, 0, c->stream>>>(n, t.front.as<int32_t>(), nfront, t.parent.as<int32_t>(),
+                                                           t.sib.as<int32_t>(), t.counters.as<uint32_t>(),
+                                                           t.node_cm.as<double4>(), t.bmin.as<float4>(),
+                                                           t.bmax.as<float4>(), c->err_dev);
+    ASTER_CUDA(cudaGetLastError());
+    c->stats.kernels += 2;
+    return ASTER_OK;
+}
+
 template <class KeyT>
 int run_build(aster_ctx* c, const aster_params* p) {
     LbvhBufs& t = c->tree;
@@ -921,24 +1051,23 @@ int run_build(aster_ctx* c, const aster_params* p) {
                                    c->stream));
         c->stats.kernels += 1;
     }
+    unsigned int* gcount = red_groups(c);  // [0] groups, [1] walk work counter, [2] bottom-up frontier
+    ASTER_CUDA(cudaMemsetAsync(gcount, 0, 3 * sizeof(unsigned int), c->stream));
     const KeyT* sc = t.sorted_codes.as<KeyT>();
     if (p->compat_mode)
         k_karras<KeyT, true><<<grid, 256, 0, c->stream>>>(
             n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.left.as<int32_t>(), t.right.as<int32_t>(),
-            t.parent.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(),
+            t.parent.as<int32_t>(), t.sib.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(),
             t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
             t.node_hi.as<float4>(), t.node_lo.as<float4>());
     else
         k_karras<KeyT, false><<<grid, 256, 0, c->stream>>>(
             n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.left.as<int32_t>(), t.right.as<int32_t>(),
-            t.parent.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(),
+            t.parent.as<int32_t>(), t.sib.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(),
             t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
             t.node_hi.as<float4>(), t.node_lo.as<float4>());
     ASTER_CUDA(cudaGetLastError());
-    k_bottom_up<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.child.as<int2>(),
-                                             t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(),
-                                             t.bmax.as<float4>(), c->err_dev);
-    ASTER_CUDA(cudaGetLastError());
+    ASTER_TRY(launch_bottom_up(c, n));
     k_node_finalize<<<grid, 256, 0, c->stream>>>(n, p->theta, t.node_cm.as<double4>(), t.bmin.as<float4>(),
                                                  t.bmax.as<float4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>());
     ASTER_CUDA(cudaGetLastError());
@@ -947,8 +1076,6 @@ int run_build(aster_ctx* c, const aster_params* p) {
                                                      t.node_lo.as<float4>(), t.crec.as<float4>());
         ASTER_CUDA(cudaGetLastError());
     }
-    unsigned int* gcount = red_groups(c);
-    ASTER_CUDA(cudaMemsetAsync(gcount, 0, 2 * sizeof(unsigned int), c->stream));
     k_make_groups<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(),
                                                t.groups.as<int2>(), gcount);
     ASTER_CUDA(cudaGetLastError());
@@ -970,6 +1097,8 @@ int ensure_tree(aster_ctx* c) {
     ASTER_TRY(t.left.ensure((size_t)m * 4));
     ASTER_TRY(t.right.ensure((size_t)m * 4));
     ASTER_TRY(t.parent.ensure((size_t)m * 4));
+    ASTER_TRY(t.sib.ensure((size_t)m * 4));
+    ASTER_TRY(t.front.ensure((size_t)n * 4));
     ASTER_TRY(t.rlo.ensure((size_t)m * 4));
     ASTER_TRY(t.rhi.ensure((size_t)m * 4));
     ASTER_TRY(t.counters.ensure((size_t)n * 4));
