@@ -58,18 +58,50 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi samples every 200 ms while the timed region runs."""
+    """SM clock and clock-event reasons sampled while the timed region runs.
+
+    NVML polled every ~2 ms from a thread (the timed C-ABI call releases the
+    GIL), so that even a timed region of a few tens of milliseconds gets
+    samples; the GPU is found by its PCI bus id, which stays right when
+    CUDA_VISIBLE_DEVICES renumbers devices. Falls back to `nvidia-smi -lms 200`
+    when NVML is unavailable. Read-only: no clock or other setting is changed."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, interval_s: float = 0.002):
         self.device = device
+        self.interval = interval_s
         self.proc = None
         self.lines: list[str] = []
+        self.nvml = None
+        self.handle = None
+        self.samples: list[tuple[float, int]] = []
+        self.max_mhz = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(device)
+            try:
+                bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+                self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.handle = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.nvml = pynvml
+        except Exception:
+            self.nvml = None
 
     def start(self):
+        if self.nvml is not None:
+            self._stop = threading.Event()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -79,11 +111,34 @@ class ClockSampler:
         except FileNotFoundError:
             self.proc = None
 
+    def _poll(self):
+        nv = self.nvml
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                self.samples.append((float(mhz), int(rs)))
+            except Exception:
+                pass
+            time.sleep(self.interval)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    @staticmethod
+    def _summary(sm, smax, reasons, source):
+        loaded = [x for x in sm if smax and x > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm), "source": source}
+
     def stop(self) -> dict:
+        if self.nvml is not None:
+            self._stop.set()
+            self.t.join(timeout=5)
+            reasons = {nm for nm, bit in self.REASONS for _, r in self.samples if r & bit}
+            return self._summary([m for m, _ in self.samples], float(self.max_mhz), reasons,
+                                 f"nvml every {self.interval * 1e3:.0f} ms")
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -92,7 +147,7 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [nm for nm, _ in self.REASONS]
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
@@ -105,9 +160,7 @@ class ClockSampler:
             for nm, v in zip(names, f[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
-        loaded = [s for s in sm if smax and s > 0.5 * smax] or sm
-        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return self._summary(sm, smax, reasons, "nvidia-smi every 200 ms")
 
 
 def max_over_ranks(ms: float, dist=None, device: str = "cpu") -> float:
@@ -254,8 +307,10 @@ def run_ours(args):
             "roofline": {"bound": "fp32", "kernel": "k_walk (tree walk + interactions)",
                          "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                          "traffic": args.walk_traffic,
-                         "peak_source": f"148 SMs x 128 FP32 lanes x 2 x median SM clock {f_mhz:.0f} MHz sampled "
-                                        f"during the run (no FP32 figure in MEASURED_PEAKS.json)",
+                         "peak_source": f"148 SMs x 128 FP32 lanes x 2 x "
+                                        + (f"median SM clock {f_mhz:.0f} MHz sampled during the timed region"
+                                           if clk.get("sm_mhz") else f"max SM clock {f_mhz:.0f} MHz (no clock samples)")
+                                        + " (no FP32 figure in MEASURED_PEAKS.json)",
                          "flop_per_interaction": FLOP_PER_PAIR},
             "e2e": e2e,
             "gpu_launches": kernels,
