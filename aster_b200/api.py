@@ -27,6 +27,8 @@ LIB_PATH = Path(__file__).resolve().parent / "libaster_cuda.so"
 OK = 0
 NEWTON = 0x0001
 PN1 = 0x0010
+PN2 = 0x0100   # ensemble only
+PN25 = 0x1000  # ensemble only
 FP64 = 0
 MIXED = 1
 SOLVER_ALLPAIRS = 0

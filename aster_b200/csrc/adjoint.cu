@@ -319,7 +319,7 @@ extern "C" int aster_adjoint_leapfrog(aster_ctx* c, const aster_params* p, int p
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
-    if (p->force_law & ASTER_PN1) return ASTER_ERR_UNSUPPORTED;
+    if (p->force_law & (ASTER_PN1 | ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
     AdjBufs& a = c->adj;

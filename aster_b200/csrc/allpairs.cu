@@ -349,6 +349,7 @@ void launch_mixed(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32
 // optional closing kick, or out_dev[nt*3].
 int aster_allpairs_launch(aster_ctx* c, const aster_params* p, int precision, bool closing_kick, int64_t nt,
                           const int32_t* targets_dev, double* out_dev) {
+    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;  // ensemble only
     const int64_t n = c->n;
     const int64_t per_block = (int64_t)BLOCK * IPT;
     const int64_t iblocks = (nt + per_block - 1) / per_block;
@@ -401,6 +402,7 @@ extern "C" int aster_allpairs(aster_ctx* c, const aster_params* p, int precision
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
     cudaEventRecord(c->ev[0], c->stream);
@@ -420,6 +422,7 @@ extern "C" int aster_allpairs_targets(aster_ctx* c, const aster_params* p, int p
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;
     for (int64_t t = 0; t < nt; ++t)
         if (targets[t] < 0 || targets[t] >= c->n) return ASTER_ERR_INVALID_ARG;
     ASTER_TRY(aster_begin(c));

@@ -63,8 +63,9 @@ int aster_check_params(const aster_params* p) {
     if (!p) return ASTER_ERR_INVALID_ARG;
     if (!std::isfinite(p->G) || !std::isfinite(p->eps2) || p->eps2 < 0.0) return ASTER_ERR_INVALID_ARG;
     if (!std::isfinite(p->dt) || !std::isfinite(p->theta) || p->theta < 0.0) return ASTER_ERR_INVALID_ARG;
-    if ((p->force_law & ASTER_PN1) && !(std::isfinite(p->c) && p->c > 0.0)) return ASTER_ERR_INVALID_ARG;
-    if (p->force_law & ~(ASTER_NEWTON | ASTER_PN1)) return ASTER_ERR_UNSUPPORTED;
+    const int32_t pn_bits = ASTER_PN1 | ASTER_PN2 | ASTER_PN25;
+    if ((p->force_law & pn_bits) && !(std::isfinite(p->c) && p->c > 0.0)) return ASTER_ERR_INVALID_ARG;
+    if (p->force_law & ~(ASTER_NEWTON | pn_bits)) return ASTER_ERR_UNSUPPORTED;
     if (p->morton_bits != 30 && p->morton_bits != 63) return ASTER_ERR_INVALID_ARG;
     if (p->compat_mode != 0 && p->compat_mode != 1) return ASTER_ERR_INVALID_ARG;
     if (p->compat_mode == 1 && p->morton_bits != 30) return ASTER_ERR_UNSUPPORTED;

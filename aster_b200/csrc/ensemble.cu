@@ -3,8 +3,10 @@
 //
 // The reference has no batched solver (a Simulation per system would also
 // share Parallelized's function-static pointer, builder_endpoint.cpp:731). The
-// pair law is the reference's compute_gravitational with the pairwise 1PN term
-// of get_pn1 (src/physics/tool_chain_impl.cpp:110-137); the integrators are
+// pair law is the reference's compute_gravitational
+// (src/physics/tool_chain_impl.cpp:120-137) with the pairwise post-Newtonian
+// terms of get_pn1 (c^-2, :110-118), get_pn2 (c^-4, :79-107) and get_pn25
+// (c^-5, :65-77), selected by the force-law bits; the integrators are
 // drift-kick-drift compositions: leapfrog (the map of update_leapfrog,
 // tool_chain_impl.cpp:169-185) and Yoshida's (1990) fourth-order triple jump.
 //
@@ -62,13 +64,78 @@ struct EnsSlab<false> {
     double4 v[64];  // (vx, vy, vz, |v|^2)
 };
 
-// Acceleration on body i from every body of the slab (j == i contributes 0:
-// zero separation is skipped), G applied by the caller.
-template <bool PN, int UNROLL>
+// Post-Newtonian constants and the terms in use: f bit 0 = 1PN, bit 1 = 2PN,
+// bit 2 = 2.5PN (warp-uniform). PN level PNL (a template parameter): 0 Newton
+// only, 1 Newton + 1PN, 2 Newton + the terms f selects.
+template <class T>
+struct PnK {
+    T c2, c4, c5;
+    int f;
+};
+
+// Acceleration on body i from every body of the slab, divided by G, in three
+// sums kept apart so that the small post-Newtonian corrections are not lost
+// against the Newtonian sum in FP32: aN (Newton), a1 (1PN), a2 (2PN + 2.5PN).
+// j == i contributes 0 (zero separation and relative velocity). With n the
+// unit vector from j to i (the reference's -norm):
+//   1PN : c^-2 m_j/r^2 [n A + (v_i - v_j) B]
+//   2PN : c^-4 { m_j/r^2 [n S_n + (v_i - v_j) S_v] + G^2 m_j/r^4 n S_m }
+//   2.5PN: c^-5 4/5 G m_i m_j/r^3 [(v_i - v_j) I_1 + n (n.(v_i - v_j)) I_2]
+// with A, B, S_n, S_v, S_m, I_1, I_2 the scalar brackets of get_pn1, get_pn2
+// and get_pn25.
+template <class T>
+struct PnPair {
+    // per-pair inputs
+    T nx, ny, nz, dvx, dvy, dvz, inv, inv2, mi, mj, vi2, vj2, v12, nv1, nv2, G;
+    __device__ __forceinline__ void pn1(T c2, T& px, T& py, T& pz) const {
+        const T A = -vi2 - T(2) * vj2 + T(4) * v12 + T(1.5) * nv2 * nv2 + (T(5) * mi + T(4) * mj) * G * inv;
+        const T B = T(4) * nv1 - T(3) * nv2;
+        const T f = mj * inv2 * c2;
+        px += (nx * A + dvx * B) * f;
+        py += (ny * A + dvy * B) * f;
+        pz += (nz * A + dvz * B) * f;
+    }
+    __device__ __forceinline__ void pn2(T c4, T& qx, T& qy, T& qz) const {
+        const T nv22 = nv2 * nv2, nv12 = nv1 * nv1;
+        const T p1 = G * mi * inv, p2 = G * mj * inv;
+        const T Sn = T(-2) * vj2 * vj2 + T(4) * vj2 * v12 - T(2) * v12 * v12 + T(1.5) * vi2 * nv22 +
+                     T(4.5) * vj2 * nv22 - T(6) * v12 * nv22 - T(1.875) * nv22 * nv22 +
+                     p1 * (T(-3.75) * vi2 + T(1.25) * vj2 - T(2.5) * v12 + T(19.5) * nv12 - T(39) * nv1 * nv2 +
+                           T(8.5) * nv22) +
+                     p2 * (T(4) * vj2 - T(8) * v12 + T(2) * nv12 - T(4) * nv1 * nv2 - T(6) * nv22);
+        const T Sv = vi2 * nv2 + T(4) * vj2 * nv1 - T(5) * vj2 * nv2 - T(4) * v12 * nv1 + T(4) * v12 * nv2 -
+                     T(6) * nv1 * nv22 + T(4.5) * nv22 * nv2 + p1 * (T(-15.75) * nv1 + T(13.75) * nv2) +
+                     p2 * (T(-2) * nv1 - T(2) * nv2);
+        const T Sm = T(-14.25) * mi * mi - T(9) * mj * mj - T(34.5) * mi * mj;
+        const T f = mj * inv2 * c4, g = G * G * mj * inv2 * inv2 * Sm * c4;
+        qx += f * (nx * Sn + dvx * Sv) + g * nx;
+        qy += f * (ny * Sn + dvy * Sv) + g * ny;
+        qz += f * (nz * Sn + dvz * Sv) + g * nz;
+    }
+    __device__ __forceinline__ void pn25(T c5, T& qx, T& qy, T& qz) const {
+        const T p1 = G * mi * inv, p2 = G * mj * inv;
+        const T sq = dvx * dvx + dvy * dvy + dvz * dvz;
+        const T I1 = -sq + T(2) * p1 - T(8) * p2;
+        const T I2 = (nv1 - nv2) * (T(3) * sq - T(6) * p1 + T(52) / T(3) * p2);
+        const T f = T(0.8) * G * mi * mj * inv * inv2 * c5;
+        qx += (dvx * I1 + nx * I2) * f;
+        qy += (dvy * I1 + ny * I2) * f;
+        qz += (dvz * I1 + nz * I2) * f;
+    }
+};
+
+template <int PNL, class T>
+__device__ __forceinline__ void pn_terms(const PnK<T>& k, const PnPair<T>& q, T& px, T& py, T& pz, T& qx, T& qy,
+                                         T& qz) {
+    if (PNL == 1 || (PNL == 2 && (k.f & 1))) q.pn1(k.c2, px, py, pz);
+    if (PNL == 2 && (k.f & 2)) q.pn2(k.c4, qx, qy, qz);
+    if (PNL == 2 && (k.f & 4)) q.pn25(k.c5, qx, qy, qz);
+}
+
+template <int PNL, int UNROLL>
 __device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int n, float4 hi, float4 lo, float4 vi, float eps2,
-                                          float G, float inv_c2, float& ax, float& ay, float& az) {
-    float px = 0.f, py = 0.f, pz = 0.f;
-    ax = ay = az = 0.f;
+                                          float G, const PnK<float>& k, float3& aN, float3& a1, float3& a2) {
+    float ax = 0.f, ay = 0.f, az = 0.f, px = 0.f, py = 0.f, pz = 0.f, qx = 0.f, qy = 0.f, qz = 0.f;
 #pragma unroll UNROLL
     for (int j = 0; j < n; ++j) {
         const float4 h = s.hi[j], l = s.lo[j];
@@ -81,26 +148,28 @@ __device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int n, float4 
         const float inv2 = inv * inv;
         const float sN = h.w * inv * inv2;
         ax = fmaf(dx, sN, ax); ay = fmaf(dy, sN, ay); az = fmaf(dz, sN, az);
-        if (PN) {
+        if (PNL > 0) {
             const float4 vj = s.v[j];
-            const float nx = -dx * inv, ny = -dy * inv, nz = -dz * inv;
-            const float v12 = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
-            const float nv1 = nx * vi.x + ny * vi.y + nz * vi.z;
-            const float nv2 = nx * vj.x + ny * vj.y + nz * vj.z;
-            const float A = -vi.w - 2.f * vj.w + 4.f * v12 + 1.5f * nv2 * nv2 + (5.f * hi.w + 4.f * h.w) * G * inv;
-            const float B = 4.f * nv1 - 3.f * nv2;
-            const float f = h.w * inv2 * inv_c2;
-            px = fmaf(nx * A + (vi.x - vj.x) * B, f, px);
-            py = fmaf(ny * A + (vi.y - vj.y) * B, f, py);
-            pz = fmaf(nz * A + (vi.z - vj.z) * B, f, pz);
+            PnPair<float> q;
+            q.nx = -dx * inv; q.ny = -dy * inv; q.nz = -dz * inv;
+            q.dvx = vi.x - vj.x; q.dvy = vi.y - vj.y; q.dvz = vi.z - vj.z;
+            q.inv = inv; q.inv2 = inv2; q.mi = hi.w; q.mj = h.w; q.vi2 = vi.w; q.vj2 = vj.w;
+            q.v12 = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
+            q.nv1 = q.nx * vi.x + q.ny * vi.y + q.nz * vi.z;
+            q.nv2 = q.nx * vj.x + q.ny * vj.y + q.nz * vj.z;
+            q.G = G;
+            pn_terms<PNL>(k, q, px, py, pz, qx, qy, qz);
         }
     }
-    ax += px; ay += py; az += pz;
+    aN = make_float3(ax, ay, az);
+    a1 = make_float3(px, py, pz);
+    a2 = make_float3(qx, qy, qz);
 }
 
-template <bool PN, int UNROLL>
+template <int PNL, int UNROLL>
 __device__ __forceinline__ void accel_f64(const EnsSlab<false>& s, int n, double4 xi, double4 vi, double eps2,
-                                          double G, double inv_c2, double& ax, double& ay, double& az) {
+                                          double G, const PnK<double>& k, double& ax, double& ay, double& az) {
+    double px = 0.0, py = 0.0, pz = 0.0, qx = 0.0, qy = 0.0, qz = 0.0;
     ax = ay = az = 0.0;
 #pragma unroll UNROLL
     for (int j = 0; j < n; ++j) {
@@ -111,32 +180,32 @@ __device__ __forceinline__ void accel_f64(const EnsSlab<false>& s, int n, double
         const double inv2 = inv * inv;
         const double sN = xj.w * inv * inv2;
         ax = fma(dx, sN, ax); ay = fma(dy, sN, ay); az = fma(dz, sN, az);
-        if (PN) {
+        if (PNL > 0) {
             const double4 vj = s.v[j];
-            const double nx = -dx * inv, ny = -dy * inv, nz = -dz * inv;
-            const double v12 = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
-            const double nv1 = nx * vi.x + ny * vi.y + nz * vi.z;
-            const double nv2 = nx * vj.x + ny * vj.y + nz * vj.z;
-            const double A = -vi.w - 2.0 * vj.w + 4.0 * v12 + 1.5 * nv2 * nv2 + 5.0 * G * xi.w * inv +
-                             4.0 * G * xj.w * inv;
-            const double B = 4.0 * nv1 - 3.0 * nv2;
-            const double f = xj.w * inv2 * inv_c2;
-            ax += (nx * A + (vi.x - vj.x) * B) * f;
-            ay += (ny * A + (vi.y - vj.y) * B) * f;
-            az += (nz * A + (vi.z - vj.z) * B) * f;
+            PnPair<double> q;
+            q.nx = -dx * inv; q.ny = -dy * inv; q.nz = -dz * inv;
+            q.dvx = vi.x - vj.x; q.dvy = vi.y - vj.y; q.dvz = vi.z - vj.z;
+            q.inv = inv; q.inv2 = inv2; q.mi = xi.w; q.mj = xj.w; q.vi2 = vi.w; q.vj2 = vj.w;
+            q.v12 = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
+            q.nv1 = q.nx * vi.x + q.ny * vi.y + q.nz * vi.z;
+            q.nv2 = q.nx * vj.x + q.ny * vj.y + q.nz * vj.z;
+            q.G = G;
+            pn_terms<PNL>(k, q, px, py, pz, qx, qy, qz);
         }
     }
+    ax += px + qx; ay += py + qy; az += pz + qz;
 }
 
-template <bool MIXED, bool PN, int UNROLL, int NST>
+template <bool MIXED, int PNL, int UNROLL, int NST>
 __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, const int32_t* __restrict__ off,
-                           double4* __restrict__ pm, double4* __restrict__ vel, double G, double eps2, double inv_c2,
+                           double4* __restrict__ pm, double4* __restrict__ vel, double G, double eps2, PnK<double> pk,
                            Coeffs k, int64_t nsteps, int check_every, unsigned int* __restrict__ work,
                            const volatile int* __restrict__ cancel, int* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char ens_smem[];
     EnsSlab<MIXED>& slab = reinterpret_cast<EnsSlab<MIXED>*>(ens_smem)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
-    const float Gf = (float)G, epsf = (float)eps2, icf = (float)inv_c2;
+    const float Gf = (float)G, epsf = (float)eps2;
+    const PnK<float> pkf{(float)pk.c2, (float)pk.c4, (float)pk.c5, pk.f};
     for (;;) {
         unsigned int w = 0;
         if (lane == 0) w = atomicAdd(work, 1u);
@@ -198,13 +267,15 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
                     const int idx = (q ? v1 : v0) ? lane + 32 * q : 0;  // idle slots read body 0
                     if (MIXED) {
                         const EnsSlab<true>& sl = reinterpret_cast<const EnsSlab<true>&>(slab);
-                        float ax, ay, az;
-                        accel_f32<PN, UNROLL>(sl, n, sl.hi[idx], sl.lo[idx], sl.v[idx], epsf, Gf, icf, ax, ay, az);
-                        a[q][0] = G * ax; a[q][1] = G * ay; a[q][2] = G * az;
+                        float3 aN, a1, a2;
+                        accel_f32<PNL, UNROLL>(sl, n, sl.hi[idx], sl.lo[idx], sl.v[idx], epsf, Gf, pkf, aN, a1, a2);
+                        a[q][0] = G * (((double)aN.x + (double)a1.x) + (double)a2.x);
+                        a[q][1] = G * (((double)aN.y + (double)a1.y) + (double)a2.y);
+                        a[q][2] = G * (((double)aN.z + (double)a1.z) + (double)a2.z);
                     } else {
                         const EnsSlab<false>& sl = reinterpret_cast<const EnsSlab<false>&>(slab);
                         double ax, ay, az;
-                        accel_f64<PN, UNROLL>(sl, n, sl.x[idx], sl.v[idx], eps2, G, inv_c2, ax, ay, az);
+                        accel_f64<PNL, UNROLL>(sl, n, sl.x[idx], sl.v[idx], eps2, G, pk, ax, ay, az);
                         a[q][0] = G * ax; a[q][1] = G * ay; a[q][2] = G * az;
                     }
                 }
@@ -279,11 +350,24 @@ __global__ void k_unpack_ens(int64_t n, const double4* __restrict__ src, double*
     }
 }
 
-template <bool MIXED, bool PN, int UNROLL>
+PnK<double> make_pn(const aster_params* p) {
+    PnK<double> k{0.0, 0.0, 0.0, 0};
+    k.f = ((p->force_law & ASTER_PN1) ? 1 : 0) | ((p->force_law & ASTER_PN2) ? 2 : 0) |
+          ((p->force_law & ASTER_PN25) ? 4 : 0);
+    if (k.f) {
+        const double ic = 1.0 / p->c;  // powers in the reference's order: inv_c * inv_c * ...
+        k.c2 = ic * ic;
+        k.c4 = ic * ic * ic * ic;
+        k.c5 = ic * ic * ic * ic * ic;
+    }
+    return k;
+}
+
+template <bool MIXED, int PNL, int UNROLL>
 int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_t nsteps, int wpb, int check_every,
                     bool use_graph) {
     EnsBufs& e = c->ens;
-    auto kern = k.nst == 3 ? k_ensemble<MIXED, PN, UNROLL, 3> : k_ensemble<MIXED, PN, UNROLL, 1>;
+    auto kern = k.nst == 3 ? k_ensemble<MIXED, PNL, UNROLL, 3> : k_ensemble<MIXED, PNL, UNROLL, 1>;
     const size_t smem = (size_t)wpb * sizeof(EnsSlab<MIXED>);
     if (smem > 48 * 1024) ASTER_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -292,12 +376,12 @@ int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_
     int64_t blocks = (int64_t)c->sm_count * per_sm;
     const int64_t need = (e.nsys + wpb - 1) / wpb;
     if (blocks > need) blocks = need;
-    const double inv_c2 = PN ? 1.0 / (p->c * p->c) : 0.0;
+    const PnK<double> pk = make_pn(p);
     unsigned int* work = e.counter.as<unsigned int>();
     auto enqueue = [&](cudaStream_t s) -> int {
         ASTER_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned int), s));
         kern<<<(unsigned)blocks, wpb * 32, smem, s>>>(e.nsys, e.order.as<int32_t>(), e.off.as<int32_t>(),
-                                                     e.pm.as<double4>(), e.vel.as<double4>(), p->G, p->eps2, inv_c2, k,
+                                                     e.pm.as<double4>(), e.vel.as<double4>(), p->G, p->eps2, pk, k,
                                                      nsteps, check_every, work, e.cancel_dev, c->err_dev);
         ASTER_CUDA(cudaGetLastError());
         return ASTER_OK;
@@ -320,13 +404,13 @@ int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_
     return ASTER_OK;
 }
 
-template <bool MIXED, bool PN>
+template <bool MIXED, int PNL>
 int dispatch_unroll(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_t nsteps, int wpb, int unroll,
                     int check_every, bool g) {
     switch (unroll) {
-        case 1: return launch_ensemble<MIXED, PN, 1>(c, p, k, nsteps, wpb, check_every, g);
-        case 4: return launch_ensemble<MIXED, PN, 4>(c, p, k, nsteps, wpb, check_every, g);
-        default: return launch_ensemble<MIXED, PN, 2>(c, p, k, nsteps, wpb, check_every, g);
+        case 1: return launch_ensemble<MIXED, PNL, 1>(c, p, k, nsteps, wpb, check_every, g);
+        case 4: return launch_ensemble<MIXED, PNL, 4>(c, p, k, nsteps, wpb, check_every, g);
+        default: return launch_ensemble<MIXED, PNL, 2>(c, p, k, nsteps, wpb, check_every, g);
     }
 }
 
@@ -434,15 +518,18 @@ extern "C" int aster_ensemble_run(aster_ctx* c, const aster_params* p, int integ
     c->stats = aster_stats{};
     *c->ens.cancel_host = 0;
     const Coeffs k = make_coeffs(integrator, p->dt);
-    const bool pn = (p->force_law & ASTER_PN1) != 0;
+    // PN level: 2 when a 2PN or 2.5PN term is requested, else 1 for 1PN alone
+    const int pnl = (p->force_law & (ASTER_PN2 | ASTER_PN25)) ? 2 : ((p->force_law & ASTER_PN1) ? 1 : 0);
     cudaEventRecord(c->ev[0], c->stream);
     int st;
     if (precision == ASTER_MIXED)
-        st = pn ? dispatch_unroll<true, true>(c, p, k, nsteps, wpb, unroll, check, graph)
-                : dispatch_unroll<true, false>(c, p, k, nsteps, wpb, unroll, check, graph);
+        st = pnl == 2 ? dispatch_unroll<true, 2>(c, p, k, nsteps, wpb, unroll, check, graph)
+           : pnl == 1 ? dispatch_unroll<true, 1>(c, p, k, nsteps, wpb, unroll, check, graph)
+                      : dispatch_unroll<true, 0>(c, p, k, nsteps, wpb, unroll, check, graph);
     else
-        st = pn ? dispatch_unroll<false, true>(c, p, k, nsteps, wpb, unroll, check, graph)
-                : dispatch_unroll<false, false>(c, p, k, nsteps, wpb, unroll, check, graph);
+        st = pnl == 2 ? dispatch_unroll<false, 2>(c, p, k, nsteps, wpb, unroll, check, graph)
+           : pnl == 1 ? dispatch_unroll<false, 1>(c, p, k, nsteps, wpb, unroll, check, graph)
+                      : dispatch_unroll<false, 0>(c, p, k, nsteps, wpb, unroll, check, graph);
     if (st != ASTER_OK) return st;
     cudaEventRecord(c->ev[1], c->stream);
     st = aster_finish(c);

@@ -204,6 +204,7 @@ extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, 
     if (solver != ASTER_SOLVER_ALLPAIRS && solver != ASTER_SOLVER_LBVH) return ASTER_ERR_INVALID_ARG;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
     if (solver == ASTER_SOLVER_LBVH && (p->force_law & ASTER_PN1)) return ASTER_ERR_UNSUPPORTED;
+    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;  // ensemble only
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
     const bool mixed_ap = solver == ASTER_SOLVER_ALLPAIRS && precision == ASTER_MIXED;

@@ -481,9 +481,6 @@ __global__ void __launch_bounds__(BU_LEAVES) k_bottom_up_local(
         float4 plo, phi;
         bu_merge(right ? oc : cm, right ? cm : oc, right ? ol : lo, right ? lo : ol, right ? oh : hi, right ? hi : oh,
                  pc, plo, phi);
-        node_cm[par] = pc;
-        bmin[par] = plo;
-        bmax[par] = phi;
         s_cm[1][pslot] = pc;
         s_lo[1][pslot] = plo;
         s_hi[1][pslot] = phi;
@@ -496,8 +493,27 @@ __global__ void __launch_bounds__(BU_LEAVES) k_bottom_up_local(
     }
     __syncthreads();  // one global reservation per block for its frontier nodes
     if (j == 0) s_fbase = s_nf ? atomicAdd(nfront, s_nf) : 0u;
+    // the block's completed internal nodes (both children arrived) go to global
+    // memory in one coalesced pass, not from inside the climb, so that the
+    // block-scope fences there wait for shared-memory stores only
+    if (k < n - 1 && s_cnt[j] == 2u) {
+        node_cm[n + k] = s_cm[1][j];
+        bmin[n + k] = s_lo[1][j];
+        bmax[n + k] = s_hi[1][j];
+    }
     __syncthreads();
     if ((unsigned)j < s_nf) front[s_fbase + j] = s_front[j];
+}
+
+#ifndef ASTER_BU_FENCE_ACQREL
+#define ASTER_BU_FENCE_ACQREL 0
+#endif
+__device__ __forceinline__ void bu_fence_gpu() {
+#if ASTER_BU_FENCE_ACQREL
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+#else
+    __threadfence();
+#endif
 }
 
 __global__ void __launch_bounds__(256) k_bottom_up_front(int64_t n, const int32_t* __restrict__ front,
@@ -510,26 +526,37 @@ __global__ void __launch_bounds__(256) k_bottom_up_front(int64_t n, const int32_
     const int64_t nf = *nfront;
     for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nf; f += (int64_t)gridDim.x * blockDim.x) {
         int32_t cur = front[f];
-        for (int level = 0;; ++level) {
-            const int32_t par = parent[cur];
-            if (par < 0) break;
+        // the climb's own node data stays in registers; only the sibling's is loaded
+        double4 cm = ld_cg(node_cm + cur);
+        float4 lo = ld_cg(bmin + cur), hi = ld_cg(bmax + cur);
+        int32_t par = parent[cur], sb = sib[cur];
+        for (int level = 0; par >= 0; ++level) {
             if (level >= MAX_CLIMB) {
                 atomicOr(err, ASTER_DEVERR_TREE);
                 break;
             }
-            const int32_t sb = sib[cur];
-            __threadfence();
+            // the next level's links load while this level synchronises
+            const int32_t par_next = parent[par], sb_next = sib[par];
+            bu_fence_gpu();  // release: this chain's node data
             if (atomicAdd(&counters[par - n], 1u) == 0u) break;  // first arrival: the sibling finishes it
-            __threadfence();
-            const int32_t a = sb >= 0 ? cur : ~sb, b = sb >= 0 ? sb : cur;  // left, right
+            bu_fence_gpu();  // acquire: the sibling's node data
+            const int32_t so = sb >= 0 ? sb : ~sb;
+            const double4 oc = ld_cg(node_cm + so);
+            const float4 ol = ld_cg(bmin + so), oh = ld_cg(bmax + so);
+            const bool right = sb < 0;  // cur is the right child
             double4 pc;
             float4 plo, phi;
-            bu_merge(ld_cg(node_cm + a), ld_cg(node_cm + b), ld_cg(bmin + a), ld_cg(bmin + b), ld_cg(bmax + a),
-                     ld_cg(bmax + b), pc, plo, phi);
+            bu_merge(right ? oc : cm, right ? cm : oc, right ? ol : lo, right ? lo : ol, right ? oh : hi,
+                     right ? hi : oh, pc, plo, phi);
             node_cm[par] = pc;
             bmin[par] = plo;
             bmax[par] = phi;
+            cm = pc;
+            lo = plo;
+            hi = phi;
             cur = par;
+            par = par_next;
+            sb = sb_next;
         }
     }
 }
@@ -1246,7 +1273,7 @@ extern "C" int aster_lbvh_forces(aster_ctx* c, const aster_params* p, int precis
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
-    if (p->force_law & ASTER_PN1) return ASTER_ERR_UNSUPPORTED;
+    if (p->force_law & (ASTER_PN1 | ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
     int32_t* cnt = nullptr;

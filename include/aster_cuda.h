@@ -46,7 +46,9 @@ extern "C" {
 /* ---- force law bits: the reference PN_expansion_type bitmask
  *      (include/Aster/simulations/basic.h:39-53) ------------------------- */
 #define ASTER_NEWTON 0x0001
-#define ASTER_PN1 0x0010
+#define ASTER_PN1 0x0010  /* get_pn1, c^-2 (src/physics/tool_chain_impl.cpp:110-118)  */
+#define ASTER_PN2 0x0100  /* get_pn2, c^-4 (tool_chain_impl.cpp:79-107); ensemble only */
+#define ASTER_PN25 0x1000 /* get_pn25, c^-5 (tool_chain_impl.cpp:65-77); ensemble only */
 
 /* ---- enums ------------------------------------------------------------- */
 #define ASTER_FP64 0   /* plain FP64 pair arithmetic                          */
@@ -66,7 +68,7 @@ typedef struct aster_params {
     double eps2;        /* softening added to r^2 (Simulation::softening)      */
     double theta;       /* opening angle (Simulation::theta)                   */
     double dt;          /* time step (get_dt)                                  */
-    int32_t force_law;  /* ASTER_NEWTON | ASTER_PN1                            */
+    int32_t force_law;  /* ASTER_NEWTON | ASTER_PN1 [| ASTER_PN2 | ASTER_PN25]   */
     int32_t morton_bits;/* 30 (reference) or 63                                */
     int32_t compat_mode;/* 1: OpenCL BH_hyper tree semantics (descending order,
                            body-index tie-break, 1024->0 Morton wrap)         */

@@ -14,7 +14,8 @@
  * (oracle/_ref/libaster_ref.so) and with the committed golden fixtures.
  *
  * Functions and the reference code they restate:
- *   orc_pair_acc        src/physics/tool_chain_impl.cpp:110-137 (Newton + 1PN, CPU form)
+ *   orc_pair_acc        src/physics/tool_chain_impl.cpp:65-137 (compute_gravitational: Newton
+ *                       + get_pn1 + get_pn2 + get_pn25, CPU forms, as accelerations)
  *   orc_allpairs        src/utils/builder_endpoint.cpp:729-757 (Parallelized)
  *   orc_morton30        src/solvers/bh_specialization.cpp:30-46 (get_morton, part1by2)
  *   orc_morton30_compat include/Aster/kernels/morton_writer.cl.h:72-122 (gen_mortons 3-D)
@@ -36,6 +37,8 @@
 #include <unistd.h>
 
 #define PN1_FLAG 0x10
+#define PN2_FLAG 0x100
+#define PN25_FLAG 0x1000
 
 /* ------------------------------------------------------------------------ */
 /* threading helper                                                          */
@@ -94,7 +97,12 @@ static void orc_parallel(long n, orc_range_fn fn, void* ctx) {
  *                     + (v1 - v2)(4 n.v1 - 3 n.v2) ] / c^2
  * (the reference multiplies by m1 to make a force and Parallelized divides it
  * back out, so the acceleration is a1 itself). */
-void orc_pair_acc(double G, double inv_c2, double eps2, int pn,
+/* Acceleration of body 1 (the reference's force divided by m1). inv_c = 1/c.
+ * The post-Newtonian terms use n = (x1 - x2)/r (the reference passes -norm)
+ * and are scaled by c^-2, c^-4, c^-5 as in compute_gravitational
+ * (tool_chain_impl.cpp:120-137); get_pn2 (:79-107) and get_pn25 (:65-77) are
+ * written out in the reference's operation order. */
+void orc_pair_acc(double G, double inv_c, double eps2, int pn,
                   double m1, double m2, const double* v1, const double* v2,
                   const double* p1, const double* p2, double* a) {
     double d[3] = {p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]};
@@ -103,23 +111,53 @@ void orc_pair_acc(double G, double inv_c2, double eps2, int pn,
     double inv_r2 = inv_r * inv_r;
     double s = G * m2 * inv_r2 * inv_r;
     a[0] = d[0] * s; a[1] = d[1] * s; a[2] = d[2] * s;
+    if (!(pn & (PN1_FLAG | PN2_FLAG | PN25_FLAG))) return;
+    double n[3] = {-d[0] * inv_r, -d[1] * inv_r, -d[2] * inv_r};
+    double v1sq = v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2];
+    double v2sq = v2[0] * v2[0] + v2[1] * v2[1] + v2[2] * v2[2];
+    double v12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
+    double nv1 = n[0] * v1[0] + n[1] * v1[1] + n[2] * v1[2];
+    double nv2 = n[0] * v2[0] + n[1] * v2[1] + n[2] * v2[2];
+    double inv_c2 = inv_c * inv_c;
     if (pn & PN1_FLAG) {
-        double n[3] = {-d[0] * inv_r, -d[1] * inv_r, -d[2] * inv_r};
-        double v1sq = v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2];
-        double v2sq = v2[0] * v2[0] + v2[1] * v2[1] + v2[2] * v2[2];
-        double v12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
-        double nv1 = n[0] * v1[0] + n[1] * v1[1] + n[2] * v1[2];
-        double nv2 = n[0] * v2[0] + n[1] * v2[1] + n[2] * v2[2];
         double A = -v1sq - 2.0 * v2sq + 4.0 * v12 + 1.5 * nv2 * nv2 + 5.0 * G * m1 * inv_r + 4.0 * G * m2 * inv_r;
         double Bc = 4.0 * nv1 - 3.0 * nv2;
         double f = G * m2 * inv_r2 * inv_c2;
         for (int k = 0; k < 3; ++k) a[k] += (n[k] * A + (v1[k] - v2[k]) * Bc) * f;
     }
+    if (pn & PN2_FLAG) {
+        double nv22 = nv2 * nv2, nv12 = nv1 * nv1;
+        double pn1 = G * m1 * inv_r, pn2 = G * m2 * inv_r;
+        double Sn = -2 * v2sq * v2sq + 4 * v2sq * v12 - 2 * v12 * v12 + 3.0 / 2.0 * v1sq * nv22 +
+                    9.0 / 2.0 * v2sq * nv22 - 6 * v12 * nv22 - 15.0 / 8.0 * nv22 * nv22 +
+                    pn1 * (-15.0 / 4.0 * v1sq + 5.0 / 4.0 * v2sq - 5.0 / 2.0 * v12 + 39.0 / 2.0 * nv12 -
+                           39.0 * nv1 * nv2 + 17.0 / 2.0 * nv22) +
+                    pn2 * (4 * v2sq - 8 * v12 + 2 * nv12 - 4 * nv1 * nv2 - 6 * nv22);
+        double Sv = v1sq * nv2 + 4 * v2sq * nv1 - 5 * v2sq * nv2 - 4 * v12 * nv1 + 4 * v12 * nv2 -
+                    6 * nv1 * nv22 + 9.0 / 2.0 * nv22 * nv2 + pn1 * (-63.0 / 4.0 * nv1 + 55.0 / 4.0 * nv2) +
+                    pn2 * (-2 * nv1 - 2 * nv2);
+        double f = G * m2 * inv_r * inv_r;
+        double g3 = G * G * G * m2 * inv_r * inv_r * inv_r * inv_r;
+        double Sm = -57.0 / 4.0 * m1 * m1 - 9 * m2 * m2 - 69.0 / 2.0 * m1 * m2;
+        double c4 = inv_c * inv_c * inv_c * inv_c;
+        for (int k = 0; k < 3; ++k) a[k] += c4 * (f * (n[k] * Sn + (v1[k] - v2[k]) * Sv) + g3 * n[k] * Sm);
+    }
+    if (pn & PN25_FLAG) {
+        double pn1 = G * m1 * inv_r, pn2 = G * m2 * inv_r;
+        double dv[3] = {v1[0] - v2[0], v1[1] - v2[1], v1[2] - v2[2]};
+        double sq = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+        double i1 = -sq + 2 * pn1 - 8 * pn2;
+        double nd = nv1 - nv2;
+        double i2 = 3 * sq - 6 * pn1 + 52.0 / 3.0 * pn2;
+        double f = 4.0 / 5.0 * G * G * m1 * m2 * inv_r * inv_r * inv_r;
+        double c5 = inv_c * inv_c * inv_c * inv_c * inv_c;
+        for (int k = 0; k < 3; ++k) a[k] += c5 * ((dv[k] * i1 + n[k] * nd * i2) * f);
+    }
 }
 
 typedef struct {
     long n, ns; const double *pos, *vel, *m; const long* targets;
-    double G, inv_c2, eps2; int pn; double* acc;
+    double G, inv_c, eps2; int pn; double* acc;
 } allpairs_ctx;
 
 static void allpairs_range(void* c_, long lo, long hi) {
@@ -129,7 +167,7 @@ static void allpairs_range(void* c_, long lo, long hi) {
         double ax = 0, ay = 0, az = 0, a[3];
         for (long j = 0; j < c->n; ++j) {
             if (j == i) continue;
-            orc_pair_acc(c->G, c->inv_c2, c->eps2, c->pn, c->m[i], c->m[j], c->vel + 3 * i, c->vel + 3 * j,
+            orc_pair_acc(c->G, c->inv_c, c->eps2, c->pn, c->m[i], c->m[j], c->vel + 3 * i, c->vel + 3 * j,
                          c->pos + 3 * i, c->pos + 3 * j, a);
             ax += a[0]; ay += a[1]; az += a[2];
         }
@@ -140,11 +178,11 @@ static void allpairs_range(void* c_, long lo, long hi) {
 /* All-pairs accelerations (skip j == i). targets == NULL: every body, else the
  * nt listed bodies (acc has nt rows). vel may be NULL when pn has no PN bit. */
 void orc_allpairs(long n, const double* pos, const double* vel, const double* m,
-                  double G, double inv_c2, double eps2, int pn,
+                  double G, double inv_c, double eps2, int pn,
                   long nt, const long* targets, double* acc) {
     double* vtmp = NULL;
     if (!vel) { vtmp = (double*)calloc((size_t)n * 3, sizeof(double)); vel = vtmp; }
-    allpairs_ctx c = {n, nt, pos, vel, m, targets, G, inv_c2, eps2, pn, acc};
+    allpairs_ctx c = {n, nt, pos, vel, m, targets, G, inv_c, eps2, pn, acc};
     orc_parallel(targets ? nt : n, allpairs_range, &c);
     free(vtmp);
 }
@@ -200,14 +238,14 @@ void orc_momentum(long n, const double* vel, const double* m, double* p) {
  * A twice per step; both produce the same trajectory up to rounding.
  * acc (n*3) must hold A(x0) on entry (computed here if acc_valid == 0);
  * acc_steps (nsteps*n*3, optional) receives A(x_{k+1}). */
-void orc_kdk(long n, double* pos, double* vel, const double* m, double G, double inv_c2,
+void orc_kdk(long n, double* pos, double* vel, const double* m, double G, double inv_c,
              double eps2, int pn, double dt, int nsteps, double* acc, int acc_valid,
              double* acc_steps) {
-    if (!acc_valid) orc_allpairs(n, pos, vel, m, G, inv_c2, eps2, pn, 0, NULL, acc);
+    if (!acc_valid) orc_allpairs(n, pos, vel, m, G, inv_c, eps2, pn, 0, NULL, acc);
     const double h = 0.5 * dt;
     for (int k = 0; k < nsteps; ++k) {
         for (long i = 0; i < 3 * n; ++i) { vel[i] += acc[i] * h; pos[i] += vel[i] * dt; }
-        orc_allpairs(n, pos, vel, m, G, inv_c2, eps2, pn, 0, NULL, acc);
+        orc_allpairs(n, pos, vel, m, G, inv_c, eps2, pn, 0, NULL, acc);
         for (long i = 0; i < 3 * n; ++i) vel[i] += acc[i] * h;
         if (acc_steps) memcpy(acc_steps + (size_t)k * n * 3, acc, (size_t)n * 3 * sizeof(double));
     }
@@ -564,7 +602,7 @@ void orc_ens_coeffs(int integrator, double* c, double* d, int* nstages) {
 }
 
 typedef struct {
-    const int64_t* off; double *pos, *vel; const double* m; double G, inv_c2, eps2, dt; int pn, integrator;
+    const int64_t* off; double *pos, *vel; const double* m; double G, inv_c, eps2, dt; int pn, integrator;
     long nsteps;
 } ens_ctx;
 
@@ -586,7 +624,7 @@ static void ens_range(void* c_, long lo, long hi) {
                     double ax = 0, ay = 0, az = 0;
                     for (long j = 0; j < n; ++j) {
                         if (j == i) continue;
-                        orc_pair_acc(c->G, c->inv_c2, c->eps2, c->pn, m[i], m[j], v + 3 * i, v + 3 * j, x + 3 * i,
+                        orc_pair_acc(c->G, c->inv_c, c->eps2, c->pn, m[i], m[j], v + 3 * i, v + 3 * j, x + 3 * i,
                                      x + 3 * j, a);
                         ax += a[0]; ay += a[1]; az += a[2];
                     }
@@ -600,9 +638,9 @@ static void ens_range(void* c_, long lo, long hi) {
 }
 
 /* Advances every system (bodies off[s]..off[s+1]-1, at most 64) nsteps. */
-void orc_ens_run(long nsys, const int64_t* off, double* pos, double* vel, const double* m, double G, double inv_c2,
+void orc_ens_run(long nsys, const int64_t* off, double* pos, double* vel, const double* m, double G, double inv_c,
                  double eps2, int pn, int integrator, double dt, long nsteps) {
-    ens_ctx c = {off, pos, vel, m, G, inv_c2, eps2, dt, pn, integrator, nsteps};
+    ens_ctx c = {off, pos, vel, m, G, inv_c, eps2, dt, pn, integrator, nsteps};
     orc_parallel(nsys, ens_range, &c);
 }
 
@@ -617,7 +655,7 @@ void orc_ens_run(long nsys, const int64_t* off, double* pos, double* vel, const 
  * velocity-dependent force at the current velocity, as the reference's
  * integrators do, so the PN part is integrated to first order in dt. */
 void orc_ens_energy(long nsys, const int64_t* off, const double* pos, const double* vel, const double* m,
-                    double G, double inv_c2, double eps2, int pn, double* e_out) {
+                    double G, double inv_c, double eps2, int pn, double* e_out) {
     for (long s = 0; s < nsys; ++s) {
         long b0 = off[s], n = off[s + 1] - b0;
         const double* x = pos + 3 * b0;
@@ -640,7 +678,7 @@ void orc_ens_energy(long nsys, const int64_t* off, const double* pos, const doub
                 e1 += G * G * mm[i] * mm[j] * (mm[i] + mm[j]) / (2.0 * r * r);
             }
         }
-        e_out[s] = e + ((pn & PN1_FLAG) ? inv_c2 * e1 : 0.0);
+        e_out[s] = e + ((pn & PN1_FLAG) ? inv_c * inv_c * e1 : 0.0);
     }
 }
 

@@ -30,6 +30,8 @@ _L = ctypes.POINTER(ctypes.c_long)
 
 NEWTON = 0x1
 PN1 = 0x10
+PN2 = 0x100
+PN25 = 0x1000
 
 
 def _p(a, t):
@@ -161,20 +163,20 @@ class Orc:
     def set_threads(self, t: int):
         self.lib.orc_set_threads(int(t))
 
-    def pair_acc(self, G, inv_c2, eps2, pn, m1, m2, v1, v2, p1, p2):
+    def pair_acc(self, G, inv_c, eps2, pn, m1, m2, v1, v2, p1, p2):
         a = np.zeros(3)
         args = [_c64(v1), _c64(v2), _c64(p1), _c64(p2)]
-        self.lib.orc_pair_acc(G, inv_c2, eps2, pn, m1, m2, *[_p(x, _D) for x in args], _p(a, _D))
+        self.lib.orc_pair_acc(G, inv_c, eps2, pn, m1, m2, *[_p(x, _D) for x in args], _p(a, _D))
         return a
 
-    def allpairs(self, pos, m, G=1.0, eps2=0.0, vel=None, inv_c2=0.0, pn=NEWTON, targets=None):
+    def allpairs(self, pos, m, G=1.0, eps2=0.0, vel=None, inv_c=0.0, pn=NEWTON, targets=None):
         pos, m = _c64(pos), _c64(m)
         vel = _c64(vel) if vel is not None else None
         n = len(m)
         tg = None if targets is None else np.ascontiguousarray(targets, dtype=np.int64)
         nt = n if tg is None else len(tg)
         acc = np.zeros((nt, 3))
-        self.lib.orc_allpairs(n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, inv_c2, eps2, pn, nt,
+        self.lib.orc_allpairs(n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, inv_c, eps2, pn, nt,
                               _p(tg, _L) if tg is not None else None, _p(acc, _D))
         return acc
 
@@ -188,12 +190,12 @@ class Orc:
         self.lib.orc_momentum(len(m), _p(vel, _D), _p(m, _D), _p(p, _D))
         return p
 
-    def kdk(self, pos, vel, m, dt, nsteps, G=1.0, eps2=0.0, inv_c2=0.0, pn=NEWTON, record_acc=False):
+    def kdk(self, pos, vel, m, dt, nsteps, G=1.0, eps2=0.0, inv_c=0.0, pn=NEWTON, record_acc=False):
         pos, vel, m = _c64(pos).copy(), _c64(vel).copy(), _c64(m)
         n = len(m)
         acc = np.zeros((n, 3))
         accs = np.zeros((nsteps, n, 3)) if record_acc else None
-        self.lib.orc_kdk(n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, inv_c2, eps2, pn, dt, nsteps,
+        self.lib.orc_kdk(n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, inv_c, eps2, pn, dt, nsteps,
                          _p(acc, _D), 0, _p(accs, _D))
         return pos, vel, acc, accs
 
@@ -273,25 +275,28 @@ class Orc:
         return t
 
     # -- batched ensembles --------------------------------------------------
-    def ens_run(self, offsets, pos, vel, m, dt, nsteps, G=1.0, c=None, eps2=0.0, integrator=1):
-        """Advance every system nsteps (integrator 1 = Yoshida-4, 0 = leapfrog);
-        PN1 when c is given. Returns new (pos, vel)."""
+    def ens_run(self, offsets, pos, vel, m, dt, nsteps, G=1.0, c=None, eps2=0.0, integrator=1, pn=None):
+        """Advance every system nsteps (integrator 1 = Yoshida-4, 0 = leapfrog).
+        Force law `pn` (NEWTON | PN1 | PN2 | PN25); default NEWTON, plus PN1
+        when c is given. Returns new (pos, vel)."""
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         pos, vel, m = _c64(pos).copy(), _c64(vel).copy(), _c64(m)
-        pn = NEWTON | (PN1 if c else 0)
-        inv_c2 = 1.0 / (c * c) if c else 0.0
+        if pn is None:
+            pn = NEWTON | (PN1 if c else 0)
+        inv_c = 1.0 / c if c else 0.0
         self.lib.orc_ens_run(len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(pos, _D),
-                             _p(vel, _D), _p(m, _D), G, inv_c2, eps2, pn, integrator, dt, nsteps)
+                             _p(vel, _D), _p(m, _D), G, inv_c, eps2, pn, integrator, dt, nsteps)
         return pos, vel
 
     def ens_energy(self, offsets, pos, vel, m, G=1.0, c=None, eps2=0.0):
+        """Newtonian energy, plus the two-body 1PN energy when c is given."""
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         pos, vel, m = _c64(pos), _c64(vel), _c64(m)
         e = np.zeros(len(off) - 1)
         pn = NEWTON | (PN1 if c else 0)
-        inv_c2 = 1.0 / (c * c) if c else 0.0
+        inv_c = 1.0 / c if c else 0.0
         self.lib.orc_ens_energy(len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(pos, _D),
-                                _p(vel, _D), _p(m, _D), G, inv_c2, eps2, pn, _p(e, _D))
+                                _p(vel, _D), _p(m, _D), G, inv_c, eps2, pn, _p(e, _D))
         return e
 
     # -- adjoint -------------------------------------------------------------

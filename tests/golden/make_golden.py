@@ -18,6 +18,11 @@ Fixtures:
                             Plummer sphere with 64 duplicated positions (forces
                             Morton ties): codes, left, right, node masses/COMs.
   tree_small.npz            the same for n = 2, 3, 5, 33 and an all-equal set.
+  pn_pairs.npz              compute_gravitational on 64 seeded pairs (c = 10,
+                            eps2 = 1e-4) for force laws NEWTON|PN1, NEWTON|PN2,
+                            NEWTON|PN25 and all four terms: the force on body 1.
+
+`python tests/golden/make_golden.py pn_pairs` regenerates one fixture only.
 """
 from __future__ import annotations
 
@@ -30,7 +35,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from aster_b200 import gen  # noqa: E402
-from oracle.oracle import NEWTON, PN1, Ref  # noqa: E402
+from oracle.oracle import NEWTON, PN1, PN2, PN25, Ref  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 
@@ -96,11 +101,33 @@ def tree_fixture(ref: Ref):
     np.savez_compressed(OUT / "tree_small.npz", **small)
 
 
+PN_LAWS = {"pn1": NEWTON | PN1, "pn2": NEWTON | PN2, "pn25": NEWTON | PN25, "all": NEWTON | PN1 | PN2 | PN25}
+
+
+def pn_fixture(ref: Ref):
+    rng = np.random.default_rng(1006)
+    npair, c, eps2 = 64, 10.0, 1e-4
+    m = rng.lognormal(0.0, 0.5, (npair, 2))
+    p1 = rng.normal(0.0, 1.0, (npair, 3))
+    p2 = p1 + rng.normal(0.0, 0.5, (npair, 3))
+    v1 = rng.normal(0.0, 1.0, (npair, 3))
+    v2 = rng.normal(0.0, 1.0, (npair, 3))
+    out = dict(m=m, p1=p1, p2=p2, v1=v1, v2=v2, c=c, eps2=eps2)
+    for name, law in PN_LAWS.items():
+        ref.setup(np.stack([p1[0], p2[0]]), np.stack([v1[0], v2[0]]), m[0], G=1.0, c=c, eps2=eps2, force_law=law)
+        out[f"force_{name}"] = np.stack([ref.pair_force(m[k, 0], m[k, 1], v1[k], v2[k], p1[k], p2[k])
+                                         for k in range(npair)])
+    np.savez_compressed(OUT / "pn_pairs.npz", **out)
+
+
+FIXTURES = {"allpairs": allpairs_fixture, "leapfrog": leapfrog_fixture, "tree": tree_fixture,
+            "pn_pairs": pn_fixture}
+
+
 def main():
     ref = Ref()
-    allpairs_fixture(ref)
-    leapfrog_fixture(ref)
-    tree_fixture(ref)
+    for name in (sys.argv[1:] or FIXTURES):
+        FIXTURES[name](ref)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

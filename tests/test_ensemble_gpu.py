@@ -13,7 +13,8 @@ import numpy as np
 import pytest
 
 from aster_b200 import gen
-from aster_b200.api import (ERR_CANCELLED, FP64, LEAPFROG, MIXED, NEWTON, PN1, YOSHIDA4, AsterError, Params)
+from aster_b200.api import (ERR_CANCELLED, FP64, LEAPFROG, MIXED, NEWTON, PN1, PN2, PN25, YOSHIDA4, AsterError,
+                            Params)
 
 pytestmark = pytest.mark.gpu
 
@@ -39,6 +40,59 @@ def test_ensemble_vs_oracle(ctx, orc, prec, tol, integrator):
     op, ov = orc.ens_run(off, pos, vel, m, P.dt, 50, c=C_LIGHT, integrator=integrator)
     assert _per_system_err(gp, op, off) < tol
     assert _per_system_err(gv, ov, off) < tol
+
+
+def _strong_pn_ensemble():
+    """64 softened systems of 2..40 bodies, v ~ 1, eps = 0.1: with c = 10 the
+    2PN and 2.5PN terms change the velocities after 20 steps by up to ~10% of
+    the total change, far above the tolerances."""
+    rng = np.random.default_rng(1007)
+    sizes = rng.integers(2, 41, 64)
+    off = np.r_[0, np.cumsum(sizes)]
+    pos = rng.normal(size=(off[-1], 3))
+    vel = rng.normal(size=(off[-1], 3))
+    m = rng.uniform(0.5, 1.5, off[-1])
+    return pos, vel, m, off
+
+
+@pytest.mark.parametrize("law", [NEWTON | PN1 | PN2, NEWTON | PN1 | PN25, NEWTON | PN2 | PN25,
+                                 NEWTON | PN1 | PN2 | PN25])
+def test_higher_pn_ensemble_vs_oracle(ctx, orc, law):
+    """get_pn2 / get_pn25 pair terms (the oracle's restatement is pinned to the
+    reference in test_oracle.py). FP64 kernel: positions and velocities to
+    1e-10. Mixed kernel: the change the 2PN/2.5PN terms make to the state after
+    the run (against a run with the same law minus those terms) matches the
+    oracle's change to 1e-3 of its size."""
+    pos, vel, m, off = _strong_pn_ensemble()
+    c, eps2, dt, steps = 10.0, 1e-2, 1e-3, 20
+    base = law & ~(PN2 | PN25)
+
+    def run(prec, fl):
+        ctx.ensemble_upload(off, pos, vel, m)
+        ctx.ensemble_run(Params(G=1.0, c=c, eps2=eps2, dt=dt, force_law=fl), steps, LEAPFROG, prec)
+        return ctx.ensemble_download()
+
+    op, ov = orc.ens_run(off, pos, vel, m, dt, steps, c=c, eps2=eps2, integrator=LEAPFROG, pn=law)
+    gp, gv = run(FP64, law)
+    assert _per_system_err(gp, op, off) < 1e-10
+    assert _per_system_err(gv, ov, off) < 1e-10
+    bp, bv = orc.ens_run(off, pos, vel, m, dt, steps, c=c, eps2=eps2, integrator=LEAPFROG, pn=base)
+    assert np.linalg.norm(ov - bv) > 1e-4 * np.linalg.norm(ov - vel)  # the terms matter
+    mp, mv = run(MIXED, law)
+    mbp, mbv = run(MIXED, base)
+    dv_gpu, dv_orc = mv - mbv, ov - bv
+    assert np.linalg.norm(dv_gpu - dv_orc) < 1e-3 * np.linalg.norm(dv_orc)
+    assert _per_system_err(mv, ov, off) < 1e-5
+
+
+def test_higher_pn_is_ensemble_only(ctx):
+    pos, vel, m = gen.plummer(256, 3)
+    ctx.upload(pos, vel, m)
+    p = Params(G=1.0, c=5.0, eps2=1e-3, dt=1e-3, force_law=NEWTON | PN2)
+    for call in (lambda: ctx.allpairs(p, FP64), lambda: ctx.kdk_steps(p, 1)):
+        with pytest.raises(AsterError) as ei:
+            call()
+        assert ei.value.status == 9  # ASTER_ERR_UNSUPPORTED
 
 
 def test_newtonian_ensemble_and_edge_sizes(ctx, orc):

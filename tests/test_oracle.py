@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import golden, rel_l2
-from oracle.oracle import NEWTON, PN1, Ref
+from oracle.oracle import NEWTON, PN1, PN2, PN25, Ref
 
 
 def test_allpairs_matches_reference_golden(orc):
@@ -18,10 +18,31 @@ def test_allpairs_matches_reference_golden(orc):
 def test_pn1_matches_reference_golden(orc):
     g = golden("allpairs_plummer512.npz")
     c = float(g["c_pn"])
-    a = orc.allpairs(g["pos"], g["m"], 1.0, float(g["eps2"]), vel=g["vel_pn"], inv_c2=1.0 / c**2, pn=NEWTON | PN1)
+    a = orc.allpairs(g["pos"], g["m"], 1.0, float(g["eps2"]), vel=g["vel_pn"], inv_c=1.0 / c, pn=NEWTON | PN1)
     assert rel_l2(a, g["acc_pn1"]) < 1e-14
     newton = orc.allpairs(g["pos"], g["m"], 1.0, float(g["eps2"]))
     assert rel_l2(a, newton) > 1e-3  # the PN term is really there
+
+
+@pytest.mark.parametrize("name,law", [("pn1", NEWTON | PN1), ("pn2", NEWTON | PN2), ("pn25", NEWTON | PN25),
+                                      ("all", NEWTON | PN1 | PN2 | PN25)])
+def test_pn_terms_match_reference_golden(orc, name, law):
+    """get_pn1 / get_pn2 / get_pn25 through compute_gravitational (force on
+    body 1, divided by m1), c = 10 so every term is large enough to check:
+    the total to 1e-14 and each post-Newtonian term to 1e-11 of its own size."""
+    d = golden("pn_pairs.npz")
+    inv_c, eps2 = 1.0 / float(d["c"]), float(d["eps2"])
+
+    def acc(pn):
+        return np.stack([orc.pair_acc(1.0, inv_c, eps2, pn, d["m"][k, 0], d["m"][k, 1], d["v1"][k], d["v2"][k],
+                                      d["p1"][k], d["p2"][k]) for k in range(len(d["m"]))])
+
+    ref = d[f"force_{name}"] / d["m"][:, :1]
+    a, newton = acc(law), acc(NEWTON)
+    assert np.abs(a - ref).max() < 1e-14 * np.abs(ref).max()
+    term = ref - newton
+    assert np.linalg.norm(term) > 1e-4 * np.linalg.norm(newton)  # the term is really there
+    assert np.abs((a - newton) - term).max() < 1e-11 * np.abs(term).max()
 
 
 def test_reference_energy_form(orc):
