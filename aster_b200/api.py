@@ -40,7 +40,7 @@ ERR_CANCELLED = 8
 EXPORTS = [
     "aster_strerror", "aster_version", "aster_ctx_create", "aster_ctx_destroy", "aster_state_upload",
     "aster_state_download", "aster_state_size", "aster_allpairs", "aster_allpairs_targets", "aster_lbvh_build",
-    "aster_lbvh_forces", "aster_kdk_steps", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
+    "aster_lbvh_forces", "aster_kdk_steps", "aster_saba_steps", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
     "aster_ensemble_download", "aster_ensemble_run", "aster_ensemble_energy", "aster_ensemble_cancel",
     "aster_adjoint_leapfrog",
 ]
@@ -117,6 +117,8 @@ def load_library(path: Path | str | None = None) -> ctypes.CDLL:
     lib.aster_lbvh_build.argtypes = [vp, ctypes.POINTER(CParams), ctypes.POINTER(CTreeView)]
     lib.aster_lbvh_forces.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, vp, vp]
     lib.aster_kdk_steps.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.aster_saba_steps.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int]
     lib.aster_energy.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.POINTER(dbl), vp]
     lib.aster_get_stats.argtypes = [vp, ctypes.POINTER(CStats)]
     lib.aster_ensemble_upload.argtypes = [vp, ctypes.c_int32, vp, vp, vp, vp]
@@ -236,6 +238,12 @@ class Context:
     def kdk_steps(self, p: Params, nsteps: int, solver: int = SOLVER_ALLPAIRS, precision: int = FP64):
         cp = p.c_struct()
         self._check(self.lib.aster_kdk_steps(self.h, ctypes.byref(cp), solver, precision, nsteps), "aster_kdk_steps")
+
+    def saba_steps(self, p: Params, order: int, nsteps: int, solver: int = SOLVER_ALLPAIRS, precision: int = FP64):
+        """nsteps of SABA_order (1..10; order 1 is the reference's Euler step)."""
+        cp = p.c_struct()
+        self._check(self.lib.aster_saba_steps(self.h, ctypes.byref(cp), solver, precision, order, nsteps),
+                    "aster_saba_steps")
 
     def energy(self, p: Params, ref_form: bool = False):
         e = ctypes.c_double()
@@ -378,6 +386,25 @@ class CudaKDK(Updater):
         s._ensure_uploaded()
         sol = s.solver
         s.ctx.kdk_steps(s.params(sol.force_law), nsteps, sol.kind, sol.precision)
+        s._device_newer = True
+
+
+class CudaSABA(Updater):
+    """Replaces update_SABA1..10 (src/integrators/SABA.cpp:14-553) and the
+    OpenCL SABA updater (tc_impl_cl.cpp:269-299) for order 1..10, the
+    Laskar-Robutel sequence with n force evaluations per step."""
+
+    def __init__(self, sim: "Simulation", order: int = 4):
+        super().__init__(sim)
+        if not 1 <= order <= 10:
+            raise ValueError("SABA order must be 1..10")
+        self.order = order
+
+    def update_bodies(self, nsteps: int = 1):
+        s = self._s
+        s._ensure_uploaded()
+        sol = s.solver
+        s.ctx.saba_steps(s.params(sol.force_law), self.order, nsteps, sol.kind, sol.precision)
         s._device_newer = True
 
 

@@ -118,6 +118,9 @@ int aster_allpairs_launch(aster_ctx* ctx, const aster_params* p, int precision,
                           double* out_dev /* nt*3 or null: write ctx->acc */);
 // integrate.cu
 int aster_kick_drift_launch(aster_ctx* ctx, const aster_params* p, bool want_box, bool want_mixed);
+// v += a * kick_dt (skipped when !kick), x += v * drift_dt, refresh derived copies
+int aster_kick_drift_coef(aster_ctx* ctx, double kick_dt, double drift_dt, bool kick, bool want_box,
+                          bool want_mixed);
 // lbvh.cu
 int aster_lbvh_build_dev(aster_ctx* ctx, const aster_params* p, bool box_ready);
 int aster_lbvh_walk_launch(aster_ctx* ctx, const aster_params* p, int precision,

@@ -14,9 +14,11 @@
 //
 // Energy replaces Graphs::get_total_energy (src/utils/collectors.cpp:19-53).
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <mutex>
+#include <vector>
 
 #include "aster_internal.cuh"
 
@@ -36,8 +38,10 @@ __global__ void __launch_bounds__(256) k_kick_drift(int64_t n, double half_dt, d
     double bmax = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double4 p = pm[i], v = vel[i];
-        const double4 a = acc[i];
-        v.x += a.x * half_dt; v.y += a.y * half_dt; v.z += a.z * half_dt;
+        if (acc) {  // null: drift only (no stale acceleration times zero)
+            const double4 a = acc[i];
+            v.x += a.x * half_dt; v.y += a.y * half_dt; v.z += a.z * half_dt;
+        }
         p.x += v.x * dt; p.y += v.y * dt; p.z += v.z * dt;
         pm[i] = p;
         vel[i] = v;
@@ -132,6 +136,11 @@ __global__ void k_energy_final(int nblocks, const double* __restrict__ part, dou
 }  // namespace
 
 int aster_kick_drift_launch(aster_ctx* c, const aster_params* p, bool want_box, bool want_mixed) {
+    return aster_kick_drift_coef(c, 0.5 * p->dt, p->dt, true, want_box, want_mixed);
+}
+
+// v += a * kick_dt (skipped when !kick); x += v * drift_dt.
+int aster_kick_drift_coef(aster_ctx* c, double kick_dt, double drift_dt, bool kick, bool want_box, bool want_mixed) {
     const int64_t n = c->n;
     int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 8);
     if (grid < 1) grid = 1;
@@ -143,8 +152,8 @@ int aster_kick_drift_launch(aster_ctx* c, const aster_params* p, bool want_box, 
     }
     auto* pm = c->pm.as<double4>();
     auto* v = c->vel.as<double4>();
-    auto* a = c->acc.as<double4>();
-    const double h = 0.5 * p->dt, dt = p->dt;
+    auto* a = kick ? c->acc.as<double4>() : nullptr;
+    const double h = kick_dt, dt = drift_dt;
     if (want_mixed && want_box)
         k_kick_drift<true, true><<<grid, 256, 0, c->stream>>>(n, h, dt, pm, v, a, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), box);
     else if (want_mixed)
@@ -243,6 +252,115 @@ extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, 
         delete tm;
     }
     c->acc_valid = st == ASTER_OK;
+    c->tree.built = false;
+    return st;
+}
+
+// SABA_n drift/kick coefficients (Laskar & Robutel 2001): with x_1 < ... < x_n
+// the Gauss-Legendre nodes on [0,1] and w_k the weights, the drifts are
+// c_1 = x_1, c_{k+1} = x_{k+1} - x_k, c_{n+1} = 1 - x_n and the kicks d_k = w_k
+// (the values include/Aster/physics/coeffs.h:8-161 tabulates, there to 35
+// digits). Nodes by Newton's method on the Legendre three-term recurrence in
+// long double, then rounded once. Returns the number of kicks.
+static int saba_coeffs(int order, double* c, double* d) {
+    const int n = order;
+    long double x[10] = {0}, w[10] = {0};
+    const long double pi = 3.141592653589793238462643383279502884L;
+    auto legendre = [n](long double z, long double& dp) {
+        long double p0 = 1.0L, p1 = z;
+        for (int k = 2; k <= n; ++k) {
+            const long double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+            p0 = p1;
+            p1 = p2;
+        }
+        dp = n * (z * p1 - p0) / (z * z - 1.0L);
+        return p1;
+    };
+    for (int i = 0; i < n; ++i) {
+        long double z = std::cos(pi * (i + 0.75L) / (n + 0.5L)), dp = 1.0L;
+        for (int it = 0; it < 100; ++it) {
+            const long double dz = legendre(z, dp) / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-19L) break;
+        }
+        legendre(z, dp);
+        x[n - 1 - i] = 0.5L * (1.0L + z);  // ascending on [0,1]
+        w[n - 1 - i] = 1.0L / ((1.0L - z * z) * dp * dp);
+    }
+    c[0] = (double)x[0];
+    for (int k = 1; k < n; ++k) c[k] = (double)(x[k] - x[k - 1]);
+    c[n] = (double)(1.0L - x[n - 1]);
+    for (int k = 0; k < n; ++k) d[k] = (double)w[k];
+    return n;
+}
+
+// Replaces update_SABA1..10 (src/integrators/SABA.cpp:14-553) and the OpenCL
+// SABA updater (src/utils/tc_impl_cl.cpp:270-299 + generalized_intgrt3d.cl.h).
+// Order n >= 2, per step: drift c_1; then n times: forces, kick d_k and drift
+// c_{k+1} in one launch. Order 1 is the reference's SABA1 = update_euler:
+// forces, v += a dt, x += v dt. Differences from the reference, on purpose:
+// its OpenCL updater binds d to the kernel's c argument and c to d (the kick
+// uses the drift coefficient and vice versa) and evaluates the forces twice
+// per slot; its CPU update_SABA6 kicks with d2 where the sequence (and its own
+// coefficient table) has d3. Here every order follows the published sequence.
+extern "C" int aster_saba_steps(aster_ctx* c, const aster_params* p, int solver, int precision, int order,
+                                int nsteps) {
+    if (!c || nsteps < 0 || order < 1 || order > 10) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (c->n <= 0) return ASTER_ERR_NO_STATE;
+    if (solver != ASTER_SOLVER_ALLPAIRS && solver != ASTER_SOLVER_LBVH) return ASTER_ERR_INVALID_ARG;
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    if (solver == ASTER_SOLVER_LBVH && (p->force_law & ASTER_PN1)) return ASTER_ERR_UNSUPPORTED;
+    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;  // ensemble only
+    double cc[11], dd[10];
+    int nk = 1;
+    if (order > 1) nk = saba_coeffs(order, cc, dd);
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    const bool lbvh = solver == ASTER_SOLVER_LBVH;
+    const bool mixed_ap = solver == ASTER_SOLVER_ALLPAIRS && precision == ASTER_MIXED;
+    PhaseTimer* tm = (int64_t)(nsteps * nk + 1) * 3 <= 2 * PhaseTimer::kMax ? new PhaseTimer() : nullptr;
+    std::vector<std::array<int, 3>> marks;
+    auto force = [&](bool box_ready) -> int {
+        int m3[3] = {-1, -1, -1};
+        ASTER_TRY(force_eval(c, p, solver, precision, false, box_ready, tm, nullptr, nullptr, m3));
+        if (tm) marks.push_back({m3[0], m3[1], m3[2]});
+        return ASTER_OK;
+    };
+    ASTER_TRY(c->red.ensure(4096));
+    unsigned long long* inter = red_inter(c);
+    ASTER_CUDA(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), c->stream));
+    cudaEventRecord(c->ev[0], c->stream);
+    const double dt = p->dt;
+    if (order == 1 && mixed_ap) ASTER_TRY(aster_refresh_mixed(c));
+    for (int s = 0; s < nsteps; ++s) {
+        if (order == 1) {
+            ASTER_TRY(force(s > 0));
+            ASTER_TRY(aster_kick_drift_coef(c, dt, dt, true, lbvh, mixed_ap));
+            continue;
+        }
+        ASTER_TRY(aster_kick_drift_coef(c, 0.0, cc[0] * dt, false, lbvh, mixed_ap));
+        for (int k = 0; k < nk; ++k) {
+            ASTER_TRY(force(true));
+            ASTER_TRY(aster_kick_drift_coef(c, dd[k] * dt, cc[k + 1] * dt, true, lbvh, mixed_ap));
+        }
+    }
+    cudaEventRecord(c->ev[1], c->stream);
+    unsigned long long ic = 0;
+    if (lbvh) ASTER_CUDA(cudaMemcpyAsync(&ic, inter, sizeof(ic), cudaMemcpyDeviceToHost, c->stream));
+    int st = aster_finish(c);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    if (lbvh) c->stats.interactions = (double)ic;
+    if (tm) {
+        for (const auto& m3 : marks) {
+            c->stats.ms_build += tm->span(m3[0], m3[1]);
+            c->stats.ms_force += tm->span(m3[1], m3[2]);
+        }
+        delete tm;
+    }
+    c->acc_valid = false;  // the last drift moved the bodies after the last force evaluation
     c->tree.built = false;
     return st;
 }

@@ -96,4 +96,24 @@ void CudaKDK::update_bodies() {
     if (st != ASTER_OK) critical_if(true, std::string("CudaKDK: ") + aster_strerror(st));
 }
 
+CudaSABA::CudaSABA(Simulation* s, CudaAllPairs* solver, int order)
+    : Updater(s, order - 1, SABA), solver_(solver), saba_order_(order) {}
+
+void CudaSABA::update_bodies() {
+    auto& b = _s->bodies;
+    if (b.positions.empty()) return;
+    if (!uploaded_) {
+        solver_->upload();
+        uploaded_ = true;
+    }
+    const aster_params p = solver_->params();
+    aster_ctx* ctx = solver_->context();
+    int st = aster_saba_steps(ctx, &p, solver_->solver_kind(), solver_->precision(), saba_order_, 1);
+    if (st == ASTER_OK) {
+        b.accs.resize(b.positions.size());
+        st = aster_state_download(ctx, &b.positions[0].x, &b.velocities[0].x, &b.accs[0].x);
+    }
+    if (st != ASTER_OK) critical_if(true, std::string("CudaSABA: ") + aster_strerror(st));
+}
+
 }  // namespace Aster

@@ -70,4 +70,19 @@ private:
     bool uploaded_ = false;
 };
 
+// Drop-in for update_SABA1..10 (src/integrators/SABA.cpp:14-553) and the
+// OpenCL SABA updater (src/utils/tc_impl_cl.cpp:269-299): one SABA_order step
+// per update_bodies() on the device, order 1..10 (the reference's
+// Updater(s, order - 1, SABA) numbering), bodies refreshed after every step.
+class CudaSABA : public Updater {
+public:
+    CudaSABA(Simulation* s, CudaAllPairs* solver, int order);
+    void update_bodies() override;
+    void invalidate() { uploaded_ = false; }
+private:
+    CudaAllPairs* solver_;
+    int saba_order_;
+    bool uploaded_ = false;
+};
+
 }  // namespace Aster

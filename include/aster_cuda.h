@@ -154,6 +154,16 @@ int aster_lbvh_forces(aster_ctx* ctx, const aster_params* p, int precision,
 int aster_kdk_steps(aster_ctx* ctx, const aster_params* p, int solver, int precision,
                     int nsteps);
 
+/* nsteps of the symplectic SABA_order integrator (order 1..10) on the
+ * resident state. Replaces update_SABA1..10 (src/integrators/SABA.cpp:14-553)
+ * and the OpenCL SABA updater (src/utils/tc_impl_cl.cpp:269-299). Order n >= 2:
+ * drift c_1, then n times (forces, kick d_k, drift c_{k+1}) with the Laskar-
+ * Robutel coefficients (Gauss-Legendre nodes and weights on [0,1]); order 1
+ * is the reference's SABA1 = update_euler (forces, v += a dt, x += v dt).
+ * n force evaluations per step; the cached acceleration is invalidated. */
+int aster_saba_steps(aster_ctx* ctx, const aster_params* p, int solver, int precision,
+                     int order, int nsteps);
+
 /* FP64 diagnostics of the current state: total energy with the Plummer
  * potential -G m_i m_j / sqrt(r^2 + eps2) (consistent with the force), total
  * momentum p[3]. ref_form = 1 uses the reference formula

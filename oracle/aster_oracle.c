@@ -26,6 +26,11 @@
  *   orc_lbvh_forces     new group-based traversal (same decisions as the GPU kernel)
  *   orc_kdk             src/physics/tool_chain_impl.cpp:169-185 restated as kick-drift-kick
  *                       with the acceleration cached across steps
+ *   orc_saba            src/integrators/SABA.cpp:14-553 (update_SABA1..10, CPU forms;
+ *                       SABA1 is update_euler, tool_chain_impl.cpp:158-167)
+ *   orc_saba_coeffs     the SABA_n drift/kick coefficients (Laskar & Robutel 2001):
+ *                       Gauss-Legendre nodes and weights on [0,1], the values
+ *                       include/Aster/physics/coeffs.h:8-161 tabulates
  *   orc_energy          Plummer-softened energy (the reference's collectors.cpp:19-53
  *                       uses -Gm_im_j/(r+softening); orc_energy_ref restates that too)
  */
@@ -248,6 +253,90 @@ void orc_kdk(long n, double* pos, double* vel, const double* m, double G, double
         orc_allpairs(n, pos, vel, m, G, inv_c, eps2, pn, 0, NULL, acc);
         for (long i = 0; i < 3 * n; ++i) vel[i] += acc[i] * h;
         if (acc_steps) memcpy(acc_steps + (size_t)k * n * 3, acc, (size_t)n * 3 * sizeof(double));
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* SABA_n                                                                    */
+/* ------------------------------------------------------------------------ */
+/* SABA_n (n >= 2): drift c1, then for k = 1..n: forces, kick d_k, drift
+ * c_{k+1}. With x_1 < ... < x_n the Gauss-Legendre nodes on [0,1] and w_k the
+ * weights: c_1 = x_1, c_{k+1} = x_{k+1} - x_k, c_{n+1} = 1 - x_n, d_k = w_k.
+ * Nodes by Newton's method on the Legendre recurrence in long double. Returns
+ * the number of kicks; c_out gets n + 1 drifts, d_out n kicks. Order 1 is the
+ * reference's SABA1 = update_euler: one kick of 1 followed by a drift of 1
+ * (c_out = {0, 1}, d_out = {1}). */
+int orc_saba_coeffs(int order, double* c_out, double* d_out) {
+    if (order < 1 || order > 10) return -1;
+    if (order == 1) { c_out[0] = 0.0; c_out[1] = 1.0; d_out[0] = 1.0; return 1; }
+    const int n = order;
+    long double x[10] = {0}, w[10] = {0};
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i < n; ++i) {
+        long double z = cosl(pi * (i + 0.75L) / (n + 0.5L)), dp = 1.0L;
+        for (int it = 0; it < 100; ++it) {
+            long double p0 = 1.0L, p1 = z;
+            for (int k = 2; k <= n; ++k) {
+                long double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1.0L);
+            long double dz = p1 / dp;
+            z -= dz;
+            if (fabsl(dz) < 1e-19L) break;
+        }
+        {
+            long double p0 = 1.0L, p1 = z;
+            for (int k = 2; k <= n; ++k) {
+                long double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1.0L);
+        }
+        /* i = 0 is the largest root: store ascending on [0,1] */
+        x[n - 1 - i] = 0.5L * (1.0L + z);
+        w[n - 1 - i] = 1.0L / ((1.0L - z * z) * dp * dp);
+    }
+    c_out[0] = (double)x[0];
+    for (int k = 1; k < n; ++k) c_out[k] = (double)(x[k] - x[k - 1]);
+    c_out[n] = (double)(1.0L - x[n - 1]);
+    for (int k = 0; k < n; ++k) d_out[k] = (double)w[k];
+    return n;
+}
+
+/* nsteps of a drift/kick sequence with all-pairs forces: drift c[0], then for
+ * k = 0..nk-1: forces, kick d[k], drift c[k+1] (the form of every
+ * update_SABAn for n >= 2, SABA.cpp:19-553). */
+void orc_saba_seq(long n, double* pos, double* vel, const double* m, double G, double inv_c, double eps2, int pn,
+                  double dt, int nk, const double* c, const double* d, int nsteps, double* acc) {
+    for (int s = 0; s < nsteps; ++s) {
+        for (long i = 0; i < 3 * n; ++i) pos[i] += vel[i] * c[0] * dt;
+        for (int k = 0; k < nk; ++k) {
+            orc_allpairs(n, pos, vel, m, G, inv_c, eps2, pn, 0, NULL, acc);
+            for (long i = 0; i < 3 * n; ++i) {
+                vel[i] += acc[i] * d[k] * dt;
+                pos[i] += vel[i] * c[k + 1] * dt;
+            }
+        }
+    }
+}
+
+/* nsteps of SABA_order with all-pairs forces. Order 1 is the reference's
+ * update_euler (forces, v += a dt, x += v dt). */
+void orc_saba(long n, double* pos, double* vel, const double* m, double G, double inv_c, double eps2, int pn,
+              double dt, int order, int nsteps, double* acc) {
+    double c[11], d[10];
+    const int nk = orc_saba_coeffs(order, c, d);
+    if (nk < 0) return;
+    if (order > 1) {
+        orc_saba_seq(n, pos, vel, m, G, inv_c, eps2, pn, dt, nk, c, d, nsteps, acc);
+        return;
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        orc_allpairs(n, pos, vel, m, G, inv_c, eps2, pn, 0, NULL, acc);
+        for (long i = 0; i < 3 * n; ++i) { vel[i] += acc[i] * dt; pos[i] += vel[i] * dt; }
     }
 }
 

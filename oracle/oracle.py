@@ -59,6 +59,8 @@ class Ref:
             lib.ref_energy.restype = ctypes.c_double
             lib.ref_bh_tree.argtypes = [_U32, _I32, _I32, _D, _D]
             lib.ref_pair_force.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D, _D, _D, _D]
+            lib.ref_saba.argtypes = [ctypes.c_int, ctypes.c_int]
+            lib.ref_saba_coeffs.argtypes = [ctypes.c_int, _D]
             Ref._lib = lib
         self.lib = Ref._lib
         self.n = 0
@@ -113,6 +115,17 @@ class Ref:
             raise RuntimeError(f"ref_bh_tree failed: {rc}")
         return dict(codes=codes, left=left, right=right, node_mass=nm, node_com=nc)
 
+    def saba(self, order, nsteps):
+        """nsteps of the reference CPU SABA_order (update_SABA1..10)."""
+        if self.lib.ref_saba(order, nsteps) != 0:
+            raise RuntimeError("ref_saba failed")
+
+    def saba_coeffs(self, order):
+        """The reference's SABA table for the order: (d, c) slot pairs."""
+        out = np.zeros(22)
+        ln = self.lib.ref_saba_coeffs(order, _p(out, _D))
+        return out[:ln].copy()
+
     def pair_force(self, m1, m2, v1, v2, p1, p2):
         f = np.zeros(3)
         args = [_c64(v1), _c64(v2), _c64(p1), _c64(p2)]
@@ -137,6 +150,12 @@ class Orc:
             lib.orc_energy.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int]
             lib.orc_energy.restype = ctypes.c_double
             lib.orc_momentum.argtypes = [ctypes.c_long, _D, _D, _D]
+            lib.orc_saba_coeffs.argtypes = [ctypes.c_int, _D, _D]
+            lib.orc_saba.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D]
+            lib.orc_saba_seq.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, _D, _D,
+                                         ctypes.c_int, _D]
             lib.orc_kdk.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_int, ctypes.c_double, ctypes.c_int, _D, ctypes.c_int, _D]
             lib.orc_morton30.argtypes = [ctypes.c_long, _D, ctypes.c_double, _U32]
@@ -189,6 +208,35 @@ class Orc:
         p = np.zeros(3)
         self.lib.orc_momentum(len(m), _p(vel, _D), _p(m, _D), _p(p, _D))
         return p
+
+    def saba_coeffs(self, order):
+        """(drifts c[0..n], kicks d[0..n-1]) of SABA_order; order 1 is Euler."""
+        c, d = np.zeros(11), np.zeros(10)
+        nk = self.lib.orc_saba_coeffs(order, _p(c, _D), _p(d, _D))
+        if nk < 0:
+            raise ValueError("order must be 1..10")
+        return c[:nk + 1].copy(), d[:nk].copy()
+
+    def saba(self, pos, vel, m, dt, order, nsteps, G=1.0, eps2=0.0, inv_c=0.0, pn=NEWTON):
+        """nsteps of SABA_order (the reference update_SABAn) with all-pairs
+        forces; returns new (pos, vel)."""
+        n = len(m)
+        pos, vel, m = _c64(pos).copy(), _c64(vel).copy(), _c64(m)
+        acc = np.zeros((n, 3))
+        self.lib.orc_saba(n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, inv_c, eps2, pn, dt, order, nsteps, _p(acc, _D))
+        return pos, vel
+
+    def saba_seq(self, pos, vel, m, dt, c, d, nsteps, G=1.0, eps2=0.0, inv_c=0.0, pn=NEWTON):
+        """nsteps of an explicit drift/kick sequence: drift c[0], then
+        (forces, kick d[k], drift c[k+1]) for every k."""
+        n = len(m)
+        c, d = _c64(c), _c64(d)
+        assert len(c) == len(d) + 1
+        pos, vel, m = _c64(pos).copy(), _c64(vel).copy(), _c64(m)
+        acc = np.zeros((n, 3))
+        self.lib.orc_saba_seq(n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, inv_c, eps2, pn, dt, len(d), _p(c, _D),
+                              _p(d, _D), nsteps, _p(acc, _D))
+        return pos, vel
 
     def kdk(self, pos, vel, m, dt, nsteps, G=1.0, eps2=0.0, inv_c=0.0, pn=NEWTON, record_acc=False):
         pos, vel, m = _c64(pos).copy(), _c64(vel).copy(), _c64(m)

@@ -9,6 +9,8 @@
 //   Barnes_Hut::compute_forces     src/solvers/barnes_hut.cpp:402-418
 //   get_morton                     src/solvers/bh_specialization.cpp:38-46
 //   update_leapfrog                src/physics/tool_chain_impl.cpp:169-185
+//   update_SABA1..10               src/integrators/SABA.cpp:14-553 (CPU forms)
+//   GPU::saba_coeffs               include/Aster/physics/coeffs.h:8-161
 //   compute_gravitational          src/physics/tool_chain_impl.cpp:120-137
 //   Graphs::get_total_energy       src/utils/collectors.cpp:19-53
 //
@@ -23,6 +25,7 @@
 #include "Aster/simulations/barnes-hut.h"
 #include "Aster/building-api/builder.h"
 #include "Aster/physics/tool-chain.h"
+#include "Aster/physics/coeffs.h"
 #include "Aster/graphs/graph_collection.h"
 #include <tbb/parallel_for.h>
 
@@ -121,6 +124,27 @@ int ref_leapfrog(int nsteps, double* acc_steps) {
         if (acc_steps) ref_get_state(nullptr, nullptr, acc_steps + (size_t)k * n * 3);
     }
     return 0;
+}
+
+// nsteps of the reference CPU SABA_order (order 1..10; SABA1 is update_euler).
+int ref_saba(int order, int nsteps) {
+    HarnessSim* s = sim();
+    if (!s->solver || order < 1 || order > 10) return -1;
+    void (*const fns[10])(Aster::Simulation*) = {Aster::update_SABA1, Aster::update_SABA2, Aster::update_SABA3,
+                                                 Aster::update_SABA4, Aster::update_SABA5, Aster::update_SABA6,
+                                                 Aster::update_SABA7, Aster::update_SABA8, Aster::update_SABA9,
+                                                 Aster::update_SABA10};
+    for (int k = 0; k < nsteps; ++k) fns[order - 1](s);
+    return 0;
+}
+
+// The reference's SABA coefficient table for order 1..10, as stored
+// ((d, c) slot pairs, d = 0 in the first slot); returns its length.
+int ref_saba_coeffs(int order, double* out) {
+    if (order < 1 || order > 10) return -1;
+    const int len = (int)Aster::GPU::saba_coeff_lng[order - 1];
+    for (int i = 0; i < len; ++i) out[i] = Aster::GPU::saba_coeffs[order - 1][i];
+    return len;
 }
 
 double ref_energy() { return Aster::Graphs::get_total_energy(sim()); }

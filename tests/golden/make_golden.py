@@ -22,6 +22,10 @@ Fixtures:
                             eps2 = 1e-4) for force laws NEWTON|PN1, NEWTON|PN2,
                             NEWTON|PN25 and all four terms: the force on body 1.
 
+  saba_plummer256.npz       update_SABA1..10 with Parallelized: 4 steps each from one
+                            N=256 Plummer state (eps2 = 1e-4, dt = 1e-3), and the
+                            reference coefficient tables (GPU::saba_coeffs).
+
 `python tests/golden/make_golden.py pn_pairs` regenerates one fixture only.
 """
 from __future__ import annotations
@@ -120,8 +124,21 @@ def pn_fixture(ref: Ref):
     np.savez_compressed(OUT / "pn_pairs.npz", **out)
 
 
+def saba_fixture(ref: Ref):
+    pos, vel, m = gen.plummer(256, 1008)
+    eps2, dt, steps = 1e-4, 1e-3, 4
+    out = dict(pos=pos, vel=vel, m=m, eps2=eps2, dt=dt, steps=steps)
+    for order in range(1, 11):
+        ref.setup(pos, vel, m, G=1.0, dt=dt, eps2=eps2)
+        ref.saba(order, steps)
+        p1, v1, _ = ref.state()
+        out[f"pos_{order}"], out[f"vel_{order}"] = p1, v1
+        out[f"coeffs_{order}"] = ref.saba_coeffs(order)
+    np.savez_compressed(OUT / "saba_plummer256.npz", **out)
+
+
 FIXTURES = {"allpairs": allpairs_fixture, "leapfrog": leapfrog_fixture, "tree": tree_fixture,
-            "pn_pairs": pn_fixture}
+            "pn_pairs": pn_fixture, "saba": saba_fixture}
 
 
 def main():

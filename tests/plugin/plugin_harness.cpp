@@ -1,8 +1,8 @@
 // Test driver for the reference-side binding (aster_b200/plugin): builds a
 // reference Aster::Simulation (the reference library compiled from its own
 // sources, oracle/_ref), attaches CudaAllPairs / CudaLBVH and either the
-// reference's own leapfrog updater or CudaKDK, runs Simulation::step() and
-// exports the bodies. TEST INFRASTRUCTURE ONLY.
+// reference's own leapfrog or SABA updater, or CudaKDK / CudaSABA, runs
+// Simulation::step() and exports the bodies. TEST INFRASTRUCTURE ONLY.
 #include <cstdint>
 #include <vector>
 
@@ -43,8 +43,13 @@ extern "C" int plg_run(int n, const double* pos, const double* vel, const double
     solver->force_law = Aster::PN_expansion_type((short)force_law);
     s->solver = solver;
     solver->load();
-    Aster::Updater* up = use_cuda_kdk ? static_cast<Aster::Updater*>(new Aster::CudaKDK(s, solver))
-                                      : new Aster::Updater(s, 0, Aster::LEAPFROG);
+    // use_cuda_kdk: 0 reference leapfrog, 1 CudaKDK, 100 + k CudaSABA(order k),
+    // 200 + k the reference's own SABA updater (update_SABAk) over the solver
+    Aster::Updater* up;
+    if (use_cuda_kdk == 1) up = new Aster::CudaKDK(s, solver);
+    else if (use_cuda_kdk > 100 && use_cuda_kdk <= 110) up = new Aster::CudaSABA(s, solver, use_cuda_kdk - 100);
+    else if (use_cuda_kdk > 200 && use_cuda_kdk <= 210) up = new Aster::Updater(s, use_cuda_kdk - 201, Aster::SABA);
+    else up = new Aster::Updater(s, 0, Aster::LEAPFROG);
     s->updater = up;
     if (nsteps == 0) solver->compute_forces();
     for (int k = 0; k < nsteps; ++k) s->step();

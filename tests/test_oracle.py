@@ -133,3 +133,59 @@ def test_live_reference_agrees(orc):
     np.testing.assert_array_equal(rt["node_com"], ot["node_com"])
     ref.setup(pos, vel, m, G=1.0, eps2=1e-4, box=B)
     assert rel_l2(orc.allpairs(pos, m, 1.0, 1e-4), ref.forces()) < 1e-14
+
+
+# ---- SABA_n (src/integrators/SABA.cpp, include/Aster/physics/coeffs.h) ------
+def _ulps(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return np.max(np.abs(a - b) / np.spacing(np.maximum(np.abs(a), np.abs(b))))
+
+
+@pytest.mark.parametrize("order", range(2, 11))
+def test_saba_coeffs_match_reference_table(orc, order):
+    """Drifts and kicks from the Gauss-Legendre rule against the reference's
+    35-digit table ((d, c) slot pairs, d = 0 first). Ours are the correctly
+    rounded values; the table's decimal literals for n <= 5 are off by up to 2
+    ulp (its SABA2 c1 ends ...7134 where (1 - 1/sqrt(3))/2 is ...7118)."""
+    tab = golden("saba_plummer256.npz")[f"coeffs_{order}"]
+    c, d = orc.saba_coeffs(order)
+    assert len(tab) == 2 * (order + 1)
+    assert tab[0] == 0.0
+    assert _ulps(c, tab[1::2]) <= 2
+    assert _ulps(d, tab[2::2]) <= 2
+    assert abs(c.sum() - 1.0) < 1e-15 and abs(d.sum() - 1.0) < 1e-15
+
+
+def test_saba1_is_reference_euler(orc):
+    tab = golden("saba_plummer256.npz")["coeffs_1"]
+    np.testing.assert_array_equal(tab, [1.0, 1.0])  # one slot: kick 1, drift 1
+    c, d = orc.saba_coeffs(1)
+    np.testing.assert_array_equal(d, [1.0])
+    np.testing.assert_array_equal(c, [0.0, 1.0])
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 4, 5, 7, 8, 9, 10])
+def test_saba_matches_reference_golden(orc, order):
+    """update_SABAn with Parallelized forces, 4 steps from one Plummer state."""
+    g = golden("saba_plummer256.npz")
+    p, v = orc.saba(g["pos"], g["vel"], g["m"], float(g["dt"]), order, int(g["steps"]), eps2=float(g["eps2"]))
+    assert rel_l2(p, g[f"pos_{order}"]) < 1e-14
+    assert rel_l2(v, g[f"vel_{order}"]) < 1e-13
+
+
+def test_reference_saba6_kick_defect(orc):
+    """The reference's CPU update_SABA6 (SABA.cpp:176-250) kicks with d2 in
+    its fourth slot where the sequence, and its own table (coeffs.h), has d3:
+    its kicks sum to 0.946 dt, not dt. Restating that one slot reproduces its
+    trajectory; the correct SABA6 (ours, on the GPU too) differs from it."""
+    g = golden("saba_plummer256.npz")
+    c, d = orc.saba_coeffs(6)
+    bad = d.copy()
+    bad[3] = d[1]
+    assert abs(bad.sum() - 0.946) < 1e-3
+    args = (g["pos"], g["vel"], g["m"], float(g["dt"]))
+    p, v = orc.saba_seq(*args, c, bad, int(g["steps"]), eps2=float(g["eps2"]))
+    assert rel_l2(p, g["pos_6"]) < 1e-14
+    assert rel_l2(v, g["vel_6"]) < 1e-13
+    p6, v6 = orc.saba(*args, 6, int(g["steps"]), eps2=float(g["eps2"]))
+    assert rel_l2(v6, g["vel_6"]) > 1e-6
