@@ -40,7 +40,7 @@ ERR_CANCELLED = 8
 EXPORTS = [
     "aster_strerror", "aster_version", "aster_ctx_create", "aster_ctx_destroy", "aster_state_upload",
     "aster_state_download", "aster_state_size", "aster_allpairs", "aster_allpairs_targets", "aster_lbvh_build",
-    "aster_lbvh_forces", "aster_kdk_steps", "aster_saba_steps", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
+    "aster_lbvh_forces", "aster_kdk_steps", "aster_saba_steps", "aster_wh_steps", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
     "aster_ensemble_download", "aster_ensemble_run", "aster_ensemble_energy", "aster_ensemble_cancel",
     "aster_adjoint_leapfrog",
 ]
@@ -119,6 +119,7 @@ def load_library(path: Path | str | None = None) -> ctypes.CDLL:
     lib.aster_kdk_steps.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.aster_saba_steps.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int]
+    lib.aster_wh_steps.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int]
     lib.aster_energy.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.POINTER(dbl), vp]
     lib.aster_get_stats.argtypes = [vp, ctypes.POINTER(CStats)]
     lib.aster_ensemble_upload.argtypes = [vp, ctypes.c_int32, vp, vp, vp, vp]
@@ -238,6 +239,11 @@ class Context:
     def kdk_steps(self, p: Params, nsteps: int, solver: int = SOLVER_ALLPAIRS, precision: int = FP64):
         cp = p.c_struct()
         self._check(self.lib.aster_kdk_steps(self.h, ctypes.byref(cp), solver, precision, nsteps), "aster_kdk_steps")
+
+    def wh_steps(self, p: Params, nsteps: int, precision: int = FP64):
+        """nsteps of the Wisdom-Holman planetary integrator (body 0 central)."""
+        cp = p.c_struct()
+        self._check(self.lib.aster_wh_steps(self.h, ctypes.byref(cp), precision, nsteps), "aster_wh_steps")
 
     def saba_steps(self, p: Params, order: int, nsteps: int, solver: int = SOLVER_ALLPAIRS, precision: int = FP64):
         """nsteps of SABA_order (1..10; order 1 is the reference's Euler step)."""
@@ -405,6 +411,18 @@ class CudaSABA(Updater):
         s._ensure_uploaded()
         sol = s.solver
         s.ctx.saba_steps(s.params(sol.force_law), self.order, nsteps, sol.kind, sol.precision)
+        s._device_newer = True
+
+
+class CudaWH(Updater):
+    """Replaces update_WH_planetary (tool_chain_impl.cpp:186-290) and its
+    OpenCL form (WH_planetary.cl.h): Wisdom-Holman with body 0 as the central
+    mass, the interaction from the solver's all-pairs kernel at its precision."""
+
+    def update_bodies(self, nsteps: int = 1):
+        s = self._s
+        s._ensure_uploaded()
+        s.ctx.wh_steps(s.params(NEWTON), nsteps, s.solver.precision)
         s._device_newer = True
 
 

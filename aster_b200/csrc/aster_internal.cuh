@@ -16,6 +16,7 @@
 #define ASTER_DEVERR_NONFINITE 0x4
 #define ASTER_DEVERR_CANCEL 0x8
 #define ASTER_DEVERR_LIST 0x10
+#define ASTER_DEVERR_KEPLER 0x20
 
 #define ASTER_TRY(...)                                    \
     do {                                                  \
@@ -82,6 +83,7 @@ struct aster_ctx {
     DevBuf targets;   // target list for aster_allpairs_targets
     DevBuf stage;     // device staging for AoS <-> SoA-4 conversion
     DevBuf red;       // small reduction buffers (box, energy)
+    DevBuf wh;        // Wisdom-Holman: reduction partials and state scalars
     bool acc_valid = false;
     int* err_dev = nullptr;     // device error flags
     int* err_host = nullptr;    // pinned copy

@@ -53,6 +53,7 @@ extern "C" const char* aster_strerror(int s) {
         case ASTER_ERR_CANCELLED: return "cancelled";
         case ASTER_ERR_UNSUPPORTED: return "unsupported option";
         case ASTER_ERR_TOO_LARGE: return "size beyond fixed capacity";
+        case ASTER_ERR_KEPLER: return "Kepler drift did not converge (or a body sits on the central mass)";
         default: return "unknown status";
     }
 }
@@ -113,7 +114,7 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->pm, &c->vel, &c->acc, &c->phi, &c->plo, &c->vf, &c->scratch, &c->targets,
-                      &c->stage, &c->red,
+                      &c->stage, &c->red, &c->wh,
                       &c->tree.codes, &c->tree.codes_alt, &c->tree.sorted_codes, &c->tree.perm,
                       &c->tree.perm_alt, &c->tree.hist, &c->tree.digit_off, &c->tree.left, &c->tree.right,
                       &c->tree.parent, &c->tree.sib, &c->tree.rlo, &c->tree.rhi, &c->tree.counters, &c->tree.node_cm,
@@ -151,6 +152,7 @@ int aster_finish(aster_ctx* c) {
     if (f & ASTER_DEVERR_TREE) return ASTER_ERR_TREE;
     if (f & ASTER_DEVERR_CANCEL) return ASTER_ERR_CANCELLED;
     if (f & ASTER_DEVERR_NONFINITE) return ASTER_ERR_NONFINITE;
+    if (f & ASTER_DEVERR_KEPLER) return ASTER_ERR_KEPLER;
     return ASTER_OK;
 }
 

@@ -17,6 +17,7 @@ __all__ = [
     "plummer",
     "exponential_disk",
     "hierarchical_ensemble",
+    "planetary_system",
     "lognormal_masses",
     "com_centre",
     "bounding_cube",
@@ -222,3 +223,48 @@ def hierarchical_ensemble(n_systems: int, seed: int, n_min: int = 3, n_max: int 
     pos -= cp[sys_of]
     vel -= cv[sys_of]
     return pos, vel, m, offsets
+
+
+def planetary_system(n_planets: int, n_particles: int, seed: int, M_star: float = 1.0, G: float = 1.0,
+                     planet_mass: tuple = (1e-5, 1e-3), a_range: tuple = (1.0, 30.0),
+                     particle_a: tuple = (0.5, 40.0), particle_e: float = 0.6, inclination: float = 0.05):
+    """A central star (body 0) with planets and massless test particles.
+
+    Planets: masses log-uniform in planet_mass, semi-major axes log-uniform in
+    a_range, e ~ U[0, 0.1]; test particles: m = 0, a log-uniform in particle_a,
+    e ~ U[0, particle_e]. All orbits: inclination ~ U[0, inclination] rad,
+    uniform node, argument of pericentre and mean anomaly; elements about mu =
+    G (M_star + m) (heliocentric), as in Murray & Dermott (1999) ch. 2. The
+    system is centred on its barycentre.
+    """
+    rng = np.random.default_rng(seed)
+    n = 1 + n_planets + n_particles
+    m = np.zeros(n)
+    m[0] = M_star
+    m[1:1 + n_planets] = np.exp(rng.uniform(np.log(planet_mass[0]), np.log(planet_mass[1]), n_planets))
+    a = np.empty(n - 1)
+    e = np.empty(n - 1)
+    a[:n_planets] = np.exp(rng.uniform(np.log(a_range[0]), np.log(a_range[1]), n_planets))
+    e[:n_planets] = rng.uniform(0.0, 0.1, n_planets)
+    a[n_planets:] = np.exp(rng.uniform(np.log(particle_a[0]), np.log(particle_a[1]), n_particles))
+    e[n_planets:] = rng.uniform(0.0, particle_e, n_particles)
+    inc = rng.uniform(0.0, inclination, n - 1)
+    node = rng.uniform(0.0, 2.0 * np.pi, n - 1)
+    argp = rng.uniform(0.0, 2.0 * np.pi, n - 1)
+    E = _kepler_E(rng.uniform(0.0, 2.0 * np.pi, n - 1), e)
+    mu = G * (M_star + m[1:])
+    xo = a * (np.cos(E) - e)
+    yo = a * np.sqrt(1.0 - e * e) * np.sin(E)
+    Edot = np.sqrt(mu / a ** 3) / (1.0 - e * np.cos(E))
+    vxo = -a * np.sin(E) * Edot
+    vyo = a * np.sqrt(1.0 - e * e) * np.cos(E) * Edot
+    cO, sO, cw, sw, ci, si = np.cos(node), np.sin(node), np.cos(argp), np.sin(argp), np.cos(inc), np.sin(inc)
+    # perifocal -> reference frame (R_z(node) R_x(inc) R_z(argp))
+    px = np.stack([cO * cw - sO * sw * ci, sO * cw + cO * sw * ci, sw * si], axis=1)
+    qx = np.stack([-cO * sw - sO * cw * ci, -sO * sw + cO * cw * ci, cw * si], axis=1)
+    pos = np.zeros((n, 3))
+    vel = np.zeros((n, 3))
+    pos[1:] = xo[:, None] * px + yo[:, None] * qx
+    vel[1:] = vxo[:, None] * px + vyo[:, None] * qx
+    pos, vel = com_centre(pos, vel, m)
+    return pos, vel, m

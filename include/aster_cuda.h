@@ -42,6 +42,8 @@ extern "C" {
 #define ASTER_ERR_CANCELLED 8      /* persistent kernel stopped by cancel flag */
 #define ASTER_ERR_UNSUPPORTED 9    /* option combination not implemented       */
 #define ASTER_ERR_TOO_LARGE 10     /* size beyond a fixed capacity             */
+#define ASTER_ERR_KEPLER 11        /* Kepler drift: no convergence, or a body at
+                                      the central mass's position             */
 
 /* ---- force law bits: the reference PN_expansion_type bitmask
  *      (include/Aster/simulations/basic.h:39-53) ------------------------- */
@@ -163,6 +165,18 @@ int aster_kdk_steps(aster_ctx* ctx, const aster_params* p, int solver, int preci
  * n force evaluations per step; the cached acceleration is invalidated. */
 int aster_saba_steps(aster_ctx* ctx, const aster_params* p, int solver, int precision,
                      int order, int nsteps);
+
+/* nsteps of the Wisdom-Holman planetary integrator: body 0 is the central mass
+ * (positive), every other body moves on a Kepler orbit about it (universal
+ * variables, on the device) perturbed by the others' Newtonian attraction (the
+ * all-pairs kernel at `precision`, softened by eps2). Democratic heliocentric
+ * splitting, one interaction evaluation per step. Replaces update_WH_planetary
+ * (src/physics/tool_chain_impl.cpp:186-290) and its OpenCL form
+ * (include/Aster/kernels/WH_planetary.cl.h), whose kick re-applies the
+ * central attraction. Newtonian force law only. ASTER_ERR_KEPLER when a Kepler
+ * drift does not converge or a body sits on the central mass (that body is
+ * then left undrifted). The cached acceleration is invalidated. */
+int aster_wh_steps(aster_ctx* ctx, const aster_params* p, int precision, int nsteps);
 
 /* FP64 diagnostics of the current state: total energy with the Plummer
  * potential -G m_i m_j / sqrt(r^2 + eps2) (consistent with the force), total

@@ -28,6 +28,13 @@
  *                       with the acceleration cached across steps
  *   orc_saba            src/integrators/SABA.cpp:14-553 (update_SABA1..10, CPU forms;
  *                       SABA1 is update_euler, tool_chain_impl.cpp:158-167)
+ *   orc_wh              Wisdom-Holman in democratic heliocentric coordinates (Wisdom &
+ *                       Holman 1991; Duncan, Levison & Lee 1998), the published method
+ *                       the reference's update_WH_planetary (tool_chain_impl.cpp:186-290,
+ *                       WH_planetary.cl.h) aims at; its own step re-applies the central
+ *                       force in the kick, so parity is with the published method
+ *   orc_kepler          universal-variable Kepler drift (Stumpff functions, Laguerre-
+ *                       Conway iteration)
  *   orc_saba_coeffs     the SABA_n drift/kick coefficients (Laskar & Robutel 2001):
  *                       Gauss-Legendre nodes and weights on [0,1], the values
  *                       include/Aster/physics/coeffs.h:8-161 tabulates
@@ -338,6 +345,161 @@ void orc_saba(long n, double* pos, double* vel, const double* m, double G, doubl
         orc_allpairs(n, pos, vel, m, G, inv_c, eps2, pn, 0, NULL, acc);
         for (long i = 0; i < 3 * n; ++i) { vel[i] += acc[i] * dt; pos[i] += vel[i] * dt; }
     }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Wisdom-Holman (democratic heliocentric)                                  */
+/* ------------------------------------------------------------------------ */
+/* Stumpff functions c2(z) = (1 - cos sqrt z)/z and c3(z) = (sqrt z - sin sqrt z)/
+ * sqrt(z)^3 (hyperbolic forms for z < 0), by their power series near 0. */
+static void orc_stumpff(double z, double* c2, double* c3) {
+    if (fabs(z) < 0.5) {
+        double t2 = 0.5, t3 = 1.0 / 6.0, s2 = 0.0, s3 = 0.0;
+        for (int k = 1; k <= 10; ++k) {
+            s2 += t2;
+            s3 += t3;
+            t2 *= -z / ((2.0 * k + 1.0) * (2.0 * k + 2.0));
+            t3 *= -z / ((2.0 * k + 2.0) * (2.0 * k + 3.0));
+        }
+        *c2 = s2;
+        *c3 = s3;
+    } else if (z > 0.0) {
+        double s = sqrt(z), h = sin(0.5 * s);
+        *c2 = 2.0 * h * h / z;
+        *c3 = (s - sin(s)) / (z * s);
+    } else {
+        double s = sqrt(-z);
+        *c2 = (cosh(s) - 1.0) / (-z);
+        *c3 = (sinh(s) - s) / (-z * s);
+    }
+}
+
+/* Advances the relative state (r, v) along its Kepler orbit about mu for dt.
+ * Universal anomaly chi solves sqrt(mu) dt = r0 chi + s0 chi^2 c2 + (1 - a r0)
+ * chi^3 c3 (s0 = r.v / sqrt mu, a = 2/r0 - v^2/mu, z = a chi^2), by
+ * Laguerre-Conway steps from chi = sqrt(mu) dt / r0; then the f and g
+ * functions. Returns 0, or -1 (state unchanged) for r = 0 or no convergence. */
+int orc_kepler(double* r, double* v, double mu, double dt) {
+    const double r0 = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    if (!(r0 > 0.0) || !(mu > 0.0)) return -1;
+    if (dt == 0.0) return 0;
+    const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const double smu = sqrt(mu);
+    const double s0 = (r[0] * v[0] + r[1] * v[1] + r[2] * v[2]) / smu;
+    const double a = 2.0 / r0 - v2 / mu;
+    const double b = 1.0 - a * r0;
+    double chi = smu * dt / r0, c2 = 0.5, c3 = 1.0 / 6.0;
+    int ok = 0;
+    for (int it = 0; it < 64; ++it) {
+        const double z = a * chi * chi;
+        orc_stumpff(z, &c2, &c3);
+        const double F = r0 * chi + s0 * chi * chi * c2 + b * chi * chi * chi * c3 - smu * dt;
+        const double Fp = r0 + s0 * chi * (1.0 - z * c3) + b * chi * chi * c2;
+        const double Fpp = s0 * (1.0 - z * c2) + b * chi * (1.0 - z * c3);
+        const double disc = fabs(16.0 * Fp * Fp - 20.0 * F * Fpp);
+        const double den = Fp + (Fp >= 0.0 ? 1.0 : -1.0) * sqrt(disc);
+        const double d = den != 0.0 ? 5.0 * F / den : F / Fp;
+        chi -= d;
+        if (fabs(d) <= 1e-15 * (1.0 + fabs(chi))) { ok = 1; break; }
+    }
+    if (!ok || !isfinite(chi)) return -1;
+    const double z = a * chi * chi;
+    orc_stumpff(z, &c2, &c3);
+    const double f = 1.0 - chi * chi * c2 / r0;
+    const double g = dt - chi * chi * chi * c3 / smu;
+    double rn[3];
+    for (int k = 0; k < 3; ++k) rn[k] = f * r[k] + g * v[k];
+    const double rr = sqrt(rn[0] * rn[0] + rn[1] * rn[1] + rn[2] * rn[2]);
+    const double fd = smu / (rr * r0) * chi * (z * c3 - 1.0);
+    const double gd = 1.0 - chi * chi * c2 / rr;
+    for (int k = 0; k < 3; ++k) {
+        const double vn = fd * r[k] + gd * v[k];
+        r[k] = rn[k];
+        v[k] = vn;
+    }
+    return 0;
+}
+
+/* Interaction acceleration among bodies 1..n-1 (body 0 excluded as source
+ * and target): Newtonian, softened, from heliocentric positions Q. */
+static void orc_wh_interaction(long n, const double* Q, const double* m, double G, double eps2, double* a) {
+    memset(a, 0, (size_t)n * 3 * sizeof(double));
+    for (long i = 1; i < n; ++i)
+        for (long j = 1; j < n; ++j) {
+            if (j == i) continue;
+            double d[3] = {Q[3 * j] - Q[3 * i], Q[3 * j + 1] - Q[3 * i + 1], Q[3 * j + 2] - Q[3 * i + 2]};
+            double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
+            double inv = 1.0 / sqrt(r2);
+            double s = G * m[j] * inv * inv * inv;
+            for (int k = 0; k < 3; ++k) a[3 * i + k] += d[k] * s;
+        }
+}
+
+/* nsteps of Wisdom-Holman with body 0 as the central mass, in democratic
+ * heliocentric coordinates: Q_i = x_i - x_0, V_i = v_i - v_cm (i >= 1).
+ * H = sum_i (V_i^2/2 - G m_0/|Q_i|) m_i  [Kepler, A]
+ *   - sum_{1<=i<j} G m_i m_j / |Q_i - Q_j|  [interaction, B]
+ *   + |sum_i m_i V_i|^2 / (2 m_0)  [linear drift of the centre, C].
+ * One step: C(dt/2) B(dt/2) A(dt) C(dt/2) B(dt/2) (B and C commute: the
+ * interaction kick does not change sum_i m_i V_i, and the linear drift moves
+ * every Q_i alike, so the interaction of the step's end is the next step's). The
+ * barycentre moves uniformly; the inertial state is rebuilt at the end.
+ * Returns 0 or -1 (a Kepler drift failed). */
+int orc_wh(long n, double* pos, double* vel, const double* m, double G, double eps2, double dt, int nsteps) {
+    if (n < 2 || !(m[0] > 0.0)) return -1;
+    double M = 0.0, xc[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
+    for (long i = 0; i < n; ++i) {
+        M += m[i];
+        for (int k = 0; k < 3; ++k) { xc[k] += m[i] * pos[3 * i + k]; vc[k] += m[i] * vel[3 * i + k]; }
+    }
+    for (int k = 0; k < 3; ++k) { xc[k] /= M; vc[k] /= M; }
+    double* Q = (double*)malloc((size_t)n * 3 * sizeof(double));
+    double* V = (double*)malloc((size_t)n * 3 * sizeof(double));
+    double* a = (double*)malloc((size_t)n * 3 * sizeof(double));
+    for (long i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            Q[3 * i + k] = i ? pos[3 * i + k] - pos[k] : 0.0;
+            V[3 * i + k] = i ? vel[3 * i + k] - vc[k] : 0.0;
+        }
+    const double mu = G * m[0], h = 0.5 * dt;
+    int st = 0;
+    orc_wh_interaction(n, Q, m, G, eps2, a);
+    for (int s = 0; s < nsteps && st == 0; ++s) {
+        double P[3] = {0, 0, 0};
+        /* C(h), B(h) with the cached interaction, A(dt) */
+        for (long i = 1; i < n; ++i)
+            for (int k = 0; k < 3; ++k) P[k] += m[i] * V[3 * i + k];
+        for (long i = 1; i < n; ++i) {
+            for (int k = 0; k < 3; ++k) {
+                Q[3 * i + k] += P[k] / m[0] * h;
+                V[3 * i + k] += a[3 * i + k] * h;
+            }
+            if (orc_kepler(Q + 3 * i, V + 3 * i, mu, dt) != 0) st = -1;
+        }
+        /* C(h), then B(h) with the interaction at the new positions */
+        P[0] = P[1] = P[2] = 0.0;
+        for (long i = 1; i < n; ++i)
+            for (int k = 0; k < 3; ++k) P[k] += m[i] * V[3 * i + k];
+        for (long i = 1; i < n; ++i)
+            for (int k = 0; k < 3; ++k) Q[3 * i + k] += P[k] / m[0] * h;
+        orc_wh_interaction(n, Q, m, G, eps2, a);
+        for (long i = 1; i < n; ++i)
+            for (int k = 0; k < 3; ++k) V[3 * i + k] += a[3 * i + k] * h;
+    }
+    /* inertial state: barycentre at xc + vc t */
+    double T = dt * nsteps, S[3] = {0, 0, 0}, P[3] = {0, 0, 0};
+    for (long i = 1; i < n; ++i)
+        for (int k = 0; k < 3; ++k) { S[k] += m[i] * Q[3 * i + k]; P[k] += m[i] * V[3 * i + k]; }
+    double x0[3];
+    for (int k = 0; k < 3; ++k) x0[k] = xc[k] + vc[k] * T - S[k] / M;
+    for (int k = 0; k < 3; ++k) { pos[k] = x0[k]; vel[k] = vc[k] - P[k] / m[0]; }
+    for (long i = 1; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            pos[3 * i + k] = x0[k] + Q[3 * i + k];
+            vel[3 * i + k] = vc[k] + V[3 * i + k];
+        }
+    free(Q); free(V); free(a);
+    return st;
 }
 
 /* ------------------------------------------------------------------------ */

@@ -60,6 +60,7 @@ class Ref:
             lib.ref_bh_tree.argtypes = [_U32, _I32, _I32, _D, _D]
             lib.ref_pair_force.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D, _D, _D, _D]
             lib.ref_saba.argtypes = [ctypes.c_int, ctypes.c_int]
+            lib.ref_wh.argtypes = [ctypes.c_int]
             lib.ref_saba_coeffs.argtypes = [ctypes.c_int, _D]
             Ref._lib = lib
         self.lib = Ref._lib
@@ -120,6 +121,11 @@ class Ref:
         if self.lib.ref_saba(order, nsteps) != 0:
             raise RuntimeError("ref_saba failed")
 
+    def wh(self, nsteps):
+        """nsteps of the reference CPU update_WH_planetary (body 0 central)."""
+        if self.lib.ref_wh(nsteps) != 0:
+            raise RuntimeError("ref_wh failed")
+
     def saba_coeffs(self, order):
         """The reference's SABA table for the order: (d, c) slot pairs."""
         out = np.zeros(22)
@@ -153,6 +159,9 @@ class Orc:
             lib.orc_saba_coeffs.argtypes = [ctypes.c_int, _D, _D]
             lib.orc_saba.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D]
+            lib.orc_wh.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_int]
+            lib.orc_kepler.argtypes = [_D, _D, ctypes.c_double, ctypes.c_double]
             lib.orc_saba_seq.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, _D, _D,
                                          ctypes.c_int, _D]
@@ -225,6 +234,20 @@ class Orc:
         acc = np.zeros((n, 3))
         self.lib.orc_saba(n, _p(pos, _D), _p(vel, _D), _p(m, _D), G, inv_c, eps2, pn, dt, order, nsteps, _p(acc, _D))
         return pos, vel
+
+    def wh(self, pos, vel, m, dt, nsteps, G=1.0, eps2=0.0):
+        """nsteps of Wisdom-Holman (democratic heliocentric, body 0 central);
+        returns new (pos, vel). Raises if a Kepler drift fails."""
+        pos, vel, m = _c64(pos).copy(), _c64(vel).copy(), _c64(m)
+        if self.lib.orc_wh(len(m), _p(pos, _D), _p(vel, _D), _p(m, _D), G, eps2, dt, nsteps) != 0:
+            raise RuntimeError("orc_wh: Kepler drift failed or bad input")
+        return pos, vel
+
+    def kepler(self, r, v, mu, dt):
+        r, v = _c64(r).copy(), _c64(v).copy()
+        if self.lib.orc_kepler(_p(r, _D), _p(v, _D), mu, dt) != 0:
+            raise RuntimeError("orc_kepler failed")
+        return r, v
 
     def saba_seq(self, pos, vel, m, dt, c, d, nsteps, G=1.0, eps2=0.0, inv_c=0.0, pn=NEWTON):
         """nsteps of an explicit drift/kick sequence: drift c[0], then

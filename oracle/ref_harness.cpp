@@ -10,6 +10,7 @@
 //   get_morton                     src/solvers/bh_specialization.cpp:38-46
 //   update_leapfrog                src/physics/tool_chain_impl.cpp:169-185
 //   update_SABA1..10               src/integrators/SABA.cpp:14-553 (CPU forms)
+//   update_WH_planetary            src/physics/tool_chain_impl.cpp:186-290
 //   GPU::saba_coeffs               include/Aster/physics/coeffs.h:8-161
 //   compute_gravitational          src/physics/tool_chain_impl.cpp:120-137
 //   Graphs::get_total_energy       src/utils/collectors.cpp:19-53
@@ -145,6 +146,14 @@ int ref_saba_coeffs(int order, double* out) {
     const int len = (int)Aster::GPU::saba_coeff_lng[order - 1];
     for (int i = 0; i < len; ++i) out[i] = Aster::GPU::saba_coeffs[order - 1][i];
     return len;
+}
+
+// nsteps of the reference CPU Wisdom-Holman planetary step (body 0 central).
+int ref_wh(int nsteps) {
+    HarnessSim* s = sim();
+    if (!s->solver) return -1;
+    for (int k = 0; k < nsteps; ++k) Aster::update_WH_planetary(s);
+    return 0;
 }
 
 double ref_energy() { return Aster::Graphs::get_total_energy(sim()); }

@@ -189,3 +189,65 @@ def test_reference_saba6_kick_defect(orc):
     assert rel_l2(v, g["vel_6"]) < 1e-13
     p6, v6 = orc.saba(*args, 6, int(g["steps"]), eps2=float(g["eps2"]))
     assert rel_l2(v6, g["vel_6"]) > 1e-6
+
+
+# ---- Wisdom-Holman (published method; the reference's step is defective) ----
+def test_kepler_drift_properties(orc):
+    """Universal-variable Kepler drift: a circular orbit returns after one
+    period; energy and angular momentum are conserved on eccentric and
+    hyperbolic orbits; the drift is time-reversible."""
+    r1, v1 = orc.kepler([1.0, 0, 0], [0, 1.0, 0], 1.0, 2 * np.pi)
+    assert np.abs(r1 - [1, 0, 0]).max() < 1e-13 and np.abs(v1 - [0, 1, 0]).max() < 1e-13
+    for v0, dt in (([0, 1.3, 0.1], 3.7), ([0, 1.6, 0.0], 5.0), ([0.2, 0.4, 0.1], 11.0)):
+        r0 = np.array([1.0, 0.0, 0.0])
+        v0 = np.array(v0)
+        r1, v1 = orc.kepler(r0, v0, 1.0, dt)
+        E0, E1 = 0.5 * v0 @ v0 - 1 / np.linalg.norm(r0), 0.5 * v1 @ v1 - 1 / np.linalg.norm(r1)
+        assert abs(E1 - E0) < 1e-14
+        assert np.abs(np.cross(r1, v1) - np.cross(r0, v0)).max() < 1e-14
+        r2, v2 = orc.kepler(r1, v1, 1.0, -dt)
+        assert np.abs(r2 - r0).max() < 1e-12 and np.abs(v2 - v0).max() < 1e-12
+
+
+def test_reference_wh_double_counts_central_force(orc):
+    """The reference's update_WH_planetary (tool_chain_impl.cpp:256-290) kicks
+    with the full acceleration after a Kepler drift that already holds the
+    central pull: a circular orbit falls to ~1/3 of its radius within one
+    period. The published method (the oracle, and aster_wh_steps) keeps it."""
+    pos = np.array([[0.0, 0, 0], [1.0, 0, 0]])
+    vel = np.array([[0.0, 0, 0], [0, 1.0, 0]])
+    m = np.array([1.0, 1e-9])
+    dt = 2 * np.pi / 200
+    p, v = orc.wh(pos, vel, m, dt, 200)
+    assert np.abs(np.linalg.norm(p[1] - p[0]) - 1.0) < 1e-7
+    from oracle.oracle import Ref
+    if not Ref.available():
+        pytest.skip("reference build absent")
+    ref = Ref().setup(pos, vel, m, G=1.0, dt=dt, eps2=0.0)
+    rmin = np.inf
+    for _ in range(200):
+        ref.wh(1)
+        rp, _, _ = ref.state()
+        rmin = min(rmin, np.linalg.norm(rp[1] - rp[0]))
+    assert rmin < 0.5
+
+
+def test_wh_energy_bounded(orc):
+    """Sun, a Jupiter and a Saturn on near-circular orbits, dt ~ P_J/45:
+    energy error stays below 1e-7 over 10,000 steps (symplectic)."""
+    m = np.array([1.0, 9.5e-4, 2.9e-4])
+    pos = np.array([[0, 0, 0], [5.2, 0, 0], [0, 9.5, 0.0]])
+    vel = np.array([[0, 0, 0], [0, np.sqrt(1 / 5.2), 0], [-np.sqrt(1 / 9.5), 0, 0.0]])
+
+    def energy(p, v):
+        e = 0.5 * (m * (v * v).sum(1)).sum()
+        for i in range(3):
+            for j in range(i + 1, 3):
+                e -= m[i] * m[j] / np.linalg.norm(p[i] - p[j])
+        return e
+
+    e0 = energy(pos, vel)
+    p, v = pos, vel
+    for _ in range(10):
+        p, v = orc.wh(p, v, m, 0.5, 1000)
+        assert abs(energy(p, v) - e0) < 1e-7 * abs(e0)
