@@ -116,4 +116,24 @@ void CudaSABA::update_bodies() {
     if (st != ASTER_OK) critical_if(true, std::string("CudaSABA: ") + aster_strerror(st));
 }
 
+CudaWH::CudaWH(Simulation* s, CudaAllPairs* solver) : Updater(s, 0, WH_PLANETARY), solver_(solver) {}
+
+void CudaWH::update_bodies() {
+    auto& b = _s->bodies;
+    if (b.positions.empty()) return;
+    if (!uploaded_) {
+        solver_->upload();
+        uploaded_ = true;
+    }
+    aster_params p = solver_->params();
+    p.force_law = ASTER_NEWTON;
+    aster_ctx* ctx = solver_->context();
+    int st = aster_wh_steps(ctx, &p, solver_->precision(), 1);
+    if (st == ASTER_OK) {
+        b.accs.resize(b.positions.size());
+        st = aster_state_download(ctx, &b.positions[0].x, &b.velocities[0].x, &b.accs[0].x);
+    }
+    if (st != ASTER_OK) critical_if(true, std::string("CudaWH: ") + aster_strerror(st));
+}
+
 }  // namespace Aster

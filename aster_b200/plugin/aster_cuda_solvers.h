@@ -85,4 +85,20 @@ private:
     bool uploaded_ = false;
 };
 
+// Drop-in for update_WH_planetary (src/physics/tool_chain_impl.cpp:186-290)
+// and its OpenCL form (include/Aster/kernels/WH_planetary.cl.h): one
+// Wisdom-Holman step per update_bodies() with body 0 as the central mass (the
+// published democratic heliocentric method; the reference's step re-applies
+// the central attraction in its kick). The interaction uses the solver's
+// all-pairs kernel at its precision.
+class CudaWH : public Updater {
+public:
+    CudaWH(Simulation* s, CudaAllPairs* solver);
+    void update_bodies() override;
+    void invalidate() { uploaded_ = false; }
+private:
+    CudaAllPairs* solver_;
+    bool uploaded_ = false;
+};
+
 }  // namespace Aster

@@ -44,11 +44,13 @@ extern "C" int plg_run(int n, const double* pos, const double* vel, const double
     s->solver = solver;
     solver->load();
     // use_cuda_kdk: 0 reference leapfrog, 1 CudaKDK, 100 + k CudaSABA(order k),
-    // 200 + k the reference's own SABA updater (update_SABAk) over the solver
+    // 200 + k the reference's own SABA updater (update_SABAk) over the solver,
+    // 300 CudaWH
     Aster::Updater* up;
     if (use_cuda_kdk == 1) up = new Aster::CudaKDK(s, solver);
     else if (use_cuda_kdk > 100 && use_cuda_kdk <= 110) up = new Aster::CudaSABA(s, solver, use_cuda_kdk - 100);
     else if (use_cuda_kdk > 200 && use_cuda_kdk <= 210) up = new Aster::Updater(s, use_cuda_kdk - 201, Aster::SABA);
+    else if (use_cuda_kdk == 300) up = new Aster::CudaWH(s, solver);
     else up = new Aster::Updater(s, 0, Aster::LEAPFROG);
     s->updater = up;
     if (nsteps == 0) solver->compute_forces();

@@ -34,7 +34,7 @@ def _lib():
 def plugin_run(pos, vel, m, *, G=1.0, c=299792458.0, dt=1e-3, eps2=1e-4, theta=0.5, force_law=NEWTON, solver=0,
                precision=FP64, cuda_kdk=False, nsteps=10, updater=None):
     """updater (overrides cuda_kdk): 0 reference leapfrog, 1 CudaKDK,
-    100 + k CudaSABA(k), 200 + k the reference's update_SABAk."""
+    100 + k CudaSABA(k), 200 + k the reference's update_SABAk, 300 CudaWH."""
     lib = _lib()
     n = len(m)
     pos, vel, m = (np.ascontiguousarray(a, dtype=np.float64) for a in (pos, vel, m))
@@ -94,3 +94,13 @@ def test_cuda_saba_plugin_matches_reference_saba_updater(order):
     assert rel_l2(po, ro) < 1e-12
     assert rel_l2(pv, rv) < 1e-12
     assert rel_l2(pv, vel) > 1e-4  # the bodies moved
+
+
+def test_cuda_wh_plugin_matches_oracle(orc):
+    """CudaWH inside the reference Simulation: Simulation::step() x 4 equals
+    the published Wisdom-Holman method (the oracle)."""
+    pos, vel, m = gen.planetary_system(3, 300, 65)
+    po, pv, _ = plugin_run(pos, vel, m, dt=0.05, eps2=0.0, updater=300, nsteps=4)
+    op, ov = orc.wh(pos, vel, m, 0.05, 4)
+    assert rel_l2(po, op) < 1e-12
+    assert rel_l2(pv, ov) < 1e-12
