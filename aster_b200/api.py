@@ -29,6 +29,8 @@ NEWTON = 0x0001
 PN1 = 0x0010
 PN2 = 0x0100   # ensemble only
 PN25 = 0x1000  # ensemble only
+UPDATER_KDK, UPDATER_SABA, UPDATER_WH = 0, 1, 2
+COLLECT_ENERGY, COLLECT_ENERGY_ERROR, COLLECT_MOMENTUM, COLLECT_CENTER, COLLECT_DISTANCE = 0x1, 0x2, 0x4, 0x8, 0x10
 FP64 = 0
 MIXED = 1
 SOLVER_ALLPAIRS = 0
@@ -40,7 +42,8 @@ ERR_CANCELLED = 8
 EXPORTS = [
     "aster_strerror", "aster_version", "aster_ctx_create", "aster_ctx_destroy", "aster_state_upload",
     "aster_state_download", "aster_state_size", "aster_allpairs", "aster_allpairs_targets", "aster_lbvh_build",
-    "aster_lbvh_forces", "aster_kdk_steps", "aster_saba_steps", "aster_wh_steps", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
+    "aster_lbvh_forces", "aster_kdk_steps", "aster_saba_steps", "aster_wh_steps", "aster_record",
+    "aster_record_columns", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
     "aster_ensemble_download", "aster_ensemble_run", "aster_ensemble_energy", "aster_ensemble_cancel",
     "aster_adjoint_leapfrog",
 ]
@@ -69,6 +72,11 @@ class CTreeView(ctypes.Structure):
 class CEnsembleConfig(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int32), ("unroll", ctypes.c_int32), ("check_every", ctypes.c_int32),
                 ("use_graph", ctypes.c_int32)]
+
+
+class CRecordConfig(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in ("updater", "order", "solver", "precision", "rate", "collect",
+                                             "ref_form", "reserved")]
 
 
 class CStats(ctypes.Structure):
@@ -120,6 +128,9 @@ def load_library(path: Path | str | None = None) -> ctypes.CDLL:
     lib.aster_saba_steps.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int]
     lib.aster_wh_steps.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int]
+    lib.aster_record_columns.restype = ctypes.c_int64
+    lib.aster_record_columns.argtypes = [ctypes.POINTER(CRecordConfig), ctypes.c_int64]
+    lib.aster_record.argtypes = [vp, ctypes.POINTER(CParams), ctypes.POINTER(CRecordConfig), ctypes.c_int64, vp]
     lib.aster_energy.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.POINTER(dbl), vp]
     lib.aster_get_stats.argtypes = [vp, ctypes.POINTER(CStats)]
     lib.aster_ensemble_upload.argtypes = [vp, ctypes.c_int32, vp, vp, vp, vp]
@@ -239,6 +250,33 @@ class Context:
     def kdk_steps(self, p: Params, nsteps: int, solver: int = SOLVER_ALLPAIRS, precision: int = FP64):
         cp = p.c_struct()
         self._check(self.lib.aster_kdk_steps(self.h, ctypes.byref(cp), solver, precision, nsteps), "aster_kdk_steps")
+
+    def record(self, p: Params, nsteps: int, *, updater: int = UPDATER_KDK, order: int = 4,
+               solver: int = SOLVER_ALLPAIRS, precision: int = FP64, rate: int = 1,
+               collect: int = COLLECT_ENERGY, ref_form: bool = True):
+        """Step nsteps on the device, sampling every `rate` steps (and at step
+        0). Returns (rows, names): rows[k] = [step, columns...] as in the
+        reference's Graph CSV files; names are the column names."""
+        cfg = CRecordConfig(updater, order, solver, precision, rate, collect, int(ref_form), 0)
+        ncol = self.lib.aster_record_columns(ctypes.byref(cfg), self.n)
+        if ncol < 1:
+            raise AsterError(1, "aster_record_columns", "invalid argument")
+        rows = np.empty((nsteps // max(rate, 1) + 1, ncol))
+        cp = p.c_struct()
+        self._check(self.lib.aster_record(self.h, ctypes.byref(cp), ctypes.byref(cfg), nsteps, _ptr(rows)),
+                    "aster_record")
+        names = ["time"]
+        if collect & COLLECT_ENERGY:
+            names.append("energy")
+        if collect & COLLECT_ENERGY_ERROR:
+            names.append("energy_error")
+        if collect & COLLECT_MOMENTUM:
+            names += ["px", "py", "pz"]
+        if collect & COLLECT_CENTER:
+            names += ["x_cm", "y_cm", "z_cm"]
+        if collect & COLLECT_DISTANCE:
+            names += [f"Body{i}" for i in range(self.n)]
+        return rows, names
 
     def wh_steps(self, p: Params, nsteps: int, precision: int = FP64):
         """nsteps of the Wisdom-Holman planetary integrator (body 0 central)."""
@@ -488,3 +526,20 @@ class Simulation:
         prec = abs(e1 - e0) / abs(e0) if (precision_test and e0) else 0.0
         return dict(total_time=st["ms_total"], time_per_step=st["ms_total"] / max(n, 1), initial_energy=e0,
                     final_energy=e1, precision=prec, tested_precision=precision_test)
+
+
+def graph_csv(times, values) -> str:
+    """CSV text in the layout of the reference's Graph files
+    (src/utils/graph_collection.cpp:60-150): one value per sample ->
+    "time,data" rows; one value per body per sample (FOR_EACH) -> header
+    "time,Body0,...,Body{n-1}," and rows "t,v0,...,v{n-1}"."""
+    times = np.asarray(times)
+    values = np.asarray(values)
+    out = []
+    if values.ndim == 1:
+        out.append("time,data\n")
+        out += [f"{int(t)},{v!r}\n" for t, v in zip(times, values.tolist())]
+    else:
+        out.append("time," + "".join(f"Body{i}," for i in range(values.shape[1])) + "\n")
+        out += [f"{int(t)}," + ",".join(repr(x) for x in row) + "\n" for t, row in zip(times, values.tolist())]
+    return "".join(out)

@@ -84,6 +84,7 @@ struct aster_ctx {
     DevBuf stage;     // device staging for AoS <-> SoA-4 conversion
     DevBuf red;       // small reduction buffers (box, energy)
     DevBuf wh;        // Wisdom-Holman: reduction partials and state scalars
+    DevBuf rec;       // aster_record: the sample table and its reductions
     bool acc_valid = false;
     int* err_dev = nullptr;     // device error flags
     int* err_host = nullptr;    // pinned copy
@@ -120,6 +121,14 @@ int aster_allpairs_launch(aster_ctx* ctx, const aster_params* p, int precision,
                           double* out_dev /* nt*3 or null: write ctx->acc */);
 // integrate.cu
 int aster_kick_drift_launch(aster_ctx* ctx, const aster_params* p, bool want_box, bool want_mixed);
+// Enqueue-only cores of the stepping entry points (argument checks included,
+// no synchronisation): used by aster_record to step and sample on the device.
+int aster_kdk_enqueue(aster_ctx* ctx, const aster_params* p, int solver, int precision, int nsteps);
+int aster_saba_enqueue(aster_ctx* ctx, const aster_params* p, int solver, int precision, int order, int nsteps);
+int aster_wh_central_mass(aster_ctx* ctx, double* m0);  // synchronises; ASTER_ERR_INVALID_ARG if <= 0
+int aster_wh_enqueue(aster_ctx* ctx, const aster_params* p, int precision, int nsteps, double m0);
+// energy and momentum into out4 (device); part: (n + 255) / 256 * 5 doubles
+int aster_energy_enqueue(aster_ctx* ctx, const aster_params* p, int ref_form, double* part, double* out4);
 // v += a * kick_dt (skipped when !kick), x += v * drift_dt, refresh derived copies
 int aster_kick_drift_coef(aster_ctx* ctx, double kick_dt, double drift_dt, bool kick, bool want_box,
                           bool want_mixed);

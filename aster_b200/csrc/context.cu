@@ -114,7 +114,7 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->pm, &c->vel, &c->acc, &c->phi, &c->plo, &c->vf, &c->scratch, &c->targets,
-                      &c->stage, &c->red, &c->wh,
+                      &c->stage, &c->red, &c->wh, &c->rec,
                       &c->tree.codes, &c->tree.codes_alt, &c->tree.sorted_codes, &c->tree.perm,
                       &c->tree.perm_alt, &c->tree.hist, &c->tree.digit_off, &c->tree.left, &c->tree.right,
                       &c->tree.parent, &c->tree.sib, &c->tree.rlo, &c->tree.rhi, &c->tree.counters, &c->tree.node_cm,

@@ -206,7 +206,27 @@ static int force_eval(aster_ctx* c, const aster_params* p, int solver, int preci
     return ASTER_OK;
 }
 
-extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps) {
+// Enqueues nsteps KDK steps (no synchronisation); marks/tm optional.
+static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps, PhaseTimer* tm,
+                    int (*marks)[3], int* nm) {
+    const bool mixed_ap = solver == ASTER_SOLVER_ALLPAIRS && precision == ASTER_MIXED;
+    int dummy[3];
+    if (!c->acc_valid) {
+        if (mixed_ap) ASTER_TRY(aster_refresh_mixed(c));
+        ASTER_TRY(force_eval(c, p, solver, precision, false, false, tm, nullptr, nullptr, tm ? marks[*nm] : dummy));
+        if (tm) ++*nm;
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        ASTER_TRY(aster_kick_drift_launch(c, p, solver == ASTER_SOLVER_LBVH, mixed_ap));
+        ASTER_TRY(force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, tm ? marks[*nm] : dummy));
+        if (tm) ++*nm;
+    }
+    c->acc_valid = true;  // a(x) of the final positions (valid once the work completes without error)
+    c->tree.built = false;
+    return ASTER_OK;
+}
+
+static int kdk_check(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps) {
     if (!c || nsteps < 0) return ASTER_ERR_INVALID_ARG;
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
@@ -214,9 +234,18 @@ extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, 
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
     if (solver == ASTER_SOLVER_LBVH && (p->force_law & ASTER_PN1)) return ASTER_ERR_UNSUPPORTED;
     if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;  // ensemble only
+    return ASTER_OK;
+}
+
+int aster_kdk_enqueue(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps) {
+    ASTER_TRY(kdk_check(c, p, solver, precision, nsteps));
+    return kdk_core(c, p, solver, precision, nsteps, nullptr, nullptr, nullptr);
+}
+
+extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps) {
+    ASTER_TRY(kdk_check(c, p, solver, precision, nsteps));
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
-    const bool mixed_ap = solver == ASTER_SOLVER_ALLPAIRS && precision == ASTER_MIXED;
     // phase timing only when the event budget covers every step
     PhaseTimer* tm = (nsteps + 1) * 3 <= 2 * PhaseTimer::kMax ? new PhaseTimer() : nullptr;
     int marks[3 * (PhaseTimer::kMax / 3 + 2)][3];
@@ -225,21 +254,17 @@ extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, 
     unsigned long long* inter = red_inter(c);  // walk interaction counter
     ASTER_CUDA(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), c->stream));
     cudaEventRecord(c->ev[0], c->stream);
-    if (!c->acc_valid) {
-        if (mixed_ap) ASTER_TRY(aster_refresh_mixed(c));
-        ASTER_TRY(force_eval(c, p, solver, precision, false, false, tm, nullptr, nullptr, marks[nm]));
-        if (tm) ++nm;
-    }
-    for (int s = 0; s < nsteps; ++s) {
-        ASTER_TRY(aster_kick_drift_launch(c, p, solver == ASTER_SOLVER_LBVH, mixed_ap));
-        ASTER_TRY(force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, marks[nm]));
-        if (tm) ++nm;
+    int st = kdk_core(c, p, solver, precision, nsteps, tm, marks, &nm);
+    if (st != ASTER_OK) {
+        delete tm;
+        c->acc_valid = false;
+        return st;
     }
     cudaEventRecord(c->ev[1], c->stream);
     unsigned long long ic = 0;
     if (solver == ASTER_SOLVER_LBVH)
         ASTER_CUDA(cudaMemcpyAsync(&ic, inter, sizeof(ic), cudaMemcpyDeviceToHost, c->stream));
-    int st = aster_finish(c);
+    st = aster_finish(c);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
     c->stats.ms_total = ms;
@@ -252,7 +277,6 @@ extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, 
         delete tm;
     }
     c->acc_valid = st == ASTER_OK;
-    c->tree.built = false;
     return st;
 }
 
@@ -294,43 +318,20 @@ static int saba_coeffs(int order, double* c, double* d) {
     return n;
 }
 
-// Replaces update_SABA1..10 (src/integrators/SABA.cpp:14-553) and the OpenCL
-// SABA updater (src/utils/tc_impl_cl.cpp:270-299 + generalized_intgrt3d.cl.h).
-// Order n >= 2, per step: drift c_1; then n times: forces, kick d_k and drift
-// c_{k+1} in one launch. Order 1 is the reference's SABA1 = update_euler:
-// forces, v += a dt, x += v dt. Differences from the reference, on purpose:
-// its OpenCL updater binds d to the kernel's c argument and c to d (the kick
-// uses the drift coefficient and vice versa) and evaluates the forces twice
-// per slot; its CPU update_SABA6 kicks with d2 where the sequence (and its own
-// coefficient table) has d3. Here every order follows the published sequence.
-extern "C" int aster_saba_steps(aster_ctx* c, const aster_params* p, int solver, int precision, int order,
-                                int nsteps) {
-    if (!c || nsteps < 0 || order < 1 || order > 10) return ASTER_ERR_INVALID_ARG;
-    ASTER_TRY(aster_check_params(p));
-    if (c->n <= 0) return ASTER_ERR_NO_STATE;
-    if (solver != ASTER_SOLVER_ALLPAIRS && solver != ASTER_SOLVER_LBVH) return ASTER_ERR_INVALID_ARG;
-    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
-    if (solver == ASTER_SOLVER_LBVH && (p->force_law & ASTER_PN1)) return ASTER_ERR_UNSUPPORTED;
-    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;  // ensemble only
+// Enqueues nsteps SABA_order steps (no synchronisation).
+static int saba_core(aster_ctx* c, const aster_params* p, int solver, int precision, int order, int nsteps,
+                     PhaseTimer* tm, std::vector<std::array<int, 3>>* marks) {
     double cc[11], dd[10];
     int nk = 1;
     if (order > 1) nk = saba_coeffs(order, cc, dd);
-    ASTER_TRY(aster_begin(c));
-    c->stats = aster_stats{};
     const bool lbvh = solver == ASTER_SOLVER_LBVH;
     const bool mixed_ap = solver == ASTER_SOLVER_ALLPAIRS && precision == ASTER_MIXED;
-    PhaseTimer* tm = (int64_t)(nsteps * nk + 1) * 3 <= 2 * PhaseTimer::kMax ? new PhaseTimer() : nullptr;
-    std::vector<std::array<int, 3>> marks;
     auto force = [&](bool box_ready) -> int {
         int m3[3] = {-1, -1, -1};
         ASTER_TRY(force_eval(c, p, solver, precision, false, box_ready, tm, nullptr, nullptr, m3));
-        if (tm) marks.push_back({m3[0], m3[1], m3[2]});
+        if (tm) marks->push_back({m3[0], m3[1], m3[2]});
         return ASTER_OK;
     };
-    ASTER_TRY(c->red.ensure(4096));
-    unsigned long long* inter = red_inter(c);
-    ASTER_CUDA(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), c->stream));
-    cudaEventRecord(c->ev[0], c->stream);
     const double dt = p->dt;
     if (order == 1 && mixed_ap) ASTER_TRY(aster_refresh_mixed(c));
     for (int s = 0; s < nsteps; ++s) {
@@ -345,10 +346,52 @@ extern "C" int aster_saba_steps(aster_ctx* c, const aster_params* p, int solver,
             ASTER_TRY(aster_kick_drift_coef(c, dd[k] * dt, cc[k + 1] * dt, true, lbvh, mixed_ap));
         }
     }
+    c->acc_valid = false;  // the last drift moved the bodies after the last force evaluation
+    c->tree.built = false;
+    return ASTER_OK;
+}
+
+static int saba_check(aster_ctx* c, const aster_params* p, int solver, int precision, int order, int nsteps) {
+    if (!c || nsteps < 0 || order < 1 || order > 10) return ASTER_ERR_INVALID_ARG;
+    return kdk_check(c, p, solver, precision, nsteps);
+}
+
+int aster_saba_enqueue(aster_ctx* c, const aster_params* p, int solver, int precision, int order, int nsteps) {
+    ASTER_TRY(saba_check(c, p, solver, precision, order, nsteps));
+    return saba_core(c, p, solver, precision, order, nsteps, nullptr, nullptr);
+}
+
+// Replaces update_SABA1..10 (src/integrators/SABA.cpp:14-553) and the OpenCL
+// SABA updater (src/utils/tc_impl_cl.cpp:269-299 + generalized_intgrt3d.cl.h).
+// Order n >= 2, per step: drift c_1; then n times: forces, kick d_k and drift
+// c_{k+1} in one launch. Order 1 is the reference's SABA1 = update_euler:
+// forces, v += a dt, x += v dt. Differences from the reference, on purpose:
+// its OpenCL updater binds d to the kernel's c argument and c to d (the kick
+// uses the drift coefficient and vice versa) and evaluates the forces twice
+// per slot; its CPU update_SABA6 kicks with d2 where the sequence (and its own
+// coefficient table) has d3. Here every order follows the published sequence.
+extern "C" int aster_saba_steps(aster_ctx* c, const aster_params* p, int solver, int precision, int order,
+                                int nsteps) {
+    ASTER_TRY(saba_check(c, p, solver, precision, order, nsteps));
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    const bool lbvh = solver == ASTER_SOLVER_LBVH;
+    const int nk = order > 1 ? order : 1;
+    PhaseTimer* tm = (int64_t)(nsteps * nk + 1) * 3 <= 2 * PhaseTimer::kMax ? new PhaseTimer() : nullptr;
+    std::vector<std::array<int, 3>> marks;
+    ASTER_TRY(c->red.ensure(4096));
+    unsigned long long* inter = red_inter(c);
+    ASTER_CUDA(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), c->stream));
+    cudaEventRecord(c->ev[0], c->stream);
+    int st = saba_core(c, p, solver, precision, order, nsteps, tm, &marks);
+    if (st != ASTER_OK) {
+        delete tm;
+        return st;
+    }
     cudaEventRecord(c->ev[1], c->stream);
     unsigned long long ic = 0;
     if (lbvh) ASTER_CUDA(cudaMemcpyAsync(&ic, inter, sizeof(ic), cudaMemcpyDeviceToHost, c->stream));
-    int st = aster_finish(c);
+    st = aster_finish(c);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
     c->stats.ms_total = ms;
@@ -360,9 +403,22 @@ extern "C" int aster_saba_steps(aster_ctx* c, const aster_params* p, int solver,
         }
         delete tm;
     }
-    c->acc_valid = false;  // the last drift moved the bodies after the last force evaluation
-    c->tree.built = false;
     return st;
+}
+
+// FP64 energy and momentum of the resident state into out4 (device:
+// energy, px, py, pz); part holds (n + 255) / 256 * 5 doubles. No sync.
+int aster_energy_enqueue(aster_ctx* c, const aster_params* p, int ref_form, double* part, double* out4) {
+    const int64_t n = c->n;
+    const int nb = (int)((n + 255) / 256);
+    if (ref_form)
+        k_energy_partial<true><<<nb, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2, part);
+    else
+        k_energy_partial<false><<<nb, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2, part);
+    ASTER_CUDA(cudaGetLastError());
+    k_energy_final<<<1, 32, 0, c->stream>>>(nb, part, p->G, out4);
+    ASTER_CUDA(cudaGetLastError());
+    return ASTER_OK;
 }
 
 extern "C" int aster_energy(aster_ctx* c, const aster_params* p, int ref_form, double* energy, double* momentum3) {
@@ -376,13 +432,7 @@ extern "C" int aster_energy(aster_ctx* c, const aster_params* p, int ref_form, d
     ASTER_TRY(c->red.ensure(4096));
     double* part = c->scratch.as<double>();
     double* out = red_energy(c);
-    if (ref_form)
-        k_energy_partial<true><<<nb, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2, part);
-    else
-        k_energy_partial<false><<<nb, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2, part);
-    ASTER_CUDA(cudaGetLastError());
-    k_energy_final<<<1, 32, 0, c->stream>>>(nb, part, p->G, out);
-    ASTER_CUDA(cudaGetLastError());
+    ASTER_TRY(aster_energy_enqueue(c, p, ref_form, part, out));
     double host[4];
     ASTER_CUDA(cudaMemcpyAsync(host, out, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     ASTER_TRY(aster_finish(c));

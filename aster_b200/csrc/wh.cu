@@ -240,7 +240,7 @@ static int wh_reduce(aster_ctx* c, const WhLayout& L, int64_t i0, const double4*
     return ASTER_OK;
 }
 
-extern "C" int aster_wh_steps(aster_ctx* c, const aster_params* p, int precision, int nsteps) {
+static int wh_check(aster_ctx* c, const aster_params* p, int precision, int nsteps) {
     if (!c || nsteps < 0) return ASTER_ERR_INVALID_ARG;
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
@@ -248,22 +248,31 @@ extern "C" int aster_wh_steps(aster_ctx* c, const aster_params* p, int precision
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
     if (p->force_law & ~ASTER_NEWTON) return ASTER_ERR_UNSUPPORTED;
     if (!(p->G > 0.0)) return ASTER_ERR_INVALID_ARG;
-    ASTER_TRY(aster_begin(c));
-    c->stats = aster_stats{};
+    return ASTER_OK;
+}
+
+// The central body's mass (synchronises the stream): must be positive.
+int aster_wh_central_mass(aster_ctx* c, double* m0) {
+    double4 b0;
+    ASTER_CUDA(cudaMemcpyAsync(&b0, c->pm.ptr, sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+    ASTER_CUDA(cudaStreamSynchronize(c->stream));
+    *m0 = b0.w;
+    return b0.w > 0.0 ? ASTER_OK : ASTER_ERR_INVALID_ARG;
+}
+
+// Enqueues nsteps Wisdom-Holman steps (no synchronisation); m0 = the central
+// mass (> 0, from aster_wh_central_mass). The state is inertial before and after.
+int aster_wh_enqueue(aster_ctx* c, const aster_params* p, int precision, int nsteps, double m0) {
+    ASTER_TRY(wh_check(c, p, precision, nsteps));
     const int64_t n = c->n;
     const int64_t nbmax = std::min<int64_t>((n + WH_BLOCK - 1) / WH_BLOCK, (int64_t)c->sm_count * 4);
     ASTER_TRY(c->wh.ensure((size_t)(4 * std::max<int64_t>(nbmax, 1) + 32) * sizeof(double)));
     const WhLayout L = wh_layout(c);
-    double4 b0;  // the central body: its mass must be positive
-    ASTER_CUDA(cudaMemcpyAsync(&b0, c->pm.ptr, sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
-    ASTER_CUDA(cudaStreamSynchronize(c->stream));
-    if (!(b0.w > 0.0)) return ASTER_ERR_INVALID_ARG;
-    const double mu = p->G * b0.w;
+    const double mu = p->G * m0;
     double4* pm = c->pm.as<double4>();
     double4* vel = c->vel.as<double4>();
     const int grid = (int)L.nb;
     const double dt = p->dt, h = 0.5 * dt;
-    cudaEventRecord(c->ev[0], c->stream);
     // barycentre: (sum m x, M) -> st[20..22], st[11]; (sum m v) -> st[12..14]
     ASTER_TRY(wh_reduce(c, L, 0, pm));
     k_wh_copy3<<<1, 32, 0, c->stream>>>(L.st, 8, 20);
@@ -276,21 +285,18 @@ extern "C" int aster_wh_steps(aster_ctx* c, const aster_params* p, int precision
     int st = ASTER_OK;
     int done = 0;  // steps completed: the barycentre advances by done * dt
     const aster_params& pk = *p;  // the interaction launch; its closing kick is dt/2
-    {
-        // interaction at the initial positions
-        if (precision == ASTER_MIXED) st = aster_refresh_mixed(c);
-        if (st == ASTER_OK) st = aster_allpairs_launch(c, &pk, precision, false, n, nullptr, nullptr);
-        for (int s = 0; s < nsteps && st == ASTER_OK; ++s, ++done) {
-            if ((st = wh_reduce(c, L, 1, vel)) != ASTER_OK) break;  // P
-            k_wh_cba<<<grid, WH_BLOCK, 0, c->stream>>>(n, pm, vel, c->acc.as<double4>(), L.st, mu, h, dt,
-                                                       c->err_dev);
-            if ((st = wh_reduce(c, L, 1, vel)) != ASTER_OK) break;  // P after the Kepler drift
-            k_wh_c<<<grid, WH_BLOCK, 0, c->stream>>>(n, pm, L.st, h);
-            c->stats.kernels += 2;
-            if (precision == ASTER_MIXED && (st = aster_refresh_mixed(c)) != ASTER_OK) break;
-            st = aster_allpairs_launch(c, &pk, precision, true, n, nullptr, nullptr);  // + closing kick B(h)
-            if (st != ASTER_OK) break;
-        }
+    // interaction at the initial positions
+    if (precision == ASTER_MIXED) st = aster_refresh_mixed(c);
+    if (st == ASTER_OK) st = aster_allpairs_launch(c, &pk, precision, false, n, nullptr, nullptr);
+    for (int s = 0; s < nsteps && st == ASTER_OK; ++s, ++done) {
+        if ((st = wh_reduce(c, L, 1, vel)) != ASTER_OK) break;  // P
+        k_wh_cba<<<grid, WH_BLOCK, 0, c->stream>>>(n, pm, vel, c->acc.as<double4>(), L.st, mu, h, dt, c->err_dev);
+        if ((st = wh_reduce(c, L, 1, vel)) != ASTER_OK) break;  // P after the Kepler drift
+        k_wh_c<<<grid, WH_BLOCK, 0, c->stream>>>(n, pm, L.st, h);
+        c->stats.kernels += 2;
+        if (precision == ASTER_MIXED && (st = aster_refresh_mixed(c)) != ASTER_OK) break;
+        st = aster_allpairs_launch(c, &pk, precision, true, n, nullptr, nullptr);  // + closing kick B(h)
+        if (st != ASTER_OK) break;
     }
     // back to the inertial state (also after an error, so the state stays meaningful)
     if (wh_reduce(c, L, 1, pm) == ASTER_OK) {  // S = sum m Q
@@ -300,13 +306,24 @@ extern "C" int aster_wh_steps(aster_ctx* c, const aster_params* p, int precision
             c->stats.kernels += 2;
         }
     }
+    c->acc_valid = false;  // acc holds the interaction, not the full acceleration
+    if (precision == ASTER_MIXED && st == ASTER_OK) st = aster_refresh_mixed(c);
+    return st;
+}
+
+extern "C" int aster_wh_steps(aster_ctx* c, const aster_params* p, int precision, int nsteps) {
+    ASTER_TRY(wh_check(c, p, precision, nsteps));
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    double m0 = 0.0;
+    ASTER_TRY(aster_wh_central_mass(c, &m0));
+    cudaEventRecord(c->ev[0], c->stream);
+    int st = aster_wh_enqueue(c, p, precision, nsteps, m0);
     cudaEventRecord(c->ev[1], c->stream);
     const int fin = aster_finish(c);
     if (st == ASTER_OK) st = fin;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
     c->stats.ms_total = ms;
-    c->acc_valid = false;  // acc holds the interaction, not the full acceleration
-    if (precision == ASTER_MIXED) aster_refresh_mixed(c);
     return st;
 }

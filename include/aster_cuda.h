@@ -178,6 +178,45 @@ int aster_saba_steps(aster_ctx* ctx, const aster_params* p, int solver, int prec
  * then left undrifted). The cached acceleration is invalidated. */
 int aster_wh_steps(aster_ctx* ctx, const aster_params* p, int precision, int nsteps);
 
+/* ---- device-resident stepping with recorded time series ---------------
+ * Replaces Simulation::step/integrate with its Graph collectors
+ * (src/utils/builder_endpoint.cpp:274-352, src/utils/graph_collection.cpp,
+ * src/utils/collectors.cpp): the reference reads the bodies back every step
+ * and evaluates the collectors on the host; here the updater advances the
+ * resident state `rate` steps at a time, collector kernels write one row per
+ * sample into a device table, and the table is copied back once. */
+#define ASTER_UPDATER_KDK 0   /* aster_kdk_steps                            */
+#define ASTER_UPDATER_SABA 1  /* aster_saba_steps (order)                   */
+#define ASTER_UPDATER_WH 2    /* aster_wh_steps (body 0 central)            */
+
+#define ASTER_COLLECT_ENERGY 0x1        /* hamiltonian_collector: total energy */
+#define ASTER_COLLECT_ENERGY_ERROR 0x2  /* error_collector: |E - E0| / |E0|, E0 at the start */
+#define ASTER_COLLECT_MOMENTUM 0x4      /* total momentum (3 columns)          */
+#define ASTER_COLLECT_CENTER 0x8        /* centre of mass (3 columns)          */
+#define ASTER_COLLECT_DISTANCE 0x10     /* distance_collector: |x_cm - x_b + 0.1| per body (n columns) */
+
+typedef struct aster_record_config {
+    int32_t updater;    /* ASTER_UPDATER_*                                     */
+    int32_t order;      /* SABA order 1..10 (ASTER_UPDATER_SABA)              */
+    int32_t solver;     /* ASTER_SOLVER_* (KDK, SABA; WH uses all-pairs)       */
+    int32_t precision;  /* ASTER_FP64 or ASTER_MIXED                           */
+    int32_t rate;       /* a sample after every `rate` steps (>= 1)           */
+    int32_t collect;    /* ASTER_COLLECT_* bits                                */
+    int32_t ref_form;   /* energy with the reference formula (1) or Plummer (0) */
+    int32_t reserved;   /* 0                                                   */
+} aster_record_config;
+
+/* Columns of one recorded row: time + the collected quantities, in the order
+ * of the bits above (the per-body distances last). */
+int64_t aster_record_columns(const aster_record_config* cfg, int64_t n);
+
+/* nsteps with cfg->updater, sampling at steps 0, rate, 2 rate, ... (nsteps /
+ * rate + 1 rows; any steps after the last sample are still taken). rows_out
+ * (host): rows x aster_record_columns doubles, row-major, each row
+ * [step, columns...] -- the rows of the reference's Graph CSV files. */
+int aster_record(aster_ctx* ctx, const aster_params* p, const aster_record_config* cfg, int64_t nsteps,
+                 double* rows_out);
+
 /* FP64 diagnostics of the current state: total energy with the Plummer
  * potential -G m_i m_j / sqrt(r^2 + eps2) (consistent with the force), total
  * momentum p[3]. ref_form = 1 uses the reference formula

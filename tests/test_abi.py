@@ -13,7 +13,7 @@ LIB = ROOT / "aster_b200" / "libaster_cuda.so"
 
 def declared():
     src = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:const\s+char\s*\*|int)\s+(aster_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const\s+char\s*\*|int|int64_t)\s+(aster_\w+)\s*\(", src, re.M)))
 
 
 def exported():
@@ -68,3 +68,11 @@ def test_params_struct_layout():
     from aster_b200 import api
     assert ctypes.sizeof(api.CParams) == 5 * 8 + 4 * 4
     assert ctypes.sizeof(api.CTreeView) == 13 * 8 + 8
+
+
+def test_graph_csv_layout():
+    """The reference Graph files: "time,data" for one value per sample, a
+    "time,Body0,...," header (trailing comma) for per-body graphs."""
+    from aster_b200.api import graph_csv
+    assert graph_csv([1, 2], [0.5, 0.25]) == "time,data\n1,0.5\n2,0.25\n"
+    assert graph_csv([3], [[1.0, 2.0]]) == "time,Body0,Body1,\n3,1.0,2.0\n"
