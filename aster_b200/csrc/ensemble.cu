@@ -132,12 +132,15 @@ __device__ __forceinline__ void pn_terms(const PnK<T>& k, const PnPair<T>& q, T&
     if (PNL == 2 && (k.f & 4)) q.pn25(k.c5, qx, qy, qz);
 }
 
+// Sums over j = j0, j0 + js, ... < n (js > 1: the lanes that share a target
+// split its sources).
 template <int PNL, int UNROLL>
-__device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int n, float4 hi, float4 lo, float4 vi, float eps2,
-                                          float G, const PnK<float>& k, float3& aN, float3& a1, float3& a2) {
+__device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int n, int j0, int js, float4 hi, float4 lo,
+                                          float4 vi, float eps2, float G, const PnK<float>& k, float3& aN, float3& a1,
+                                          float3& a2) {
     float ax = 0.f, ay = 0.f, az = 0.f, px = 0.f, py = 0.f, pz = 0.f, qx = 0.f, qy = 0.f, qz = 0.f;
 #pragma unroll UNROLL
-    for (int j = 0; j < n; ++j) {
+    for (int j = j0; j < n; j += js) {
         const float4 h = s.hi[j], l = s.lo[j];
         const float dx = (h.x - hi.x) + (l.x - lo.x);
         const float dy = (h.y - hi.y) + (l.y - lo.y);
@@ -167,12 +170,13 @@ __device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int n, float4 
 }
 
 template <int PNL, int UNROLL>
-__device__ __forceinline__ void accel_f64(const EnsSlab<false>& s, int n, double4 xi, double4 vi, double eps2,
-                                          double G, const PnK<double>& k, double& ax, double& ay, double& az) {
+__device__ __forceinline__ void accel_f64(const EnsSlab<false>& s, int n, int j0, int js, double4 xi, double4 vi,
+                                          double eps2, double G, const PnK<double>& k, double& ax, double& ay,
+                                          double& az) {
     double px = 0.0, py = 0.0, pz = 0.0, qx = 0.0, qy = 0.0, qz = 0.0;
     ax = ay = az = 0.0;
 #pragma unroll UNROLL
-    for (int j = 0; j < n; ++j) {
+    for (int j = j0; j < n; j += js) {
         const double4 xj = s.x[j];
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
@@ -215,6 +219,13 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
         const int b0 = off[sys], n = off[sys + 1] - b0;
         const bool two = n > 32;
         const bool v0 = lane < n, v1 = lane + 32 < n;
+        // the r = n - 32 bodies beyond the first 32 get lps lanes each (the
+        // largest power of two with lps * r <= 32), which split its sources
+        const int r = two ? n - 32 : 0;
+        int lps = 32;
+        while (lps > 1 && lps * r > 32) lps >>= 1;
+        const int sb = lane / lps, sub = lane & (lps - 1);
+        const bool sec = two && sb < r;
         double4 x[2], v[2];
         x[0] = v0 ? pm[b0 + lane] : make_double4(0, 0, 0, 0);
         v[0] = v0 ? vel[b0 + lane] : make_double4(0, 0, 0, 0);
@@ -264,20 +275,37 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     if (q == 1 && !two) { a[1][0] = a[1][1] = a[1][2] = 0.0; continue; }
-                    const int idx = (q ? v1 : v0) ? lane + 32 * q : 0;  // idle slots read body 0
+                    // body `lane` (q = 0, all sources); for q = 1 body 32 + sb, its
+                    // sources split among the lps lanes of group sb
+                    const int idx = q ? (sec ? 32 + sb : 0) : (v0 ? lane : 0);  // idle slots read body 0
+                    const int j0 = q ? sub : 0, js = q ? lps : 1;
+                    double sx, sy, sz;
                     if (MIXED) {
                         const EnsSlab<true>& sl = reinterpret_cast<const EnsSlab<true>&>(slab);
                         float3 aN, a1, a2;
-                        accel_f32<PNL, UNROLL>(sl, n, sl.hi[idx], sl.lo[idx], sl.v[idx], epsf, Gf, pkf, aN, a1, a2);
-                        a[q][0] = G * (((double)aN.x + (double)a1.x) + (double)a2.x);
-                        a[q][1] = G * (((double)aN.y + (double)a1.y) + (double)a2.y);
-                        a[q][2] = G * (((double)aN.z + (double)a1.z) + (double)a2.z);
+                        accel_f32<PNL, UNROLL>(sl, n, j0, js, sl.hi[idx], sl.lo[idx], sl.v[idx], epsf, Gf, pkf, aN,
+                                               a1, a2);
+                        sx = ((double)aN.x + (double)a1.x) + (double)a2.x;
+                        sy = ((double)aN.y + (double)a1.y) + (double)a2.y;
+                        sz = ((double)aN.z + (double)a1.z) + (double)a2.z;
                     } else {
                         const EnsSlab<false>& sl = reinterpret_cast<const EnsSlab<false>&>(slab);
-                        double ax, ay, az;
-                        accel_f64<PNL, UNROLL>(sl, n, sl.x[idx], sl.v[idx], eps2, G, pk, ax, ay, az);
-                        a[q][0] = G * ax; a[q][1] = G * ay; a[q][2] = G * az;
+                        accel_f64<PNL, UNROLL>(sl, n, j0, js, sl.x[idx], sl.v[idx], eps2, G, pk, sx, sy, sz);
                     }
+                    if (q == 1) {
+                        // add the lps partial sums (aligned lane groups), then lane s
+                        // (owner of body 32 + s) takes its group's total
+                        for (int o = lps >> 1; o >= 1; o >>= 1) {
+                            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+                            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+                            sz += __shfl_xor_sync(0xffffffffu, sz, o);
+                        }
+                        const int src = v1 ? lane * lps : 0;
+                        sx = __shfl_sync(0xffffffffu, sx, src);
+                        sy = __shfl_sync(0xffffffffu, sy, src);
+                        sz = __shfl_sync(0xffffffffu, sz, src);
+                    }
+                    a[q][0] = G * sx; a[q][1] = G * sy; a[q][2] = G * sz;
                 }
                 __syncwarp();
 #pragma unroll
