@@ -41,6 +41,7 @@ ERR_CANCELLED = 8
 
 EXPORTS = [
     "aster_strerror", "aster_version", "aster_ctx_create", "aster_ctx_destroy", "aster_state_upload",
+    "aster_state_upload_acc",
     "aster_state_download", "aster_state_size", "aster_allpairs", "aster_allpairs_targets", "aster_lbvh_build",
     "aster_lbvh_forces", "aster_kdk_steps", "aster_saba_steps", "aster_wh_steps", "aster_record",
     "aster_record_columns", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
@@ -118,6 +119,7 @@ def load_library(path: Path | str | None = None) -> ctypes.CDLL:
     lib.aster_ctx_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, vp]
     lib.aster_ctx_destroy.argtypes = [vp]
     lib.aster_state_upload.argtypes = [vp, i64, vp, vp, vp]
+    lib.aster_state_upload_acc.argtypes = [vp, i64, vp, vp, vp, vp]
     lib.aster_state_download.argtypes = [vp, vp, vp, vp]
     lib.aster_state_size.argtypes = [vp, ctypes.POINTER(i64)]
     lib.aster_allpairs.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, vp]
@@ -192,12 +194,19 @@ class Context:
         self.close()
 
     # -- state -----------------------------------------------------------
-    def upload(self, pos, vel, mass):
+    def upload(self, pos, vel, mass, acc=None):
+        """State to the device; acc (the bodies' current accelerations) becomes
+        the cached acceleration when given."""
         n = len(mass)
         pos = _aos(pos, n)
         vel = None if vel is None else _aos(vel, n)
         mass = np.ascontiguousarray(mass, dtype=np.float64)
-        self._check(self.lib.aster_state_upload(self.h, n, _ptr(pos), _ptr(vel), _ptr(mass)), "aster_state_upload")
+        if acc is None:
+            self._check(self.lib.aster_state_upload(self.h, n, _ptr(pos), _ptr(vel), _ptr(mass)), "aster_state_upload")
+        else:
+            acc = _aos(acc, n)
+            self._check(self.lib.aster_state_upload_acc(self.h, n, _ptr(pos), _ptr(vel), _ptr(mass), _ptr(acc)),
+                        "aster_state_upload_acc")
         self.n = n
         return self
 

@@ -208,6 +208,16 @@ __global__ void k_unpack3(int64_t n, const double4* __restrict__ src, double* __
     }
 }
 
+// AoS double3 accelerations -> the cached double4 array (w = 0); non-finite
+// values raise the error flag
+__global__ void k_pack3(int64_t n, const double* __restrict__ src, double4* __restrict__ dst, int* __restrict__ err) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = src[3 * i], y = src[3 * i + 1], z = src[3 * i + 2];
+        if (!(isfinite(x) && isfinite(y) && isfinite(z))) atomicOr(err, ASTER_DEVERR_NONFINITE);
+        dst[i] = make_double4(x, y, z, 0.0);
+    }
+}
+
 static int grid_for(aster_ctx* c, int64_t n, int block) {
     int64_t g = (n + block - 1) / block;
     int64_t cap = (int64_t)c->sm_count * 16;
@@ -222,8 +232,8 @@ int aster_refresh_mixed(aster_ctx* c) {
     return ASTER_OK;
 }
 
-extern "C" int aster_state_upload(aster_ctx* c, int64_t n, const double* pos, const double* vel,
-                                  const double* mass) {
+static int state_upload(aster_ctx* c, int64_t n, const double* pos, const double* vel, const double* mass,
+                        const double* acc) {
     if (!c || !pos || !mass || n <= 0 || n > (int64_t)1 << 30) return ASTER_ERR_INVALID_ARG;
     ASTER_TRY(aster_begin(c));
     const size_t n4d = (size_t)n * sizeof(double4), n4f = (size_t)n * sizeof(float4);
@@ -234,10 +244,11 @@ extern "C" int aster_state_upload(aster_ctx* c, int64_t n, const double* pos, co
     ASTER_TRY(c->plo.ensure(n4f));
     ASTER_TRY(c->vf.ensure(n4f));
     const size_t v3 = (size_t)n * 3 * sizeof(double);
-    ASTER_TRY(c->stage.ensure(2 * v3 + (size_t)n * sizeof(double)));
+    ASTER_TRY(c->stage.ensure(3 * v3 + (size_t)n * sizeof(double)));
     double* sp = c->stage.as<double>();
     double* sv = sp + 3 * n;
     double* sm = sv + 3 * n;
+    double* sa = sm + n;
     ASTER_CUDA(cudaMemcpyAsync(sp, pos, v3, cudaMemcpyHostToDevice, c->stream));
     if (vel) ASTER_CUDA(cudaMemcpyAsync(sv, vel, v3, cudaMemcpyHostToDevice, c->stream));
     ASTER_CUDA(cudaMemcpyAsync(sm, mass, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -245,13 +256,33 @@ extern "C" int aster_state_upload(aster_ctx* c, int64_t n, const double* pos, co
                                                              c->vel.as<double4>(), c->phi.as<float4>(),
                                                              c->plo.as<float4>(), c->vf.as<float4>(), c->err_dev);
     ASTER_CUDA(cudaGetLastError());
-    ASTER_CUDA(cudaMemsetAsync(c->acc.ptr, 0, n4d, c->stream));
+    if (acc) {
+        ASTER_CUDA(cudaMemcpyAsync(sa, acc, v3, cudaMemcpyHostToDevice, c->stream));
+        k_pack3<<<grid_for(c, n, 256), 256, 0, c->stream>>>(n, sa, c->acc.as<double4>(), c->err_dev);
+        ASTER_CUDA(cudaGetLastError());
+    } else {
+        ASTER_CUDA(cudaMemsetAsync(c->acc.ptr, 0, n4d, c->stream));
+    }
     c->n = n;
-    c->acc_valid = false;
+    c->acc_valid = acc != nullptr;
     c->tree.built = false;
     int st = aster_finish(c);
-    if (st != ASTER_OK) c->n = 0;
+    if (st != ASTER_OK) {
+        c->n = 0;
+        c->acc_valid = false;
+    }
     return st;
+}
+
+extern "C" int aster_state_upload(aster_ctx* c, int64_t n, const double* pos, const double* vel,
+                                  const double* mass) {
+    return state_upload(c, n, pos, vel, mass, nullptr);
+}
+
+extern "C" int aster_state_upload_acc(aster_ctx* c, int64_t n, const double* pos, const double* vel,
+                                      const double* mass, const double* acc) {
+    if (!acc) return ASTER_ERR_INVALID_ARG;
+    return state_upload(c, n, pos, vel, mass, acc);
 }
 
 extern "C" int aster_state_download(aster_ctx* c, double* pos, double* vel, double* acc) {

@@ -120,6 +120,14 @@ int aster_ctx_destroy(aster_ctx* ctx);
  * Invalidates the cached acceleration. */
 int aster_state_upload(aster_ctx* ctx, int64_t n, const double* pos,
                        const double* vel, const double* mass);
+/* aster_state_upload plus the bodies' current accelerations (AoS double3, the
+ * reference's BodyArray::accs): they become the cached acceleration, so the
+ * next KDK step starts with its kick instead of a force evaluation, as a
+ * device-resident run would. acc must be the acceleration of these positions
+ * under the next call's parameters (what aster_state_download returned after
+ * a KDK call, or the reference update_leapfrog's a(x_{n+1})). */
+int aster_state_upload_acc(aster_ctx* ctx, int64_t n, const double* pos,
+                           const double* vel, const double* mass, const double* acc);
 /* Device -> host copy (read_bodies_gpu, builder_endpoint.cpp:424-434); any
  * pointer may be NULL. acc is the cached acceleration of the current state. */
 int aster_state_download(aster_ctx* ctx, double* pos, double* vel, double* acc);

@@ -9,7 +9,8 @@ steps (only rounding differs); mixed 1e-6. Energy drift over 100 steps
 import numpy as np
 import pytest
 
-from aster_b200.api import FP64, MIXED, SOLVER_ALLPAIRS, Params
+from aster_b200 import gen
+from aster_b200.api import FP64, MIXED, SOLVER_ALLPAIRS, SOLVER_LBVH, Params
 from conftest import golden, rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -77,3 +78,24 @@ def test_simulation_interface(orc):
     assert sim.time_passed == 10
     op, ov, _, _ = orc.kdk(g["pos"], g["vel"], g["m"], float(g["dt"]), 10, eps2=float(g["eps2"]))
     assert rel_l2(sim.bodies.positions, op) < 1e-12
+
+
+def test_upload_with_accelerations_continues_bit_exactly(ctx):
+    """A host round trip of (positions, velocities, accelerations) through
+    aster_state_upload_acc continues exactly like the device-resident run (no
+    extra force evaluation, same cached acceleration)."""
+    from aster_b200.api import Context
+    pos, vel, m = gen.plummer(3000, 1021)
+    p = Params(G=1.0, eps2=1e-4, dt=1e-3, theta=0.5)
+    for solver, prec in ((SOLVER_ALLPAIRS, FP64), (SOLVER_LBVH, MIXED)):
+        ctx.upload(pos, vel, m)
+        ctx.kdk_steps(p, 3, solver, prec)
+        xp, xv, xa = ctx.download()
+        with Context(0) as other:
+            other.upload(xp, xv, m, acc=xa)
+            other.kdk_steps(p, 2, solver, prec)
+            op, ov, _ = other.download()
+        ctx.kdk_steps(p, 2, solver, prec)
+        cp, cv, _ = ctx.download()
+        np.testing.assert_array_equal(op, cp)
+        np.testing.assert_array_equal(ov, cv)
