@@ -397,7 +397,10 @@ __device__ __forceinline__ float4 ld_cg(const float4* p) { return __ldcg(p); }
 //     (boundary-crossing) nodes with global counters and device-scope fences.
 // sib[v] names v's sibling and side (>= 0: v is a left child), so a climb
 // reads both children without loading child[parent] first.
-constexpr int BU_LEAVES = 256;
+#ifndef ASTER_BU_LEAVES
+#define ASTER_BU_LEAVES 256
+#endif
+constexpr int BU_LEAVES = ASTER_BU_LEAVES;
 
 __device__ __forceinline__ void bu_merge(const double4 cl, const double4 cr, const float4 l0, const float4 l1,
                                          const float4 h0, const float4 h1, double4& cm, float4& lo, float4& hi) {
