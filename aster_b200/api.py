@@ -41,7 +41,7 @@ ERR_CANCELLED = 8
 
 EXPORTS = [
     "aster_strerror", "aster_version", "aster_ctx_create", "aster_ctx_destroy", "aster_state_upload",
-    "aster_state_upload_acc",
+    "aster_state_upload_acc", "aster_kdk_steps_host",
     "aster_state_download", "aster_state_size", "aster_allpairs", "aster_allpairs_targets", "aster_lbvh_build",
     "aster_lbvh_forces", "aster_kdk_steps", "aster_saba_steps", "aster_wh_steps", "aster_record",
     "aster_record_columns", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
@@ -120,6 +120,8 @@ def load_library(path: Path | str | None = None) -> ctypes.CDLL:
     lib.aster_ctx_destroy.argtypes = [vp]
     lib.aster_state_upload.argtypes = [vp, i64, vp, vp, vp]
     lib.aster_state_upload_acc.argtypes = [vp, i64, vp, vp, vp, vp]
+    lib.aster_kdk_steps_host.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_int, i64,
+                                         vp, vp, vp, vp]
     lib.aster_state_download.argtypes = [vp, vp, vp, vp]
     lib.aster_state_size.argtypes = [vp, ctypes.POINTER(i64)]
     lib.aster_allpairs.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, vp]
@@ -291,6 +293,21 @@ class Context:
         """nsteps of the Wisdom-Holman planetary integrator (body 0 central)."""
         cp = p.c_struct()
         self._check(self.lib.aster_wh_steps(self.h, ctypes.byref(cp), precision, nsteps), "aster_wh_steps")
+
+    def kdk_steps_host(self, p: Params, nsteps: int, pos, vel, acc, mass, solver: int = SOLVER_ALLPAIRS,
+                       precision: int = FP64):
+        """Host-resident loop in one call: uploads (pos, vel, mass, acc), takes
+        nsteps KDK steps and writes pos, vel, acc back in place (float64
+        C-contiguous (n, 3) arrays; acc = the accelerations of pos)."""
+        n = len(mass)
+        for a in (pos, vel, acc):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape != (n, 3):
+                raise ValueError("pos, vel, acc must be C-contiguous float64 (n, 3) arrays")
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        cp = p.c_struct()
+        self._check(self.lib.aster_kdk_steps_host(self.h, ctypes.byref(cp), solver, precision, nsteps, n, _ptr(pos),
+                                                  _ptr(vel), _ptr(acc), _ptr(mass)), "aster_kdk_steps_host")
+        self.n = n
 
     def saba_steps(self, p: Params, order: int, nsteps: int, solver: int = SOLVER_ALLPAIRS, precision: int = FP64):
         """nsteps of SABA_order (1..10; order 1 is the reference's Euler step)."""

@@ -72,6 +72,7 @@ struct aster_ctx {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t copy_stream = nullptr;  // device->host copies overlapped with compute (created on first use)
     int64_t n = 0;
     DevBuf pm;    // double4 (x, y, z, m), input order
     DevBuf vel;   // double4 (vx, vy, vz, 0)
@@ -127,6 +128,12 @@ int aster_kdk_enqueue(aster_ctx* ctx, const aster_params* p, int solver, int pre
 int aster_saba_enqueue(aster_ctx* ctx, const aster_params* p, int solver, int precision, int order, int nsteps);
 int aster_wh_central_mass(aster_ctx* ctx, double* m0);  // synchronises; ASTER_ERR_INVALID_ARG if <= 0
 int aster_wh_enqueue(aster_ctx* ctx, const aster_params* p, int precision, int nsteps, double m0);
+// host state -> device on the context stream (no synchronisation; arguments
+// checked by the caller); acc (optional) becomes the cached acceleration
+int aster_upload_enqueue(aster_ctx* ctx, int64_t n, const double* pos, const double* vel, const double* mass,
+                         const double* acc);
+// state array `which` (0 positions, 1 velocities, 2 accelerations) -> host on `stream`
+int aster_download_enqueue(aster_ctx* ctx, int which, double* host, cudaStream_t stream);
 // energy and momentum into out4 (device); part: (n + 255) / 256 * 5 doubles
 int aster_energy_enqueue(aster_ctx* ctx, const aster_params* p, int ref_form, double* part, double* out4);
 // v += a * kick_dt (skipped when !kick), x += v * drift_dt, refresh derived copies

@@ -131,6 +131,7 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
     if (c->err_dev) cudaFree(c->err_dev);
     if (c->err_host) cudaFreeHost(c->err_host);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     delete c;
     return ASTER_OK;
 }
@@ -232,10 +233,11 @@ int aster_refresh_mixed(aster_ctx* c) {
     return ASTER_OK;
 }
 
-static int state_upload(aster_ctx* c, int64_t n, const double* pos, const double* vel, const double* mass,
-                        const double* acc) {
-    if (!c || !pos || !mass || n <= 0 || n > (int64_t)1 << 30) return ASTER_ERR_INVALID_ARG;
-    ASTER_TRY(aster_begin(c));
+// Host state -> device, enqueued on the context stream (no synchronisation);
+// acc (optional) becomes the cached acceleration. The host arrays must stay
+// valid until the stream has consumed them.
+int aster_upload_enqueue(aster_ctx* c, int64_t n, const double* pos, const double* vel, const double* mass,
+                         const double* acc) {
     const size_t n4d = (size_t)n * sizeof(double4), n4f = (size_t)n * sizeof(float4);
     ASTER_TRY(c->pm.ensure(n4d));
     ASTER_TRY(c->vel.ensure(n4d));
@@ -266,12 +268,33 @@ static int state_upload(aster_ctx* c, int64_t n, const double* pos, const double
     c->n = n;
     c->acc_valid = acc != nullptr;
     c->tree.built = false;
-    int st = aster_finish(c);
+    return ASTER_OK;
+}
+
+static int state_upload(aster_ctx* c, int64_t n, const double* pos, const double* vel, const double* mass,
+                        const double* acc) {
+    if (!c || !pos || !mass || n <= 0 || n > (int64_t)1 << 30) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_begin(c));
+    int st = aster_upload_enqueue(c, n, pos, vel, mass, acc);
+    if (st == ASTER_OK) st = aster_finish(c);
     if (st != ASTER_OK) {
         c->n = 0;
         c->acc_valid = false;
     }
     return st;
+}
+
+// One of the state arrays (0 positions, 1 velocities, 2 accelerations) ->
+// host AoS double3 through the staging area, on `stream` (no synchronisation).
+int aster_download_enqueue(aster_ctx* c, int which, double* host, cudaStream_t stream) {
+    const int64_t n = c->n;
+    const size_t v3 = (size_t)n * 3 * sizeof(double);
+    const DevBuf* srcs[3] = {&c->pm, &c->vel, &c->acc};
+    double* st = c->stage.as<double>() + 3 * n * which;
+    k_unpack3<<<grid_for(c, n, 256), 256, 0, stream>>>(n, srcs[which]->as<double4>(), st);
+    ASTER_CUDA(cudaGetLastError());
+    ASTER_CUDA(cudaMemcpyAsync(host, st, v3, cudaMemcpyDeviceToHost, stream));
+    return ASTER_OK;
 }
 
 extern "C" int aster_state_upload(aster_ctx* c, int64_t n, const double* pos, const double* vel,

@@ -280,6 +280,51 @@ extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, 
     return st;
 }
 
+// Host-resident state in, nsteps KDK steps, host state out, in one call: the
+// final positions exist after the last step's kick-drift, so their copy to
+// the host runs on a second stream while the last force evaluation (tree
+// build and walk) runs; velocities and accelerations follow it.
+extern "C" int aster_kdk_steps_host(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps,
+                                    int64_t n, double* pos, double* vel, double* acc, const double* mass) {
+    if (!c || !pos || !vel || !acc || !mass || n <= 0 || n > (int64_t)1 << 30 || nsteps < 1)
+        return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (solver != ASTER_SOLVER_ALLPAIRS && solver != ASTER_SOLVER_LBVH) return ASTER_ERR_INVALID_ARG;
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    if (solver == ASTER_SOLVER_LBVH && (p->force_law & ASTER_PN1)) return ASTER_ERR_UNSUPPORTED;
+    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;
+    if (!c->copy_stream) ASTER_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    cudaEventRecord(c->ev[0], c->stream);
+    int st = aster_upload_enqueue(c, n, pos, vel, mass, acc);
+    const bool mixed_ap = solver == ASTER_SOLVER_ALLPAIRS && precision == ASTER_MIXED;
+    int dummy[3];
+    if (st == ASTER_OK && nsteps > 1) st = kdk_core(c, p, solver, precision, nsteps - 1, nullptr, nullptr, nullptr);
+    if (st == ASTER_OK) st = aster_kick_drift_launch(c, p, solver == ASTER_SOLVER_LBVH, mixed_ap);
+    if (st == ASTER_OK) {
+        // positions are final: copy them out on the second stream
+        cudaEventRecord(c->ev[2], c->stream);
+        ASTER_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev[2], 0));
+        st = aster_download_enqueue(c, 0, pos, c->copy_stream);
+    }
+    if (st == ASTER_OK) st = force_eval(c, p, solver, precision, true, true, nullptr, nullptr, nullptr, dummy);
+    if (st == ASTER_OK) st = aster_download_enqueue(c, 1, vel, c->stream);
+    if (st == ASTER_OK) st = aster_download_enqueue(c, 2, acc, c->stream);
+    cudaEventRecord(c->ev[1], c->stream);
+    const cudaError_t ce = cudaStreamSynchronize(c->copy_stream);
+    const int fin = aster_finish(c);
+    if (st == ASTER_OK && ce != cudaSuccess) st = aster_cuda_fail(ce, "cudaStreamSynchronize", __FILE__, __LINE__);
+    if (st == ASTER_OK) st = fin;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    c->acc_valid = st == ASTER_OK;
+    c->tree.built = false;
+    if (st != ASTER_OK) c->n = 0;  // the resident state is not trustworthy after a failed upload or step
+    return st;
+}
+
 // SABA_n drift/kick coefficients (Laskar & Robutel 2001): with x_1 < ... < x_n
 // the Gauss-Legendre nodes on [0,1] and w_k the weights, the drifts are
 // c_1 = x_1, c_{k+1} = x_{k+1} - x_k, c_{n+1} = 1 - x_n and the kicks d_k = w_k

@@ -331,10 +331,10 @@ def e2e_c2(ctx, p, pos, vel, m, args):
     """Same metric through the public C ABI with host buffers, as a host loop
     keeping its state in host memory would drive it: every step copies the
     state (positions, velocities, masses and the bodies' accelerations, the
-    reference BodyArray's fields) host->device from pinned memory
-    (aster_state_upload_acc), runs one KDK step, and copies positions,
-    velocities and accelerations back into the same host arrays, which are
-    the next step's input."""
+    reference BodyArray's fields) host->device from pinned memory, runs one KDK
+    step, and copies positions, velocities and accelerations back into the
+    same host arrays, which are the next step's input (aster_kdk_steps_host:
+    the positions' copy back overlaps the step's force evaluation)."""
     import ctypes
     from aster_b200.api import MIXED, SOLVER_LBVH
     n = len(m)
@@ -362,10 +362,10 @@ def e2e_c2(ctx, p, pos, vel, m, args):
         raise RuntimeError(f"e2e setup failed: {st}")
 
     def one():
-        st = lib.aster_state_upload_acc(ctx.h, n, vp(hp.ctypes.data), vp(hv.ctypes.data), vp(hm.ctypes.data),
-                                        vp(ha.ctypes.data))
-        st = st or lib.aster_kdk_steps(ctx.h, ctypes.byref(cp), SOLVER_LBVH, MIXED, 1)
-        st = st or lib.aster_state_download(ctx.h, vp(hp.ctypes.data), vp(hv.ctypes.data), vp(ha.ctypes.data))
+        # upload, one KDK step, download, in one call (the positions' copy back
+        # overlaps the force evaluation)
+        st = lib.aster_kdk_steps_host(ctx.h, ctypes.byref(cp), SOLVER_LBVH, MIXED, 1, n, vp(hp.ctypes.data),
+                                      vp(hv.ctypes.data), vp(ha.ctypes.data), vp(hm.ctypes.data))
         if st:
             raise RuntimeError(f"e2e step failed: {st}")
 

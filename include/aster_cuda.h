@@ -164,6 +164,16 @@ int aster_lbvh_forces(aster_ctx* ctx, const aster_params* p, int precision,
 int aster_kdk_steps(aster_ctx* ctx, const aster_params* p, int solver, int precision,
                     int nsteps);
 
+/* Host-resident loop in one call: uploads (pos, vel, mass, acc), takes
+ * nsteps >= 1 KDK steps and writes pos, vel, acc back (n bodies, AoS double3,
+ * acc = the accelerations of pos on input and output, as
+ * aster_state_upload_acc expects). The copy of the final positions to the host
+ * overlaps the last force evaluation. Use pinned host memory for the copies
+ * to run asynchronously. The resident state is the stepped state afterwards. */
+int aster_kdk_steps_host(aster_ctx* ctx, const aster_params* p, int solver, int precision,
+                         int nsteps, int64_t n, double* pos, double* vel, double* acc,
+                         const double* mass);
+
 /* nsteps of the symplectic SABA_order integrator (order 1..10) on the
  * resident state. Replaces update_SABA1..10 (src/integrators/SABA.cpp:14-553)
  * and the OpenCL SABA updater (src/utils/tc_impl_cl.cpp:269-299). Order n >= 2:

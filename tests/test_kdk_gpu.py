@@ -99,3 +99,23 @@ def test_upload_with_accelerations_continues_bit_exactly(ctx):
         cp, cv, _ = ctx.download()
         np.testing.assert_array_equal(op, cp)
         np.testing.assert_array_equal(ov, cv)
+
+
+def test_kdk_steps_host_equals_separate_calls(ctx):
+    """aster_kdk_steps_host (one call, the positions' copy overlapping the last
+    force evaluation) equals upload_acc + kdk_steps + download bit for bit."""
+    from aster_b200.api import Context
+    pos, vel, m = gen.plummer(5000, 1022, masses="lognormal")
+    p = Params(G=1.0, eps2=0.005 ** 2, dt=5e-4, theta=0.5)
+    ctx.upload(pos, vel, m)
+    acc0 = ctx.lbvh_forces(p, MIXED)
+    for nsteps in (1, 3):
+        hp, hv, ha = pos.copy(), vel.copy(), acc0.copy()
+        ctx.kdk_steps_host(p, nsteps, hp, hv, ha, m, SOLVER_LBVH, MIXED)
+        with Context(0) as other:
+            other.upload(pos, vel, m, acc=acc0)
+            other.kdk_steps(p, nsteps, SOLVER_LBVH, MIXED)
+            op, ov, oa = other.download()
+        np.testing.assert_array_equal(hp, op)
+        np.testing.assert_array_equal(hv, ov)
+        np.testing.assert_array_equal(ha, oa)
