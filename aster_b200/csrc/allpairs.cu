@@ -89,8 +89,9 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
         sp[threadIdx.x] = j < j1 ? pm[j] : make_double4(1e300, 1e300, 1e300, 0.0);
         if (PN) sv[threadIdx.x] = j < j1 ? vel[j] : make_double4(0, 0, 0, 0);
         __syncthreads();
+        const int cnt = (int)min((int64_t)BLOCK, j1 - base);  // a partial last tile stops at its last source
 #pragma unroll 4
-        for (int q = 0; q < BLOCK; ++q) {
+        for (int q = 0; q < cnt; ++q) {
             const double4 pj = sp[q];
 #pragma unroll
             for (int k = 0; k < IPT; ++k) {
@@ -172,10 +173,11 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
             if (PN) sv[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
         __syncthreads();
+        const int cnt = (int)min((int64_t)BLOCK, j1 - base);  // a partial last tile stops at its last source
 #pragma unroll 1
-        for (int c0 = 0; c0 < BLOCK; c0 += FOLD) {
+        for (int c0 = 0; c0 < cnt; c0 += FOLD) {
 #pragma unroll 8
-            for (int q = c0; q < c0 + FOLD; ++q) {
+            for (int q = c0; q < min(c0 + FOLD, cnt); ++q) {
                 const float4 h = sh[q];
                 const float4 l = sl[q];
 #pragma unroll
@@ -265,30 +267,39 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed2(
         fc[4 * q + hh] = l.x; fc[4 * q + 2 + hh] = l.y;
         fd[4 * q + hh] = l.z; fd[4 * q + 2 + hh] = 0.f;
         __syncthreads();
-#pragma unroll 1
-        for (int c0 = 0; c0 < BLOCK / 2; c0 += FOLD / 2) {
-#pragma unroll 4
-            for (int pq = c0; pq < c0 + FOLD / 2; ++pq) {
-                const float4 A = pa[pq], B = pb[pq], C = pc[pq], D = pd[pq];
+        auto pair2 = [&](int pq) {
+            const float4 A = pa[pq], B = pb[pq], C = pc[pq], D = pd[pq];
 #pragma unroll
-                for (int k = 0; k < IPT; ++k) {
-                    const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(A.x, A.y), nhx[k]), __fadd2_rn(make_float2(C.x, C.y), nlx[k]));
-                    const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(A.z, A.w), nhy[k]), __fadd2_rn(make_float2(C.z, C.w), nly[k]));
-                    const float2 dz = __fadd2_rn(__fadd2_rn(make_float2(B.x, B.y), nhz[k]), __fadd2_rn(make_float2(D.x, D.y), nlz[k]));
-                    float2 r2 = __ffma2_rn(dz, dz, e2);
-                    r2 = __ffma2_rn(dy, dy, r2);
-                    r2 = __ffma2_rn(dx, dx, r2);
-                    float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                    if (GUARD) {
-                        inv.x = r2.x > 0.f ? inv.x : 0.f;
-                        inv.y = r2.y > 0.f ? inv.y : 0.f;
-                    }
-                    const float2 inv2 = __fmul2_rn(inv, inv);
-                    const float2 s = __fmul2_rn(__fmul2_rn(make_float2(B.z, B.w), inv), inv2);
-                    ax[k] = __ffma2_rn(dx, s, ax[k]);
-                    ay[k] = __ffma2_rn(dy, s, ay[k]);
-                    az[k] = __ffma2_rn(dz, s, az[k]);
+            for (int k = 0; k < IPT; ++k) {
+                const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(A.x, A.y), nhx[k]), __fadd2_rn(make_float2(C.x, C.y), nlx[k]));
+                const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(A.z, A.w), nhy[k]), __fadd2_rn(make_float2(C.z, C.w), nly[k]));
+                const float2 dz = __fadd2_rn(__fadd2_rn(make_float2(B.x, B.y), nhz[k]), __fadd2_rn(make_float2(D.x, D.y), nlz[k]));
+                float2 r2 = __ffma2_rn(dz, dz, e2);
+                r2 = __ffma2_rn(dy, dy, r2);
+                r2 = __ffma2_rn(dx, dx, r2);
+                float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                if (GUARD) {
+                    inv.x = r2.x > 0.f ? inv.x : 0.f;
+                    inv.y = r2.y > 0.f ? inv.y : 0.f;
                 }
+                const float2 inv2 = __fmul2_rn(inv, inv);
+                const float2 s = __fmul2_rn(__fmul2_rn(make_float2(B.z, B.w), inv), inv2);
+                ax[k] = __ffma2_rn(dx, s, ax[k]);
+                ay[k] = __ffma2_rn(dy, s, ay[k]);
+                az[k] = __ffma2_rn(dz, s, az[k]);
+            }
+        };
+        // a partial last tile stops at its last source pair (the padding pairs
+        // contribute zero)
+        const int npair = (int)((min((int64_t)BLOCK, j1 - base) + 1) / 2);
+#pragma unroll 1
+        for (int c0 = 0; c0 < npair; c0 += FOLD / 2) {
+            if (npair == BLOCK / 2) {
+#pragma unroll 4
+                for (int pq = c0; pq < c0 + FOLD / 2; ++pq) pair2(pq);
+            } else {
+#pragma unroll 1
+                for (int pq = c0; pq < min(c0 + FOLD / 2, npair); ++pq) pair2(pq);
             }
 #pragma unroll
             for (int k = 0; k < IPT; ++k) {
@@ -350,7 +361,9 @@ void launch_mixed(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32
 int aster_allpairs_launch(aster_ctx* c, const aster_params* p, int precision, bool closing_kick, int64_t nt,
                           const int32_t* targets_dev, double* out_dev) {
     if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;  // ensemble only
-    const int64_t n = c->n;
+    // sources: bodies [0, n_src) (the trailing massless bodies contribute zero
+    // in the Newtonian and 1PN laws alike); targets: nt bodies or the list
+    const int64_t n = c->n_src > 0 ? c->n_src : c->n;
     const int64_t per_block = (int64_t)BLOCK * IPT;
     const int64_t iblocks = (nt + per_block - 1) / per_block;
     // j-slices so that small n still fill the GPU (>= 2 blocks per SM).

@@ -74,6 +74,7 @@ struct aster_ctx {
     bool own_stream = false;
     cudaStream_t copy_stream = nullptr;  // device->host copies overlapped with compute (created on first use)
     int64_t n = 0;
+    int64_t n_src = 0;  // 1 + index of the last body with non-zero mass: all-pairs sources stop there
     DevBuf pm;    // double4 (x, y, z, m), input order
     DevBuf vel;   // double4 (vx, vy, vz, 0)
     DevBuf acc;   // double4 (ax, ay, az, 0): cached acceleration

@@ -266,6 +266,11 @@ int aster_upload_enqueue(aster_ctx* c, int64_t n, const double* pos, const doubl
         ASTER_CUDA(cudaMemsetAsync(c->acc.ptr, 0, n4d, c->stream));
     }
     c->n = n;
+    // trailing massless bodies (test particles) attract nothing: the
+    // all-pairs source loop ends at the last massive body (scanned from the end)
+    int64_t last = n - 1;
+    while (last > 0 && mass[last] == 0.0) --last;
+    c->n_src = last + 1;
     c->acc_valid = acc != nullptr;
     c->tree.built = false;
     return ASTER_OK;

@@ -33,7 +33,9 @@ namespace {
 constexpr int WH_BLOCK = 256;
 
 // state scalars in ctx->wh after the partials: [0] m0, [1] M, [2..4] x_cm,
-// [5..7] v_cm, [8..11] reduction result (sum m a.x, .y, .z, sum m)
+// [5..7] v_cm, [8..11] reduction result (sum m a.x, .y, .z, sum m), [12..14]
+// sum m v, [16..18] sum m Q, [20..22] sum m x, [30] the reduction's block
+// counter (an unsigned int, zero between launches)
 struct WhLayout {
     int64_t nb;  // reduction blocks
     double* part;
@@ -49,16 +51,21 @@ WhLayout wh_layout(aster_ctx* c) {
     return L;
 }
 
-// Block partials of (sum m_i a_i, sum m_i) over i in [i0, n); m from pm[i].w.
-__global__ void __launch_bounds__(WH_BLOCK) k_wh_partial(int64_t n, int64_t i0, const double4* __restrict__ pm,
-                                                         const double4* __restrict__ a, double* __restrict__ part) {
+// sum over i in [i0, n) of (m_i a_i, m_i), m from pm[i].w, into out4[0..3]:
+// block partials into part[4 * block], then the last block to finish adds them
+// in block order (deterministic whichever block is last) and re-arms the
+// counter for the next launch.
+__global__ void __launch_bounds__(WH_BLOCK) k_wh_reduce(int64_t n, int64_t i0, const double4* __restrict__ pm,
+                                                        const double4* __restrict__ a, double* __restrict__ part,
+                                                        unsigned int* __restrict__ done, double* __restrict__ out4) {
     double s[4] = {0, 0, 0, 0};
     for (int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double m = pm[i].w;
         const double4 x = a[i];
         s[0] += m * x.x; s[1] += m * x.y; s[2] += m * x.z; s[3] += m;
     }
-    __shared__ double red[4][WH_BLOCK / 32];
+    __shared__ double red[4][WH_BLOCK / 4];
+    __shared__ bool last;
     for (int k = 0; k < 4; ++k) {
         double v = s[k];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -69,15 +76,26 @@ __global__ void __launch_bounds__(WH_BLOCK) k_wh_partial(int64_t n, int64_t i0, 
         double v = 0;
         for (int w = 0; w < WH_BLOCK / 32; ++w) v += red[threadIdx.x][w];
         part[blockIdx.x * 4 + threadIdx.x] = v;
+        __threadfence();
     }
-}
-
-__global__ void k_wh_final(int64_t nb, const double* __restrict__ part, double* __restrict__ out4) {
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // thread t adds component t & 3 of blocks g, g + G, g + 2G, ... (g = t >> 2,
+    // G = WH_BLOCK / 4), then thread k < 4 adds the G group sums in order
+    const int k = threadIdx.x & 3, g = threadIdx.x >> 2;
+    double v = 0;
+    for (unsigned b = g; b < gridDim.x; b += WH_BLOCK / 4) v += __ldcg(part + 4 * b + k);
+    red[k][g] = v;
+    __syncthreads();
     if (threadIdx.x < 4) {
-        double v = 0;
-        for (int64_t b = 0; b < nb; ++b) v += part[b * 4 + threadIdx.x];  // fixed order: deterministic
-        out4[threadIdx.x] = v;
+        double t = 0;
+        for (int q = 0; q < WH_BLOCK / 4; ++q) t += red[threadIdx.x][q];
+        out4[threadIdx.x] = t;
     }
+    if (threadIdx.x == 0) *done = 0u;
 }
 
 // inertial -> working state. Reads the reductions: st[8..11] = (sum m x, M)
@@ -97,18 +115,34 @@ __global__ void __launch_bounds__(WH_BLOCK) k_wh_to_dhc(int64_t n, double4* __re
     }
 }
 
+// Stumpff functions c2(z) = (1 - cos sqrt z) / z, c3(z) = (sqrt z - sin sqrt z) / z^1.5.
+// |z| < 0.5: their Maclaurin series c2 = sum (-z)^k / (2k+2)!, c3 = sum (-z)^k /
+// (2k+3)!, ten terms (the first omitted term is below 2^-53 of the sum) in
+// Horner form with the reciprocal factorials as constants (folded at compile
+// time, each correctly rounded).
 __device__ __forceinline__ void stumpff(double z, double& c2, double& c3) {
     if (fabs(z) < 0.5) {
-        double t2 = 0.5, t3 = 1.0 / 6.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll
-        for (int k = 1; k <= 10; ++k) {
-            s2 += t2;
-            s3 += t3;
-            t2 *= -z / ((2.0 * k + 1.0) * (2.0 * k + 2.0));
-            t3 *= -z / ((2.0 * k + 2.0) * (2.0 * k + 3.0));
-        }
-        c2 = s2;
-        c3 = s3;
+        const double x = -z;
+        c2 = 1.0 / 2432902008176640000.0;                     // 1/20!
+        c2 = fma(c2, x, 1.0 / 6402373705728000.0);            // 1/18!
+        c2 = fma(c2, x, 1.0 / 20922789888000.0);              // 1/16!
+        c2 = fma(c2, x, 1.0 / 87178291200.0);                 // 1/14!
+        c2 = fma(c2, x, 1.0 / 479001600.0);                   // 1/12!
+        c2 = fma(c2, x, 1.0 / 3628800.0);                     // 1/10!
+        c2 = fma(c2, x, 1.0 / 40320.0);                       // 1/8!
+        c2 = fma(c2, x, 1.0 / 720.0);                         // 1/6!
+        c2 = fma(c2, x, 1.0 / 24.0);                          // 1/4!
+        c2 = fma(c2, x, 0.5);                                 // 1/2!
+        c3 = 1.0 / 51090942171709440000.0;                    // 1/21!
+        c3 = fma(c3, x, 1.0 / 121645100408832000.0);          // 1/19!
+        c3 = fma(c3, x, 1.0 / 355687428096000.0);             // 1/17!
+        c3 = fma(c3, x, 1.0 / 1307674368000.0);               // 1/15!
+        c3 = fma(c3, x, 1.0 / 6227020800.0);                  // 1/13!
+        c3 = fma(c3, x, 1.0 / 39916800.0);                    // 1/11!
+        c3 = fma(c3, x, 1.0 / 362880.0);                      // 1/9!
+        c3 = fma(c3, x, 1.0 / 5040.0);                        // 1/7!
+        c3 = fma(c3, x, 1.0 / 120.0);                         // 1/5!
+        c3 = fma(c3, x, 1.0 / 6.0);                           // 1/3!
     } else if (z > 0.0) {
         const double s = sqrt(z), h = sin(0.5 * s);
         c2 = 2.0 * h * h / z;
@@ -232,11 +266,10 @@ __global__ void k_wh_copy3(double* __restrict__ st, int from, int to) {
 
 // sum over i in [i0, n) of (m_i a_i, m_i) into st[8..11]
 static int wh_reduce(aster_ctx* c, const WhLayout& L, int64_t i0, const double4* a) {
-    k_wh_partial<<<(unsigned)L.nb, WH_BLOCK, 0, c->stream>>>(c->n, i0, c->pm.as<double4>(), a, L.part);
+    k_wh_reduce<<<(unsigned)L.nb, WH_BLOCK, 0, c->stream>>>(c->n, i0, c->pm.as<double4>(), a, L.part,
+                                                           reinterpret_cast<unsigned int*>(L.st + 30), L.st + 8);
     ASTER_CUDA(cudaGetLastError());
-    k_wh_final<<<1, 32, 0, c->stream>>>(L.nb, L.part, L.st + 8);
-    ASTER_CUDA(cudaGetLastError());
-    c->stats.kernels += 2;
+    c->stats.kernels += 1;
     return ASTER_OK;
 }
 
@@ -268,6 +301,7 @@ int aster_wh_enqueue(aster_ctx* c, const aster_params* p, int precision, int nst
     const int64_t nbmax = std::min<int64_t>((n + WH_BLOCK - 1) / WH_BLOCK, (int64_t)c->sm_count * 4);
     ASTER_TRY(c->wh.ensure((size_t)(4 * std::max<int64_t>(nbmax, 1) + 32) * sizeof(double)));
     const WhLayout L = wh_layout(c);
+    ASTER_CUDA(cudaMemsetAsync(L.st + 30, 0, sizeof(double), c->stream));  // arm the reduction counter
     const double mu = p->G * m0;
     double4* pm = c->pm.as<double4>();
     double4* vel = c->vel.as<double4>();

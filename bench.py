@@ -530,6 +530,14 @@ def run_case(args):
             out[f"ms_{prec}"] = ctx.stats()["ms_force"]
     elif args.case == "c3drift":
         out.update(c3_drift(ctx))
+    elif args.case == "wh":
+        # Wisdom-Holman: a star, 8 planets and 262,144 massless test particles, 20 steps
+        pos, vel, m = gen.planetary_system(8, 262144, 1023)
+        ctx.upload(pos, vel, m)
+        p = Params(G=1.0, dt=0.02)
+        ctx.wh_steps(p, 2)
+        ctx.wh_steps(p, 20)
+        out["ms_20_steps"] = ctx.stats()["ms_total"]
     elif args.case == "ensemble":
         pos, vel, m, off = gen.hierarchical_ensemble(16384, 1004)
         p = Params(G=1.0, c=100.0, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1)
@@ -562,7 +570,7 @@ def main():
                     help="bodies in the headline workload (default 2^20; smaller only for profiling captures)")
     ap.add_argument("--walk-traffic", type=float, default=WALK_TRAFFIC_BYTES,
                     help="DRAM bytes per walk launch from an ncu capture (reported as roofline.traffic)")
-    ap.add_argument("--case", default=None, choices=["allpairs", "ensemble", "adjoint", "c3drift"],
+    ap.add_argument("--case", default=None, choices=["allpairs", "ensemble", "adjoint", "c3drift", "wh"],
                     help="run one secondary workload briefly (used for profiling captures) and exit")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -122,3 +122,30 @@ def test_invalid_arguments(ctx):
         ctx.allpairs(Params(), 7)
     with pytest.raises(AsterError):
         ctx.upload(np.array([[np.nan, 0, 0]]), None, np.ones(1))
+
+
+@pytest.mark.parametrize("n_massive", [1, 5, 700])
+def test_trailing_massless_sources(ctx, orc, n_massive):
+    """Bodies after the last massive one are skipped as sources (they attract
+    nothing); results equal the oracle's sum over every body, for Newton and
+    1PN, all targets and a target list, and a later upload with massive tail
+    bodies uses them again."""
+    n = 3000
+    pos, vel, m = gen.plummer(n, 77 + n_massive)
+    vel = vel * 0.1
+    m0 = m.copy()
+    m[n_massive:] = 0.0
+    if n_massive > 2:
+        m[n_massive // 2] = 0.0  # a massless body before the last massive one
+    ctx.upload(pos, vel, m)
+    for law, cval in ((NEWTON, 0.0), (NEWTON | PN1, 30.0)):
+        p = Params(eps2=1e-4, c=cval, force_law=law)
+        ref = orc.allpairs(pos, m, 1.0, 1e-4, vel=vel, inv_c=1.0 / cval if cval else 0.0, pn=law)
+        assert rel_l2(ctx.allpairs(p, FP64), ref) < TOL_FP64
+        assert rel_l2(ctx.allpairs(p, MIXED), ref) < TOL_MIXED
+    tg = np.arange(n - 200, n, dtype=np.int32)
+    ref = orc.allpairs(pos, m, 1.0, 1e-4, targets=tg)
+    assert rel_l2(ctx.allpairs_targets(Params(eps2=1e-4), tg, MIXED), ref) < TOL_MIXED
+    ctx.upload(pos, vel, m0)
+    ref = orc.allpairs(pos, m0, 1.0, 1e-4)
+    assert rel_l2(ctx.allpairs(Params(eps2=1e-4), FP64), ref) < TOL_FP64
