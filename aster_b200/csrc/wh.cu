@@ -34,8 +34,9 @@ constexpr int WH_BLOCK = 256;
 
 // state scalars in ctx->wh after the partials: [0] m0, [1] M, [2..4] x_cm,
 // [5..7] v_cm, [8..11] reduction result (sum m a.x, .y, .z, sum m), [12..14]
-// sum m v, [16..18] sum m Q, [20..22] sum m x, [30] the reduction's block
-// counter (an unsigned int, zero between launches)
+// sum m v, [16..18] sum m Q, [20..22] sum m x, [24..27] the second slot for P
+// (k_wh_cba reads P from one slot and writes the next P to the other), [30] the
+// reductions' block counter (an unsigned int, zero between launches)
 struct WhLayout {
     int64_t nb;  // reduction blocks
     double* part;
@@ -51,19 +52,12 @@ WhLayout wh_layout(aster_ctx* c) {
     return L;
 }
 
-// sum over i in [i0, n) of (m_i a_i, m_i), m from pm[i].w, into out4[0..3]:
-// block partials into part[4 * block], then the last block to finish adds them
-// in block order (deterministic whichever block is last) and re-arms the
-// counter for the next launch.
-__global__ void __launch_bounds__(WH_BLOCK) k_wh_reduce(int64_t n, int64_t i0, const double4* __restrict__ pm,
-                                                        const double4* __restrict__ a, double* __restrict__ part,
-                                                        unsigned int* __restrict__ done, double* __restrict__ out4) {
-    double s[4] = {0, 0, 0, 0};
-    for (int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double m = pm[i].w;
-        const double4 x = a[i];
-        s[0] += m * x.x; s[1] += m * x.y; s[2] += m * x.z; s[3] += m;
-    }
+// Block-wide sum of each thread's s[0..3] into part[4 * block]; the last block
+// to finish then adds the partials in block order (deterministic whichever
+// block is last), writes the total to out4[0..3] and re-arms *done (zero
+// between launches). Every thread of every block calls it once.
+__device__ __forceinline__ void block_sum4_last(const double s[4], double* part, unsigned int* done,
+                                                double* out4) {
     __shared__ double red[4][WH_BLOCK / 4];
     __shared__ bool last;
     for (int k = 0; k < 4; ++k) {
@@ -96,6 +90,19 @@ __global__ void __launch_bounds__(WH_BLOCK) k_wh_reduce(int64_t n, int64_t i0, c
         out4[threadIdx.x] = t;
     }
     if (threadIdx.x == 0) *done = 0u;
+}
+
+// sum over i in [i0, n) of (m_i a_i, m_i), m from pm[i].w, into out4[0..3]
+__global__ void __launch_bounds__(WH_BLOCK) k_wh_reduce(int64_t n, int64_t i0, const double4* __restrict__ pm,
+                                                        const double4* __restrict__ a, double* part,
+                                                        unsigned int* done, double* out4) {
+    double s[4] = {0, 0, 0, 0};
+    for (int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double m = pm[i].w;
+        const double4 x = a[i];
+        s[0] += m * x.x; s[1] += m * x.y; s[2] += m * x.z; s[3] += m;
+    }
+    block_sum4_last(s, part, done, out4);
 }
 
 // inertial -> working state. Reads the reductions: st[8..11] = (sum m x, M)
@@ -195,29 +202,36 @@ __device__ bool kepler_drift(double3& r, double3& v, double mu, double dt) {
     return true;
 }
 
-// First half of a step and the Kepler drift, per body i >= 1:
-// C(h) with P = st[8..10], B(h) with the cached interaction acc, A(dt).
+// Per body i >= 1: C(hc) with P = pin[0..2], B(hb) with the cached
+// interaction acc, A(dt); then P = sum m_i V_i after the drift into pout[0..2]
+// (pout[3] = sum m_i), pin and pout distinct slots of the state scalars.
 __global__ void __launch_bounds__(WH_BLOCK) k_wh_cba(int64_t n, double4* __restrict__ pm, double4* __restrict__ vel,
-                                                     const double4* __restrict__ acc, const double* __restrict__ st,
-                                                     double mu, double h, double dt, int* __restrict__ err) {
+                                                     const double4* __restrict__ acc, const double* st,
+                                                     const double* pin, double hc, double hb, double mu, double dt,
+                                                     int* __restrict__ err, double* part, unsigned int* done,
+                                                     double* pout) {
     const double m0 = st[0];
-    const double px = st[8] / m0 * h, py = st[9] / m0 * h, pz = st[10] / m0 * h;
+    const double px = pin[0] / m0 * hc, py = pin[1] / m0 * hc, pz = pin[2] / m0 * hc;
+    double sum[4] = {0, 0, 0, 0};
     for (int64_t i = 1 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double4 p = pm[i], v = vel[i];
         const double4 a = acc[i];
         double3 r = make_double3(p.x + px, p.y + py, p.z + pz);
-        double3 u = make_double3(v.x + a.x * h, v.y + a.y * h, v.z + a.z * h);
+        double3 u = make_double3(v.x + a.x * hb, v.y + a.y * hb, v.z + a.z * hb);
         if (!kepler_drift(r, u, mu, dt)) atomicOr(err, ASTER_DEVERR_KEPLER);
         pm[i] = make_double4(r.x, r.y, r.z, p.w);
         vel[i] = make_double4(u.x, u.y, u.z, v.w);
+        sum[0] += p.w * u.x; sum[1] += p.w * u.y; sum[2] += p.w * u.z; sum[3] += p.w;
     }
+    block_sum4_last(sum, part, done, pout);
 }
 
-// C(h) alone (second half; B follows in the force launch's closing kick).
-__global__ void __launch_bounds__(WH_BLOCK) k_wh_c(int64_t n, double4* __restrict__ pm, const double* __restrict__ st,
-                                                   double h) {
+// C(h) alone with P = pin[0..2] (a run's last half step; B follows in the
+// force launch's closing kick).
+__global__ void __launch_bounds__(WH_BLOCK) k_wh_c(int64_t n, double4* __restrict__ pm, const double* st,
+                                                   const double* pin, double h) {
     const double m0 = st[0];
-    const double px = st[8] / m0 * h, py = st[9] / m0 * h, pz = st[10] / m0 * h;
+    const double px = pin[0] / m0 * h, py = pin[1] / m0 * h, pz = pin[2] / m0 * h;
     for (int64_t i = 1 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double4 p = pm[i];
         p.x += px; p.y += py; p.z += pz;
@@ -263,6 +277,12 @@ __global__ void k_wh_copy3(double* __restrict__ st, int from, int to) {
 }
 
 }  // namespace
+
+// ASTER_OK, or the error of the last launch
+static int wh_launch_status() {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ASTER_OK : aster_cuda_fail(e, "WH kernel launch", __FILE__, __LINE__);
+}
 
 // sum over i in [i0, n) of (m_i a_i, m_i) into st[8..11]
 static int wh_reduce(aster_ctx* c, const WhLayout& L, int64_t i0, const double4* a) {
@@ -317,20 +337,33 @@ int aster_wh_enqueue(aster_ctx* c, const aster_params* p, int precision, int nst
     ASTER_CUDA(cudaGetLastError());
     c->stats.kernels += 4;
     int st = ASTER_OK;
-    int done = 0;  // steps completed: the barycentre advances by done * dt
-    const aster_params& pk = *p;  // the interaction launch; its closing kick is dt/2
-    // interaction at the initial positions
-    if (precision == ASTER_MIXED) st = aster_refresh_mixed(c);
-    if (st == ASTER_OK) st = aster_allpairs_launch(c, &pk, precision, false, n, nullptr, nullptr);
-    for (int s = 0; s < nsteps && st == ASTER_OK; ++s, ++done) {
-        if ((st = wh_reduce(c, L, 1, vel)) != ASTER_OK) break;  // P
-        k_wh_cba<<<grid, WH_BLOCK, 0, c->stream>>>(n, pm, vel, c->acc.as<double4>(), L.st, mu, h, dt, c->err_dev);
-        if ((st = wh_reduce(c, L, 1, vel)) != ASTER_OK) break;  // P after the Kepler drift
-        k_wh_c<<<grid, WH_BLOCK, 0, c->stream>>>(n, pm, L.st, h);
-        c->stats.kernels += 2;
+    int done = 0;  // Kepler drifts taken: the barycentre advances by done * dt
+    // Steps C(h) B(h) A(dt) C(h) B(h) in sequence: between two drifts A the
+    // C(h) B(h) C(h) B(h) collapse to C(dt) B(dt) (B leaves P = sum m V
+    // unchanged, and the interaction does not change under the uniform shift
+    // C), so a run is C(h) B(h) A [C(dt) B(dt) A] x (nsteps - 1) C(h) B(h):
+    // one interaction launch and one k_wh_cba (with P for the next C) a step.
+    unsigned int* cnt = reinterpret_cast<unsigned int*>(L.st + 30);
+    double* pslot[2] = {L.st + 8, L.st + 24};
+    int cur = 0;
+    for (int s = 0; s < nsteps && st == ASTER_OK; ++s) {
         if (precision == ASTER_MIXED && (st = aster_refresh_mixed(c)) != ASTER_OK) break;
-        st = aster_allpairs_launch(c, &pk, precision, true, n, nullptr, nullptr);  // + closing kick B(h)
-        if (st != ASTER_OK) break;
+        if ((st = aster_allpairs_launch(c, p, precision, false, n, nullptr, nullptr)) != ASTER_OK) break;
+        if (s == 0 && (st = wh_reduce(c, L, 1, vel)) != ASTER_OK) break;  // P of the initial state
+        const double hcb = s == 0 ? h : dt;
+        k_wh_cba<<<grid, WH_BLOCK, 0, c->stream>>>(n, pm, vel, c->acc.as<double4>(), L.st, pslot[cur], hcb, hcb, mu,
+                                                   dt, c->err_dev, L.part, cnt, pslot[cur ^ 1]);
+        if ((st = wh_launch_status()) != ASTER_OK) break;
+        cur ^= 1;
+        ++done;
+        c->stats.kernels += 1;
+    }
+    if (st == ASTER_OK && done > 0) {  // the last C(h) B(h)
+        k_wh_c<<<grid, WH_BLOCK, 0, c->stream>>>(n, pm, L.st, pslot[cur], h);
+        st = wh_launch_status();
+        c->stats.kernels += 1;
+        if (st == ASTER_OK && precision == ASTER_MIXED) st = aster_refresh_mixed(c);
+        if (st == ASTER_OK) st = aster_allpairs_launch(c, p, precision, true, n, nullptr, nullptr);  // + B(h)
     }
     // back to the inertial state (also after an error, so the state stays meaningful)
     if (wh_reduce(c, L, 1, pm) == ASTER_OK) {  // S = sum m Q
