@@ -27,8 +27,8 @@ LIB_PATH = Path(__file__).resolve().parent / "libaster_cuda.so"
 OK = 0
 NEWTON = 0x0001
 PN1 = 0x0010
-PN2 = 0x0100   # ensemble only
-PN25 = 0x1000  # ensemble only
+PN2 = 0x0100   # all-pairs solver and ensemble
+PN25 = 0x1000  # all-pairs solver and ensemble
 UPDATER_KDK, UPDATER_SABA, UPDATER_WH = 0, 1, 2
 COLLECT_ENERGY, COLLECT_ENERGY_ERROR, COLLECT_MOMENTUM, COLLECT_CENTER, COLLECT_DISTANCE = 0x1, 0x2, 0x4, 0x8, 0x10
 FP64 = 0

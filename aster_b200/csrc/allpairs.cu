@@ -1,14 +1,16 @@
 // All-pairs force kernels: the replacement for Parallelized::compute_forces
 // (src/utils/builder_endpoint.cpp:729-757), SimpleGPU::compute_forces +
 // cl3d_newton (src/solvers/SimpleGPU.cpp:17-71,
-// include/Aster/kernels/newton_update3d.cl.h:28-72) and the PN pair law of
-// compute_gravitational/get_pn1 (src/physics/tool_chain_impl.cpp:110-137).
+// include/Aster/kernels/newton_update3d.cl.h:28-72) and the pair law of
+// compute_gravitational (src/physics/tool_chain_impl.cpp:120-137) with every
+// post-Newtonian term it offers (get_pn1, get_pn2, get_pn25; pn.cuh).
 //
 // Pair law (acceleration on i from j, d = x_j - x_i, r^2 = d.d + eps2):
 //   a_i += G m_j d / r^3
 //   PN1:  + G m_j / (c^2 r^2) [ n A + (v_i - v_j) B ],  n = -d/r,
 //         A = -v_i^2 - 2 v_j^2 + 4 v_i.v_j + 1.5 (n.v_j)^2 + 5 G m_i/r + 4 G m_j/r,
 //         B = 4 n.v_i - 3 n.v_j                  (tool_chain_impl.cpp:110-118)
+//   PN2, PN2.5: the c^-4 and c^-5 terms (tool_chain_impl.cpp:65-107)
 //
 // Two arithmetic paths, one tiling:
 //  * FP64: double4 (x,y,z,m) j-tiles in shared memory, FP64 throughout; the
@@ -22,6 +24,7 @@
 // and walks one j-slice; small n use several j-slices whose partial sums are
 // added by k_reduce_slices (scratch memory).
 #include "aster_internal.cuh"
+#include "pn.cuh"
 
 namespace {
 
@@ -61,18 +64,19 @@ __device__ __forceinline__ void store_result(int64_t t, int64_t body, double ax,
 }
 
 // ---------------------------------------------------------------- FP64 path
-template <bool PN, bool GUARD>
+// PNL: 0 Newton, 1 Newton + 1PN, 2 Newton + the PN terms pk.f selects.
+template <int PNL, bool GUARD>
 __global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
     int64_t n, int64_t nt, const int32_t* __restrict__ targets, const double4* __restrict__ pm,
-    const double4* __restrict__ vel, double G, double eps2, double inv_c2, int64_t slice_len, int nslices,
+    const double4* __restrict__ vel, double G, double eps2, PnK<double> pk, int64_t slice_len, int nslices,
     double4* __restrict__ partial, double4* __restrict__ acc, double* __restrict__ out3, KickArgs kick) {
     __shared__ double4 sp[BLOCK];
-    __shared__ double4 sv[PN ? BLOCK : 1];
+    __shared__ double4 sv[PNL ? BLOCK : 1];  // (vx, vy, vz, |v|^2)
     const int slice = blockIdx.y;
     const int64_t j0 = (int64_t)slice * slice_len;
     const int64_t j1 = min(n, j0 + slice_len);
     int64_t tt[IPT], bi[IPT];
-    double xi[IPT], yi[IPT], zi[IPT], mi[IPT], vxi[IPT], vyi[IPT], vzi[IPT];
+    double xi[IPT], yi[IPT], zi[IPT], mi[IPT], vxi[IPT], vyi[IPT], vzi[IPT], v1sq[IPT];
     double ax[IPT], ay[IPT], az[IPT];
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
@@ -80,14 +84,22 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
         bi[k] = tt[k] < nt ? (targets ? (int64_t)targets[tt[k]] : tt[k]) : 0;
         double4 p = pm[bi[k]];
         xi[k] = p.x; yi[k] = p.y; zi[k] = p.z; mi[k] = p.w;
-        if (PN) { double4 v = vel[bi[k]]; vxi[k] = v.x; vyi[k] = v.y; vzi[k] = v.z; }
+        if (PNL) {
+            double4 v = vel[bi[k]];
+            vxi[k] = v.x; vyi[k] = v.y; vzi[k] = v.z;
+            v1sq[k] = v.x * v.x + v.y * v.y + v.z * v.z;
+        }
         ax[k] = ay[k] = az[k] = 0.0;
     }
     for (int64_t base = j0; base < j1; base += BLOCK) {
         const int64_t j = base + threadIdx.x;
         __syncthreads();
         sp[threadIdx.x] = j < j1 ? pm[j] : make_double4(1e300, 1e300, 1e300, 0.0);
-        if (PN) sv[threadIdx.x] = j < j1 ? vel[j] : make_double4(0, 0, 0, 0);
+        if (PNL) {
+            double4 v = j < j1 ? vel[j] : make_double4(0, 0, 0, 0);
+            v.w = v.x * v.x + v.y * v.y + v.z * v.z;
+            sv[threadIdx.x] = v;
+        }
         __syncthreads();
         const int cnt = (int)min((int64_t)BLOCK, j1 - base);  // a partial last tile stops at its last source
 #pragma unroll 4
@@ -102,21 +114,17 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
                 double inv2 = inv * inv;
                 double s = pj.w * inv * inv2;
                 ax[k] = fma(dx, s, ax[k]); ay[k] = fma(dy, s, ay[k]); az[k] = fma(dz, s, az[k]);
-                if (PN) {
+                if (PNL) {
                     const double4 vj = sv[q];
-                    double nx = -dx * inv, ny = -dy * inv, nz = -dz * inv;
-                    double v1sq = vxi[k] * vxi[k] + vyi[k] * vyi[k] + vzi[k] * vzi[k];
-                    double v2sq = vj.x * vj.x + vj.y * vj.y + vj.z * vj.z;
-                    double v12 = vxi[k] * vj.x + vyi[k] * vj.y + vzi[k] * vj.z;
-                    double nv1 = nx * vxi[k] + ny * vyi[k] + nz * vzi[k];
-                    double nv2 = nx * vj.x + ny * vj.y + nz * vj.z;
-                    double A = -v1sq - 2.0 * v2sq + 4.0 * v12 + 1.5 * nv2 * nv2 + 5.0 * G * mi[k] * inv +
-                               4.0 * G * pj.w * inv;
-                    double B = 4.0 * nv1 - 3.0 * nv2;
-                    double f = pj.w * inv2 * inv_c2;  // G applied in store_result
-                    ax[k] += (nx * A + (vxi[k] - vj.x) * B) * f;
-                    ay[k] += (ny * A + (vyi[k] - vj.y) * B) * f;
-                    az[k] += (nz * A + (vzi[k] - vj.z) * B) * f;
+                    PnPair<double> w;
+                    w.nx = -dx * inv; w.ny = -dy * inv; w.nz = -dz * inv;
+                    w.dvx = vxi[k] - vj.x; w.dvy = vyi[k] - vj.y; w.dvz = vzi[k] - vj.z;
+                    w.inv = inv; w.inv2 = inv2; w.mi = mi[k]; w.mj = pj.w; w.vi2 = v1sq[k]; w.vj2 = vj.w;
+                    w.v12 = vxi[k] * vj.x + vyi[k] * vj.y + vzi[k] * vj.z;
+                    w.nv1 = w.nx * vxi[k] + w.ny * vyi[k] + w.nz * vzi[k];
+                    w.nv2 = w.nx * vj.x + w.ny * vj.y + w.nz * vj.z;
+                    w.G = G;  // the sums are accelerations / G; G is applied in store_result
+                    pn_terms<PNL>(pk, w, ax[k], ay[k], az[k], ax[k], ay[k], az[k]);
                 }
             }
         }
@@ -127,15 +135,17 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
 }
 
 // --------------------------------------------------------------- mixed path
-template <bool PN, bool GUARD>
+// With post-Newtonian terms (PNL 1 or 2): the Newtonian part as below, the
+// 1PN terms and the 2PN/2.5PN terms in two further FP32 sums per target.
+template <int PNL, bool GUARD>
 __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
     int64_t n, int64_t nt, const int32_t* __restrict__ targets, const float4* __restrict__ phi,
-    const float4* __restrict__ plo, const float4* __restrict__ vf, float G, float eps2, float inv_c2,
+    const float4* __restrict__ plo, const float4* __restrict__ vf, float G, float eps2, PnK<float> pk,
     double Gd, int64_t slice_len, int nslices, double4* __restrict__ partial, double4* __restrict__ acc,
     double* __restrict__ out3, KickArgs kick) {
     __shared__ float4 sh[BLOCK];
     __shared__ float4 sl[BLOCK];
-    __shared__ float4 sv[PN ? BLOCK : 1];
+    __shared__ float4 sv[BLOCK];  // (vx, vy, vz, |v|^2)
     const int slice = blockIdx.y;
     const int64_t j0 = (int64_t)slice * slice_len;
     const int64_t j1 = min(n, j0 + slice_len);
@@ -143,7 +153,7 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
     float xh[IPT], yh[IPT], zh[IPT], xl[IPT], yl[IPT], zl[IPT], mi[IPT];
     float vxi[IPT], vyi[IPT], vzi[IPT], v1sq[IPT];
     float ax[IPT], ay[IPT], az[IPT];
-    float px[IPT], py[IPT], pz[IPT];
+    float px[IPT], py[IPT], pz[IPT], qx[IPT], qy[IPT], qz[IPT];
     CompSum cx[IPT], cy[IPT], cz[IPT];
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
@@ -152,13 +162,12 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
         float4 h = phi[bi[k]], l = plo[bi[k]];
         xh[k] = h.x; yh[k] = h.y; zh[k] = h.z; mi[k] = h.w;
         xl[k] = l.x; yl[k] = l.y; zl[k] = l.z;
-        if (PN) {
-            float4 v = vf[bi[k]];
-            vxi[k] = v.x; vyi[k] = v.y; vzi[k] = v.z;
-            v1sq[k] = v.x * v.x + v.y * v.y + v.z * v.z;
-        }
+        float4 v = vf[bi[k]];
+        vxi[k] = v.x; vyi[k] = v.y; vzi[k] = v.z;
+        v1sq[k] = v.x * v.x + v.y * v.y + v.z * v.z;
         ax[k] = ay[k] = az[k] = 0.f;
         px[k] = py[k] = pz[k] = 0.f;
+        qx[k] = qy[k] = qz[k] = 0.f;
     }
     for (int64_t base = j0; base < j1; base += BLOCK) {
         const int64_t j = base + threadIdx.x;
@@ -166,11 +175,13 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
         if (j < j1) {
             sh[threadIdx.x] = phi[j];
             sl[threadIdx.x] = plo[j];
-            if (PN) sv[threadIdx.x] = vf[j];
+            float4 v = vf[j];
+            v.w = v.x * v.x + v.y * v.y + v.z * v.z;
+            sv[threadIdx.x] = v;
         } else {
             sh[threadIdx.x] = make_float4(PAD_POS, PAD_POS, PAD_POS, 0.f);
             sl[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (PN) sv[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+            sv[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
         __syncthreads();
         const int cnt = (int)min((int64_t)BLOCK, j1 - base);  // a partial last tile stops at its last source
@@ -180,6 +191,7 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
             for (int q = c0; q < min(c0 + FOLD, cnt); ++q) {
                 const float4 h = sh[q];
                 const float4 l = sl[q];
+                const float4 vj = sv[q];
 #pragma unroll
                 for (int k = 0; k < IPT; ++k) {
                     float dx = (h.x - xh[k]) + (l.x - xl[k]);
@@ -191,21 +203,15 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
                     float inv2 = inv * inv;
                     float s = h.w * inv * inv2;
                     ax[k] = fmaf(dx, s, ax[k]); ay[k] = fmaf(dy, s, ay[k]); az[k] = fmaf(dz, s, az[k]);
-                    if (PN) {
-                        const float4 vj = sv[q];
-                        float nx = -dx * inv, ny = -dy * inv, nz = -dz * inv;
-                        float v2sq = vj.x * vj.x + vj.y * vj.y + vj.z * vj.z;
-                        float v12 = vxi[k] * vj.x + vyi[k] * vj.y + vzi[k] * vj.z;
-                        float nv1 = nx * vxi[k] + ny * vyi[k] + nz * vzi[k];
-                        float nv2 = nx * vj.x + ny * vj.y + nz * vj.z;
-                        float A = -v1sq[k] - 2.f * v2sq + 4.f * v12 + 1.5f * nv2 * nv2 +
-                                  (5.f * mi[k] + 4.f * h.w) * G * inv;
-                        float B = 4.f * nv1 - 3.f * nv2;
-                        float f = h.w * inv2 * inv_c2;
-                        px[k] = fmaf(nx * A + (vxi[k] - vj.x) * B, f, px[k]);
-                        py[k] = fmaf(ny * A + (vyi[k] - vj.y) * B, f, py[k]);
-                        pz[k] = fmaf(nz * A + (vzi[k] - vj.z) * B, f, pz[k]);
-                    }
+                    PnPair<float> w;
+                    w.nx = -dx * inv; w.ny = -dy * inv; w.nz = -dz * inv;
+                    w.dvx = vxi[k] - vj.x; w.dvy = vyi[k] - vj.y; w.dvz = vzi[k] - vj.z;
+                    w.inv = inv; w.inv2 = inv2; w.mi = mi[k]; w.mj = h.w; w.vi2 = v1sq[k]; w.vj2 = vj.w;
+                    w.v12 = vxi[k] * vj.x + vyi[k] * vj.y + vzi[k] * vj.z;
+                    w.nv1 = w.nx * vxi[k] + w.ny * vyi[k] + w.nz * vzi[k];
+                    w.nv2 = w.nx * vj.x + w.ny * vj.y + w.nz * vj.z;
+                    w.G = G;
+                    pn_terms<PNL>(pk, w, px[k], py[k], pz[k], qx[k], qy[k], qz[k]);
                 }
             }
 #pragma unroll
@@ -218,8 +224,10 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
 #pragma unroll
     for (int k = 0; k < IPT; ++k)
         if (tt[k] < nt)
-            store_result(tt[k], bi[k], cx[k].value() + (double)px[k], cy[k].value() + (double)py[k],
-                         cz[k].value() + (double)pz[k], Gd, nslices, slice, nt, partial, acc, out3, kick);
+            store_result(tt[k], bi[k], cx[k].value() + ((double)px[k] + (double)qx[k]),
+                         cy[k].value() + ((double)py[k] + (double)qy[k]),
+                         cz[k].value() + ((double)pz[k] + (double)qz[k]), Gd, nslices, slice, nt, partial, acc, out3,
+                         kick);
 }
 
 // Newtonian mixed path with the paired FP32 instructions of sm_100
@@ -329,28 +337,39 @@ __global__ void k_reduce_slices(int64_t nt, int nslices, const double4* __restri
     }
 }
 
-template <bool PN, bool GUARD>
+template <int PNL, bool GUARD>
 void launch_fp64(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32_t* tg, aster_ctx* c,
                  const aster_params* p, int64_t slice_len, int ns, double4* partial, double* out3, KickArgs kick) {
-    const double inv_c2 = PN ? 1.0 / (p->c * p->c) : 0.0;
-    k_allpairs_fp64<PN, GUARD><<<grid, BLOCK, 0, st>>>(n, nt, tg, c->pm.as<double4>(), c->vel.as<double4>(), p->G,
-                                                        p->eps2, inv_c2, slice_len, ns, partial,
-                                                        c->acc.as<double4>(), out3, kick);
+    k_allpairs_fp64<PNL, GUARD><<<grid, BLOCK, 0, st>>>(n, nt, tg, c->pm.as<double4>(), c->vel.as<double4>(), p->G,
+                                                         p->eps2, make_pn(p), slice_len, ns, partial,
+                                                         c->acc.as<double4>(), out3, kick);
 }
 
-template <bool PN, bool GUARD>
+template <int PNL, bool GUARD>
 void launch_mixed(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32_t* tg, aster_ctx* c,
                   const aster_params* p, int64_t slice_len, int ns, double4* partial, double* out3, KickArgs kick) {
-    const float inv_c2 = PN ? (float)(1.0 / (p->c * p->c)) : 0.f;
-    if (!PN) {
+    if constexpr (PNL == 0) {
         k_allpairs_mixed2<GUARD><<<grid, BLOCK, 0, st>>>(n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(),
                                                           (float)p->eps2, p->G, slice_len, ns, partial,
                                                           c->acc.as<double4>(), out3, kick);
-        return;
+    } else {
+        k_allpairs_mixed<PNL, GUARD><<<grid, BLOCK, 0, st>>>(
+            n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), (float)p->G, (float)p->eps2,
+            pn_float(make_pn(p)), p->G, slice_len, ns, partial, c->acc.as<double4>(), out3, kick);
     }
-    k_allpairs_mixed<PN, GUARD><<<grid, BLOCK, 0, st>>>(
-        n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), (float)p->G, (float)p->eps2,
-        inv_c2, p->G, slice_len, ns, partial, c->acc.as<double4>(), out3, kick);
+}
+
+template <int PNL>
+void launch_pnl(int precision, bool guard, dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32_t* tg,
+                aster_ctx* c, const aster_params* p, int64_t slice_len, int ns, double4* partial, double* out3,
+                KickArgs kick) {
+    if (precision == ASTER_FP64) {
+        if (guard) launch_fp64<PNL, true>(grid, st, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
+        else       launch_fp64<PNL, false>(grid, st, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
+    } else {
+        if (guard) launch_mixed<PNL, true>(grid, st, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
+        else       launch_mixed<PNL, false>(grid, st, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
+    }
 }
 
 }  // namespace
@@ -360,7 +379,6 @@ void launch_mixed(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32
 // optional closing kick, or out_dev[nt*3].
 int aster_allpairs_launch(aster_ctx* c, const aster_params* p, int precision, bool closing_kick, int64_t nt,
                           const int32_t* targets_dev, double* out_dev) {
-    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;  // ensemble only
     // sources: bodies [0, n_src) (the trailing massless bodies contribute zero
     // in the Newtonian and 1PN laws alike); targets: nt bodies or the list
     const int64_t n = c->n_src > 0 ? c->n_src : c->n;
@@ -382,21 +400,12 @@ int aster_allpairs_launch(aster_ctx* c, const aster_params* p, int precision, bo
     }
     KickArgs kick{closing_kick && !out_dev, 0.5 * p->dt, c->vel.as<double4>()};
     dim3 grid((unsigned)iblocks, (unsigned)ns);
-    const bool pn = (p->force_law & ASTER_PN1) != 0;
     const bool guard = !(p->eps2 > 0.0);
-    if (precision == ASTER_FP64) {
-        if (pn) { if (guard) launch_fp64<true, true>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
-                  else launch_fp64<true, false>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick); }
-        else    { if (guard) launch_fp64<false, true>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
-                  else launch_fp64<false, false>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick); }
-    } else if (precision == ASTER_MIXED) {
-        if (pn) { if (guard) launch_mixed<true, true>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
-                  else launch_mixed<true, false>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick); }
-        else    { if (guard) launch_mixed<false, true>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
-                  else launch_mixed<false, false>(grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick); }
-    } else {
-        return ASTER_ERR_INVALID_ARG;
-    }
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    const int pnl = pn_level(p);
+    if (pnl == 2) launch_pnl<2>(precision, guard, grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
+    else if (pnl == 1) launch_pnl<1>(precision, guard, grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
+    else launch_pnl<0>(precision, guard, grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
     ASTER_CUDA(cudaGetLastError());
     c->stats.kernels += 1;
     if (ns > 1) {
@@ -415,7 +424,6 @@ extern "C" int aster_allpairs(aster_ctx* c, const aster_params* p, int precision
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
-    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
     cudaEventRecord(c->ev[0], c->stream);
@@ -435,7 +443,6 @@ extern "C" int aster_allpairs_targets(aster_ctx* c, const aster_params* p, int p
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
-    if (p->force_law & (ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;
     for (int64_t t = 0; t < nt; ++t)
         if (targets[t] < 0 || targets[t] >= c->n) return ASTER_ERR_INVALID_ARG;
     ASTER_TRY(aster_begin(c));

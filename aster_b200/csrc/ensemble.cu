@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "aster_internal.cuh"
+#include "pn.cuh"
 
 namespace {
 
@@ -63,74 +64,6 @@ struct EnsSlab<false> {
     double4 x[64];  // (x, y, z, m)
     double4 v[64];  // (vx, vy, vz, |v|^2)
 };
-
-// Post-Newtonian constants and the terms in use: f bit 0 = 1PN, bit 1 = 2PN,
-// bit 2 = 2.5PN (warp-uniform). PN level PNL (a template parameter): 0 Newton
-// only, 1 Newton + 1PN, 2 Newton + the terms f selects.
-template <class T>
-struct PnK {
-    T c2, c4, c5;
-    int f;
-};
-
-// Acceleration on body i from every body of the slab, divided by G, in three
-// sums kept apart so that the small post-Newtonian corrections are not lost
-// against the Newtonian sum in FP32: aN (Newton), a1 (1PN), a2 (2PN + 2.5PN).
-// j == i contributes 0 (zero separation and relative velocity). With n the
-// unit vector from j to i (the reference's -norm):
-//   1PN : c^-2 m_j/r^2 [n A + (v_i - v_j) B]
-//   2PN : c^-4 { m_j/r^2 [n S_n + (v_i - v_j) S_v] + G^2 m_j/r^4 n S_m }
-//   2.5PN: c^-5 4/5 G m_i m_j/r^3 [(v_i - v_j) I_1 + n (n.(v_i - v_j)) I_2]
-// with A, B, S_n, S_v, S_m, I_1, I_2 the scalar brackets of get_pn1, get_pn2
-// and get_pn25.
-template <class T>
-struct PnPair {
-    // per-pair inputs
-    T nx, ny, nz, dvx, dvy, dvz, inv, inv2, mi, mj, vi2, vj2, v12, nv1, nv2, G;
-    __device__ __forceinline__ void pn1(T c2, T& px, T& py, T& pz) const {
-        const T A = -vi2 - T(2) * vj2 + T(4) * v12 + T(1.5) * nv2 * nv2 + (T(5) * mi + T(4) * mj) * G * inv;
-        const T B = T(4) * nv1 - T(3) * nv2;
-        const T f = mj * inv2 * c2;
-        px += (nx * A + dvx * B) * f;
-        py += (ny * A + dvy * B) * f;
-        pz += (nz * A + dvz * B) * f;
-    }
-    __device__ __forceinline__ void pn2(T c4, T& qx, T& qy, T& qz) const {
-        const T nv22 = nv2 * nv2, nv12 = nv1 * nv1;
-        const T p1 = G * mi * inv, p2 = G * mj * inv;
-        const T Sn = T(-2) * vj2 * vj2 + T(4) * vj2 * v12 - T(2) * v12 * v12 + T(1.5) * vi2 * nv22 +
-                     T(4.5) * vj2 * nv22 - T(6) * v12 * nv22 - T(1.875) * nv22 * nv22 +
-                     p1 * (T(-3.75) * vi2 + T(1.25) * vj2 - T(2.5) * v12 + T(19.5) * nv12 - T(39) * nv1 * nv2 +
-                           T(8.5) * nv22) +
-                     p2 * (T(4) * vj2 - T(8) * v12 + T(2) * nv12 - T(4) * nv1 * nv2 - T(6) * nv22);
-        const T Sv = vi2 * nv2 + T(4) * vj2 * nv1 - T(5) * vj2 * nv2 - T(4) * v12 * nv1 + T(4) * v12 * nv2 -
-                     T(6) * nv1 * nv22 + T(4.5) * nv22 * nv2 + p1 * (T(-15.75) * nv1 + T(13.75) * nv2) +
-                     p2 * (T(-2) * nv1 - T(2) * nv2);
-        const T Sm = T(-14.25) * mi * mi - T(9) * mj * mj - T(34.5) * mi * mj;
-        const T f = mj * inv2 * c4, g = G * G * mj * inv2 * inv2 * Sm * c4;
-        qx += f * (nx * Sn + dvx * Sv) + g * nx;
-        qy += f * (ny * Sn + dvy * Sv) + g * ny;
-        qz += f * (nz * Sn + dvz * Sv) + g * nz;
-    }
-    __device__ __forceinline__ void pn25(T c5, T& qx, T& qy, T& qz) const {
-        const T p1 = G * mi * inv, p2 = G * mj * inv;
-        const T sq = dvx * dvx + dvy * dvy + dvz * dvz;
-        const T I1 = -sq + T(2) * p1 - T(8) * p2;
-        const T I2 = (nv1 - nv2) * (T(3) * sq - T(6) * p1 + T(52) / T(3) * p2);
-        const T f = T(0.8) * G * mi * mj * inv * inv2 * c5;
-        qx += (dvx * I1 + nx * I2) * f;
-        qy += (dvy * I1 + ny * I2) * f;
-        qz += (dvz * I1 + nz * I2) * f;
-    }
-};
-
-template <int PNL, class T>
-__device__ __forceinline__ void pn_terms(const PnK<T>& k, const PnPair<T>& q, T& px, T& py, T& pz, T& qx, T& qy,
-                                         T& qz) {
-    if (PNL == 1 || (PNL == 2 && (k.f & 1))) q.pn1(k.c2, px, py, pz);
-    if (PNL == 2 && (k.f & 2)) q.pn2(k.c4, qx, qy, qz);
-    if (PNL == 2 && (k.f & 4)) q.pn25(k.c5, qx, qy, qz);
-}
 
 // Sums over j = j0, j0 + js, ... < n (js > 1: the lanes that share a target
 // split its sources).
@@ -209,7 +142,7 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
     EnsSlab<MIXED>& slab = reinterpret_cast<EnsSlab<MIXED>*>(ens_smem)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const float Gf = (float)G, epsf = (float)eps2;
-    const PnK<float> pkf{(float)pk.c2, (float)pk.c4, (float)pk.c5, pk.f};
+    const PnK<float> pkf = pn_float(pk);
     for (;;) {
         unsigned int w = 0;
         if (lane == 0) w = atomicAdd(work, 1u);
@@ -378,19 +311,6 @@ __global__ void k_unpack_ens(int64_t n, const double4* __restrict__ src, double*
     }
 }
 
-PnK<double> make_pn(const aster_params* p) {
-    PnK<double> k{0.0, 0.0, 0.0, 0};
-    k.f = ((p->force_law & ASTER_PN1) ? 1 : 0) | ((p->force_law & ASTER_PN2) ? 2 : 0) |
-          ((p->force_law & ASTER_PN25) ? 4 : 0);
-    if (k.f) {
-        const double ic = 1.0 / p->c;  // powers in the reference's order: inv_c * inv_c * ...
-        k.c2 = ic * ic;
-        k.c4 = ic * ic * ic * ic;
-        k.c5 = ic * ic * ic * ic * ic;
-    }
-    return k;
-}
-
 template <bool MIXED, int PNL, int UNROLL>
 int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_t nsteps, int wpb, int check_every,
                     bool use_graph) {
@@ -547,7 +467,7 @@ extern "C" int aster_ensemble_run(aster_ctx* c, const aster_params* p, int integ
     *c->ens.cancel_host = 0;
     const Coeffs k = make_coeffs(integrator, p->dt);
     // PN level: 2 when a 2PN or 2.5PN term is requested, else 1 for 1PN alone
-    const int pnl = (p->force_law & (ASTER_PN2 | ASTER_PN25)) ? 2 : ((p->force_law & ASTER_PN1) ? 1 : 0);
+    const int pnl = pn_level(p);
     cudaEventRecord(c->ev[0], c->stream);
     int st;
     if (precision == ASTER_MIXED)

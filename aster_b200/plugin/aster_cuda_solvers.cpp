@@ -32,7 +32,7 @@ aster_params CudaAllPairs::params() const {
     p.eps2 = _s->softening;
     p.theta = _s->theta;
     p.dt = _s->get_dt();
-    p.force_law = force_law.type & (ASTER_NEWTON | ASTER_PN1);
+    p.force_law = force_law.type & (ASTER_NEWTON | ASTER_PN1 | ASTER_PN2 | ASTER_PN25);
     p.morton_bits = 30;
     p.compat_mode = 0;
     p.reserved = 0;

@@ -21,7 +21,7 @@ namespace Aster {
 // Drop-in for Parallelized / SimpleGPU (src/utils/builder_endpoint.cpp:729-757,
 // src/solvers/SimpleGPU.cpp:17-71): compute_forces() uploads the bodies,
 // evaluates all pairs on the GPU and writes accelerations to bodies.accs,
-// honouring force_law (Newton, PN1), softening, G and c.
+// honouring force_law (Newton, PN1, PN2, PN2.5), softening, G and c.
 class CudaAllPairs : public Solver {
 public:
     explicit CudaAllPairs(Simulation* s, int precision = ASTER_MIXED, int device = 0);

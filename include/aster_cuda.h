@@ -49,8 +49,8 @@ extern "C" {
  *      (include/Aster/simulations/basic.h:39-53) ------------------------- */
 #define ASTER_NEWTON 0x0001
 #define ASTER_PN1 0x0010  /* get_pn1, c^-2 (src/physics/tool_chain_impl.cpp:110-118)  */
-#define ASTER_PN2 0x0100  /* get_pn2, c^-4 (tool_chain_impl.cpp:79-107); ensemble only */
-#define ASTER_PN25 0x1000 /* get_pn25, c^-5 (tool_chain_impl.cpp:65-77); ensemble only */
+#define ASTER_PN2 0x0100  /* get_pn2, c^-4 (tool_chain_impl.cpp:79-107); all-pairs and ensemble */
+#define ASTER_PN25 0x1000 /* get_pn25, c^-5 (tool_chain_impl.cpp:65-77); all-pairs and ensemble */
 
 /* ---- enums ------------------------------------------------------------- */
 #define ASTER_FP64 0   /* plain FP64 pair arithmetic                          */

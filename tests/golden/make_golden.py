@@ -22,6 +22,10 @@ Fixtures:
                             eps2 = 1e-4) for force laws NEWTON|PN1, NEWTON|PN2,
                             NEWTON|PN25 and all four terms: the force on body 1.
 
+  allpairs_pn_plummer256.npz  Parallelized::compute_forces on a lognormal-mass
+                            N=256 Plummer sphere with velocities x5, c = 10,
+                            eps2 = 1e-4, for NEWTON and the four PN force laws
+                            of pn_pairs.npz.
   saba_plummer256.npz       update_SABA1..10 with Parallelized: 4 steps each from one
                             N=256 Plummer state (eps2 = 1e-4, dt = 1e-3), and the
                             reference coefficient tables (GPU::saba_coeffs).
@@ -124,6 +128,18 @@ def pn_fixture(ref: Ref):
     np.savez_compressed(OUT / "pn_pairs.npz", **out)
 
 
+def allpairs_pn_fixture(ref: Ref):
+    pos, vel, m = gen.plummer(256, 1015, masses="lognormal")
+    vb = vel * 5.0
+    B = gen.bounding_cube(pos)
+    c, eps2 = 10.0, 1e-4
+    out = dict(pos=pos, vel=vb, m=m, c=c, eps2=eps2)
+    for name, law in {"newton": NEWTON, **PN_LAWS}.items():
+        ref.setup(pos, vb, m, G=1.0, c=c, eps2=eps2, box=B, force_law=law)
+        out[f"acc_{name}"] = ref.forces()
+    np.savez_compressed(OUT / "allpairs_pn_plummer256.npz", **out)
+
+
 def saba_fixture(ref: Ref):
     pos, vel, m = gen.plummer(256, 1008)
     eps2, dt, steps = 1e-4, 1e-3, 4
@@ -138,7 +154,7 @@ def saba_fixture(ref: Ref):
 
 
 FIXTURES = {"allpairs": allpairs_fixture, "leapfrog": leapfrog_fixture, "tree": tree_fixture,
-            "pn_pairs": pn_fixture, "saba": saba_fixture}
+            "pn_pairs": pn_fixture, "saba": saba_fixture, "allpairs_pn": allpairs_pn_fixture}
 
 
 def main():

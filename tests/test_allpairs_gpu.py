@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from aster_b200 import gen
-from aster_b200.api import FP64, MIXED, NEWTON, PN1, Params
+from aster_b200.api import FP64, MIXED, NEWTON, PN1, PN2, PN25, Params
 from conftest import golden, rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -42,6 +42,58 @@ def test_pn1_matches_reference_golden(ctx, prec, tol):
     # the PN part alone (acc_pn1 - newton) to 1e-4 relative in mixed precision
     newton = golden("allpairs_plummer512.npz")["acc"]
     assert rel_l2(a - newton, g["acc_pn1"] - newton) < (1e-10 if prec == FP64 else 1e-3)
+
+
+PN_LAWS = {"pn1": NEWTON | PN1, "pn2": NEWTON | PN2, "pn25": NEWTON | PN25, "all": NEWTON | PN1 | PN2 | PN25}
+
+
+@pytest.mark.parametrize("name", list(PN_LAWS))
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_pn_laws_match_reference_golden(ctx, name, prec):
+    """Parallelized::compute_forces with each post-Newtonian force law (N = 256,
+    c = 10; the 1PN, 2PN and 2.5PN parts are 0.15, 0.02 and 3e-5 of the
+    Newtonian sum). Total: FP64 1e-12, mixed 1e-6. Post-Newtonian part (law
+    minus the reference's Newtonian accelerations), as an absolute L2 bound:
+    FP64 1e-13 |Newton| + 1e-10 |part|; mixed 2e-7 |Newton| (the Newtonian
+    sum's own error) + 1e-5 |part| (FP32 post-Newtonian sums)."""
+    g = golden("allpairs_pn_plummer256.npz")
+    ctx.upload(g["pos"], g["vel"], g["m"])
+    p = Params(eps2=float(g["eps2"]), c=float(g["c"]), force_law=PN_LAWS[name])
+    a = ctx.allpairs(p, prec)
+    ref, newton = g[f"acc_{name}"], g["acc_newton"]
+    assert rel_l2(a, ref) < (1e-12 if prec == FP64 else 1e-6)
+    part = ref - newton
+    bound = (1e-13 * np.linalg.norm(newton) + 1e-10 * np.linalg.norm(part) if prec == FP64
+             else 2e-7 * np.linalg.norm(newton) + 1e-5 * np.linalg.norm(part))
+    assert np.linalg.norm((a - newton) - part) < bound
+
+
+def test_pn_laws_in_si_units(ctx, orc):
+    """A star of 2e30 kg with 500 planets and planetesimals at 0.05-5 AU on
+    near-circular orbits, SI units, physical c, every PN term: FP64 equals the
+    oracle to 1e-12 and the mixed kernel (FP32 post-Newtonian sums, written so
+    that m^2 and c^-5 never appear alone) stays finite and within 1e-6."""
+    rng = np.random.default_rng(23)
+    n = 501
+    G, msun, au = 6.674e-11, 2.0e30, 1.495978707e11
+    r = au * np.exp(rng.uniform(np.log(0.05), np.log(5.0), n - 1))
+    ang = rng.uniform(0, 2 * np.pi, n - 1)
+    pos = np.zeros((n, 3))
+    vel = np.zeros((n, 3))
+    pos[1:, 0], pos[1:, 1] = r * np.cos(ang), r * np.sin(ang)
+    pos[1:, 2] = r * rng.normal(0, 0.01, n - 1)
+    vc = np.sqrt(G * msun / r)
+    vel[1:, 0], vel[1:, 1] = -vc * np.sin(ang), vc * np.cos(ang)
+    m = np.r_[msun, 6e24 * np.exp(rng.uniform(np.log(1e-3), np.log(300.0), n - 1))]
+    law = NEWTON | PN1 | PN2 | PN25
+    p = Params(G=G, c=299792458.0, eps2=0.0, force_law=law)
+    ctx.upload(pos, vel, m)
+    ref = orc.allpairs(pos, m, G, 0.0, vel=vel, inv_c=1.0 / 299792458.0, pn=law)
+    a64 = ctx.allpairs(p, FP64)
+    a32 = ctx.allpairs(p, MIXED)
+    assert rel_l2(a64, ref) < 1e-12
+    assert np.isfinite(a32).all()
+    assert rel_l2(a32, ref) < 1e-6
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 31, 33, 127, 129, 1000, 4097])

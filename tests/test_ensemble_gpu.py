@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from aster_b200 import gen
-from aster_b200.api import (ERR_CANCELLED, FP64, LEAPFROG, MIXED, NEWTON, PN1, PN2, PN25, YOSHIDA4, AsterError,
+from aster_b200.api import (ERR_CANCELLED, FP64, SOLVER_LBVH, LEAPFROG, MIXED, NEWTON, PN1, PN2, PN25, YOSHIDA4, AsterError,
                             Params)
 
 pytestmark = pytest.mark.gpu
@@ -85,14 +85,48 @@ def test_higher_pn_ensemble_vs_oracle(ctx, orc, law):
     assert _per_system_err(mv, ov, off) < 1e-5
 
 
-def test_higher_pn_is_ensemble_only(ctx):
+def test_post_newtonian_terms_are_rejected_by_the_tree_solver(ctx):
+    """The LBVH walk sums Newtonian monopoles only: any post-Newtonian bit is
+    refused there (the all-pairs solver takes every term)."""
     pos, vel, m = gen.plummer(256, 3)
     ctx.upload(pos, vel, m)
-    p = Params(G=1.0, c=5.0, eps2=1e-3, dt=1e-3, force_law=NEWTON | PN2)
-    for call in (lambda: ctx.allpairs(p, FP64), lambda: ctx.kdk_steps(p, 1)):
-        with pytest.raises(AsterError) as ei:
-            call()
-        assert ei.value.status == 9  # ASTER_ERR_UNSUPPORTED
+    for law in (NEWTON | PN1, NEWTON | PN2, NEWTON | PN25):
+        p = Params(G=1.0, c=5.0, eps2=1e-3, dt=1e-3, force_law=law)
+        for call in (lambda: ctx.lbvh_forces(p, FP64), lambda: ctx.kdk_steps(p, 1, SOLVER_LBVH)):
+            with pytest.raises(AsterError) as ei:
+                call()
+            assert ei.value.status == 9  # ASTER_ERR_UNSUPPORTED
+    assert np.isfinite(ctx.allpairs(Params(G=1.0, c=5.0, eps2=1e-3, force_law=NEWTON | PN2), FP64)).all()
+
+
+def test_higher_pn_ensemble_in_si_units(ctx):
+    """Sun-like central masses, AU distances, km/s velocities and the physical
+    speed of light: the FP32 post-Newtonian terms stay in range (m_i^2 and
+    c^-5 alone would not) and the mixed kernel agrees with FP64."""
+    rng = np.random.default_rng(17)
+    nsys, k = 64, 4
+    off = np.arange(nsys + 1) * k
+    au, msun = 1.495978707e11, 1.989e30
+    pos = np.zeros((nsys * k, 3))
+    vel = np.zeros((nsys * k, 3))
+    m = np.zeros(nsys * k)
+    for s in range(nsys):
+        m[s * k] = msun * rng.uniform(0.5, 2.0)
+        for b in range(1, k):
+            r = au * rng.uniform(0.05, 2.0)
+            ang = rng.uniform(0, 2 * np.pi)
+            pos[s * k + b] = [r * np.cos(ang), r * np.sin(ang), 0.0]
+            vc = np.sqrt(6.674e-11 * m[s * k] / r)
+            vel[s * k + b] = [-vc * np.sin(ang), vc * np.cos(ang), 0.0]
+            m[s * k + b] = 6e24 * rng.uniform(0.1, 300.0)
+    p = Params(G=6.674e-11, c=299792458.0, eps2=0.0, dt=3600.0, force_law=NEWTON | PN1 | PN2 | PN25)
+    out = {}
+    for prec in (FP64, MIXED):
+        ctx.ensemble_upload(off, pos, vel, m)
+        ctx.ensemble_run(p, 24, LEAPFROG, prec)
+        out[prec] = ctx.ensemble_download()
+    assert np.isfinite(out[MIXED][0]).all() and np.isfinite(out[MIXED][1]).all()
+    assert _per_system_err(out[MIXED][0], out[FP64][0], off) < 1e-6
 
 
 def test_newtonian_ensemble_and_edge_sizes(ctx, orc):

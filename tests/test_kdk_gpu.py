@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from aster_b200 import gen
-from aster_b200.api import FP64, MIXED, SOLVER_ALLPAIRS, SOLVER_LBVH, Params
+from aster_b200.api import FP64, MIXED, NEWTON, PN1, PN2, PN25, SOLVER_ALLPAIRS, SOLVER_LBVH, Params
 from conftest import golden, rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -51,6 +51,22 @@ def test_kdk_matches_oracle_kdk(ctx, orc):
     assert rel_l2(pos, op) < 1e-13
     assert rel_l2(vel, ov) < 1e-12
     assert rel_l2(acc, oa) < 1e-12
+
+
+@pytest.mark.parametrize("prec,tol", [(FP64, 1e-12), (MIXED, 1e-6)])
+def test_kdk_with_every_pn_term_matches_oracle(ctx, orc, prec, tol):
+    """KDK on the all-pairs solver with Newton + 1PN + 2PN + 2.5PN (c = 10,
+    velocities x5, 5 steps) against the oracle's KDK with the same law."""
+    g = golden("allpairs_pn_plummer256.npz")
+    law = NEWTON | PN1 | PN2 | PN25
+    p = Params(eps2=float(g["eps2"]), dt=1e-3, c=float(g["c"]), force_law=law)
+    ctx.upload(g["pos"], g["vel"], g["m"])
+    ctx.kdk_steps(p, 5, SOLVER_ALLPAIRS, prec)
+    pos, vel, acc = ctx.download()
+    op, ov, oa, _ = orc.kdk(g["pos"], g["vel"], g["m"], p.dt, 5, eps2=p.eps2, inv_c=1.0 / p.c, pn=law)
+    assert rel_l2(pos, op) < tol
+    assert rel_l2(vel, ov) < tol
+    assert rel_l2(acc, oa) < tol
 
 
 def test_energy_matches_oracle(ctx, orc):

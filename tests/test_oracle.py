@@ -26,6 +26,21 @@ def test_pn1_matches_reference_golden(orc):
 
 @pytest.mark.parametrize("name,law", [("pn1", NEWTON | PN1), ("pn2", NEWTON | PN2), ("pn25", NEWTON | PN25),
                                       ("all", NEWTON | PN1 | PN2 | PN25)])
+def test_allpairs_pn_matches_reference_golden(orc, name, law):
+    """The oracle's all-pairs sum against Parallelized::compute_forces with
+    each post-Newtonian force law (N = 256, c = 10): the total to 1e-14 and
+    the post-Newtonian part (law minus Newton) to 1e-10 of its own size."""
+    g = golden("allpairs_pn_plummer256.npz")
+    inv_c, eps2 = 1.0 / float(g["c"]), float(g["eps2"])
+    a = orc.allpairs(g["pos"], g["m"], 1.0, eps2, vel=g["vel"], inv_c=inv_c, pn=law)
+    newton = orc.allpairs(g["pos"], g["m"], 1.0, eps2)
+    assert rel_l2(newton, g["acc_newton"]) < 1e-14
+    assert rel_l2(a, g[f"acc_{name}"]) < 1e-14
+    assert rel_l2(a - newton, g[f"acc_{name}"] - g["acc_newton"]) < 1e-10
+
+
+@pytest.mark.parametrize("name,law", [("pn1", NEWTON | PN1), ("pn2", NEWTON | PN2), ("pn25", NEWTON | PN25),
+                                      ("all", NEWTON | PN1 | PN2 | PN25)])
 def test_pn_terms_match_reference_golden(orc, name, law):
     """get_pn1 / get_pn2 / get_pn25 through compute_gravitational (force on
     body 1, divided by m1), c = 10 so every term is large enough to check:

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from aster_b200 import gen
-from aster_b200.api import FP64, MIXED, NEWTON, PN1, SOLVER_LBVH, Params
+from aster_b200.api import FP64, MIXED, NEWTON, PN1, PN2, PN25, SOLVER_LBVH, Params
 from conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -61,14 +61,16 @@ def test_allpairs_plugin_matches_reference_leapfrog(cuda_kdk):
     assert rel_l2(vo, rv) < 1e-12
 
 
-def test_pn1_through_the_plugin_matches_reference():
+@pytest.mark.parametrize("law", [NEWTON | PN1, NEWTON | PN1 | PN2 | PN25])
+def test_pn_through_the_plugin_matches_reference(law):
+    """CudaAllPairs reads the Solver's force_law like Parallelized does."""
     from oracle.oracle import Ref
     if not Ref.available():
         pytest.skip("reference build absent")
     pos, vel, m = gen.plummer(700, 62)
     vel = vel * 30.0
-    _, _, ao = plugin_run(pos, vel, m, c=100.0, force_law=NEWTON | PN1, nsteps=0)
-    ref = Ref().setup(pos, vel, m, G=1.0, c=100.0, eps2=1e-4, force_law=NEWTON | PN1)
+    _, _, ao = plugin_run(pos, vel, m, c=100.0, force_law=law, nsteps=0)
+    ref = Ref().setup(pos, vel, m, G=1.0, c=100.0, eps2=1e-4, force_law=law)
     assert rel_l2(ao, ref.forces()) < 1e-12
 
 
