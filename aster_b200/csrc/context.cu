@@ -119,7 +119,8 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
                       &c->tree.perm_alt, &c->tree.hist, &c->tree.digit_off, &c->tree.left, &c->tree.right,
                       &c->tree.parent, &c->tree.sib, &c->tree.rlo, &c->tree.rhi, &c->tree.counters, &c->tree.node_cm,
                       &c->tree.bmin, &c->tree.bmax, &c->tree.node_hi,
-                      &c->tree.node_lo, &c->tree.child, &c->tree.groups, &c->tree.crec, &c->tree.front};
+                      &c->tree.node_lo, &c->tree.child, &c->tree.groups, &c->tree.crec, &c->tree.front,
+                      &c->tree.node_v};
     for (DevBuf* b : bufs) b->release();
     DevBuf* ens[] = {&c->ens.pm, &c->ens.vel, &c->ens.off, &c->ens.order, &c->ens.counter,
                      &c->adj.ckpt, &c->adj.segx, &c->adj.lx, &c->adj.lv, &c->adj.lm, &c->adj.w,

@@ -232,8 +232,6 @@ static int kdk_check(aster_ctx* c, const aster_params* p, int solver, int precis
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
     if (solver != ASTER_SOLVER_ALLPAIRS && solver != ASTER_SOLVER_LBVH) return ASTER_ERR_INVALID_ARG;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
-    if (solver == ASTER_SOLVER_LBVH && (p->force_law & (ASTER_PN1 | ASTER_PN2 | ASTER_PN25)))
-        return ASTER_ERR_UNSUPPORTED;
     return ASTER_OK;
 }
 
@@ -291,8 +289,6 @@ extern "C" int aster_kdk_steps_host(aster_ctx* c, const aster_params* p, int sol
     ASTER_TRY(aster_check_params(p));
     if (solver != ASTER_SOLVER_ALLPAIRS && solver != ASTER_SOLVER_LBVH) return ASTER_ERR_INVALID_ARG;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
-    if (solver == ASTER_SOLVER_LBVH && (p->force_law & (ASTER_PN1 | ASTER_PN2 | ASTER_PN25)))
-        return ASTER_ERR_UNSUPPORTED;
     if (!c->copy_stream) ASTER_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};

@@ -31,8 +31,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "aster_internal.cuh"
+#include "pn.cuh"
 
 namespace {
 
@@ -404,11 +406,20 @@ constexpr int BU_LEAVES = ASTER_BU_LEAVES;
 
 __device__ __forceinline__ void bu_merge(const double4 cl, const double4 cr, const float4 l0, const float4 l1,
                                          const float4 h0, const float4 h1, double4& cm, float4& lo, float4& hi) {
-    // NodesArray::unite order: M = m_R + m_L; c = (c_R m_R + c_L m_L) / M
+    // NodesArray::unite order: M = m_R + m_L; c = (c_R m_R + c_L m_L) / M.
+    // A node without mass (M <= 0: only massless bodies below it) takes the
+    // midpoint (c_R + c_L) / 2, finite, so that its ancestors' centres stay
+    // finite too (unite leaves such a node's previous contents in place).
     const double M = __dadd_rn(cr.w, cl.w);
-    cm.x = __ddiv_rn(__dadd_rn(__dmul_rn(cr.x, cr.w), __dmul_rn(cl.x, cl.w)), M);
-    cm.y = __ddiv_rn(__dadd_rn(__dmul_rn(cr.y, cr.w), __dmul_rn(cl.y, cl.w)), M);
-    cm.z = __ddiv_rn(__dadd_rn(__dmul_rn(cr.z, cr.w), __dmul_rn(cl.z, cl.w)), M);
+    if (M > 0.0) {
+        cm.x = __ddiv_rn(__dadd_rn(__dmul_rn(cr.x, cr.w), __dmul_rn(cl.x, cl.w)), M);
+        cm.y = __ddiv_rn(__dadd_rn(__dmul_rn(cr.y, cr.w), __dmul_rn(cl.y, cl.w)), M);
+        cm.z = __ddiv_rn(__dadd_rn(__dmul_rn(cr.z, cr.w), __dmul_rn(cl.z, cl.w)), M);
+    } else {
+        cm.x = __dmul_rn(0.5, __dadd_rn(cr.x, cl.x));
+        cm.y = __dmul_rn(0.5, __dadd_rn(cr.y, cl.y));
+        cm.z = __dmul_rn(0.5, __dadd_rn(cr.z, cl.z));
+    }
     cm.w = M;
     lo = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
     hi = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
@@ -564,6 +575,58 @@ __global__ void __launch_bounds__(256) k_bottom_up_front(int64_t n, const int32_
     }
 }
 
+// Node velocities for the post-Newtonian walk, in NodesArray::unite form
+// (src/solvers/barnes_hut.cpp:150): leaf k holds the velocity of sorted body k,
+// an internal node the mass-weighted mean of its children,
+// v = (v_R m_R + v_L m_L) / M, with M the node mass from the bottom-up pass
+// (M <= 0: (v_R + v_L) / 2). One climb per leaf with the arrival counters of
+// the internal nodes (zero on entry); the second arrival merges. Only the
+// post-Newtonian walk needs it, so it is a pass of its own.
+__global__ void __launch_bounds__(256) k_node_vel(int64_t n, const int32_t* __restrict__ parent,
+                                                  const int32_t* __restrict__ sib, const int32_t* __restrict__ perm,
+                                                  const double4* __restrict__ vel, const double4* __restrict__ node_cm,
+                                                  uint32_t* __restrict__ counters, double4* __restrict__ node_v,
+                                                  int* __restrict__ err) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double4 v = vel[perm[k]];
+        v.w = 0.0;
+        node_v[k] = v;
+        int32_t cur = (int32_t)k;
+        int32_t par = n >= 2 ? parent[cur] : -1, sb = n >= 2 ? sib[cur] : 0;
+        for (int level = 0; par >= 0; ++level) {
+            if (level >= MAX_CLIMB) {
+                atomicOr(err, ASTER_DEVERR_TREE);
+                break;
+            }
+            __threadfence();  // release: this chain's node velocity
+            if (atomicAdd(&counters[par - n], 1u) == 0u) break;  // first arrival: the sibling finishes it
+            __threadfence();  // acquire: the sibling's
+            const int32_t so = sb >= 0 ? sb : ~sb;
+            const double4 ov = ld_cg(node_v + so);
+            const double mc = node_cm[cur].w, mo = node_cm[so].w, M = node_cm[par].w;
+            const bool right = sb < 0;  // cur is the right child
+            const double4 vR = right ? v : ov, vL = right ? ov : v;
+            const double mR = right ? mc : mo, mL = right ? mo : mc;
+            double4 pv;
+            if (M > 0.0) {
+                pv.x = __ddiv_rn(__dadd_rn(__dmul_rn(vR.x, mR), __dmul_rn(vL.x, mL)), M);
+                pv.y = __ddiv_rn(__dadd_rn(__dmul_rn(vR.y, mR), __dmul_rn(vL.y, mL)), M);
+                pv.z = __ddiv_rn(__dadd_rn(__dmul_rn(vR.z, mR), __dmul_rn(vL.z, mL)), M);
+            } else {
+                pv.x = __dmul_rn(0.5, __dadd_rn(vR.x, vL.x));
+                pv.y = __dmul_rn(0.5, __dadd_rn(vR.y, vL.y));
+                pv.z = __dmul_rn(0.5, __dadd_rn(vR.z, vL.z));
+            }
+            pv.w = 0.0;
+            node_v[par] = pv;
+            v = pv;
+            cur = par;
+            par = parent[cur];
+            sb = sib[cur];
+        }
+    }
+}
+
 // Per internal node, after the climb (no dependencies, fully parallel): the
 // squared opening radius r_crit = l/theta + |com - box centre| (l = longest
 // AABB side; FP64, rounded up to FP32) and the traversal records
@@ -652,6 +715,14 @@ struct WalkShared {
     double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST_FP64];  // FP64 (com, mass)
 };
 
+// Post-Newtonian walk: each list entry also carries the node's velocity
+// (vx, vy, vz, |v|^2), FP32 for the mixed walk and FP64 for the FP64 walk.
+template <bool MIXED>
+struct WalkSharedPn : WalkShared<MIXED> {
+    float4 lvf[WALK_WARPS][MIXED ? WALK_LIST_MIXED : 1];
+    double4 lvd[WALK_WARPS][MIXED ? 1 : WALK_LIST_FP64];
+};
+
 __device__ __forceinline__ float warp_min_f(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
@@ -698,6 +769,61 @@ __device__ __forceinline__ void interact_f64(const double4 e, const double4 b, d
     az = fma(dz, s, az);
 }
 
+// One entry with a post-Newtonian force law: the Newtonian term into (ax, ay,
+// az) as interact2_f32/interact_f64 form it, the 1PN terms into p and the 2PN
+// and 2.5PN terms into q (pn.cuh), all divided by G. Entry e (position, mass,
+// velocity ev) acts on the body at b with velocity vi and mass mi.
+template <int PNL, bool GUARD>
+__device__ __forceinline__ void interact_pn_f32(float ex, float ey, float ez, float em, const float4 ev,
+                                                const float3 b, const float4 vi, float mi, float eps2, float G,
+                                                const PnK<float>& k, float& ax, float& ay, float& az, float3& p,
+                                                float3& q) {
+    const float dx = ex - b.x, dy = ey - b.y, dz = ez - b.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+    float inv = rsqrt_approx(r2);
+    if (GUARD) inv = r2 > 0.f ? inv : 0.f;
+    const float inv2 = inv * inv;
+    const float sN = em * inv * inv2;
+    ax = fmaf(dx, sN, ax); ay = fmaf(dy, sN, ay); az = fmaf(dz, sN, az);
+    PnPair<float> w;
+    w.nx = -dx * inv; w.ny = -dy * inv; w.nz = -dz * inv;
+    w.dvx = vi.x - ev.x; w.dvy = vi.y - ev.y; w.dvz = vi.z - ev.z;
+    w.inv = inv; w.inv2 = inv2; w.mi = mi; w.mj = em; w.vi2 = vi.w; w.vj2 = ev.w;
+    w.v12 = vi.x * ev.x + vi.y * ev.y + vi.z * ev.z;
+    w.nv1 = w.nx * vi.x + w.ny * vi.y + w.nz * vi.z;
+    w.nv2 = w.nx * ev.x + w.ny * ev.y + w.nz * ev.z;
+    w.G = G;
+    pn_terms<PNL>(k, w, p.x, p.y, p.z, q.x, q.y, q.z);
+}
+
+template <int PNL, bool GUARD>
+__device__ __forceinline__ void interact_pn_f64(const double4 e, const double4 ev, const double4 b, const double4 vi,
+                                                double eps2, double G, const PnK<double>& k, double& ax, double& ay,
+                                                double& az) {
+    const double dx = e.x - b.x, dy = e.y - b.y, dz = e.z - b.z;
+    const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+    double inv = rsqrt(r2);
+    if (GUARD) inv = r2 > 0.0 ? inv : 0.0;
+    const double s = e.w * inv * inv * inv;
+    ax = fma(dx, s, ax); ay = fma(dy, s, ay); az = fma(dz, s, az);
+    PnPair<double> w;
+    w.nx = -dx * inv; w.ny = -dy * inv; w.nz = -dz * inv;
+    w.dvx = vi.x - ev.x; w.dvy = vi.y - ev.y; w.dvz = vi.z - ev.z;
+    w.inv = inv; w.inv2 = inv * inv; w.mi = b.w; w.mj = e.w; w.vi2 = vi.w; w.vj2 = ev.w;
+    w.v12 = vi.x * ev.x + vi.y * ev.y + vi.z * ev.z;
+    w.nv1 = w.nx * vi.x + w.ny * vi.y + w.nz * vi.z;
+    w.nv2 = w.nx * ev.x + w.ny * ev.y + w.nz * ev.z;
+    w.G = G;
+    pn_terms<PNL>(k, w, ax, ay, az, ax, ay, az);
+}
+
+__device__ __forceinline__ float4 vel_f4(const double4 v) {
+    return make_float4((float)v.x, (float)v.y, (float)v.z, (float)(v.x * v.x + v.y * v.y + v.z * v.z));
+}
+__device__ __forceinline__ double4 vel_d4(const double4 v) {
+    return make_double4(v.x, v.y, v.z, v.x * v.x + v.y * v.y + v.z * v.z);
+}
+
 __device__ __forceinline__ float max3_f32(float a, float b, float c) {
     float d;
     asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
@@ -739,15 +865,19 @@ __device__ __forceinline__ float2 box_dist2_pair(const float2 cx, const float2 c
 // centre cg (FP32 of hi - cg plus the double-single low part), so an
 // interaction needs one subtraction per axis; the group is compact, so the
 // relative coordinates keep FP32 precision of the separation.
-template <bool MIXED, bool GUARD, bool KICK>
-__global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS : 6) k_walk(
+// PNL > 0: the post-Newtonian walk (the terms pk selects, with the nodes'
+// velocities node_v); PNL == 0 is the Newtonian kernel.
+template <bool MIXED, bool GUARD, bool KICK, int PNL = 0>
+__global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK_MINBLOCKS : 6)) k_walk(
     int64_t n, const int2* __restrict__ groups, const unsigned int* __restrict__ ngroups_p,
     unsigned int* __restrict__ work, const float4* __restrict__ node_hi, const float4* __restrict__ node_lo,
     const float4* __restrict__ crec, const double4* __restrict__ node_cm, const int2* __restrict__ child,
     const int32_t* __restrict__ perm, double G, double eps2, double half_dt, double4* __restrict__ acc,
     double4* __restrict__ vel, int* __restrict__ err, int* __restrict__ stack_hw, int stack_limit,
-    int32_t* __restrict__ body_counts, unsigned long long* __restrict__ inter_count) {
-    __shared__ WalkShared<MIXED> sm;
+    int32_t* __restrict__ body_counts, unsigned long long* __restrict__ inter_count,
+    const double4* __restrict__ node_v, PnK<double> pk) {
+    using Shared = typename std::conditional<PNL != 0, WalkSharedPn<MIXED>, WalkShared<MIXED>>::type;
+    __shared__ Shared sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     const unsigned int ngroups = *ngroups_p;
@@ -791,6 +921,20 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
             c0 = node_cm[k0];
             c1 = two ? node_cm[k1] : c0;
         }
+        // post-Newtonian walk: the bodies' own velocities and the running
+        // 1PN (p) and 2PN + 2.5PN (q) sums of the mixed walk
+        float4 vf0 = make_float4(0.f, 0.f, 0.f, 0.f), vf1 = vf0;
+        double4 vd0 = make_double4(0, 0, 0, 0), vd1 = vd0;
+        float3 p0 = make_float3(0.f, 0.f, 0.f), q0 = p0, p1 = p0, q1 = p0;
+        if constexpr (PNL > 0) {
+            if (MIXED) {
+                vf0 = vel_f4(node_v[k0]);
+                vf1 = two ? vel_f4(node_v[k1]) : vf0;
+            } else {
+                vd0 = vel_d4(node_v[k0]);
+                vd1 = two ? vel_d4(node_v[k1]) : vd0;
+            }
+        }
 
         CompSum sx0, sy0, sz0, sx1, sy1, sz1;
         double dx0 = 0, dy0 = 0, dz0 = 0, dx1 = 0, dy1 = 0, dz1 = 0;
@@ -809,7 +953,49 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
             B[o + 2] = mass;
         };
 
+        // post-Newtonian walk: the velocity of list entry `pos`
+        auto put_v = [&](int pos, const double4 v) {
+            if constexpr (PNL > 0) {
+                if (MIXED) sm.lvf[warp][pos] = vel_f4(v);
+                else sm.lvd[warp][pos] = vel_d4(v);
+            }
+        };
+
         auto evaluate = [&](int cnt) {
+            if constexpr (PNL > 0) {  // one entry at a time, scalar
+                if (MIXED) {
+                    const float* A = reinterpret_cast<const float*>(&sm.lpa[warp][0]);
+                    const float* B = reinterpret_cast<const float*>(&sm.lpb[warp][0]);
+                    const float Gf = (float)G, e2 = (float)eps2;
+                    const PnK<float> pkf = pn_float(pk);
+                    float ax = 0.f, ay = 0.f, az = 0.f;
+                    for (int e = 0; e < cnt; ++e) {
+                        const int o = ((e >> 1) << 2) | (e & 1);
+                        interact_pn_f32<PNL, GUARD>(A[o], A[o + 2], B[o], B[o + 2], sm.lvf[warp][e], b0, vf0, h0.w,
+                                                    e2, Gf, pkf, ax, ay, az, p0, q0);
+                    }
+                    sx0.add(ax); sy0.add(ay); sz0.add(az);
+                    if (two) {
+                        float bx = 0.f, by = 0.f, bz = 0.f;
+                        for (int e = sub; e < cnt; e += lps) {
+                            const int o = ((e >> 1) << 2) | (e & 1);
+                            interact_pn_f32<PNL, GUARD>(A[o], A[o + 2], B[o], B[o + 2], sm.lvf[warp][e], b1, vf1,
+                                                        h1.w, e2, Gf, pkf, bx, by, bz, p1, q1);
+                        }
+                        sx1.add(bx); sy1.add(by); sz1.add(bz);
+                    }
+                } else {
+                    for (int e = 0; e < cnt; ++e)
+                        interact_pn_f64<PNL, GUARD>(sm.lcm[warp][e], sm.lvd[warp][e], c0, vd0, eps2, G, pk, dx0, dy0,
+                                                    dz0);
+                    if (two)
+                        for (int e = sub; e < cnt; e += lps)
+                            interact_pn_f64<PNL, GUARD>(sm.lcm[warp][e], sm.lvd[warp][e], c1, vd1, eps2, G, pk, dx1,
+                                                        dy1, dz1);
+                }
+                total += cnt;
+                return;
+            }
             if (MIXED) {
                 // an odd cnt has its last slot half zero-padded by the caller
                 const int np = (cnt + 1) >> 1;
@@ -861,6 +1047,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
                 } else {
                     sm.lcm[warp][0] = node_cm[0];
                 }
+                put_v(0, PNL > 0 ? node_v[0] : make_double4(0, 0, 0, 0));
             }
             lc = 1;
         }
@@ -912,6 +1099,10 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
                     if (aL) sm.lcm[warp][pos] = node_cm[ch.x];
                     if (aR) sm.lcm[warp][pos + (aL ? 1 : 0)] = node_cm[ch.y];
                 }
+                if constexpr (PNL > 0) {
+                    if (aL) put_v(pos, node_v[ch.x]);
+                    if (aR) put_v(pos + (aL ? 1 : 0), node_v[ch.y]);
+                }
             }
             lc += __popc(mAL) + __popc(mAR);
             __syncwarp();
@@ -935,6 +1126,24 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
                     if (m0) sm.lcm[warp][lane] = x0;
                     if (m1) sm.lcm[warp][32 + lane] = x1;
                 }
+                if constexpr (PNL > 0) {  // the entries' velocities: [FL, FL + rest) -> [0, rest), rest < 64
+                    const bool m0 = lane < rest, m1 = lane + 32 < rest;
+                    if (MIXED) {
+                        float4 x0 = make_float4(0, 0, 0, 0), x1 = x0;
+                        if (m0) x0 = sm.lvf[warp][FL + lane];
+                        if (m1) x1 = sm.lvf[warp][FL + 32 + lane];
+                        __syncwarp();
+                        if (m0) sm.lvf[warp][lane] = x0;
+                        if (m1) sm.lvf[warp][32 + lane] = x1;
+                    } else {
+                        double4 x0 = make_double4(0, 0, 0, 0), x1 = x0;
+                        if (m0) x0 = sm.lvd[warp][FL + lane];
+                        if (m1) x1 = sm.lvd[warp][FL + 32 + lane];
+                        __syncwarp();
+                        if (m0) sm.lvd[warp][lane] = x0;
+                        if (m1) sm.lvd[warp][32 + lane] = x1;
+                    }
+                }
                 lc = rest;
                 __syncwarp();
             }
@@ -955,6 +1164,13 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
         wtotal += (unsigned long long)total * (unsigned long long)gr.y;
         // secondary bodies: add the lps partial sums (aligned lane groups)
         double s1x = MIXED ? sx1.value() : dx1, s1y = MIXED ? sy1.value() : dy1, s1z = MIXED ? sz1.value() : dz1;
+        if constexpr (PNL > 0) {
+            if (MIXED) {
+                s1x += (double)p1.x + (double)q1.x;
+                s1y += (double)p1.y + (double)q1.y;
+                s1z += (double)p1.z + (double)q1.z;
+            }
+        }
         if (two) {
             for (int o = lps >> 1; o >= 1; o >>= 1) {
                 s1x += __shfl_xor_sync(0xffffffffu, s1x, o);
@@ -970,7 +1186,13 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
             if (q) {
                 ax = G * s1x; ay = G * s1y; az = G * s1z;
             } else if (MIXED) {
-                ax = G * sx0.value(); ay = G * sy0.value(); az = G * sz0.value();
+                if constexpr (PNL > 0) {
+                    ax = G * (sx0.value() + ((double)p0.x + (double)q0.x));
+                    ay = G * (sy0.value() + ((double)p0.y + (double)q0.y));
+                    az = G * (sz0.value() + ((double)p0.z + (double)q0.z));
+                } else {
+                    ax = G * sx0.value(); ay = G * sy0.value(); az = G * sz0.value();
+                }
             } else {
                 ax = G * dx0; ay = G * dy0; az = G * dz0;
             }
@@ -990,10 +1212,10 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, MIXED ? ASTER_WALK_MINBLOCKS 
     }
 }
 
-template <bool MIXED, bool GUARD, bool KICK>
+template <bool MIXED, bool GUARD, bool KICK, int PNL = 0>
 int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts) {
     LbvhBufs& t = c->tree;
-    auto kern = k_walk<MIXED, GUARD, KICK>;
+    auto kern = k_walk<MIXED, GUARD, KICK, PNL>;
     int per_sm = 0;
     ASTER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WALK_WARPS * 32, 0));
     if (per_sm < 1) per_sm = 1;
@@ -1005,7 +1227,7 @@ int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts) {
         c->n, t.groups.as<int2>(), gcount, gcount + 1, t.node_hi.as<float4>(), t.node_lo.as<float4>(),
         t.crec.as<float4>(), t.node_cm.as<double4>(), t.child.as<int2>(), t.perm.as<int32_t>(), p->G, p->eps2, 0.5 * p->dt,
         c->acc.as<double4>(), c->vel.as<double4>(), c->err_dev, c->stack_hw_dev, c->walk_stack_limit, counts,
-        red_inter(c));
+        red_inter(c), PNL > 0 ? t.node_v.as<double4>() : nullptr, make_pn(p));
     ASTER_CUDA(cudaGetLastError());
     return ASTER_OK;
 }
@@ -1166,14 +1388,37 @@ int aster_lbvh_build_dev(aster_ctx* c, const aster_params* p, bool box_ready) {
 int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, bool kick, int32_t* counts) {
     ASTER_CUDA(cudaMemsetAsync(red_groups(c) + 1, 0, sizeof(unsigned int), c->stream));  // work counter
     const bool guard = !(p->eps2 > 0.0);
-    if (precision == ASTER_MIXED) {
+    if (precision != ASTER_MIXED && precision != ASTER_FP64) return ASTER_ERR_INVALID_ARG;
+    const bool mixed = precision == ASTER_MIXED;
+    if (pn_level(p) > 0) {
+        // post-Newtonian law: node velocities from the current body velocities
+        // (one climb, fresh arrival counters), then the walk with the pair law
+        LbvhBufs& t = c->tree;
+        const int64_t n = c->n;
+        ASTER_TRY(t.node_v.ensure((size_t)2 * n * sizeof(double4)));
+        if (n >= 2) ASTER_CUDA(cudaMemsetAsync(t.counters.ptr, 0, (size_t)(n - 1) * sizeof(uint32_t), c->stream));
+        const int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 8);
+        k_node_vel<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.sib.as<int32_t>(), t.perm.as<int32_t>(),
+                                                c->vel.as<double4>(), t.node_cm.as<double4>(),
+                                                t.counters.as<uint32_t>(), t.node_v.as<double4>(), c->err_dev);
+        ASTER_CUDA(cudaGetLastError());
+        c->stats.kernels += 1;
+        if (mixed) {
+            if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true, 2>(c, p, counts) : launch_walk<true, true, false, 2>(c, p, counts)); }
+            else       { ASTER_TRY(kick ? launch_walk<true, false, true, 2>(c, p, counts) : launch_walk<true, false, false, 2>(c, p, counts)); }
+        } else {
+            if (guard) { ASTER_TRY(kick ? launch_walk<false, true, true, 2>(c, p, counts) : launch_walk<false, true, false, 2>(c, p, counts)); }
+            else       { ASTER_TRY(kick ? launch_walk<false, false, true, 2>(c, p, counts) : launch_walk<false, false, false, 2>(c, p, counts)); }
+        }
+        c->stats.kernels += 1;
+        return ASTER_OK;
+    }
+    if (mixed) {
         if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true>(c, p, counts) : launch_walk<true, true, false>(c, p, counts)); }
         else       { ASTER_TRY(kick ? launch_walk<true, false, true>(c, p, counts) : launch_walk<true, false, false>(c, p, counts)); }
-    } else if (precision == ASTER_FP64) {
+    } else {
         if (guard) { ASTER_TRY(kick ? launch_walk<false, true, true>(c, p, counts) : launch_walk<false, true, false>(c, p, counts)); }
         else       { ASTER_TRY(kick ? launch_walk<false, false, true>(c, p, counts) : launch_walk<false, false, false>(c, p, counts)); }
-    } else {
-        return ASTER_ERR_INVALID_ARG;
     }
     c->stats.kernels += 1;
     return ASTER_OK;
@@ -1276,7 +1521,6 @@ extern "C" int aster_lbvh_forces(aster_ctx* c, const aster_params* p, int precis
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
-    if (p->force_law & (ASTER_PN1 | ASTER_PN2 | ASTER_PN25)) return ASTER_ERR_UNSUPPORTED;
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
     int32_t* cnt = nullptr;

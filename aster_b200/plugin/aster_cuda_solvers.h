@@ -45,7 +45,8 @@ protected:
 
 // Drop-in for Barnes_Hut / BH_hyper (src/solvers/barnes_hut.cpp:402-418,
 // src/solvers/full_GPU.cpp:519-527): LBVH build + warp-group walk at
-// Simulation::theta (Newtonian force law only).
+// Simulation::theta; with post-Newtonian bits each accepted node acts with
+// its mass-weighted velocity, as Barnes_Hut::get_node_body does.
 class CudaLBVH : public CudaAllPairs {
 public:
     explicit CudaLBVH(Simulation* s, int precision = ASTER_MIXED, int device = 0);

@@ -24,6 +24,9 @@
  *                       include/Aster/kernels/BHH_specific.cl.h:171-272 (compat: body index)
  *   orc_bottom_up       src/solvers/barnes_hut.cpp:137-152 (NodesArray::unite) + new AABB/opening radius
  *   orc_lbvh_forces     new group-based traversal (same decisions as the GPU kernel)
+ *   orc_node_velocities src/solvers/barnes_hut.cpp:150 (NodesArray::unite, velocities)
+ *   orc_lbvh_forces_pn  the traversal with the pair law of compute_gravitational and node
+ *                       velocities, as Barnes_Hut::get_node_body (barnes_hut.cpp:202-258)
  *   orc_kdk             src/physics/tool_chain_impl.cpp:169-185 restated as kick-drift-kick
  *                       with the acceleration cached across steps
  *   orc_saba            src/integrators/SABA.cpp:14-553 (update_SABA1..10, CPU forms;
@@ -677,6 +680,9 @@ static float f_ru(double d) { float f = (float)d; if ((double)f < d) f = nextaft
 
 /* Node moments in FP64 exactly as NodesArray::unite (barnes_hut.cpp:137-152):
  *   M = m_R + m_L; c = (c_R m_R + c_L m_L) / M   (component-wise, this order)
+ * except for a node without mass (M <= 0), which unite leaves with whatever
+ * the array held before: here c = (c_R + c_L) / 2 (finite; the node adds
+ * nothing to any force, and its ancestors' centres stay finite)
  * plus (new) the node AABB in FP32 (leaf: position rounded outwards; internal:
  * union of the children) and the squared opening radius
  *   r_crit = l/theta + |c - box_centre|, l = longest AABB side,
@@ -712,7 +718,9 @@ void orc_bottom_up(long n, const int32_t* left, const int32_t* right, const int3
         node_mass[v] = M;
         double lmax = 0.0, ctr[3];
         for (int a = 0; a < 3; ++a) {
-            node_com[3 * v + a] = (node_com[3 * R + a] * node_mass[R] + node_com[3 * L + a] * node_mass[L]) / M;
+            node_com[3 * v + a] = M > 0.0
+                ? (node_com[3 * R + a] * node_mass[R] + node_com[3 * L + a] * node_mass[L]) / M
+                : 0.5 * (node_com[3 * R + a] + node_com[3 * L + a]);
             bmin[3 * v + a] = fminf(bmin[3 * L + a], bmin[3 * R + a]);
             bmax[3 * v + a] = fmaxf(bmax[3 * L + a], bmax[3 * R + a]);
             double ext = (double)bmax[3 * v + a] - (double)bmin[3 * v + a];
@@ -770,6 +778,9 @@ typedef struct {
     long n; const int32_t *gstart, *gcount; const int32_t *left, *right, *perm; const double *pos, *node_mass,
         *node_com;
     const float* rcrit2; double G, eps2; double* acc; int32_t* count;
+    /* post-Newtonian walk (pn has a PN bit): body velocities (input order),
+     * node velocities (node order), 1/c */
+    const double *vel, *node_vel; double inv_c; int pn;
 } trav_ctx;
 
 static void trav_range(void* c_, long glo, long ghi) {
@@ -807,6 +818,22 @@ static void trav_range(void* c_, long glo, long ghi) {
             if (c->count) c->count[b] = (int32_t)nl;
             const double* x = c->pos + 3 * b;
             double ax = 0, ay = 0, az = 0;
+            if (c->pn & (PN1_FLAG | PN2_FLAG | PN25_FLAG)) {
+                /* the reference pair law with the node's mass-weighted velocity
+                 * (Barnes_Hut::get_node_body, barnes_hut.cpp:232-239) */
+                for (long e = 0; e < nl; ++e) {
+                    int32_t v = list[e];
+                    const double* y = c->node_com + 3 * v;
+                    double dx = y[0] - x[0], dy = y[1] - x[1], dz = y[2] - x[2];
+                    if (dx * dx + dy * dy + dz * dz + c->eps2 == 0.0) continue;
+                    double a[3];
+                    orc_pair_acc(c->G, c->inv_c, c->eps2, c->pn, c->node_mass[k], c->node_mass[v], c->vel + 3 * b,
+                                 c->node_vel + 3 * v, x, y, a);
+                    ax += a[0]; ay += a[1]; az += a[2];
+                }
+                c->acc[3 * b] = ax; c->acc[3 * b + 1] = ay; c->acc[3 * b + 2] = az;
+                continue;
+            }
             for (long e = 0; e < nl; ++e) {
                 int32_t v = list[e];
                 const double* y = c->node_com + 3 * v;
@@ -1022,7 +1049,58 @@ void orc_lbvh_forces(long n, int group, const int32_t* left, const int32_t* righ
     int32_t* gs = (int32_t*)malloc((size_t)n * 4);
     int32_t* gc = (int32_t*)malloc((size_t)n * 4);
     long ng = orc_groups(n, group, parent, rlo, rhi, gs, gc);
-    trav_ctx c = {n, gs, gc, left, right, perm, pos, node_mass, node_com, rcrit2, G, eps2, acc, body_count};
+    trav_ctx c = {n, gs, gc, left, right, perm, pos, node_mass, node_com, rcrit2, G, eps2, acc, body_count,
+                  NULL, NULL, 0.0, 0};
+    orc_parallel(ng, trav_range, &c);
+    free(gs);
+    free(gc);
+}
+
+/* Node velocities in NodesArray::unite form (barnes_hut.cpp:150): leaf k =
+ * vel[perm[k]]; internal v = (v_R m_R + v_L m_L) / M with M = node_mass[v]
+ * (from orc_bottom_up), or (v_R + v_L) / 2 when M <= 0. Post-order. */
+void orc_node_velocities(long n, const int32_t* left, const int32_t* right, const int32_t* perm,
+                         const double* vel, const double* node_mass, double* node_vel) {
+    for (long k = 0; k < n; ++k)
+        for (int a = 0; a < 3; ++a) node_vel[3 * k + a] = vel[3 * (long)perm[k] + a];
+    if (n < 2) return;
+    long total = 2 * n - 1;
+    int32_t* stack = (int32_t*)malloc((size_t)total * 4);
+    char* done = (char*)calloc((size_t)total, 1);
+    long sp = 0;
+    stack[sp++] = (int32_t)n;
+    while (sp > 0) {
+        int32_t v = stack[sp - 1];
+        int32_t L = left[v], R = right[v];
+        if (v >= n && (!done[L] && L >= n)) { stack[sp++] = L; continue; }
+        if (v >= n && (!done[R] && R >= n)) { stack[sp++] = R; continue; }
+        sp--;
+        if (v < n) { done[v] = 1; continue; }
+        double M = node_mass[v];
+        for (int a = 0; a < 3; ++a)
+            node_vel[3 * v + a] = M > 0.0
+                ? (node_vel[3 * R + a] * node_mass[R] + node_vel[3 * L + a] * node_mass[L]) / M
+                : 0.5 * (node_vel[3 * R + a] + node_vel[3 * L + a]);
+        done[v] = 1;
+    }
+    free(stack);
+    free(done);
+}
+
+/* The group walk with a post-Newtonian force law: the same lists as
+ * orc_lbvh_forces, each entry through orc_pair_acc with the target's velocity
+ * and the node's (node_vel from orc_node_velocities). */
+void orc_lbvh_forces_pn(long n, int group, const int32_t* left, const int32_t* right, const int32_t* parent,
+                        const int32_t* rlo, const int32_t* rhi, const int32_t* perm,
+                        const double* pos, const double* vel, const double* node_mass, const double* node_com,
+                        const double* node_vel, const float* rcrit2, double G, double inv_c, double eps2, int pn,
+                        double* acc, int32_t* body_count) {
+    if (group <= 0) group = ORC_GROUP;
+    int32_t* gs = (int32_t*)malloc((size_t)n * 4);
+    int32_t* gc = (int32_t*)malloc((size_t)n * 4);
+    long ng = orc_groups(n, group, parent, rlo, rhi, gs, gc);
+    trav_ctx c = {n, gs, gc, left, right, perm, pos, node_mass, node_com, rcrit2, G, eps2, acc, body_count,
+                  vel, node_vel, inv_c, pn};
     orc_parallel(ng, trav_range, &c);
     free(gs);
     free(gc);

@@ -177,6 +177,10 @@ class Orc:
                                           _D, _D, _F, _F, _F]
             lib.orc_lbvh_forces.argtypes = [ctypes.c_long, ctypes.c_int, _I32, _I32, _I32, _I32, _I32, _I32,
                                             _D, _D, _D, _F, ctypes.c_double, ctypes.c_double, _D, _I32]
+            lib.orc_node_velocities.argtypes = [ctypes.c_long, _I32, _I32, _I32, _D, _D, _D]
+            lib.orc_lbvh_forces_pn.argtypes = [ctypes.c_long, ctypes.c_int, _I32, _I32, _I32, _I32, _I32, _I32,
+                                               _D, _D, _D, _D, _D, _F, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_int, _D, _I32]
             lib.orc_groups.argtypes = [ctypes.c_long, ctypes.c_int, _I32, _I32, _I32, _I32, _I32]
             lib.orc_groups.restype = ctypes.c_long
             lib.orc_set_threads.argtypes = [ctypes.c_int]
@@ -324,6 +328,31 @@ class Orc:
         self.lib.orc_lbvh_forces(n, group, *[_p(a, _I32) for a in args], _p(pos, _D),
                                  _p(tree["node_mass"], _D), _p(tree["node_com"], _D), _p(tree["rcrit2"], _F),
                                  G, eps2, _p(acc, _D), _p(cnt, _I32))
+        return acc, cnt
+
+    def node_velocities(self, tree, perm, vel):
+        """Per node (2n - 1, node order): leaves the sorted body velocities,
+        internal nodes the mass-weighted mean of their children (unite form)."""
+        n = len(perm)
+        out = np.zeros((max(2 * n - 1, 1), 3))
+        args = [np.ascontiguousarray(a, dtype=np.int32) for a in (tree["left"], tree["right"], perm)]
+        self.lib.orc_node_velocities(n, *[_p(a, _I32) for a in args], _p(_c64(vel), _D),
+                                     _p(np.ascontiguousarray(tree["node_mass"], dtype=np.float64), _D), _p(out, _D))
+        return out
+
+    def lbvh_forces_pn(self, tree, perm, pos, vel, G, eps2, inv_c, pn, group=64):
+        """Group walk with a post-Newtonian force law (node velocities as
+        node_velocities); returns (acc per body, list length per body)."""
+        n = len(perm)
+        pos, vel = _c64(pos), _c64(vel)
+        nv = self.node_velocities(tree, perm, vel)
+        acc = np.zeros((n, 3))
+        cnt = np.zeros(n, np.int32)
+        args = [np.ascontiguousarray(a, dtype=np.int32)
+                for a in (tree["left"], tree["right"], tree["parent"], tree["range_lo"], tree["range_hi"], perm)]
+        self.lib.orc_lbvh_forces_pn(n, group, *[_p(a, _I32) for a in args], _p(pos, _D), _p(vel, _D),
+                                    _p(tree["node_mass"], _D), _p(tree["node_com"], _D), _p(nv, _D),
+                                    _p(tree["rcrit2"], _F), G, inv_c, eps2, pn, _p(acc, _D), _p(cnt, _I32))
         return acc, cnt
 
     def groups(self, tree, group=64):

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from aster_b200 import gen
-from aster_b200.api import (ERR_CANCELLED, FP64, SOLVER_LBVH, LEAPFROG, MIXED, NEWTON, PN1, PN2, PN25, YOSHIDA4, AsterError,
+from aster_b200.api import (ERR_CANCELLED, FP64, LEAPFROG, MIXED, NEWTON, PN1, PN2, PN25, YOSHIDA4, AsterError,
                             Params)
 
 pytestmark = pytest.mark.gpu
@@ -85,18 +85,18 @@ def test_higher_pn_ensemble_vs_oracle(ctx, orc, law):
     assert _per_system_err(mv, ov, off) < 1e-5
 
 
-def test_post_newtonian_terms_are_rejected_by_the_tree_solver(ctx):
-    """The LBVH walk sums Newtonian monopoles only: any post-Newtonian bit is
-    refused there (the all-pairs solver takes every term)."""
+def test_post_newtonian_terms_are_rejected_by_the_adjoint(ctx):
+    """The adjoint differentiates the Newtonian pair law only: any
+    post-Newtonian bit is refused there (every force solver takes them)."""
     pos, vel, m = gen.plummer(256, 3)
     ctx.upload(pos, vel, m)
     for law in (NEWTON | PN1, NEWTON | PN2, NEWTON | PN25):
         p = Params(G=1.0, c=5.0, eps2=1e-3, dt=1e-3, force_law=law)
-        for call in (lambda: ctx.lbvh_forces(p, FP64), lambda: ctx.kdk_steps(p, 1, SOLVER_LBVH)):
-            with pytest.raises(AsterError) as ei:
-                call()
-            assert ei.value.status == 9  # ASTER_ERR_UNSUPPORTED
-    assert np.isfinite(ctx.allpairs(Params(G=1.0, c=5.0, eps2=1e-3, force_law=NEWTON | PN2), FP64)).all()
+        with pytest.raises(AsterError) as ei:
+            ctx.adjoint(p, 2, pos, FP64, 1)
+        assert ei.value.status == 9  # ASTER_ERR_UNSUPPORTED
+        assert np.isfinite(ctx.allpairs(p, FP64)).all()
+        assert np.isfinite(ctx.lbvh_forces(p, FP64)).all()
 
 
 def test_higher_pn_ensemble_in_si_units(ctx):

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from aster_b200 import gen
-from aster_b200.api import FP64, MIXED, SOLVER_LBVH, Params
+from aster_b200.api import FP64, MIXED, NEWTON, PN1, PN2, PN25, SOLVER_ALLPAIRS, SOLVER_LBVH, Params
 from conftest import golden, rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -103,6 +103,82 @@ def test_walk_matches_oracle_lists(ctx, orc, theta):
     err = rel_l2(a64, exact)
     bound = {0.0: 1e-12, 0.3: 1e-3, 0.5: 3e-3, 0.8: 1e-2}[theta]  # monopole approximation error
     assert err < bound, err
+
+
+def test_massless_subtrees_stay_finite_and_cheap(ctx, orc):
+    """A massive Plummer sphere and a separate cloud of massless test
+    particles: subtrees without mass take the midpoint of their children's
+    centres (finite), so they and their ancestors are accepted or opened on
+    geometry like any other node. Tree, lists and forces equal the oracle's,
+    and a cloud body's list is no longer than a sphere body's several times
+    over (a node with no finite centre would be opened down to its leaves)."""
+    pos, vel, m = gen.plummer(20000, 1017, masses="lognormal")
+    cloud, cvel, _ = gen.plummer(20000, 1018)
+    pos2 = np.concatenate([pos, cloud * 0.5 + np.array([3.0, 0.0, 0.0])])
+    vel2 = np.concatenate([vel, cvel])
+    m2 = np.concatenate([m, np.zeros(20000)])
+    eps2 = 0.005 ** 2
+    ctx.upload(pos2, vel2, m2)
+    t = ctx.lbvh_build(Params(theta=0.5))
+    o = orc.lbvh(pos2, m2, 0.5)
+    assert np.isfinite(t["node_com"]).all()
+    np.testing.assert_array_equal(t["node_mass"], o["node_mass"])
+    np.testing.assert_array_equal(t["node_com"], o["node_com"])
+    np.testing.assert_array_equal(t["node_rcrit2"], o["rcrit2"])
+    oacc, ocnt = orc.lbvh_forces(o, o["perm"], pos2, 1.0, eps2)
+    p = Params(eps2=eps2, theta=0.5)
+    a64, c64 = ctx.lbvh_forces(p, FP64, list_counts=True)
+    a32 = ctx.lbvh_forces(p, MIXED)
+    np.testing.assert_array_equal(c64, ocnt)
+    assert rel_l2(a64, oacc) < 1e-12
+    assert rel_l2(a32, oacc) < 1e-6
+    assert ocnt[20000:].mean() < 3 * ocnt[:20000].mean()
+
+
+@pytest.mark.parametrize("law", [NEWTON | PN1, NEWTON | PN1 | PN2 | PN25])
+def test_pn_walk_matches_oracle(ctx, orc, law):
+    """Post-Newtonian force law on the tree: as Barnes_Hut::get_node_body,
+    every accepted node acts through compute_gravitational with the node's
+    mass-weighted velocity (the unite form). Same lists as the oracle's walk;
+    forces FP64 1e-12, mixed 1e-6; at theta = 0 (every node opened) the walk
+    is the all-pairs sum with the same law."""
+    pos, vel, m = gen.plummer(20000, 1019, masses="lognormal")
+    vel = vel * 5.0
+    c, eps2 = 10.0, 0.005 ** 2
+    ctx.upload(pos, vel, m)
+    p = Params(eps2=eps2, theta=0.5, c=c, force_law=law)
+    o = orc.lbvh(pos, m, 0.5)
+    oacc, ocnt = orc.lbvh_forces_pn(o, o["perm"], pos, vel, 1.0, eps2, 1.0 / c, law)
+    a64, c64 = ctx.lbvh_forces(p, FP64, list_counts=True)
+    a32 = ctx.lbvh_forces(p, MIXED)
+    np.testing.assert_array_equal(c64, ocnt)
+    assert rel_l2(a64, oacc) < 1e-12
+    assert rel_l2(a32, oacc) < 1e-6
+    newton, _ = orc.lbvh_forces(o, o["perm"], pos, 1.0, eps2)
+    assert rel_l2(oacc, newton) > 1e-3  # the post-Newtonian part is there
+    sub = slice(0, 4000)
+    ctx.upload(pos[sub], vel[sub], m[sub])
+    exact = orc.allpairs(pos[sub], m[sub], 1.0, eps2, vel=vel[sub], inv_c=1.0 / c, pn=law)
+    assert rel_l2(ctx.lbvh_forces(Params(eps2=eps2, theta=0.0, c=c, force_law=law), FP64), exact) < 1e-12
+
+
+def test_pn_lbvh_kdk_at_theta0_equals_allpairs_kdk(ctx):
+    """KDK on the tree with every post-Newtonian term (closing kick fused
+    into the walk, node velocities rebuilt each step from the half-kicked
+    velocities) at theta = 0 equals KDK on the all-pairs solver: FP64 1e-12,
+    mixed tree vs FP64 all-pairs 1e-6."""
+    pos, vel, m = gen.plummer(4096, 1020)
+    vel = vel * 5.0
+    p = Params(eps2=1e-4, dt=1e-3, theta=0.0, c=10.0, force_law=NEWTON | PN1 | PN2 | PN25)
+    out = {}
+    for solver, prec in ((SOLVER_LBVH, FP64), (SOLVER_LBVH, MIXED), (SOLVER_ALLPAIRS, FP64)):
+        ctx.upload(pos, vel, m)
+        ctx.kdk_steps(p, 3, solver, prec)
+        out[(solver, prec)] = ctx.download()
+    ref = out[(SOLVER_ALLPAIRS, FP64)]
+    for key, tol in (((SOLVER_LBVH, FP64), 1e-12), ((SOLVER_LBVH, MIXED), 1e-6)):
+        for k in range(3):
+            assert rel_l2(out[key][k], ref[k]) < tol, (key, k)
 
 
 def test_zero_softening_walk_is_finite(ctx):

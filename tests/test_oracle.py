@@ -266,3 +266,44 @@ def test_wh_energy_bounded(orc):
     for _ in range(10):
         p, v = orc.wh(p, v, m, 0.5, 1000)
         assert abs(energy(p, v) - e0) < 1e-7 * abs(e0)
+
+
+def test_massless_subtree_centres_are_finite(orc):
+    """A node whose bodies are all massless gets the midpoint of its children's
+    centres (unite would leave the array's previous contents); its massive
+    ancestors' centres are the mass-weighted ones, unaffected by it."""
+    rng = np.random.default_rng(31)
+    pos = np.concatenate([rng.normal(0.0, 1.0, (300, 3)), rng.normal(5.0, 0.2, (200, 3))])
+    m = np.concatenate([rng.uniform(0.5, 1.5, 300), np.zeros(200)])
+    o = orc.lbvh(pos, m, 0.5)
+    assert np.isfinite(o["node_com"]).all()
+    root = len(m)
+    assert o["node_mass"][root] == pytest.approx(m.sum(), rel=1e-14)
+    com = (pos * m[:, None]).sum(0) / m.sum()
+    assert np.abs(o["node_com"][root] - com).max() < 1e-12
+
+
+@pytest.mark.skipif(not Ref.available(), reason="reference build absent")
+def test_pn_tree_walk_at_theta0_matches_reference_barnes_hut(orc):
+    """The oracle's post-Newtonian tree walk against Barnes_Hut::compute_forces
+    with every PN term at theta = 0, where both open every node and sum the
+    pair law of compute_gravitational over all bodies."""
+    from aster_b200 import gen
+    pos, vel, m = gen.plummer(700, 66)
+    vel = vel * 30.0
+    law = NEWTON | PN1 | PN2 | PN25
+    ref = Ref().setup(pos, vel, m, G=1.0, c=100.0, eps2=1e-4, theta=0.0, force_law=law, solver="bh").forces()
+    o = orc.lbvh(pos, m, 0.0)
+    a, _ = orc.lbvh_forces_pn(o, o["perm"], pos, vel, 1.0, 1e-4, 0.01, law)
+    assert rel_l2(a, ref) < 1e-13
+
+
+def test_node_velocities_are_mass_weighted(orc):
+    """Node velocities in unite form: the root holds the mass-weighted mean
+    velocity of all bodies, each leaf its own body's velocity."""
+    rng = np.random.default_rng(41)
+    pos, vel, m = rng.normal(size=(500, 3)), rng.normal(size=(500, 3)), rng.uniform(0.1, 2.0, 500)
+    o = orc.lbvh(pos, m, 0.5)
+    nv = orc.node_velocities(o, o["perm"], vel)
+    np.testing.assert_array_equal(nv[:500], vel[o["perm"]])
+    assert np.abs(nv[500] - (vel * m[:, None]).sum(0) / m.sum()).max() < 1e-13

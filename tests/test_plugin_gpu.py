@@ -74,6 +74,21 @@ def test_pn_through_the_plugin_matches_reference(law):
     assert rel_l2(ao, ref.forces()) < 1e-12
 
 
+def test_pn_lbvh_plugin_matches_reference_bh_at_theta0():
+    """CudaLBVH with every post-Newtonian term at theta = 0 (every node
+    opened) against the reference's Barnes_Hut at theta = 0: both are the full
+    pair sum with compute_gravitational."""
+    from oracle.oracle import Ref
+    if not Ref.available():
+        pytest.skip("reference build absent")
+    pos, vel, m = gen.plummer(700, 66)
+    vel = vel * 30.0
+    law = NEWTON | PN1 | PN2 | PN25
+    _, _, ao = plugin_run(pos, vel, m, c=100.0, theta=0.0, force_law=law, solver=1, precision=FP64, nsteps=0)
+    ref = Ref().setup(pos, vel, m, G=1.0, c=100.0, eps2=1e-4, theta=0.0, force_law=law, solver="bh")
+    assert rel_l2(ao, ref.forces()) < 1e-12
+
+
 def test_lbvh_plugin_equals_c_abi(ctx):
     pos, vel, m = gen.plummer(20000, 63, masses="lognormal")
     po, vo, ao = plugin_run(pos, vel, m, eps2=0.005 ** 2, dt=5e-4, solver=1, precision=MIXED, cuda_kdk=True, nsteps=5)
