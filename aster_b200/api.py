@@ -42,7 +42,8 @@ ERR_CANCELLED = 8
 EXPORTS = [
     "aster_strerror", "aster_version", "aster_ctx_create", "aster_ctx_destroy", "aster_state_upload",
     "aster_state_upload_acc", "aster_kdk_steps_host",
-    "aster_state_download", "aster_state_size", "aster_allpairs", "aster_allpairs_targets", "aster_lbvh_build",
+    "aster_state_download", "aster_state_size", "aster_allpairs", "aster_allpairs_range", "aster_allpairs_targets",
+    "aster_lbvh_build",
     "aster_lbvh_forces", "aster_kdk_steps", "aster_saba_steps", "aster_wh_steps", "aster_record",
     "aster_record_columns", "aster_energy", "aster_get_stats", "aster_ensemble_upload",
     "aster_ensemble_download", "aster_ensemble_run", "aster_ensemble_energy", "aster_ensemble_cancel",
@@ -125,6 +126,8 @@ def load_library(path: Path | str | None = None) -> ctypes.CDLL:
     lib.aster_state_download.argtypes = [vp, vp, vp, vp]
     lib.aster_state_size.argtypes = [vp, ctypes.POINTER(i64)]
     lib.aster_allpairs.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, vp]
+    lib.aster_allpairs_range.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int64, ctypes.c_int64,
+                                         vp]
     lib.aster_allpairs_targets.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, i64, vp, vp]
     lib.aster_lbvh_build.argtypes = [vp, ctypes.POINTER(CParams), ctypes.POINTER(CTreeView)]
     lib.aster_lbvh_forces.argtypes = [vp, ctypes.POINTER(CParams), ctypes.c_int, vp, vp]
@@ -222,6 +225,15 @@ class Context:
         acc = np.empty((self.n, 3))
         cp = p.c_struct()
         self._check(self.lib.aster_allpairs(self.h, ctypes.byref(cp), precision, _ptr(acc)), "aster_allpairs")
+        return acc
+
+    def allpairs_range(self, p: Params, lower: int, upper: int = -1, precision: int = FP64):
+        """Accelerations of every body from the sources [lower, upper) only
+        (upper = -1: to the end), as Parallelized sums over set_bounds."""
+        acc = np.empty((self.n, 3))
+        cp = p.c_struct()
+        self._check(self.lib.aster_allpairs_range(self.h, ctypes.byref(cp), precision, lower, upper, _ptr(acc)),
+                    "aster_allpairs_range")
         return acc
 
     def allpairs_targets(self, p: Params, targets, precision: int = FP64):

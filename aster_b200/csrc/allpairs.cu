@@ -67,13 +67,13 @@ __device__ __forceinline__ void store_result(int64_t t, int64_t body, double ax,
 // PNL: 0 Newton, 1 Newton + 1PN, 2 Newton + the PN terms pk.f selects.
 template <int PNL, bool GUARD>
 __global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
-    int64_t n, int64_t nt, const int32_t* __restrict__ targets, const double4* __restrict__ pm,
+    int64_t j_lo, int64_t n, int64_t nt, const int32_t* __restrict__ targets, const double4* __restrict__ pm,
     const double4* __restrict__ vel, double G, double eps2, PnK<double> pk, int64_t slice_len, int nslices,
     double4* __restrict__ partial, double4* __restrict__ acc, double* __restrict__ out3, KickArgs kick) {
     __shared__ double4 sp[BLOCK];
     __shared__ double4 sv[PNL ? BLOCK : 1];  // (vx, vy, vz, |v|^2)
     const int slice = blockIdx.y;
-    const int64_t j0 = (int64_t)slice * slice_len;
+    const int64_t j0 = j_lo + (int64_t)slice * slice_len;  // sources [j_lo, n), sliced
     const int64_t j1 = min(n, j0 + slice_len);
     int64_t tt[IPT], bi[IPT];
     double xi[IPT], yi[IPT], zi[IPT], mi[IPT], vxi[IPT], vyi[IPT], vzi[IPT], v1sq[IPT];
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
 // 1PN terms and the 2PN/2.5PN terms in two further FP32 sums per target.
 template <int PNL, bool GUARD>
 __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
-    int64_t n, int64_t nt, const int32_t* __restrict__ targets, const float4* __restrict__ phi,
+    int64_t j_lo, int64_t n, int64_t nt, const int32_t* __restrict__ targets, const float4* __restrict__ phi,
     const float4* __restrict__ plo, const float4* __restrict__ vf, float G, float eps2, PnK<float> pk,
     double Gd, int64_t slice_len, int nslices, double4* __restrict__ partial, double4* __restrict__ acc,
     double* __restrict__ out3, KickArgs kick) {
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
     __shared__ float4 sl[BLOCK];
     __shared__ float4 sv[BLOCK];  // (vx, vy, vz, |v|^2)
     const int slice = blockIdx.y;
-    const int64_t j0 = (int64_t)slice * slice_len;
+    const int64_t j0 = j_lo + (int64_t)slice * slice_len;  // sources [j_lo, n), sliced
     const int64_t j1 = min(n, j0 + slice_len);
     int64_t tt[IPT], bi[IPT];
     float xh[IPT], yh[IPT], zh[IPT], xl[IPT], yl[IPT], zl[IPT], mi[IPT];
@@ -239,12 +239,12 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
 // rsqrt, FP32 partials folded into compensated sums every FOLD j).
 template <bool GUARD>
 __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed2(
-    int64_t n, int64_t nt, const int32_t* __restrict__ targets, const float4* __restrict__ phi,
+    int64_t j_lo, int64_t n, int64_t nt, const int32_t* __restrict__ targets, const float4* __restrict__ phi,
     const float4* __restrict__ plo, float eps2, double Gd, int64_t slice_len, int nslices,
     double4* __restrict__ partial, double4* __restrict__ acc, double* __restrict__ out3, KickArgs kick) {
     __shared__ float4 pa[BLOCK / 2], pb[BLOCK / 2], pc[BLOCK / 2], pd[BLOCK / 2];
     const int slice = blockIdx.y;
-    const int64_t j0 = (int64_t)slice * slice_len;
+    const int64_t j0 = j_lo + (int64_t)slice * slice_len;  // sources [j_lo, n), sliced
     const int64_t j1 = min(n, j0 + slice_len);
     int64_t tt[IPT], bi[IPT];
     float2 nhx[IPT], nhy[IPT], nhz[IPT], nlx[IPT], nly[IPT], nlz[IPT];
@@ -338,37 +338,38 @@ __global__ void k_reduce_slices(int64_t nt, int nslices, const double4* __restri
 }
 
 template <int PNL, bool GUARD>
-void launch_fp64(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32_t* tg, aster_ctx* c,
+void launch_fp64(dim3 grid, cudaStream_t st, int64_t j_lo, int64_t n, int64_t nt, const int32_t* tg, aster_ctx* c,
                  const aster_params* p, int64_t slice_len, int ns, double4* partial, double* out3, KickArgs kick) {
-    k_allpairs_fp64<PNL, GUARD><<<grid, BLOCK, 0, st>>>(n, nt, tg, c->pm.as<double4>(), c->vel.as<double4>(), p->G,
+    k_allpairs_fp64<PNL, GUARD><<<grid, BLOCK, 0, st>>>(j_lo, n, nt, tg, c->pm.as<double4>(), c->vel.as<double4>(), p->G,
                                                          p->eps2, make_pn(p), slice_len, ns, partial,
                                                          c->acc.as<double4>(), out3, kick);
 }
 
 template <int PNL, bool GUARD>
-void launch_mixed(dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32_t* tg, aster_ctx* c,
+void launch_mixed(dim3 grid, cudaStream_t st, int64_t j_lo, int64_t n, int64_t nt, const int32_t* tg, aster_ctx* c,
                   const aster_params* p, int64_t slice_len, int ns, double4* partial, double* out3, KickArgs kick) {
     if constexpr (PNL == 0) {
-        k_allpairs_mixed2<GUARD><<<grid, BLOCK, 0, st>>>(n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(),
+        k_allpairs_mixed2<GUARD><<<grid, BLOCK, 0, st>>>(j_lo, n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(),
                                                           (float)p->eps2, p->G, slice_len, ns, partial,
                                                           c->acc.as<double4>(), out3, kick);
     } else {
         k_allpairs_mixed<PNL, GUARD><<<grid, BLOCK, 0, st>>>(
-            n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), (float)p->G, (float)p->eps2,
+            j_lo, n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), (float)p->G, (float)p->eps2,
             pn_float(make_pn(p)), p->G, slice_len, ns, partial, c->acc.as<double4>(), out3, kick);
     }
 }
 
 template <int PNL>
-void launch_pnl(int precision, bool guard, dim3 grid, cudaStream_t st, int64_t n, int64_t nt, const int32_t* tg,
+void launch_pnl(int precision, bool guard, dim3 grid, cudaStream_t st, int64_t j_lo, int64_t n, int64_t nt,
+                const int32_t* tg,
                 aster_ctx* c, const aster_params* p, int64_t slice_len, int ns, double4* partial, double* out3,
                 KickArgs kick) {
     if (precision == ASTER_FP64) {
-        if (guard) launch_fp64<PNL, true>(grid, st, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
-        else       launch_fp64<PNL, false>(grid, st, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
+        if (guard) launch_fp64<PNL, true>(grid, st, j_lo, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
+        else       launch_fp64<PNL, false>(grid, st, j_lo, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
     } else {
-        if (guard) launch_mixed<PNL, true>(grid, st, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
-        else       launch_mixed<PNL, false>(grid, st, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
+        if (guard) launch_mixed<PNL, true>(grid, st, j_lo, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
+        else       launch_mixed<PNL, false>(grid, st, j_lo, n, nt, tg, c, p, slice_len, ns, partial, out3, kick);
     }
 }
 
@@ -377,22 +378,30 @@ void launch_pnl(int precision, bool guard, dim3 grid, cudaStream_t st, int64_t n
 // Launch one all-pairs evaluation. Targets: every body (targets_dev == null,
 // nt == n) or an explicit list. Output: ctx->acc (out_dev == null) with an
 // optional closing kick, or out_dev[nt*3].
-int aster_allpairs_launch(aster_ctx* c, const aster_params* p, int precision, bool closing_kick, int64_t nt,
-                          const int32_t* targets_dev, double* out_dev) {
-    // sources: bodies [0, n_src) (the trailing massless bodies contribute zero
-    // in the Newtonian and 1PN laws alike); targets: nt bodies or the list
-    const int64_t n = c->n_src > 0 ? c->n_src : c->n;
+// Launch one all-pairs evaluation over the sources [src_lo, src_hi) (bodies
+// beyond the last massive one are dropped: they attract nothing under any of
+// the force laws). Targets: every body (targets_dev == null, nt == n) or an
+// explicit list. Output: ctx->acc (out_dev == null) with an optional closing
+// kick, or out_dev[nt*3].
+int aster_allpairs_launch_range(aster_ctx* c, const aster_params* p, int precision, bool closing_kick, int64_t nt,
+                                const int32_t* targets_dev, double* out_dev, int64_t src_lo, int64_t src_hi) {
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    const int64_t n_src = c->n_src > 0 ? c->n_src : c->n;
+    const int64_t lo = src_lo, hi = src_hi < n_src ? src_hi : n_src;
+    const int64_t len = hi > lo ? hi - lo : 0;
     const int64_t per_block = (int64_t)BLOCK * IPT;
     const int64_t iblocks = (nt + per_block - 1) / per_block;
     // j-slices so that small n still fill the GPU (>= 2 blocks per SM).
     int64_t want = 2 * (int64_t)c->sm_count;
     int64_t ns = iblocks >= want ? 1 : (want + iblocks - 1) / iblocks;
-    int64_t max_ns = (n + BLOCK - 1) / BLOCK;
+    int64_t max_ns = (len + BLOCK - 1) / BLOCK;
     if (ns > max_ns) ns = max_ns;
     if (ns > 64) ns = 64;
     if (ns < 1) ns = 1;
-    int64_t slice_len = ((n + ns - 1) / ns + BLOCK - 1) / BLOCK * BLOCK;
-    ns = (n + slice_len - 1) / slice_len;
+    int64_t slice_len = ((len + ns - 1) / ns + BLOCK - 1) / BLOCK * BLOCK;
+    if (slice_len < BLOCK) slice_len = BLOCK;
+    ns = (len + slice_len - 1) / slice_len;
+    if (ns < 1) ns = 1;  // no sources: one slice that writes zeros
     double4* partial = nullptr;
     if (ns > 1) {
         ASTER_TRY(c->scratch.ensure((size_t)ns * nt * sizeof(double4)));
@@ -401,11 +410,11 @@ int aster_allpairs_launch(aster_ctx* c, const aster_params* p, int precision, bo
     KickArgs kick{closing_kick && !out_dev, 0.5 * p->dt, c->vel.as<double4>()};
     dim3 grid((unsigned)iblocks, (unsigned)ns);
     const bool guard = !(p->eps2 > 0.0);
-    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
     const int pnl = pn_level(p);
-    if (pnl == 2) launch_pnl<2>(precision, guard, grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
-    else if (pnl == 1) launch_pnl<1>(precision, guard, grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
-    else launch_pnl<0>(precision, guard, grid, c->stream, n, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
+    const int64_t j_hi = lo + len;
+    if (pnl == 2) launch_pnl<2>(precision, guard, grid, c->stream, lo, j_hi, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
+    else if (pnl == 1) launch_pnl<1>(precision, guard, grid, c->stream, lo, j_hi, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
+    else launch_pnl<0>(precision, guard, grid, c->stream, lo, j_hi, nt, targets_dev, c, p, slice_len, (int)ns, partial, out_dev, kick);
     ASTER_CUDA(cudaGetLastError());
     c->stats.kernels += 1;
     if (ns > 1) {
@@ -415,8 +424,14 @@ int aster_allpairs_launch(aster_ctx* c, const aster_params* p, int precision, bo
         ASTER_CUDA(cudaGetLastError());
         c->stats.kernels += 1;
     }
-    c->stats.interactions += (double)nt * (double)n;
+    c->stats.interactions += (double)nt * (double)len;
     return ASTER_OK;
+}
+
+// Every source body [0, n).
+int aster_allpairs_launch(aster_ctx* c, const aster_params* p, int precision, bool closing_kick, int64_t nt,
+                          const int32_t* targets_dev, double* out_dev) {
+    return aster_allpairs_launch_range(c, p, precision, closing_kick, nt, targets_dev, out_dev, 0, c->n);
 }
 
 extern "C" int aster_allpairs(aster_ctx* c, const aster_params* p, int precision, double* acc_out) {
@@ -434,6 +449,31 @@ extern "C" int aster_allpairs(aster_ctx* c, const aster_params* p, int precision
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
     c->stats.ms_total = c->stats.ms_force = ms;
     c->acc_valid = true;
+    return aster_copy_acc_out(c, acc_out);
+}
+
+// Accelerations of every body from the sources [src_lo, src_hi) only
+// (src_hi < 0: up to n), as Parallelized::compute_forces sums over the
+// solver's set_bounds range. The cached acceleration is not the full one
+// afterwards, so the next KDK step evaluates it afresh.
+extern "C" int aster_allpairs_range(aster_ctx* c, const aster_params* p, int precision, int64_t src_lo,
+                                    int64_t src_hi, double* acc_out) {
+    if (!c) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_check_params(p));
+    if (c->n <= 0) return ASTER_ERR_NO_STATE;
+    if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    if (src_hi < 0) src_hi = c->n;
+    if (src_lo < 0 || src_lo > src_hi || src_hi > c->n) return ASTER_ERR_INVALID_ARG;
+    ASTER_TRY(aster_begin(c));
+    c->stats = aster_stats{};
+    cudaEventRecord(c->ev[0], c->stream);
+    ASTER_TRY(aster_allpairs_launch_range(c, p, precision, false, c->n, nullptr, nullptr, src_lo, src_hi));
+    cudaEventRecord(c->ev[1], c->stream);
+    ASTER_TRY(aster_finish(c));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = c->stats.ms_force = ms;
+    c->acc_valid = false;
     return aster_copy_acc_out(c, acc_out);
 }
 

@@ -122,6 +122,8 @@ int aster_copy_acc_out(aster_ctx* ctx, double* acc_out);
 int aster_allpairs_launch(aster_ctx* ctx, const aster_params* p, int precision,
                           bool closing_kick, int64_t nt, const int32_t* targets_dev,
                           double* out_dev /* nt*3 or null: write ctx->acc */);
+int aster_allpairs_launch_range(aster_ctx* ctx, const aster_params* p, int precision, bool closing_kick, int64_t nt,
+                                const int32_t* targets_dev, double* out_dev, int64_t src_lo, int64_t src_hi);
 // integrate.cu
 int aster_kick_drift_launch(aster_ctx* ctx, const aster_params* p, bool want_box, bool want_mixed);
 // Enqueue-only cores of the stepping entry points (argument checks included,

@@ -52,14 +52,18 @@ void CudaAllPairs::upload() {
 void CudaAllPairs::compute_forces() {
     auto& b = _s->bodies;
     if (b.positions.empty()) return;
-    if (get_lower_bound() != 0 || get_upper_bound() != (int)b.positions.size()) {
-        critical_if(true, "CudaAllPairs: set_bounds ranges are not supported; use aster_allpairs_targets");
+    // set_bounds restricts the sources, as in Parallelized::compute_forces
+    // (builder_endpoint.cpp:729-757): every body gets the pull of [lower, upper)
+    const int lo = get_lower_bound(), hi = get_upper_bound();
+    if (warn_if(hi - lo <= 0, "either upper or lower bound were set too high in the gravity solver, resulting in a negative amount of bodies to load"))
         return;
-    }
     upload();
     b.accs.resize(b.positions.size());
     const aster_params p = params();
-    check(aster_allpairs(ctx_, &p, precision_, &b.accs[0].x), "aster_allpairs");
+    if (lo != 0 || hi != (int)b.positions.size())
+        check(aster_allpairs_range(ctx_, &p, precision_, lo, hi, &b.accs[0].x), "aster_allpairs_range");
+    else
+        check(aster_allpairs(ctx_, &p, precision_, &b.accs[0].x), "aster_allpairs");
 }
 
 CudaLBVH::CudaLBVH(Simulation* s, int precision, int device) : CudaAllPairs(s, precision, device) {
@@ -69,6 +73,13 @@ CudaLBVH::CudaLBVH(Simulation* s, int precision, int device) : CudaAllPairs(s, p
 void CudaLBVH::compute_forces() {
     auto& b = _s->bodies;
     if (b.positions.empty()) return;
+    // Barnes_Hut::compute_forces with bounds builds its tree from misnumbered
+    // bodies (make_tree stores i - lower as the body index and keeps the root
+    // at N): there is no consistent meaning to reproduce, so ranges are refused
+    if (get_lower_bound() != 0 || get_upper_bound() != (int)b.positions.size()) {
+        critical_if(true, "CudaLBVH: set_bounds ranges are not supported; use CudaAllPairs for a source range");
+        return;
+    }
     upload();
     b.accs.resize(b.positions.size());
     const aster_params p = params();

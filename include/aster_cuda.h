@@ -137,6 +137,14 @@ int aster_state_size(aster_ctx* ctx, int64_t* n);
  * Parallelized / SimpleGPU replacement. Accelerations are cached on the device
  * and copied to acc_out (host, n*3) when it is not NULL. */
 int aster_allpairs(aster_ctx* ctx, const aster_params* p, int precision, double* acc_out);
+/* Accelerations of every body from the sources [src_lo, src_hi) only
+ * (src_hi < 0: up to n): Parallelized::compute_forces over a Solver::set_bounds
+ * range (builder_endpoint.cpp:64-69, 729-757), e.g. set_bounds(1, -1) in
+ * update_WH_planetary (updater.cpp:100). acc_out: host, n*3, or NULL. The
+ * cached acceleration is not the full one afterwards (the next KDK step
+ * evaluates it afresh). */
+int aster_allpairs_range(aster_ctx* ctx, const aster_params* p, int precision, int64_t src_lo, int64_t src_hi,
+                         double* acc_out);
 
 /* All-pairs accelerations for an explicit target list against every body:
  * targets[nt] body indices, acc_out[nt*3] host. FP64 or mixed. Used for the

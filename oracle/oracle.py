@@ -55,6 +55,7 @@ class Ref:
             lib.ref_setup.argtypes = [ctypes.c_int, _D, _D, _D] + [ctypes.c_double] * 6 + [ctypes.c_int, ctypes.c_int]
             lib.ref_get_state.argtypes = [_D, _D, _D]
             lib.ref_compute_forces.argtypes = [_D]
+            lib.ref_set_bounds.argtypes = [ctypes.c_int, ctypes.c_int]
             lib.ref_leapfrog.argtypes = [ctypes.c_int, _D]
             lib.ref_energy.restype = ctypes.c_double
             lib.ref_bh_tree.argtypes = [_U32, _I32, _I32, _D, _D]
@@ -131,6 +132,12 @@ class Ref:
         out = np.zeros(22)
         ln = self.lib.ref_saba_coeffs(order, _p(out, _D))
         return out[:ln].copy()
+
+    def set_bounds(self, lower, upper=-1):
+        """Solver::set_bounds on the current solver (reset by every setup)."""
+        if self.lib.ref_set_bounds(lower, upper) != 0:
+            raise RuntimeError("ref_set_bounds failed")
+        return self
 
     def pair_force(self, m1, m2, v1, v2, p1, p2):
         f = np.zeros(3)

@@ -89,6 +89,15 @@ int ref_setup(int n, const double* pos, const double* vel, const double* mass,
         g_solver_kind = solver_kind;
     }
     s->solver->force_law = Aster::PN_expansion_type((short)force_law);
+    s->solver->set_bounds(0, -1);  // the solver outlives setups: every setup starts with the whole range
+    return 0;
+}
+
+// Solver::set_bounds (builder_endpoint.cpp:64-67) on the current solver.
+int ref_set_bounds(int lower, int upper) {
+    HarnessSim* s = sim();
+    if (!s->solver) return -1;
+    s->solver->set_bounds(lower, upper);
     return 0;
 }
 

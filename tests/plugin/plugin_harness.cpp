@@ -21,6 +21,43 @@ struct PluginSim : public Aster::Simulation {
 };
 }  // namespace
 
+// One compute_forces() of CudaAllPairs (solver_kind 0) or CudaLBVH (1) after
+// Solver::set_bounds(lower, upper); accelerations out, 1e300 for every body
+// whose acceleration the solver did not write (errors go to critical_if).
+extern "C" int plg_forces_bounds(int n, const double* pos, const double* vel, const double* m, double G, double c,
+                                 double eps2, int force_law, int solver_kind, int precision, int lower, int upper,
+                                 double* acc_out) {
+    if (n <= 0) return -1;
+    auto* s = new PluginSim();
+    s->bodies.positions.resize(n);
+    s->bodies.velocities.resize(n);
+    s->bodies.accs.assign(n, Aster::vec3(0.0));
+    s->bodies.masses.assign(m, m + n);
+    s->bodies.temps.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        s->bodies.positions[i] = Aster::vec3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        s->bodies.velocities[i] = Aster::vec3(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+    }
+    s->set_consts(G, c, 1e-3);
+    s->softening = eps2;
+    s->force_law = Aster::PN_expansion_type((short)force_law);
+    Aster::CudaAllPairs* solver = solver_kind == 1 ? new Aster::CudaLBVH(s, precision) : new Aster::CudaAllPairs(s, precision);
+    solver->force_law = Aster::PN_expansion_type((short)force_law);
+    s->solver = solver;
+    solver->load();
+    solver->set_bounds(lower, upper);
+    for (int i = 0; i < n; ++i) s->bodies.accs[i] = Aster::vec3(1e300, 1e300, 1e300);  // marks untouched bodies
+    solver->compute_forces();
+    for (int i = 0; i < n; ++i) {
+        const auto& a = s->bodies.accs[i];
+        acc_out[3 * i] = a.x; acc_out[3 * i + 1] = a.y; acc_out[3 * i + 2] = a.z;
+    }
+    s->solver = nullptr;
+    delete solver;
+    delete s;
+    return 0;
+}
+
 extern "C" int plg_run(int n, const double* pos, const double* vel, const double* m, double G, double c, double dt,
                        double eps2, double theta, int force_law, int solver_kind, int precision, int use_cuda_kdk,
                        int nsteps, double* pos_out, double* vel_out, double* acc_out) {

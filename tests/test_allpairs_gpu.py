@@ -68,6 +68,27 @@ def test_pn_laws_match_reference_golden(ctx, name, prec):
     assert np.linalg.norm((a - newton) - part) < bound
 
 
+@pytest.mark.parametrize("law", [NEWTON, NEWTON | PN1 | PN2 | PN25])
+def test_source_range_matches_reference_set_bounds(ctx, law):
+    """aster_allpairs_range against Parallelized::compute_forces after
+    Solver::set_bounds(lower, upper): every body gets the pull of the sources
+    [lower, upper) only (FP64 1e-12, mixed 1e-6); an empty range gives zeros."""
+    from oracle.oracle import Ref
+    if not Ref.available():
+        pytest.skip("reference build absent")
+    pos, vel, m = gen.plummer(1500, 71)
+    vel = vel * 30.0
+    p = Params(eps2=1e-4, c=100.0, force_law=law)
+    ctx.upload(pos, vel, m)
+    for lo, hi in ((1, -1), (100, 900), (0, 1500), (1499, 1500)):
+        ref = Ref().setup(pos, vel, m, G=1.0, c=100.0, eps2=1e-4, force_law=law).set_bounds(lo, hi).forces()
+        assert rel_l2(ctx.allpairs_range(p, lo, hi, FP64), ref) < 1e-12, (lo, hi)
+        assert rel_l2(ctx.allpairs_range(p, lo, hi, MIXED), ref) < 1e-6, (lo, hi)
+    assert np.all(ctx.allpairs_range(p, 700, 700, FP64) == 0.0)
+    full = ctx.allpairs(p, FP64)
+    assert rel_l2(ctx.allpairs_range(p, 0, -1, FP64), full) == 0.0
+
+
 def test_pn_laws_in_si_units(ctx, orc):
     """A star of 2e30 kg with 500 planets and planetesimals at 0.05-5 AU on
     near-circular orbits, SI units, physical c, every PN term: FP64 equals the

@@ -28,6 +28,7 @@ def _lib():
         pytest.skip("plugin harness not built (needs the reference headers at build time)")
     lib = ctypes.CDLL(str(LIB))
     lib.plg_run.argtypes = [ctypes.c_int, _D, _D, _D] + [ctypes.c_double] * 5 + [ctypes.c_int] * 5 + [_D, _D, _D]
+    lib.plg_forces_bounds.argtypes = [ctypes.c_int, _D, _D, _D] + [ctypes.c_double] * 3 + [ctypes.c_int] * 5 + [_D]
     return lib
 
 
@@ -87,6 +88,36 @@ def test_pn_lbvh_plugin_matches_reference_bh_at_theta0():
     _, _, ao = plugin_run(pos, vel, m, c=100.0, theta=0.0, force_law=law, solver=1, precision=FP64, nsteps=0)
     ref = Ref().setup(pos, vel, m, G=1.0, c=100.0, eps2=1e-4, theta=0.0, force_law=law, solver="bh")
     assert rel_l2(ao, ref.forces()) < 1e-12
+
+
+def plugin_forces_bounds(pos, vel, m, lower, upper, *, c=100.0, eps2=1e-4, force_law=NEWTON, solver=0,
+                         precision=FP64):
+    lib = _lib()
+    pos, vel, m = (np.ascontiguousarray(a, dtype=np.float64) for a in (pos, vel, m))
+    ao = np.empty((len(m), 3))
+    p = lambda a: a.ctypes.data_as(_D)  # noqa: E731
+    assert lib.plg_forces_bounds(len(m), p(pos), p(vel), p(m), 1.0, c, eps2, force_law, solver, precision, lower,
+                                 upper, p(ao)) == 0
+    return ao
+
+
+@pytest.mark.parametrize("law", [NEWTON, NEWTON | PN1 | PN2 | PN25])
+def test_set_bounds_through_the_plugin_matches_parallelized(law):
+    """Solver::set_bounds on CudaAllPairs restricts the sources like
+    Parallelized (the reference's OpenCL Wisdom-Holman updater sets (1, -1));
+    CudaLBVH refuses a range (the reference tree misnumbers its bodies there)
+    and leaves the accelerations untouched."""
+    from oracle.oracle import Ref
+    if not Ref.available():
+        pytest.skip("reference build absent")
+    pos, vel, m = gen.plummer(900, 67)
+    vel = vel * 30.0
+    for lo, hi in ((1, -1), (50, 600)):
+        ao = plugin_forces_bounds(pos, vel, m, lo, hi, force_law=law)
+        ref = Ref().setup(pos, vel, m, G=1.0, c=100.0, eps2=1e-4, force_law=law).set_bounds(lo, hi).forces()
+        assert rel_l2(ao, ref) < 1e-12
+    untouched = plugin_forces_bounds(pos, vel, m, 1, -1, force_law=law, solver=1)
+    assert np.all(untouched == 1e300)
 
 
 def test_lbvh_plugin_equals_c_abi(ctx):
