@@ -138,8 +138,9 @@ int aster_upload_enqueue(aster_ctx* ctx, int64_t n, const double* pos, const dou
                          const double* acc);
 // state array `which` (0 positions, 1 velocities, 2 accelerations) -> host on `stream`
 int aster_download_enqueue(aster_ctx* ctx, int which, double* host, cudaStream_t stream);
-// energy and momentum into out4 (device); part: (n + 255) / 256 * 5 doubles
+// energy and momentum into out4 (device); part: aster_energy_parts(ctx) * 5 doubles
 int aster_energy_enqueue(aster_ctx* ctx, const aster_params* p, int ref_form, double* part, double* out4);
+int64_t aster_energy_parts(const aster_ctx* ctx);
 // v += a * kick_dt (skipped when !kick), x += v * drift_dt, refresh derived copies
 int aster_kick_drift_coef(aster_ctx* ctx, double kick_dt, double drift_dt, bool kick, bool want_box,
                           bool want_mixed);

@@ -75,20 +75,24 @@ __global__ void __launch_bounds__(256) k_kick_drift(int64_t n, double half_dt, d
 // FP64 energy/momentum: per-block partials (ke, pe, px, py, pz), then one
 // block adds them in a fixed order (deterministic).
 template <bool REF_FORM>
+// Block (x, slice y): bodies i of block x against the sources of slice y,
+// [y * slice_len, (y + 1) * slice_len); the kinetic energy and momentum of i
+// come with slice 0. Partials in part[(y * gridDim.x + x) * 5 + k].
 __global__ void __launch_bounds__(256) k_energy_partial(int64_t n, const double4* __restrict__ pm,
                                                         const double4* __restrict__ vel, double eps2,
-                                                        double* __restrict__ part) {
+                                                        int64_t slice_len, double* __restrict__ part) {
     __shared__ double4 sp[256];
     __shared__ double red[5][8];
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t j0 = (int64_t)blockIdx.y * slice_len, j1 = min(n, j0 + slice_len);
     double4 pi = i < n ? pm[i] : make_double4(0, 0, 0, 0);
     double pot = 0.0;
-    for (int64_t base = 0; base < n; base += 256) {
+    for (int64_t base = j0; base < j1; base += 256) {
         __syncthreads();
         const int64_t j = base + threadIdx.x;
-        sp[threadIdx.x] = j < n ? pm[j] : make_double4(0, 0, 0, 0);
+        sp[threadIdx.x] = j < j1 ? pm[j] : make_double4(0, 0, 0, 0);
         __syncthreads();
-        const int lim = (int)min((int64_t)256, n - base);
+        const int lim = (int)min((int64_t)256, j1 - base);
         for (int q = 0; q < lim; ++q) {
             if (base + q == i) continue;
             const double4 pj = sp[q];
@@ -100,10 +104,12 @@ __global__ void __launch_bounds__(256) k_energy_partial(int64_t n, const double4
     }
     double v[5] = {0, 0, 0, 0, 0};
     if (i < n) {
-        const double4 vi = vel[i];
-        v[0] = 0.5 * pi.w * (vi.x * vi.x + vi.y * vi.y + vi.z * vi.z);
         v[1] = -0.5 * pi.w * pot;
-        v[2] = pi.w * vi.x; v[3] = pi.w * vi.y; v[4] = pi.w * vi.z;
+        if (blockIdx.y == 0) {
+            const double4 vi = vel[i];
+            v[0] = 0.5 * pi.w * (vi.x * vi.x + vi.y * vi.y + vi.z * vi.z);
+            v[2] = pi.w * vi.x; v[3] = pi.w * vi.y; v[4] = pi.w * vi.z;
+        }
     }
     for (int k = 0; k < 5; ++k) {
         double x = v[k];
@@ -114,17 +120,22 @@ __global__ void __launch_bounds__(256) k_energy_partial(int64_t n, const double4
     if (threadIdx.x < 5) {
         double s = 0;
         for (int w = 0; w < 8; ++w) s += red[threadIdx.x][w];
-        part[blockIdx.x * 5 + threadIdx.x] = s;
+        part[((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * 5 + threadIdx.x] = s;
     }
 }
 
-__global__ void k_energy_final(int nblocks, const double* __restrict__ part, double G, double* __restrict__ out) {
-    // out[0] = energy, out[1..3] = momentum; 5 threads, fixed order
+// out[0] = energy, out[1..3] = momentum from nparts partials: lane l of warp k
+// adds component k of partials l, l + 32, ... in order, then a fixed shuffle
+// tree (deterministic). 160 threads.
+__global__ void __launch_bounds__(160) k_energy_final(int nparts, const double* __restrict__ part, double G,
+                                                      double* __restrict__ out) {
     __shared__ double s[5];
-    if (threadIdx.x < 5) {
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (k < 5) {
         double a = 0;
-        for (int b = 0; b < nblocks; ++b) a += part[b * 5 + threadIdx.x];
-        s[threadIdx.x] = a;
+        for (int b = lane; b < nparts; b += 32) a += part[(int64_t)b * 5 + k];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) s[k] = a;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -449,15 +460,34 @@ extern "C" int aster_saba_steps(aster_ctx* c, const aster_params* p, int solver,
 
 // FP64 energy and momentum of the resident state into out4 (device:
 // energy, px, py, pz); part holds (n + 255) / 256 * 5 doubles. No sync.
+// Source slices of the energy sum: enough blocks to fill the GPU when n is
+// small (each slice a whole number of 256-body tiles).
+static int energy_slices(const aster_ctx* c, int64_t n) {
+    const int64_t tiles = (n + 255) / 256;
+    int64_t ns = ((int64_t)4 * c->sm_count + tiles - 1) / tiles;
+    if (ns > tiles) ns = tiles;
+    if (ns > 64) ns = 64;
+    if (ns < 1) ns = 1;
+    return (int)ns;
+}
+
+// Partials (5 doubles each) that aster_energy_enqueue writes.
+int64_t aster_energy_parts(const aster_ctx* c) { return (c->n + 255) / 256 * energy_slices(c, c->n); }
+
 int aster_energy_enqueue(aster_ctx* c, const aster_params* p, int ref_form, double* part, double* out4) {
     const int64_t n = c->n;
     const int nb = (int)((n + 255) / 256);
+    const int ns = energy_slices(c, n);
+    const int64_t slice_len = (nb + ns - 1) / ns * (int64_t)256;
+    const dim3 grid((unsigned)nb, (unsigned)ns);
     if (ref_form)
-        k_energy_partial<true><<<nb, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2, part);
+        k_energy_partial<true><<<grid, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2,
+                                                            slice_len, part);
     else
-        k_energy_partial<false><<<nb, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2, part);
+        k_energy_partial<false><<<grid, 256, 0, c->stream>>>(n, c->pm.as<double4>(), c->vel.as<double4>(), p->eps2,
+                                                             slice_len, part);
     ASTER_CUDA(cudaGetLastError());
-    k_energy_final<<<1, 32, 0, c->stream>>>(nb, part, p->G, out4);
+    k_energy_final<<<1, 160, 0, c->stream>>>(nb * ns, part, p->G, out4);
     ASTER_CUDA(cudaGetLastError());
     return ASTER_OK;
 }
@@ -467,9 +497,7 @@ extern "C" int aster_energy(aster_ctx* c, const aster_params* p, int ref_form, d
     ASTER_TRY(aster_check_params(p));
     if (c->n <= 0) return ASTER_ERR_NO_STATE;
     ASTER_TRY(aster_begin(c));
-    const int64_t n = c->n;
-    const int nb = (int)((n + 255) / 256);
-    ASTER_TRY(c->scratch.ensure((size_t)nb * 5 * sizeof(double) + 64));
+    ASTER_TRY(c->scratch.ensure((size_t)aster_energy_parts(c) * 5 * sizeof(double) + 64));
     ASTER_TRY(c->red.ensure(4096));
     double* part = c->scratch.as<double>();
     double* out = red_energy(c);
@@ -526,12 +554,13 @@ extern "C" int aster_energy_noalloc(int64_t n, const double* pm_dev, const doubl
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const double4* pm = reinterpret_cast<const double4*>(pm_dev);
     const double4* vel = reinterpret_cast<const double4*>(vel_dev);
+    const int64_t whole = (int64_t)nb * 256;  // one slice: every source
     if (ref_form)
-        k_energy_partial<true><<<nb, 256, 0, st>>>(n, pm, vel, p->eps2, part);
+        k_energy_partial<true><<<nb, 256, 0, st>>>(n, pm, vel, p->eps2, whole, part);
     else
-        k_energy_partial<false><<<nb, 256, 0, st>>>(n, pm, vel, p->eps2, part);
+        k_energy_partial<false><<<nb, 256, 0, st>>>(n, pm, vel, p->eps2, whole, part);
     ASTER_CUDA(cudaGetLastError());
-    k_energy_final<<<1, 32, 0, st>>>(nb, part, p->G, out_dev);
+    k_energy_final<<<1, 160, 0, st>>>(nb, part, p->G, out_dev);
     ASTER_CUDA(cudaGetLastError());
     return ASTER_OK;
 }

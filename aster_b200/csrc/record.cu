@@ -123,7 +123,7 @@ extern "C" int aster_record(aster_ctx* c, const aster_params* p, const aster_rec
     const int64_t nsamp = nsteps / cfg->rate + 1;
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
-    const int64_t nbe = (n + 255) / 256;                                                    // energy partials
+    const int64_t nbe = aster_energy_parts(c);                                              // energy partials
     const int64_t nbc = std::min<int64_t>((n + REC_BLOCK - 1) / REC_BLOCK, (int64_t)c->sm_count * 4);  // com
     const size_t table = (size_t)(nsamp * ncol);
     ASTER_TRY(c->rec.ensure((table + (size_t)nbe * 5 + (size_t)nbc * 4 + 16) * sizeof(double)));

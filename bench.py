@@ -425,6 +425,77 @@ def secondary(ctx, args):
     out["ensemble"] = ensemble_c4(ctx)
     out["adjoint"] = adjoint_c5(ctx)
     out["c1"] = kdk_c1(ctx)
+    out["next_rows"] = next_rows(ctx)
+    return out
+
+
+def next_rows(ctx):
+    """The rows beyond the headline path, each on its parity-test setup at a
+    measurable size (device time, CUDA events): SABA4 (C1 all-pairs, and C2
+    LBVH), Wisdom-Holman (8 planets + 262,144 test particles), device-resident
+    stepping with collectors against plain stepping (C1), the C4 ensemble with
+    every post-Newtonian term, and the post-Newtonian LBVH walk (C2)."""
+    from aster_b200 import gen
+    from aster_b200.api import (COLLECT_CENTER, COLLECT_ENERGY, COLLECT_MOMENTUM, FP64, MIXED, NEWTON,
+                                PN1, PN2, PN25, SOLVER_ALLPAIRS, SOLVER_LBVH, UPDATER_KDK, YOSHIDA4, Params)
+    out = {}
+    # SABA4: 4 force evaluations a step
+    pos, vel, m = gen.plummer(4096, 1001)
+    p = Params(eps2=1e-4, dt=1e-3)
+    saba = {"workload": "SABA4, C1 Plummer N=4096 all-pairs, 100 steps; C2 N=1048576 LBVH mixed, 2 steps"}
+    for name, prec in (("c1_fp64", FP64), ("c1_mixed", MIXED)):
+        ctx.upload(pos, vel, m)
+        e0, _ = ctx.energy(p)
+        ctx.saba_steps(p, 4, 100, SOLVER_ALLPAIRS, prec)
+        ms = ctx.stats()["ms_total"]
+        e1, _ = ctx.energy(p)
+        saba[name] = {"ms_per_step": ms / 100, "energy_drift": abs(e1 - e0) / abs(e0)}
+    pos2, vel2, m2 = gen.plummer(N_C2, SEED_C2, masses="lognormal")
+    p2 = Params(G=1.0, eps2=EPS * EPS, theta=THETA, dt=DT)
+    ctx.upload(pos2, vel2, m2)
+    ctx.saba_steps(p2, 4, 1, SOLVER_LBVH, MIXED)
+    ctx.saba_steps(p2, 4, 2, SOLVER_LBVH, MIXED)
+    saba["c2_lbvh_mixed"] = {"ms_per_step": ctx.stats()["ms_total"] / 2}
+    out["saba4"] = saba
+    # post-Newtonian LBVH walk at C2 (KDK, mixed, 1PN and every term; c = 100)
+    pnl = {"workload": "C2 LBVH KDK mixed with post-Newtonian laws, c=100, 3 steps (Newtonian step for scale)"}
+    for name, law in (("newton", NEWTON), ("pn1", NEWTON | PN1), ("all_terms", NEWTON | PN1 | PN2 | PN25)):
+        q = Params(G=1.0, eps2=EPS * EPS, theta=THETA, dt=DT, c=100.0, force_law=law)
+        ctx.upload(pos2, vel2, m2)
+        ctx.kdk_steps(q, 1, SOLVER_LBVH, MIXED)
+        ctx.kdk_steps(q, 3, SOLVER_LBVH, MIXED)
+        pnl[name] = {"ms_per_step": ctx.stats()["ms_total"] / 3}
+    out["pn_lbvh"] = pnl
+    # Wisdom-Holman
+    pw, vw, mw = gen.planetary_system(8, 262144, 1023)
+    ctx.upload(pw, vw, mw)
+    pwh = Params(G=1.0, dt=0.02)
+    ctx.wh_steps(pwh, 2)
+    ctx.wh_steps(pwh, 200)
+    ms = ctx.stats()["ms_total"]
+    out["wisdom_holman"] = {"workload": "star + 8 planets + 262144 test particles, FP64, dt=0.02, 200 steps",
+                            "ms_per_step": ms / 200, "body_steps_per_s": len(mw) * 200 / (ms / 1e3)}
+    # device-resident stepping with collectors vs plain stepping (C1)
+    rec = {"workload": "C1 Plummer N=4096 KDK all-pairs FP64, 100 steps; energy+momentum+centre every 10 steps"}
+    ctx.upload(pos, vel, m)
+    ctx.kdk_steps(p, 100, SOLVER_ALLPAIRS, FP64)
+    rec["plain_ms"] = ctx.stats()["ms_total"]
+    ctx.upload(pos, vel, m)
+    ctx.record(p, 100, updater=UPDATER_KDK, solver=SOLVER_ALLPAIRS, precision=FP64, rate=10,
+               collect=COLLECT_ENERGY | COLLECT_MOMENTUM | COLLECT_CENTER)
+    rec["recorded_ms"] = ctx.stats()["ms_total"]
+    out["record"] = rec
+    # C4 ensemble with every post-Newtonian term
+    pe, ve, me, off = gen.hierarchical_ensemble(16384, 1004)
+    ens = {"workload": "C4 16384 systems n~U[3,64], Newton+1PN+2PN+2.5PN c=100, Yoshida-4, dt=1e-4, 1000 steps"}
+    q = Params(G=1.0, c=100.0, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1 | PN2 | PN25)
+    cfg = {"warps_per_block": 8, "unroll": 2, "use_graph": 1}
+    ctx.ensemble_upload(off, pe, ve, me)
+    ctx.ensemble_run(q, 20, YOSHIDA4, MIXED, cfg)
+    ctx.ensemble_run(q, 1000, YOSHIDA4, MIXED, cfg)
+    st = ctx.stats()
+    ens.update(steps_per_s=1000 / (st["ms_total"] / 1e3), pair_terms_per_s=st["interactions"] / (st["ms_total"] / 1e3))
+    out["pn_ensemble"] = ens
     return out
 
 
