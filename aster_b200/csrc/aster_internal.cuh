@@ -44,7 +44,7 @@ struct DevBuf {
 // LBVH device arrays (sized for n bodies, 2n-1 nodes).
 struct LbvhBufs {
     DevBuf codes, codes_alt, sorted_codes, perm, perm_alt, hist, digit_off;
-    DevBuf left, right, parent, sib, rlo, rhi, counters;
+    DevBuf parent, sib, rlo, rhi, counters;
     DevBuf node_cm, bmin, bmax;  // node_cm: double4 (com x, y, z, mass)
     DevBuf node_hi, node_lo, child, groups, crec, front;
     DevBuf node_v;  // double4 (vx, vy, vz, 0) per node: post-Newtonian walk only

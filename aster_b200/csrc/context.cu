@@ -116,7 +116,7 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
     DevBuf* bufs[] = {&c->pm, &c->vel, &c->acc, &c->phi, &c->plo, &c->vf, &c->scratch, &c->targets,
                       &c->stage, &c->red, &c->wh, &c->rec,
                       &c->tree.codes, &c->tree.codes_alt, &c->tree.sorted_codes, &c->tree.perm,
-                      &c->tree.perm_alt, &c->tree.hist, &c->tree.digit_off, &c->tree.left, &c->tree.right,
+                      &c->tree.perm_alt, &c->tree.hist, &c->tree.digit_off,
                       &c->tree.parent, &c->tree.sib, &c->tree.rlo, &c->tree.rhi, &c->tree.counters, &c->tree.node_cm,
                       &c->tree.bmin, &c->tree.bmax, &c->tree.node_hi,
                       &c->tree.node_lo, &c->tree.child, &c->tree.groups, &c->tree.crec, &c->tree.front,

@@ -296,6 +296,15 @@ __global__ void k_reverse(int64_t n, const KeyT* __restrict__ kin, const int32_t
     }
 }
 
+// A leaf's box: its position rounded outwards to FP32 (not stored: computed
+// from the leaf's node_cm wherever it is needed).
+__device__ __forceinline__ float4 leaf_lo(const double4 p) {
+    return make_float4(__double2float_rd(p.x), __double2float_rd(p.y), __double2float_rd(p.z), 0.f);
+}
+__device__ __forceinline__ float4 leaf_hi(const double4 p) {
+    return make_float4(__double2float_ru(p.x), __double2float_ru(p.y), __double2float_ru(p.z), 0.f);
+}
+
 // -------------------------------------------------------------- karras
 template <class KeyT, bool COMPAT>
 __device__ __forceinline__ int kdelta(const KeyT* __restrict__ codes, const int32_t* __restrict__ perm,
@@ -311,20 +320,16 @@ __device__ __forceinline__ int kdelta(const KeyT* __restrict__ codes, const int3
 
 template <class KeyT, bool COMPAT>
 __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restrict__ codes, const int32_t* __restrict__ perm,
-                                                const double4* __restrict__ pm, int32_t* __restrict__ left,
-                                                int32_t* __restrict__ right, int32_t* __restrict__ parent,
+                                                const double4* __restrict__ pm, int32_t* __restrict__ parent,
                                                 int32_t* __restrict__ sib, int32_t* __restrict__ rlo, int32_t* __restrict__ rhi,
                                                 int2* __restrict__ child, uint32_t* __restrict__ counters,
-                                                double4* __restrict__ node_cm, float4* __restrict__ bmin,
-                                                float4* __restrict__ bmax, float4* __restrict__ node_hi,
+                                                double4* __restrict__ node_cm, float4* __restrict__ node_hi,
                                                 float4* __restrict__ node_lo) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         // leaf i: gather body perm[i]
         {
             const double4 p = pm[perm[i]];
             node_cm[i] = p;
-            bmin[i] = make_float4(__double2float_rd(p.x), __double2float_rd(p.y), __double2float_rd(p.z), 0.f);
-            bmax[i] = make_float4(__double2float_ru(p.x), __double2float_ru(p.y), __double2float_ru(p.z), 0.f);
             float4 h, l;
             ds_split(p.x, h.x, l.x);
             ds_split(p.y, h.y, l.y);
@@ -333,11 +338,8 @@ __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restric
             l.w = 0.f;
             node_hi[i] = h;
             node_lo[i] = l;
-            left[i] = -1;
-            right[i] = -1;
             rlo[i] = (int32_t)i;
             rhi[i] = (int32_t)i;
-            child[i] = make_int2(-1, -1);
             if (n == 1) parent[0] = -1;
         }
         if (i == n - 1) {
@@ -366,8 +368,6 @@ __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restric
         const int64_t node = n + i;
         const int32_t L = (int32_t)(lo == gamma ? gamma : n + gamma);
         const int32_t R = (int32_t)(hi == gamma + 1 ? gamma + 1 : n + gamma + 1);
-        left[node] = L;
-        right[node] = R;
         child[node] = make_int2(L, R);
         parent[L] = (int32_t)node;
         parent[R] = (int32_t)node;
@@ -445,9 +445,10 @@ __global__ void __launch_bounds__(BU_LEAVES) k_bottom_up_local(
     s_cnt[j] = 0u;
     if (j == 0) s_nf = 0u;
     if (k < n) {
-        s_cm[0][j] = node_cm[k];
-        s_lo[0][j] = bmin[k];
-        s_hi[0][j] = bmax[k];
+        const double4 lc = node_cm[k];
+        s_cm[0][j] = lc;
+        s_lo[0][j] = leaf_lo(lc);
+        s_hi[0][j] = leaf_hi(lc);
         s_par[0][j] = parent[k];
         s_sib[0][j] = sib[k];
     }
@@ -519,14 +520,25 @@ __global__ void __launch_bounds__(BU_LEAVES) k_bottom_up_local(
     if ((unsigned)j < s_nf) front[s_fbase + j] = s_front[j];
 }
 
-#ifndef ASTER_BU_FENCE_ACQREL
-#define ASTER_BU_FENCE_ACQREL 0
+// Arrival at a node in the global phase: one atomic with acquire-release
+// semantics at GPU scope. Its release half publishes this climb's node data
+// (written before it) to the climb that arrives second; its acquire half
+// makes the sibling's data, published by the first arrival's release, visible
+// to the loads that follow. (ASTER_BU_FENCES=1: the equivalent form with a
+// full fence on either side of a relaxed atomicAdd.)
+#ifndef ASTER_BU_FENCES
+#define ASTER_BU_FENCES 0
 #endif
-__device__ __forceinline__ void bu_fence_gpu() {
-#if ASTER_BU_FENCE_ACQREL
-    asm volatile("fence.acq_rel.gpu;" ::: "memory");
-#else
+__device__ __forceinline__ unsigned int bu_arrive(unsigned int* counter) {
+#if ASTER_BU_FENCES
     __threadfence();
+    const unsigned int old = atomicAdd(counter, 1u);
+    __threadfence();
+    return old;
+#else
+    unsigned int old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+    return old;
 #endif
 }
 
@@ -542,7 +554,7 @@ __global__ void __launch_bounds__(256) k_bottom_up_front(int64_t n, const int32_
         int32_t cur = front[f];
         // the climb's own node data stays in registers; only the sibling's is loaded
         double4 cm = ld_cg(node_cm + cur);
-        float4 lo = ld_cg(bmin + cur), hi = ld_cg(bmax + cur);
+        float4 lo = cur < n ? leaf_lo(cm) : ld_cg(bmin + cur), hi = cur < n ? leaf_hi(cm) : ld_cg(bmax + cur);
         int32_t par = parent[cur], sb = sib[cur];
         for (int level = 0; par >= 0; ++level) {
             if (level >= MAX_CLIMB) {
@@ -551,12 +563,10 @@ __global__ void __launch_bounds__(256) k_bottom_up_front(int64_t n, const int32_
             }
             // the next level's links load while this level synchronises
             const int32_t par_next = parent[par], sb_next = sib[par];
-            bu_fence_gpu();  // release: this chain's node data
-            if (atomicAdd(&counters[par - n], 1u) == 0u) break;  // first arrival: the sibling finishes it
-            bu_fence_gpu();  // acquire: the sibling's node data
+            if (bu_arrive(&counters[par - n]) == 0u) break;  // first arrival: the sibling finishes it
             const int32_t so = sb >= 0 ? sb : ~sb;
             const double4 oc = ld_cg(node_cm + so);
-            const float4 ol = ld_cg(bmin + so), oh = ld_cg(bmax + so);
+            const float4 ol = so < n ? leaf_lo(oc) : ld_cg(bmin + so), oh = so < n ? leaf_hi(oc) : ld_cg(bmax + so);
             const bool right = sb < 0;  // cur is the right child
             double4 pc;
             float4 plo, phi;
@@ -598,9 +608,7 @@ __global__ void __launch_bounds__(256) k_node_vel(int64_t n, const int32_t* __re
                 atomicOr(err, ASTER_DEVERR_TREE);
                 break;
             }
-            __threadfence();  // release: this chain's node velocity
-            if (atomicAdd(&counters[par - n], 1u) == 0u) break;  // first arrival: the sibling finishes it
-            __threadfence();  // acquire: the sibling's
+            if (bu_arrive(&counters[par - n]) == 0u) break;  // first arrival: the sibling finishes it
             const int32_t so = sb >= 0 ? sb : ~sb;
             const double4 ov = ld_cg(node_v + so);
             const double mc = node_cm[cur].w, mo = node_cm[so].w, M = node_cm[par].w;
@@ -1308,16 +1316,14 @@ int run_build(aster_ctx* c, const aster_params* p) {
     const KeyT* sc = t.sorted_codes.as<KeyT>();
     if (p->compat_mode)
         k_karras<KeyT, true><<<grid, 256, 0, c->stream>>>(
-            n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.left.as<int32_t>(), t.right.as<int32_t>(),
-            t.parent.as<int32_t>(), t.sib.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(),
-            t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
-            t.node_hi.as<float4>(), t.node_lo.as<float4>());
+            n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.parent.as<int32_t>(), t.sib.as<int32_t>(),
+            t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(), t.counters.as<uint32_t>(),
+            t.node_cm.as<double4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>());
     else
         k_karras<KeyT, false><<<grid, 256, 0, c->stream>>>(
-            n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.left.as<int32_t>(), t.right.as<int32_t>(),
-            t.parent.as<int32_t>(), t.sib.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(),
-            t.counters.as<uint32_t>(), t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
-            t.node_hi.as<float4>(), t.node_lo.as<float4>());
+            n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.parent.as<int32_t>(), t.sib.as<int32_t>(),
+            t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(), t.counters.as<uint32_t>(),
+            t.node_cm.as<double4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>());
     ASTER_CUDA(cudaGetLastError());
     ASTER_TRY(launch_bottom_up(c, n));
     k_node_finalize<<<grid, 256, 0, c->stream>>>(n, p->theta, t.node_cm.as<double4>(), t.bmin.as<float4>(),
@@ -1346,8 +1352,6 @@ int ensure_tree(aster_ctx* c) {
     ASTER_TRY(t.perm_alt.ensure((size_t)n * 4));
     ASTER_TRY(t.hist.ensure((size_t)nblocks * RADIX * 4));
     ASTER_TRY(t.digit_off.ensure((size_t)RADIX * 4));
-    ASTER_TRY(t.left.ensure((size_t)m * 4));
-    ASTER_TRY(t.right.ensure((size_t)m * 4));
     ASTER_TRY(t.parent.ensure((size_t)m * 4));
     ASTER_TRY(t.sib.ensure((size_t)m * 4));
     ASTER_TRY(t.front.ensure((size_t)n * 4));
@@ -1426,15 +1430,22 @@ int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, b
 
 // ---- tree export -------------------------------------------------------------
 namespace {
-__global__ void k_export_nodes(int64_t m, const double4* __restrict__ cm, const float4* __restrict__ bmin,
+// Node i of m = 2n - 1 in the view's layout: leaves (i < n) have no children
+// and the box of their position; internal nodes' children come from child[].
+__global__ void k_export_nodes(int64_t n, int64_t m, const double4* __restrict__ cm, const float4* __restrict__ bmin,
                                const float4* __restrict__ bmax, const float4* __restrict__ lo,
-                               double* __restrict__ mass, double* __restrict__ com, float* __restrict__ fmin3,
-                               float* __restrict__ fmax3, float* __restrict__ rc2) {
+                               const int2* __restrict__ child, double* __restrict__ mass, double* __restrict__ com,
+                               float* __restrict__ fmin3, float* __restrict__ fmax3, float* __restrict__ rc2,
+                               int32_t* __restrict__ left, int32_t* __restrict__ right) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
         const double4 c = cm[i];
         mass[i] = c.w;
         com[3 * i] = c.x; com[3 * i + 1] = c.y; com[3 * i + 2] = c.z;
-        const float4 a = bmin[i], b = bmax[i];
+        const bool leaf = i < n;
+        const float4 a = leaf ? leaf_lo(c) : bmin[i], b = leaf ? leaf_hi(c) : bmax[i];
+        const int2 ch = leaf ? make_int2(-1, -1) : child[i];
+        left[i] = ch.x;
+        right[i] = ch.y;
         fmin3[3 * i] = a.x; fmin3[3 * i + 1] = a.y; fmin3[3 * i + 2] = a.z;
         fmax3[3 * i] = b.x; fmax3[3 * i + 1] = b.y; fmax3[3 * i + 2] = b.z;
         rc2[i] = lo[i].w;
@@ -1451,7 +1462,7 @@ static int export_tree(aster_ctx* c, const aster_params* p, aster_tree_view* v) 
     LbvhBufs& t = c->tree;
     const int64_t n = c->n, m = 2 * n - 1;
     cudaStream_t st = c->stream;
-    const size_t need = (size_t)m * (8 + 24 + 12 + 12 + 4) + (size_t)n * 16 + 1024;
+    const size_t need = (size_t)m * (8 + 24 + 12 + 12 + 4 + 8) + (size_t)n * 16 + 1024;
     ASTER_TRY(c->stage.ensure(need));
     char* base = c->stage.as<char>();
     double* mass = (double*)base;
@@ -1459,11 +1470,14 @@ static int export_tree(aster_ctx* c, const aster_params* p, aster_tree_view* v) 
     float* fmin3 = (float*)(com + 3 * m);
     float* fmax3 = fmin3 + 3 * m;
     float* rc2 = fmax3 + 3 * m;
-    uint64_t* wide = (uint64_t*)(((uintptr_t)(rc2 + m) + 15) & ~(uintptr_t)15);
+    int32_t* lft = (int32_t*)(rc2 + m);
+    int32_t* rgt = lft + m;
+    uint64_t* wide = (uint64_t*)(((uintptr_t)(rgt + m) + 15) & ~(uintptr_t)15);
     uint64_t* wide2 = wide + n;
     const int grid = (int)std::min<int64_t>((m + 255) / 256, (int64_t)c->sm_count * 16);
-    k_export_nodes<<<grid, 256, 0, st>>>(m, t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
-                                         t.node_lo.as<float4>(), mass, com, fmin3, fmax3, rc2);
+    k_export_nodes<<<grid, 256, 0, st>>>(n, m, t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
+                                         t.node_lo.as<float4>(), t.child.as<int2>(), mass, com, fmin3, fmax3, rc2,
+                                         lft, rgt);
     if (p->morton_bits == 63) {
         k_widen<uint64_t><<<grid, 256, 0, st>>>(n, t.codes.as<uint64_t>(), wide);
         k_widen<uint64_t><<<grid, 256, 0, st>>>(n, t.sorted_codes.as<uint64_t>(), wide2);
@@ -1479,8 +1493,8 @@ static int export_tree(aster_ctx* c, const aster_params* p, aster_tree_view* v) 
     ASTER_TRY(cp(v->codes, wide, (size_t)n * 8));
     ASTER_TRY(cp(v->sorted_codes, wide2, (size_t)n * 8));
     ASTER_TRY(cp(v->perm, t.perm.ptr, (size_t)n * 4));
-    ASTER_TRY(cp(v->left, t.left.ptr, (size_t)m * 4));
-    ASTER_TRY(cp(v->right, t.right.ptr, (size_t)m * 4));
+    ASTER_TRY(cp(v->left, lft, (size_t)m * 4));
+    ASTER_TRY(cp(v->right, rgt, (size_t)m * 4));
     ASTER_TRY(cp(v->parent, t.parent.ptr, (size_t)m * 4));
     ASTER_TRY(cp(v->range_lo, t.rlo.ptr, (size_t)m * 4));
     ASTER_TRY(cp(v->range_hi, t.rhi.ptr, (size_t)m * 4));
