@@ -46,7 +46,7 @@ struct LbvhBufs {
     DevBuf codes, codes_alt, sorted_codes, perm, perm_alt, hist, digit_off;
     DevBuf parent, sib, rlo, rhi, counters;
     DevBuf node_cm, bmin, bmax;  // node_cm: double4 (com x, y, z, mass)
-    DevBuf node_hi, node_lo, child, groups, crec, front;
+    DevBuf child, groups, crec, front;
     DevBuf node_v;  // double4 (vx, vy, vz, 0) per node: post-Newtonian walk only
     int64_t n = 0;
     bool built = false;

@@ -118,8 +118,7 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
                       &c->tree.codes, &c->tree.codes_alt, &c->tree.sorted_codes, &c->tree.perm,
                       &c->tree.perm_alt, &c->tree.hist, &c->tree.digit_off,
                       &c->tree.parent, &c->tree.sib, &c->tree.rlo, &c->tree.rhi, &c->tree.counters, &c->tree.node_cm,
-                      &c->tree.bmin, &c->tree.bmax, &c->tree.node_hi,
-                      &c->tree.node_lo, &c->tree.child, &c->tree.groups, &c->tree.crec, &c->tree.front,
+                      &c->tree.bmin, &c->tree.bmax, &c->tree.child, &c->tree.groups, &c->tree.crec, &c->tree.front,
                       &c->tree.node_v};
     for (DevBuf* b : bufs) b->release();
     DevBuf* ens[] = {&c->ens.pm, &c->ens.vel, &c->ens.off, &c->ens.order, &c->ens.counter,

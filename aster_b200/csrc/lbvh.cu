@@ -305,6 +305,38 @@ __device__ __forceinline__ float4 leaf_hi(const double4 p) {
     return make_float4(__double2float_ru(p.x), __double2float_ru(p.y), __double2float_ru(p.z), 0.f);
 }
 
+// Traversal data of a node (the walk's view of it): h = (rn(com), rn(mass)),
+// l = (com - rn(com), rcrit2). Internal node: the squared opening radius
+// r_crit = l/theta + |com - box centre| (l = longest AABB side; FP64, rounded
+// up to FP32). Leaf: rcrit2 = 0.
+__device__ __forceinline__ void node_trav(const double4 c, const float4 lo, const float4 hi, double theta, float4& h,
+                                          float4& l) {
+    const double ex = __dsub_rn((double)hi.x, (double)lo.x), ey = __dsub_rn((double)hi.y, (double)lo.y),
+                 ez = __dsub_rn((double)hi.z, (double)lo.z);
+    double lmax = 0.0;
+    lmax = ex > lmax ? ex : lmax;
+    lmax = ey > lmax ? ey : lmax;
+    lmax = ez > lmax ? ez : lmax;
+    const double cx = __dmul_rn(0.5, __dadd_rn((double)lo.x, (double)hi.x));
+    const double cy = __dmul_rn(0.5, __dadd_rn((double)lo.y, (double)hi.y));
+    const double cz = __dmul_rn(0.5, __dadd_rn((double)lo.z, (double)hi.z));
+    const double dx = __dsub_rn(c.x, cx), dy = __dsub_rn(c.y, cy), dz = __dsub_rn(c.z, cz);
+    const double delta = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    const double rc = __dadd_rn(__ddiv_rn(lmax, theta), delta);
+    ds_split(c.x, h.x, l.x);
+    ds_split(c.y, h.y, l.y);
+    ds_split(c.z, h.z, l.z);
+    h.w = __double2float_rn(c.w);
+    l.w = __double2float_ru(__dmul_rn(rc, rc));
+}
+__device__ __forceinline__ void leaf_trav(const double4 c, float4& h, float4& l) {
+    ds_split(c.x, h.x, l.x);
+    ds_split(c.y, h.y, l.y);
+    ds_split(c.z, h.z, l.z);
+    h.w = __double2float_rn(c.w);
+    l.w = 0.f;
+}
+
 // -------------------------------------------------------------- karras
 template <class KeyT, bool COMPAT>
 __device__ __forceinline__ int kdelta(const KeyT* __restrict__ codes, const int32_t* __restrict__ perm,
@@ -323,21 +355,11 @@ __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restric
                                                 const double4* __restrict__ pm, int32_t* __restrict__ parent,
                                                 int32_t* __restrict__ sib, int32_t* __restrict__ rlo, int32_t* __restrict__ rhi,
                                                 int2* __restrict__ child, uint32_t* __restrict__ counters,
-                                                double4* __restrict__ node_cm, float4* __restrict__ node_hi,
-                                                float4* __restrict__ node_lo) {
+                                                double4* __restrict__ node_cm) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         // leaf i: gather body perm[i]
         {
-            const double4 p = pm[perm[i]];
-            node_cm[i] = p;
-            float4 h, l;
-            ds_split(p.x, h.x, l.x);
-            ds_split(p.y, h.y, l.y);
-            ds_split(p.z, h.z, l.z);
-            h.w = __double2float_rn(p.w);
-            l.w = 0.f;
-            node_hi[i] = h;
-            node_lo[i] = l;
+            node_cm[i] = pm[perm[i]];
             rlo[i] = (int32_t)i;
             rhi[i] = (int32_t)i;
             if (n == 1) parent[0] = -1;
@@ -635,83 +657,56 @@ __global__ void __launch_bounds__(256) k_node_vel(int64_t n, const int32_t* __re
     }
 }
 
-// Per internal node, after the climb (no dependencies, fully parallel): the
-// squared opening radius r_crit = l/theta + |com - box centre| (l = longest
-// AABB side; FP64, rounded up to FP32) and the traversal records
-// node_hi = (rn(com), rn(mass)), node_lo = (com - rn(com), rcrit2).
-__global__ void __launch_bounds__(256) k_node_finalize(int64_t n, double theta, const double4* __restrict__ node_cm,
-                                                       const float4* __restrict__ bmin,
-                                                       const float4* __restrict__ bmax, float4* __restrict__ node_hi,
-                                                       float4* __restrict__ node_lo) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n - 1; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t v = n + i;
-        const double4 c = node_cm[v];
-        const float4 lo = bmin[v], hi = bmax[v];
-        const double ex = __dsub_rn((double)hi.x, (double)lo.x), ey = __dsub_rn((double)hi.y, (double)lo.y),
-                     ez = __dsub_rn((double)hi.z, (double)lo.z);
-        double lmax = 0.0;
-        lmax = ex > lmax ? ex : lmax;
-        lmax = ey > lmax ? ey : lmax;
-        lmax = ez > lmax ? ez : lmax;
-        const double cx = __dmul_rn(0.5, __dadd_rn((double)lo.x, (double)hi.x));
-        const double cy = __dmul_rn(0.5, __dadd_rn((double)lo.y, (double)hi.y));
-        const double cz = __dmul_rn(0.5, __dadd_rn((double)lo.z, (double)hi.z));
-        const double dx = __dsub_rn(c.x, cx), dy = __dsub_rn(c.y, cy), dz = __dsub_rn(c.z, cz);
-        const double delta = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-        const double rc = __dadd_rn(__ddiv_rn(lmax, theta), delta);
-        float4 h, l;
-        ds_split(c.x, h.x, l.x);
-        ds_split(c.y, h.y, l.y);
-        ds_split(c.z, h.z, l.z);
-        h.w = __double2float_rn(c.w);
-        l.w = __double2float_ru(__dmul_rn(rc, rc));
-        node_hi[v] = h;
-        node_lo[v] = l;
-    }
-}
-
-// Child records for the walk: for internal node i (node n+i) the traversal
-// records of its two children in one contiguous 64-byte record, so opening a
-// node costs one load (layout below).
-__global__ void __launch_bounds__(256) k_child_records(int64_t n, const int2* __restrict__ child,
-                                                       const float4* __restrict__ node_hi,
-                                                       const float4* __restrict__ node_lo, float4* __restrict__ crec) {
-    // One 64-byte record per internal node holding both children, each field
-    // as a (left, right) pair so that the walk's paired FP32 opening test and
-    // list-entry arithmetic read aligned register pairs:
-    // (xL xR yL yR) (zL zR mL mR) (lxL lxR lyL lyR) (lzL lzR rcrit2L rcrit2R).
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n - 1; i += (int64_t)gridDim.x * blockDim.x) {
-        const int2 ch = child[n + i];
-        const float4 hL = node_hi[ch.x], lL = node_lo[ch.x], hR = node_hi[ch.y], lR = node_lo[ch.y];
-        float4* dst = crec + 4 * i;
-        dst[0] = make_float4(hL.x, hR.x, hL.y, hR.y);
-        dst[1] = make_float4(hL.z, hR.z, hL.w, hR.w);
-        dst[2] = make_float4(lL.x, lR.x, lL.y, lR.y);
-        dst[3] = make_float4(lL.z, lR.z, lL.w, lR.w);
-    }
-}
-
-// ----------------------------------------------------------------- walk
 // Groups: a node whose subtree holds at most GROUP_MAX leaves while its
 // parent's holds more (the root when n <= GROUP_MAX). Its leaves are a
 // contiguous sorted run sharing a Morton prefix, so the group is spatially
 // compact (a fixed run of consecutive sorted bodies is not: it can straddle a
 // Morton jump and span the whole system).
-__global__ void __launch_bounds__(256) k_make_groups(int64_t n, const int32_t* __restrict__ parent,
-                                                     const int32_t* __restrict__ rlo,
-                                                     const int32_t* __restrict__ rhi, int2* __restrict__ groups,
-                                                     unsigned int* __restrict__ ngroups) {
-    const int64_t m = 2 * n - 1;
-    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < m; v += (int64_t)gridDim.x * blockDim.x) {
-        const int sz = rhi[v] - rlo[v] + 1;
-        if (sz > GROUP_MAX) continue;
+//
+// Per internal node i (node v = n + i), after the climb (fully parallel): the
+// traversal data of both children go into one contiguous 64-byte child
+// record, so opening a node costs one load, each field as a (left, right)
+// pair so that the walk's paired FP32 opening test and list-entry arithmetic
+// read aligned register pairs:
+// (xL xR yL yR) (zL zR mL mR) (lxL lxR lyL lyR) (lzL lzR rcrit2L rcrit2R);
+// and the walk groups among node n + i and leaf i are listed.
+__global__ void __launch_bounds__(256) k_node_records(int64_t n, double theta, const int2* __restrict__ child,
+                                                      const double4* __restrict__ node_cm,
+                                                      const float4* __restrict__ bmin, const float4* __restrict__ bmax,
+                                                      const int32_t* __restrict__ parent,
+                                                      const int32_t* __restrict__ rlo, const int32_t* __restrict__ rhi,
+                                                      float4* __restrict__ crec, int2* __restrict__ groups,
+                                                      unsigned int* __restrict__ ngroups) {
+    // thread i: internal node n + i (record and group test) and leaf i (group
+    // test), so groups are listed roughly in sorted-leaf order, which keeps
+    // consecutive walk groups close in space
+    auto group_test = [&](int64_t v, int sz) {
+        if (sz > GROUP_MAX) return;
         const int32_t p = n == 1 ? -1 : parent[v];
-        if (p >= 0 && rhi[p] - rlo[p] + 1 <= GROUP_MAX) continue;
-        const unsigned slot = atomicAdd(ngroups, 1u);
-        groups[slot] = make_int2(rlo[v], sz);
+        if (p >= 0 && rhi[p] - rlo[p] + 1 <= GROUP_MAX) return;
+        groups[atomicAdd(ngroups, 1u)] = make_int2(v < n ? (int32_t)v : rlo[v], sz);
+    };
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        group_test(i, 1);
+        if (i >= n - 1) continue;
+        const int64_t v = n + i;
+        const int2 ch = child[v];
+        float4 hL, lL, hR, lR;
+        const double4 cL = node_cm[ch.x], cR = node_cm[ch.y];
+        if (ch.x < n) leaf_trav(cL, hL, lL);
+        else node_trav(cL, bmin[ch.x], bmax[ch.x], theta, hL, lL);
+        if (ch.y < n) leaf_trav(cR, hR, lR);
+        else node_trav(cR, bmin[ch.y], bmax[ch.y], theta, hR, lR);
+        float4* dst = crec + 4 * i;
+        dst[0] = make_float4(hL.x, hR.x, hL.y, hR.y);
+        dst[1] = make_float4(hL.z, hR.z, hL.w, hR.w);
+        dst[2] = make_float4(lL.x, lR.x, lL.y, lR.y);
+        dst[3] = make_float4(lL.z, lR.z, lL.w, lR.w);
+        group_test(v, rhi[v] - rlo[v] + 1);
     }
 }
 
+// ----------------------------------------------------------------- walk
 template <bool MIXED>
 struct WalkShared {
     int stack[WALK_WARPS][WALK_STACK];
@@ -878,7 +873,7 @@ __device__ __forceinline__ float2 box_dist2_pair(const float2 cx, const float2 c
 template <bool MIXED, bool GUARD, bool KICK, int PNL = 0>
 __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK_MINBLOCKS : 6)) k_walk(
     int64_t n, const int2* __restrict__ groups, const unsigned int* __restrict__ ngroups_p,
-    unsigned int* __restrict__ work, const float4* __restrict__ node_hi, const float4* __restrict__ node_lo,
+    unsigned int* __restrict__ work,
     const float4* __restrict__ crec, const double4* __restrict__ node_cm, const int2* __restrict__ child,
     const int32_t* __restrict__ perm, double G, double eps2, double half_dt, double4* __restrict__ acc,
     double4* __restrict__ vel, int* __restrict__ err, int* __restrict__ stack_hw, int stack_limit,
@@ -910,8 +905,14 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK
         const int64_t k0 = (int64_t)gr.x + (v0 ? lane : 0);
         const int64_t k1 = (int64_t)gr.x + (v1 ? 32 + sb : 0);
 
-        const float4 h0 = node_hi[k0], l0 = node_lo[k0];
-        const float4 h1 = two ? node_hi[k1] : h0, l1 = two ? node_lo[k1] : l0;
+        float4 h0, l0, h1, l1;  // the bodies' traversal data, from their leaves
+        leaf_trav(node_cm[k0], h0, l0);
+        if (two) {
+            leaf_trav(node_cm[k1], h1, l1);
+        } else {
+            h1 = h0;
+            l1 = l0;
+        }
         const float glox = warp_min_f(fminf(v0 ? h0.x : INFINITY, v1 ? h1.x : INFINITY));
         const float gloy = warp_min_f(fminf(v0 ? h0.y : INFINITY, v1 ? h1.y : INFINITY));
         const float gloz = warp_min_f(fminf(v0 ? h0.z : INFINITY, v1 ? h1.z : INFINITY));
@@ -1050,7 +1051,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK
         } else {
             if (lane == 0) {  // a single body: its own leaf
                 if (MIXED) {
-                    const float4 h = node_hi[0], l = node_lo[0];
+                    float4 h, l;
+                    leaf_trav(node_cm[0], h, l);
                     put(0, (h.x - cgx) + l.x, (h.y - cgy) + l.y, (h.z - cgz) + l.z, h.w);
                 } else {
                     sm.lcm[warp][0] = node_cm[0];
@@ -1232,7 +1234,7 @@ int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts) {
     if (blocks > need) blocks = need;
     unsigned int* gcount = red_groups(c);
     kern<<<(unsigned)blocks, WALK_WARPS * 32, 0, c->stream>>>(
-        c->n, t.groups.as<int2>(), gcount, gcount + 1, t.node_hi.as<float4>(), t.node_lo.as<float4>(),
+        c->n, t.groups.as<int2>(), gcount, gcount + 1,
         t.crec.as<float4>(), t.node_cm.as<double4>(), t.child.as<int2>(), t.perm.as<int32_t>(), p->G, p->eps2, 0.5 * p->dt,
         c->acc.as<double4>(), c->vel.as<double4>(), c->err_dev, c->stack_hw_dev, c->walk_stack_limit, counts,
         red_inter(c), PNL > 0 ? t.node_v.as<double4>() : nullptr, make_pn(p));
@@ -1318,26 +1320,20 @@ int run_build(aster_ctx* c, const aster_params* p) {
         k_karras<KeyT, true><<<grid, 256, 0, c->stream>>>(
             n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.parent.as<int32_t>(), t.sib.as<int32_t>(),
             t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(), t.counters.as<uint32_t>(),
-            t.node_cm.as<double4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>());
+            t.node_cm.as<double4>());
     else
         k_karras<KeyT, false><<<grid, 256, 0, c->stream>>>(
             n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.parent.as<int32_t>(), t.sib.as<int32_t>(),
             t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(), t.counters.as<uint32_t>(),
-            t.node_cm.as<double4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>());
+            t.node_cm.as<double4>());
     ASTER_CUDA(cudaGetLastError());
     ASTER_TRY(launch_bottom_up(c, n));
-    k_node_finalize<<<grid, 256, 0, c->stream>>>(n, p->theta, t.node_cm.as<double4>(), t.bmin.as<float4>(),
-                                                 t.bmax.as<float4>(), t.node_hi.as<float4>(), t.node_lo.as<float4>());
+    k_node_records<<<grid, 256, 0, c->stream>>>(n, p->theta, t.child.as<int2>(), t.node_cm.as<double4>(),
+                                                t.bmin.as<float4>(), t.bmax.as<float4>(), t.parent.as<int32_t>(),
+                                                t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.crec.as<float4>(),
+                                                t.groups.as<int2>(), gcount);
     ASTER_CUDA(cudaGetLastError());
-    if (n >= 2) {
-        k_child_records<<<grid, 256, 0, c->stream>>>(n, t.child.as<int2>(), t.node_hi.as<float4>(),
-                                                     t.node_lo.as<float4>(), t.crec.as<float4>());
-        ASTER_CUDA(cudaGetLastError());
-    }
-    k_make_groups<<<grid, 256, 0, c->stream>>>(n, t.parent.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(),
-                                               t.groups.as<int2>(), gcount);
-    ASTER_CUDA(cudaGetLastError());
-    c->stats.kernels += 4;
+    c->stats.kernels += 2;
     return ASTER_OK;
 }
 
@@ -1361,8 +1357,6 @@ int ensure_tree(aster_ctx* c) {
     ASTER_TRY(t.node_cm.ensure((size_t)m * sizeof(double4)));
     ASTER_TRY(t.bmin.ensure((size_t)m * sizeof(float4)));
     ASTER_TRY(t.bmax.ensure((size_t)m * sizeof(float4)));
-    ASTER_TRY(t.node_hi.ensure((size_t)m * sizeof(float4)));
-    ASTER_TRY(t.node_lo.ensure((size_t)m * sizeof(float4)));
     ASTER_TRY(t.child.ensure((size_t)m * sizeof(int2)));
     ASTER_TRY(t.groups.ensure((size_t)n * sizeof(int2)));
     ASTER_TRY(t.crec.ensure((size_t)4 * n * sizeof(float4)));
@@ -1432,8 +1426,8 @@ int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, b
 namespace {
 // Node i of m = 2n - 1 in the view's layout: leaves (i < n) have no children
 // and the box of their position; internal nodes' children come from child[].
-__global__ void k_export_nodes(int64_t n, int64_t m, const double4* __restrict__ cm, const float4* __restrict__ bmin,
-                               const float4* __restrict__ bmax, const float4* __restrict__ lo,
+__global__ void k_export_nodes(int64_t n, int64_t m, double theta, const double4* __restrict__ cm,
+                               const float4* __restrict__ bmin, const float4* __restrict__ bmax,
                                const int2* __restrict__ child, double* __restrict__ mass, double* __restrict__ com,
                                float* __restrict__ fmin3, float* __restrict__ fmax3, float* __restrict__ rc2,
                                int32_t* __restrict__ left, int32_t* __restrict__ right) {
@@ -1448,7 +1442,10 @@ __global__ void k_export_nodes(int64_t n, int64_t m, const double4* __restrict__
         right[i] = ch.y;
         fmin3[3 * i] = a.x; fmin3[3 * i + 1] = a.y; fmin3[3 * i + 2] = a.z;
         fmax3[3 * i] = b.x; fmax3[3 * i + 1] = b.y; fmax3[3 * i + 2] = b.z;
-        rc2[i] = lo[i].w;
+        float4 h, l;
+        if (leaf) leaf_trav(c, h, l);
+        else node_trav(c, a, b, theta, h, l);
+        rc2[i] = l.w;
     }
 }
 template <class KeyT>
@@ -1475,9 +1472,9 @@ static int export_tree(aster_ctx* c, const aster_params* p, aster_tree_view* v) 
     uint64_t* wide = (uint64_t*)(((uintptr_t)(rgt + m) + 15) & ~(uintptr_t)15);
     uint64_t* wide2 = wide + n;
     const int grid = (int)std::min<int64_t>((m + 255) / 256, (int64_t)c->sm_count * 16);
-    k_export_nodes<<<grid, 256, 0, st>>>(n, m, t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
-                                         t.node_lo.as<float4>(), t.child.as<int2>(), mass, com, fmin3, fmax3, rc2,
-                                         lft, rgt);
+    k_export_nodes<<<grid, 256, 0, st>>>(n, m, p->theta, t.node_cm.as<double4>(), t.bmin.as<float4>(),
+                                         t.bmax.as<float4>(), t.child.as<int2>(), mass, com, fmin3, fmax3, rc2, lft,
+                                         rgt);
     if (p->morton_bits == 63) {
         k_widen<uint64_t><<<grid, 256, 0, st>>>(n, t.codes.as<uint64_t>(), wide);
         k_widen<uint64_t><<<grid, 256, 0, st>>>(n, t.sorted_codes.as<uint64_t>(), wide2);
