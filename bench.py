@@ -609,6 +609,29 @@ def run_case(args):
         ctx.wh_steps(p, 2)
         ctx.wh_steps(p, 20)
         out["ms_20_steps"] = ctx.stats()["ms_total"]
+    elif args.case == "scale":
+        # the C2 step (mixed LBVH KDK, theta = 0.5, eps = 0.005) at larger N
+        from aster_b200.api import SOLVER_LBVH
+        out["runs"] = []
+        for lg in (22, 24, 25):
+            n = 1 << lg
+            pos, vel, m = gen.plummer(n, SEED_C2, masses="lognormal")
+            p = Params(G=1.0, eps2=EPS * EPS, theta=THETA, dt=DT)
+            ctx.upload(pos, vel, m)
+            ctx.kdk_steps(p, 1, SOLVER_LBVH, MIXED)
+            ctx.kdk_steps(p, 3, SOLVER_LBVH, MIXED)
+            st = ctx.stats()
+            run = {"n": n, "ms_per_step": st["ms_total"] / 3, "ms_build": st["ms_build"] / 3,
+                   "ms_walk": st["ms_force"] / 3, "interactions_per_step": st["interactions"] / 3,
+                   "walk_stack_high_water": st["max_stack"]}
+            if lg == 24:
+                tg = np.random.default_rng(4096).choice(n, 4096, replace=False)
+                a = ctx.lbvh_forces(p, MIXED)
+                exact = ctx.allpairs_targets(p, tg, FP64)
+                run["approx_rel_l2_vs_fp64_allpairs_4096_sample"] = float(
+                    np.linalg.norm(a[tg] - exact) / np.linalg.norm(exact))
+            out["runs"].append(run)
+            del pos, vel, m
     elif args.case == "ensemble":
         pos, vel, m, off = gen.hierarchical_ensemble(16384, 1004)
         p = Params(G=1.0, c=100.0, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1)
@@ -641,7 +664,7 @@ def main():
                     help="bodies in the headline workload (default 2^20; smaller only for profiling captures)")
     ap.add_argument("--walk-traffic", type=float, default=WALK_TRAFFIC_BYTES,
                     help="DRAM bytes per walk launch from an ncu capture (reported as roofline.traffic)")
-    ap.add_argument("--case", default=None, choices=["allpairs", "ensemble", "adjoint", "c3drift", "wh"],
+    ap.add_argument("--case", default=None, choices=["allpairs", "ensemble", "adjoint", "c3drift", "wh", "scale"],
                     help="run one secondary workload briefly (used for profiling captures) and exit")
     args = ap.parse_args()
     if args.warmup < 3:
