@@ -386,6 +386,7 @@ void launch_pnl(int precision, bool guard, dim3 grid, cudaStream_t st, int64_t j
 int aster_allpairs_launch_range(aster_ctx* c, const aster_params* p, int precision, bool closing_kick, int64_t nt,
                                 const int32_t* targets_dev, double* out_dev, int64_t src_lo, int64_t src_hi) {
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
+    if (precision == ASTER_MIXED && !c->mixed_valid) ASTER_TRY(aster_refresh_mixed(c));
     const int64_t n_src = c->n_src > 0 ? c->n_src : c->n;
     const int64_t lo = src_lo, hi = src_hi < n_src ? src_hi : n_src;
     const int64_t len = hi > lo ? hi - lo : 0;
@@ -408,6 +409,7 @@ int aster_allpairs_launch_range(aster_ctx* c, const aster_params* p, int precisi
         partial = c->scratch.as<double4>();
     }
     KickArgs kick{closing_kick && !out_dev, 0.5 * p->dt, c->vel.as<double4>()};
+    if (kick.on) c->mixed_valid = false;  // the closing kick moves the velocities
     dim3 grid((unsigned)iblocks, (unsigned)ns);
     const bool guard = !(p->eps2 > 0.0);
     const int pnl = pn_level(p);

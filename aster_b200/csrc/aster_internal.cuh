@@ -89,6 +89,10 @@ struct aster_ctx {
     DevBuf wh;        // Wisdom-Holman: reduction partials and state scalars
     DevBuf rec;       // aster_record: the sample table and its reductions
     bool acc_valid = false;
+    // phi/plo/vf (the FP32 copies the mixed all-pairs kernels read) match
+    // pm/vel; anything that moves positions or velocities without refreshing
+    // them clears it, and a mixed all-pairs launch refreshes them first
+    bool mixed_valid = false;
     int* err_dev = nullptr;     // device error flags
     int* err_host = nullptr;    // pinned copy
     int* stack_hw_dev = nullptr;  // tree-walk stack high-water mark

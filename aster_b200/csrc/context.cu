@@ -230,6 +230,7 @@ int aster_refresh_mixed(aster_ctx* c) {
         c->n, c->pm.as<double4>(), c->vel.as<double4>(), c->phi.as<float4>(), c->plo.as<float4>(),
         c->vf.as<float4>());
     ASTER_CUDA(cudaGetLastError());
+    c->mixed_valid = true;
     return ASTER_OK;
 }
 
@@ -266,6 +267,7 @@ int aster_upload_enqueue(aster_ctx* c, int64_t n, const double* pos, const doubl
         ASTER_CUDA(cudaMemsetAsync(c->acc.ptr, 0, n4d, c->stream));
     }
     c->n = n;
+    c->mixed_valid = true;  // k_pack_state wrote the FP32 copies
     // trailing massless bodies (test particles) attract nothing: the
     // all-pairs source loop ends at the last massive body (scanned from the end)
     int64_t last = n - 1;

@@ -152,6 +152,7 @@ int aster_kick_drift_launch(aster_ctx* c, const aster_params* p, bool want_box, 
 
 // v += a * kick_dt (skipped when !kick); x += v * drift_dt.
 int aster_kick_drift_coef(aster_ctx* c, double kick_dt, double drift_dt, bool kick, bool want_box, bool want_mixed) {
+    c->mixed_valid = want_mixed;  // the kernel refreshes the FP32 copies only when asked
     const int64_t n = c->n;
     int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 8);
     if (grid < 1) grid = 1;

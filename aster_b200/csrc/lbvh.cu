@@ -1384,6 +1384,7 @@ int aster_lbvh_build_dev(aster_ctx* c, const aster_params* p, bool box_ready) {
 }
 
 int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, bool kick, int32_t* counts) {
+    if (kick) c->mixed_valid = false;  // the closing kick moves the velocities
     ASTER_CUDA(cudaMemsetAsync(red_groups(c) + 1, 0, sizeof(unsigned int), c->stream));  // work counter
     const bool guard = !(p->eps2 > 0.0);
     if (precision != ASTER_MIXED && precision != ASTER_FP64) return ASTER_ERR_INVALID_ARG;

@@ -322,6 +322,7 @@ int aster_wh_enqueue(aster_ctx* c, const aster_params* p, int precision, int nst
     ASTER_TRY(c->wh.ensure((size_t)(4 * std::max<int64_t>(nbmax, 1) + 32) * sizeof(double)));
     const WhLayout L = wh_layout(c);
     ASTER_CUDA(cudaMemsetAsync(L.st + 30, 0, sizeof(double), c->stream));  // arm the reduction counter
+    c->mixed_valid = false;  // the steps move positions and velocities (mixed runs refresh as they go)
     const double mu = p->G * m0;
     double4* pm = c->pm.as<double4>();
     double4* vel = c->vel.as<double4>();

@@ -222,3 +222,27 @@ def test_trailing_massless_sources(ctx, orc, n_massive):
     ctx.upload(pos, vel, m0)
     ref = orc.allpairs(pos, m0, 1.0, 1e-4)
     assert rel_l2(ctx.allpairs(Params(eps2=1e-4), FP64), ref) < TOL_FP64
+
+
+def test_mixed_allpairs_sees_the_state_left_by_other_steppers(ctx):
+    """A mixed all-pairs evaluation after steps taken another way (tree KDK,
+    FP64 all-pairs KDK, SABA, mixed KDK whose closing kick moved the
+    velocities) uses the current positions and velocities: it agrees with the
+    FP64 evaluation of the same state, Newtonian and 1PN."""
+    from aster_b200.api import SOLVER_ALLPAIRS, SOLVER_LBVH
+    pos, vel, m = gen.plummer(4096, 91)
+    step = Params(eps2=1e-4, dt=5e-3, c=30.0, force_law=NEWTON | PN1)
+    steppers = {
+        "lbvh_fp64": lambda: ctx.kdk_steps(Params(eps2=1e-4, dt=5e-3), 3, SOLVER_LBVH, FP64),
+        "allpairs_fp64": lambda: ctx.kdk_steps(step, 3, SOLVER_ALLPAIRS, FP64),
+        "allpairs_mixed_pn": lambda: ctx.kdk_steps(step, 3, SOLVER_ALLPAIRS, MIXED),
+        "saba2_fp64": lambda: ctx.saba_steps(step, 2, 2, SOLVER_ALLPAIRS, FP64),
+    }
+    for name, run in steppers.items():
+        ctx.upload(pos, vel * 3.0, m)
+        run()
+        for law in (NEWTON, NEWTON | PN1):
+            q = Params(eps2=1e-4, c=30.0, force_law=law)
+            a64 = ctx.allpairs(q, FP64)
+            a32 = ctx.allpairs(q, MIXED)
+            assert rel_l2(a32, a64) < TOL_MIXED, (name, law)
