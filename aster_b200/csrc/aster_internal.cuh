@@ -103,7 +103,12 @@ struct aster_ctx {
     EnsBufs ens;
     AdjBufs adj;
     aster_stats stats{};
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // [0], [1] timing; [2] final positions ready; [3] upload copies issued;
+    // [4] masses copied (overlapped upload)
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // masses still on their way (overlapped upload): staging copy on the
+    // device, applied to pm[].w before the tree build reads them
+    const double* mass_pending = nullptr;
 };
 
 // Layout of ctx->red (4 KB of small device scalars).
@@ -119,6 +124,11 @@ int aster_check_params(const aster_params* p);
 int aster_begin(aster_ctx* ctx);                // clears the device error flag
 int aster_finish(aster_ctx* ctx);               // syncs, turns flags into status
 int aster_refresh_mixed(aster_ctx* ctx);        // rebuild phi/plo/vf from pm/vel
+// Host state -> device with the masses' copy overlapped (see context.cu)
+int aster_upload_enqueue_overlapped(aster_ctx* c, int64_t n, const double* pos, const double* vel, const double* mass,
+                                    const double* acc);
+// applies masses still on their way (waits for their copy); no-op otherwise
+int aster_apply_pending_mass(aster_ctx* c);
 int aster_copy_acc_out(aster_ctx* ctx, double* acc_out);
 
 // ---- kernels exposed across translation units ------------------------------

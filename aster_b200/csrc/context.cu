@@ -94,7 +94,7 @@ extern "C" int aster_ctx_create(aster_ctx** out, int device, void* stream) {
     }
     cudaError_t e = cudaMalloc(&c->err_dev, 2 * sizeof(int));
     if (e == cudaSuccess) e = cudaHostAlloc(&c->err_host, 2 * sizeof(int), cudaHostAllocDefault);
-    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
     if (e != cudaSuccess) {
         aster_ctx_destroy(c);
         return aster_cuda_fail(e, "aster_ctx_create", __FILE__, __LINE__);
@@ -126,7 +126,7 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
                      &c->adj.target, &c->adj.part};
     for (DevBuf* b : ens) b->release();
     if (c->ens.cancel_host) cudaFreeHost((void*)c->ens.cancel_host);
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 6; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->err_dev) cudaFree(c->err_dev);
     if (c->err_host) cudaFreeHost(c->err_host);
@@ -275,6 +275,84 @@ int aster_upload_enqueue(aster_ctx* c, int64_t n, const double* pos, const doubl
     c->n_src = last + 1;
     c->acc_valid = acc != nullptr;
     c->tree.built = false;
+    return ASTER_OK;
+}
+
+// Positions, velocities and accelerations into pm.xyz, vel, acc (pm.w is set
+// by k_set_mass once the masses have arrived).
+__global__ void k_pack_pva(int64_t n, const double* __restrict__ pos, const double* __restrict__ vel,
+                           const double* __restrict__ acc, double4* __restrict__ pm, double4* __restrict__ v4,
+                           double4* __restrict__ a4, int* err) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+        const double vx = vel[3 * i], vy = vel[3 * i + 1], vz = vel[3 * i + 2];
+        const double ax = acc[3 * i], ay = acc[3 * i + 1], az = acc[3 * i + 2];
+        if (!(isfinite(x) && isfinite(y) && isfinite(z) && isfinite(vx) && isfinite(vy) && isfinite(vz) &&
+              isfinite(ax) && isfinite(ay) && isfinite(az)))
+            atomicOr(err, ASTER_DEVERR_NONFINITE);
+        pm[i] = make_double4(x, y, z, 0.0);
+        v4[i] = make_double4(vx, vy, vz, 0.0);
+        a4[i] = make_double4(ax, ay, az, 0.0);
+    }
+}
+
+__global__ void k_set_mass(int64_t n, const double* __restrict__ mass, double4* __restrict__ pm, int* err) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double m = mass[i];
+        if (!isfinite(m)) atomicOr(err, ASTER_DEVERR_NONFINITE);
+        pm[i].w = m;
+    }
+}
+
+// Host state -> device for a step on the tree solver, with the masses' copy
+// off the critical path: positions, velocities and accelerations go first,
+// back to back on the context stream; the masses follow on the copy stream
+// and arrive while the kick-drift, bounding box, Morton codes and sort run
+// (none of which reads a mass). aster_apply_pending_mass, called by the tree
+// build before its first mass read, waits for them. The FP32 copies are not
+// written (the tree path does not read them). Requires c->copy_stream.
+int aster_upload_enqueue_overlapped(aster_ctx* c, int64_t n, const double* pos, const double* vel, const double* mass,
+                                    const double* acc) {
+    const size_t n4d = (size_t)n * sizeof(double4), n4f = (size_t)n * sizeof(float4);
+    ASTER_TRY(c->pm.ensure(n4d));
+    ASTER_TRY(c->vel.ensure(n4d));
+    ASTER_TRY(c->acc.ensure(n4d));
+    ASTER_TRY(c->phi.ensure(n4f));
+    ASTER_TRY(c->plo.ensure(n4f));
+    ASTER_TRY(c->vf.ensure(n4f));
+    const size_t v3 = (size_t)n * 3 * sizeof(double);
+    ASTER_TRY(c->stage.ensure(3 * v3 + (size_t)n * sizeof(double)));
+    double* sp = c->stage.as<double>();
+    double* sv = sp + 3 * n;
+    double* sm = sv + 3 * n;
+    double* sa = sm + n;
+    ASTER_CUDA(cudaMemcpyAsync(sp, pos, v3, cudaMemcpyHostToDevice, c->stream));
+    ASTER_CUDA(cudaMemcpyAsync(sv, vel, v3, cudaMemcpyHostToDevice, c->stream));
+    ASTER_CUDA(cudaMemcpyAsync(sa, acc, v3, cudaMemcpyHostToDevice, c->stream));
+    ASTER_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    ASTER_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev[3], 0));
+    ASTER_CUDA(cudaMemcpyAsync(sm, mass, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->copy_stream));
+    ASTER_CUDA(cudaEventRecord(c->ev[4], c->copy_stream));
+    k_pack_pva<<<grid_for(c, n, 256), 256, 0, c->stream>>>(n, sp, sv, sa, c->pm.as<double4>(), c->vel.as<double4>(),
+                                                           c->acc.as<double4>(), c->err_dev);
+    ASTER_CUDA(cudaGetLastError());
+    c->mass_pending = sm;
+    c->n = n;
+    c->mixed_valid = false;
+    int64_t last = n - 1;
+    while (last > 0 && mass[last] == 0.0) --last;
+    c->n_src = last + 1;
+    c->acc_valid = true;
+    c->tree.built = false;
+    return ASTER_OK;
+}
+
+int aster_apply_pending_mass(aster_ctx* c) {
+    if (!c->mass_pending) return ASTER_OK;
+    ASTER_CUDA(cudaStreamWaitEvent(c->stream, c->ev[4], 0));
+    k_set_mass<<<grid_for(c, c->n, 256), 256, 0, c->stream>>>(c->n, c->mass_pending, c->pm.as<double4>(), c->err_dev);
+    ASTER_CUDA(cudaGetLastError());
+    c->mass_pending = nullptr;
     return ASTER_OK;
 }
 

@@ -305,7 +305,9 @@ extern "C" int aster_kdk_steps_host(aster_ctx* c, const aster_params* p, int sol
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
     cudaEventRecord(c->ev[0], c->stream);
-    int st = aster_upload_enqueue(c, n, pos, vel, mass, acc);
+    // the tree path reads no mass before its build: their copy overlaps the first kick-drift and sort
+    int st = solver == ASTER_SOLVER_LBVH ? aster_upload_enqueue_overlapped(c, n, pos, vel, mass, acc)
+                                         : aster_upload_enqueue(c, n, pos, vel, mass, acc);
     const bool mixed_ap = solver == ASTER_SOLVER_ALLPAIRS && precision == ASTER_MIXED;
     int dummy[3];
     if (st == ASTER_OK && nsteps > 1) st = kdk_core(c, p, solver, precision, nsteps - 1, nullptr, nullptr, nullptr);
@@ -329,6 +331,7 @@ extern "C" int aster_kdk_steps_host(aster_ctx* c, const aster_params* p, int sol
     c->stats.ms_total = ms;
     c->acc_valid = st == ASTER_OK;
     c->tree.built = false;
+    c->mass_pending = nullptr;  // consumed by the build, or void after an error
     if (st != ASTER_OK) c->n = 0;  // the resident state is not trustworthy after a failed upload or step
     return st;
 }

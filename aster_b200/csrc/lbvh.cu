@@ -1315,6 +1315,7 @@ int run_build(aster_ctx* c, const aster_params* p) {
     }
     unsigned int* gcount = red_groups(c);  // [0] groups, [1] walk work counter, [2] bottom-up frontier
     ASTER_CUDA(cudaMemsetAsync(gcount, 0, 3 * sizeof(unsigned int), c->stream));
+    ASTER_TRY(aster_apply_pending_mass(c));  // the leaf gather below is the first reader of the masses
     const KeyT* sc = t.sorted_codes.as<KeyT>();
     if (p->compat_mode)
         k_karras<KeyT, true><<<grid, 256, 0, c->stream>>>(
