@@ -127,6 +127,8 @@ int aster_refresh_mixed(aster_ctx* ctx);        // rebuild phi/plo/vf from pm/ve
 // Host state -> device with the masses' copy overlapped (see context.cu)
 int aster_upload_enqueue_overlapped(aster_ctx* c, int64_t n, const double* pos, const double* vel, const double* mass,
                                     const double* acc);
+// velocities and accelerations -> host (one unpack, two back-to-back copies)
+int aster_download_va_enqueue(aster_ctx* c, double* vel, double* acc, cudaStream_t stream);
 // applies masses still on their way (waits for their copy); no-op otherwise
 int aster_apply_pending_mass(aster_ctx* c);
 int aster_copy_acc_out(aster_ctx* ctx, double* acc_out);

@@ -200,6 +200,16 @@ __global__ void k_refresh_mixed(int64_t n, const double4* __restrict__ pm, const
     }
 }
 
+// velocities and accelerations to AoS staging in one pass
+__global__ void k_unpack_va(int64_t n, const double4* __restrict__ v4, const double4* __restrict__ a4,
+                            double* __restrict__ dv, double* __restrict__ da) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double4 v = v4[i], a = a4[i];
+        dv[3 * i] = v.x; dv[3 * i + 1] = v.y; dv[3 * i + 2] = v.z;
+        da[3 * i] = a.x; da[3 * i + 1] = a.y; da[3 * i + 2] = a.z;
+    }
+}
+
 __global__ void k_unpack3(int64_t n, const double4* __restrict__ src, double* __restrict__ dst) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double4 v = src[i];
@@ -379,6 +389,20 @@ int aster_download_enqueue(aster_ctx* c, int which, double* host, cudaStream_t s
     k_unpack3<<<grid_for(c, n, 256), 256, 0, stream>>>(n, srcs[which]->as<double4>(), st);
     ASTER_CUDA(cudaGetLastError());
     ASTER_CUDA(cudaMemcpyAsync(host, st, v3, cudaMemcpyDeviceToHost, stream));
+    return ASTER_OK;
+}
+
+// Velocities and accelerations -> host: one unpack kernel, then the two copies
+// back to back (no kernel between the transfers).
+int aster_download_va_enqueue(aster_ctx* c, double* vel, double* acc, cudaStream_t stream) {
+    const int64_t n = c->n;
+    const size_t v3 = (size_t)n * 3 * sizeof(double);
+    double* sv = c->stage.as<double>() + 3 * n;
+    double* sa = sv + 3 * n;
+    k_unpack_va<<<grid_for(c, n, 256), 256, 0, stream>>>(n, c->vel.as<double4>(), c->acc.as<double4>(), sv, sa);
+    ASTER_CUDA(cudaGetLastError());
+    ASTER_CUDA(cudaMemcpyAsync(vel, sv, v3, cudaMemcpyDeviceToHost, stream));
+    ASTER_CUDA(cudaMemcpyAsync(acc, sa, v3, cudaMemcpyDeviceToHost, stream));
     return ASTER_OK;
 }
 

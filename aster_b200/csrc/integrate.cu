@@ -319,8 +319,7 @@ extern "C" int aster_kdk_steps_host(aster_ctx* c, const aster_params* p, int sol
         st = aster_download_enqueue(c, 0, pos, c->copy_stream);
     }
     if (st == ASTER_OK) st = force_eval(c, p, solver, precision, true, true, nullptr, nullptr, nullptr, dummy);
-    if (st == ASTER_OK) st = aster_download_enqueue(c, 1, vel, c->stream);
-    if (st == ASTER_OK) st = aster_download_enqueue(c, 2, acc, c->stream);
+    if (st == ASTER_OK) st = aster_download_va_enqueue(c, vel, acc, c->stream);
     cudaEventRecord(c->ev[1], c->stream);
     const cudaError_t ce = cudaStreamSynchronize(c->copy_stream);
     const int fin = aster_finish(c);
