@@ -6,6 +6,8 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <utility>
+#include <vector>
 
 #include "../../include/aster_cuda.h"
 
@@ -109,6 +111,9 @@ struct aster_ctx {
     // masses still on their way (overlapped upload): staging copy on the
     // device, applied to pm[].w before the tree build reads them
     const double* mass_pending = nullptr;
+    // executable graphs of the last call's repeated steps; destroyed by the
+    // next call's aster_begin (its work has finished by then) or at destroy
+    std::vector<std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
 };
 
 // Layout of ctx->red (4 KB of small device scalars).

@@ -13,6 +13,7 @@
 #include "aster_internal.cuh"
 
 static thread_local char g_last_error[256] = "";
+static void release_graphs(aster_ctx* c);
 
 int aster_cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
     snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
@@ -113,6 +114,7 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
     if (!c) return ASTER_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    release_graphs(c);
     DevBuf* bufs[] = {&c->pm, &c->vel, &c->acc, &c->phi, &c->plo, &c->vf, &c->scratch, &c->targets,
                       &c->stage, &c->red, &c->wh, &c->rec,
                       &c->tree.codes, &c->tree.codes_alt, &c->tree.sorted_codes, &c->tree.perm,
@@ -136,8 +138,17 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
     return ASTER_OK;
 }
 
+static void release_graphs(aster_ctx* c) {
+    for (auto& g : c->graphs) {
+        if (g.second) cudaGraphExecDestroy(g.second);
+        if (g.first) cudaGraphDestroy(g.first);
+    }
+    c->graphs.clear();
+}
+
 int aster_begin(aster_ctx* c) {
     ASTER_CUDA(cudaSetDevice(c->device));
+    release_graphs(c);  // the previous call synchronised before returning
     ASTER_CUDA(cudaMemsetAsync(c->err_dev, 0, 2 * sizeof(int), c->stream));
     return ASTER_OK;
 }

@@ -218,6 +218,46 @@ static int force_eval(aster_ctx* c, const aster_params* p, int solver, int preci
     return ASTER_OK;
 }
 
+// Enqueues step() n times. With graph set, the first step runs as usual
+// (allocating whatever a step needs) and the second is captured into a CUDA
+// graph that is launched for the remaining n - 1: one launch a step instead of
+// one per kernel, for steps of a few short kernels whose launch gaps rival
+// the kernels. The captured step's host-side statistics are scaled to n. Falls
+// back to plain launches when the stream cannot be captured (the legacy
+// default stream).
+template <class F>
+static int repeat_steps(aster_ctx* c, int n, bool graph, F step) {
+    if (n <= 0) return ASTER_OK;
+    ASTER_TRY(step());
+    if (n == 1) return ASTER_OK;
+    if (graph) {
+        const double inter0 = c->stats.interactions;
+        const int64_t kern0 = c->stats.kernels;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const int st = step();
+            const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            cudaGraphExec_t ge = nullptr;
+            if (st == ASTER_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess) {
+                c->graphs.push_back({g, ge});
+                const double di = c->stats.interactions - inter0;
+                const int64_t dk = c->stats.kernels - kern0;
+                for (int s = 1; s < n; ++s) ASTER_CUDA(cudaGraphLaunch(ge, c->stream));
+                c->stats.interactions += di * (n - 2);
+                c->stats.kernels += dk * (n - 2);
+                return ASTER_OK;
+            }
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();  // the failed capture's error
+            if (st != ASTER_OK) return st;
+        } else {
+            cudaGetLastError();
+        }
+    }
+    for (int s = 1; s < n; ++s) ASTER_TRY(step());
+    return ASTER_OK;
+}
+
 // Enqueues nsteps KDK steps (no synchronisation); marks/tm optional.
 static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps, PhaseTimer* tm,
                     int (*marks)[3], int* nm) {
@@ -228,11 +268,13 @@ static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precisi
         ASTER_TRY(force_eval(c, p, solver, precision, false, false, tm, nullptr, nullptr, tm ? marks[*nm] : dummy));
         if (tm) ++*nm;
     }
-    for (int s = 0; s < nsteps; ++s) {
+    // the all-pairs step (kick-drift, force, closing kick) replays as a graph
+    ASTER_TRY(repeat_steps(c, nsteps, solver == ASTER_SOLVER_ALLPAIRS && !tm, [&]() -> int {
         ASTER_TRY(aster_kick_drift_launch(c, p, solver == ASTER_SOLVER_LBVH, mixed_ap));
         ASTER_TRY(force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, tm ? marks[*nm] : dummy));
         if (tm) ++*nm;
-    }
+        return ASTER_OK;
+    }));
     c->acc_valid = true;  // a(x) of the final positions (valid once the work completes without error)
     c->tree.built = false;
     return ASTER_OK;
@@ -256,8 +298,8 @@ extern "C" int aster_kdk_steps(aster_ctx* c, const aster_params* p, int solver, 
     ASTER_TRY(kdk_check(c, p, solver, precision, nsteps));
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
-    // phase timing only when the event budget covers every step
-    PhaseTimer* tm = (nsteps + 1) * 3 <= 2 * PhaseTimer::kMax ? new PhaseTimer() : nullptr;
+    // phase timing (tree path only: build and walk) when the event budget covers every step
+    PhaseTimer* tm = solver == ASTER_SOLVER_LBVH && (nsteps + 1) * 3 <= 2 * PhaseTimer::kMax ? new PhaseTimer() : nullptr;
     int marks[3 * (PhaseTimer::kMax / 3 + 2)][3];
     int nm = 0;
     ASTER_TRY(c->red.ensure(4096));
@@ -389,18 +431,24 @@ static int saba_core(aster_ctx* c, const aster_params* p, int solver, int precis
     };
     const double dt = p->dt;
     if (order == 1 && mixed_ap) ASTER_TRY(aster_refresh_mixed(c));
-    for (int s = 0; s < nsteps; ++s) {
+    if (order == 1 && nsteps > 0) {
+        ASTER_TRY(force(false));  // the first Euler step computes its own box
+        ASTER_TRY(aster_kick_drift_coef(c, dt, dt, true, lbvh, mixed_ap));
+        --nsteps;
+    }
+    // the all-pairs step replays as a graph
+    ASTER_TRY(repeat_steps(c, nsteps, !lbvh && !tm, [&]() -> int {
         if (order == 1) {
-            ASTER_TRY(force(s > 0));
-            ASTER_TRY(aster_kick_drift_coef(c, dt, dt, true, lbvh, mixed_ap));
-            continue;
+            ASTER_TRY(force(true));
+            return aster_kick_drift_coef(c, dt, dt, true, lbvh, mixed_ap);
         }
         ASTER_TRY(aster_kick_drift_coef(c, 0.0, cc[0] * dt, false, lbvh, mixed_ap));
         for (int k = 0; k < nk; ++k) {
             ASTER_TRY(force(true));
             ASTER_TRY(aster_kick_drift_coef(c, dd[k] * dt, cc[k + 1] * dt, true, lbvh, mixed_ap));
         }
-    }
+        return ASTER_OK;
+    }));
     c->acc_valid = false;  // the last drift moved the bodies after the last force evaluation
     c->tree.built = false;
     return ASTER_OK;
@@ -432,7 +480,7 @@ extern "C" int aster_saba_steps(aster_ctx* c, const aster_params* p, int solver,
     c->stats = aster_stats{};
     const bool lbvh = solver == ASTER_SOLVER_LBVH;
     const int nk = order > 1 ? order : 1;
-    PhaseTimer* tm = (int64_t)(nsteps * nk + 1) * 3 <= 2 * PhaseTimer::kMax ? new PhaseTimer() : nullptr;
+    PhaseTimer* tm = lbvh && (int64_t)(nsteps * nk + 1) * 3 <= 2 * PhaseTimer::kMax ? new PhaseTimer() : nullptr;
     std::vector<std::array<int, 3>> marks;
     ASTER_TRY(c->red.ensure(4096));
     unsigned long long* inter = red_inter(c);
