@@ -189,9 +189,18 @@ struct PhaseTimer {
     ~PhaseTimer() {
         for (int i = 0; i < used; ++i) cudaEventDestroy(ev[i]);
     }
+    int fresh() {  // a new event, not recorded; its index, -1 if out of slots
+        if (used >= 2 * kMax || cudaEventCreate(&ev[used]) != cudaSuccess) return -1;
+        return used++;
+    }
     int mark(cudaStream_t s) {  // returns the event index, -1 if out of slots
         if (used >= 2 * kMax || cudaEventCreate(&ev[used]) != cudaSuccess) return -1;
-        cudaEventRecord(ev[used], s);
+        // under stream capture a plain record only orders streams; External
+        // makes it an event-record node of the graph
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(s, &cs);
+        if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(ev[used], s, cudaEventRecordExternal);
+        else cudaEventRecord(ev[used], s);
         return used++;
     }
     double span(int a, int b) const {
@@ -221,14 +230,17 @@ static int force_eval(aster_ctx* c, const aster_params* p, int solver, int preci
 // Enqueues step() n times. With graph set, the first step runs as usual
 // (allocating whatever a step needs) and the second is captured into a CUDA
 // graph that is launched for the remaining n - 1: one launch a step instead of
-// one per kernel, for steps of a few short kernels whose launch gaps rival
-// the kernels. The captured step's host-side statistics are scaled to n. Falls
-// back to plain launches when the stream cannot be captured (the legacy
-// default stream).
-template <class F>
-static int repeat_steps(aster_ctx* c, int n, bool graph, F step) {
+// one per kernel, which removes the gaps between a step's kernels. The
+// captured step's host-side statistics are scaled to n. done() follows every
+// step that ran as plain launches; replay(g, ge) precedes every graph launch
+// (the timed path re-points the graph's event-record nodes there, so every
+// step keeps its own timestamps). Falls back to plain launches when the
+// stream cannot be captured (the legacy default stream).
+template <class F, class D, class R>
+static int repeat_steps(aster_ctx* c, int n, bool graph, F step, D done, R replay) {
     if (n <= 0) return ASTER_OK;
     ASTER_TRY(step());
+    ASTER_TRY(done());
     if (n == 1) return ASTER_OK;
     if (graph) {
         const double inter0 = c->stats.interactions;
@@ -242,7 +254,10 @@ static int repeat_steps(aster_ctx* c, int n, bool graph, F step) {
                 c->graphs.push_back({g, ge});
                 const double di = c->stats.interactions - inter0;
                 const int64_t dk = c->stats.kernels - kern0;
-                for (int s = 1; s < n; ++s) ASTER_CUDA(cudaGraphLaunch(ge, c->stream));
+                for (int s = 1; s < n; ++s) {
+                    ASTER_TRY(replay(g, ge));
+                    ASTER_CUDA(cudaGraphLaunch(ge, c->stream));
+                }
                 c->stats.interactions += di * (n - 2);
                 c->stats.kernels += dk * (n - 2);
                 return ASTER_OK;
@@ -254,9 +269,15 @@ static int repeat_steps(aster_ctx* c, int n, bool graph, F step) {
             cudaGetLastError();
         }
     }
-    for (int s = 1; s < n; ++s) ASTER_TRY(step());
+    for (int s = 1; s < n; ++s) {
+        ASTER_TRY(step());
+        ASTER_TRY(done());
+    }
     return ASTER_OK;
 }
+
+static int no_op() { return ASTER_OK; }
+static int no_replay(cudaGraph_t, cudaGraphExec_t) { return ASTER_OK; }
 
 // Enqueues nsteps KDK steps (no synchronisation); marks/tm optional.
 static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps, PhaseTimer* tm,
@@ -268,13 +289,60 @@ static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precisi
         ASTER_TRY(force_eval(c, p, solver, precision, false, false, tm, nullptr, nullptr, tm ? marks[*nm] : dummy));
         if (tm) ++*nm;
     }
-    // the all-pairs step (kick-drift, force, closing kick) replays as a graph
-    ASTER_TRY(repeat_steps(c, nsteps, solver == ASTER_SOLVER_ALLPAIRS && !tm, [&]() -> int {
+    // the step (kick-drift, force, closing kick) replays as a graph; with phase
+    // timing, its three marks are event-record nodes re-pointed before each launch
+    int last[3] = {-1, -1, -1};
+    cudaGraphNode_t evnode[3] = {nullptr, nullptr, nullptr};
+    bool found = false;
+    auto step = [&]() -> int {
         ASTER_TRY(aster_kick_drift_launch(c, p, solver == ASTER_SOLVER_LBVH, mixed_ap));
-        ASTER_TRY(force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, tm ? marks[*nm] : dummy));
-        if (tm) ++*nm;
+        return force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, last);
+    };
+    auto done = [&]() -> int {
+        if (tm) {
+            for (int k = 0; k < 3; ++k) marks[*nm][k] = last[k];
+            ++*nm;
+        }
         return ASTER_OK;
-    }));
+    };
+    auto replay = [&](cudaGraph_t g, cudaGraphExec_t ge) -> int {
+        if (!tm) return ASTER_OK;
+        if (!found) {  // the captured marks' event-record nodes (last[] names the captured events)
+            size_t nn = 0;
+            ASTER_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+            std::vector<cudaGraphNode_t> nodes(nn);
+            ASTER_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+            for (cudaGraphNode_t nd : nodes) {
+                cudaGraphNodeType ty;
+                ASTER_CUDA(cudaGraphNodeGetType(nd, &ty));
+                if (ty != cudaGraphNodeTypeEventRecord) continue;
+                cudaEvent_t e = nullptr;
+                ASTER_CUDA(cudaGraphEventRecordNodeGetEvent(nd, &e));
+                for (int k = 0; k < 3; ++k)
+                    if (last[k] >= 0 && tm->ev[last[k]] == e) evnode[k] = nd;
+            }
+            found = true;
+        }
+        int m3[3] = {-1, -1, -1};
+        for (int k = 0; k < 3; ++k) {
+            if (!evnode[k]) continue;
+            // a mark that names the same event as an earlier one (all-pairs: no build span) shares it
+            int same = -1;
+            for (int q = 0; q < k; ++q)
+                if (evnode[q] == evnode[k]) same = q;
+            if (same >= 0) {
+                m3[k] = m3[same];
+                continue;
+            }
+            m3[k] = tm->fresh();
+            if (m3[k] < 0) return ASTER_OK;  // out of event slots: the step runs untimed
+            ASTER_CUDA(cudaGraphExecEventRecordNodeSetEvent(ge, evnode[k], tm->ev[m3[k]]));
+        }
+        for (int k = 0; k < 3; ++k) marks[*nm][k] = m3[k];
+        ++*nm;
+        return ASTER_OK;
+    };
+    ASTER_TRY(repeat_steps(c, nsteps, true, step, done, replay));
     c->acc_valid = true;  // a(x) of the final positions (valid once the work completes without error)
     c->tree.built = false;
     return ASTER_OK;
@@ -448,7 +516,7 @@ static int saba_core(aster_ctx* c, const aster_params* p, int solver, int precis
             ASTER_TRY(aster_kick_drift_coef(c, dd[k] * dt, cc[k + 1] * dt, true, lbvh, mixed_ap));
         }
         return ASTER_OK;
-    }));
+    }, no_op, no_replay));
     c->acc_valid = false;  // the last drift moved the bodies after the last force evaluation
     c->tree.built = false;
     return ASTER_OK;
