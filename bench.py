@@ -44,9 +44,9 @@ SEED_C2 = 1002
 N_C3, EPS_C3, SEED_C3 = 262144, 0.002, 1003
 FLOP_PER_PAIR = 20  # Newtonian pair, Nyland et al. GPU Gems 3 ch. 31 convention
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_walk launch captured with
-# ncu at N = 2^19 (68.7 MB, profiles/k_walk_c2_plummer524288.md), scaled by the
-# number of bodies to N = 2^20 (the walk reads each tree node about once).
-WALK_TRAFFIC_BYTES = 68.7e6 * 2
+# ncu at N = 2^19 (74.04 + 4.71 MB, profiles/k_walk_c2_plummer524288.md), scaled
+# by the number of bodies to N = 2^20 (the walk reads each tree node about once).
+WALK_TRAFFIC_BYTES = 78.75e6 * 2
 
 
 def log(*a):
