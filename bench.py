@@ -43,10 +43,37 @@ THETA, EPS, DT = 0.5, 0.005, 5e-4
 SEED_C2 = 1002
 N_C3, EPS_C3, SEED_C3 = 262144, 0.002, 1003
 FLOP_PER_PAIR = 20  # Newtonian pair, Nyland et al. GPU Gems 3 ch. 31 convention
+# 1PN pair term (compute_gravitational with get_pn1): the Newtonian 20 + unit
+# vector 3, v_i - v_j 3, v_i.v_j 5, n.v_i 5, n.v_j 5, bracket A 13, bracket B 3,
+# prefactor 2, the three components 12 = 71 FLOP
+FLOP_PER_PN1_PAIR = 71
+# Tree build, algorithmic bytes per body: Morton 32 (read the position 24,
+# write code and index 8) + sort 16 (one read and one write of the 8-byte
+# key/value, whatever the pass count) + Karras 24 (read the code, write links
+# and ranges) + leaf gather 48 (read position and mass 32, write 16) +
+# bottom-up 120 (per internal node: read two 40-byte child records, write 40)
+BUILD_BYTES_PER_BODY = 240
+
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_walk launch captured with
 # ncu at N = 2^19 (74.04 + 4.71 MB, profiles/k_walk_c2_plummer524288.md), scaled
 # by the number of bodies to N = 2^20 (the walk reads each tree node about once).
 WALK_TRAFFIC_BYTES = 78.75e6 * 2
+
+
+def fp_peaks(f_mhz: float):
+    """FP32 and FP64 pipe peaks in TFLOP/s (an FMA counted as 2) at SM clock f_mhz:
+    148 SMs x 128 FP32 lanes, x 64 FP64 lanes."""
+    return 148 * 128 * 2 * f_mhz * 1e6 / 1e12, 148 * 64 * 2 * f_mhz * 1e6 / 1e12
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def log(*a):
@@ -199,6 +226,7 @@ def cpu_baseline_c2(pos, vel, m, steps: int = 1):
     ref.leapfrog(steps)
     dt = time.perf_counter() - t0
     return {"value": steps / dt, "unit": "steps/s", "cores": ref.threads(), "kind": "reference",
+            "cpu_model": cpu_model(),
             "sample": f"{steps} update_leapfrog step(s) of Barnes_Hut at N={len(m)} (full workload), "
                       f"reference sources compiled unmodified with a std::thread TBB stand-in"}
 
@@ -229,6 +257,7 @@ def run_reference(args):
         "config": {"workload": "C2 LBVH Barnes-Hut KDK step, Plummer N=1048576 lognormal masses, theta=0.5, "
                                "eps=0.005, dt=5e-4", "n": N_C2},
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": ref.threads(), "kind": "reference",
+                         "cpu_model": cpu_model(),
                          "sample": f"full N={N_C2} update_leapfrog steps with Barnes_Hut (2 tree builds + walks "
                                    f"each), reference sources compiled unmodified, std::thread TBB stand-in"},
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -291,6 +320,8 @@ def run_ours(args):
         sms = 148
         fp32_peak = sms * 128 * 2 * f_mhz * 1e6 / 1e12
         achieved = inter_per_step * FLOP_PER_PAIR / (walk_ms / 1e3) / 1e12
+        build_gbs = BUILD_BYTES_PER_BODY * args.n / (build_ms / 1e3) / 1e9 if build_ms > 0 else None
+        args.sm_mhz = f_mhz
         extra = secondary(ctx, args) if not args.quick else {}
         line = {
             "metric": "LBVH-BH steps/s @N=1M", "value": value, "unit": "steps/s", "n_gpus": world,
@@ -312,6 +343,12 @@ def run_ours(args):
                                            if clk.get("sm_mhz") else f"max SM clock {f_mhz:.0f} MHz (no clock samples)")
                                         + " (no FP32 figure in MEASURED_PEAKS.json)",
                          "flop_per_interaction": FLOP_PER_PAIR},
+            "build_roofline": None if build_gbs is None else {
+                "bound": "hbm", "kernels": "tree build (Morton, sort, Karras, bottom-up, node records)",
+                "achieved": build_gbs, "peak": peaks.get("hbm_gbs", 6650.0), "unit": "GB/s",
+                "frac": build_gbs / peaks.get("hbm_gbs", 6650.0), "bytes_per_body": BUILD_BYTES_PER_BODY,
+                "peak_source": f"{src} copy bandwidth (MEASURED_PEAKS.json)" if src == "measured"
+                else "fallback copy bandwidth"},
             "e2e": e2e,
             "gpu_launches": kernels,
             "clocks": clk,
@@ -419,10 +456,15 @@ def secondary(ctx, args):
             times.append(ctx.stats()["ms_force"])
         t = min(times)
         res[name] = {"ms_per_eval": t, "pairs_per_s": N_C3 * (N_C3 - 1) / (t / 1e3)}
+    f32p, f64p = fp_peaks(getattr(args, "sm_mhz", 1965.0))
+    for name, peak in (("fp64", f64p), ("mixed", f32p)):
+        tf = res[name]["pairs_per_s"] * FLOP_PER_PAIR / 1e12
+        res[name]["roofline"] = {"bound": "fp64" if name == "fp64" else "fp32", "achieved": tf, "peak": peak,
+                                 "unit": "TFLOP/s", "frac": tf / peak}
     res["mixed_vs_fp64_rel_l2"] = float(np.linalg.norm(accs["mixed"] - accs["fp64"]) / np.linalg.norm(accs["fp64"]))
     res["workload"] = "C3 cold exponential disk N=262144 (+central mass 0.1), eps=0.002, one force evaluation"
     out["allpairs"] = res
-    out["ensemble"] = ensemble_c4(ctx)
+    out["ensemble"] = ensemble_c4(ctx, sm_mhz=getattr(args, "sm_mhz", 1965.0))
     out["adjoint"] = adjoint_c5(ctx)
     out["c1"] = kdk_c1(ctx)
     out["next_rows"] = next_rows(ctx)
@@ -515,6 +557,17 @@ def kdk_c1(ctx):
         e1, mom = ctx.energy(p)
         out[name] = {"ms_per_step": ms / 100, "pairs_per_s": 100 * 4096 * 4095 / (ms / 1e3),
                      "energy_drift": abs(e1 - e0) / abs(e0), "momentum_abs": float(np.abs(mom).max())}
+    try:
+        from oracle.oracle import Ref
+        if Ref.available():  # the reference's Parallelized + update_leapfrog (2 force evaluations a step)
+            ref = Ref().setup(pos, vel, m, G=1.0, dt=1e-3, eps2=1e-4)
+            t0 = time.perf_counter()
+            ref.leapfrog(10)
+            el = time.perf_counter() - t0
+            out["cpu_reference"] = {"steps_per_s": 10 / el, "cores": ref.threads(), "cpu_model": cpu_model(),
+                                    "sample": "10 of the 100 steps, reference sources compiled unmodified"}
+    except Exception as exc:  # the CPU figure is reported beside the GPU one, never instead of it
+        out["cpu_reference"] = {"unavailable": str(exc)[:200]}
     return out
 
 
@@ -540,7 +593,7 @@ def c3_drift(ctx, nsteps: int = 1000):
     return out
 
 
-def ensemble_c4(ctx, nsteps: int = 10_000):
+def ensemble_c4(ctx, nsteps: int = 10_000, sm_mhz: float = 1965.0):
     """C4: 16384 hierarchical systems (n in [3, 64]), pairwise 1PN (c = 100),
     Yoshida-4, dt = 1e-4, nsteps in one persistent graph-captured launch with
     the autotuned launch shape; FP32 pair terms, FP64 state."""
@@ -557,9 +610,13 @@ def ensemble_c4(ctx, nsteps: int = 10_000):
     st = ctx.stats()
     e1 = ctx.ensemble_energy(p)
     de = np.abs((e1 - e0) / e0)
+    rate = st["interactions"] / (st["ms_total"] / 1e3)
+    tf, f32p = rate * FLOP_PER_PN1_PAIR / 1e12, fp_peaks(sm_mhz)[0]
     return {"workload": "C4 16384 systems n~U[3,64], 1PN c=100, Yoshida-4, dt=1e-4, one graph-captured launch",
             "steps": nsteps, "ms": st["ms_total"], "steps_per_s": nsteps / (st["ms_total"] / 1e3),
-            "pair_terms_per_s": st["interactions"] / (st["ms_total"] / 1e3), "config": cfg,
+            "pair_terms_per_s": rate, "config": cfg,
+            "roofline": {"bound": "fp32", "achieved": tf, "peak": f32p, "unit": "TFLOP/s", "frac": tf / f32p,
+                         "flop_per_pair": FLOP_PER_PN1_PAIR},
             "energy_drift_median": float(np.median(de)), "energy_drift_p90": float(np.percentile(de, 90))}
 
 
