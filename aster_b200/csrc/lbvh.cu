@@ -59,9 +59,10 @@ constexpr int WALK_STACK = 1024;   // nodes per warp
 constexpr int GROUP_MAX = 64;      // leaves per walk group (1 or 2 per lane)
 // Interaction list: evaluated (and its FP32 partial sums folded into the
 // compensated accumulators) every WALK_FLUSH entries; capacity = flush - 1 +
-// the 64 entries one round can append.
-constexpr int WALK_FLUSH_MIXED = 64, WALK_FLUSH_FP64 = 32;
-constexpr int WALK_LIST_MIXED = 128, WALK_LIST_FP64 = 96;
+// the 64 entries one round can append. The post-Newtonian mixed walk, whose
+// entries also carry a velocity, flushes every WALK_FLUSH_PN.
+constexpr int WALK_FLUSH_MIXED = 128, WALK_FLUSH_FP64 = 32, WALK_FLUSH_PN = 64;
+constexpr int WALK_LIST_MIXED = 192, WALK_LIST_FP64 = 96, WALK_LIST_PN = 128;
 
 // ----------------------------------------------------------------- box
 __device__ __forceinline__ double warp_max_d(double v) {
@@ -722,7 +723,7 @@ struct WalkShared {
 // (vx, vy, vz, |v|^2), FP32 for the mixed walk and FP64 for the FP64 walk.
 template <bool MIXED>
 struct WalkSharedPn : WalkShared<MIXED> {
-    float4 lvf[WALK_WARPS][MIXED ? WALK_LIST_MIXED : 1];
+    float4 lvf[WALK_WARPS][MIXED ? WALK_LIST_PN : 1];
     double4 lvd[WALK_WARPS][MIXED ? 1 : WALK_LIST_FP64];
 };
 
@@ -1116,7 +1117,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK
             }
             lc += __popc(mAL) + __popc(mAR);
             __syncwarp();
-            constexpr int FL = MIXED ? WALK_FLUSH_MIXED : WALK_FLUSH_FP64;
+            constexpr int FL = MIXED ? (PNL ? WALK_FLUSH_PN : WALK_FLUSH_MIXED) : WALK_FLUSH_FP64;
             while (lc >= FL) {
                 evaluate(FL);
                 __syncwarp();
