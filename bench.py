@@ -55,9 +55,9 @@ FLOP_PER_PN1_PAIR = 71
 BUILD_BYTES_PER_BODY = 240
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_walk launch captured with
-# ncu at N = 2^19 (74.04 + 4.71 MB, profiles/k_walk_c2_plummer524288.md), scaled
+# ncu at N = 2^19 (74.04 + 4.59 MB, profiles/k_walk_c2_plummer524288.md), scaled
 # by the number of bodies to N = 2^20 (the walk reads each tree node about once).
-WALK_TRAFFIC_BYTES = 78.75e6 * 2
+WALK_TRAFFIC_BYTES = 78.63e6 * 2
 
 
 def fp_peaks(f_mhz: float):
@@ -327,8 +327,10 @@ def run_ours(args):
             "metric": "LBVH-BH steps/s @N=1M", "value": value, "unit": "steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 pairs / f64 state", "data": "synthetic",
-            "config": {"workload": "C2 LBVH Barnes-Hut KDK step, Plummer N=1048576 lognormal(0,0.5) masses, "
-                                   "30-bit Morton on the bounding cube, theta=0.5, eps=0.005, dt=5e-4, mixed",
+            "config": {"workload": ("C2 LBVH Barnes-Hut KDK step, Plummer N=1048576" if args.n == N_C2 else
+                                    f"LBVH Barnes-Hut KDK step (C2 at reduced size), Plummer N={args.n}")
+                                   + " lognormal(0,0.5) masses, 30-bit Morton on the bounding cube, theta=0.5, "
+                                     "eps=0.005, dt=5e-4, mixed",
                        "n": args.n, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "per-step working set > L2: the tree rebuild writes ~0.4 GB every step"},
             "phases_ms": {"build": build_ms, "walk": walk_ms, "other": ms / args.steps - build_ms - walk_ms},
