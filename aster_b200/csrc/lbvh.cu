@@ -338,6 +338,26 @@ __device__ __forceinline__ void leaf_trav(const double4 c, float4& h, float4& l)
     l.w = 0.f;
 }
 
+// The child record of an internal node: the traversal data of both children
+// in one contiguous 64 bytes, so opening a node costs one load, each field as
+// a (left, right) pair so that the walk's paired FP32 opening test and
+// list-entry arithmetic read aligned register pairs:
+// (xL xR yL yR) (zL zR mL mR) (lxL lxR lyL lyR) (lzL lzR rcrit2L rcrit2R).
+// Child ids below n are leaves (their boxes are not needed).
+__device__ __forceinline__ void put_child_record(float4* __restrict__ dst, int64_t n, double theta, int32_t L,
+                                                 const double4 cL, const float4 loL, const float4 hiL, int32_t R,
+                                                 const double4 cR, const float4 loR, const float4 hiR) {
+    float4 hL, lL, hR, lR;
+    if (L < n) leaf_trav(cL, hL, lL);
+    else node_trav(cL, loL, hiL, theta, hL, lL);
+    if (R < n) leaf_trav(cR, hR, lR);
+    else node_trav(cR, loR, hiR, theta, hR, lR);
+    dst[0] = make_float4(hL.x, hR.x, hL.y, hR.y);
+    dst[1] = make_float4(hL.z, hR.z, hL.w, hR.w);
+    dst[2] = make_float4(lL.x, lR.x, lL.y, lR.y);
+    dst[3] = make_float4(lL.z, lR.z, lL.w, lR.w);
+}
+
 // -------------------------------------------------------------- karras
 template <class KeyT, bool COMPAT>
 __device__ __forceinline__ int kdelta(const KeyT* __restrict__ codes, const int32_t* __restrict__ perm,
@@ -351,19 +371,31 @@ __device__ __forceinline__ int kdelta(const KeyT* __restrict__ codes, const int3
     return sizeof(KeyT) == 8 ? __clzll((long long)(a ^ b)) : __clz((int)(uint32_t)(a ^ b));
 }
 
+// Walk groups: a node whose subtree holds at most GROUP_MAX leaves while its
+// parent's holds more (the root when n <= GROUP_MAX). Its leaves are a
+// contiguous sorted run sharing a Morton prefix, so the group is spatially
+// compact (a fixed run of consecutive sorted bodies is not: it can straddle a
+// Morton jump and span the whole system). Listed here as (first leaf, size):
+// internal node n + i knows its own range and both children's, and thread i
+// lists the groups among its children, so groups come roughly in sorted-leaf
+// order, which keeps consecutive walk groups close in space.
 template <class KeyT, bool COMPAT>
 __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restrict__ codes, const int32_t* __restrict__ perm,
                                                 const double4* __restrict__ pm, int32_t* __restrict__ parent,
                                                 int32_t* __restrict__ sib, int32_t* __restrict__ rlo, int32_t* __restrict__ rhi,
                                                 int2* __restrict__ child, uint32_t* __restrict__ counters,
-                                                double4* __restrict__ node_cm) {
+                                                double4* __restrict__ node_cm, int2* __restrict__ groups,
+                                                unsigned int* __restrict__ ngroups) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         // leaf i: gather body perm[i]
         {
             node_cm[i] = pm[perm[i]];
             rlo[i] = (int32_t)i;
             rhi[i] = (int32_t)i;
-            if (n == 1) parent[0] = -1;
+            if (n == 1) {
+                parent[0] = -1;
+                groups[atomicAdd(ngroups, 1u)] = make_int2(0, 1);
+            }
         }
         if (i == n - 1) {
             parent[n] = -1;  // root (n >= 2) or unused slot
@@ -399,6 +431,13 @@ __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restric
         rlo[node] = (int32_t)lo;
         rhi[node] = (int32_t)hi;
         counters[i] = 0u;
+        if (hi - lo + 1 > GROUP_MAX) {
+            const int64_t szL = gamma - lo + 1, szR = hi - gamma;
+            if (szL <= GROUP_MAX) groups[atomicAdd(ngroups, 1u)] = make_int2((int32_t)lo, (int32_t)szL);
+            if (szR <= GROUP_MAX) groups[atomicAdd(ngroups, 1u)] = make_int2((int32_t)(gamma + 1), (int32_t)szR);
+        } else if (i == 0) {  // the root holds at most GROUP_MAX leaves
+            groups[atomicAdd(ngroups, 1u)] = make_int2(0, (int32_t)n);
+        }
     }
 }
 
@@ -448,10 +487,11 @@ __device__ __forceinline__ void bu_merge(const double4 cl, const double4 cr, con
     hi = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
 }
 
-__global__ void __launch_bounds__(BU_LEAVES) k_bottom_up_local(
+__global__ void __launch_bounds__(BU_LEAVES, 4) k_bottom_up_local(
     int64_t n, const int32_t* __restrict__ parent, const int32_t* __restrict__ sib, const int32_t* __restrict__ rlo,
     const int32_t* __restrict__ rhi, double4* __restrict__ node_cm, float4* __restrict__ bmin,
-    float4* __restrict__ bmax, int32_t* __restrict__ front, unsigned int* __restrict__ nfront, int* __restrict__ err) {
+    float4* __restrict__ bmax, int32_t* __restrict__ front, unsigned int* __restrict__ nfront, int* __restrict__ err,
+    double theta, const int2* __restrict__ child, float4* __restrict__ crec) {
     // [0][j]: leaf B0 + j; [1][j]: internal node n + B0 + j (Karras numbering:
     // an internal node inside the block has its index inside the block too)
     __shared__ double4 s_cm[2][BU_LEAVES];
@@ -533,11 +573,19 @@ __global__ void __launch_bounds__(BU_LEAVES) k_bottom_up_local(
     if (j == 0) s_fbase = s_nf ? atomicAdd(nfront, s_nf) : 0u;
     // the block's completed internal nodes (both children arrived) go to global
     // memory in one coalesced pass, not from inside the climb, so that the
-    // block-scope fences there wait for shared-memory stores only
+    // block-scope fences there wait for shared-memory stores only; with them
+    // their child records, from the children's data still in shared memory
+    // (a completed node's children lie in the block: leaves B0..B1, internal
+    // nodes n + B0..B1)
     if (k < n - 1 && s_cnt[j] == 2u) {
         node_cm[n + k] = s_cm[1][j];
         bmin[n + k] = s_lo[1][j];
         bmax[n + k] = s_hi[1][j];
+        const int2 ch = child[n + k];
+        const int sL = (int)(ch.x < n ? ch.x - B0 : ch.x - n - B0), sR = (int)(ch.y < n ? ch.y - B0 : ch.y - n - B0);
+        const int tL = ch.x < n ? 0 : 1, tR = ch.y < n ? 0 : 1;
+        put_child_record(crec + 4 * k, n, theta, ch.x, s_cm[tL][sL], s_lo[tL][sL], s_hi[tL][sL], ch.y, s_cm[tR][sR],
+                         s_lo[tR][sR], s_hi[tR][sR]);
     }
     __syncthreads();
     if ((unsigned)j < s_nf) front[s_fbase + j] = s_front[j];
@@ -658,52 +706,21 @@ __global__ void __launch_bounds__(256) k_node_vel(int64_t n, const int32_t* __re
     }
 }
 
-// Groups: a node whose subtree holds at most GROUP_MAX leaves while its
-// parent's holds more (the root when n <= GROUP_MAX). Its leaves are a
-// contiguous sorted run sharing a Morton prefix, so the group is spatially
-// compact (a fixed run of consecutive sorted bodies is not: it can straddle a
-// Morton jump and span the whole system).
-//
-// Per internal node i (node v = n + i), after the climb (fully parallel): the
-// traversal data of both children go into one contiguous 64-byte child
-// record, so opening a node costs one load, each field as a (left, right)
-// pair so that the walk's paired FP32 opening test and list-entry arithmetic
-// read aligned register pairs:
-// (xL xR yL yR) (zL zR mL mR) (lxL lxR lyL lyR) (lzL lzR rcrit2L rcrit2R);
-// and the walk groups among node n + i and leaf i are listed.
-__global__ void __launch_bounds__(256) k_node_records(int64_t n, double theta, const int2* __restrict__ child,
-                                                      const double4* __restrict__ node_cm,
-                                                      const float4* __restrict__ bmin, const float4* __restrict__ bmax,
-                                                      const int32_t* __restrict__ parent,
-                                                      const int32_t* __restrict__ rlo, const int32_t* __restrict__ rhi,
-                                                      float4* __restrict__ crec, int2* __restrict__ groups,
-                                                      unsigned int* __restrict__ ngroups) {
-    // thread i: internal node n + i (record and group test) and leaf i (group
-    // test), so groups are listed roughly in sorted-leaf order, which keeps
-    // consecutive walk groups close in space
-    auto group_test = [&](int64_t v, int sz) {
-        if (sz > GROUP_MAX) return;
-        const int32_t p = n == 1 ? -1 : parent[v];
-        if (p >= 0 && rhi[p] - rlo[p] + 1 <= GROUP_MAX) return;
-        groups[atomicAdd(ngroups, 1u)] = make_int2(v < n ? (int32_t)v : rlo[v], sz);
-    };
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        group_test(i, 1);
-        if (i >= n - 1) continue;
-        const int64_t v = n + i;
-        const int2 ch = child[v];
-        float4 hL, lL, hR, lR;
-        const double4 cL = node_cm[ch.x], cR = node_cm[ch.y];
-        if (ch.x < n) leaf_trav(cL, hL, lL);
-        else node_trav(cL, bmin[ch.x], bmax[ch.x], theta, hL, lL);
-        if (ch.y < n) leaf_trav(cR, hR, lR);
-        else node_trav(cR, bmin[ch.y], bmax[ch.y], theta, hR, lR);
-        float4* dst = crec + 4 * i;
-        dst[0] = make_float4(hL.x, hR.x, hL.y, hR.y);
-        dst[1] = make_float4(hL.z, hR.z, hL.w, hR.w);
-        dst[2] = make_float4(lL.x, lR.x, lL.y, lR.y);
-        dst[3] = make_float4(lL.z, lR.z, lL.w, lR.w);
-        group_test(v, rhi[v] - rlo[v] + 1);
+// Child records of the internal nodes completed by the global phase of the
+// bottom-up merge (their arrival counters read 2; the block-local phase writes
+// the records of the nodes it completes and leaves their counters at 0).
+__global__ void __launch_bounds__(256) k_front_records(int64_t n, double theta, const uint32_t* __restrict__ counters,
+                                                       const int2* __restrict__ child,
+                                                       const double4* __restrict__ node_cm,
+                                                       const float4* __restrict__ bmin,
+                                                       const float4* __restrict__ bmax, float4* __restrict__ crec) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n - 1; i += (int64_t)gridDim.x * blockDim.x) {
+        if (counters[i] != 2u) continue;
+        const int2 ch = child[n + i];
+        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+        put_child_record(crec + 4 * i, n, theta, ch.x, node_cm[ch.x], ch.x < n ? z : bmin[ch.x],
+                         ch.x < n ? z : bmax[ch.x], ch.y, node_cm[ch.y], ch.y < n ? z : bmin[ch.y],
+                         ch.y < n ? z : bmax[ch.y]);
     }
 }
 
@@ -1273,13 +1290,14 @@ int run_sort(aster_ctx* c, int bits) {
     return ASTER_OK;
 }
 
-int launch_bottom_up(aster_ctx* c, int64_t n) {
+int launch_bottom_up(aster_ctx* c, int64_t n, double theta) {
     LbvhBufs& t = c->tree;
     unsigned int* nfront = red_groups(c) + 2;  // zeroed at the start of the build
     const int64_t blocks = (n + BU_LEAVES - 1) / BU_LEAVES;
     k_bottom_up_local<<<(unsigned)blocks, BU_LEAVES, 0, c->stream>>>(
         n, t.parent.as<int32_t>(), t.sib.as<int32_t>(), t.rlo.as<int32_t>(), t.rhi.as<int32_t>(),
-        t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(), t.front.as<int32_t>(), nfront, c->err_dev);
+        t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(), t.front.as<int32_t>(), nfront, c->err_dev,
+        theta, t.child.as<int2>(), t.crec.as<float4>());
     ASTER_CUDA(cudaGetLastError());
     const int64_t fb = std::min<int64_t>(blocks, (int64_t)c->sm_count * 8);
     k_bottom_up_front<<<(unsigned)fb, 256, 0, c->stream>>>(n, t.front.as<int32_t>(), nfront, t.parent.as<int32_t>(),
@@ -1322,18 +1340,17 @@ int run_build(aster_ctx* c, const aster_params* p) {
         k_karras<KeyT, true><<<grid, 256, 0, c->stream>>>(
             n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.parent.as<int32_t>(), t.sib.as<int32_t>(),
             t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(), t.counters.as<uint32_t>(),
-            t.node_cm.as<double4>());
+            t.node_cm.as<double4>(), t.groups.as<int2>(), gcount);
     else
         k_karras<KeyT, false><<<grid, 256, 0, c->stream>>>(
             n, sc, t.perm.as<int32_t>(), c->pm.as<double4>(), t.parent.as<int32_t>(), t.sib.as<int32_t>(),
             t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.child.as<int2>(), t.counters.as<uint32_t>(),
-            t.node_cm.as<double4>());
+            t.node_cm.as<double4>(), t.groups.as<int2>(), gcount);
     ASTER_CUDA(cudaGetLastError());
-    ASTER_TRY(launch_bottom_up(c, n));
-    k_node_records<<<grid, 256, 0, c->stream>>>(n, p->theta, t.child.as<int2>(), t.node_cm.as<double4>(),
-                                                t.bmin.as<float4>(), t.bmax.as<float4>(), t.parent.as<int32_t>(),
-                                                t.rlo.as<int32_t>(), t.rhi.as<int32_t>(), t.crec.as<float4>(),
-                                                t.groups.as<int2>(), gcount);
+    ASTER_TRY(launch_bottom_up(c, n, p->theta));
+    k_front_records<<<grid, 256, 0, c->stream>>>(n, p->theta, t.counters.as<uint32_t>(), t.child.as<int2>(),
+                                                 t.node_cm.as<double4>(), t.bmin.as<float4>(), t.bmax.as<float4>(),
+                                                 t.crec.as<float4>());
     ASTER_CUDA(cudaGetLastError());
     c->stats.kernels += 2;
     return ASTER_OK;
