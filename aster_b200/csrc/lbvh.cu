@@ -740,7 +740,9 @@ struct WalkShared {
 // (vx, vy, vz, |v|^2), FP32 for the mixed walk and FP64 for the FP64 walk.
 template <bool MIXED>
 struct WalkSharedPn : WalkShared<MIXED> {
-    float4 lvf[WALK_WARPS][MIXED ? WALK_LIST_PN : 1];
+    // mixed: paired like lpa/lpb, lva = (vx0, vx1, vy0, vy1), lvb = (vz0, vz1, w0, w1), w = |v|^2
+    float4 lva[WALK_WARPS][MIXED ? WALK_LIST_PN / 2 : 1];
+    float4 lvb[WALK_WARPS][MIXED ? WALK_LIST_PN / 2 : 1];
     double4 lvd[WALK_WARPS][MIXED ? 1 : WALK_LIST_FP64];
 };
 
@@ -838,6 +840,58 @@ __device__ __forceinline__ void interact_pn_f64(const double4 e, const double4 e
     pn_terms<PNL>(k, w, ax, ay, az, ax, ay, az);
 }
 
+// Two entries at once with the paired FP32 instructions, force law Newton +
+// 1PN: the Newtonian term into (ax, ay, az) as interact2_f32 forms it and the
+// 1PN term (PnPair::pn1) into (px, py, pz), both divided by G. A, B: entry
+// positions and masses as in interact2_f32; VA = (vx0, vx1, vy0, vy1),
+// VB = (vz0, vz1, |v0|^2, |v1|^2) the entries' velocities. Per body,
+// broadcast to both halves: nb = -(position), vi = velocity, nvi2 = -|vi|^2,
+// mi5 = 5 m_i.
+template <bool GUARD>
+__device__ __forceinline__ void interact2_pn1_f32(const float4 A, const float4 B, const float4 VA, const float4 VB,
+                                                  const float2 nbx, const float2 nby, const float2 nbz,
+                                                  const float2 vix, const float2 viy, const float2 viz,
+                                                  const float2 nvi2, const float2 mi5, const float2 eps2,
+                                                  const float2 G, const float2 c2, float2& ax, float2& ay, float2& az,
+                                                  float2& px, float2& py, float2& pz) {
+    const float2 dx = __fadd2_rn(make_float2(A.x, A.y), nbx);  // entry - body
+    const float2 dy = __fadd2_rn(make_float2(A.z, A.w), nby);
+    const float2 dz = __fadd2_rn(make_float2(B.x, B.y), nbz);
+    float2 r2 = __ffma2_rn(dz, dz, eps2);
+    r2 = __ffma2_rn(dy, dy, r2);
+    r2 = __ffma2_rn(dx, dx, r2);
+    float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    if (GUARD) {
+        inv.x = r2.x > 0.f ? inv.x : 0.f;
+        inv.y = r2.y > 0.f ? inv.y : 0.f;
+    }
+    const float2 mj = make_float2(B.z, B.w);
+    const float2 inv2 = __fmul2_rn(inv, inv);
+    const float2 sN = __fmul2_rn(__fmul2_rn(mj, inv), inv2);
+    ax = __ffma2_rn(dx, sN, ax);
+    ay = __ffma2_rn(dy, sN, ay);
+    az = __ffma2_rn(dz, sN, az);
+    const float2 m1 = make_float2(-1.f, -1.f);
+    const float2 ninv = __fmul2_rn(inv, m1);
+    const float2 nx = __fmul2_rn(dx, ninv), ny = __fmul2_rn(dy, ninv), nz = __fmul2_rn(dz, ninv);  // entry -> body
+    const float2 vjx = make_float2(VA.x, VA.y), vjy = make_float2(VA.z, VA.w), vjz = make_float2(VB.x, VB.y);
+    const float2 vj2 = make_float2(VB.z, VB.w);
+    const float2 dvx = __ffma2_rn(vjx, m1, vix), dvy = __ffma2_rn(vjy, m1, viy), dvz = __ffma2_rn(vjz, m1, viz);
+    const float2 v12 = __ffma2_rn(vix, vjx, __ffma2_rn(viy, vjy, __fmul2_rn(viz, vjz)));
+    const float2 nv1 = __ffma2_rn(nx, vix, __ffma2_rn(ny, viy, __fmul2_rn(nz, viz)));
+    const float2 nv2 = __ffma2_rn(nx, vjx, __ffma2_rn(ny, vjy, __fmul2_rn(nz, vjz)));
+    // A = -vi^2 - 2 vj^2 + 4 vi.vj + 1.5 (n.vj)^2 + (5 mi + 4 mj) G / r;  B = 4 n.vi - 3 n.vj
+    float2 Aa = __ffma2_rn(vj2, make_float2(-2.f, -2.f), nvi2);
+    Aa = __ffma2_rn(v12, make_float2(4.f, 4.f), Aa);
+    Aa = __ffma2_rn(__fmul2_rn(nv2, nv2), make_float2(1.5f, 1.5f), Aa);
+    Aa = __ffma2_rn(__ffma2_rn(mj, make_float2(4.f, 4.f), mi5), __fmul2_rn(G, inv), Aa);
+    const float2 Bb = __ffma2_rn(nv1, make_float2(4.f, 4.f), __fmul2_rn(nv2, make_float2(-3.f, -3.f)));
+    const float2 f = __fmul2_rn(__fmul2_rn(mj, inv2), c2);
+    px = __ffma2_rn(__ffma2_rn(nx, Aa, __fmul2_rn(dvx, Bb)), f, px);
+    py = __ffma2_rn(__ffma2_rn(ny, Aa, __fmul2_rn(dvy, Bb)), f, py);
+    pz = __ffma2_rn(__ffma2_rn(nz, Aa, __fmul2_rn(dvz, Bb)), f, pz);
+}
+
 __device__ __forceinline__ float4 vel_f4(const double4 v) {
     return make_float4((float)v.x, (float)v.y, (float)v.z, (float)(v.x * v.x + v.y * v.y + v.z * v.z));
 }
@@ -889,7 +943,7 @@ __device__ __forceinline__ float2 box_dist2_pair(const float2 cx, const float2 c
 // PNL > 0: the post-Newtonian walk (the terms pk selects, with the nodes'
 // velocities node_v); PNL == 0 is the Newtonian kernel.
 template <bool MIXED, bool GUARD, bool KICK, int PNL = 0>
-__global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK_MINBLOCKS : 6)) k_walk(
+__global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK_MINBLOCKS : 6)) k_walk(
     int64_t n, const int2* __restrict__ groups, const unsigned int* __restrict__ ngroups_p,
     unsigned int* __restrict__ work,
     const float4* __restrict__ crec, const double4* __restrict__ node_cm, const int2* __restrict__ child,
@@ -983,22 +1037,56 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK
         // post-Newtonian walk: the velocity of list entry `pos`
         auto put_v = [&](int pos, const double4 v) {
             if constexpr (PNL > 0) {
-                if (MIXED) sm.lvf[warp][pos] = vel_f4(v);
-                else sm.lvd[warp][pos] = vel_d4(v);
+                if (MIXED) {
+                    const float4 f = vel_f4(v);
+                    float* VA = reinterpret_cast<float*>(&sm.lva[warp][0]);
+                    float* VB = reinterpret_cast<float*>(&sm.lvb[warp][0]);
+                    const int o = ((pos >> 1) << 2) | (pos & 1);
+                    VA[o] = f.x;
+                    VA[o + 2] = f.y;
+                    VB[o] = f.z;
+                    VB[o + 2] = f.w;
+                } else {
+                    sm.lvd[warp][pos] = vel_d4(v);
+                }
             }
         };
 
         auto evaluate = [&](int cnt) {
-            if constexpr (PNL > 0) {  // one entry at a time, scalar
-                if (MIXED) {
+            if constexpr (PNL > 0) {
+                if constexpr (MIXED && PNL == 1) {  // Newton + 1PN only: two entries per paired instruction
+                    // an odd cnt has its last slot half zero-padded by the caller
+                    const int np = (cnt + 1) >> 1;
+                    const float2 G2 = make_float2((float)G, (float)G);
+                    const float2 c22 = make_float2((float)pk.c2, (float)pk.c2);
+                    auto body = [&](const float2 nbx, const float2 nby, const float2 nbz, const float4 vf, float mi,
+                                    int q0i, int step, CompSum& sx, CompSum& sy, CompSum& sz, float3& p) {
+                        const float2 vix = make_float2(vf.x, vf.x), viy = make_float2(vf.y, vf.y),
+                                     viz = make_float2(vf.z, vf.z), nvi2 = make_float2(-vf.w, -vf.w),
+                                     mi5 = make_float2(5.f * mi, 5.f * mi);
+                        float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax, px = ax, py = ax, pz = ax;
+#pragma unroll 2
+                        for (int q = q0i; q < np; q += step)
+                            interact2_pn1_f32<GUARD>(sm.lpa[warp][q], sm.lpb[warp][q], sm.lva[warp][q],
+                                                     sm.lvb[warp][q], nbx, nby, nbz, vix, viy, viz, nvi2, mi5,
+                                                     eps2f2, G2, c22, ax, ay, az, px, py, pz);
+                        sx.add(ax.x + ax.y); sy.add(ay.x + ay.y); sz.add(az.x + az.y);
+                        p.x += px.x + px.y; p.y += py.x + py.y; p.z += pz.x + pz.y;
+                    };
+                    body(nb0x, nb0y, nb0z, vf0, h0.w, 0, 1, sx0, sy0, sz0, p0);
+                    if (two) body(nb1x, nb1y, nb1z, vf1, h1.w, sub, lps, sx1, sy1, sz1, p1);
+                } else if (MIXED) {  // one entry at a time, scalar
                     const float* A = reinterpret_cast<const float*>(&sm.lpa[warp][0]);
                     const float* B = reinterpret_cast<const float*>(&sm.lpb[warp][0]);
+                    const float* VA = reinterpret_cast<const float*>(&sm.lva[warp][0]);
+                    const float* VB = reinterpret_cast<const float*>(&sm.lvb[warp][0]);
                     const float Gf = (float)G, e2 = (float)eps2;
                     const PnK<float> pkf = pn_float(pk);
                     float ax = 0.f, ay = 0.f, az = 0.f;
                     for (int e = 0; e < cnt; ++e) {
                         const int o = ((e >> 1) << 2) | (e & 1);
-                        interact_pn_f32<PNL, GUARD>(A[o], A[o + 2], B[o], B[o + 2], sm.lvf[warp][e], b0, vf0, h0.w,
+                        interact_pn_f32<PNL, GUARD>(A[o], A[o + 2], B[o], B[o + 2],
+                                                    make_float4(VA[o], VA[o + 2], VB[o], VB[o + 2]), b0, vf0, h0.w,
                                                     e2, Gf, pkf, ax, ay, az, p0, q0);
                     }
                     sx0.add(ax); sy0.add(ay); sz0.add(az);
@@ -1006,7 +1094,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK
                         float bx = 0.f, by = 0.f, bz = 0.f;
                         for (int e = sub; e < cnt; e += lps) {
                             const int o = ((e >> 1) << 2) | (e & 1);
-                            interact_pn_f32<PNL, GUARD>(A[o], A[o + 2], B[o], B[o + 2], sm.lvf[warp][e], b1, vf1,
+                            interact_pn_f32<PNL, GUARD>(A[o], A[o + 2], B[o], B[o + 2],
+                                                        make_float4(VA[o], VA[o + 2], VB[o], VB[o + 2]), b1, vf1,
                                                         h1.w, e2, Gf, pkf, bx, by, bz, p1, q1);
                         }
                         sx1.add(bx); sy1.add(by); sz1.add(bz);
@@ -1156,13 +1245,12 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK
                 }
                 if constexpr (PNL > 0) {  // the entries' velocities: [FL, FL + rest) -> [0, rest), rest < 64
                     const bool m0 = lane < rest, m1 = lane + 32 < rest;
-                    if (MIXED) {
-                        float4 x0 = make_float4(0, 0, 0, 0), x1 = x0;
-                        if (m0) x0 = sm.lvf[warp][FL + lane];
-                        if (m1) x1 = sm.lvf[warp][FL + 32 + lane];
+                    if (MIXED) {  // whole slots, as for the positions
+                        const int ns = (rest + 1) >> 1;
+                        float4 a = make_float4(0, 0, 0, 0), b = a;
+                        if (lane < ns) { a = sm.lva[warp][FL / 2 + lane]; b = sm.lvb[warp][FL / 2 + lane]; }
                         __syncwarp();
-                        if (m0) sm.lvf[warp][lane] = x0;
-                        if (m1) sm.lvf[warp][32 + lane] = x1;
+                        if (lane < ns) { sm.lva[warp][lane] = a; sm.lvb[warp][lane] = b; }
                     } else {
                         double4 x0 = make_double4(0, 0, 0, 0), x1 = x0;
                         if (m0) x0 = sm.lvd[warp][FL + lane];
@@ -1185,6 +1273,11 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 3 : (MIXED ? ASTER_WALK
             float* B = reinterpret_cast<float*>(&sm.lpb[warp][0]);
             const int q = lc >> 1;
             A[4 * q + 1] = 0.f; A[4 * q + 3] = 0.f; B[4 * q + 1] = 0.f; B[4 * q + 3] = 0.f;
+            if constexpr (PNL > 0) {  // and zero velocity, so the 1PN term is 0 * finite
+                float* VA = reinterpret_cast<float*>(&sm.lva[warp][0]);
+                float* VB = reinterpret_cast<float*>(&sm.lvb[warp][0]);
+                VA[4 * q + 1] = 0.f; VA[4 * q + 3] = 0.f; VB[4 * q + 1] = 0.f; VB[4 * q + 3] = 0.f;
+            }
         }
         __syncwarp();
         if (lc > 0) evaluate(lc);
@@ -1421,7 +1514,10 @@ int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, b
                                                 t.counters.as<uint32_t>(), t.node_v.as<double4>(), c->err_dev);
         ASTER_CUDA(cudaGetLastError());
         c->stats.kernels += 1;
-        if (mixed) {
+        if (mixed && pn_level(p) == 1) {  // Newton + 1PN: the paired-FP32 list evaluation
+            if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true, 1>(c, p, counts) : launch_walk<true, true, false, 1>(c, p, counts)); }
+            else       { ASTER_TRY(kick ? launch_walk<true, false, true, 1>(c, p, counts) : launch_walk<true, false, false, 1>(c, p, counts)); }
+        } else if (mixed) {
             if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true, 2>(c, p, counts) : launch_walk<true, true, false, 2>(c, p, counts)); }
             else       { ASTER_TRY(kick ? launch_walk<true, false, true, 2>(c, p, counts) : launch_walk<true, false, false, 2>(c, p, counts)); }
         } else {

@@ -197,6 +197,36 @@ def test_invalid_arguments(ctx):
         ctx.upload(np.array([[np.nan, 0, 0]]), None, np.ones(1))
 
 
+def test_empty_input_and_missing_state():
+    """A context with no bodies answers every solver, stepper and readback
+    with ASTER_ERR_NO_STATE and stays usable; an empty body array is an
+    invalid argument and leaves the context without state (the C++ plugin
+    returns early for an empty body array, as the reference's solvers do)."""
+    from aster_b200.api import SOLVER_LBVH, AsterError, Context
+    with Context(0) as c:
+        calls = (lambda: c.allpairs(Params(), FP64), lambda: c.allpairs(Params(), MIXED),
+                 lambda: c.lbvh_forces(Params()), lambda: c.kdk_steps(Params(), 1),
+                 lambda: c.kdk_steps(Params(), 1, SOLVER_LBVH, MIXED), lambda: c.energy(Params()),
+                 lambda: c.download())
+        for call in calls:
+            with pytest.raises(AsterError) as e:
+                call()
+            assert e.value.status == 4  # ASTER_ERR_NO_STATE
+        with pytest.raises(AsterError) as e:
+            c.upload(np.zeros((0, 3)), None, np.zeros(0))
+        assert e.value.status == 1  # ASTER_ERR_INVALID_ARG
+        with pytest.raises(AsterError) as e:
+            c.allpairs(Params(), FP64)
+        assert e.value.status == 4
+        # above the largest supported n (2^30: node ids are int32) the size is
+        # refused before any pointer is read
+        pos, vel, m = gen.plummer(100, 5)
+        too_many = c.lib.aster_state_upload(c.h, (1 << 30) + 1, pos.ctypes.data, vel.ctypes.data, m.ctypes.data)
+        assert too_many == 1  # ASTER_ERR_INVALID_ARG
+        c.upload(pos, vel, m)
+        assert np.all(np.isfinite(c.allpairs(Params(eps2=1e-4), FP64)))
+
+
 @pytest.mark.parametrize("n_massive", [1, 5, 700])
 def test_trailing_massless_sources(ctx, orc, n_massive):
     """Bodies after the last massive one are skipped as sources (they attract

@@ -182,11 +182,14 @@ def test_pn_lbvh_kdk_at_theta0_equals_allpairs_kdk(ctx):
 
 
 def test_zero_softening_walk_is_finite(ctx):
+    """eps = 0 with two coincident bodies: the zero separations contribute
+    nothing (Newton, and Newton + 1PN, whose mixed walk pairs list entries)."""
     pos, vel, m = gen.plummer(5000, 3)
     pos[1] = pos[2]
     ctx.upload(pos, vel, m)
-    for prec in (FP64, MIXED):
-        assert np.isfinite(ctx.lbvh_forces(Params(eps2=0.0), prec)).all()
+    for law in (NEWTON, NEWTON | PN1):
+        for prec in (FP64, MIXED):
+            assert np.isfinite(ctx.lbvh_forces(Params(eps2=0.0, c=10.0, force_law=law), prec)).all()
 
 
 def test_c2_full_size_tree_bit_exact(ctx, orc):
