@@ -465,6 +465,18 @@ def secondary(ctx, args):
                                  "unit": "TFLOP/s", "frac": tf / peak}
     res["mixed_vs_fp64_rel_l2"] = float(np.linalg.norm(accs["mixed"] - accs["fp64"]) / np.linalg.norm(accs["fp64"]))
     res["workload"] = "C3 cold exponential disk N=262144 (+central mass 0.1), eps=0.002, one force evaluation"
+    try:
+        from oracle.oracle import Ref
+        if Ref.available():  # the reference's Parallelized solver, sources [0, 4096) only
+            ref = Ref().setup(pos, vel, m, G=1.0, dt=1e-4, eps2=EPS_C3 ** 2).set_bounds(0, 4096)
+            t0 = time.perf_counter()
+            ref.forces()
+            el = time.perf_counter() - t0
+            res["cpu_reference"] = {"pairs_per_s": N_C3 * 4096 / el, "cores": ref.threads(), "cpu_model": cpu_model(),
+                                    "sample": f"all {N_C3} targets against sources [0, 4096) (Solver::set_bounds), "
+                                              "one force evaluation, reference sources compiled unmodified"}
+    except Exception as exc:  # the CPU figure is reported beside the GPU one, never instead of it
+        res["cpu_reference"] = {"unavailable": str(exc)[:200]}
     out["allpairs"] = res
     out["ensemble"] = ensemble_c4(ctx, sm_mhz=getattr(args, "sm_mhz", 1965.0))
     out["adjoint"] = adjoint_c5(ctx)
