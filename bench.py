@@ -703,6 +703,16 @@ def run_case(args):
                     np.linalg.norm(a[tg] - exact) / np.linalg.norm(exact))
             out["runs"].append(run)
             del pos, vel, m
+    elif args.case == "pnlbvh":
+        # the C2 step with Newton + 1PN (c = 100) at args.n bodies: one step, then three
+        from aster_b200.api import SOLVER_LBVH
+        pos, vel, m = gen.plummer(args.n, SEED_C2, masses="lognormal")
+        p = Params(G=1.0, eps2=EPS * EPS, theta=THETA, dt=DT, c=100.0, force_law=NEWTON | PN1)
+        ctx.upload(pos, vel, m)
+        ctx.kdk_steps(p, 1, SOLVER_LBVH, MIXED)
+        ctx.kdk_steps(p, 3, SOLVER_LBVH, MIXED)
+        st = ctx.stats()
+        out.update(n=args.n, ms_per_step=st["ms_total"] / 3, interactions_per_step=st["interactions"] / 3)
     elif args.case == "ensemble":
         pos, vel, m, off = gen.hierarchical_ensemble(16384, 1004)
         p = Params(G=1.0, c=100.0, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1)
@@ -735,7 +745,8 @@ def main():
                     help="bodies in the headline workload (default 2^20; smaller only for profiling captures)")
     ap.add_argument("--walk-traffic", type=float, default=WALK_TRAFFIC_BYTES,
                     help="DRAM bytes per walk launch from an ncu capture (reported as roofline.traffic)")
-    ap.add_argument("--case", default=None, choices=["allpairs", "ensemble", "adjoint", "c3drift", "wh", "scale"],
+    ap.add_argument("--case", default=None,
+                    choices=["allpairs", "ensemble", "adjoint", "c3drift", "wh", "scale", "pnlbvh"],
                     help="run one secondary workload briefly (used for profiling captures) and exit")
     args = ap.parse_args()
     if args.warmup < 3:
