@@ -268,3 +268,37 @@ def planetary_system(n_planets: int, n_particles: int, seed: int, M_star: float 
     vel[1:] = vxo[:, None] * px + vyo[:, None] * qx
     pos, vel = com_centre(pos, vel, m)
     return pos, vel, m
+
+
+def kepler_orbits(n: int, seed: int, mu: float = 1.0):
+    """A unit central mass (body 0, at rest at the origin) and n massless
+    bodies on conic orbits about it, for checking Kepler drifts on their own:
+    half elliptic (e ~ U[0, 0.95]), a quarter hyperbolic (e ~ U[1.05, 3]) and
+    the rest near-parabolic (e ~ U[0.97, 1.03]). Pericentre distance
+    log-uniform in [0.3, 5]; true anomaly U[-2, 2] rad, clipped to 0.9 of a
+    hyperbola's asymptote angle; each orbit plane turned by a uniform random
+    rotation (a normalised Gaussian quaternion). Returns (pos, vel, m, e)."""
+    rng = np.random.default_rng(seed)
+    e = np.concatenate([rng.uniform(0.0, 0.95, n // 2), rng.uniform(1.05, 3.0, n // 4),
+                        rng.uniform(0.97, 1.03, n - n // 2 - n // 4)])
+    q = np.exp(rng.uniform(np.log(0.3), np.log(5.0), n))
+    f = rng.uniform(-2.0, 2.0, n)
+    lim = np.where(e > 1.0, 0.9 * np.arccos(-1.0 / np.maximum(e, 1.0 + 1e-9)), np.pi)
+    f = np.clip(f, -lim, lim)
+    p = q * (1.0 + e)
+    r = p / (1.0 + e * np.cos(f))
+    x = np.stack([r * np.cos(f), r * np.sin(f), np.zeros(n)], axis=1)
+    v = np.sqrt(mu / p)[:, None] * np.stack([-np.sin(f), e + np.cos(f), np.zeros(n)], axis=1)
+    qt = rng.normal(size=(n, 4))
+    qt /= np.linalg.norm(qt, axis=1, keepdims=True)
+    w, a, b, c = qt.T
+    rot = np.stack([np.stack([1 - 2 * (b * b + c * c), 2 * (a * b - c * w), 2 * (a * c + b * w)], 1),
+                    np.stack([2 * (a * b + c * w), 1 - 2 * (a * a + c * c), 2 * (b * c - a * w)], 1),
+                    np.stack([2 * (a * c - b * w), 2 * (b * c + a * w), 1 - 2 * (a * a + b * b)], 1)], axis=1)
+    x = np.einsum("nij,nj->ni", rot, x)
+    v = np.einsum("nij,nj->ni", rot, v)
+    pos = np.vstack([np.zeros(3), x])
+    vel = np.vstack([np.zeros(3), v])
+    m = np.zeros(n + 1)
+    m[0] = mu
+    return pos, vel, m, e

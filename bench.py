@@ -42,11 +42,19 @@ N_C2 = 1 << 20
 THETA, EPS, DT = 0.5, 0.005, 5e-4
 SEED_C2 = 1002
 N_C3, EPS_C3, SEED_C3 = 262144, 0.002, 1003
+# the workload both arms (this library and the reference CPU code) run
+C2_WORKLOAD = ("C2 LBVH Barnes-Hut KDK step, Plummer N=1048576 lognormal(0,0.5) masses, 30-bit Morton on the "
+               "bounding cube, theta=0.5, eps=0.005, dt=5e-4")
 FLOP_PER_PAIR = 20  # Newtonian pair, Nyland et al. GPU Gems 3 ch. 31 convention
 # 1PN pair term (compute_gravitational with get_pn1): the Newtonian 20 + unit
 # vector 3, v_i - v_j 3, v_i.v_j 5, n.v_i 5, n.v_j 5, bracket A 13, bracket B 3,
 # prefactor 2, the three components 12 = 71 FLOP
 FLOP_PER_PN1_PAIR = 71
+# Adjoint pair term (J^T w and the mass gradient, one pair): separation 3,
+# r^2 with softening 6, rsqrt 1, s^3 and s^5 3, u = m_k w_j - m_j w_k 9,
+# d.u 5, 3 s^5 (d.u) 2, the three components 12, w_j.d 5, mass-gradient
+# term 2 = 48 FLOP
+FLOP_PER_ADJ_PAIR = 48
 # Tree build, algorithmic bytes per body: Morton 32 (read the position 24,
 # write code and index 8) + sort 16 (one read and one write of the 8-byte
 # key/value, whatever the pass count) + Karras 24 (read the code, write links
@@ -55,7 +63,7 @@ FLOP_PER_PN1_PAIR = 71
 BUILD_BYTES_PER_BODY = 240
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_walk launch captured with
-# ncu at N = 2^19 (74.04 + 4.59 MB, profiles/k_walk_c2_plummer524288.md), scaled
+# ncu at N = 2^19 (74.04 + 4.59 MB read + written), scaled
 # by the number of bodies to N = 2^20 (the walk reads each tree node about once).
 WALK_TRAFFIC_BYTES = 78.63e6 * 2
 
@@ -254,8 +262,8 @@ def run_reference(args):
         "impl": "reference", "metric": "LBVH-BH steps/s @N=1M", "value": v, "unit": "steps/s", "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "C2 LBVH Barnes-Hut KDK step, Plummer N=1048576 lognormal masses, theta=0.5, "
-                               "eps=0.005, dt=5e-4", "n": N_C2},
+        "config": {"workload": C2_WORKLOAD, "n": N_C2,
+                   "precision": "FP64 throughout (the reference CPU Barnes_Hut)"},
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": ref.threads(), "kind": "reference",
                          "cpu_model": cpu_model(),
                          "sample": f"full N={N_C2} update_leapfrog steps with Barnes_Hut (2 tree builds + walks "
@@ -327,11 +335,10 @@ def run_ours(args):
             "metric": "LBVH-BH steps/s @N=1M", "value": value, "unit": "steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 pairs / f64 state", "data": "synthetic",
-            "config": {"workload": ("C2 LBVH Barnes-Hut KDK step, Plummer N=1048576" if args.n == N_C2 else
-                                    f"LBVH Barnes-Hut KDK step (C2 at reduced size), Plummer N={args.n}")
-                                   + " lognormal(0,0.5) masses, 30-bit Morton on the bounding cube, theta=0.5, "
-                                     "eps=0.005, dt=5e-4, mixed",
-                       "n": args.n, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "config": {"workload": (C2_WORKLOAD if args.n == N_C2 else
+                                    C2_WORKLOAD.replace("C2 LBVH", "C2 at reduced size: LBVH")
+                                    .replace("N=1048576", f"N={args.n}")),
+                       "n": args.n, "precision": "mixed: FP32 interactions on double-single positions, FP64 state", "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "per-step working set > L2: the tree rebuild writes ~0.4 GB every step"},
             "phases_ms": {"build": build_ms, "walk": walk_ms, "other": ms / args.steps - build_ms - walk_ms},
             "interactions_per_step": inter_per_step,
@@ -477,9 +484,11 @@ def secondary(ctx, args):
                                               "one force evaluation, reference sources compiled unmodified"}
     except Exception as exc:  # the CPU figure is reported beside the GPU one, never instead of it
         res["cpu_reference"] = {"unavailable": str(exc)[:200]}
+    res["c3_drift"] = c3_drift(ctx)
     out["allpairs"] = res
+    out["allpairs_1m"] = allpairs_1m(ctx, getattr(args, "sm_mhz", 1965.0))
     out["ensemble"] = ensemble_c4(ctx, sm_mhz=getattr(args, "sm_mhz", 1965.0))
-    out["adjoint"] = adjoint_c5(ctx)
+    out["adjoint"] = adjoint_c5(ctx, getattr(args, "sm_mhz", 1965.0))
     out["c1"] = kdk_c1(ctx)
     out["next_rows"] = next_rows(ctx)
     return out
@@ -585,9 +594,45 @@ def kdk_c1(ctx):
     return out
 
 
+def allpairs_1m(ctx, sm_mhz: float):
+    """One mixed and one FP64 all-pairs evaluation of the C2 bodies (N = 2^20
+    lognormal Plummer, eps = 0.005): pair rates against the FP32 and FP64
+    pipe peaks, and the mixed-vs-FP64 force error over all bodies. Each
+    precision is first run once on a 2^14-body state (module load, first-use
+    allocation), then timed on one full evaluation (CUDA events)."""
+    from aster_b200 import gen
+    from aster_b200.api import FP64, MIXED, Params
+    p = Params(G=1.0, eps2=EPS * EPS)
+    pw, vw, mw = gen.plummer(1 << 14, 7, masses="lognormal")
+    ctx.upload(pw, vw, mw)
+    for prec in (FP64, MIXED):
+        ctx.allpairs(p, prec)
+    pos, vel, m = gen.plummer(N_C2, SEED_C2, masses="lognormal")
+    ctx.upload(pos, vel, m)
+    f32p, f64p = fp_peaks(sm_mhz)
+    out = {"workload": "C2 bodies: Plummer N=1048576, lognormal(0,0.5) masses, eps=0.005, one all-pairs "
+                       "force evaluation per precision (N(N-1) pairs)"}
+    accs = {}
+    for name, prec, peak in (("mixed", MIXED, f32p), ("fp64", FP64, f64p)):
+        accs[name] = ctx.allpairs(p, prec)
+        t = ctx.stats()["ms_force"]
+        rate = N_C2 * (N_C2 - 1) / (t / 1e3)
+        tf = rate * FLOP_PER_PAIR / 1e12
+        out[name] = {"ms_per_eval": t, "pairs_per_s": rate,
+                     "roofline": {"bound": "fp32" if prec == MIXED else "fp64", "achieved": tf, "peak": peak,
+                                  "unit": "TFLOP/s", "frac": tf / peak, "flop_per_pair": FLOP_PER_PAIR}}
+    out["mixed_vs_fp64_rel_l2"] = float(np.linalg.norm(accs["mixed"] - accs["fp64"]) /
+                                        np.linalg.norm(accs["fp64"]))
+    out["mixed_speedup_over_fp64"] = out["fp64"]["ms_per_eval"] / out["mixed"]["ms_per_eval"]
+    return out
+
+
 def c3_drift(ctx, nsteps: int = 1000):
     """C3 long run: 1000 KDK steps (dt = 1e-4) of the N = 262144 cold disk
-    with FP64 and with mixed all-pairs forces; energy drift of each."""
+    with FP64 and with mixed all-pairs forces; energy drift of each (FP64
+    O(N^2) energy with the Plummer-softened potential that the force is the
+    gradient of), the momentum at the end and how far apart the two runs'
+    final positions are."""
     from aster_b200 import gen
     from aster_b200.api import FP64, MIXED, SOLVER_ALLPAIRS, Params
     pos, vel, m = gen.exponential_disk(N_C3, SEED_C3)
@@ -634,9 +679,13 @@ def ensemble_c4(ctx, nsteps: int = 10_000, sm_mhz: float = 1965.0):
             "energy_drift_median": float(np.median(de)), "energy_drift_p90": float(np.percentile(de, 90))}
 
 
-def adjoint_c5(ctx):
+def adjoint_c5(ctx, sm_mhz: float = 1965.0):
     """C5: N=16384 Plummer, eps=0.01, dt=1e-3, 1000 KDK steps, checkpoints
-    every 32; forward + reverse sweep time for dL/d(x0, v0, m)."""
+    every 32; forward + reverse sweep time for dL/d(x0, v0, m). Roofline over
+    the whole run: the forward pass and the per-segment recomputation each
+    evaluate N(N-1) force pairs per step (20 FLOP), the reverse sweep one
+    adjoint pair term per pair per step (48 FLOP), against the FP32 pipe
+    (mixed) or FP64 pipe (FP64) peak at the sampled SM clock."""
     from aster_b200 import gen
     from aster_b200.api import FP64, MIXED, SOLVER_ALLPAIRS, Params
     n, T = 16384, 1000
@@ -648,9 +697,17 @@ def adjoint_c5(ctx):
     target, _, _ = ctx.download()
     ctx.upload(x0, v0, m)
     out = {"workload": "C5 Plummer N=16384, eps=0.01, dt=1e-3, 1000 KDK steps, loss=mean|x_T-x*|^2, K=32"}
-    for name, prec in (("mixed", MIXED), ("fp64", FP64)):
+    f32p, f64p = fp_peaks(sm_mhz)
+    pairs = n * (n - 1)
+    flop = pairs * T * (2 * FLOP_PER_PAIR + FLOP_PER_ADJ_PAIR)
+    for name, prec, peak in (("mixed", MIXED, f32p), ("fp64", FP64, f64p)):
         loss, *_ = ctx.adjoint(p, T, target, prec, 32)
-        out[name] = {"ms_forward_plus_adjoint": ctx.stats()["ms_total"], "loss": loss}
+        ms = ctx.stats()["ms_total"]
+        tf = flop / (ms / 1e3) / 1e12
+        out[name] = {"ms_forward_plus_adjoint": ms, "loss": loss,
+                     "roofline": {"bound": "fp32" if prec == MIXED else "fp64", "achieved": tf, "peak": peak,
+                                  "unit": "TFLOP/s", "frac": tf / peak,
+                                  "flop_per_step": f"N(N-1) x (2 x {FLOP_PER_PAIR} + {FLOP_PER_ADJ_PAIR})"}}
     return out
 
 

@@ -325,7 +325,13 @@ int aster_adjoint_leapfrog(aster_ctx* ctx, const aster_params* p, int precision,
  * work is queued on `stream` (a cudaStream_t, NULL for the default stream) and
  * the call returns without waiting; synchronise before reading out_dev.
  * The first call on a device looks up that device's address of the array, so
- * make that first call before any stream capture. All calls share the one
+ * make that first call before any stream capture. The address is kept for the
+ * life of the process: calling cudaDeviceReset after the first call on that
+ * device is not supported (the module is reloaded elsewhere and the kept
+ * address goes stale). Every block adds up 256 bodies against all sources in
+ * one launch, so below about 40,000 bodies the GPU is only partly filled and
+ * this call is several times slower than aster_energy, which also splits the
+ * sources over blocks. All calls share the one
  * array: calls that overlap on the GPU (on different streams) race and give
  * wrong results. Each call fully rewrites the partials it reads, so nothing
  * needs clearing between calls. */

@@ -50,7 +50,7 @@ class Ref:
     def __init__(self):
         if Ref._lib is None:
             if not REF_LIB.exists():
-                raise FileNotFoundError(f"{REF_LIB} missing: run `make -C oracle`")
+                raise FileNotFoundError(f"{REF_LIB} missing: run `make -C oracle REF=<reference source tree>`")
             lib = ctypes.CDLL(str(REF_LIB))
             lib.ref_setup.argtypes = [ctypes.c_int, _D, _D, _D] + [ctypes.c_double] * 6 + [ctypes.c_int, ctypes.c_int]
             lib.ref_get_state.argtypes = [_D, _D, _D]
@@ -62,6 +62,7 @@ class Ref:
             lib.ref_pair_force.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D, _D, _D, _D]
             lib.ref_saba.argtypes = [ctypes.c_int, ctypes.c_int]
             lib.ref_wh.argtypes = [ctypes.c_int]
+            lib.ref_wh_drift_only.argtypes = [ctypes.c_int]
             lib.ref_saba_coeffs.argtypes = [ctypes.c_int, _D]
             Ref._lib = lib
         self.lib = Ref._lib
@@ -126,6 +127,13 @@ class Ref:
         """nsteps of the reference CPU update_WH_planetary (body 0 central)."""
         if self.lib.ref_wh(nsteps) != 0:
             raise RuntimeError("ref_wh failed")
+
+    def wh_drift_only(self, nsteps):
+        """nsteps of update_WH_planetary under a zero-force solver: the
+        reference's update_kepler drift of every body about body 0 (two
+        half-steps per step), with no kick."""
+        if self.lib.ref_wh_drift_only(nsteps) != 0:
+            raise RuntimeError("ref_wh_drift_only failed")
 
     def saba_coeffs(self, order):
         """The reference's SABA table for the order: (d, c) slot pairs."""

@@ -11,6 +11,7 @@
 //   update_leapfrog                src/physics/tool_chain_impl.cpp:169-185
 //   update_SABA1..10               src/integrators/SABA.cpp:14-553 (CPU forms)
 //   update_WH_planetary            src/physics/tool_chain_impl.cpp:186-290
+//     (also under a zero-force solver: update_kepler, :186-254, on its own)
 //   GPU::saba_coeffs               include/Aster/physics/coeffs.h:8-161
 //   compute_gravitational          src/physics/tool_chain_impl.cpp:120-137
 //   Graphs::get_total_energy       src/utils/collectors.cpp:19-53
@@ -45,6 +46,17 @@ struct HarnessSim : public Aster::Simulation {
 
 HarnessSim* g_sim = nullptr;
 int g_solver_kind = 0;
+
+// A Solver whose compute_forces() writes zero accelerations. Under it the
+// kick of update_WH_planetary does nothing, so one step is two update_kepler
+// half-drifts of every body i >= 1 about body 0 (mu = G m_0) plus body 0's
+// linear drift: the reference's Kepler drift on its own.
+struct ZeroForce : public Aster::Solver {
+    explicit ZeroForce(Aster::Simulation* s) { _s = s; }
+    void compute_forces() override {
+        for (auto& a : _s->bodies.accs) a = Aster::vec3(0.0);
+    }
+};
 
 HarnessSim* sim() {
     if (!g_sim) g_sim = new HarnessSim();
@@ -162,6 +174,20 @@ int ref_wh(int nsteps) {
     HarnessSim* s = sim();
     if (!s->solver) return -1;
     for (int k = 0; k < nsteps; ++k) Aster::update_WH_planetary(s);
+    return 0;
+}
+
+// nsteps of update_WH_planetary with the zero-force solver above in place of
+// the current one (restored afterwards): the reference's update_kepler drift
+// (tool_chain_impl.cpp:186-254) applied as two half-steps per step.
+int ref_wh_drift_only(int nsteps) {
+    HarnessSim* s = sim();
+    if (s->bodies.positions.empty()) return -1;
+    Aster::Solver* keep = s->solver;
+    ZeroForce zero(s);
+    s->solver = &zero;
+    for (int k = 0; k < nsteps; ++k) Aster::update_WH_planetary(s);
+    s->solver = keep;
     return 0;
 }
 

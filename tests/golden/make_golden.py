@@ -2,7 +2,7 @@
 code, compiled unmodified from its sources (oracle/Makefile ->
 oracle/_ref/libaster_ref.so). Run here, where the reference sources exist:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference source tree> && python tests/golden/make_golden.py
 
 The fixtures are committed; the tests read them on machines without the
 reference. Inputs come from the seeded generators in aster_b200/gen.py.
@@ -29,6 +29,12 @@ Fixtures:
   saba_plummer256.npz       update_SABA1..10 with Parallelized: 4 steps each from one
                             N=256 Plummer state (eps2 = 1e-4, dt = 1e-3), and the
                             reference coefficient tables (GPU::saba_coeffs).
+
+  kepler_drift.npz          update_WH_planetary under a zero-force solver (so the
+                            reference's update_kepler drift alone, two half-steps
+                            a step) on 400 massless bodies about a unit mass
+                            (gen.kepler_orbits: elliptic, near-parabolic and
+                            hyperbolic), dt = 0.05, 40 steps: final x, v.
 
 `python tests/golden/make_golden.py pn_pairs` regenerates one fixture only.
 """
@@ -153,8 +159,19 @@ def saba_fixture(ref: Ref):
     np.savez_compressed(OUT / "saba_plummer256.npz", **out)
 
 
+def kepler_fixture(ref: Ref):
+    pos, vel, m, e = gen.kepler_orbits(400, 1025)
+    dt, nsteps = 0.05, 40
+    ref.setup(pos, vel, m, G=1.0, dt=dt)
+    ref.wh_drift_only(nsteps)
+    rp, rv, _ = ref.state()
+    np.savez_compressed(OUT / "kepler_drift.npz", pos=pos, vel=vel, m=m, e=e, dt=dt, steps=nsteps,
+                        ref_pos=rp, ref_vel=rv)
+
+
 FIXTURES = {"allpairs": allpairs_fixture, "leapfrog": leapfrog_fixture, "tree": tree_fixture,
-            "pn_pairs": pn_fixture, "saba": saba_fixture, "allpairs_pn": allpairs_pn_fixture}
+            "pn_pairs": pn_fixture, "saba": saba_fixture, "allpairs_pn": allpairs_pn_fixture,
+            "kepler": kepler_fixture}
 
 
 def main():

@@ -211,6 +211,31 @@ def test_c2_full_size_tree_bit_exact(ctx, orc):
     assert np.all(t["perm"][1:][ties] > t["perm"][:-1][ties])
 
 
+def test_c2_full_size_tree_bit_exact_vs_reference_build(ctx):
+    """C2 at full size against the reference itself: Barnes_Hut::make_tree
+    (src/solvers/barnes_hut.cpp:309-400, unite :137-152) run by the reference
+    CPU library on the same 2^20 bodies and Morton box. Morton codes, left and
+    right children of every node, FP64 node masses and centres of mass are
+    bit-identical; the leaves hold the bodies in our sorted order (the
+    reference stores each sorted body's position and mass in leaf i)."""
+    from oracle.oracle import Ref
+    if not Ref.available():
+        pytest.skip("reference CPU build absent")
+    n = 1 << 20
+    pos, vel, m = gen.plummer(n, 1002, masses="lognormal")
+    ctx.upload(pos, vel, m)
+    t = ctx.lbvh_build(Params(theta=0.5, eps2=0.005 ** 2))
+    ref = Ref().setup(pos, vel, m, G=1.0, eps2=0.005 ** 2, theta=0.5, box=t["box"], solver="bh")
+    r = ref.bh_tree()
+    np.testing.assert_array_equal(t["codes"], r["codes"].astype(np.uint64))
+    np.testing.assert_array_equal(t["left"], r["left"])
+    np.testing.assert_array_equal(t["right"], r["right"])
+    np.testing.assert_array_equal(t["node_mass"], r["node_mass"])
+    np.testing.assert_array_equal(t["node_com"], r["node_com"])
+    np.testing.assert_array_equal(pos[t["perm"]], r["node_com"][:n])
+    np.testing.assert_array_equal(m[t["perm"]], r["node_mass"][:n])
+
+
 def test_c2_full_size_forces_sampled(ctx):
     """C2 forces at full size: mixed vs FP64 walk on every body (same lists),
     approximation error vs FP64 all-pairs on a fixed 4096-body sample."""

@@ -49,6 +49,27 @@ def test_wh_hyperbolic_and_calls_compose(ctx, orc):
     assert rel_l2(gv, ov) < 1e-11
 
 
+def test_wh_kepler_drift_matches_reference_update_kepler(ctx):
+    """The device Kepler drift against the reference's own update_kepler
+    (tool_chain_impl.cpp:186-254; golden kepler_drift.npz: update_WH_planetary
+    under a zero-force solver on 400 massless bodies about a unit mass,
+    elliptic, near-parabolic and hyperbolic orbits, dt = 0.05, 40 steps). With
+    only massless bodies a Wisdom-Holman step is one Kepler drift by dt. Per
+    body, relative: 1e-11 on elliptic and hyperbolic orbits, 1e-9 near e = 1
+    (the device's sin/cos/sinh/cosh against the host's, through 40 drifts)."""
+    from conftest import golden
+    g = golden("kepler_drift.npz")
+    ctx.upload(g["pos"], g["vel"], g["m"])
+    ctx.wh_steps(Params(G=1.0, dt=float(g["dt"])), int(g["steps"]), FP64)
+    gp, gv = ctx.download()[:2]
+    e = g["e"]
+    ep = np.linalg.norm(gp[1:] - g["ref_pos"][1:], axis=1) / np.linalg.norm(g["ref_pos"][1:], axis=1)
+    ev = np.linalg.norm(gv[1:] - g["ref_vel"][1:], axis=1) / np.linalg.norm(g["ref_vel"][1:], axis=1)
+    near = (e > 0.96) & (e < 1.04)
+    assert ep[~near].max() < 1e-11 and ev[~near].max() < 1e-11, (ep[~near].max(), ev[~near].max())
+    assert ep[near].max() < 1e-9 and ev[near].max() < 1e-9, (ep[near].max(), ev[near].max())
+
+
 def test_wh_circular_orbit_closes(ctx):
     pos = np.array([[0.0, 0, 0], [1.0, 0, 0]])
     vel = np.array([[0.0, 0, 0], [0, 1.0, 0]])

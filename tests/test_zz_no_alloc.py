@@ -4,9 +4,12 @@ loops that must not allocate mid-run). It takes the caller's device arrays and
 keeps its scratch in a fixed array inside the library.
 
 Checked through the C ABI against the context-based aster_energy on two calls
-in a row (the shared scratch keeps the previous call's contents; the second
-call must not depend on them). Tolerance: relative 1e-12 on the energy,
-absolute 1e-14 on the momentum (the two paths run the same kernels).
+in a row per size (the shared scratch keeps the previous call's contents; the
+second call must not depend on them). The sizes run small, large, then small
+again, so a small call also follows a large one that filled more of the
+scratch; the last size runs on a stream of its own (the call queues its work
+there and returns). Tolerance: relative 1e-12 on the energy, absolute 1e-14 on
+the momentum (the two paths run the same kernels).
 
 This file sorts last so that a run stopping at the first failure has already
 run every other test.
@@ -39,7 +42,8 @@ def test_noalloc_energy_matches_context_energy(ref_form):
 
     f = _entry()
     dev = torch.device("cuda", 0)
-    for n, seed in ((1000, 11), (70001, 12)):
+    side = torch.cuda.Stream(device=dev)
+    for n, seed, stream in ((1000, 11, None), (70001, 12, None), (1000, 13, side)):
         pos, vel, m = gen.plummer(n, seed)
         p = Params(eps2=1e-4)
         with Context(0) as ctx:
@@ -52,9 +56,13 @@ def test_noalloc_energy_matches_context_energy(ref_form):
         for _ in range(2):
             out.fill_(float("nan"))
             torch.cuda.synchronize()
-            st = f(n, pm.data_ptr(), v4.data_ptr(), ctypes.byref(cp), ref_form, out.data_ptr(), None)
-            torch.cuda.synchronize()
+            handle = stream.cuda_stream if stream is not None else None
+            st = f(n, pm.data_ptr(), v4.data_ptr(), ctypes.byref(cp), ref_form, out.data_ptr(), handle)
             assert st == 0
+            if stream is not None:
+                stream.synchronize()  # only the stream the work was queued on
+            else:
+                torch.cuda.synchronize()
             got = out.cpu().numpy()
             assert abs(got[0] - e_ref) <= 1e-12 * abs(e_ref), (got[0], e_ref)
             np.testing.assert_allclose(got[1:], mom_ref, rtol=0, atol=1e-14)
