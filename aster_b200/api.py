@@ -29,6 +29,7 @@ NEWTON = 0x0001
 PN1 = 0x0010
 PN2 = 0x0100   # all-pairs solver and ensemble
 PN25 = 0x1000  # all-pairs solver and ensemble
+EIH = 0x10000  # with PN1, ensembles only: the N-body Einstein-Infeld-Hoffmann 1PN acceleration
 UPDATER_KDK, UPDATER_SABA, UPDATER_WH = 0, 1, 2
 COLLECT_ENERGY, COLLECT_ENERGY_ERROR, COLLECT_MOMENTUM, COLLECT_CENTER, COLLECT_DISTANCE = 0x1, 0x2, 0x4, 0x8, 0x10
 FP64 = 0

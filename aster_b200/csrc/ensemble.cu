@@ -10,6 +10,20 @@
 // drift-kick-drift compositions: leapfrog (the map of update_leapfrog,
 // tool_chain_impl.cpp:169-185) and Yoshida's (1990) fourth-order triple jump.
 //
+// Force laws: Newton; Newton + the pairwise post-Newtonian terms (PN level
+// 1: 1PN only, 2: any of 1PN/2PN/2.5PN); or (level 3, force-law bit
+// ASTER_EIH with ASTER_PN1) the N-body Einstein-Infeld-Hoffmann 1PN
+// acceleration, which adds the three-body couplings that get_pn1 leaves out
+// (Einstein, Infeld & Hoffmann 1938; Will 1993, sec. 6.2). With
+// r_ab = sqrt(|x_a - x_b|^2 + eps2), d = x_b - x_a, n_ab = -d / r_ab,
+// Phi_a = sum_{c != a} G m_c / r_ac and A_b the Newtonian acceleration of b:
+//   a_a = A_a + c^-2 G sum_{b != a} { m_b / r_ab^2 [d/r_ab B_ab + W_ab (v_a - v_b)] + 7/2 m_b A_b / r_ab }
+//   B_ab = -4 Phi_a - Phi_b + v_a^2 + 2 v_b^2 - 4 v_a.v_b - 3/2 (n_ab.v_b)^2 + 1/2 d.A_b
+//   W_ab = n_ab.(4 v_a - 3 v_b)
+// Level 3 evaluates it in two passes over the system: the first sums A and
+// Phi of every body and publishes them beside the positions, the second
+// sums the bracketed terms. For two unsoftened bodies it equals get_pn1.
+//
 // Mapping: one warp per system (at most 64 bodies: one body per lane, or two
 // when the system has more than 32), the whole state in registers for the
 // entire run; per force evaluation every lane publishes its bodies to the
@@ -26,6 +40,25 @@
 #include "pn.cuh"
 
 namespace {
+
+template <class T>
+struct T3 {
+    T x, y, z;
+};
+
+// Per-body (A, Phi) of EIH pass 1 (level 3), in shared memory after the slabs.
+template <bool MIXED>
+struct EnsAux;
+template <>
+struct EnsAux<true> {
+    using T = float;
+    using T4 = float4;
+};
+template <>
+struct EnsAux<false> {
+    using T = double;
+    using T4 = double4;
+};
 
 struct Coeffs {
     double cdt[4];  // drift coefficients x dt
@@ -133,6 +166,174 @@ __device__ __forceinline__ void accel_f64(const EnsSlab<false>& s, int n, int j0
     ax += px + qx; ay += py + qy; az += pz + qz;
 }
 
+// EIH pass 1 (level 3): Newtonian sum m_j d / r^3 and potential sum m_j / r
+// over j = j0, j0 + js, ... < n (both without G).
+template <int UNROLL>
+__device__ __forceinline__ void newton_phi_f32(const EnsSlab<true>& s, int n, int j0, int js, float4 hi, float4 lo,
+                                               float eps2, float3& aN, float& phi) {
+    float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+#pragma unroll UNROLL
+    for (int j = j0; j < n; j += js) {
+        const float4 h = s.hi[j], l = s.lo[j];
+        const float dx = (h.x - hi.x) + (l.x - lo.x);
+        const float dy = (h.y - hi.y) + (l.y - lo.y);
+        const float dz = (h.z - hi.z) + (l.z - lo.z);
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+        float inv = rsqrt_approx(r2);
+        inv = r2 > 0.f ? inv : 0.f;
+        const float mi = h.w * inv;
+        const float sN = mi * inv * inv;
+        ax = fmaf(dx, sN, ax); ay = fmaf(dy, sN, ay); az = fmaf(dz, sN, az);
+        ph += mi;
+    }
+    aN = make_float3(ax, ay, az);
+    phi = ph;
+}
+
+template <int UNROLL>
+__device__ __forceinline__ void newton_phi_f64(const EnsSlab<false>& s, int n, int j0, int js, double4 xi,
+                                               double eps2, double3& aN, double& phi) {
+    double ax = 0.0, ay = 0.0, az = 0.0, ph = 0.0;
+#pragma unroll UNROLL
+    for (int j = j0; j < n; j += js) {
+        const double4 xj = s.x[j];
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+        const double inv = r2 > 0.0 ? rsqrt(r2) : 0.0;
+        const double mi = xj.w * inv;
+        const double sN = mi * inv * inv;
+        ax = fma(dx, sN, ax); ay = fma(dy, sN, ay); az = fma(dz, sN, az);
+        ph += mi;
+    }
+    aN = make_double3(ax, ay, az);
+    phi = ph;
+}
+
+// EIH pass 2 (level 3): sum over j of m_j / r^2 [d/r B + W (v_i - v_j)] +
+// 7/2 m_j A_j / r (without G), with aux[j] = (A_j, Phi_j) published by pass
+// 1 (G included) and ai = the target's own. Zero separations contribute 0.
+template <class T, class T4, int UNROLL, class Pos>
+__device__ __forceinline__ void eih_terms(const Pos& sep, const T4* __restrict__ vs, const T4* __restrict__ aux,
+                                          int n, int j0, int js, T4 vi, T4 ai, T3<T>& S) {
+    T sx = T(0), sy = T(0), sz = T(0);
+#pragma unroll UNROLL
+    for (int j = j0; j < n; j += js) {
+        T dx, dy, dz, mj, inv;
+        sep(j, dx, dy, dz, mj, inv);
+        const T4 vj = vs[j], aj = aux[j];
+        const T inv2 = inv * inv;
+        const T vij = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
+        const T dvi = dx * vi.x + dy * vi.y + dz * vi.z;   // d.v_i = -r n.v_i
+        const T dvj = dx * vj.x + dy * vj.y + dz * vj.z;
+        const T dA = dx * aj.x + dy * aj.y + dz * aj.z;
+        const T nvj = dvj * inv;
+        const T B = T(-4) * ai.w - aj.w + vi.w + T(2) * vj.w - T(4) * vij - T(1.5) * nvj * nvj + T(0.5) * dA;
+        const T W = (T(3) * dvj - T(4) * dvi) * inv;
+        const T f = mj * inv2, fb = f * inv * B, g7 = T(3.5) * mj * inv;
+        sx += fb * dx + f * W * (vi.x - vj.x) + g7 * aj.x;
+        sy += fb * dy + f * W * (vi.y - vj.y) + g7 * aj.y;
+        sz += fb * dz + f * W * (vi.z - vj.z) + g7 * aj.z;
+    }
+    S.x = sx; S.y = sy; S.z = sz;
+}
+
+// Separation, mass and inverse distance of source j from the target, FP32
+// from the double-single slab (mixed) or FP64.
+struct SepF32 {
+    const EnsSlab<true>& s;
+    float4 hi, lo;
+    float eps2;
+    __device__ __forceinline__ void operator()(int j, float& dx, float& dy, float& dz, float& mj, float& inv) const {
+        const float4 h = s.hi[j], l = s.lo[j];
+        dx = (h.x - hi.x) + (l.x - lo.x);
+        dy = (h.y - hi.y) + (l.y - lo.y);
+        dz = (h.z - hi.z) + (l.z - lo.z);
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+        const float iv = rsqrt_approx(r2);
+        inv = r2 > 0.f ? iv : 0.f;
+        mj = h.w;
+    }
+};
+struct SepF64 {
+    const EnsSlab<false>& s;
+    double4 xi;
+    double eps2;
+    __device__ __forceinline__ void operator()(int j, double& dx, double& dy, double& dz, double& mj,
+                                               double& inv) const {
+        const double4 xj = s.x[j];
+        dx = xj.x - xi.x; dy = xj.y - xi.y; dz = xj.z - xi.z;
+        const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+        inv = r2 > 0.0 ? rsqrt(r2) : 0.0;
+        mj = xj.w;
+    }
+};
+
+// Sum of the lps partial sums of the aligned lane groups (the sources of a
+// body beyond the first 32 are split among lps lanes); afterwards lane s holds
+// the total of group s (the owner of body 32 + s) when `own`.
+__device__ __forceinline__ double group_total(double v, int lps, int lane, bool own) {
+    for (int o = lps >> 1; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return __shfl_sync(0xffffffffu, v, own ? lane * lps : 0);
+}
+
+// Level-3 (EIH) accelerations of the warp's bodies lane and 32 + lane:
+// pass 1 sums A and Phi of every body and publishes them to aux, pass 2 the
+// EIH terms. a[q] = A + c^-2 G S (FP64 results; FP32 pair arithmetic when
+// MIXED).
+template <bool MIXED, int UNROLL>
+__device__ __forceinline__ void eih_accel(const EnsSlab<MIXED>& slab, typename EnsAux<MIXED>::T4* aux, int n,
+                                          int lane, bool two, bool v0, bool v1, bool sec, int sb, int sub, int lps,
+                                          double eps2, double G, double c2, double a[2][3]) {
+    using T = typename EnsAux<MIXED>::T;
+    using T4 = typename EnsAux<MIXED>::T4;
+    double A[2][4];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        if (q == 1 && !two) { A[1][0] = A[1][1] = A[1][2] = A[1][3] = 0.0; continue; }
+        const int idx = q ? (sec ? 32 + sb : 0) : (v0 ? lane : 0);
+        const int j0 = q ? sub : 0, js = q ? lps : 1;
+        double sx, sy, sz, sp;
+        if constexpr (MIXED) {
+            float3 aN;
+            float ph;
+            newton_phi_f32<UNROLL>(slab, n, j0, js, slab.hi[idx], slab.lo[idx], (float)eps2, aN, ph);
+            sx = aN.x; sy = aN.y; sz = aN.z; sp = ph;
+        } else {
+            double3 aN;
+            newton_phi_f64<UNROLL>(slab, n, j0, js, slab.x[idx], eps2, aN, sp);
+            sx = aN.x; sy = aN.y; sz = aN.z;
+        }
+        if (q == 1) {
+            sx = group_total(sx, lps, lane, v1); sy = group_total(sy, lps, lane, v1);
+            sz = group_total(sz, lps, lane, v1); sp = group_total(sp, lps, lane, v1);
+        }
+        A[q][0] = G * sx; A[q][1] = G * sy; A[q][2] = G * sz; A[q][3] = G * sp;
+    }
+    if (v0) aux[lane] = T4{(T)A[0][0], (T)A[0][1], (T)A[0][2], (T)A[0][3]};
+    if (v1) aux[32 + lane] = T4{(T)A[1][0], (T)A[1][1], (T)A[1][2], (T)A[1][3]};
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        if (q == 1 && !two) { a[1][0] = a[1][1] = a[1][2] = 0.0; continue; }
+        const int idx = q ? (sec ? 32 + sb : 0) : (v0 ? lane : 0);
+        const int j0 = q ? sub : 0, js = q ? lps : 1;
+        T3<T> S;
+        if constexpr (MIXED)
+            eih_terms<float, float4, UNROLL>(SepF32{slab, slab.hi[idx], slab.lo[idx], (float)eps2}, slab.v, aux, n,
+                                             j0, js, slab.v[idx], aux[idx], S);
+        else
+            eih_terms<double, double4, UNROLL>(SepF64{slab, slab.x[idx], eps2}, slab.v, aux, n, j0, js,
+                                               slab.v[idx], aux[idx], S);
+        double sx = S.x, sy = S.y, sz = S.z;
+        if (q == 1) {
+            sx = group_total(sx, lps, lane, v1); sy = group_total(sy, lps, lane, v1);
+            sz = group_total(sz, lps, lane, v1);
+        }
+        const double k = G * c2;
+        a[q][0] = A[q][0] + k * sx; a[q][1] = A[q][1] + k * sy; a[q][2] = A[q][2] + k * sz;
+    }
+}
+
 template <bool MIXED, int PNL, int UNROLL, int NST>
 __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, const int32_t* __restrict__ off,
                            double4* __restrict__ pm, double4* __restrict__ vel, double G, double eps2, PnK<double> pk,
@@ -140,6 +341,10 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
                            const volatile int* __restrict__ cancel, int* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char ens_smem[];
     EnsSlab<MIXED>& slab = reinterpret_cast<EnsSlab<MIXED>*>(ens_smem)[threadIdx.x >> 5];
+    // level 3 only: 64 (A, Phi) records per warp after all the block's slabs
+    using Aux4 = typename EnsAux<MIXED>::T4;
+    Aux4* aux = reinterpret_cast<Aux4*>(ens_smem + (blockDim.x >> 5) * sizeof(EnsSlab<MIXED>)) +
+                (threadIdx.x >> 5) * 64;
     const int lane = threadIdx.x & 31;
     const float Gf = (float)G, epsf = (float)eps2;
     const PnK<float> pkf = pn_float(pk);
@@ -205,6 +410,9 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
                 }
                 __syncwarp();
                 double a[2][3];
+                if constexpr (PNL == 3) {
+                    eih_accel<MIXED, UNROLL>(slab, aux, n, lane, two, v0, v1, sec, sb, sub, lps, eps2, G, pk.c2, a);
+                } else {
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     if (q == 1 && !two) { a[1][0] = a[1][1] = a[1][2] = 0.0; continue; }
@@ -240,6 +448,7 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
                     }
                     a[q][0] = G * sx; a[q][1] = G * sy; a[q][2] = G * sz;
                 }
+                }
                 __syncwarp();
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
@@ -258,10 +467,13 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
     }
 }
 
-// FP64 energy of one system per warp (Newtonian + pairwise 1PN energy).
+// FP64 energy of one system per warp: Newtonian, plus (pn) the 1PN energy of
+// the EIH Lagrangian. Its G^2 term is (1/2) sum_a m_a Phi_a^2; for the
+// pairwise law (eih = 0) only its two-body part, sum over pairs of
+// G^2 m_i m_j (m_i + m_j) / (2 r^2), is kept.
 __global__ void k_ensemble_energy(int32_t nsys, const int32_t* __restrict__ off, const double4* __restrict__ pm,
                                   const double4* __restrict__ vel, double G, double eps2, double inv_c2, int pn,
-                                  double* __restrict__ out) {
+                                  int eih, double* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const int64_t sys = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (sys >= nsys) return;
@@ -272,6 +484,16 @@ __global__ void k_ensemble_energy(int32_t nsys, const int32_t* __restrict__ off,
         const double v2 = vi.x * vi.x + vi.y * vi.y + vi.z * vi.z;
         e += 0.5 * xi.w * v2;
         e1 += 0.375 * xi.w * v2 * v2;
+        if (pn && eih) {
+            double phi = 0.0;
+            for (int j = 0; j < n; ++j) {
+                if (j == i) continue;
+                const double4 xj = pm[b0 + j];
+                const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+                phi += G * xj.w / sqrt(dx * dx + dy * dy + dz * dz + eps2);
+            }
+            e1 += 0.5 * xi.w * phi * phi;
+        }
         for (int j = i + 1; j < n; ++j) {
             const double4 xj = pm[b0 + j], vj = vel[b0 + j];
             const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
@@ -282,7 +504,7 @@ __global__ void k_ensemble_energy(int32_t nsys, const int32_t* __restrict__ off,
             const double nvi = (dx * vi.x + dy * vi.y + dz * vi.z) / r;
             const double nvj = (dx * vj.x + dy * vj.y + dz * vj.z) / r;
             e1 += G * xi.w * xj.w / (2.0 * r) * (3.0 * (v2 + vj2) - 7.0 * vij - nvi * nvj);
-            e1 += G * G * xi.w * xj.w * (xi.w + xj.w) / (2.0 * r * r);
+            if (!eih) e1 += G * G * xi.w * xj.w * (xi.w + xj.w) / (2.0 * r * r);
         }
     }
     double t = e + (pn ? inv_c2 * e1 : 0.0);
@@ -316,7 +538,8 @@ int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_
                     bool use_graph) {
     EnsBufs& e = c->ens;
     auto kern = k.nst == 3 ? k_ensemble<MIXED, PNL, UNROLL, 3> : k_ensemble<MIXED, PNL, UNROLL, 1>;
-    const size_t smem = (size_t)wpb * sizeof(EnsSlab<MIXED>);
+    const size_t smem = (size_t)wpb * (sizeof(EnsSlab<MIXED>) +
+                                       (PNL == 3 ? 64 * sizeof(typename EnsAux<MIXED>::T4) : 0));
     if (smem > 48 * 1024) ASTER_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     ASTER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
@@ -360,6 +583,19 @@ int dispatch_unroll(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_
         case 4: return launch_ensemble<MIXED, PNL, 4>(c, p, k, nsteps, wpb, check_every, g);
         default: return launch_ensemble<MIXED, PNL, 2>(c, p, k, nsteps, wpb, check_every, g);
     }
+}
+
+// The ensemble's force law: ASTER_EIH (with ASTER_PN1, and neither 2PN nor
+// 2.5PN) selects level 3; the other bits are checked as everywhere else.
+int ens_check_params(const aster_params* p, int* level) {
+    if (!p) return ASTER_ERR_INVALID_ARG;
+    aster_params q = *p;
+    const bool eih = (q.force_law & ASTER_EIH) != 0;
+    q.force_law &= ~ASTER_EIH;
+    ASTER_TRY(aster_check_params(&q));
+    if (eih && (!(q.force_law & ASTER_PN1) || (q.force_law & (ASTER_PN2 | ASTER_PN25)))) return ASTER_ERR_UNSUPPORTED;
+    *level = eih ? 3 : pn_level(&q);
+    return ASTER_OK;
 }
 
 }  // namespace
@@ -452,7 +688,8 @@ extern "C" int aster_ensemble_download(aster_ctx* c, double* pos, double* vel) {
 extern "C" int aster_ensemble_run(aster_ctx* c, const aster_params* p, int integrator, int precision, int64_t nsteps,
                                   const aster_ensemble_config* cfg) {
     if (!c || nsteps < 0) return ASTER_ERR_INVALID_ARG;
-    ASTER_TRY(aster_check_params(p));
+    int pnl = 0;
+    ASTER_TRY(ens_check_params(p, &pnl));
     if (c->ens.nsys <= 0) return ASTER_ERR_NO_STATE;
     if (integrator != ASTER_INTEGRATOR_LEAPFROG && integrator != ASTER_INTEGRATOR_YOSHIDA4) return ASTER_ERR_INVALID_ARG;
     if (precision != ASTER_FP64 && precision != ASTER_MIXED) return ASTER_ERR_INVALID_ARG;
@@ -466,16 +703,17 @@ extern "C" int aster_ensemble_run(aster_ctx* c, const aster_params* p, int integ
     c->stats = aster_stats{};
     *c->ens.cancel_host = 0;
     const Coeffs k = make_coeffs(integrator, p->dt);
-    // PN level: 2 when a 2PN or 2.5PN term is requested, else 1 for 1PN alone
-    const int pnl = pn_level(p);
+    // PN level: 3 EIH; 2 when a 2PN or 2.5PN term is requested, else 1 for 1PN alone
     cudaEventRecord(c->ev[0], c->stream);
     int st;
     if (precision == ASTER_MIXED)
-        st = pnl == 2 ? dispatch_unroll<true, 2>(c, p, k, nsteps, wpb, unroll, check, graph)
+        st = pnl == 3 ? dispatch_unroll<true, 3>(c, p, k, nsteps, wpb, unroll, check, graph)
+           : pnl == 2 ? dispatch_unroll<true, 2>(c, p, k, nsteps, wpb, unroll, check, graph)
            : pnl == 1 ? dispatch_unroll<true, 1>(c, p, k, nsteps, wpb, unroll, check, graph)
                       : dispatch_unroll<true, 0>(c, p, k, nsteps, wpb, unroll, check, graph);
     else
-        st = pnl == 2 ? dispatch_unroll<false, 2>(c, p, k, nsteps, wpb, unroll, check, graph)
+        st = pnl == 3 ? dispatch_unroll<false, 3>(c, p, k, nsteps, wpb, unroll, check, graph)
+           : pnl == 2 ? dispatch_unroll<false, 2>(c, p, k, nsteps, wpb, unroll, check, graph)
            : pnl == 1 ? dispatch_unroll<false, 1>(c, p, k, nsteps, wpb, unroll, check, graph)
                       : dispatch_unroll<false, 0>(c, p, k, nsteps, wpb, unroll, check, graph);
     if (st != ASTER_OK) return st;
@@ -491,7 +729,8 @@ extern "C" int aster_ensemble_run(aster_ctx* c, const aster_params* p, int integ
 
 extern "C" int aster_ensemble_energy(aster_ctx* c, const aster_params* p, double* energy) {
     if (!c || !energy) return ASTER_ERR_INVALID_ARG;
-    ASTER_TRY(aster_check_params(p));
+    int pnl = 0;
+    ASTER_TRY(ens_check_params(p, &pnl));
     EnsBufs& e = c->ens;
     if (e.nsys <= 0) return ASTER_ERR_NO_STATE;
     ASTER_TRY(aster_begin(c));
@@ -502,7 +741,7 @@ extern "C" int aster_ensemble_energy(aster_ctx* c, const aster_params* p, double
     k_ensemble_energy<<<blocks, wpb * 32, 0, c->stream>>>(e.nsys, e.off.as<int32_t>(), e.pm.as<double4>(),
                                                            e.vel.as<double4>(), p->G, p->eps2,
                                                            pn ? 1.0 / (p->c * p->c) : 0.0, pn ? 1 : 0,
-                                                           c->scratch.as<double>());
+                                                           pnl == 3 ? 1 : 0, c->scratch.as<double>());
     ASTER_CUDA(cudaGetLastError());
     ASTER_CUDA(cudaMemcpyAsync(energy, c->scratch.ptr, (size_t)e.nsys * sizeof(double), cudaMemcpyDeviceToHost,
                                c->stream));

@@ -51,6 +51,11 @@ extern "C" {
 #define ASTER_PN1 0x0010  /* get_pn1, c^-2 (src/physics/tool_chain_impl.cpp:110-118)  */
 #define ASTER_PN2 0x0100  /* get_pn2, c^-4 (tool_chain_impl.cpp:79-107); all-pairs and ensemble */
 #define ASTER_PN25 0x1000 /* get_pn25, c^-5 (tool_chain_impl.cpp:65-77); all-pairs and ensemble */
+/* Not a reference bit: with ASTER_PN1, the 1PN term is the N-body
+ * Einstein-Infeld-Hoffmann acceleration (the pairwise get_pn1 terms plus the
+ * three-body couplings it leaves out). Ensemble entry points only, without
+ * ASTER_PN2/ASTER_PN25; every other entry point returns ASTER_ERR_UNSUPPORTED. */
+#define ASTER_EIH 0x10000
 
 /* ---- enums ------------------------------------------------------------- */
 #define ASTER_FP64 0   /* plain FP64 pair arithmetic                          */
@@ -255,7 +260,8 @@ int aster_energy(aster_ctx* ctx, const aster_params* p, int ref_form, double* en
  * persistent kernel (one warp per system, systems taken largest first from a
  * work counter), launched through a captured CUDA graph. The pair law is the
  * reference's (compute_gravitational / get_pn1, tool_chain_impl.cpp:110-137,
- * Newton + optional pairwise 1PN); the integrators are compositions of
+ * Newton + optional pairwise 1PN, 2PN, 2.5PN), or with ASTER_EIH the N-body
+ * Einstein-Infeld-Hoffmann 1PN acceleration; the integrators are compositions of
  * drift-kick-drift leapfrog steps: the reference's leapfrog
  * (tool_chain_impl.cpp:169-185, same map) and Yoshida's (1990) fourth-order
  * triple jump, which the reference lacks. The reference has no batched
@@ -285,8 +291,10 @@ int aster_ensemble_download(aster_ctx* ctx, double* pos, double* vel);
 int aster_ensemble_run(aster_ctx* ctx, const aster_params* p, int integrator, int precision, int64_t nsteps,
                        const aster_ensemble_config* cfg);
 /* FP64 energy per system (energy[nsys]): Newtonian with the softened
- * potential, plus the two-body 1PN (EIH) energy of every pair when the
- * force law has the PN1 bit. */
+ * potential, plus, when the force law has the PN1 bit, the 1PN energy of the
+ * EIH Lagrangian: with ASTER_EIH its full N-body form (the energy the EIH
+ * equations conserve to order c^-4), otherwise the sum of its two-body
+ * terms over pairs. */
 int aster_ensemble_energy(aster_ctx* ctx, const aster_params* p, double* energy);
 /* Thread-safe request to stop a running aster_ensemble_run. */
 int aster_ensemble_cancel(aster_ctx* ctx);

@@ -54,6 +54,7 @@
 #define PN1_FLAG 0x10
 #define PN2_FLAG 0x100
 #define PN25_FLAG 0x1000
+#define EIH_FLAG 0x10000
 
 /* ------------------------------------------------------------------------ */
 /* threading helper                                                          */
@@ -879,6 +880,73 @@ void orc_ens_coeffs(int integrator, double* c, double* d, int* nstages) {
     }
 }
 
+/* N-body 1PN accelerations of one system (n <= 64 bodies) in the
+ * Einstein-Infeld-Hoffmann form (Einstein, Infeld & Hoffmann 1938; as written
+ * in Will, Theory and Experiment in Gravitational Physics, 1993, sec. 6.2, and
+ * Poisson & Will, Gravity, 2014, sec. 9.3), the accelerations of the other
+ * bodies inside the 1PN terms taken at Newtonian order. With
+ * r_ab = sqrt(|x_a - x_b|^2 + eps2), n_ab = (x_a - x_b)/r_ab,
+ * phi_a = sum_{c != a} G m_c / r_ac and A_b the Newtonian acceleration of b:
+ *   a_a = sum_{b != a} G m_b / r_ab^2 (-n_ab) [1 + (1/c^2)(-4 phi_a - phi_b + v_a^2 + 2 v_b^2
+ *           - 4 v_a.v_b - 3/2 (n_ab.v_b)^2 + 1/2 (x_b - x_a).A_b)]
+ *       + (1/c^2) sum_{b != a} G m_b / r_ab^2 [n_ab.(4 v_a - 3 v_b)] (v_a - v_b)
+ *       + (7/(2 c^2)) sum_{b != a} G m_b A_b / r_ab
+ * For two unsoftened bodies this is the pairwise law of get_pn1
+ * (tool_chain_impl.cpp:110-118): the A_b terms give the 5 G m_a / r of its
+ * bracket (1 from phi_b, 1/2 from (x_b - x_a).A_b, 7/2 from the last sum).
+ * Beyond two bodies it adds the three-body couplings that get_pn1 omits. */
+static void ens_eih_acc(long n, const double* x, const double* v, const double* m, double G, double inv_c2,
+                        double eps2, double* acc) {
+    double phi[64], an[64 * 3];
+    for (long a = 0; a < n; ++a) {
+        double p = 0, ax = 0, ay = 0, az = 0;
+        for (long b = 0; b < n; ++b) {
+            if (b == a) continue;
+            double d[3] = {x[3 * b] - x[3 * a], x[3 * b + 1] - x[3 * a + 1], x[3 * b + 2] - x[3 * a + 2]};
+            double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
+            if (r2 == 0.0) continue;
+            double inv = 1.0 / sqrt(r2);
+            p += G * m[b] * inv;
+            double s = G * m[b] * inv * inv * inv;
+            ax += d[0] * s; ay += d[1] * s; az += d[2] * s;
+        }
+        phi[a] = p;
+        an[3 * a] = ax; an[3 * a + 1] = ay; an[3 * a + 2] = az;
+    }
+    for (long a = 0; a < n; ++a) {
+        const double* va = v + 3 * a;
+        double va2 = va[0] * va[0] + va[1] * va[1] + va[2] * va[2];
+        double pn[3] = {0, 0, 0};
+        for (long b = 0; b < n; ++b) {
+            if (b == a) continue;
+            const double* vb = v + 3 * b;
+            const double* Ab = an + 3 * b;
+            double d[3] = {x[3 * b] - x[3 * a], x[3 * b + 1] - x[3 * a + 1], x[3 * b + 2] - x[3 * a + 2]};
+            double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
+            if (r2 == 0.0) continue;
+            double inv = 1.0 / sqrt(r2);
+            double nab[3] = {-d[0] * inv, -d[1] * inv, -d[2] * inv};
+            double vb2 = vb[0] * vb[0] + vb[1] * vb[1] + vb[2] * vb[2];
+            double vab = va[0] * vb[0] + va[1] * vb[1] + va[2] * vb[2];
+            double nvb = nab[0] * vb[0] + nab[1] * vb[1] + nab[2] * vb[2];
+            double nva = nab[0] * va[0] + nab[1] * va[1] + nab[2] * va[2];
+            double dA = d[0] * Ab[0] + d[1] * Ab[1] + d[2] * Ab[2];
+            double br = -4.0 * phi[a] - phi[b] + va2 + 2.0 * vb2 - 4.0 * vab - 1.5 * nvb * nvb + 0.5 * dA;
+            double f = G * m[b] * inv * inv;
+            double w = 4.0 * nva - 3.0 * nvb;
+            double g7 = 3.5 * G * m[b] * inv;
+            for (int k = 0; k < 3; ++k) pn[k] += f * (-nab[k] * br + w * (va[k] - vb[k])) + g7 * Ab[k];
+        }
+        for (int k = 0; k < 3; ++k) acc[3 * a + k] = an[3 * a + k] + inv_c2 * pn[k];
+    }
+}
+
+/* The EIH accelerations of one system (exported for the tests). */
+void orc_eih_acc(long n, const double* x, const double* v, const double* m, double G, double inv_c, double eps2,
+                 double* acc) {
+    ens_eih_acc(n, x, v, m, G, inv_c * inv_c, eps2, acc);
+}
+
 typedef struct {
     const int64_t* off; double *pos, *vel; const double* m; double G, inv_c, eps2, dt; int pn, integrator;
     long nsteps;
@@ -898,15 +966,19 @@ static void ens_range(void* c_, long lo, long hi) {
         for (long step = 0; step < c->nsteps; ++step) {
             for (int st = 0; st < ns; ++st) {
                 for (long i = 0; i < 3 * n; ++i) x[i] += cc[st] * c->dt * v[i];
-                for (long i = 0; i < n; ++i) {
-                    double ax = 0, ay = 0, az = 0;
-                    for (long j = 0; j < n; ++j) {
-                        if (j == i) continue;
-                        orc_pair_acc(c->G, c->inv_c, c->eps2, c->pn, m[i], m[j], v + 3 * i, v + 3 * j, x + 3 * i,
-                                     x + 3 * j, a);
-                        ax += a[0]; ay += a[1]; az += a[2];
+                if ((c->pn & EIH_FLAG) && (c->pn & PN1_FLAG)) {
+                    ens_eih_acc(n, x, v, m, c->G, c->inv_c * c->inv_c, c->eps2, acc);
+                } else {
+                    for (long i = 0; i < n; ++i) {
+                        double ax = 0, ay = 0, az = 0;
+                        for (long j = 0; j < n; ++j) {
+                            if (j == i) continue;
+                            orc_pair_acc(c->G, c->inv_c, c->eps2, c->pn, m[i], m[j], v + 3 * i, v + 3 * j,
+                                         x + 3 * i, x + 3 * j, a);
+                            ax += a[0]; ay += a[1]; az += a[2];
+                        }
+                        acc[3 * i] = ax; acc[3 * i + 1] = ay; acc[3 * i + 2] = az;
                     }
-                    acc[3 * i] = ax; acc[3 * i + 1] = ay; acc[3 * i + 2] = az;
                 }
                 for (long i = 0; i < 3 * n; ++i) v[i] += dd[st] * c->dt * acc[i];
             }
@@ -929,7 +1001,11 @@ void orc_ens_run(long nsys, const int64_t* off, double* pos, double* vel, const 
  *           + sum_{i<j} G m_i m_j/(2r) (3(v_i^2 + v_j^2) - 7 v_i.v_j - (n.v_i)(n.v_j))
  *           + sum_{i<j} G^2 m_i m_j (m_i + m_j)/(2 r^2) ]
  * (the energy of the two-body Einstein-Infeld-Hoffmann Lagrangian, whose
- * equations of motion are the pairwise 1PN law). The kicks evaluate the
+ * equations of motion are the pairwise 1PN law). With the EIH bit the last
+ * sum is the N-body one, (1/2) sum_a m_a phi_a^2 with phi_a = sum_{b != a}
+ * G m_b / r_ab (the pair sum above plus the three-body terms
+ * (1/2) sum_a sum_{b != a} sum_{c != a, b} G^2 m_a m_b m_c / (r_ab r_ac)): the
+ * conserved energy of the N-body EIH Lagrangian. The kicks evaluate the
  * velocity-dependent force at the current velocity, as the reference's
  * integrators do, so the PN part is integrated to first order in dt. */
 void orc_ens_energy(long nsys, const int64_t* off, const double* pos, const double* vel, const double* m,
@@ -940,10 +1016,20 @@ void orc_ens_energy(long nsys, const int64_t* off, const double* pos, const doub
         const double* v = vel + 3 * b0;
         const double* mm = m + b0;
         double e = 0, e1 = 0;
+        const int eih = (pn & EIH_FLAG) != 0;
         for (long i = 0; i < n; ++i) {
             double v2 = v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2];
             e += 0.5 * mm[i] * v2;
             e1 += 0.375 * mm[i] * v2 * v2;
+            if (eih) {
+                double phi = 0;
+                for (long j = 0; j < n; ++j) {
+                    if (j == i) continue;
+                    double d[3] = {x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]};
+                    phi += G * mm[j] / sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2);
+                }
+                e1 += 0.5 * mm[i] * phi * phi;
+            }
             for (long j = i + 1; j < n; ++j) {
                 double d[3] = {x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]};
                 double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2);
@@ -953,7 +1039,7 @@ void orc_ens_energy(long nsys, const int64_t* off, const double* pos, const doub
                 double nvi = (d[0] * v[3 * i] + d[1] * v[3 * i + 1] + d[2] * v[3 * i + 2]) / r;
                 double nvj = (d[0] * v[3 * j] + d[1] * v[3 * j + 1] + d[2] * v[3 * j + 2]) / r;
                 e1 += G * mm[i] * mm[j] / (2.0 * r) * (3.0 * (v2 + vj2) - 7.0 * vij - nvi * nvj);
-                e1 += G * G * mm[i] * mm[j] * (mm[i] + mm[j]) / (2.0 * r * r);
+                if (!eih) e1 += G * G * mm[i] * mm[j] * (mm[i] + mm[j]) / (2.0 * r * r);
             }
         }
         e_out[s] = e + ((pn & PN1_FLAG) ? inv_c * inv_c * e1 : 0.0);

@@ -32,6 +32,7 @@ NEWTON = 0x1
 PN1 = 0x10
 PN2 = 0x100
 PN25 = 0x1000
+EIH = 0x10000  # with PN1: the N-body Einstein-Infeld-Hoffmann 1PN acceleration (ensembles)
 
 
 def _p(a, t):
@@ -202,6 +203,8 @@ class Orc:
             _I64 = ctypes.POINTER(ctypes.c_int64)
             lib.orc_ens_run.argtypes = [ctypes.c_long, _I64, _D, _D, _D, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_long]
+            lib.orc_eih_acc.argtypes = [ctypes.c_long, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, _D]
             lib.orc_ens_energy.argtypes = [ctypes.c_long, _I64, _D, _D, _D, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_int, _D]
             Orc._lib = lib
@@ -403,12 +406,23 @@ class Orc:
                              _p(vel, _D), _p(m, _D), G, inv_c, eps2, pn, integrator, dt, nsteps)
         return pos, vel
 
-    def ens_energy(self, offsets, pos, vel, m, G=1.0, c=None, eps2=0.0):
-        """Newtonian energy, plus the two-body 1PN energy when c is given."""
+    def eih_acc(self, pos, vel, m, G=1.0, c=100.0, eps2=0.0):
+        """Accelerations of one system (n <= 64) under Newton + the N-body
+        Einstein-Infeld-Hoffmann 1PN terms."""
+        pos, vel, m = _c64(pos), _c64(vel), _c64(m)
+        acc = np.zeros((len(m), 3))
+        self.lib.orc_eih_acc(len(m), _p(pos, _D), _p(vel, _D), _p(m, _D), G, 1.0 / c, eps2, _p(acc, _D))
+        return acc
+
+    def ens_energy(self, offsets, pos, vel, m, G=1.0, c=None, eps2=0.0, pn=None):
+        """Newtonian energy, plus the 1PN energy when c is given: the sum of
+        two-body terms for the pairwise law, the N-body EIH energy when pn
+        carries EIH."""
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         pos, vel, m = _c64(pos), _c64(vel), _c64(m)
         e = np.zeros(len(off) - 1)
-        pn = NEWTON | (PN1 if c else 0)
+        if pn is None:
+            pn = NEWTON | (PN1 if c else 0)
         inv_c = 1.0 / c if c else 0.0
         self.lib.orc_ens_energy(len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(pos, _D),
                                 _p(vel, _D), _p(m, _D), G, inv_c, eps2, pn, _p(e, _D))

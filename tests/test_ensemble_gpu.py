@@ -13,8 +13,8 @@ import numpy as np
 import pytest
 
 from aster_b200 import gen
-from aster_b200.api import (ERR_CANCELLED, FP64, LEAPFROG, MIXED, NEWTON, PN1, PN2, PN25, YOSHIDA4, AsterError,
-                            Params)
+from aster_b200.api import (EIH, ERR_CANCELLED, FP64, LEAPFROG, MIXED, NEWTON, PN1, PN2, PN25, YOSHIDA4,
+                            AsterError, Params)
 
 pytestmark = pytest.mark.gpu
 
@@ -192,6 +192,61 @@ def test_cancel_stops_a_running_kernel(ctx):
     # the context stays usable
     ctx.ensemble_upload(off, pos, vel, m)
     ctx.ensemble_run(P, 5, YOSHIDA4, MIXED)
+
+
+@pytest.mark.parametrize("prec,tol", [(FP64, 1e-9), (MIXED, 1e-5)])
+def test_eih_ensemble_vs_oracle(ctx, orc, prec, tol):
+    """The N-body Einstein-Infeld-Hoffmann 1PN law (force-law bit EIH) on the
+    C4 setup against the oracle's EIH (pinned in test_eih.py to the EIH
+    Lagrangian and, for two bodies, to the reference's get_pn1): positions
+    and velocities after 50 Yoshida-4 steps per system, FP64 1e-9, mixed
+    1e-5; the EIH energy per system 1e-12; and the three-body terms change the
+    velocities (against the pairwise law) by 2% of their change over the run
+    (asserted > 0.1%), far above either tolerance."""
+    pos, vel, m, off = gen.hierarchical_ensemble(96, 1004)
+    q = Params(G=1.0, c=C_LIGHT, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1 | EIH)
+    ctx.ensemble_upload(off, pos, vel, m)
+    e_gpu = ctx.ensemble_energy(q)
+    e_orc = orc.ens_energy(off, pos, vel, m, c=C_LIGHT, pn=NEWTON | PN1 | EIH)
+    assert np.abs(e_gpu - e_orc).max() <= 1e-12 * np.abs(e_orc).max()
+    ctx.ensemble_run(q, 50, YOSHIDA4, prec)
+    gp, gv = ctx.ensemble_download()
+    op, ov = orc.ens_run(off, pos, vel, m, q.dt, 50, c=C_LIGHT, integrator=YOSHIDA4, pn=NEWTON | PN1 | EIH)
+    assert _per_system_err(gp, op, off) < tol
+    assert _per_system_err(gv, ov, off) < tol
+    pp, pv = orc.ens_run(off, pos, vel, m, q.dt, 50, c=C_LIGHT, integrator=YOSHIDA4, pn=NEWTON | PN1)
+    assert np.linalg.norm(ov - pv) > 1e-3 * np.linalg.norm(ov - vel)
+
+
+def test_eih_strong_field_and_shared_lanes(ctx, orc):
+    """EIH where its three-body terms are large (c = 10, softened systems of
+    2..40 bodies, v ~ 1; systems above 32 bodies exercise the lanes that split
+    a body's sources), leapfrog, 20 steps: FP64 kernel 1e-10, mixed 1e-5."""
+    pos, vel, m, off = _strong_pn_ensemble()
+    c, eps2, dt, steps = 10.0, 1e-2, 1e-3, 20
+    q = Params(G=1.0, c=c, eps2=eps2, dt=dt, force_law=NEWTON | PN1 | EIH)
+    ctx.ensemble_upload(off, pos, vel, m)
+    ctx.ensemble_run(q, steps, LEAPFROG, FP64)
+    gp, gv = ctx.ensemble_download()
+    op, ov = orc.ens_run(off, pos, vel, m, dt, steps, c=c, eps2=eps2, integrator=LEAPFROG, pn=NEWTON | PN1 | EIH)
+    assert _per_system_err(gp, op, off) < 1e-10
+    assert _per_system_err(gv, ov, off) < 1e-10
+    ctx.ensemble_upload(off, pos, vel, m)
+    ctx.ensemble_run(q, steps, LEAPFROG, MIXED)
+    gp, gv = ctx.ensemble_download()
+    assert _per_system_err(gp, op, off) < 1e-5
+    assert _per_system_err(gv, ov, off) < 1e-5
+
+
+def test_eih_rejected_outside_ensembles_and_with_higher_orders(ctx):
+    pos, vel, m, off = gen.hierarchical_ensemble(8, 5)
+    ctx.ensemble_upload(off, pos, vel, m)
+    for law in (NEWTON | EIH, NEWTON | PN1 | PN2 | EIH):
+        with pytest.raises(AsterError):
+            ctx.ensemble_run(Params(c=100.0, force_law=law), 1, YOSHIDA4, FP64)
+    ctx.upload(pos, vel, m)
+    with pytest.raises(AsterError):
+        ctx.allpairs(Params(c=100.0, force_law=NEWTON | PN1 | EIH), FP64)
 
 
 def test_autotuner_picks_and_caches(ctx, tmp_path):

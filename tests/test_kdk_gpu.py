@@ -135,3 +135,34 @@ def test_kdk_steps_host_equals_separate_calls(ctx):
         np.testing.assert_array_equal(hp, op)
         np.testing.assert_array_equal(hv, ov)
         np.testing.assert_array_equal(ha, oa)
+
+
+def test_c3_disk_long_run_mixed_tracks_fp64():
+    """The C3 long run at reduced size: the cold exponential disk (seed of the
+    C3 workload) at N = 16384, eps = 0.002, 1000 KDK steps of dt = 1e-4 on
+    the all-pairs solver, FP64 and mixed. Energy with the softened potential
+    the force derives from (FP64 O(N^2)). Bounds: each drift |dE/E0| < 1e-6
+    (measured 1.6e-8 .. 4.4e-8 over the run, a step-size effect common to
+    both); mixed minus FP64 drift < 2e-9 (measured 1e-10); final positions
+    mixed vs FP64 relative L2 < 1e-8 (measured 5e-10); momentum: FP64
+    < 1e-15, mixed < 1e-9 (measured 3e-17 and 6e-11: the FP32 pair terms are
+    not exactly antisymmetric). The full-size run (N = 262144) is measured by
+    bench.py (allpairs.c3_drift)."""
+    from aster_b200.api import Context
+    pos, vel, m = gen.exponential_disk(16384, 1003)
+    p = Params(G=1.0, eps2=0.002 ** 2, dt=1e-4)
+    out = {}
+    with Context(0) as c:
+        for prec in (FP64, MIXED):
+            c.upload(pos, vel, m)
+            e0, _ = c.energy(p)
+            c.kdk_steps(p, 1000, SOLVER_ALLPAIRS, prec)
+            e1, mom = c.energy(p)
+            out[prec] = ((e1 - e0) / abs(e0), float(np.abs(mom).max()), c.download()[0])
+    d64, mom64, x64 = out[FP64]
+    d32, mom32, x32 = out[MIXED]
+    assert abs(d64) < 1e-6 and abs(d32) < 1e-6
+    assert abs(d32 - d64) < 2e-9, (d32, d64)
+    assert rel_l2(x32, x64) < 1e-8
+    assert mom64 < 1e-15 and mom32 < 1e-9
+    assert rel_l2(x64, pos) > 1e-4  # the disk moved
