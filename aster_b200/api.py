@@ -74,7 +74,7 @@ class CTreeView(ctypes.Structure):
 
 class CEnsembleConfig(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int32), ("unroll", ctypes.c_int32), ("check_every", ctypes.c_int32),
-                ("use_graph", ctypes.c_int32)]
+                ("use_graph", ctypes.c_int32), ("schedule", ctypes.c_int32)]
 
 
 class CRecordConfig(ctypes.Structure):
@@ -177,6 +177,7 @@ class Context:
         self._check(self.lib.aster_ctx_create(ctypes.byref(h), device, stream), "aster_ctx_create")
         self.h = h
         self.n = 0
+        self.device = device
 
     def _check(self, st: int, where: str):
         if st != OK:
@@ -365,7 +366,8 @@ class Context:
         cfg = None
         if config is not None:
             cfg = CEnsembleConfig(config.get("warps_per_block", 0), config.get("unroll", 0),
-                                  config.get("check_every", 0), int(config.get("use_graph", 1)))
+                                  config.get("check_every", 0), int(config.get("use_graph", 1)),
+                                  int(config.get("schedule", 0)))
         self._check(self.lib.aster_ensemble_run(self.h, ctypes.byref(cp), integrator, precision, nsteps,
                                                 ctypes.byref(cfg) if cfg is not None else None),
                     "aster_ensemble_run")

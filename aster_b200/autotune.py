@@ -1,13 +1,17 @@
 """Autotuner for the batched-ensemble kernel.
 
-The tunables are the launch shape of the persistent kernel: warps (systems in
-flight) per block and the unroll factor of the inner pair loop. Each candidate
+The tunables are the launch shape and the schedule of the persistent kernel:
+warps (systems in flight) per block, the unroll factor of the inner pair loop,
+and the order in which warps take systems (largest first, or upload order).
+Packing several small systems into one warp is not a tunable: at the C4 size
+distribution (n uniform in 3..64) systems of 16 or fewer bodies carry under
+2% of the pair work, so it could win at most that. Each candidate
 is timed on the caller's own ensemble (the real size distribution) for a short
 run with CUDA events inside the library, after one untimed warm-up run; the
 state is saved before and restored after, so tuning leaves the ensemble
-untouched. Results are cached in a JSON file keyed by GPU name, precision,
-integrator, force law and a histogram of the system sizes, so later runs of
-the same configuration skip the search.
+untouched. Results are cached in a JSON file keyed by the name of the
+context's GPU, precision, integrator, force law and a histogram of the system
+sizes, so later runs of the same configuration skip the search.
 """
 from __future__ import annotations
 
@@ -20,25 +24,24 @@ import numpy as np
 
 from .api import MIXED, YOSHIDA4, Context, Params
 
-DEFAULT_SPACE = {"warps_per_block": (1, 2, 4, 8), "unroll": (1, 2, 4)}
+DEFAULT_SPACE = {"warps_per_block": (1, 2, 4, 8), "unroll": (1, 2, 4), "schedule": (0, 1)}
 DEFAULT_CACHE = Path(os.environ.get("ASTER_TUNE_CACHE", Path.home() / ".cache" / "aster_b200" / "ensemble.json"))
 
 
-def _gpu_name() -> str:
+def _gpu_name(device: int) -> str:
+    """Name of CUDA device `device` (the context's, in CUDA's numbering)."""
     try:
-        import subprocess
-        out = subprocess.run(["nvidia-smi", "--query-gpu=name", "--format=csv,noheader", "-i", "0"],
-                             capture_output=True, text=True, timeout=10).stdout.strip()
-        return out or "unknown"
+        import torch
+        return torch.cuda.get_device_name(device)
     except Exception:
-        return "unknown"
+        return f"cuda{device}"
 
 
-def _key(offsets, precision, integrator, force_law) -> str:
+def _key(ctx: Context, offsets, precision, integrator, force_law) -> str:
     sizes = np.diff(np.asarray(offsets, dtype=np.int64))
     hist = np.bincount(sizes, minlength=65)[:65]
     h = hashlib.sha1(hist.tobytes()).hexdigest()[:16]
-    return f"{_gpu_name()}|p{precision}|i{integrator}|f{force_law}|n{len(sizes)}|h{h}"
+    return f"{_gpu_name(getattr(ctx, 'device', 0))}|p{precision}|i{integrator}|f{force_law}|n{len(sizes)}|h{h}"
 
 
 def tune_ensemble(ctx: Context, offsets, p: Params, integrator: int = YOSHIDA4, precision: int = MIXED,
@@ -47,7 +50,7 @@ def tune_ensemble(ctx: Context, offsets, p: Params, integrator: int = YOSHIDA4, 
     """Return the fastest config for the ensemble currently uploaded to ctx
     (offsets must be the ones uploaded). Adds "ms_per_step" and "timings"."""
     space = space or DEFAULT_SPACE
-    key = _key(offsets, precision, integrator, p.force_law)
+    key = _key(ctx, offsets, precision, integrator, p.force_law)
     cache = Path(cache) if cache else None
     if cache and cache.exists() and not force:
         table = json.loads(cache.read_text())
@@ -59,11 +62,13 @@ def tune_ensemble(ctx: Context, offsets, p: Params, integrator: int = YOSHIDA4, 
     try:
         for wpb in space["warps_per_block"]:
             for unroll in space["unroll"]:
-                cfg = {"warps_per_block": wpb, "unroll": unroll, "check_every": 256, "use_graph": 1}
-                ctx.ensemble_run(p, max(2, steps // 8), integrator, precision, cfg)   # warm-up
-                ctx.ensemble_run(p, steps, integrator, precision, cfg)
-                ms = ctx.stats()["ms_total"] / steps
-                timings.append({**cfg, "ms_per_step": ms})
+                for schedule in space.get("schedule", (0,)):
+                    cfg = {"warps_per_block": wpb, "unroll": unroll, "check_every": 256, "use_graph": 1,
+                           "schedule": schedule}
+                    ctx.ensemble_run(p, max(2, steps // 8), integrator, precision, cfg)   # warm-up
+                    ctx.ensemble_run(p, steps, integrator, precision, cfg)
+                    ms = ctx.stats()["ms_total"] / steps
+                    timings.append({**cfg, "ms_per_step": ms})
     finally:
         # restore the caller's state (masses are unchanged by a run)
         mass = _masses_of(ctx)

@@ -22,7 +22,9 @@
 //   W_ab = n_ab.(4 v_a - 3 v_b)
 // Level 3 evaluates it in two passes over the system: the first sums A and
 // Phi of every body and publishes them beside the positions, the second
-// sums the bracketed terms. For two unsoftened bodies it equals get_pn1.
+// sums the bracketed terms. Sources at zero separation (the target itself,
+// or a body at exactly its position) are left out of both sums, softened or
+// not. For two unsoftened bodies it equals get_pn1.
 //
 // Mapping: one warp per system (at most 64 bodies: one body per lane, or two
 // when the system has more than 32), the whole state in registers for the
@@ -40,11 +42,6 @@
 #include "pn.cuh"
 
 namespace {
-
-template <class T>
-struct T3 {
-    T x, y, z;
-};
 
 // Per-body (A, Phi) of EIH pass 1 (level 3), in shared memory after the slabs.
 template <bool MIXED>
@@ -86,11 +83,18 @@ Coeffs make_coeffs(int integrator, double dt) {
 
 template <bool MIXED>
 struct EnsSlab;
+// Mixed slab, pair-interleaved: element k of each array holds bodies 2k and
+// 2k + 1, so that every paired FP32 operand is one aligned register pair
+// (positions double-single, hi + lo). Bodies past the system's size hold
+// zeros (zero mass), so a half-used last pair contributes nothing.
 template <>
 struct EnsSlab<true> {
-    float4 hi[64];  // (x_hi, y_hi, z_hi, m)
-    float4 lo[64];  // (x_lo, y_lo, z_lo, 0)
-    float4 v[64];   // (vx, vy, vz, |v|^2)
+    float4 A[32];  // (x_hi, x_hi', y_hi, y_hi')   ' = the odd body of the pair
+    float4 B[32];  // (z_hi, z_hi', m, m')
+    float4 C[32];  // (x_lo, x_lo', y_lo, y_lo')
+    float4 D[32];  // (z_lo, z_lo', vz, vz')
+    float4 E[32];  // (vx, vx', vy, vy')
+    float2 F[32];  // (|v|^2, |v'|^2)
 };
 template <>
 struct EnsSlab<false> {
@@ -98,40 +102,147 @@ struct EnsSlab<false> {
     double4 v[64];  // (vx, vy, vz, |v|^2)
 };
 
-// Sums over j = j0, j0 + js, ... < n (js > 1: the lanes that share a target
-// split its sources).
-template <int PNL, int UNROLL>
-__device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int n, int j0, int js, float4 hi, float4 lo,
-                                          float4 vi, float eps2, float G, const PnK<float>& k, float3& aN, float3& a1,
-                                          float3& a2) {
-    float ax = 0.f, ay = 0.f, az = 0.f, px = 0.f, py = 0.f, pz = 0.f, qx = 0.f, qy = 0.f, qz = 0.f;
-#pragma unroll UNROLL
-    for (int j = j0; j < n; j += js) {
-        const float4 h = s.hi[j], l = s.lo[j];
-        const float dx = (h.x - hi.x) + (l.x - lo.x);
-        const float dy = (h.y - hi.y) + (l.y - lo.y);
-        const float dz = (h.z - hi.z) + (l.z - lo.z);
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-        float inv = rsqrt_approx(r2);
-        inv = r2 > 0.f ? inv : 0.f;
-        const float inv2 = inv * inv;
-        const float sN = h.w * inv * inv2;
-        ax = fmaf(dx, sN, ax); ay = fmaf(dy, sN, ay); az = fmaf(dz, sN, az);
-        if (PNL > 0) {
-            const float4 vj = s.v[j];
-            PnPair<float> q;
-            q.nx = -dx * inv; q.ny = -dy * inv; q.nz = -dz * inv;
-            q.dvx = vi.x - vj.x; q.dvy = vi.y - vj.y; q.dvz = vi.z - vj.z;
-            q.inv = inv; q.inv2 = inv2; q.mi = hi.w; q.mj = h.w; q.vi2 = vi.w; q.vj2 = vj.w;
-            q.v12 = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
-            q.nv1 = q.nx * vi.x + q.ny * vi.y + q.nz * vi.z;
-            q.nv2 = q.nx * vj.x + q.ny * vj.y + q.nz * vj.z;
-            q.G = G;
-            pn_terms<PNL>(k, q, px, py, pz, qx, qy, qz);
-        }
+// Float index of body b's half in a pair-interleaved float4 array (its x
+// half; the y half is 2 further on).
+__device__ __forceinline__ int pslot(int b) { return ((b >> 1) << 2) | (b & 1); }
+
+// One body of the mixed slab as scalars.
+struct BodyF32 {
+    float hx, hy, hz, m, lx, ly, lz, vx, vy, vz, w;
+};
+__device__ __forceinline__ BodyF32 slab_body(const EnsSlab<true>& s, int b) {
+    const float* A = reinterpret_cast<const float*>(s.A);
+    const float* B = reinterpret_cast<const float*>(s.B);
+    const float* C = reinterpret_cast<const float*>(s.C);
+    const float* D = reinterpret_cast<const float*>(s.D);
+    const float* E = reinterpret_cast<const float*>(s.E);
+    const float* F = reinterpret_cast<const float*>(s.F);
+    const int o = pslot(b);
+    return BodyF32{A[o], A[o + 2], B[o], B[o + 2], C[o], C[o + 2], D[o], E[o], E[o + 2], D[o + 2], F[b]};
+}
+__device__ __forceinline__ void slab_put(EnsSlab<true>& s, int b, const double4& x, const double4& v) {
+    float* A = reinterpret_cast<float*>(s.A);
+    float* B = reinterpret_cast<float*>(s.B);
+    float* C = reinterpret_cast<float*>(s.C);
+    float* D = reinterpret_cast<float*>(s.D);
+    float* E = reinterpret_cast<float*>(s.E);
+    float* F = reinterpret_cast<float*>(s.F);
+    const int o = pslot(b);
+    float h, l;
+    ds_split(x.x, h, l); A[o] = h; C[o] = l;
+    ds_split(x.y, h, l); A[o + 2] = h; C[o + 2] = l;
+    ds_split(x.z, h, l); B[o] = h; D[o] = l;
+    B[o + 2] = (float)x.w;
+    D[o + 2] = (float)v.z;
+    E[o] = (float)v.x;
+    E[o + 2] = (float)v.y;
+    F[b] = (float)(v.x * v.x + v.y * v.y + v.z * v.z);
+}
+
+// Per target: minus its double-single position, broadcast to both halves.
+struct TargetX2 {
+    float2 nhx, nhy, nhz, nlx, nly, nlz;
+    __device__ __forceinline__ explicit TargetX2(const BodyF32& t)
+        : nhx(make_float2(-t.hx, -t.hx)), nhy(make_float2(-t.hy, -t.hy)), nhz(make_float2(-t.hz, -t.hz)),
+          nlx(make_float2(-t.lx, -t.lx)), nly(make_float2(-t.ly, -t.ly)), nlz(make_float2(-t.lz, -t.lz)) {}
+    // d = x_j - x_i for the pair in slot q: (h_j - h_i) + (l_j - l_i)
+    __device__ __forceinline__ void sep(const EnsSlab<true>& s, int q, float2& dx, float2& dy, float2& dz) const {
+        const float4 a = s.A[q], b = s.B[q], c = s.C[q], d = s.D[q];
+        dx = __fadd2_rn(__fadd2_rn(make_float2(a.x, a.y), nhx), __fadd2_rn(make_float2(c.x, c.y), nlx));
+        dy = __fadd2_rn(__fadd2_rn(make_float2(a.z, a.w), nhy), __fadd2_rn(make_float2(c.z, c.w), nly));
+        dz = __fadd2_rn(__fadd2_rn(make_float2(b.x, b.y), nhz), __fadd2_rn(make_float2(d.x, d.y), nlz));
     }
-    aN = make_float3(ax, ay, az);
-    a1 = make_float3(px, py, pz);
+};
+
+// r^-1 of both halves; a zero r^2 (the target itself, unsoftened) gives 0.
+__device__ __forceinline__ float2 inv_r_x2(const float2 dx, const float2 dy, const float2 dz, const float2 eps2) {
+    float2 r2 = __ffma2_rn(dz, dz, eps2);
+    r2 = __ffma2_rn(dy, dy, r2);
+    r2 = __ffma2_rn(dx, dx, r2);
+    float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    inv.x = r2.x > 0.f ? inv.x : 0.f;
+    inv.y = r2.y > 0.f ? inv.y : 0.f;
+    return inv;
+}
+
+// EIH form: r^-1 with r^2 = |d|^2 + eps2, 0 where d itself is zero. With
+// softening the target's own slot has r^2 = eps2 > 0; its potential m / r and
+// 7/2 m A / r terms must not count, so the guard is on |d|^2.
+__device__ __forceinline__ float2 inv_r_x2_nz(const float2 dx, const float2 dy, const float2 dz, const float2 eps2) {
+    const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+    const float2 r2 = __fadd2_rn(d2, eps2);
+    float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    inv.x = d2.x > 0.f ? inv.x : 0.f;
+    inv.y = d2.y > 0.f ? inv.y : 0.f;
+    return inv;
+}
+
+// Mixed accelerations of target t (without G): sums over the source pairs
+// q = q0, q0 + qs, ... < np (qs > 1: the lanes that share a target split its
+// sources). Levels 0 and 1: two sources per paired FP32 instruction; level 2
+// (any of 1PN/2PN/2.5PN by flags): one source at a time with the pair terms
+// of pn.cuh. The Newtonian, 1PN and 2PN + 2.5PN sums are kept apart.
+template <int PNL, int UNROLL>
+__device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int np, int q0, int qs, const BodyF32& t,
+                                          float eps2, float G, const PnK<float>& k, float3& aN, float3& a1,
+                                          float3& a2) {
+    const TargetX2 tx(t);
+    const float2 e2 = make_float2(eps2, eps2);
+    float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax, px = ax, py = ax, pz = ax;
+    float qx = 0.f, qy = 0.f, qz = 0.f;
+    if constexpr (PNL == 0) {
+#pragma unroll UNROLL
+        for (int q = q0; q < np; q += qs) {
+            float2 dx, dy, dz;
+            tx.sep(s, q, dx, dy, dz);
+            const float4 b = s.B[q];
+            const float2 inv = inv_r_x2(dx, dy, dz, e2);
+            const float2 sN = __fmul2_rn(__fmul2_rn(make_float2(b.z, b.w), inv), __fmul2_rn(inv, inv));
+            ax = __ffma2_rn(dx, sN, ax);
+            ay = __ffma2_rn(dy, sN, ay);
+            az = __ffma2_rn(dz, sN, az);
+        }
+    } else if constexpr (PNL == 1) {
+        const float2 vix = make_float2(t.vx, t.vx), viy = make_float2(t.vy, t.vy), viz = make_float2(t.vz, t.vz);
+        const float2 nvi2 = make_float2(-t.w, -t.w), mi5 = make_float2(5.f * t.m, 5.f * t.m);
+        const float2 G2 = make_float2(G, G), c2 = make_float2(k.c2, k.c2);
+#pragma unroll UNROLL
+        for (int q = q0; q < np; q += qs) {
+            float2 dx, dy, dz;
+            tx.sep(s, q, dx, dy, dz);
+            const float4 b = s.B[q], d = s.D[q], e = s.E[q];
+            newton_pn1_x2<true>(dx, dy, dz, make_float2(b.z, b.w), make_float2(e.x, e.y), make_float2(e.z, e.w),
+                                make_float2(d.z, d.w), s.F[q], vix, viy, viz, nvi2, mi5, e2, G2, c2, ax, ay, az, px,
+                                py, pz);
+        }
+    } else {
+        float sx = 0.f, sy = 0.f, sz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
+        for (int j = 2 * q0; j < 2 * np; j += (j & 1) ? 2 * qs - 1 : 1) {  // both bodies of each visited pair
+            const BodyF32 o = slab_body(s, j);
+            const float dx = (o.hx - t.hx) + (o.lx - t.lx);
+            const float dy = (o.hy - t.hy) + (o.ly - t.ly);
+            const float dz = (o.hz - t.hz) + (o.lz - t.lz);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+            float inv = rsqrt_approx(r2);
+            inv = r2 > 0.f ? inv : 0.f;
+            const float inv2 = inv * inv;
+            const float sN = o.m * inv * inv2;
+            sx = fmaf(dx, sN, sx); sy = fmaf(dy, sN, sy); sz = fmaf(dz, sN, sz);
+            PnPair<float> w;
+            w.nx = -dx * inv; w.ny = -dy * inv; w.nz = -dz * inv;
+            w.dvx = t.vx - o.vx; w.dvy = t.vy - o.vy; w.dvz = t.vz - o.vz;
+            w.inv = inv; w.inv2 = inv2; w.mi = t.m; w.mj = o.m; w.vi2 = t.w; w.vj2 = o.w;
+            w.v12 = t.vx * o.vx + t.vy * o.vy + t.vz * o.vz;
+            w.nv1 = w.nx * t.vx + w.ny * t.vy + w.nz * t.vz;
+            w.nv2 = w.nx * o.vx + w.ny * o.vy + w.nz * o.vz;
+            w.G = G;
+            pn_terms<PNL>(k, w, rx, ry, rz, qx, qy, qz);
+        }
+        ax.x = sx; ay.x = sy; az.x = sz;
+        px.x = rx; py.x = ry; pz.x = rz;
+    }
+    aN = make_float3(ax.x + ax.y, ay.x + ay.y, az.x + az.y);
+    a1 = make_float3(px.x + px.y, py.x + py.y, pz.x + pz.y);
     a2 = make_float3(qx, qy, qz);
 }
 
@@ -167,27 +278,28 @@ __device__ __forceinline__ void accel_f64(const EnsSlab<false>& s, int n, int j0
 }
 
 // EIH pass 1 (level 3): Newtonian sum m_j d / r^3 and potential sum m_j / r
-// over j = j0, j0 + js, ... < n (both without G).
+// (both without G), mixed: source pairs q = q0, q0 + qs, ... < np.
 template <int UNROLL>
-__device__ __forceinline__ void newton_phi_f32(const EnsSlab<true>& s, int n, int j0, int js, float4 hi, float4 lo,
+__device__ __forceinline__ void newton_phi_f32(const EnsSlab<true>& s, int np, int q0, int qs, const BodyF32& t,
                                                float eps2, float3& aN, float& phi) {
-    float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+    const TargetX2 tx(t);
+    const float2 e2 = make_float2(eps2, eps2);
+    float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax, ph = ax;
 #pragma unroll UNROLL
-    for (int j = j0; j < n; j += js) {
-        const float4 h = s.hi[j], l = s.lo[j];
-        const float dx = (h.x - hi.x) + (l.x - lo.x);
-        const float dy = (h.y - hi.y) + (l.y - lo.y);
-        const float dz = (h.z - hi.z) + (l.z - lo.z);
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-        float inv = rsqrt_approx(r2);
-        inv = r2 > 0.f ? inv : 0.f;
-        const float mi = h.w * inv;
-        const float sN = mi * inv * inv;
-        ax = fmaf(dx, sN, ax); ay = fmaf(dy, sN, ay); az = fmaf(dz, sN, az);
-        ph += mi;
+    for (int q = q0; q < np; q += qs) {
+        float2 dx, dy, dz;
+        tx.sep(s, q, dx, dy, dz);
+        const float4 b = s.B[q];
+        const float2 inv = inv_r_x2_nz(dx, dy, dz, e2);
+        const float2 mi = __fmul2_rn(make_float2(b.z, b.w), inv);
+        const float2 sN = __fmul2_rn(mi, __fmul2_rn(inv, inv));
+        ax = __ffma2_rn(dx, sN, ax);
+        ay = __ffma2_rn(dy, sN, ay);
+        az = __ffma2_rn(dz, sN, az);
+        ph = __fadd2_rn(ph, mi);
     }
-    aN = make_float3(ax, ay, az);
-    phi = ph;
+    aN = make_float3(ax.x + ax.y, ay.x + ay.y, az.x + az.y);
+    phi = ph.x + ph.y;
 }
 
 template <int UNROLL>
@@ -198,8 +310,8 @@ __device__ __forceinline__ void newton_phi_f64(const EnsSlab<false>& s, int n, i
     for (int j = j0; j < n; j += js) {
         const double4 xj = s.x[j];
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-        const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-        const double inv = r2 > 0.0 ? rsqrt(r2) : 0.0;
+        const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+        const double inv = d2 > 0.0 ? rsqrt(d2 + eps2) : 0.0;  // not the target itself
         const double mi = xj.w * inv;
         const double sN = mi * inv * inv;
         ax = fma(dx, sN, ax); ay = fma(dy, sN, ay); az = fma(dz, sN, az);
@@ -210,63 +322,84 @@ __device__ __forceinline__ void newton_phi_f64(const EnsSlab<false>& s, int n, i
 }
 
 // EIH pass 2 (level 3): sum over j of m_j / r^2 [d/r B + W (v_i - v_j)] +
-// 7/2 m_j A_j / r (without G), with aux[j] = (A_j, Phi_j) published by pass
-// 1 (G included) and ai = the target's own. Zero separations contribute 0.
-template <class T, class T4, int UNROLL, class Pos>
-__device__ __forceinline__ void eih_terms(const Pos& sep, const T4* __restrict__ vs, const T4* __restrict__ aux,
-                                          int n, int j0, int js, T4 vi, T4 ai, T3<T>& S) {
-    T sx = T(0), sy = T(0), sz = T(0);
+// 7/2 m_j A_j / r (without G), with (A_j, Phi_j) published by pass 1 (G
+// included). Zero separations contribute 0. Mixed: source pairs q = q0,
+// q0 + qs, ... < np of the pair-interleaved slab, aux = (A_x, A_x', A_y, A_y')
+// in auxA and (A_z, A_z', Phi, Phi') in auxB; Ki = -4 Phi_i + |v_i|^2.
+template <int UNROLL>
+__device__ __forceinline__ void eih_terms_f32(const EnsSlab<true>& s, const float4* __restrict__ auxA,
+                                              const float4* __restrict__ auxB, int np, int q0, int qs,
+                                              const BodyF32& t, float Phi_i, float eps2, float3& S) {
+    const TargetX2 tx(t);
+    const float2 e2 = make_float2(eps2, eps2);
+    const float2 vix = make_float2(t.vx, t.vx), viy = make_float2(t.vy, t.vy), viz = make_float2(t.vz, t.vz);
+    const float ki = fmaf(-4.f, Phi_i, t.w);
+    const float2 Ki = make_float2(ki, ki);
+    const float2 m1 = make_float2(-1.f, -1.f);
+    float2 sx = make_float2(0.f, 0.f), sy = sx, sz = sx;
+#pragma unroll UNROLL
+    for (int q = q0; q < np; q += qs) {
+        float2 dx, dy, dz;
+        tx.sep(s, q, dx, dy, dz);
+        const float4 b = s.B[q], d = s.D[q], e = s.E[q], xa = auxA[q], xb = auxB[q];
+        const float2 vj2 = s.F[q];
+        const float2 inv = inv_r_x2_nz(dx, dy, dz, e2);
+        const float2 mj = make_float2(b.z, b.w);
+        const float2 vjx = make_float2(e.x, e.y), vjy = make_float2(e.z, e.w), vjz = make_float2(d.z, d.w);
+        const float2 Ajx = make_float2(xa.x, xa.y), Ajy = make_float2(xa.z, xa.w), Ajz = make_float2(xb.x, xb.y);
+        const float2 Pj = make_float2(xb.z, xb.w);
+        const float2 vij = __ffma2_rn(vix, vjx, __ffma2_rn(viy, vjy, __fmul2_rn(viz, vjz)));
+        const float2 dvi = __ffma2_rn(dx, vix, __ffma2_rn(dy, viy, __fmul2_rn(dz, viz)));
+        const float2 dvj = __ffma2_rn(dx, vjx, __ffma2_rn(dy, vjy, __fmul2_rn(dz, vjz)));
+        const float2 dA = __ffma2_rn(dx, Ajx, __ffma2_rn(dy, Ajy, __fmul2_rn(dz, Ajz)));
+        const float2 nvj = __fmul2_rn(dvj, inv);
+        // B = Ki - Phi_j + 2 |v_j|^2 - 4 v_i.v_j - 3/2 (n.v_j)^2 + 1/2 d.A_j
+        float2 B = __ffma2_rn(Pj, m1, Ki);
+        B = __ffma2_rn(vj2, make_float2(2.f, 2.f), B);
+        B = __ffma2_rn(vij, make_float2(-4.f, -4.f), B);
+        B = __ffma2_rn(__fmul2_rn(nvj, nvj), make_float2(-1.5f, -1.5f), B);
+        B = __ffma2_rn(dA, make_float2(0.5f, 0.5f), B);
+        // W = n.(4 v_i - 3 v_j) = (3 d.v_j - 4 d.v_i) / r
+        const float2 W = __fmul2_rn(__ffma2_rn(dvj, make_float2(3.f, 3.f), __fmul2_rn(dvi, make_float2(-4.f, -4.f))),
+                                    inv);
+        const float2 f = __fmul2_rn(mj, __fmul2_rn(inv, inv));
+        const float2 fb = __fmul2_rn(__fmul2_rn(f, inv), B);
+        const float2 fW = __fmul2_rn(f, W);
+        const float2 g7 = __fmul2_rn(__fmul2_rn(mj, make_float2(3.5f, 3.5f)), inv);
+        sx = __ffma2_rn(g7, Ajx, __ffma2_rn(fW, __ffma2_rn(vjx, m1, vix), __ffma2_rn(fb, dx, sx)));
+        sy = __ffma2_rn(g7, Ajy, __ffma2_rn(fW, __ffma2_rn(vjy, m1, viy), __ffma2_rn(fb, dy, sy)));
+        sz = __ffma2_rn(g7, Ajz, __ffma2_rn(fW, __ffma2_rn(vjz, m1, viz), __ffma2_rn(fb, dz, sz)));
+    }
+    S = make_float3(sx.x + sx.y, sy.x + sy.y, sz.x + sz.y);
+}
+
+// FP64: sources j = j0, j0 + js, ... < n; aux[j] = (A_j, Phi_j).
+template <int UNROLL>
+__device__ __forceinline__ void eih_terms_f64(const EnsSlab<false>& s, const double4* __restrict__ aux, int n,
+                                              int j0, int js, double4 xi, double4 vi, double4 ai, double eps2,
+                                              double3& S) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
 #pragma unroll UNROLL
     for (int j = j0; j < n; j += js) {
-        T dx, dy, dz, mj, inv;
-        sep(j, dx, dy, dz, mj, inv);
-        const T4 vj = vs[j], aj = aux[j];
-        const T inv2 = inv * inv;
-        const T vij = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
-        const T dvi = dx * vi.x + dy * vi.y + dz * vi.z;   // d.v_i = -r n.v_i
-        const T dvj = dx * vj.x + dy * vj.y + dz * vj.z;
-        const T dA = dx * aj.x + dy * aj.y + dz * aj.z;
-        const T nvj = dvj * inv;
-        const T B = T(-4) * ai.w - aj.w + vi.w + T(2) * vj.w - T(4) * vij - T(1.5) * nvj * nvj + T(0.5) * dA;
-        const T W = (T(3) * dvj - T(4) * dvi) * inv;
-        const T f = mj * inv2, fb = f * inv * B, g7 = T(3.5) * mj * inv;
+        const double4 xj = s.x[j], vj = s.v[j], aj = aux[j];
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+        const double inv = d2 > 0.0 ? rsqrt(d2 + eps2) : 0.0;  // not the target itself
+        const double inv2 = inv * inv;
+        const double vij = vi.x * vj.x + vi.y * vj.y + vi.z * vj.z;
+        const double dvi = dx * vi.x + dy * vi.y + dz * vi.z;
+        const double dvj = dx * vj.x + dy * vj.y + dz * vj.z;
+        const double dA = dx * aj.x + dy * aj.y + dz * aj.z;
+        const double nvj = dvj * inv;
+        const double B = -4.0 * ai.w - aj.w + vi.w + 2.0 * vj.w - 4.0 * vij - 1.5 * nvj * nvj + 0.5 * dA;
+        const double W = (3.0 * dvj - 4.0 * dvi) * inv;
+        const double f = xj.w * inv2, fb = f * inv * B, g7 = 3.5 * xj.w * inv;
         sx += fb * dx + f * W * (vi.x - vj.x) + g7 * aj.x;
         sy += fb * dy + f * W * (vi.y - vj.y) + g7 * aj.y;
         sz += fb * dz + f * W * (vi.z - vj.z) + g7 * aj.z;
     }
-    S.x = sx; S.y = sy; S.z = sz;
+    S = make_double3(sx, sy, sz);
 }
-
-// Separation, mass and inverse distance of source j from the target, FP32
-// from the double-single slab (mixed) or FP64.
-struct SepF32 {
-    const EnsSlab<true>& s;
-    float4 hi, lo;
-    float eps2;
-    __device__ __forceinline__ void operator()(int j, float& dx, float& dy, float& dz, float& mj, float& inv) const {
-        const float4 h = s.hi[j], l = s.lo[j];
-        dx = (h.x - hi.x) + (l.x - lo.x);
-        dy = (h.y - hi.y) + (l.y - lo.y);
-        dz = (h.z - hi.z) + (l.z - lo.z);
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-        const float iv = rsqrt_approx(r2);
-        inv = r2 > 0.f ? iv : 0.f;
-        mj = h.w;
-    }
-};
-struct SepF64 {
-    const EnsSlab<false>& s;
-    double4 xi;
-    double eps2;
-    __device__ __forceinline__ void operator()(int j, double& dx, double& dy, double& dz, double& mj,
-                                               double& inv) const {
-        const double4 xj = s.x[j];
-        dx = xj.x - xi.x; dy = xj.y - xi.y; dz = xj.z - xi.z;
-        const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-        inv = r2 > 0.0 ? rsqrt(r2) : 0.0;
-        mj = xj.w;
-    }
-};
 
 // Sum of the lps partial sums of the aligned lane groups (the sources of a
 // body beyond the first 32 are split among lps lanes); afterwards lane s holds
@@ -279,52 +412,70 @@ __device__ __forceinline__ double group_total(double v, int lps, int lane, bool 
 // Level-3 (EIH) accelerations of the warp's bodies lane and 32 + lane:
 // pass 1 sums A and Phi of every body and publishes them to aux, pass 2 the
 // EIH terms. a[q] = A + c^-2 G S (FP64 results; FP32 pair arithmetic when
-// MIXED).
+// MIXED, with aux pair-interleaved like the slab: 32 float4 of
+// (A_x, A_x', A_y, A_y') then 32 of (A_z, A_z', Phi, Phi')).
 template <bool MIXED, int UNROLL>
 __device__ __forceinline__ void eih_accel(const EnsSlab<MIXED>& slab, typename EnsAux<MIXED>::T4* aux, int n,
                                           int lane, bool two, bool v0, bool v1, bool sec, int sb, int sub, int lps,
                                           double eps2, double G, double c2, double a[2][3]) {
-    using T = typename EnsAux<MIXED>::T;
-    using T4 = typename EnsAux<MIXED>::T4;
+    const int np = (n + 1) >> 1;
     double A[2][4];
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         if (q == 1 && !two) { A[1][0] = A[1][1] = A[1][2] = A[1][3] = 0.0; continue; }
         const int idx = q ? (sec ? 32 + sb : 0) : (v0 ? lane : 0);
-        const int j0 = q ? sub : 0, js = q ? lps : 1;
         double sx, sy, sz, sp;
         if constexpr (MIXED) {
             float3 aN;
             float ph;
-            newton_phi_f32<UNROLL>(slab, n, j0, js, slab.hi[idx], slab.lo[idx], (float)eps2, aN, ph);
+            newton_phi_f32<UNROLL>(slab, np, q ? sub : 0, q ? lps : 1, slab_body(slab, idx), (float)eps2, aN, ph);
             sx = aN.x; sy = aN.y; sz = aN.z; sp = ph;
         } else {
             double3 aN;
-            newton_phi_f64<UNROLL>(slab, n, j0, js, slab.x[idx], eps2, aN, sp);
+            newton_phi_f64<UNROLL>(slab, n, q ? sub : 0, q ? lps : 1, slab.x[idx], eps2, aN, sp);
             sx = aN.x; sy = aN.y; sz = aN.z;
         }
         if (q == 1) {
             sx = group_total(sx, lps, lane, v1); sy = group_total(sy, lps, lane, v1);
             sz = group_total(sz, lps, lane, v1); sp = group_total(sp, lps, lane, v1);
         }
-        A[q][0] = G * sx; A[q][1] = G * sy; A[q][2] = G * sz; A[q][3] = G * sp;
+        const bool valid = q ? v1 : v0;  // zeros past n: a half-used last pair adds nothing
+        A[q][0] = valid ? G * sx : 0.0; A[q][1] = valid ? G * sy : 0.0;
+        A[q][2] = valid ? G * sz : 0.0; A[q][3] = valid ? G * sp : 0.0;
     }
-    if (v0) aux[lane] = T4{(T)A[0][0], (T)A[0][1], (T)A[0][2], (T)A[0][3]};
-    if (v1) aux[32 + lane] = T4{(T)A[1][0], (T)A[1][1], (T)A[1][2], (T)A[1][3]};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        if (q == 1 && !two) continue;
+        const int b = lane + 32 * q;
+        if constexpr (MIXED) {
+            float* xa = reinterpret_cast<float*>(aux);
+            float* xb = reinterpret_cast<float*>(aux + 32);
+            const int o = pslot(b);
+            xa[o] = (float)A[q][0]; xa[o + 2] = (float)A[q][1];
+            xb[o] = (float)A[q][2]; xb[o + 2] = (float)A[q][3];
+        } else {
+            if (q ? v1 : v0) aux[b] = make_double4(A[q][0], A[q][1], A[q][2], A[q][3]);
+        }
+    }
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         if (q == 1 && !two) { a[1][0] = a[1][1] = a[1][2] = 0.0; continue; }
         const int idx = q ? (sec ? 32 + sb : 0) : (v0 ? lane : 0);
-        const int j0 = q ? sub : 0, js = q ? lps : 1;
-        T3<T> S;
-        if constexpr (MIXED)
-            eih_terms<float, float4, UNROLL>(SepF32{slab, slab.hi[idx], slab.lo[idx], (float)eps2}, slab.v, aux, n,
-                                             j0, js, slab.v[idx], aux[idx], S);
-        else
-            eih_terms<double, double4, UNROLL>(SepF64{slab, slab.x[idx], eps2}, slab.v, aux, n, j0, js,
-                                               slab.v[idx], aux[idx], S);
-        double sx = S.x, sy = S.y, sz = S.z;
+        double sx, sy, sz;
+        if constexpr (MIXED) {
+            const float4* xa = reinterpret_cast<const float4*>(aux);
+            const float phi_i = reinterpret_cast<const float*>(aux + 32)[pslot(idx) + 2];
+            float3 S;
+            eih_terms_f32<UNROLL>(slab, xa, xa + 32, np, q ? sub : 0, q ? lps : 1, slab_body(slab, idx), phi_i,
+                                  (float)eps2, S);
+            sx = S.x; sy = S.y; sz = S.z;
+        } else {
+            double3 S;
+            eih_terms_f64<UNROLL>(slab, aux, n, q ? sub : 0, q ? lps : 1, slab.x[idx], slab.v[idx], aux[idx], eps2,
+                                  S);
+            sx = S.x; sy = S.y; sz = S.z;
+        }
         if (q == 1) {
             sx = group_total(sx, lps, lane, v1); sy = group_total(sy, lps, lane, v1);
             sz = group_total(sz, lps, lane, v1);
@@ -353,7 +504,7 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
         if (lane == 0) w = atomicAdd(work, 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
         if (w >= (unsigned)nsys) break;
-        const int sys = order[w];
+        const int sys = order ? order[w] : (int)w;  // no order: upload order
         const int b0 = off[sys], n = off[sys + 1] - b0;
         const bool two = n > 32;
         const bool v0 = lane < n, v1 = lane + 32 < n;
@@ -387,25 +538,16 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     x[q].x += c * v[q].x; x[q].y += c * v[q].y; x[q].z += c * v[q].z;
-                    const bool vq = q ? v1 : v0;
-                    if (!vq) continue;
                     const int idx = lane + 32 * q;
-                    const double vsq = v[q].x * v[q].x + v[q].y * v[q].y + v[q].z * v[q].z;
-                    if (MIXED) {
-                        EnsSlab<true>& sl = reinterpret_cast<EnsSlab<true>&>(slab);
-                        float4 h, l;
-                        ds_split(x[q].x, h.x, l.x);
-                        ds_split(x[q].y, h.y, l.y);
-                        ds_split(x[q].z, h.z, l.z);
-                        h.w = (float)x[q].w;
-                        l.w = 0.f;
-                        sl.hi[idx] = h;
-                        sl.lo[idx] = l;
-                        sl.v[idx] = make_float4((float)v[q].x, (float)v[q].y, (float)v[q].z, (float)vsq);
+                    if constexpr (MIXED) {
+                        // every slot the pairs can reach: lanes past n hold zero state
+                        if (q == 1 && !two) continue;
+                        slab_put(slab, idx, x[q], v[q]);
                     } else {
-                        EnsSlab<false>& sl = reinterpret_cast<EnsSlab<false>&>(slab);
-                        sl.x[idx] = x[q];
-                        sl.v[idx] = make_double4(v[q].x, v[q].y, v[q].z, vsq);
+                        if (!(q ? v1 : v0)) continue;
+                        const double vsq = v[q].x * v[q].x + v[q].y * v[q].y + v[q].z * v[q].z;
+                        slab.x[idx] = x[q];
+                        slab.v[idx] = make_double4(v[q].x, v[q].y, v[q].z, vsq);
                     }
                 }
                 __syncwarp();
@@ -419,19 +561,18 @@ __global__ void k_ensemble(int32_t nsys, const int32_t* __restrict__ order, cons
                     // body `lane` (q = 0, all sources); for q = 1 body 32 + sb, its
                     // sources split among the lps lanes of group sb
                     const int idx = q ? (sec ? 32 + sb : 0) : (v0 ? lane : 0);  // idle slots read body 0
-                    const int j0 = q ? sub : 0, js = q ? lps : 1;
                     double sx, sy, sz;
-                    if (MIXED) {
-                        const EnsSlab<true>& sl = reinterpret_cast<const EnsSlab<true>&>(slab);
+                    if constexpr (MIXED) {
+                        // source pairs, split among the lps lanes for q = 1
                         float3 aN, a1, a2;
-                        accel_f32<PNL, UNROLL>(sl, n, j0, js, sl.hi[idx], sl.lo[idx], sl.v[idx], epsf, Gf, pkf, aN,
-                                               a1, a2);
+                        accel_f32<PNL, UNROLL>(slab, (n + 1) >> 1, q ? sub : 0, q ? lps : 1, slab_body(slab, idx),
+                                               epsf, Gf, pkf, aN, a1, a2);
                         sx = ((double)aN.x + (double)a1.x) + (double)a2.x;
                         sy = ((double)aN.y + (double)a1.y) + (double)a2.y;
                         sz = ((double)aN.z + (double)a1.z) + (double)a2.z;
                     } else {
-                        const EnsSlab<false>& sl = reinterpret_cast<const EnsSlab<false>&>(slab);
-                        accel_f64<PNL, UNROLL>(sl, n, j0, js, sl.x[idx], sl.v[idx], eps2, G, pk, sx, sy, sz);
+                        accel_f64<PNL, UNROLL>(slab, n, q ? sub : 0, q ? lps : 1, slab.x[idx], slab.v[idx], eps2, G,
+                                               pk, sx, sy, sz);
                     }
                     if (q == 1) {
                         // add the lps partial sums (aligned lane groups), then lane s
@@ -490,7 +631,8 @@ __global__ void k_ensemble_energy(int32_t nsys, const int32_t* __restrict__ off,
                 if (j == i) continue;
                 const double4 xj = pm[b0 + j];
                 const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-                phi += G * xj.w / sqrt(dx * dx + dy * dy + dz * dz + eps2);
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 > 0.0) phi += G * xj.w / sqrt(d2 + eps2);
             }
             e1 += 0.5 * xi.w * phi * phi;
         }
@@ -535,7 +677,7 @@ __global__ void k_unpack_ens(int64_t n, const double4* __restrict__ src, double*
 
 template <bool MIXED, int PNL, int UNROLL>
 int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_t nsteps, int wpb, int check_every,
-                    bool use_graph) {
+                    bool use_graph, bool lpt) {
     EnsBufs& e = c->ens;
     auto kern = k.nst == 3 ? k_ensemble<MIXED, PNL, UNROLL, 3> : k_ensemble<MIXED, PNL, UNROLL, 1>;
     const size_t smem = (size_t)wpb * (sizeof(EnsSlab<MIXED>) +
@@ -551,7 +693,7 @@ int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_
     unsigned int* work = e.counter.as<unsigned int>();
     auto enqueue = [&](cudaStream_t s) -> int {
         ASTER_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned int), s));
-        kern<<<(unsigned)blocks, wpb * 32, smem, s>>>(e.nsys, e.order.as<int32_t>(), e.off.as<int32_t>(),
+        kern<<<(unsigned)blocks, wpb * 32, smem, s>>>(e.nsys, lpt ? e.order.as<int32_t>() : nullptr, e.off.as<int32_t>(),
                                                      e.pm.as<double4>(), e.vel.as<double4>(), p->G, p->eps2, pk, k,
                                                      nsteps, check_every, work, e.cancel_dev, c->err_dev);
         ASTER_CUDA(cudaGetLastError());
@@ -577,11 +719,11 @@ int launch_ensemble(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_
 
 template <bool MIXED, int PNL>
 int dispatch_unroll(aster_ctx* c, const aster_params* p, const Coeffs& k, int64_t nsteps, int wpb, int unroll,
-                    int check_every, bool g) {
+                    int check_every, bool g, bool lpt) {
     switch (unroll) {
-        case 1: return launch_ensemble<MIXED, PNL, 1>(c, p, k, nsteps, wpb, check_every, g);
-        case 4: return launch_ensemble<MIXED, PNL, 4>(c, p, k, nsteps, wpb, check_every, g);
-        default: return launch_ensemble<MIXED, PNL, 2>(c, p, k, nsteps, wpb, check_every, g);
+        case 1: return launch_ensemble<MIXED, PNL, 1>(c, p, k, nsteps, wpb, check_every, g, lpt);
+        case 4: return launch_ensemble<MIXED, PNL, 4>(c, p, k, nsteps, wpb, check_every, g, lpt);
+        default: return launch_ensemble<MIXED, PNL, 2>(c, p, k, nsteps, wpb, check_every, g, lpt);
     }
 }
 
@@ -698,7 +840,10 @@ extern "C" int aster_ensemble_run(aster_ctx* c, const aster_params* p, int integ
     int check = cfg && cfg->check_every ? cfg->check_every : 256;
     // stream capture is not possible on the legacy default stream
     bool graph = (cfg ? cfg->use_graph != 0 : true) && c->stream != nullptr;
+    const int schedule = cfg ? cfg->schedule : 0;
     if (wpb < 1 || wpb > 16 || (unroll != 1 && unroll != 2 && unroll != 4) || check < 1) return ASTER_ERR_INVALID_ARG;
+    if (schedule != 0 && schedule != 1) return ASTER_ERR_INVALID_ARG;
+    const bool lpt = schedule == 0;
     ASTER_TRY(aster_begin(c));
     c->stats = aster_stats{};
     *c->ens.cancel_host = 0;
@@ -707,15 +852,15 @@ extern "C" int aster_ensemble_run(aster_ctx* c, const aster_params* p, int integ
     cudaEventRecord(c->ev[0], c->stream);
     int st;
     if (precision == ASTER_MIXED)
-        st = pnl == 3 ? dispatch_unroll<true, 3>(c, p, k, nsteps, wpb, unroll, check, graph)
-           : pnl == 2 ? dispatch_unroll<true, 2>(c, p, k, nsteps, wpb, unroll, check, graph)
-           : pnl == 1 ? dispatch_unroll<true, 1>(c, p, k, nsteps, wpb, unroll, check, graph)
-                      : dispatch_unroll<true, 0>(c, p, k, nsteps, wpb, unroll, check, graph);
+        st = pnl == 3 ? dispatch_unroll<true, 3>(c, p, k, nsteps, wpb, unroll, check, graph, lpt)
+           : pnl == 2 ? dispatch_unroll<true, 2>(c, p, k, nsteps, wpb, unroll, check, graph, lpt)
+           : pnl == 1 ? dispatch_unroll<true, 1>(c, p, k, nsteps, wpb, unroll, check, graph, lpt)
+                      : dispatch_unroll<true, 0>(c, p, k, nsteps, wpb, unroll, check, graph, lpt);
     else
-        st = pnl == 3 ? dispatch_unroll<false, 3>(c, p, k, nsteps, wpb, unroll, check, graph)
-           : pnl == 2 ? dispatch_unroll<false, 2>(c, p, k, nsteps, wpb, unroll, check, graph)
-           : pnl == 1 ? dispatch_unroll<false, 1>(c, p, k, nsteps, wpb, unroll, check, graph)
-                      : dispatch_unroll<false, 0>(c, p, k, nsteps, wpb, unroll, check, graph);
+        st = pnl == 3 ? dispatch_unroll<false, 3>(c, p, k, nsteps, wpb, unroll, check, graph, lpt)
+           : pnl == 2 ? dispatch_unroll<false, 2>(c, p, k, nsteps, wpb, unroll, check, graph, lpt)
+           : pnl == 1 ? dispatch_unroll<false, 1>(c, p, k, nsteps, wpb, unroll, check, graph, lpt)
+                      : dispatch_unroll<false, 0>(c, p, k, nsteps, wpb, unroll, check, graph, lpt);
     if (st != ASTER_OK) return st;
     cudaEventRecord(c->ev[1], c->stream);
     st = aster_finish(c);

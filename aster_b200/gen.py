@@ -302,3 +302,32 @@ def kepler_orbits(n: int, seed: int, mu: float = 1.0):
     m = np.zeros(n + 1)
     m[0] = mu
     return pos, vel, m, e
+
+
+def ensemble_measures(pos, vel, m, offsets, G: float = 1.0):
+    """Per system of a hierarchical ensemble (bodies 0, 1 the inner binary):
+    the binary's pericentre time sqrt(r_p^3 / (G (m_0 + m_1))), the smallest
+    initial separation of any other pair, and the energy scale K + |U|
+    (kinetic plus the magnitude of the Newtonian potential energy). Returns
+    (t_peri, d_min, scale) as arrays of the system count."""
+    off = np.asarray(offsets, dtype=np.int64)
+    i0 = off[:-1]
+    r, v = pos[i0 + 1] - pos[i0], vel[i0 + 1] - vel[i0]
+    mu = G * (m[i0] + m[i0 + 1])
+    rn = np.linalg.norm(r, axis=1)
+    a = 1.0 / (2.0 / rn - (v * v).sum(1) / mu)
+    h = np.cross(r, v)
+    e = np.sqrt(np.maximum(0.0, 1.0 - (h * h).sum(1) / (mu * a)))
+    tp = np.sqrt((a * (1.0 - e)) ** 3 / mu)
+    ns = len(off) - 1
+    dmin, scale = np.empty(ns), np.empty(ns)
+    for s in range(ns):
+        x, u, mm = pos[off[s]:off[s + 1]], vel[off[s]:off[s + 1]], m[off[s]:off[s + 1]]
+        d = np.linalg.norm(x[:, None] - x[None], axis=-1)
+        iu = np.triu_indices(len(mm), 1)
+        pot = G * (mm[:, None] * mm[None] / np.where(d > 0, d, np.inf))[iu].sum()
+        scale[s] = 0.5 * (mm * (u * u).sum(1)).sum() + pot
+        d[0, 1] = d[1, 0] = np.inf
+        np.fill_diagonal(d, np.inf)
+        dmin[s] = d.min()
+    return tp, dmin, scale

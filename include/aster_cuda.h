@@ -276,6 +276,8 @@ typedef struct aster_ensemble_config {
     int32_t unroll;          /* inner-loop unroll 1, 2 or 4 (0: 2)            */
     int32_t check_every;     /* steps between cancel-flag reads (0: 256)      */
     int32_t use_graph;       /* 1: capture the launch in a CUDA graph         */
+    int32_t schedule;        /* order warps take systems in: 0 largest first
+                                (longest-processing-time), 1 upload order     */
 } aster_ensemble_config;
 
 /* offsets[nsys+1]: system s owns bodies offsets[s] .. offsets[s+1]-1 of the

@@ -891,6 +891,8 @@ void orc_ens_coeffs(int integrator, double* c, double* d, int* nstages) {
  *           - 4 v_a.v_b - 3/2 (n_ab.v_b)^2 + 1/2 (x_b - x_a).A_b)]
  *       + (1/c^2) sum_{b != a} G m_b / r_ab^2 [n_ab.(4 v_a - 3 v_b)] (v_a - v_b)
  *       + (7/(2 c^2)) sum_{b != a} G m_b A_b / r_ab
+ * Sources at zero separation (the body itself, or one at exactly its
+ * position) are left out of every sum, softened or not.
  * For two unsoftened bodies this is the pairwise law of get_pn1
  * (tool_chain_impl.cpp:110-118): the A_b terms give the 5 G m_a / r of its
  * bracket (1 from phi_b, 1/2 from (x_b - x_a).A_b, 7/2 from the last sum).
@@ -903,9 +905,9 @@ static void ens_eih_acc(long n, const double* x, const double* v, const double* 
         for (long b = 0; b < n; ++b) {
             if (b == a) continue;
             double d[3] = {x[3 * b] - x[3 * a], x[3 * b + 1] - x[3 * a + 1], x[3 * b + 2] - x[3 * a + 2]};
-            double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
-            if (r2 == 0.0) continue;
-            double inv = 1.0 / sqrt(r2);
+            double d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (d2 == 0.0) continue;
+            double inv = 1.0 / sqrt(d2 + eps2);
             p += G * m[b] * inv;
             double s = G * m[b] * inv * inv * inv;
             ax += d[0] * s; ay += d[1] * s; az += d[2] * s;
@@ -922,9 +924,9 @@ static void ens_eih_acc(long n, const double* x, const double* v, const double* 
             const double* vb = v + 3 * b;
             const double* Ab = an + 3 * b;
             double d[3] = {x[3 * b] - x[3 * a], x[3 * b + 1] - x[3 * a + 1], x[3 * b + 2] - x[3 * a + 2]};
-            double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
-            if (r2 == 0.0) continue;
-            double inv = 1.0 / sqrt(r2);
+            double d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (d2 == 0.0) continue;
+            double inv = 1.0 / sqrt(d2 + eps2);
             double nab[3] = {-d[0] * inv, -d[1] * inv, -d[2] * inv};
             double vb2 = vb[0] * vb[0] + vb[1] * vb[1] + vb[2] * vb[2];
             double vab = va[0] * vb[0] + va[1] * vb[1] + va[2] * vb[2];
@@ -1026,7 +1028,8 @@ void orc_ens_energy(long nsys, const int64_t* off, const double* pos, const doub
                 for (long j = 0; j < n; ++j) {
                     if (j == i) continue;
                     double d[3] = {x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]};
-                    phi += G * mm[j] / sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2);
+                    double d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                    if (d2 > 0.0) phi += G * mm[j] / sqrt(d2 + eps2);
                 }
                 e1 += 0.5 * mm[i] * phi * phi;
             }

@@ -60,6 +60,8 @@ class Ref:
             lib.ref_leapfrog.argtypes = [ctypes.c_int, _D]
             lib.ref_energy.restype = ctypes.c_double
             lib.ref_bh_tree.argtypes = [_U32, _I32, _I32, _D, _D]
+            lib.ref_bh_node_extra.argtypes = [_D, _D]
+            lib.ref_set_temps.argtypes = [_D]
             lib.ref_pair_force.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D, _D, _D, _D]
             lib.ref_saba.argtypes = [ctypes.c_int, ctypes.c_int]
             lib.ref_wh.argtypes = [ctypes.c_int]
@@ -117,7 +119,15 @@ class Ref:
         rc = self.lib.ref_bh_tree(_p(codes, _U32), _p(left, _I32), _p(right, _I32), _p(nm, _D), _p(nc, _D))
         if rc != 0:
             raise RuntimeError(f"ref_bh_tree failed: {rc}")
-        return dict(codes=codes, left=left, right=right, node_mass=nm, node_com=nc)
+        nv = np.zeros((2 * n - 1, 3))
+        nt = np.zeros(2 * n - 1)
+        self.lib.ref_bh_node_extra(_p(nv, _D), _p(nt, _D))
+        return dict(codes=codes, left=left, right=right, node_mass=nm, node_com=nc, node_vel=nv, node_temp=nt)
+
+    def set_temps(self, temps):
+        """BodyArray::temps of the current bodies."""
+        self.lib.ref_set_temps(_p(_c64(temps), _D))
+        return self
 
     def saba(self, order, nsteps):
         """nsteps of the reference CPU SABA_order (update_SABA1..10)."""

@@ -220,6 +220,28 @@ int ref_bh_tree(uint32_t* codes, int32_t* left, int32_t* right,
     return 0;
 }
 
+// Node velocities and temps (NodesArray::unite: mass-weighted mean, maximum)
+// of the tree the last ref_bh_tree built; vel[(2n-1)*3], temps[2n-1].
+int ref_bh_node_extra(double* vel, double* temps) {
+    HarnessSim* s = sim();
+    auto* bh = dynamic_cast<Aster::Barnes::Barnes_Hut*>(s->solver);
+    if (!bh) return -1;
+    const size_t m = bh->nodes.size();
+    for (size_t i = 0; i < m; ++i) {
+        const auto& v = bh->nodes.velocities[i];
+        if (vel) { vel[3 * i] = v.x; vel[3 * i + 1] = v.y; vel[3 * i + 2] = v.z; }
+        if (temps) temps[i] = bh->nodes.temps[i];
+    }
+    return 0;
+}
+
+// Body temperatures (BodyArray::temps; ref_setup sets them to 0).
+int ref_set_temps(const double* temps) {
+    HarnessSim* s = sim();
+    for (size_t i = 0; i < s->bodies.temps.size(); ++i) s->bodies.temps[i] = temps[i];
+    return 0;
+}
+
 // compute_gravitational for one pair (force on body 1, not acceleration),
 // with the solver's current force_law.
 int ref_pair_force(double m1, double m2, const double* v1, const double* v2,

@@ -152,3 +152,38 @@ def test_cuda_wh_plugin_matches_oracle(orc):
     op, ov = orc.wh(pos, vel, m, 0.05, 4)
     assert rel_l2(po, op) < 1e-12
     assert rel_l2(pv, ov) < 1e-12
+
+
+def test_lbvh_plugin_is_a_barnes_hut_with_the_reference_tree():
+    """CudaLBVH derives from Barnes::Barnes_Hut: with keep_tree, code that
+    casts sim->solver to Barnes_Hut* reads the tree of the last evaluation in
+    its `nodes`. Against the reference's own make_tree + NodesArray::unite on
+    the same bodies (lognormal masses, random temperatures): children, masses
+    and centres of mass bit-exact, velocities (mass-weighted) and temps
+    (maximum) bit-exact."""
+    from oracle.oracle import Ref
+    if not Ref.available():
+        pytest.skip("reference build absent")
+    lib = _lib()
+    n = 3000
+    pos, vel, m = gen.plummer(n, 4243, masses="lognormal")
+    temps = np.random.default_rng(7).uniform(0.0, 100.0, n)
+    nm = 2 * n - 1
+    mass, com, nvel, ntemp = np.empty(nm), np.empty((nm, 3)), np.empty((nm, 3)), np.empty(nm)
+    left, right = np.empty(nm, np.int32), np.empty(nm, np.int32)
+    I = ctypes.POINTER(ctypes.c_int32)
+    lib.plg_lbvh_tree.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_double, ctypes.c_int, _D, _D, _D, _D, I, I]
+    p = lambda a: a.ctypes.data_as(_D)  # noqa: E731
+    pos, vel, m = (np.ascontiguousarray(a) for a in (pos, vel, m))
+    rc = lib.plg_lbvh_tree(n, p(pos), p(vel), p(m), p(temps), 0.5, MIXED, p(mass), p(com), p(nvel), p(ntemp),
+                           left.ctypes.data_as(I), right.ctypes.data_as(I))
+    assert rc == 0
+    B = gen.bounding_cube(pos)
+    ref = Ref().setup(pos, vel, m, G=1.0, eps2=1e-4, box=B, solver="bh").set_temps(temps)
+    r = ref.bh_tree()
+    np.testing.assert_array_equal(left, r["left"])
+    np.testing.assert_array_equal(right, r["right"])
+    np.testing.assert_array_equal(mass, r["node_mass"])
+    np.testing.assert_array_equal(com, r["node_com"])
+    np.testing.assert_array_equal(nvel, r["node_vel"])
+    np.testing.assert_array_equal(ntemp, r["node_temp"])
