@@ -63,9 +63,6 @@ constexpr int GROUP_MAX = 64;      // leaves per walk group (1 or 2 per lane)
 // entries also carry a velocity, flushes every WALK_FLUSH_PN.
 constexpr int WALK_FLUSH_MIXED = 128, WALK_FLUSH_FP64 = 32, WALK_FLUSH_PN = 64;
 constexpr int WALK_LIST_MIXED = 192, WALK_LIST_FP64 = 96, WALK_LIST_PN = 128;
-// The Newtonian mixed walk pops up to 64 nodes a round (two per lane), so one
-// round can append 128 entries.
-constexpr int WALK_LIST_WIDE = 256;
 
 // ----------------------------------------------------------------- box
 __device__ __forceinline__ double warp_max_d(double v) {
@@ -728,14 +725,14 @@ __global__ void __launch_bounds__(256) k_front_records(int64_t n, double theta, 
 }
 
 // ----------------------------------------------------------------- walk
-template <bool MIXED, int LISTM = WALK_LIST_MIXED>
+template <bool MIXED>
 struct WalkShared {
     int stack[WALK_WARPS][WALK_STACK];
     // mixed list, two entries per slot so that each paired FP32 operand is an
     // aligned register pair: lpa = (x0, x1, y0, y1), lpb = (z0, z1, m0, m1),
     // positions relative to the group centre
-    float4 lpa[WALK_WARPS][MIXED ? LISTM / 2 : 1];
-    float4 lpb[WALK_WARPS][MIXED ? LISTM / 2 : 1];
+    float4 lpa[WALK_WARPS][MIXED ? WALK_LIST_MIXED / 2 : 1];
+    float4 lpb[WALK_WARPS][MIXED ? WALK_LIST_MIXED / 2 : 1];
     double4 lcm[WALK_WARPS][MIXED ? 1 : WALK_LIST_FP64];  // FP64 (com, mass)
 };
 
@@ -924,10 +921,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
     double4* __restrict__ vel, int* __restrict__ err, int* __restrict__ stack_hw, int stack_limit,
     int32_t* __restrict__ body_counts, unsigned long long* __restrict__ inter_count,
     const double4* __restrict__ node_v, PnK<double> pk) {
-    // two nodes per lane and round for the Newtonian mixed walk
-    constexpr bool WIDE = MIXED && PNL == 0;
-    using Shared = typename std::conditional<PNL != 0, WalkSharedPn<MIXED>,
-                                             WalkShared<MIXED, WIDE ? WALK_LIST_WIDE : WALK_LIST_MIXED>>::type;
+    using Shared = typename std::conditional<PNL != 0, WalkSharedPn<MIXED>, WalkShared<MIXED>>::type;
     __shared__ Shared sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
@@ -1150,10 +1144,17 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
                      nhiz2 = make_float2(-ghiz, -ghiz);
         const float2 ncgx2 = make_float2(-cgx, -cgx), ncgy2 = make_float2(-cgy, -cgy), ncgz2 = make_float2(-cgz, -cgz);
 
-        // One popped node per active lane: test both children, push the opened
-        // ones, append the accepted ones. False when the stack would overflow.
-        auto visit = [&](bool act, const float4 r0, const float4 r1, const float4 r2, const float4 r3,
-                         const int2 ch) -> bool {
+        while (top > 0) {
+            const int cnt = top < 32 ? top : 32;
+            const bool act = lane < cnt;
+            // inactive lanes read the root's record (valid memory) and are masked off
+            int v = nI;
+            if (act) v = stack[top - 1 - lane];
+            __syncwarp();
+            top -= cnt;
+            const float4* rec = crec + 4 * (int64_t)(v - nI);
+            const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3];
+            const int2 ch = child[v];
             const float2 cx = make_float2(r0.x, r0.y), cy = make_float2(r0.z, r0.w), cz = make_float2(r1.x, r1.y);
             const float2 d2 = box_dist2_pair(cx, cy, cz, lox2, loy2, loz2, nhix2, nhiy2, nhiz2);
             const bool fL = ch.x < nI || d2.x > r3.z, fR = ch.y < nI || d2.y > r3.w;  // leaf or far enough
@@ -1161,7 +1162,10 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
             const uint32_t mAL = __ballot_sync(0xffffffffu, aL), mAR = __ballot_sync(0xffffffffu, aR);
             const uint32_t mOL = __ballot_sync(0xffffffffu, oL), mOR = __ballot_sync(0xffffffffu, oR);
             const int npush = __popc(mOL) + __popc(mOR);
-            if (top + npush > stack_limit) return false;
+            if (top + npush > stack_limit) {
+                overflow = true;
+                break;
+            }
             {
                 const int pos = top + __popc(mOL & lt) + __popc(mOR & lt);
                 if (oL) stack[pos] = ch.x;
@@ -1188,51 +1192,18 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
                 }
             }
             lc += __popc(mAL) + __popc(mAR);
-            return true;
-        };
-
-        while (top > 0) {
-            // lane l pops stack[top - 1 - l]; a wide round also stack[top - 33 - l]
-            const int cnt = top < 32 ? top : 32;
-            const int cnt2 = WIDE ? (top - cnt < 32 ? top - cnt : 32) : 0;
-            const bool act = lane < cnt, act2 = lane < cnt2;
-            // inactive lanes read the root's record (valid memory) and are masked off
-            int v = nI, v2 = nI;
-            if (act) v = stack[top - 1 - lane];
-            if (act2) v2 = stack[top - 33 - lane];
-            __syncwarp();
-            top -= cnt + cnt2;
-            const float4* rec = crec + 4 * (int64_t)(v - nI);
-            const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3];
-            const int2 ch = child[v];
-            float4 s0, s1, s2, s3;
-            int2 ch2;
-            if (cnt2 > 0) {  // issued with the first node's loads: one round trip for both
-                const float4* rec2 = crec + 4 * (int64_t)(v2 - nI);
-                s0 = rec2[0]; s1 = rec2[1]; s2 = rec2[2]; s3 = rec2[3];
-                ch2 = child[v2];
-            }
-            if (!visit(act, r0, r1, r2, r3, ch) || (cnt2 > 0 && !visit(act2, s0, s1, s2, s3, ch2))) {
-                overflow = true;
-                break;
-            }
             __syncwarp();
             constexpr int FL = MIXED ? (PNL ? WALK_FLUSH_PN : WALK_FLUSH_MIXED) : WALK_FLUSH_FP64;
             while (lc >= FL) {
                 evaluate(FL);
                 __syncwarp();
-                const int rest = lc - FL;  // < 64, or < 128 for a wide round
-                if (MIXED) {  // whole slots (FL is even), at most 32 (64 wide); read all, then write
+                const int rest = lc - FL;  // < 64
+                if (MIXED) {  // whole slots (FL is even), at most 32; read all, then write
                     const int ns = (rest + 1) >> 1;
-                    float4 a = make_float4(0, 0, 0, 0), b = a, a2 = a, b2 = a;
+                    float4 a = make_float4(0, 0, 0, 0), b = a;
                     if (lane < ns) { a = sm.lpa[warp][FL / 2 + lane]; b = sm.lpb[warp][FL / 2 + lane]; }
-                    if (WIDE && lane + 32 < ns) {
-                        a2 = sm.lpa[warp][FL / 2 + 32 + lane];
-                        b2 = sm.lpb[warp][FL / 2 + 32 + lane];
-                    }
                     __syncwarp();
                     if (lane < ns) { sm.lpa[warp][lane] = a; sm.lpb[warp][lane] = b; }
-                    if (WIDE && lane + 32 < ns) { sm.lpa[warp][32 + lane] = a2; sm.lpb[warp][32 + lane] = b2; }
                 } else {
                     const bool m0 = lane < rest, m1 = lane + 32 < rest;
                     double4 x0 = make_double4(0, 0, 0, 0), x1 = x0;
