@@ -256,7 +256,7 @@ int adj_pair_launch(aster_ctx* c, const aster_params* p, int precision, const do
     AdjBufs& a = c->adj;
     const int64_t n = c->n;
     const int64_t iblocks = (n + BLOCK * IPT - 1) / (BLOCK * IPT);
-    int64_t want = 2 * (int64_t)c->sm_count;
+    int64_t want = ASTER_SLICE_BLOCKS_PER_SM * (int64_t)c->sm_count;
     int64_t ns = iblocks >= want ? 1 : (want + iblocks - 1) / iblocks;
     const int64_t max_ns = (n + BLOCK - 1) / BLOCK;
     ns = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(ns, max_ns), 64));

@@ -392,10 +392,14 @@ int aster_allpairs_launch_range(aster_ctx* c, const aster_params* p, int precisi
     const int64_t len = hi > lo ? hi - lo : 0;
     const int64_t per_block = (int64_t)BLOCK * IPT;
     const int64_t iblocks = (nt + per_block - 1) / per_block;
-    // j-slices so that small n still fill the GPU (>= 2 blocks per SM).
-    int64_t want = 2 * (int64_t)c->sm_count;
+    // j-slices so that small n still fill the GPU (>= ASTER_SLICE_BLOCKS_PER_SM blocks per SM).
+    int64_t want = ASTER_SLICE_BLOCKS_PER_SM * (int64_t)c->sm_count;
     int64_t ns = iblocks >= want ? 1 : (want + iblocks - 1) / iblocks;
-    int64_t max_ns = (len + BLOCK - 1) / BLOCK;
+    // each slice at least one j-tile; the mixed kernel's at least
+    // ASTER_SLICE_MIN_MIXED sources (its partial-sum reduction outweighs more
+    // parallelism below that)
+    const int64_t min_len = precision == ASTER_MIXED ? ASTER_SLICE_MIN_MIXED : BLOCK;
+    int64_t max_ns = (len + min_len - 1) / min_len;
     if (ns > max_ns) ns = max_ns;
     if (ns > 64) ns = 64;
     if (ns < 1) ns = 1;

@@ -20,6 +20,22 @@
 #define ASTER_DEVERR_LIST 0x10
 #define ASTER_DEVERR_KEPLER 0x20
 
+// The O(N^2) kernels (all-pairs forces, adjoint pair terms) split the sources
+// into slices when there are too few target blocks to give every SM this many
+// blocks (small N), and add the slices' partial sums afterwards. Measured
+// (same-box A/B, 2 / 4 / 6 / 8 / 12): 12 took the C5 adjoint (N = 16384,
+// 1000 steps) from 1021 to 744 ms mixed and 2057 to 1400 ms FP64, and the C1
+// FP64 step (N = 4096) from 0.048 to 0.040 ms. The mixed all-pairs kernel
+// keeps at least ASTER_SLICE_MIN_MIXED sources per slice: with 128 the C1
+// mixed step slowed from 0.0255 to 0.0274 ms, the reduction of 32 partial
+// sums per body outweighing the parallelism.
+#ifndef ASTER_SLICE_BLOCKS_PER_SM
+#define ASTER_SLICE_BLOCKS_PER_SM 12
+#endif
+#ifndef ASTER_SLICE_MIN_MIXED
+#define ASTER_SLICE_MIN_MIXED 256
+#endif
+
 #define ASTER_TRY(...)                                    \
     do {                                                  \
         int _st = (__VA_ARGS__);                          \

@@ -737,7 +737,7 @@ def run_case(args):
     FP64 and one mixed evaluation), C4 ensemble (a 50-step launch), C5 adjoint
     (8 steps, checkpoints every 4)."""
     from aster_b200 import gen
-    from aster_b200.api import FP64, MIXED, NEWTON, PN1, YOSHIDA4, Context, Params
+    from aster_b200.api import EIH, FP64, MIXED, NEWTON, PN1, YOSHIDA4, Context, Params
     ctx = Context(0)
     out = {"case": args.case}
     if args.case == "allpairs":
@@ -791,14 +791,18 @@ def run_case(args):
         ctx.kdk_steps(p, 3, SOLVER_LBVH, MIXED)
         st = ctx.stats()
         out.update(n=args.n, ms_per_step=st["ms_total"] / 3, interactions_per_step=st["interactions"] / 3)
-    elif args.case == "ensemble":
+    elif args.case in ("ensemble", "ensemble_eih"):
+        # the C4 ensemble (16384 systems), pairwise or EIH 1PN, plain launches
+        # with a launch shape the autotuner picks on B200: a 20-step launch,
+        # then one of 300 steps
+        eih = args.case == "ensemble_eih"
         pos, vel, m, off = gen.hierarchical_ensemble(16384, 1004)
-        p = Params(G=1.0, c=100.0, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1)
+        p = Params(G=1.0, c=100.0, eps2=0.0, dt=1e-4, force_law=NEWTON | PN1 | (EIH if eih else 0))
         ctx.ensemble_upload(off, pos, vel, m)
-        cfg = {"warps_per_block": 8, "unroll": 2, "use_graph": 1}
-        ctx.ensemble_run(p, 5, YOSHIDA4, MIXED, cfg)
-        ctx.ensemble_run(p, 50, YOSHIDA4, MIXED, cfg)
-        out["ms_50_steps"] = ctx.stats()["ms_total"]
+        cfg = {"warps_per_block": 2, "unroll": 1 if eih else 2, "use_graph": 0}
+        ctx.ensemble_run(p, 20, YOSHIDA4, MIXED, cfg)
+        ctx.ensemble_run(p, 300, YOSHIDA4, MIXED, cfg)
+        out["ms_300_steps"] = ctx.stats()["ms_total"]
     else:
         x0, v0, m = gen.plummer(16384, 1005)
         p = Params(eps2=1e-4, dt=1e-3)
@@ -824,7 +828,7 @@ def main():
     ap.add_argument("--walk-traffic", type=float, default=WALK_TRAFFIC_BYTES,
                     help="DRAM bytes per walk launch from an ncu capture (reported as roofline.traffic)")
     ap.add_argument("--case", default=None,
-                    choices=["allpairs", "ensemble", "adjoint", "c3drift", "wh", "scale", "pnlbvh"],
+                    choices=["allpairs", "ensemble", "ensemble_eih", "adjoint", "c3drift", "wh", "scale", "pnlbvh"],
                     help="run one secondary workload briefly (used for profiling captures) and exit")
     args = ap.parse_args()
     if args.warmup < 3:
