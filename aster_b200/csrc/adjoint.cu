@@ -93,83 +93,112 @@ __device__ __forceinline__ void adj_store(int64_t k, double jx, double jy, doubl
     lm[k] += G * g;
 }
 
+// Mixed adjoint pair terms, two sources at once with the paired FP32
+// instructions of sm_100 (add/mul/fma .f32x2): the source tile is stored
+// pair-interleaved, element k of each array holding sources 2k and 2k + 1, so
+// every paired operand is one aligned register pair. Per target (IPT per
+// thread) the FP32 partial sums are folded into compensated accumulators
+// every FOLD sources; the mass-gradient sum is kept positive (s^3 w_j.d) and
+// negated at the fold.
 template <bool GUARD>
 __global__ void __launch_bounds__(BLOCK) k_adj_pair_mixed(int64_t n, const double4* __restrict__ xs,
                                                           const float4* __restrict__ w, float eps2, double G,
                                                           int64_t slice_len, int nslices,
                                                           double4* __restrict__ partial, double4* __restrict__ lx,
                                                           double* __restrict__ lm) {
-    __shared__ float4 sh[BLOCK], sl[BLOCK], sw[BLOCK];
+    constexpr int NP = BLOCK / 2;
+    __shared__ float4 PA[NP], PB[NP], PC[NP], PD[NP], PE[NP];  // (x_hi x_hi' y_hi y_hi'), (z_hi z_hi' m m'),
+                                                               // (x_lo ..), (z_lo z_lo' w_z w_z'), (w_x .. w_y ..)
     const int slice = blockIdx.y;
     const int64_t j0 = (int64_t)slice * slice_len, j1 = min(n, j0 + slice_len);
     int64_t kk[IPT];
-    float xh[IPT], yh[IPT], zh[IPT], xl[IPT], yl[IPT], zl[IPT], mk[IPT], nwx[IPT], nwy[IPT], nwz[IPT];
-    float ax[IPT], ay[IPT], az[IPT], ag[IPT];
+    float2 nxh[IPT], nyh[IPT], nzh[IPT], nxl[IPT], nyl[IPT], nzl[IPT], mk[IPT], nwx[IPT], nwy[IPT], nwz[IPT];
+    float2 ax[IPT], ay[IPT], az[IPT], ag[IPT];
     CompSum cx[IPT], cy[IPT], cz[IPT], cg[IPT];
+    const float2 zero2 = make_float2(0.f, 0.f), e2 = make_float2(eps2, eps2);
 #pragma unroll
     for (int q = 0; q < IPT; ++q) {
         kk[q] = (int64_t)blockIdx.x * BLOCK * IPT + q * BLOCK + threadIdx.x;
         const int64_t k = kk[q] < n ? kk[q] : 0;
         const double4 x = xs[k];
-        ds_split(x.x, xh[q], xl[q]);
-        ds_split(x.y, yh[q], yl[q]);
-        ds_split(x.z, zh[q], zl[q]);
-        mk[q] = (float)x.w;
+        float h, l;
+        ds_split(x.x, h, l); nxh[q] = make_float2(-h, -h); nxl[q] = make_float2(-l, -l);
+        ds_split(x.y, h, l); nyh[q] = make_float2(-h, -h); nyl[q] = make_float2(-l, -l);
+        ds_split(x.z, h, l); nzh[q] = make_float2(-h, -h); nzl[q] = make_float2(-l, -l);
+        const float m = (float)x.w;
+        mk[q] = make_float2(m, m);
         const float4 wk = w[k];
-        nwx[q] = -wk.x; nwy[q] = -wk.y; nwz[q] = -wk.z;
-        ax[q] = ay[q] = az[q] = ag[q] = 0.f;
+        nwx[q] = make_float2(-wk.x, -wk.x); nwy[q] = make_float2(-wk.y, -wk.y); nwz[q] = make_float2(-wk.z, -wk.z);
+        ax[q] = ay[q] = az[q] = ag[q] = zero2;
     }
     for (int64_t base = j0; base < j1; base += BLOCK) {
         const int64_t j = base + threadIdx.x;
         __syncthreads();
-        if (j < j1) {
-            const double4 x = xs[j];
-            float4 h, l;
-            ds_split(x.x, h.x, l.x);
-            ds_split(x.y, h.y, l.y);
-            ds_split(x.z, h.z, l.z);
-            h.w = (float)x.w;
-            l.w = 0.f;
-            sh[threadIdx.x] = h;
-            sl[threadIdx.x] = l;
-            sw[threadIdx.x] = w[j];
-        } else {
-            sh[threadIdx.x] = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
-            sl[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-            sw[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+        {
+            float hx, lx_, hy, ly, hz, lz, m = 0.f;
+            float4 wj = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (j < j1) {
+                const double4 x = xs[j];
+                ds_split(x.x, hx, lx_);
+                ds_split(x.y, hy, ly);
+                ds_split(x.z, hz, lz);
+                m = (float)x.w;
+                wj = w[j];
+            } else {  // far away, no mass, no cotangent: contributes nothing
+                hx = hy = hz = 1.0e30f;
+                lx_ = ly = lz = 0.f;
+            }
+            const int o = ((threadIdx.x >> 1) << 2) | (threadIdx.x & 1);
+            float* A = reinterpret_cast<float*>(PA);
+            float* B = reinterpret_cast<float*>(PB);
+            float* C = reinterpret_cast<float*>(PC);
+            float* D = reinterpret_cast<float*>(PD);
+            float* E = reinterpret_cast<float*>(PE);
+            A[o] = hx; A[o + 2] = hy; B[o] = hz; B[o + 2] = m;
+            C[o] = lx_; C[o + 2] = ly; D[o] = lz; D[o + 2] = wj.z;
+            E[o] = wj.x; E[o + 2] = wj.y;
         }
         __syncthreads();
 #pragma unroll 1
-        for (int c0 = 0; c0 < BLOCK; c0 += FOLD) {
-#pragma unroll 4
-            for (int jj = c0; jj < c0 + FOLD; ++jj) {
-                const float4 h = sh[jj], l = sl[jj], wj = sw[jj];
+        for (int c0 = 0; c0 < NP; c0 += FOLD / 2) {
+#pragma unroll 2
+            for (int pp = c0; pp < c0 + FOLD / 2; ++pp) {
+                const float4 a = PA[pp], b = PB[pp], c = PC[pp], d = PD[pp], e = PE[pp];
+                const float2 mj = make_float2(b.z, b.w);
+                const float2 wjx = make_float2(e.x, e.y), wjy = make_float2(e.z, e.w), wjz = make_float2(d.z, d.w);
 #pragma unroll
                 for (int q = 0; q < IPT; ++q) {
-                    const float dx = (h.x - xh[q]) + (l.x - xl[q]);
-                    const float dy = (h.y - yh[q]) + (l.y - yl[q]);
-                    const float dz = (h.z - zh[q]) + (l.z - zl[q]);
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-                    float s = rsqrt_approx(r2);
-                    if (GUARD) s = r2 > 0.f ? s : 0.f;
-                    const float s2 = s * s, s3 = s2 * s, s5 = s3 * s2;
+                    const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(a.x, a.y), nxh[q]),
+                                                 __fadd2_rn(make_float2(c.x, c.y), nxl[q]));
+                    const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(a.z, a.w), nyh[q]),
+                                                 __fadd2_rn(make_float2(c.z, c.w), nyl[q]));
+                    const float2 dz = __fadd2_rn(__fadd2_rn(make_float2(b.x, b.y), nzh[q]),
+                                                 __fadd2_rn(make_float2(d.x, d.y), nzl[q]));
+                    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+                    float2 sv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                    if (GUARD) {
+                        sv.x = r2.x > 0.f ? sv.x : 0.f;
+                        sv.y = r2.y > 0.f ? sv.y : 0.f;
+                    }
+                    const float2 s2 = __fmul2_rn(sv, sv), s3 = __fmul2_rn(s2, sv), s5 = __fmul2_rn(s3, s2);
                     // u = m_k w_j - m_j w_k
-                    const float ux = fmaf(mk[q], wj.x, h.w * nwx[q]);
-                    const float uy = fmaf(mk[q], wj.y, h.w * nwy[q]);
-                    const float uz = fmaf(mk[q], wj.z, h.w * nwz[q]);
-                    const float du = fmaf(dx, ux, fmaf(dy, uy, dz * uz));
-                    const float t = 3.f * s5 * du;
-                    ax[q] = fmaf(-t, dx, fmaf(s3, ux, ax[q]));
-                    ay[q] = fmaf(-t, dy, fmaf(s3, uy, ay[q]));
-                    az[q] = fmaf(-t, dz, fmaf(s3, uz, az[q]));
-                    const float wd = fmaf(wj.x, dx, fmaf(wj.y, dy, wj.z * dz));
-                    ag[q] = fmaf(-s3, wd, ag[q]);
+                    const float2 ux = __ffma2_rn(mk[q], wjx, __fmul2_rn(mj, nwx[q]));
+                    const float2 uy = __ffma2_rn(mk[q], wjy, __fmul2_rn(mj, nwy[q]));
+                    const float2 uz = __ffma2_rn(mk[q], wjz, __fmul2_rn(mj, nwz[q]));
+                    const float2 du = __ffma2_rn(dx, ux, __ffma2_rn(dy, uy, __fmul2_rn(dz, uz)));
+                    const float2 nt = __fmul2_rn(__fmul2_rn(s5, make_float2(-3.f, -3.f)), du);  // -3 s^5 (d.u)
+                    ax[q] = __ffma2_rn(nt, dx, __ffma2_rn(s3, ux, ax[q]));
+                    ay[q] = __ffma2_rn(nt, dy, __ffma2_rn(s3, uy, ay[q]));
+                    az[q] = __ffma2_rn(nt, dz, __ffma2_rn(s3, uz, az[q]));
+                    const float2 wd = __ffma2_rn(wjx, dx, __ffma2_rn(wjy, dy, __fmul2_rn(wjz, dz)));
+                    ag[q] = __ffma2_rn(s3, wd, ag[q]);
                 }
             }
 #pragma unroll
             for (int q = 0; q < IPT; ++q) {
-                cx[q].add(ax[q]); cy[q].add(ay[q]); cz[q].add(az[q]); cg[q].add(ag[q]);
-                ax[q] = ay[q] = az[q] = ag[q] = 0.f;
+                cx[q].add(ax[q].x + ax[q].y); cy[q].add(ay[q].x + ay[q].y); cz[q].add(az[q].x + az[q].y);
+                cg[q].add(-(ag[q].x + ag[q].y));
+                ax[q] = ay[q] = az[q] = ag[q] = zero2;
             }
         }
     }
