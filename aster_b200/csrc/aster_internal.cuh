@@ -136,7 +136,8 @@ struct aster_ctx {
 inline unsigned long long* red_box(aster_ctx* c) { return c->red.as<unsigned long long>(); }         // byte 0
 inline double* red_energy(aster_ctx* c) { return c->red.as<double>() + 8; }                         // byte 64
 inline unsigned long long* red_inter(aster_ctx* c) { return c->red.as<unsigned long long>() + 64; } // byte 512
-inline unsigned int* red_groups(aster_ctx* c) {  // [0] group count, [1] walk work counter, [2] bottom-up frontier
+inline unsigned int* red_groups(aster_ctx* c) {  // [0] large-group count, [1] walk work counter, [2] bottom-up
+                                                 // frontier, [3] small-group count
     return reinterpret_cast<unsigned int*>(c->red.as<char>() + 1024);
 }
 

@@ -378,7 +378,19 @@ __device__ __forceinline__ int kdelta(const KeyT* __restrict__ codes, const int3
 // Morton jump and span the whole system). Listed here as (first leaf, size):
 // internal node n + i knows its own range and both children's, and thread i
 // lists the groups among its children, so groups come roughly in sorted-leaf
-// order, which keeps consecutive walk groups close in space.
+// order, which keeps consecutive walk groups close in space. Groups of more
+// than 32 bodies (a second pass over the list, or two bodies per lane) fill
+// the array from the front, groups of at most 32 (one pass) from the back;
+// the walk takes the front part first, so its last wave is made of the
+// cheaper groups and warps finish closer together.
+constexpr int GROUP_SMALL = 32;
+__device__ __forceinline__ void list_group(int2* groups, unsigned int* ngroups, int64_t n, int64_t first,
+                                           int64_t size) {
+    if (size > GROUP_SMALL)
+        groups[atomicAdd(&ngroups[0], 1u)] = make_int2((int32_t)first, (int32_t)size);
+    else
+        groups[n - 1 - atomicAdd(&ngroups[3], 1u)] = make_int2((int32_t)first, (int32_t)size);
+}
 template <class KeyT, bool COMPAT>
 __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restrict__ codes, const int32_t* __restrict__ perm,
                                                 const double4* __restrict__ pm, int32_t* __restrict__ parent,
@@ -394,7 +406,7 @@ __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restric
             rhi[i] = (int32_t)i;
             if (n == 1) {
                 parent[0] = -1;
-                groups[atomicAdd(ngroups, 1u)] = make_int2(0, 1);
+                list_group(groups, ngroups, n, 0, 1);
             }
         }
         if (i == n - 1) {
@@ -433,10 +445,10 @@ __global__ void __launch_bounds__(256) k_karras(int64_t n, const KeyT* __restric
         counters[i] = 0u;
         if (hi - lo + 1 > GROUP_MAX) {
             const int64_t szL = gamma - lo + 1, szR = hi - gamma;
-            if (szL <= GROUP_MAX) groups[atomicAdd(ngroups, 1u)] = make_int2((int32_t)lo, (int32_t)szL);
-            if (szR <= GROUP_MAX) groups[atomicAdd(ngroups, 1u)] = make_int2((int32_t)(gamma + 1), (int32_t)szR);
+            if (szL <= GROUP_MAX) list_group(groups, ngroups, n, lo, szL);
+            if (szR <= GROUP_MAX) list_group(groups, ngroups, n, gamma + 1, szR);
         } else if (i == 0) {  // the root holds at most GROUP_MAX leaves
-            groups[atomicAdd(ngroups, 1u)] = make_int2(0, (int32_t)n);
+            list_group(groups, ngroups, n, 0, n);
         }
     }
 }
@@ -925,7 +937,9 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
     __shared__ Shared sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
-    const unsigned int ngroups = *ngroups_p;
+    // ngroups_p[0] groups of more than GROUP_SMALL bodies at groups[0..), then
+    // ngroups_p[3] smaller ones at groups[n - 1], groups[n - 2], ...
+    const unsigned int nbig = ngroups_p[0], ngroups = nbig + ngroups_p[3];
     int* stack = sm.stack[warp];
     int hw = 1;
     unsigned long long wtotal = 0;
@@ -935,7 +949,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
         if (lane == 0) g = atomicAdd(work, 1u);
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= ngroups) break;
-        const int2 gr = groups[g];
+        const int2 gr = groups[g < nbig ? (int64_t)g : n - 1 - (int64_t)(g - nbig)];
         // Bodies 0..31 of the group: one per lane (primary). Bodies 32.. (r of
         // them, "secondary"): each shared by lps lanes that split the list.
         const int r = gr.y > 32 ? gr.y - 32 : 0;
@@ -1395,8 +1409,9 @@ int run_build(aster_ctx* c, const aster_params* p) {
                                    c->stream));
         c->stats.kernels += 1;
     }
-    unsigned int* gcount = red_groups(c);  // [0] groups, [1] walk work counter, [2] bottom-up frontier
-    ASTER_CUDA(cudaMemsetAsync(gcount, 0, 3 * sizeof(unsigned int), c->stream));
+    unsigned int* gcount = red_groups(c);  // [0] large groups, [1] walk work counter, [2] bottom-up frontier,
+                                           // [3] small groups
+    ASTER_CUDA(cudaMemsetAsync(gcount, 0, 4 * sizeof(unsigned int), c->stream));
     ASTER_TRY(aster_apply_pending_mass(c));  // the leaf gather below is the first reader of the masses
     const KeyT* sc = t.sorted_codes.as<KeyT>();
     if (p->compat_mode)
