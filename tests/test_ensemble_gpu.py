@@ -352,3 +352,28 @@ def test_c4_energy_drift_bounds_and_convergence(ctx, orc):
                            pn=NEWTON | PN1 | EIH)
         de_orc = orc.ens_energy(sub_off, p, u, m[sl], c=100.0, pn=NEWTON | PN1 | EIH)[0] - e0
         assert abs(de[s] - de_orc) <= 1e-2 * abs(de_orc) + 1e-12 * scale[s], (s, de[s], de_orc)
+
+
+@pytest.mark.parametrize("law", [NEWTON, NEWTON | PN1, NEWTON | PN1 | EIH])
+def test_edge_system_sizes_vs_oracle(ctx, orc, law):
+    """System sizes at every boundary of the kernel's layout: 1 and 2 bodies,
+    odd sizes (a zero-padded half of the last source pair), 31..33 and 63..64
+    (the second body per lane), 47..49 (the lanes that split a body's
+    sources), softened (eps2 = 1e-2), c = 10, leapfrog, 10 steps: FP64 kernel
+    1e-10, mixed 1e-5 against the oracle; a single body moves in a straight
+    line."""
+    rng = np.random.default_rng(1011)
+    sizes = np.array([1, 2, 3, 31, 32, 33, 47, 48, 49, 63, 64, 5, 17])
+    off = np.r_[0, np.cumsum(sizes)]
+    pos = rng.normal(size=(off[-1], 3))
+    vel = rng.normal(size=(off[-1], 3))
+    m = rng.uniform(0.5, 1.5, off[-1])
+    q = Params(G=1.0, c=10.0, eps2=1e-2, dt=1e-3, force_law=law)
+    op, ov = orc.ens_run(off, pos, vel, m, q.dt, 10, c=10.0, eps2=1e-2, integrator=LEAPFROG, pn=law)
+    for prec, tol in ((FP64, 1e-10), (MIXED, 1e-5)):
+        ctx.ensemble_upload(off, pos, vel, m)
+        ctx.ensemble_run(q, 10, LEAPFROG, prec)
+        gp, gv = ctx.ensemble_download()
+        assert _per_system_err(gp, op, off) < tol, prec
+        assert _per_system_err(gv, ov, off) < tol, prec
+        np.testing.assert_allclose(gp[0], pos[0] + 10 * q.dt * vel[0], rtol=1e-12)
