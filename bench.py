@@ -68,9 +68,9 @@ FLOP_PER_ADJ_PAIR = 48
 BUILD_BYTES_PER_BODY = 240
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_walk launch captured with
-# ncu at N = 2^19 (74.04 + 4.59 MB read + written), scaled
+# ncu at N = 2^19 (77.60 + 7.19 MB read + written), scaled
 # by the number of bodies to N = 2^20 (the walk reads each tree node about once).
-WALK_TRAFFIC_BYTES = 78.63e6 * 2
+WALK_TRAFFIC_BYTES = 84.79e6 * 2
 
 
 def fp_peaks(f_mhz: float):
