@@ -204,17 +204,23 @@ __device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int np, int q0
         }
     } else if constexpr (PNL == 1) {
         const float2 vix = make_float2(t.vx, t.vx), viy = make_float2(t.vy, t.vy), viz = make_float2(t.vz, t.vz);
-        const float2 nvi2 = make_float2(-t.w, -t.w), mi5 = make_float2(5.f * t.m, 5.f * t.m);
-        const float2 G2 = make_float2(G, G), c2 = make_float2(k.c2, k.c2);
+        const float2 vi4x = make_float2(4.f * t.vx, 4.f * t.vx), vi4y = make_float2(4.f * t.vy, 4.f * t.vy),
+                     vi4z = make_float2(4.f * t.vz, 4.f * t.vz);
+        const float2 nvi2 = make_float2(-t.w, -t.w), mi5G = make_float2(5.f * G * t.m, 5.f * G * t.m);
+        const float2 G4 = make_float2(4.f * G, 4.f * G);
 #pragma unroll UNROLL
         for (int q = q0; q < np; q += qs) {
             float2 dx, dy, dz;
             tx.sep(s, q, dx, dy, dz);
             const float4 b = s.B[q], d = s.D[q], e = s.E[q];
             newton_pn1_x2<true>(dx, dy, dz, make_float2(b.z, b.w), make_float2(e.x, e.y), make_float2(e.z, e.w),
-                                make_float2(d.z, d.w), s.F[q], vix, viy, viz, nvi2, mi5, e2, G2, c2, ax, ay, az, px,
-                                py, pz);
+                                make_float2(d.z, d.w), s.F[q], vix, viy, viz, vi4x, vi4y, vi4z, nvi2, mi5G, e2, G4,
+                                ax, ay, az, px, py, pz);
         }
+        const float mc2 = -k.c2;  // the 1PN term is -c^-2 times newton_pn1_x2's sum
+        px = __fmul2_rn(px, make_float2(mc2, mc2));
+        py = __fmul2_rn(py, make_float2(mc2, mc2));
+        pz = __fmul2_rn(pz, make_float2(mc2, mc2));
     } else {
         float sx = 0.f, sy = 0.f, sz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
         for (int j = 2 * q0; j < 2 * np; j += (j & 1) ? 2 * qs - 1 : 1) {  // both bodies of each visited pair
@@ -322,18 +328,24 @@ __device__ __forceinline__ void newton_phi_f64(const EnsSlab<false>& s, int n, i
 }
 
 // EIH pass 2 (level 3): sum over j of m_j / r^2 [d/r B + W (v_i - v_j)] +
-// 7/2 m_j A_j / r (without G), with (A_j, Phi_j) published by pass 1 (G
-// included). Zero separations contribute 0. Mixed: source pairs q = q0,
-// q0 + qs, ... < np of the pair-interleaved slab, aux = (A_x, A_x', A_y, A_y')
-// in auxA and (A_z, A_z', Phi, Phi') in auxB; Ki = -4 Phi_i + |v_i|^2.
+// 7/2 m_j A_j / r (without G), with A_j and Phi_j (G included) from pass 1.
+// Zero separations contribute 0. Mixed: source pairs q = q0, q0 + qs, ... < np
+// of the pair-interleaved slab; pass 1 publishes A'_j = A_j / 2 and
+// Q_j = 2 |v_j|^2 - Phi_j, aux = (A'_x, A'_x', A'_y, A'_y') in auxA and
+// (A'_z, A'_z', Q, Q') in auxB; per target Ki = -4 Phi_i + |v_i|^2 =
+// 4 Q_i - 7 |v_i|^2. With these B = Ki + Q_j - 4 v_i.v_j - 3/2 (d.v_j / r)^2
+// + d.A'_j, and with k3 = m_j / r^3 the three terms are k3 B d,
+// k3 (3 d.v_j - 4 d.v_i) (v_i - v_j) and 7 (m_j / r) A'_j.
 template <int UNROLL>
 __device__ __forceinline__ void eih_terms_f32(const EnsSlab<true>& s, const float4* __restrict__ auxA,
                                               const float4* __restrict__ auxB, int np, int q0, int qs,
-                                              const BodyF32& t, float Phi_i, float eps2, float3& S) {
+                                              const BodyF32& t, float Q_i, float eps2, float3& S) {
     const TargetX2 tx(t);
     const float2 e2 = make_float2(eps2, eps2);
     const float2 vix = make_float2(t.vx, t.vx), viy = make_float2(t.vy, t.vy), viz = make_float2(t.vz, t.vz);
-    const float ki = fmaf(-4.f, Phi_i, t.w);
+    const float2 n4x = make_float2(-4.f * t.vx, -4.f * t.vx), n4y = make_float2(-4.f * t.vy, -4.f * t.vy),
+                 n4z = make_float2(-4.f * t.vz, -4.f * t.vz);  // -4 v_i
+    const float ki = fmaf(4.f, Q_i, -7.f * t.w);
     const float2 Ki = make_float2(ki, ki);
     const float2 m1 = make_float2(-1.f, -1.f);
     float2 sx = make_float2(0.f, 0.f), sy = sx, sz = sx;
@@ -342,30 +354,26 @@ __device__ __forceinline__ void eih_terms_f32(const EnsSlab<true>& s, const floa
         float2 dx, dy, dz;
         tx.sep(s, q, dx, dy, dz);
         const float4 b = s.B[q], d = s.D[q], e = s.E[q], xa = auxA[q], xb = auxB[q];
-        const float2 vj2 = s.F[q];
         const float2 inv = inv_r_x2_nz(dx, dy, dz, e2);
         const float2 mj = make_float2(b.z, b.w);
         const float2 vjx = make_float2(e.x, e.y), vjy = make_float2(e.z, e.w), vjz = make_float2(d.z, d.w);
         const float2 Ajx = make_float2(xa.x, xa.y), Ajy = make_float2(xa.z, xa.w), Ajz = make_float2(xb.x, xb.y);
-        const float2 Pj = make_float2(xb.z, xb.w);
-        const float2 vij = __ffma2_rn(vix, vjx, __ffma2_rn(viy, vjy, __fmul2_rn(viz, vjz)));
-        const float2 dvi = __ffma2_rn(dx, vix, __ffma2_rn(dy, viy, __fmul2_rn(dz, viz)));
         const float2 dvj = __ffma2_rn(dx, vjx, __ffma2_rn(dy, vjy, __fmul2_rn(dz, vjz)));
-        const float2 dA = __ffma2_rn(dx, Ajx, __ffma2_rn(dy, Ajy, __fmul2_rn(dz, Ajz)));
+        const float2 dvi4 = __ffma2_rn(dx, n4x, __ffma2_rn(dy, n4y, __fmul2_rn(dz, n4z)));  // -4 d.v_i
         const float2 nvj = __fmul2_rn(dvj, inv);
-        // B = Ki - Phi_j + 2 |v_j|^2 - 4 v_i.v_j - 3/2 (n.v_j)^2 + 1/2 d.A_j
-        float2 B = __ffma2_rn(Pj, m1, Ki);
-        B = __ffma2_rn(vj2, make_float2(2.f, 2.f), B);
-        B = __ffma2_rn(vij, make_float2(-4.f, -4.f), B);
+        float2 B = __fadd2_rn(Ki, make_float2(xb.z, xb.w));
+        B = __ffma2_rn(n4x, vjx, B);
+        B = __ffma2_rn(n4y, vjy, B);
+        B = __ffma2_rn(n4z, vjz, B);
+        B = __ffma2_rn(dx, Ajx, B);
+        B = __ffma2_rn(dy, Ajy, B);
+        B = __ffma2_rn(dz, Ajz, B);
         B = __ffma2_rn(__fmul2_rn(nvj, nvj), make_float2(-1.5f, -1.5f), B);
-        B = __ffma2_rn(dA, make_float2(0.5f, 0.5f), B);
-        // W = n.(4 v_i - 3 v_j) = (3 d.v_j - 4 d.v_i) / r
-        const float2 W = __fmul2_rn(__ffma2_rn(dvj, make_float2(3.f, 3.f), __fmul2_rn(dvi, make_float2(-4.f, -4.f))),
-                                    inv);
-        const float2 f = __fmul2_rn(mj, __fmul2_rn(inv, inv));
-        const float2 fb = __fmul2_rn(__fmul2_rn(f, inv), B);
-        const float2 fW = __fmul2_rn(f, W);
-        const float2 g7 = __fmul2_rn(__fmul2_rn(mj, make_float2(3.5f, 3.5f)), inv);
+        const float2 Wr = __ffma2_rn(dvj, make_float2(3.f, 3.f), dvi4);  // W r
+        const float2 ms = __fmul2_rn(mj, inv);
+        const float2 k3 = __fmul2_rn(ms, __fmul2_rn(inv, inv));
+        const float2 fb = __fmul2_rn(k3, B), fW = __fmul2_rn(k3, Wr);
+        const float2 g7 = __fmul2_rn(ms, make_float2(7.f, 7.f));
         sx = __ffma2_rn(g7, Ajx, __ffma2_rn(fW, __ffma2_rn(vjx, m1, vix), __ffma2_rn(fb, dx, sx)));
         sy = __ffma2_rn(g7, Ajy, __ffma2_rn(fW, __ffma2_rn(vjy, m1, viy), __ffma2_rn(fb, dy, sy)));
         sz = __ffma2_rn(g7, Ajz, __ffma2_rn(fW, __ffma2_rn(vjz, m1, viz), __ffma2_rn(fb, dz, sz)));
@@ -413,7 +421,8 @@ __device__ __forceinline__ double group_total(double v, int lps, int lane, bool 
 // pass 1 sums A and Phi of every body and publishes them to aux, pass 2 the
 // EIH terms. a[q] = A + c^-2 G S (FP64 results; FP32 pair arithmetic when
 // MIXED, with aux pair-interleaved like the slab: 32 float4 of
-// (A_x, A_x', A_y, A_y') then 32 of (A_z, A_z', Phi, Phi')).
+// (A_x, A_x', A_y, A_y') / 2 then 32 of (A_z / 2, A_z' / 2, Q, Q'),
+// Q = 2 |v|^2 - Phi).
 template <bool MIXED, int UNROLL>
 __device__ __forceinline__ void eih_accel(const EnsSlab<MIXED>& slab, typename EnsAux<MIXED>::T4* aux, int n,
                                           int lane, bool two, bool v0, bool v1, bool sec, int sb, int sub, int lps,
@@ -447,12 +456,13 @@ __device__ __forceinline__ void eih_accel(const EnsSlab<MIXED>& slab, typename E
     for (int q = 0; q < 2; ++q) {
         if (q == 1 && !two) continue;
         const int b = lane + 32 * q;
-        if constexpr (MIXED) {
+        if constexpr (MIXED) {  // A / 2 and Q = 2 |v|^2 - Phi, the forms eih_terms_f32 reads
             float* xa = reinterpret_cast<float*>(aux);
             float* xb = reinterpret_cast<float*>(aux + 32);
             const int o = pslot(b);
-            xa[o] = (float)A[q][0]; xa[o + 2] = (float)A[q][1];
-            xb[o] = (float)A[q][2]; xb[o + 2] = (float)A[q][3];
+            const double w = (double)reinterpret_cast<const float*>(slab.F)[b];
+            xa[o] = (float)(0.5 * A[q][0]); xa[o + 2] = (float)(0.5 * A[q][1]);
+            xb[o] = (float)(0.5 * A[q][2]); xb[o + 2] = (float)(2.0 * w - A[q][3]);
         } else {
             if (q ? v1 : v0) aux[b] = make_double4(A[q][0], A[q][1], A[q][2], A[q][3]);
         }
@@ -465,9 +475,9 @@ __device__ __forceinline__ void eih_accel(const EnsSlab<MIXED>& slab, typename E
         double sx, sy, sz;
         if constexpr (MIXED) {
             const float4* xa = reinterpret_cast<const float4*>(aux);
-            const float phi_i = reinterpret_cast<const float*>(aux + 32)[pslot(idx) + 2];
+            const float Q_i = reinterpret_cast<const float*>(aux + 32)[pslot(idx) + 2];
             float3 S;
-            eih_terms_f32<UNROLL>(slab, xa, xa + 32, np, q ? sub : 0, q ? lps : 1, slab_body(slab, idx), phi_i,
+            eih_terms_f32<UNROLL>(slab, xa, xa + 32, np, q ? sub : 0, q ? lps : 1, slab_body(slab, idx), Q_i,
                                   (float)eps2, S);
             sx = S.x; sy = S.y; sz = S.z;
         } else {

@@ -854,24 +854,25 @@ __device__ __forceinline__ void interact_pn_f64(const double4 e, const double4 e
 
 // Two entries at once with the paired FP32 instructions, force law Newton +
 // 1PN: the Newtonian term into (ax, ay, az) as interact2_f32 forms it and the
-// 1PN term (PnPair::pn1) into (px, py, pz), both divided by G. A, B: entry
-// positions and masses as in interact2_f32; VA = (vx0, vx1, vy0, vy1),
-// VB = (vz0, vz1, |v0|^2, |v1|^2) the entries' velocities. Per body,
-// broadcast to both halves: nb = -(position), vi = velocity, nvi2 = -|vi|^2,
-// mi5 = 5 m_i.
+// 1PN sum of newton_pn1_x2 into (px, py, pz) (the 1PN term divided by G is
+// -c^-2 times it). A, B: entry positions and masses as in interact2_f32;
+// VA = (vx0, vx1, vy0, vy1), VB = (vz0, vz1, |v0|^2, |v1|^2) the entries'
+// velocities. Per body, broadcast to both halves: nb = -(position),
+// vi = velocity, vi4 = 4 vi, nvi2 = -|vi|^2, mi5G = 5 G m_i; G4 = 4 G.
 template <bool GUARD>
 __device__ __forceinline__ void interact2_pn1_f32(const float4 A, const float4 B, const float4 VA, const float4 VB,
                                                   const float2 nbx, const float2 nby, const float2 nbz,
                                                   const float2 vix, const float2 viy, const float2 viz,
-                                                  const float2 nvi2, const float2 mi5, const float2 eps2,
-                                                  const float2 G, const float2 c2, float2& ax, float2& ay, float2& az,
-                                                  float2& px, float2& py, float2& pz) {
+                                                  const float2 vi4x, const float2 vi4y, const float2 vi4z,
+                                                  const float2 nvi2, const float2 mi5G, const float2 eps2,
+                                                  const float2 G4, float2& ax, float2& ay, float2& az, float2& px,
+                                                  float2& py, float2& pz) {
     const float2 dx = __fadd2_rn(make_float2(A.x, A.y), nbx);  // entry - body
     const float2 dy = __fadd2_rn(make_float2(A.z, A.w), nby);
     const float2 dz = __fadd2_rn(make_float2(B.x, B.y), nbz);
     newton_pn1_x2<GUARD>(dx, dy, dz, make_float2(B.z, B.w), make_float2(VA.x, VA.y), make_float2(VA.z, VA.w),
-                         make_float2(VB.x, VB.y), make_float2(VB.z, VB.w), vix, viy, viz, nvi2, mi5, eps2, G, c2,
-                         ax, ay, az, px, py, pz);
+                         make_float2(VB.x, VB.y), make_float2(VB.z, VB.w), vix, viy, viz, vi4x, vi4y, vi4z, nvi2,
+                         mi5G, eps2, G4, ax, ay, az, px, py, pz);
 }
 
 __device__ __forceinline__ float4 vel_f4(const double4 v) {
@@ -1041,21 +1042,26 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
                 if constexpr (MIXED && PNL == 1) {  // Newton + 1PN only: two entries per paired instruction
                     // an odd cnt has its last slot half zero-padded by the caller
                     const int np = (cnt + 1) >> 1;
-                    const float2 G2 = make_float2((float)G, (float)G);
-                    const float2 c22 = make_float2((float)pk.c2, (float)pk.c2);
+                    const float Gf = (float)G, mc2 = -(float)pk.c2;
+                    const float2 G4 = make_float2(4.f * Gf, 4.f * Gf);
                     auto body = [&](const float2 nbx, const float2 nby, const float2 nbz, const float4 vf, float mi,
                                     int q0i, int step, CompSum& sx, CompSum& sy, CompSum& sz, float3& p) {
                         const float2 vix = make_float2(vf.x, vf.x), viy = make_float2(vf.y, vf.y),
                                      viz = make_float2(vf.z, vf.z), nvi2 = make_float2(-vf.w, -vf.w),
-                                     mi5 = make_float2(5.f * mi, 5.f * mi);
+                                     vi4x = make_float2(4.f * vf.x, 4.f * vf.x),
+                                     vi4y = make_float2(4.f * vf.y, 4.f * vf.y),
+                                     vi4z = make_float2(4.f * vf.z, 4.f * vf.z),
+                                     mi5G = make_float2(5.f * Gf * mi, 5.f * Gf * mi);
                         float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax, px = ax, py = ax, pz = ax;
 #pragma unroll 2
                         for (int q = q0i; q < np; q += step)
                             interact2_pn1_f32<GUARD>(sm.lpa[warp][q], sm.lpb[warp][q], sm.lva[warp][q],
-                                                     sm.lvb[warp][q], nbx, nby, nbz, vix, viy, viz, nvi2, mi5,
-                                                     eps2f2, G2, c22, ax, ay, az, px, py, pz);
+                                                     sm.lvb[warp][q], nbx, nby, nbz, vix, viy, viz, vi4x, vi4y,
+                                                     vi4z, nvi2, mi5G, eps2f2, G4, ax, ay, az, px, py, pz);
                         sx.add(ax.x + ax.y); sy.add(ay.x + ay.y); sz.add(az.x + az.y);
-                        p.x += px.x + px.y; p.y += py.x + py.y; p.z += pz.x + pz.y;
+                        p.x = fmaf(mc2, px.x + px.y, p.x);
+                        p.y = fmaf(mc2, py.x + py.y, p.y);
+                        p.z = fmaf(mc2, pz.x + pz.y, p.z);
                     };
                     body(nb0x, nb0y, nb0z, vf0, h0.w, 0, 1, sx0, sy0, sz0, p0);
                     if (two) body(nb1x, nb1y, nb1z, vf1, h1.w, sub, lps, sx1, sy1, sz1, p1);

@@ -72,46 +72,53 @@ struct PnPair {
 // sm_100 (add/mul/fma .f32x2), one source in each half of every operand.
 // d = x_j - x_i (both sources), mj their masses, vj their velocities and
 // vj2 = |v_j|^2; per target, broadcast to both halves: vi its velocity,
-// nvi2 = -|v_i|^2 and mi5 = 5 m_i. Adds the Newtonian m_j d / r^3 to a and the
-// 1PN term of PnPair::pn1 (same algebra) to p, both divided by G. GUARD: a
-// zero r^2 (the target itself when unsoftened) contributes nothing.
+// vi4 = 4 v_i, nvi2 = -|v_i|^2 and mi5G = 5 G m_i; G4 = 4 G. Adds the
+// Newtonian m_j d / r^3 to a (divided by G) and to p the 1PN sum
+//   P = sum_j m_j r^-3 [d A + (v_i - v_j) B'],
+//   A = -|v_i|^2 - 2 |v_j|^2 + 4 v_i.v_j + 3/2 (d.v_j / r)^2 + (5 m_i + 4 m_j) G / r,
+//   B' = 4 d.v_i - 3 d.v_j,
+// whose -c^-2 multiple is the 1PN acceleration divided by G: PnPair::pn1 with
+// n = -d / r, B = -B' / r and f = c^-2 m_j / r^2 gathered into m_j r^-3, so
+// that the unit vector and f cost no instructions of their own. GUARD: a zero
+// r^2 (the target itself when unsoftened) contributes nothing.
 template <bool GUARD>
 __device__ __forceinline__ void newton_pn1_x2(const float2 dx, const float2 dy, const float2 dz, const float2 mj,
                                               const float2 vjx, const float2 vjy, const float2 vjz, const float2 vj2,
                                               const float2 vix, const float2 viy, const float2 viz,
-                                              const float2 nvi2, const float2 mi5, const float2 eps2, const float2 G,
-                                              const float2 c2, float2& ax, float2& ay, float2& az, float2& px,
+                                              const float2 vi4x, const float2 vi4y, const float2 vi4z,
+                                              const float2 nvi2, const float2 mi5G, const float2 eps2,
+                                              const float2 G4, float2& ax, float2& ay, float2& az, float2& px,
                                               float2& py, float2& pz) {
     float2 r2 = __ffma2_rn(dz, dz, eps2);
     r2 = __ffma2_rn(dy, dy, r2);
     r2 = __ffma2_rn(dx, dx, r2);
-    float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    float2 s = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
     if (GUARD) {
-        inv.x = r2.x > 0.f ? inv.x : 0.f;
-        inv.y = r2.y > 0.f ? inv.y : 0.f;
+        s.x = r2.x > 0.f ? s.x : 0.f;
+        s.y = r2.y > 0.f ? s.y : 0.f;
     }
-    const float2 inv2 = __fmul2_rn(inv, inv);
-    const float2 sN = __fmul2_rn(__fmul2_rn(mj, inv), inv2);
+    const float2 ms = __fmul2_rn(mj, s);
+    const float2 sN = __fmul2_rn(ms, __fmul2_rn(s, s));  // m_j / r^3
     ax = __ffma2_rn(dx, sN, ax);
     ay = __ffma2_rn(dy, sN, ay);
     az = __ffma2_rn(dz, sN, az);
+    const float2 w = __ffma2_rn(dx, vjx, __ffma2_rn(dy, vjy, __fmul2_rn(dz, vjz)));     // d.v_j
+    const float2 u4 = __ffma2_rn(dx, vi4x, __ffma2_rn(dy, vi4y, __fmul2_rn(dz, vi4z)));  // 4 d.v_i
+    const float2 Bp = __ffma2_rn(w, make_float2(-3.f, -3.f), u4);
+    const float2 ws = __fmul2_rn(w, s);
+    float2 A = __ffma2_rn(vj2, make_float2(-2.f, -2.f), nvi2);
+    A = __ffma2_rn(vi4x, vjx, A);
+    A = __ffma2_rn(vi4y, vjy, A);
+    A = __ffma2_rn(vi4z, vjz, A);
+    A = __ffma2_rn(__fmul2_rn(ws, ws), make_float2(1.5f, 1.5f), A);
+    A = __ffma2_rn(ms, G4, A);
+    A = __ffma2_rn(s, mi5G, A);
+    const float2 sA = __fmul2_rn(sN, A), sB = __fmul2_rn(sN, Bp);
     const float2 m1 = make_float2(-1.f, -1.f);
-    const float2 ninv = __fmul2_rn(inv, m1);
-    const float2 nx = __fmul2_rn(dx, ninv), ny = __fmul2_rn(dy, ninv), nz = __fmul2_rn(dz, ninv);  // source -> target
     const float2 dvx = __ffma2_rn(vjx, m1, vix), dvy = __ffma2_rn(vjy, m1, viy), dvz = __ffma2_rn(vjz, m1, viz);
-    const float2 v12 = __ffma2_rn(vix, vjx, __ffma2_rn(viy, vjy, __fmul2_rn(viz, vjz)));
-    const float2 nv1 = __ffma2_rn(nx, vix, __ffma2_rn(ny, viy, __fmul2_rn(nz, viz)));
-    const float2 nv2 = __ffma2_rn(nx, vjx, __ffma2_rn(ny, vjy, __fmul2_rn(nz, vjz)));
-    // A = -vi^2 - 2 vj^2 + 4 vi.vj + 1.5 (n.vj)^2 + (5 mi + 4 mj) G / r;  B = 4 n.vi - 3 n.vj
-    float2 Aa = __ffma2_rn(vj2, make_float2(-2.f, -2.f), nvi2);
-    Aa = __ffma2_rn(v12, make_float2(4.f, 4.f), Aa);
-    Aa = __ffma2_rn(__fmul2_rn(nv2, nv2), make_float2(1.5f, 1.5f), Aa);
-    Aa = __ffma2_rn(__ffma2_rn(mj, make_float2(4.f, 4.f), mi5), __fmul2_rn(G, inv), Aa);
-    const float2 Bb = __ffma2_rn(nv1, make_float2(4.f, 4.f), __fmul2_rn(nv2, make_float2(-3.f, -3.f)));
-    const float2 f = __fmul2_rn(__fmul2_rn(mj, inv2), c2);
-    px = __ffma2_rn(__ffma2_rn(nx, Aa, __fmul2_rn(dvx, Bb)), f, px);
-    py = __ffma2_rn(__ffma2_rn(ny, Aa, __fmul2_rn(dvy, Bb)), f, py);
-    pz = __ffma2_rn(__ffma2_rn(nz, Aa, __fmul2_rn(dvz, Bb)), f, pz);
+    px = __ffma2_rn(dx, sA, __ffma2_rn(dvx, sB, px));
+    py = __ffma2_rn(dy, sA, __ffma2_rn(dvy, sB, py));
+    pz = __ffma2_rn(dz, sA, __ffma2_rn(dvz, sB, pz));
 }
 
 // The terms of level PNL: 1PN into p, 2PN and 2.5PN into q (kept apart in

@@ -270,8 +270,12 @@ def test_autotuner_picks_and_caches(ctx, tmp_path):
     cache = tmp_path / "tune.json"
     best = tune_ensemble(ctx, off, P, steps=16, space={"warps_per_block": (2, 4), "unroll": (1, 4),
                                                         "schedule": (0, 1)}, cache=cache)
-    assert best["ms_per_step"] == min(t["ms_per_step"] for t in best["timings"])
     assert len(best["timings"]) == 8
+    # the three fastest short runs were timed again, longer; the best of those wins
+    long = [t for t in best["timings"] if "ms_per_step_long" in t]
+    assert len(long) == 3
+    assert sorted(t["ms_per_step"] for t in long) == sorted(t["ms_per_step"] for t in best["timings"])[:3]
+    assert best["ms_per_step_long"] == min(t["ms_per_step_long"] for t in long)
     import torch
     assert best["key"].startswith(torch.cuda.get_device_name(ctx.device) + "|")
     assert cache.exists()
