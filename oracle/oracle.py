@@ -19,6 +19,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_LIB = HERE / "_ref" / "libaster_ref.so"
+REFCL_LIB = HERE / "_ref" / "libaster_refcl.so"
 ORC_LIB = HERE / "_build" / "libaster_oracle.so"
 
 _D = ctypes.POINTER(ctypes.c_double)
@@ -163,6 +164,47 @@ class Ref:
         args = [_c64(v1), _c64(v2), _c64(p1), _c64(p2)]
         self.lib.ref_pair_force(m1, m2, *[_p(a, _D) for a in args], _p(f, _D))
         return f
+
+
+class RefCL:
+    """The reference's OpenCL tree construction (gen_mortons, the bitonic
+    sort, build_tree) compiled from its kernel text and run on the CPU under a
+    work-group emulator (oracle/ref_cl; oracle/Makefile ->
+    oracle/_ref/libaster_refcl.so), launched as BH_hyper's host code launches
+    it (src/solvers/full_GPU.cpp:52-112, 312-338)."""
+
+    _lib = None
+
+    def __init__(self):
+        if RefCL._lib is None:
+            if not REFCL_LIB.exists():
+                raise FileNotFoundError(f"{REFCL_LIB} missing: run `make -C oracle REF=<reference source tree>`")
+            lib = ctypes.CDLL(str(REFCL_LIB))
+            lib.refcl_build.argtypes = [ctypes.c_long, _D, _D, _D, _U32, _U32, _I32, _I32, _I32, _I32]
+            lib.refcl_build.restype = ctypes.c_int
+            RefCL._lib = lib
+        self.lib = RefCL._lib
+
+    @staticmethod
+    def available() -> bool:
+        return REFCL_LIB.exists()
+
+    def build(self, pos, m, bd):
+        """pos (n, 3), masses (n,), bd: the bounding half-sizes (3,). Returns
+        the per-body codes, the sorted codes and body order of the sort's
+        first n entries, and the 2n - 1 node links (left, right, parent)."""
+        pos, m = _c64(pos), _c64(m)
+        bd = _c64(np.broadcast_to(np.asarray(bd, dtype=np.float64), (3,)))
+        n = len(m)
+        out = dict(codes=np.zeros(n, np.uint32), sorted_codes=np.zeros(n, np.uint32), perm=np.zeros(n, np.int32),
+                   left=np.zeros(2 * n - 1, np.int32), right=np.zeros(2 * n - 1, np.int32),
+                   parent=np.zeros(2 * n - 1, np.int32))
+        st = self.lib.refcl_build(n, _p(pos, _D), _p(m, _D), _p(bd, _D), _p(out["codes"], _U32),
+                                  _p(out["sorted_codes"], _U32), _p(out["perm"], _I32), _p(out["left"], _I32),
+                                  _p(out["right"], _I32), _p(out["parent"], _I32))
+        if st != 0:
+            raise ValueError("refcl_build needs n >= 2")
+        return out
 
 
 class Orc:

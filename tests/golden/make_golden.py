@@ -36,6 +36,13 @@ Fixtures:
                             (gen.kepler_orbits: elliptic, near-parabolic and
                             hyperbolic), dt = 0.05, 40 steps: final x, v.
 
+  opencl_tree.npz           the reference's OpenCL tree construction (its kernel
+                            text for gen_mortons, the bitonic sort and build_tree,
+                            run on the CPU: oracle/ref_cl -> libaster_refcl.so) on
+                            Plummer spheres of n = 2, 3, 100, 257, 1000, 3000 with a
+                            duplicated position and a coordinate at +B: per-body
+                            codes, sorted codes, body order, left/right/parent.
+
 `python tests/golden/make_golden.py pn_pairs` regenerates one fixture only.
 """
 from __future__ import annotations
@@ -49,7 +56,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from aster_b200 import gen  # noqa: E402
-from oracle.oracle import NEWTON, PN1, PN2, PN25, Ref  # noqa: E402
+from oracle.oracle import NEWTON, PN1, PN2, PN25, Ref, RefCL  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 
@@ -169,9 +176,30 @@ def kepler_fixture(ref: Ref):
                         ref_pos=rp, ref_vel=rv)
 
 
+def opencl_cases():
+    """The inputs of opencl_tree.npz: (n, positions, masses, B)."""
+    for n, seed in ((2, 1), (3, 2), (100, 3), (257, 6), (1000, 7), (3000, 8)):
+        pos, _, m = gen.plummer(n, seed)
+        if n > 10:
+            pos[7] = pos[9]                     # equal codes: tie broken by body index
+            pos[3, 0] = np.abs(pos).max()       # a coordinate at +B (1024 wraps to 0)
+        yield n, pos, m, float(np.abs(pos).max())
+
+
+def opencl_fixture(ref: Ref):
+    cl = RefCL()
+    out = {}
+    for n, pos, m, B in opencl_cases():
+        r = cl.build(pos, m, B)
+        out[f"n{n}_pos"], out[f"n{n}_m"], out[f"n{n}_B"] = pos, m, B
+        for k, v in r.items():
+            out[f"n{n}_{k}"] = v
+    np.savez_compressed(OUT / "opencl_tree.npz", **out)
+
+
 FIXTURES = {"allpairs": allpairs_fixture, "leapfrog": leapfrog_fixture, "tree": tree_fixture,
             "pn_pairs": pn_fixture, "saba": saba_fixture, "allpairs_pn": allpairs_pn_fixture,
-            "kepler": kepler_fixture}
+            "kepler": kepler_fixture, "opencl": opencl_fixture}
 
 
 def main():

@@ -70,7 +70,8 @@ def test_tree_vs_oracle_ragged(ctx, orc, bits):
 
 def test_compat_mode_matches_opencl_semantics(ctx, orc):
     """compat_mode = 1: OpenCL gen_mortons (1024 wraps to 0), descending
-    (code, index) order, Karras tie-break on body indices."""
+    (code, index) order, Karras tie-break on body indices; against the oracle
+    and, where built, the reference's OpenCL kernels run on the host."""
     pos, _, m = gen.plummer(5000, 88)
     pos[7] = pos[9]
     B = float(np.abs(pos).max())
@@ -83,6 +84,13 @@ def test_compat_mode_matches_opencl_semantics(ctx, orc):
     np.testing.assert_array_equal(t["perm"], perm)
     np.testing.assert_array_equal(t["left"], k["left"])
     np.testing.assert_array_equal(t["right"], k["right"])
+    from oracle.oracle import RefCL
+    if RefCL.available():  # the reference's own OpenCL kernels, run on the host
+        r = RefCL().build(pos, m, B)
+        np.testing.assert_array_equal(t["codes"], r["codes"])
+        np.testing.assert_array_equal(t["perm"], r["perm"])
+        np.testing.assert_array_equal(t["left"], r["left"])
+        np.testing.assert_array_equal(t["right"], r["right"])
 
 
 @pytest.mark.parametrize("theta", [0.0, 0.3, 0.5, 0.8])

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import golden, rel_l2
-from oracle.oracle import NEWTON, PN1, PN2, PN25, Ref
+from oracle.oracle import NEWTON, PN1, PN2, PN25, Ref, RefCL
 
 
 def test_allpairs_matches_reference_golden(orc):
@@ -338,3 +338,46 @@ def test_node_velocities_are_mass_weighted(orc):
     nv = orc.node_velocities(o, o["perm"], vel)
     np.testing.assert_array_equal(nv[:500], vel[o["perm"]])
     assert np.abs(nv[500] - (vel * m[:, None]).sum(0) / m.sum()).max() < 1e-13
+
+
+def _compat_oracle_tree(orc, pos, m, B):
+    codes = orc.morton30(pos, B, compat=True).astype(np.uint64)
+    sc, perm = orc.sort_codes(codes, bits=30, descending=True)
+    k = orc.karras(sc, perm, bits=30, compat=True)
+    return codes, sc, perm, k
+
+
+def _check_compat_against_opencl(orc, pos, m, B, r, n):
+    codes, sc, perm, k = _compat_oracle_tree(orc, pos, m, B)
+    np.testing.assert_array_equal(codes, r["codes"], err_msg=f"gen_mortons n={n}")
+    np.testing.assert_array_equal(sc, r["sorted_codes"], err_msg=f"bitonic sort codes n={n}")
+    np.testing.assert_array_equal(perm, r["perm"], err_msg=f"bitonic sort order n={n}")
+    for key in ("left", "right", "parent"):  # leaves carry -1 children in both
+        np.testing.assert_array_equal(k[key], r[key], err_msg=f"build_tree {key} n={n}")
+
+
+def test_compat_mode_matches_reference_opencl_golden(orc):
+    """compat_mode = 1 restated in the oracle (OpenCL gen_mortons, descending
+    (code, index) order, Karras tie-break on body indices) against the
+    reference's own OpenCL kernels (morton_writer.cl.h:72-122, radix.cl.h:26-91,
+    BHH_specific.cl.h:171-273) run on the CPU with BH_hyper's launch sequence
+    (full_GPU.cpp:52-112, 312-338): fixture opencl_tree.npz."""
+    g = golden("opencl_tree.npz")
+    sizes = sorted({int(k.split("_")[0][1:]) for k in g.files})
+    assert sizes == [2, 3, 100, 257, 1000, 3000]
+    for n in sizes:
+        r = {k: g[f"n{n}_{k}"] for k in ("codes", "sorted_codes", "perm", "left", "right", "parent")}
+        _check_compat_against_opencl(orc, g[f"n{n}_pos"], g[f"n{n}_m"], float(g[f"n{n}_B"]), r, n)
+
+
+@pytest.mark.skipif(not RefCL.available(), reason="reference OpenCL kernel build absent (fixture covers it)")
+@pytest.mark.parametrize("n", [255, 256, 511, 4097])
+def test_compat_mode_matches_live_reference_opencl(orc, n):
+    """The same against the live reference kernels at sizes around the
+    bitonic sort's power-of-two padding, with many equal codes (a cluster of
+    identical positions)."""
+    from aster_b200 import gen
+    pos, _, m = gen.plummer(n, 4000 + n)
+    pos[: n // 8] = pos[n // 8]
+    B = float(np.abs(pos).max())
+    _check_compat_against_opencl(orc, pos, m, B, RefCL().build(pos, m, B), n)
