@@ -184,8 +184,11 @@ int aster_kick_drift_coef(aster_ctx* ctx, double kick_dt, double drift_dt, bool 
                           bool want_mixed);
 // lbvh.cu
 int aster_lbvh_build_dev(aster_ctx* ctx, const aster_params* p, bool box_ready);
+// fuse_next (with closing_kick): the walk also applies the next step's
+// opening kick and drift to every body and leaves their bounding box in
+// red_box, so that step's kick-drift launch is left out.
 int aster_lbvh_walk_launch(aster_ctx* ctx, const aster_params* p, int precision,
-                           bool closing_kick, int32_t* list_counts_dev);
+                           bool closing_kick, int32_t* list_counts_dev, bool fuse_next = false);
 
 // ---- device helpers --------------------------------------------------------
 __device__ __forceinline__ void ds_split(double x, float& hi, float& lo) {

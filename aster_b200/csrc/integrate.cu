@@ -211,7 +211,8 @@ struct PhaseTimer {
 };
 
 static int force_eval(aster_ctx* c, const aster_params* p, int solver, int precision, bool closing_kick,
-                      bool box_ready, PhaseTimer* tm, double* ms_build, double* ms_force, int* pairs) {
+                      bool box_ready, PhaseTimer* tm, double* ms_build, double* ms_force, int* pairs,
+                      bool fuse_next = false) {
     int e0 = tm ? tm->mark(c->stream) : -1;
     if (solver == ASTER_SOLVER_ALLPAIRS) {
         ASTER_TRY(aster_allpairs_launch(c, p, precision, closing_kick, c->n, nullptr, nullptr));
@@ -220,7 +221,7 @@ static int force_eval(aster_ctx* c, const aster_params* p, int solver, int preci
     }
     ASTER_TRY(aster_lbvh_build_dev(c, p, box_ready));
     int e1 = tm ? tm->mark(c->stream) : -1;
-    ASTER_TRY(aster_lbvh_walk_launch(c, p, precision, closing_kick, nullptr));
+    ASTER_TRY(aster_lbvh_walk_launch(c, p, precision, closing_kick, nullptr, fuse_next));
     if (tm) pairs[0] = e0, pairs[1] = e1, pairs[2] = tm->mark(c->stream);
     (void)ms_build;
     (void)ms_force;
@@ -298,6 +299,19 @@ static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precisi
         ASTER_TRY(aster_kick_drift_launch(c, p, solver == ASTER_SOLVER_LBVH, mixed_ap));
         return force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, last);
     };
+    // Tree steps: every walk but the last also applies the next step's opening
+    // kick and drift (and its bounding box), so only the first step launches
+    // the kick-drift kernel: first = kick-drift + build + walk(fused), middle =
+    // build + walk(fused) (captured and replayed), last = build + walk.
+    const bool fuse = solver == ASTER_SOLVER_LBVH && nsteps >= 2;
+    auto first = [&]() -> int {
+        ASTER_TRY(aster_kick_drift_launch(c, p, true, false));
+        return force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, last, true);
+    };
+    auto middle = [&]() -> int { return force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, last, true); };
+    auto final_step = [&]() -> int {
+        return force_eval(c, p, solver, precision, true, true, tm, nullptr, nullptr, last, false);
+    };
     auto done = [&]() -> int {
         if (tm) {
             for (int k = 0; k < 3; ++k) marks[*nm][k] = last[k];
@@ -342,7 +356,15 @@ static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precisi
         ++*nm;
         return ASTER_OK;
     };
-    ASTER_TRY(repeat_steps(c, nsteps, true, step, done, replay));
+    if (fuse) {
+        ASTER_TRY(first());
+        ASTER_TRY(done());
+        ASTER_TRY(repeat_steps(c, nsteps - 2, true, middle, done, replay));
+        ASTER_TRY(final_step());
+        ASTER_TRY(done());
+    } else {
+        ASTER_TRY(repeat_steps(c, nsteps, true, step, done, replay));
+    }
     c->acc_valid = true;  // a(x) of the final positions (valid once the work completes without error)
     c->tree.built = false;
     return ASTER_OK;

@@ -933,7 +933,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
     const int32_t* __restrict__ perm, double G, double eps2, double half_dt, double4* __restrict__ acc,
     double4* __restrict__ vel, int* __restrict__ err, int* __restrict__ stack_hw, int stack_limit,
     int32_t* __restrict__ body_counts, unsigned long long* __restrict__ inter_count,
-    const double4* __restrict__ node_v, PnK<double> pk) {
+    const double4* __restrict__ node_v, PnK<double> pk, double4* __restrict__ pm_next, double dt_next,
+    unsigned long long* __restrict__ box_next) {
     using Shared = typename std::conditional<PNL != 0, WalkSharedPn<MIXED>, WalkShared<MIXED>>::type;
     __shared__ Shared sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -944,6 +945,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
     int* stack = sm.stack[warp];
     int hw = 1;
     unsigned long long wtotal = 0;
+    double bmax = 0.0;  // fused next drift: max |coordinate| of the drifted bodies
 
     for (;;) {
         unsigned int g = 0;
@@ -1313,9 +1315,25 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
             if (KICK) {
                 double4 vv = vel[b];
                 vv.x += ax * half_dt; vv.y += ay * half_dt; vv.z += az * half_dt;
+                if (pm_next) {
+                    // the next step's opening kick and drift, the same operations
+                    // in the same order as its kick-drift kernel would apply them
+                    // (that kernel does not run then); other bodies' positions
+                    // are read from the tree, never from pm
+                    vv.x += ax * half_dt; vv.y += ay * half_dt; vv.z += az * half_dt;
+                    double4 pp = pm_next[b];
+                    pp.x += vv.x * dt_next; pp.y += vv.y * dt_next; pp.z += vv.z * dt_next;
+                    pm_next[b] = pp;
+                    bmax = fmax(bmax, fmax(fabs(pp.x), fmax(fabs(pp.y), fabs(pp.z))));
+                }
                 vel[b] = vv;
             }
         }
+    }
+    if (box_next) {
+        for (int o = 16; o > 0; o >>= 1) bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+        // non-negative doubles order like their bit patterns
+        if (lane == 0) atomicMax(box_next, (unsigned long long)__double_as_longlong(bmax));
     }
     if (lane == 0) {
         atomicMax(stack_hw, hw);
@@ -1324,7 +1342,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
 }
 
 template <bool MIXED, bool GUARD, bool KICK, int PNL = 0>
-int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts) {
+int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts, bool fuse_next) {
     LbvhBufs& t = c->tree;
     auto kern = k_walk<MIXED, GUARD, KICK, PNL>;
     int per_sm = 0;
@@ -1338,7 +1356,8 @@ int launch_walk(aster_ctx* c, const aster_params* p, int32_t* counts) {
         c->n, t.groups.as<int2>(), gcount, gcount + 1,
         t.crec.as<float4>(), t.node_cm.as<double4>(), t.child.as<int2>(), t.perm.as<int32_t>(), p->G, p->eps2, 0.5 * p->dt,
         c->acc.as<double4>(), c->vel.as<double4>(), c->err_dev, c->stack_hw_dev, c->walk_stack_limit, counts,
-        red_inter(c), PNL > 0 ? t.node_v.as<double4>() : nullptr, make_pn(p));
+        red_inter(c), PNL > 0 ? t.node_v.as<double4>() : nullptr, make_pn(p),
+        KICK && fuse_next ? c->pm.as<double4>() : nullptr, p->dt, KICK && fuse_next ? red_box(c) : nullptr);
     ASTER_CUDA(cudaGetLastError());
     return ASTER_OK;
 }
@@ -1486,9 +1505,13 @@ int aster_lbvh_build_dev(aster_ctx* c, const aster_params* p, bool box_ready) {
     return ASTER_OK;
 }
 
-int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, bool kick, int32_t* counts) {
+int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, bool kick, int32_t* counts,
+                           bool fuse_next) {
     if (kick) c->mixed_valid = false;  // the closing kick moves the velocities
+    fuse_next = fuse_next && kick;
     ASTER_CUDA(cudaMemsetAsync(red_groups(c) + 1, 0, sizeof(unsigned int), c->stream));  // work counter
+    // the fused drift's box (the build that just ran has read the previous one)
+    if (fuse_next) ASTER_CUDA(cudaMemsetAsync(red_box(c), 0, sizeof(unsigned long long), c->stream));
     const bool guard = !(p->eps2 > 0.0);
     if (precision != ASTER_MIXED && precision != ASTER_FP64) return ASTER_ERR_INVALID_ARG;
     const bool mixed = precision == ASTER_MIXED;
@@ -1506,24 +1529,24 @@ int aster_lbvh_walk_launch(aster_ctx* c, const aster_params* p, int precision, b
         ASTER_CUDA(cudaGetLastError());
         c->stats.kernels += 1;
         if (mixed && pn_level(p) == 1) {  // Newton + 1PN: the paired-FP32 list evaluation
-            if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true, 1>(c, p, counts) : launch_walk<true, true, false, 1>(c, p, counts)); }
-            else       { ASTER_TRY(kick ? launch_walk<true, false, true, 1>(c, p, counts) : launch_walk<true, false, false, 1>(c, p, counts)); }
+            if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true, 1>(c, p, counts, fuse_next) : launch_walk<true, true, false, 1>(c, p, counts, fuse_next)); }
+            else       { ASTER_TRY(kick ? launch_walk<true, false, true, 1>(c, p, counts, fuse_next) : launch_walk<true, false, false, 1>(c, p, counts, fuse_next)); }
         } else if (mixed) {
-            if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true, 2>(c, p, counts) : launch_walk<true, true, false, 2>(c, p, counts)); }
-            else       { ASTER_TRY(kick ? launch_walk<true, false, true, 2>(c, p, counts) : launch_walk<true, false, false, 2>(c, p, counts)); }
+            if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true, 2>(c, p, counts, fuse_next) : launch_walk<true, true, false, 2>(c, p, counts, fuse_next)); }
+            else       { ASTER_TRY(kick ? launch_walk<true, false, true, 2>(c, p, counts, fuse_next) : launch_walk<true, false, false, 2>(c, p, counts, fuse_next)); }
         } else {
-            if (guard) { ASTER_TRY(kick ? launch_walk<false, true, true, 2>(c, p, counts) : launch_walk<false, true, false, 2>(c, p, counts)); }
-            else       { ASTER_TRY(kick ? launch_walk<false, false, true, 2>(c, p, counts) : launch_walk<false, false, false, 2>(c, p, counts)); }
+            if (guard) { ASTER_TRY(kick ? launch_walk<false, true, true, 2>(c, p, counts, fuse_next) : launch_walk<false, true, false, 2>(c, p, counts, fuse_next)); }
+            else       { ASTER_TRY(kick ? launch_walk<false, false, true, 2>(c, p, counts, fuse_next) : launch_walk<false, false, false, 2>(c, p, counts, fuse_next)); }
         }
         c->stats.kernels += 1;
         return ASTER_OK;
     }
     if (mixed) {
-        if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true>(c, p, counts) : launch_walk<true, true, false>(c, p, counts)); }
-        else       { ASTER_TRY(kick ? launch_walk<true, false, true>(c, p, counts) : launch_walk<true, false, false>(c, p, counts)); }
+        if (guard) { ASTER_TRY(kick ? launch_walk<true, true, true>(c, p, counts, fuse_next) : launch_walk<true, true, false>(c, p, counts, fuse_next)); }
+        else       { ASTER_TRY(kick ? launch_walk<true, false, true>(c, p, counts, fuse_next) : launch_walk<true, false, false>(c, p, counts, fuse_next)); }
     } else {
-        if (guard) { ASTER_TRY(kick ? launch_walk<false, true, true>(c, p, counts) : launch_walk<false, true, false>(c, p, counts)); }
-        else       { ASTER_TRY(kick ? launch_walk<false, false, true>(c, p, counts) : launch_walk<false, false, false>(c, p, counts)); }
+        if (guard) { ASTER_TRY(kick ? launch_walk<false, true, true>(c, p, counts, fuse_next) : launch_walk<false, true, false>(c, p, counts, fuse_next)); }
+        else       { ASTER_TRY(kick ? launch_walk<false, false, true>(c, p, counts, fuse_next) : launch_walk<false, false, false>(c, p, counts, fuse_next)); }
     }
     c->stats.kernels += 1;
     return ASTER_OK;

@@ -117,6 +117,24 @@ def test_upload_with_accelerations_continues_bit_exactly(ctx):
         np.testing.assert_array_equal(ov, cv)
 
 
+@pytest.mark.parametrize("prec,law", [(MIXED, NEWTON), (FP64, NEWTON), (MIXED, NEWTON | PN1)])
+def test_tree_steps_fused_drift_equal_single_steps(ctx, prec, law):
+    """A multi-step tree run applies each next step's opening kick and drift
+    inside the previous walk (no kick-drift launch); single-step calls run the
+    kick-drift kernel every step. Both give the same state bit for bit."""
+    pos, vel, m = gen.plummer(6000, 1030, masses="lognormal")
+    p = Params(G=1.0, eps2=0.005 ** 2, dt=5e-4, theta=0.5, c=30.0, force_law=law)
+    ctx.upload(pos, vel, m)
+    ctx.kdk_steps(p, 6, SOLVER_LBVH, prec)
+    fused = ctx.download()
+    ctx.upload(pos, vel, m)
+    for _ in range(6):
+        ctx.kdk_steps(p, 1, SOLVER_LBVH, prec)
+    single = ctx.download()
+    for a, b in zip(fused, single):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_kdk_steps_host_equals_separate_calls(ctx):
     """aster_kdk_steps_host (one call, the positions' copy overlapping the last
     force evaluation) equals upload_acc + kdk_steps + download bit for bit."""
