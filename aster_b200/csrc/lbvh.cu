@@ -758,6 +758,9 @@ struct WalkSharedPn : WalkShared<MIXED> {
     double4 lvd[WALK_WARPS][MIXED ? 1 : WALK_LIST_FP64];
 };
 
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 __device__ __forceinline__ float warp_min_f(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
@@ -963,6 +966,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
         const bool v0 = lane < gr.y, v1 = two && sb < r;
         const int64_t k0 = (int64_t)gr.x + (v0 ? lane : 0);
         const int64_t k1 = (int64_t)gr.x + (v1 ? 32 + sb : 0);
+        // the bodies' input indices, for the results (loaded now, used at the end)
+        const int32_t pb0 = perm[k0], pb1 = perm[k1];
 
         float4 h0, l0, h1, l1;  // the bodies' traversal data, from their leaves
         leaf_trav(node_cm[k0], h0, l0);
@@ -1272,6 +1277,14 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
             }
         }
         __syncwarp();
+        if (KICK) {  // the closing kick's operands into L1 while the last list is evaluated
+            prefetch_l1(vel + pb0);
+            if (pm_next) prefetch_l1(pm_next + pb0);
+            if (v1 && sub == 0) {
+                prefetch_l1(vel + pb1);
+                if (pm_next) prefetch_l1(pm_next + pb1);
+            }
+        }
         if (lc > 0) evaluate(lc);
         __syncwarp();
         wtotal += (unsigned long long)total * (unsigned long long)gr.y;
@@ -1309,7 +1322,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
             } else {
                 ax = G * dx0; ay = G * dy0; az = G * dz0;
             }
-            const int32_t b = perm[q ? k1 : k0];
+            const int32_t b = q ? pb1 : pb0;
             acc[b] = make_double4(ax, ay, az, 0.0);
             if (body_counts) body_counts[b] = total;
             if (KICK) {
