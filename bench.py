@@ -68,9 +68,10 @@ FLOP_PER_ADJ_PAIR = 48
 BUILD_BYTES_PER_BODY = 240
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_walk launch captured with
-# ncu at N = 2^19 (77.60 + 7.19 MB read + written), scaled
-# by the number of bodies to N = 2^20 (the walk reads each tree node about once).
-WALK_TRAFFIC_BYTES = 84.79e6 * 2
+# ncu at N = 2^19 (103.82 + 17.07 MB read + written, the fused next drift's
+# position read and write included), scaled by the number of bodies to
+# N = 2^20 (the walk reads each tree node about once).
+WALK_TRAFFIC_BYTES = 120.89e6 * 2
 
 
 def fp_peaks(f_mhz: float):
