@@ -146,9 +146,11 @@ int aster_check_params(const aster_params* p);
 int aster_begin(aster_ctx* ctx);                // clears the device error flag
 int aster_finish(aster_ctx* ctx);               // syncs, turns flags into status
 int aster_refresh_mixed(aster_ctx* ctx);        // rebuild phi/plo/vf from pm/vel
-// Host state -> device with the masses' copy overlapped (see context.cu)
+// Host state -> device with the masses' copy overlapped (see context.cu); with
+// kick_drift, the first KDK step's opening kick, drift and bounding box
+// (red_box) are applied while unpacking, so its kick-drift launch is left out
 int aster_upload_enqueue_overlapped(aster_ctx* c, int64_t n, const double* pos, const double* vel, const double* mass,
-                                    const double* acc);
+                                    const double* acc, const aster_params* kick_drift = nullptr);
 // velocities and accelerations -> host (one unpack, two back-to-back copies)
 int aster_download_va_enqueue(aster_ctx* c, double* vel, double* acc, cudaStream_t stream);
 // applies masses still on their way (waits for their copy); no-op otherwise

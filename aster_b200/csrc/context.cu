@@ -317,6 +317,41 @@ __global__ void k_pack_pva(int64_t n, const double* __restrict__ pos, const doub
     }
 }
 
+// k_pack_pva followed by the first KDK step's opening kick and drift
+// (v += a dt/2, x += v dt, the same operations in the same order as the
+// kick-drift kernel) and the drifted bodies' bounding box: one pass over the
+// staged state instead of two.
+__global__ void k_pack_kick_drift(int64_t n, const double* __restrict__ pos, const double* __restrict__ vel,
+                                  const double* __restrict__ acc, double half_dt, double dt,
+                                  double4* __restrict__ pm, double4* __restrict__ v4, double4* __restrict__ a4,
+                                  int* err, unsigned long long* __restrict__ box_bits) {
+    double bmax = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double4 p = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], 0.0);
+        double4 v = make_double4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], 0.0);
+        const double4 a = make_double4(acc[3 * i], acc[3 * i + 1], acc[3 * i + 2], 0.0);
+        if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z) &&
+              isfinite(a.x) && isfinite(a.y) && isfinite(a.z)))
+            atomicOr(err, ASTER_DEVERR_NONFINITE);
+        a4[i] = a;
+        v.x += a.x * half_dt; v.y += a.y * half_dt; v.z += a.z * half_dt;
+        p.x += v.x * dt; p.y += v.y * dt; p.z += v.z * dt;
+        pm[i] = p;
+        v4[i] = v;
+        bmax = fmax(bmax, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))));
+    }
+    for (int o = 16; o > 0; o >>= 1) bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bmax;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double w = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_xor_sync(0xffffffffu, w, o));
+        // non-negative doubles order like their bit patterns
+        if (threadIdx.x == 0) atomicMax(box_bits, (unsigned long long)__double_as_longlong(w));
+    }
+}
+
 __global__ void k_set_mass(int64_t n, const double* __restrict__ mass, double4* __restrict__ pm, int* err) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double m = mass[i];
@@ -333,7 +368,7 @@ __global__ void k_set_mass(int64_t n, const double* __restrict__ mass, double4* 
 // build before its first mass read, waits for them. The FP32 copies are not
 // written (the tree path does not read them). Requires c->copy_stream.
 int aster_upload_enqueue_overlapped(aster_ctx* c, int64_t n, const double* pos, const double* vel, const double* mass,
-                                    const double* acc) {
+                                    const double* acc, const aster_params* kick_drift) {
     const size_t n4d = (size_t)n * sizeof(double4), n4f = (size_t)n * sizeof(float4);
     ASTER_TRY(c->pm.ensure(n4d));
     ASTER_TRY(c->vel.ensure(n4d));
@@ -354,8 +389,16 @@ int aster_upload_enqueue_overlapped(aster_ctx* c, int64_t n, const double* pos, 
     ASTER_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev[3], 0));
     ASTER_CUDA(cudaMemcpyAsync(sm, mass, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->copy_stream));
     ASTER_CUDA(cudaEventRecord(c->ev[4], c->copy_stream));
-    k_pack_pva<<<grid_for(c, n, 256), 256, 0, c->stream>>>(n, sp, sv, sa, c->pm.as<double4>(), c->vel.as<double4>(),
-                                                           c->acc.as<double4>(), c->err_dev);
+    if (kick_drift) {
+        ASTER_TRY(c->red.ensure(4096));
+        ASTER_CUDA(cudaMemsetAsync(red_box(c), 0, sizeof(unsigned long long), c->stream));
+        k_pack_kick_drift<<<grid_for(c, n, 256), 256, 0, c->stream>>>(
+            n, sp, sv, sa, 0.5 * kick_drift->dt, kick_drift->dt, c->pm.as<double4>(), c->vel.as<double4>(),
+            c->acc.as<double4>(), c->err_dev, red_box(c));
+    } else {
+        k_pack_pva<<<grid_for(c, n, 256), 256, 0, c->stream>>>(n, sp, sv, sa, c->pm.as<double4>(),
+                                                               c->vel.as<double4>(), c->acc.as<double4>(), c->err_dev);
+    }
     ASTER_CUDA(cudaGetLastError());
     c->mass_pending = sm;
     c->n = n;

@@ -438,12 +438,14 @@ extern "C" int aster_kdk_steps_host(aster_ctx* c, const aster_params* p, int sol
     c->stats = aster_stats{};
     cudaEventRecord(c->ev[0], c->stream);
     // the tree path reads no mass before its build: their copy overlaps the first kick-drift and sort
-    int st = solver == ASTER_SOLVER_LBVH ? aster_upload_enqueue_overlapped(c, n, pos, vel, mass, acc)
+    // one tree step: its opening kick and drift are applied while the state is unpacked
+    const bool fused = solver == ASTER_SOLVER_LBVH && nsteps == 1;
+    int st = solver == ASTER_SOLVER_LBVH ? aster_upload_enqueue_overlapped(c, n, pos, vel, mass, acc, fused ? p : nullptr)
                                          : aster_upload_enqueue(c, n, pos, vel, mass, acc);
     const bool mixed_ap = solver == ASTER_SOLVER_ALLPAIRS && precision == ASTER_MIXED;
     int dummy[3];
     if (st == ASTER_OK && nsteps > 1) st = kdk_core(c, p, solver, precision, nsteps - 1, nullptr, nullptr, nullptr);
-    if (st == ASTER_OK) st = aster_kick_drift_launch(c, p, solver == ASTER_SOLVER_LBVH, mixed_ap);
+    if (st == ASTER_OK && !fused) st = aster_kick_drift_launch(c, p, solver == ASTER_SOLVER_LBVH, mixed_ap);
     if (st == ASTER_OK) {
         // positions are final: copy them out on the second stream
         cudaEventRecord(c->ev[2], c->stream);
