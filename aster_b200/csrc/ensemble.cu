@@ -179,9 +179,9 @@ __device__ __forceinline__ float2 inv_r_x2_nz(const float2 dx, const float2 dy, 
 
 // Mixed accelerations of target t (without G): sums over the source pairs
 // q = q0, q0 + qs, ... < np (qs > 1: the lanes that share a target split its
-// sources). Levels 0 and 1: two sources per paired FP32 instruction; level 2
-// (any of 1PN/2PN/2.5PN by flags): one source at a time with the pair terms
-// of pn.cuh. The Newtonian, 1PN and 2PN + 2.5PN sums are kept apart.
+// sources). Two sources per paired FP32 instruction at every level: Newton,
+// Newton + 1PN (newton_pn1_x2) and level 2, any of 1PN/2PN/2.5PN by flags
+// (newton_pn_all_x2). The Newtonian, 1PN and 2PN + 2.5PN sums are kept apart.
 template <int PNL, int UNROLL>
 __device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int np, int q0, int qs, const BodyF32& t,
                                           float eps2, float G, const PnK<float>& k, float3& aN, float3& a1,
@@ -221,31 +221,31 @@ __device__ __forceinline__ void accel_f32(const EnsSlab<true>& s, int np, int q0
         px = __fmul2_rn(px, make_float2(mc2, mc2));
         py = __fmul2_rn(py, make_float2(mc2, mc2));
         pz = __fmul2_rn(pz, make_float2(mc2, mc2));
-    } else {
-        float sx = 0.f, sy = 0.f, sz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
-        for (int j = 2 * q0; j < 2 * np; j += (j & 1) ? 2 * qs - 1 : 1) {  // both bodies of each visited pair
-            const BodyF32 o = slab_body(s, j);
-            const float dx = (o.hx - t.hx) + (o.lx - t.lx);
-            const float dy = (o.hy - t.hy) + (o.ly - t.ly);
-            const float dz = (o.hz - t.hz) + (o.lz - t.lz);
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-            float inv = rsqrt_approx(r2);
-            inv = r2 > 0.f ? inv : 0.f;
-            const float inv2 = inv * inv;
-            const float sN = o.m * inv * inv2;
-            sx = fmaf(dx, sN, sx); sy = fmaf(dy, sN, sy); sz = fmaf(dz, sN, sz);
-            PnPair<float> w;
-            w.nx = -dx * inv; w.ny = -dy * inv; w.nz = -dz * inv;
-            w.dvx = t.vx - o.vx; w.dvy = t.vy - o.vy; w.dvz = t.vz - o.vz;
-            w.inv = inv; w.inv2 = inv2; w.mi = t.m; w.mj = o.m; w.vi2 = t.w; w.vj2 = o.w;
-            w.v12 = t.vx * o.vx + t.vy * o.vy + t.vz * o.vz;
-            w.nv1 = w.nx * t.vx + w.ny * t.vy + w.nz * t.vz;
-            w.nv2 = w.nx * o.vx + w.ny * o.vy + w.nz * o.vz;
-            w.G = G;
-            pn_terms<PNL>(k, w, rx, ry, rz, qx, qy, qz);
+    } else {  // the flagged PN terms, two sources per paired instruction as well
+        const float2 vix = make_float2(t.vx, t.vx), viy = make_float2(t.vy, t.vy), viz = make_float2(t.vz, t.vz);
+        const float2 vi4x = make_float2(4.f * t.vx, 4.f * t.vx), vi4y = make_float2(4.f * t.vy, 4.f * t.vy),
+                     vi4z = make_float2(4.f * t.vz, 4.f * t.vz);
+        const float2 nvi2 = make_float2(-t.w, -t.w), vi2 = make_float2(t.w, t.w);
+        const float2 mi5G = make_float2(5.f * G * t.m, 5.f * G * t.m), Gmi = make_float2(G * t.m, G * t.m);
+        const float2 G4 = make_float2(4.f * G, 4.f * G), G2 = make_float2(G, G);
+        const float2 nk = make_float2(-0.8f * k.ic, -0.8f * k.ic);
+        float2 q2x = make_float2(0.f, 0.f), q2y = q2x, q2z = q2x;
+#pragma unroll UNROLL
+        for (int q = q0; q < np; q += qs) {
+            float2 dx, dy, dz;
+            tx.sep(s, q, dx, dy, dz);
+            const float4 b = s.B[q], d = s.D[q], e = s.E[q];
+            newton_pn_all_x2<true>(dx, dy, dz, make_float2(b.z, b.w), make_float2(e.x, e.y), make_float2(e.z, e.w),
+                                   make_float2(d.z, d.w), s.F[q], vix, viy, viz, vi4x, vi4y, vi4z, nvi2, vi2, mi5G,
+                                   Gmi, e2, G4, G2, nk, k.f, ax, ay, az, px, py, pz, q2x, q2y, q2z);
         }
-        ax.x = sx; ay.x = sy; az.x = sz;
-        px.x = rx; py.x = ry; pz.x = rz;
+        const float mc2 = -k.c2, mc4 = -k.c4;  // P and Q as newton_pn_all_x2 defines them
+        px = __fmul2_rn(px, make_float2(mc2, mc2));
+        py = __fmul2_rn(py, make_float2(mc2, mc2));
+        pz = __fmul2_rn(pz, make_float2(mc2, mc2));
+        qx = mc4 * (q2x.x + q2x.y);
+        qy = mc4 * (q2y.x + q2y.y);
+        qz = mc4 * (q2z.x + q2z.y);
     }
     aN = make_float3(ax.x + ax.y, ay.x + ay.y, az.x + az.y);
     a1 = make_float3(px.x + px.y, py.x + py.y, pz.x + pz.y);

@@ -807,33 +807,9 @@ __device__ __forceinline__ void interact_f64(const double4 e, const double4 b, d
     az = fma(dz, s, az);
 }
 
-// One entry with a post-Newtonian force law: the Newtonian term into (ax, ay,
-// az) as interact2_f32/interact_f64 form it, the 1PN terms into p and the 2PN
-// and 2.5PN terms into q (pn.cuh), all divided by G. Entry e (position, mass,
-// velocity ev) acts on the body at b with velocity vi and mass mi.
-template <int PNL, bool GUARD>
-__device__ __forceinline__ void interact_pn_f32(float ex, float ey, float ez, float em, const float4 ev,
-                                                const float3 b, const float4 vi, float mi, float eps2, float G,
-                                                const PnK<float>& k, float& ax, float& ay, float& az, float3& p,
-                                                float3& q) {
-    const float dx = ex - b.x, dy = ey - b.y, dz = ez - b.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-    float inv = rsqrt_approx(r2);
-    if (GUARD) inv = r2 > 0.f ? inv : 0.f;
-    const float inv2 = inv * inv;
-    const float sN = em * inv * inv2;
-    ax = fmaf(dx, sN, ax); ay = fmaf(dy, sN, ay); az = fmaf(dz, sN, az);
-    PnPair<float> w;
-    w.nx = -dx * inv; w.ny = -dy * inv; w.nz = -dz * inv;
-    w.dvx = vi.x - ev.x; w.dvy = vi.y - ev.y; w.dvz = vi.z - ev.z;
-    w.inv = inv; w.inv2 = inv2; w.mi = mi; w.mj = em; w.vi2 = vi.w; w.vj2 = ev.w;
-    w.v12 = vi.x * ev.x + vi.y * ev.y + vi.z * ev.z;
-    w.nv1 = w.nx * vi.x + w.ny * vi.y + w.nz * vi.z;
-    w.nv2 = w.nx * ev.x + w.ny * ev.y + w.nz * ev.z;
-    w.G = G;
-    pn_terms<PNL>(k, w, p.x, p.y, p.z, q.x, q.y, q.z);
-}
-
+// One entry with a post-Newtonian force law, FP64: the Newtonian term as
+// interact_f64 forms it plus the terms pk selects (pn.cuh), all divided by G.
+// Entry e (position, mass; velocity ev) acts on the body b (velocity vi).
 template <int PNL, bool GUARD>
 __device__ __forceinline__ void interact_pn_f64(const double4 e, const double4 ev, const double4 b, const double4 vi,
                                                 double eps2, double G, const PnK<double>& k, double& ax, double& ay,
@@ -1072,31 +1048,46 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
                     };
                     body(nb0x, nb0y, nb0z, vf0, h0.w, 0, 1, sx0, sy0, sz0, p0);
                     if (two) body(nb1x, nb1y, nb1z, vf1, h1.w, sub, lps, sx1, sy1, sz1, p1);
-                } else if (MIXED) {  // one entry at a time, scalar
-                    const float* A = reinterpret_cast<const float*>(&sm.lpa[warp][0]);
-                    const float* B = reinterpret_cast<const float*>(&sm.lpb[warp][0]);
-                    const float* VA = reinterpret_cast<const float*>(&sm.lva[warp][0]);
-                    const float* VB = reinterpret_cast<const float*>(&sm.lvb[warp][0]);
-                    const float Gf = (float)G, e2 = (float)eps2;
-                    const PnK<float> pkf = pn_float(pk);
-                    float ax = 0.f, ay = 0.f, az = 0.f;
-                    for (int e = 0; e < cnt; ++e) {
-                        const int o = ((e >> 1) << 2) | (e & 1);
-                        interact_pn_f32<PNL, GUARD>(A[o], A[o + 2], B[o], B[o + 2],
-                                                    make_float4(VA[o], VA[o + 2], VB[o], VB[o + 2]), b0, vf0, h0.w,
-                                                    e2, Gf, pkf, ax, ay, az, p0, q0);
-                    }
-                    sx0.add(ax); sy0.add(ay); sz0.add(az);
-                    if (two) {
-                        float bx = 0.f, by = 0.f, bz = 0.f;
-                        for (int e = sub; e < cnt; e += lps) {
-                            const int o = ((e >> 1) << 2) | (e & 1);
-                            interact_pn_f32<PNL, GUARD>(A[o], A[o + 2], B[o], B[o + 2],
-                                                        make_float4(VA[o], VA[o + 2], VB[o], VB[o + 2]), b1, vf1,
-                                                        h1.w, e2, Gf, pkf, bx, by, bz, p1, q1);
+                } else if (MIXED) {  // any of the PN terms by flags: two entries per paired instruction as well
+                    const int np = (cnt + 1) >> 1;  // an odd cnt: last slot half zero-padded by the caller
+                    const float Gf = (float)G, mc2 = -(float)pk.c2, mc4 = -(float)pk.c4;
+                    const float2 G4 = make_float2(4.f * Gf, 4.f * Gf), G2 = make_float2(Gf, Gf);
+                    const float nkf = -0.8f * (float)pk.ic;
+                    const float2 nk = make_float2(nkf, nkf);
+                    auto body = [&](const float2 nbx, const float2 nby, const float2 nbz, const float4 vf, float mi,
+                                    int q0i, int step, CompSum& sx, CompSum& sy, CompSum& sz, float3& p, float3& qq) {
+                        const float2 vix = make_float2(vf.x, vf.x), viy = make_float2(vf.y, vf.y),
+                                     viz = make_float2(vf.z, vf.z), nvi2 = make_float2(-vf.w, -vf.w),
+                                     vi2 = make_float2(vf.w, vf.w),
+                                     vi4x = make_float2(4.f * vf.x, 4.f * vf.x),
+                                     vi4y = make_float2(4.f * vf.y, 4.f * vf.y),
+                                     vi4z = make_float2(4.f * vf.z, 4.f * vf.z),
+                                     mi5G = make_float2(5.f * Gf * mi, 5.f * Gf * mi),
+                                     Gmi = make_float2(Gf * mi, Gf * mi);
+                        float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax, px = ax, py = ax, pz = ax, qx = ax,
+                               qy = ax, qz = ax;
+                        for (int q = q0i; q < np; q += step) {
+                            const float4 A = sm.lpa[warp][q], B = sm.lpb[warp][q], VA = sm.lva[warp][q],
+                                         VB = sm.lvb[warp][q];
+                            const float2 dx = __fadd2_rn(make_float2(A.x, A.y), nbx);  // entry - body
+                            const float2 dy = __fadd2_rn(make_float2(A.z, A.w), nby);
+                            const float2 dz = __fadd2_rn(make_float2(B.x, B.y), nbz);
+                            newton_pn_all_x2<GUARD>(dx, dy, dz, make_float2(B.z, B.w), make_float2(VA.x, VA.y),
+                                                    make_float2(VA.z, VA.w), make_float2(VB.x, VB.y),
+                                                    make_float2(VB.z, VB.w), vix, viy, viz, vi4x, vi4y, vi4z, nvi2,
+                                                    vi2, mi5G, Gmi, eps2f2, G4, G2, nk, pk.f, ax, ay, az, px, py, pz,
+                                                    qx, qy, qz);
                         }
-                        sx1.add(bx); sy1.add(by); sz1.add(bz);
-                    }
+                        sx.add(ax.x + ax.y); sy.add(ay.x + ay.y); sz.add(az.x + az.y);
+                        p.x = fmaf(mc2, px.x + px.y, p.x);
+                        p.y = fmaf(mc2, py.x + py.y, p.y);
+                        p.z = fmaf(mc2, pz.x + pz.y, p.z);
+                        qq.x = fmaf(mc4, qx.x + qx.y, qq.x);
+                        qq.y = fmaf(mc4, qy.x + qy.y, qq.y);
+                        qq.z = fmaf(mc4, qz.x + qz.y, qq.z);
+                    };
+                    body(nb0x, nb0y, nb0z, vf0, h0.w, 0, 1, sx0, sy0, sz0, p0, q0);
+                    if (two) body(nb1x, nb1y, nb1z, vf1, h1.w, sub, lps, sx1, sy1, sz1, p1, q1);
                 } else {
                     for (int e = 0; e < cnt; ++e)
                         interact_pn_f64<PNL, GUARD>(sm.lcm[warp][e], sm.lvd[warp][e], c0, vd0, eps2, G, pk, dx0, dy0,

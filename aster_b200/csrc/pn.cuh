@@ -121,6 +121,123 @@ __device__ __forceinline__ void newton_pn1_x2(const float2 dx, const float2 dy, 
     pz = __ffma2_rn(dz, sA, __ffma2_rn(dvz, sB, pz));
 }
 
+// Newton and every post-Newtonian term the flags select (bit 0 1PN, bit 1 2PN,
+// bit 2 2.5PN), two sources per paired FP32 instruction: the algebra of
+// PnPair::pn1/pn2/pn25 with the sums gathered under the Newtonian factor
+// m_j / r^3 and the c^-2, c^-4 factors applied once per target, as in
+// newton_pn1_x2. Inputs as newton_pn1_x2's, plus vi2 = |v_i|^2 and
+// Gmi = G m_i per target and nk = -0.8 c^-1. Adds m_j d / r^3 to a, to p the
+// 1PN sum P of newton_pn1_x2 (the 1PN term is -c^-2 P) and to q the sum Q whose
+// -c^-4 multiple is the 2PN + 2.5PN term (all divided by G). With
+// n = -d s, nv1 = n.v_i = -s d.v_i, nv2 = -s d.v_j, p1 = G m_i s, p2 = G m_j s:
+//   2PN:   c^-4 m_j s^2 [n (Sn + Sm) + dv Sv] = -c^-4 [m_j s^3 (Sn + Sm) d - m_j s^2 Sv dv],
+//   2.5PN: 0.8 c^-5 p1 m_j s^2 [dv I1 + n I2] = -c^-4 (-0.8 c^-1) p1 m_j s^2 [dv I1 - s I2 d].
+template <bool GUARD>
+__device__ __forceinline__ void newton_pn_all_x2(const float2 dx, const float2 dy, const float2 dz, const float2 mj,
+                                                 const float2 vjx, const float2 vjy, const float2 vjz,
+                                                 const float2 vj2, const float2 vix, const float2 viy,
+                                                 const float2 viz, const float2 vi4x, const float2 vi4y,
+                                                 const float2 vi4z, const float2 nvi2, const float2 vi2,
+                                                 const float2 mi5G, const float2 Gmi, const float2 eps2,
+                                                 const float2 G4, const float2 G2, const float2 nk, int f,
+                                                 float2& ax, float2& ay, float2& az, float2& px, float2& py,
+                                                 float2& pz, float2& qx, float2& qy, float2& qz) {
+    auto k2 = [](float v) { return make_float2(v, v); };
+    float2 r2 = __ffma2_rn(dz, dz, eps2);
+    r2 = __ffma2_rn(dy, dy, r2);
+    r2 = __ffma2_rn(dx, dx, r2);
+    float2 s = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    if (GUARD) {
+        s.x = r2.x > 0.f ? s.x : 0.f;
+        s.y = r2.y > 0.f ? s.y : 0.f;
+    }
+    const float2 ms = __fmul2_rn(mj, s);
+    const float2 mss = __fmul2_rn(ms, s);   // m_j / r^2
+    const float2 sN = __fmul2_rn(mss, s);   // m_j / r^3
+    ax = __ffma2_rn(dx, sN, ax);
+    ay = __ffma2_rn(dy, sN, ay);
+    az = __ffma2_rn(dz, sN, az);
+    if (!(f & 7)) return;
+    const float2 m1 = k2(-1.f);
+    const float2 w = __ffma2_rn(dx, vjx, __ffma2_rn(dy, vjy, __fmul2_rn(dz, vjz)));     // d.v_j
+    const float2 u4 = __ffma2_rn(dx, vi4x, __ffma2_rn(dy, vi4y, __fmul2_rn(dz, vi4z)));  // 4 d.v_i
+    const float2 dvx = __ffma2_rn(vjx, m1, vix), dvy = __ffma2_rn(vjy, m1, viy), dvz = __ffma2_rn(vjz, m1, viz);
+    if (f & 1) {  // 1PN: newton_pn1_x2's sum
+        const float2 Bp = __ffma2_rn(w, k2(-3.f), u4);
+        const float2 ws = __fmul2_rn(w, s);
+        float2 A = __ffma2_rn(vj2, k2(-2.f), nvi2);
+        A = __ffma2_rn(vi4x, vjx, A);
+        A = __ffma2_rn(vi4y, vjy, A);
+        A = __ffma2_rn(vi4z, vjz, A);
+        A = __ffma2_rn(__fmul2_rn(ws, ws), k2(1.5f), A);
+        A = __ffma2_rn(ms, G4, A);
+        A = __ffma2_rn(s, mi5G, A);
+        const float2 sA = __fmul2_rn(sN, A), sB = __fmul2_rn(sN, Bp);
+        px = __ffma2_rn(dx, sA, __ffma2_rn(dvx, sB, px));
+        py = __ffma2_rn(dy, sA, __ffma2_rn(dvy, sB, py));
+        pz = __ffma2_rn(dz, sA, __ffma2_rn(dvz, sB, pz));
+    }
+    if (!(f & 6)) return;
+    const float2 nv1 = __fmul2_rn(u4, __fmul2_rn(s, k2(-0.25f)));  // n.v_i
+    const float2 nv2 = __fmul2_rn(__fmul2_rn(w, s), m1);           // n.v_j
+    const float2 v12 = __ffma2_rn(vix, vjx, __ffma2_rn(viy, vjy, __fmul2_rn(viz, vjz)));
+    const float2 p1 = __fmul2_rn(Gmi, s), p2 = __fmul2_rn(G2, ms);  // G m_i / r, G m_j / r
+    if (f & 2) {  // 2PN (PnPair::pn2)
+        const float2 nv22 = __fmul2_rn(nv2, nv2), nv12 = __fmul2_rn(nv1, nv1), n12 = __fmul2_rn(nv1, nv2);
+        // -2 vj2^2 + 4 vj2 v12 - 2 v12^2 = -2 (vj2 - v12)^2
+        const float2 t = __ffma2_rn(v12, m1, vj2);
+        float2 Sn = __fmul2_rn(__fmul2_rn(t, t), k2(-2.f));
+        // + nv22 (1.5 vi2 + 4.5 vj2 - 6 v12) - 1.875 nv22^2
+        const float2 c1 = __ffma2_rn(v12, k2(-6.f), __ffma2_rn(vj2, k2(4.5f), __fmul2_rn(vi2, k2(1.5f))));
+        Sn = __ffma2_rn(nv22, c1, Sn);
+        Sn = __ffma2_rn(__fmul2_rn(nv22, nv22), k2(-1.875f), Sn);
+        // + p1 (-3.75 vi2 + 1.25 vj2 - 2.5 v12 + 19.5 nv12 - 39 nv1 nv2 + 8.5 nv22)
+        float2 e1 = __ffma2_rn(vj2, k2(1.25f), __fmul2_rn(vi2, k2(-3.75f)));
+        e1 = __ffma2_rn(v12, k2(-2.5f), e1);
+        e1 = __ffma2_rn(nv12, k2(19.5f), e1);
+        e1 = __ffma2_rn(n12, k2(-39.f), e1);
+        e1 = __ffma2_rn(nv22, k2(8.5f), e1);
+        Sn = __ffma2_rn(p1, e1, Sn);
+        // + p2 (4 vj2 - 8 v12 + 2 nv12 - 4 nv1 nv2 - 6 nv22)
+        float2 e2 = __ffma2_rn(v12, k2(-8.f), __fmul2_rn(vj2, k2(4.f)));
+        e2 = __ffma2_rn(nv12, k2(2.f), e2);
+        e2 = __ffma2_rn(n12, k2(-4.f), e2);
+        e2 = __ffma2_rn(nv22, k2(-6.f), e2);
+        Sn = __ffma2_rn(p2, e2, Sn);
+        // Sv = nv1 (4 vj2 - 4 v12 - 6 nv22 - 15.75 p1 - 2 p2) + nv2 (vi2 - 5 vj2 + 4 v12 + 4.5 nv22 + 13.75 p1 - 2 p2)
+        float2 A1 = __ffma2_rn(v12, k2(-4.f), __fmul2_rn(vj2, k2(4.f)));
+        A1 = __ffma2_rn(nv22, k2(-6.f), A1);
+        A1 = __ffma2_rn(p1, k2(-15.75f), A1);
+        A1 = __ffma2_rn(p2, k2(-2.f), A1);
+        float2 A2 = __ffma2_rn(vj2, k2(-5.f), vi2);
+        A2 = __ffma2_rn(v12, k2(4.f), A2);
+        A2 = __ffma2_rn(nv22, k2(4.5f), A2);
+        A2 = __ffma2_rn(p1, k2(13.75f), A2);
+        A2 = __ffma2_rn(p2, k2(-2.f), A2);
+        const float2 Sv = __ffma2_rn(nv1, A1, __fmul2_rn(nv2, A2));
+        // Sm = -14.25 p1^2 - 9 p2^2 - 34.5 p1 p2
+        const float2 Sm = __ffma2_rn(p1, __ffma2_rn(p1, k2(-14.25f), __fmul2_rn(p2, k2(-34.5f))),
+                                     __fmul2_rn(__fmul2_rn(p2, p2), k2(-9.f)));
+        // Q += m_j s^3 (Sn + Sm) d - m_j s^2 Sv dv
+        const float2 a1 = __fmul2_rn(sN, __fadd2_rn(Sn, Sm)), a2 = __fmul2_rn(__fmul2_rn(mss, Sv), m1);
+        qx = __ffma2_rn(dx, a1, __ffma2_rn(dvx, a2, qx));
+        qy = __ffma2_rn(dy, a1, __ffma2_rn(dvy, a2, qy));
+        qz = __ffma2_rn(dz, a1, __ffma2_rn(dvz, a2, qz));
+    }
+    if (f & 4) {  // 2.5PN (PnPair::pn25)
+        const float2 sq = __ffma2_rn(dvx, dvx, __ffma2_rn(dvy, dvy, __fmul2_rn(dvz, dvz)));
+        const float2 I1 = __ffma2_rn(p2, k2(-8.f), __ffma2_rn(p1, k2(2.f), __fmul2_rn(sq, m1)));
+        const float2 I2 = __fmul2_rn(__fadd2_rn(nv1, __fmul2_rn(nv2, m1)),
+                                     __ffma2_rn(p2, k2(52.f / 3.f), __ffma2_rn(sq, k2(3.f), __fmul2_rn(p1, k2(-6.f)))));
+        // Q += (-0.8 c^-1) p1 m_j s^2 (dv I1 - s I2 d)
+        const float2 g = __fmul2_rn(__fmul2_rn(p1, mss), nk);
+        const float2 gI1 = __fmul2_rn(g, I1), gsI2 = __fmul2_rn(__fmul2_rn(g, s), __fmul2_rn(I2, m1));
+        qx = __ffma2_rn(dvx, gI1, __ffma2_rn(dx, gsI2, qx));
+        qy = __ffma2_rn(dvy, gI1, __ffma2_rn(dy, gsI2, qy));
+        qz = __ffma2_rn(dvz, gI1, __ffma2_rn(dz, gsI2, qz));
+    }
+}
+
 // The terms of level PNL: 1PN into p, 2PN and 2.5PN into q (kept apart in
 // FP32 so that the smaller corrections are not lost against the larger sums).
 template <int PNL, class T>
