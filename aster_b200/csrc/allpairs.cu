@@ -135,99 +135,93 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
 }
 
 // --------------------------------------------------------------- mixed path
-// With post-Newtonian terms (PNL 1 or 2): the Newtonian part as below, the
-// 1PN terms and the 2PN/2.5PN terms in two further FP32 sums per target.
+// With post-Newtonian terms (PNL 1: Newton + 1PN; 2: the terms the force-law
+// bits select), two sources per paired FP32 instruction as in the Newtonian
+// kernel below, one target per thread: the j-tile staged pair-interleaved
+// (double-single positions, masses, velocities and |v|^2, as the batched
+// ensemble's slab), the pair terms of pn.cuh (newton_pn1_x2,
+// newton_pn_all_x2); the Newtonian sum folded into compensated sums every
+// FOLD sources, the 1PN and 2PN + 2.5PN sums kept apart in FP32.
+constexpr int IPT_PN = 1;
+
 template <int PNL, bool GUARD>
-__global__ void __launch_bounds__(BLOCK) k_allpairs_mixed(
+__global__ void __launch_bounds__(BLOCK) k_allpairs_mixed_pn(
     int64_t j_lo, int64_t n, int64_t nt, const int32_t* __restrict__ targets, const float4* __restrict__ phi,
     const float4* __restrict__ plo, const float4* __restrict__ vf, float G, float eps2, PnK<float> pk,
     double Gd, int64_t slice_len, int nslices, double4* __restrict__ partial, double4* __restrict__ acc,
     double* __restrict__ out3, KickArgs kick) {
-    __shared__ float4 sh[BLOCK];
-    __shared__ float4 sl[BLOCK];
-    __shared__ float4 sv[BLOCK];  // (vx, vy, vz, |v|^2)
+    // (hx hx' hy hy') (hz hz' m m') (lx lx' ly ly') (lz lz' vz vz') (vx vx' vy vy') (|v|^2 |v'|^2)
+    __shared__ float4 pa[BLOCK / 2], pb[BLOCK / 2], pc[BLOCK / 2], pd[BLOCK / 2], pe[BLOCK / 2];
+    __shared__ float2 pf[BLOCK / 2];
     const int slice = blockIdx.y;
     const int64_t j0 = j_lo + (int64_t)slice * slice_len;  // sources [j_lo, n), sliced
     const int64_t j1 = min(n, j0 + slice_len);
-    int64_t tt[IPT], bi[IPT];
-    float xh[IPT], yh[IPT], zh[IPT], xl[IPT], yl[IPT], zl[IPT], mi[IPT];
-    float vxi[IPT], vyi[IPT], vzi[IPT], v1sq[IPT];
-    float ax[IPT], ay[IPT], az[IPT];
-    float px[IPT], py[IPT], pz[IPT], qx[IPT], qy[IPT], qz[IPT];
-    CompSum cx[IPT], cy[IPT], cz[IPT];
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-        tt[k] = (int64_t)blockIdx.x * BLOCK * IPT + k * BLOCK + threadIdx.x;
-        bi[k] = tt[k] < nt ? (targets ? (int64_t)targets[tt[k]] : tt[k]) : 0;
-        float4 h = phi[bi[k]], l = plo[bi[k]];
-        xh[k] = h.x; yh[k] = h.y; zh[k] = h.z; mi[k] = h.w;
-        xl[k] = l.x; yl[k] = l.y; zl[k] = l.z;
-        float4 v = vf[bi[k]];
-        vxi[k] = v.x; vyi[k] = v.y; vzi[k] = v.z;
-        v1sq[k] = v.x * v.x + v.y * v.y + v.z * v.z;
-        ax[k] = ay[k] = az[k] = 0.f;
-        px[k] = py[k] = pz[k] = 0.f;
-        qx[k] = qy[k] = qz[k] = 0.f;
-    }
+    const int64_t tt = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+    const int64_t bi = tt < nt ? (targets ? (int64_t)targets[tt] : tt) : 0;
+    const float4 h = phi[bi], l = plo[bi], v = vf[bi];
+    const float2 nhx = make_float2(-h.x, -h.x), nhy = make_float2(-h.y, -h.y), nhz = make_float2(-h.z, -h.z);
+    const float2 nlx = make_float2(-l.x, -l.x), nly = make_float2(-l.y, -l.y), nlz = make_float2(-l.z, -l.z);
+    const float w2 = v.x * v.x + v.y * v.y + v.z * v.z;
+    const float2 vix = make_float2(v.x, v.x), viy = make_float2(v.y, v.y), viz = make_float2(v.z, v.z);
+    const float2 vi4x = make_float2(4.f * v.x, 4.f * v.x), vi4y = make_float2(4.f * v.y, 4.f * v.y),
+                 vi4z = make_float2(4.f * v.z, 4.f * v.z);
+    const float2 nvi2 = make_float2(-w2, -w2), vi2 = make_float2(w2, w2);
+    const float2 mi5G = make_float2(5.f * G * h.w, 5.f * G * h.w), Gmi = make_float2(G * h.w, G * h.w);
+    const float2 G4 = make_float2(4.f * G, 4.f * G), G2 = make_float2(G, G), e2 = make_float2(eps2, eps2);
+    const float2 nk = make_float2(-0.8f * pk.ic, -0.8f * pk.ic);
+    float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax, px = ax, py = ax, pz = ax, qx = ax, qy = ax, qz = ax;
+    CompSum cx, cy, cz;
+    float* fa = reinterpret_cast<float*>(pa);
+    float* fb = reinterpret_cast<float*>(pb);
+    float* fc = reinterpret_cast<float*>(pc);
+    float* fd = reinterpret_cast<float*>(pd);
+    float* fe = reinterpret_cast<float*>(pe);
+    float* ff = reinterpret_cast<float*>(pf);
+    const int o = ((threadIdx.x >> 1) << 2) | (threadIdx.x & 1);
     for (int64_t base = j0; base < j1; base += BLOCK) {
         const int64_t j = base + threadIdx.x;
         __syncthreads();
-        if (j < j1) {
-            sh[threadIdx.x] = phi[j];
-            sl[threadIdx.x] = plo[j];
-            float4 v = vf[j];
-            v.w = v.x * v.x + v.y * v.y + v.z * v.z;
-            sv[threadIdx.x] = v;
-        } else {
-            sh[threadIdx.x] = make_float4(PAD_POS, PAD_POS, PAD_POS, 0.f);
-            sl[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-            sv[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+        float4 sh = make_float4(PAD_POS, PAD_POS, PAD_POS, 0.f), sl = make_float4(0.f, 0.f, 0.f, 0.f), sv = sl;
+        if (j < j1) { sh = phi[j]; sl = plo[j]; sv = vf[j]; }
+        fa[o] = sh.x; fa[o + 2] = sh.y;
+        fb[o] = sh.z; fb[o + 2] = sh.w;
+        fc[o] = sl.x; fc[o + 2] = sl.y;
+        fd[o] = sl.z; fd[o + 2] = sv.z;
+        fe[o] = sv.x; fe[o + 2] = sv.y;
+        ff[threadIdx.x] = sv.x * sv.x + sv.y * sv.y + sv.z * sv.z;
         __syncthreads();
-        const int cnt = (int)min((int64_t)BLOCK, j1 - base);  // a partial last tile stops at its last source
+        // a partial last tile stops at its last source pair (padding: no mass)
+        const int npair = (int)((min((int64_t)BLOCK, j1 - base) + 1) / 2);
 #pragma unroll 1
-        for (int c0 = 0; c0 < cnt; c0 += FOLD) {
-#pragma unroll 8
-            for (int q = c0; q < min(c0 + FOLD, cnt); ++q) {
-                const float4 h = sh[q];
-                const float4 l = sl[q];
-                const float4 vj = sv[q];
-#pragma unroll
-                for (int k = 0; k < IPT; ++k) {
-                    float dx = (h.x - xh[k]) + (l.x - xl[k]);
-                    float dy = (h.y - yh[k]) + (l.y - yl[k]);
-                    float dz = (h.z - zh[k]) + (l.z - zl[k]);
-                    float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-                    float inv = rsqrt_approx(r2);
-                    if (GUARD) inv = r2 > 0.f ? inv : 0.f;
-                    float inv2 = inv * inv;
-                    float s = h.w * inv * inv2;
-                    ax[k] = fmaf(dx, s, ax[k]); ay[k] = fmaf(dy, s, ay[k]); az[k] = fmaf(dz, s, az[k]);
-                    PnPair<float> w;
-                    w.nx = -dx * inv; w.ny = -dy * inv; w.nz = -dz * inv;
-                    w.dvx = vxi[k] - vj.x; w.dvy = vyi[k] - vj.y; w.dvz = vzi[k] - vj.z;
-                    w.inv = inv; w.inv2 = inv2; w.mi = mi[k]; w.mj = h.w; w.vi2 = v1sq[k]; w.vj2 = vj.w;
-                    w.v12 = vxi[k] * vj.x + vyi[k] * vj.y + vzi[k] * vj.z;
-                    w.nv1 = w.nx * vxi[k] + w.ny * vyi[k] + w.nz * vzi[k];
-                    w.nv2 = w.nx * vj.x + w.ny * vj.y + w.nz * vj.z;
-                    w.G = G;
-                    pn_terms<PNL>(pk, w, px[k], py[k], pz[k], qx[k], qy[k], qz[k]);
-                }
+        for (int c0 = 0; c0 < npair; c0 += FOLD / 2) {
+#pragma unroll 2
+            for (int q = c0; q < min(c0 + FOLD / 2, npair); ++q) {
+                const float4 A = pa[q], B = pb[q], C = pc[q], D = pd[q], E = pe[q];
+                const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(A.x, A.y), nhx), __fadd2_rn(make_float2(C.x, C.y), nlx));
+                const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(A.z, A.w), nhy), __fadd2_rn(make_float2(C.z, C.w), nly));
+                const float2 dz = __fadd2_rn(__fadd2_rn(make_float2(B.x, B.y), nhz), __fadd2_rn(make_float2(D.x, D.y), nlz));
+                if constexpr (PNL == 1)
+                    newton_pn1_x2<GUARD>(dx, dy, dz, make_float2(B.z, B.w), make_float2(E.x, E.y),
+                                         make_float2(E.z, E.w), make_float2(D.z, D.w), pf[q], vix, viy, viz, vi4x,
+                                         vi4y, vi4z, nvi2, mi5G, e2, G4, ax, ay, az, px, py, pz);
+                else
+                    newton_pn_all_x2<GUARD>(dx, dy, dz, make_float2(B.z, B.w), make_float2(E.x, E.y),
+                                            make_float2(E.z, E.w), make_float2(D.z, D.w), pf[q], vix, viy, viz,
+                                            vi4x, vi4y, vi4z, nvi2, vi2, mi5G, Gmi, e2, G4, G2, nk, pk.f, ax, ay, az,
+                                            px, py, pz, qx, qy, qz);
             }
-#pragma unroll
-            for (int k = 0; k < IPT; ++k) {
-                cx[k].add(ax[k]); cy[k].add(ay[k]); cz[k].add(az[k]);
-                ax[k] = ay[k] = az[k] = 0.f;
-            }
+            cx.add(ax.x + ax.y); cy.add(ay.x + ay.y); cz.add(az.x + az.y);
+            ax = ay = az = make_float2(0.f, 0.f);
         }
     }
-#pragma unroll
-    for (int k = 0; k < IPT; ++k)
-        if (tt[k] < nt)
-            store_result(tt[k], bi[k], cx[k].value() + ((double)px[k] + (double)qx[k]),
-                         cy[k].value() + ((double)py[k] + (double)qy[k]),
-                         cz[k].value() + ((double)pz[k] + (double)qz[k]), Gd, nslices, slice, nt, partial, acc, out3,
-                         kick);
+    if (tt < nt) {
+        // the 1PN term is -c^-2 P, the 2PN + 2.5PN term -c^-4 Q (pn.cuh)
+        const double c2 = -(double)pk.c2, c4 = -(double)pk.c4;
+        store_result(tt, bi, cx.value() + (c2 * (double)(px.x + px.y) + c4 * (double)(qx.x + qx.y)),
+                     cy.value() + (c2 * (double)(py.x + py.y) + c4 * (double)(qy.x + qy.y)),
+                     cz.value() + (c2 * (double)(pz.x + pz.y) + c4 * (double)(qz.x + qz.y)), Gd, nslices, slice, nt,
+                     partial, acc, out3, kick);
+    }
 }
 
 // Newtonian mixed path with the paired FP32 instructions of sm_100
@@ -353,7 +347,7 @@ void launch_mixed(dim3 grid, cudaStream_t st, int64_t j_lo, int64_t n, int64_t n
                                                           (float)p->eps2, p->G, slice_len, ns, partial,
                                                           c->acc.as<double4>(), out3, kick);
     } else {
-        k_allpairs_mixed<PNL, GUARD><<<grid, BLOCK, 0, st>>>(
+        k_allpairs_mixed_pn<PNL, GUARD><<<grid, BLOCK, 0, st>>>(
             j_lo, n, nt, tg, c->phi.as<float4>(), c->plo.as<float4>(), c->vf.as<float4>(), (float)p->G, (float)p->eps2,
             pn_float(make_pn(p)), p->G, slice_len, ns, partial, c->acc.as<double4>(), out3, kick);
     }
@@ -390,7 +384,8 @@ int aster_allpairs_launch_range(aster_ctx* c, const aster_params* p, int precisi
     const int64_t n_src = c->n_src > 0 ? c->n_src : c->n;
     const int64_t lo = src_lo, hi = src_hi < n_src ? src_hi : n_src;
     const int64_t len = hi > lo ? hi - lo : 0;
-    const int64_t per_block = (int64_t)BLOCK * IPT;
+    // one target per thread in the mixed post-Newtonian kernel, two elsewhere
+    const int64_t per_block = (int64_t)BLOCK * (precision == ASTER_MIXED && pn_level(p) > 0 ? IPT_PN : IPT);
     const int64_t iblocks = (nt + per_block - 1) / per_block;
     // j-slices so that small n still fill the GPU (>= ASTER_SLICE_BLOCKS_PER_SM blocks per SM).
     int64_t want = ASTER_SLICE_BLOCKS_PER_SM * (int64_t)c->sm_count;
