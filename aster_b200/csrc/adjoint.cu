@@ -180,16 +180,17 @@ __global__ void __launch_bounds__(BLOCK) k_adj_pair_mixed(int64_t n, const doubl
                         sv.x = r2.x > 0.f ? sv.x : 0.f;
                         sv.y = r2.y > 0.f ? sv.y : 0.f;
                     }
-                    const float2 s2 = __fmul2_rn(sv, sv), s3 = __fmul2_rn(s2, sv), s5 = __fmul2_rn(s3, s2);
+                    const float2 s2 = __fmul2_rn(sv, sv), s3 = __fmul2_rn(s2, sv);
                     // u = m_k w_j - m_j w_k
                     const float2 ux = __ffma2_rn(mk[q], wjx, __fmul2_rn(mj, nwx[q]));
                     const float2 uy = __ffma2_rn(mk[q], wjy, __fmul2_rn(mj, nwy[q]));
                     const float2 uz = __ffma2_rn(mk[q], wjz, __fmul2_rn(mj, nwz[q]));
                     const float2 du = __ffma2_rn(dx, ux, __ffma2_rn(dy, uy, __fmul2_rn(dz, uz)));
-                    const float2 nt = __fmul2_rn(__fmul2_rn(s5, make_float2(-3.f, -3.f)), du);  // -3 s^5 (d.u)
-                    ax[q] = __ffma2_rn(nt, dx, __ffma2_rn(s3, ux, ax[q]));
-                    ay[q] = __ffma2_rn(nt, dy, __ffma2_rn(s3, uy, ay[q]));
-                    az[q] = __ffma2_rn(nt, dz, __ffma2_rn(s3, uz, az[q]));
+                    // s^3 u - 3 s^5 (d.u) d = s^3 (u + k d), k = -3 s^2 (d.u)
+                    const float2 k = __fmul2_rn(__fmul2_rn(s2, du), make_float2(-3.f, -3.f));
+                    ax[q] = __ffma2_rn(s3, __ffma2_rn(k, dx, ux), ax[q]);
+                    ay[q] = __ffma2_rn(s3, __ffma2_rn(k, dy, uy), ay[q]);
+                    az[q] = __ffma2_rn(s3, __ffma2_rn(k, dz, uz), az[q]);
                     const float2 wd = __ffma2_rn(wjx, dx, __ffma2_rn(wjy, dy, __fmul2_rn(wjz, dz)));
                     ag[q] = __ffma2_rn(s3, wd, ag[q]);
                 }
