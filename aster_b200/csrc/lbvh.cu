@@ -43,6 +43,7 @@ constexpr int SORT_ITEMS = 8;
 constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // 2048 keys per block
 constexpr int SORT_WARPS = SORT_THREADS / 32;
 constexpr int RADIX = 256;
+static_assert(SORT_THREADS == RADIX, "the scan and scatter kernels give each thread one digit");
 constexpr int MAX_CLIMB = 160;     // bottom-up level cap (tree depth <= 97 for 63-bit codes)
 #ifndef ASTER_WALK_WARPS
 #define ASTER_WALK_WARPS 4
@@ -158,9 +159,16 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(int64_t n, const Key
     for (int d = threadIdx.x; d < SORT_WARPS * RADIX; d += SORT_THREADS) (&h[0][0])[d] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * SORT_TILE;
+    KeyT k[SORT_ITEMS];  // all loads in flight before the first count
+#pragma unroll
     for (int r = 0; r < SORT_ITEMS; ++r) {
-        int64_t i = base + (int64_t)r * SORT_THREADS + threadIdx.x;
-        if (i < n) atomicAdd(&h[warp][(uint32_t)(keys[i] >> shift) & (RADIX - 1)], 1u);
+        const int64_t i = base + (int64_t)r * SORT_THREADS + threadIdx.x;
+        k[r] = i < n ? keys[i] : (KeyT)0;
+    }
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        const int64_t i = base + (int64_t)r * SORT_THREADS + threadIdx.x;
+        if (i < n) atomicAdd(&h[warp][(uint32_t)(k[r] >> shift) & (RADIX - 1)], 1u);
     }
     __syncthreads();
     for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
@@ -220,34 +228,41 @@ __global__ void __launch_bounds__(1024) k_scan_digits(uint32_t* __restrict__ his
 // Global position = (keys of smaller digits) + (same digit in earlier tiles)
 // + (same digit earlier in this tile).
 template <class KeyT, bool IDENTITY_VALS>
-__global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(int64_t n, const KeyT* __restrict__ kin,
+__global__ void __launch_bounds__(SORT_THREADS, 4) k_sort_scatter(int64_t n, const KeyT* __restrict__ kin,
                                                                const int32_t* __restrict__ vin, KeyT* __restrict__ kout,
                                                                int32_t* __restrict__ vout, int shift, int nblocks,
                                                                const uint32_t* __restrict__ tile_off,
                                                                const uint32_t* __restrict__ digit_tot) {
     __shared__ uint32_t wh[SORT_WARPS][RADIX];
     __shared__ uint32_t dstart[RADIX];
-    __shared__ uint32_t gbase[RADIX];
+    __shared__ uint32_t gofs[RADIX];
     __shared__ uint32_t s32[32];
     __shared__ KeyT sk[SORT_TILE];
     __shared__ int32_t sv[SORT_TILE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int d = threadIdx.x; d < SORT_WARPS * RADIX; d += SORT_THREADS) (&wh[0][0])[d] = 0;
-    // global base of each digit: exclusive scan of the digit totals
-    gbase[threadIdx.x] = block_exclusive_scan(digit_tot[threadIdx.x], s32, nullptr);
-    __syncthreads();
     const int64_t tile0 = (int64_t)blockIdx.x * SORT_TILE;
-    const uint32_t lt = (1u << lane) - 1u;
     KeyT key[SORT_ITEMS];
     int32_t val[SORT_ITEMS];
-    uint32_t rank[SORT_ITEMS];
-    uint32_t dig[SORT_ITEMS];
+    // the tile's keys and values: all loads in flight before the ranking
 #pragma unroll
     for (int r = 0; r < SORT_ITEMS; ++r) {
         const int64_t i = tile0 + warp * (32 * SORT_ITEMS) + r * 32 + lane;
         const bool ok = i < n;
         key[r] = ok ? kin[i] : (KeyT)0;
         val[r] = ok ? (IDENTITY_VALS ? (int32_t)i : vin[i]) : 0;
+    }
+    const uint32_t toff = tile_off[(int64_t)threadIdx.x * nblocks + blockIdx.x];  // digit threadIdx.x
+    for (int d = threadIdx.x; d < SORT_WARPS * RADIX; d += SORT_THREADS) (&wh[0][0])[d] = 0;
+    // global base of each digit: exclusive scan of the digit totals
+    const uint32_t gb = block_exclusive_scan(digit_tot[threadIdx.x], s32, nullptr);
+    __syncthreads();
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t rank[SORT_ITEMS];
+    uint32_t dig[SORT_ITEMS];
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        const int64_t i = tile0 + warp * (32 * SORT_ITEMS) + r * 32 + lane;
+        const bool ok = i < n;
         const uint32_t d = ok ? ((uint32_t)(key[r] >> shift) & (RADIX - 1)) : 0xFFFFu;
         dig[r] = d;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
@@ -268,6 +283,8 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(int64_t n, const 
     }
     const uint32_t ds = block_exclusive_scan(tot, s32, nullptr);
     dstart[threadIdx.x] = ds;
+    // output position of the tile's p-th key (digit d) = gofs[d] + p
+    gofs[threadIdx.x] = gb + toff - ds;
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < SORT_ITEMS; ++r) {
@@ -282,7 +299,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(int64_t n, const 
     for (int p = threadIdx.x; p < valid; p += SORT_THREADS) {
         const KeyT k = sk[p];
         const uint32_t d = (uint32_t)(k >> shift) & (RADIX - 1);
-        const int64_t g = (int64_t)gbase[d] + tile_off[(int64_t)d * nblocks + blockIdx.x] + (p - dstart[d]);
+        const int64_t g = (int64_t)(uint32_t)(gofs[d] + (uint32_t)p);
         kout[g] = k;
         vout[g] = sv[p];
     }
