@@ -491,7 +491,7 @@ __device__ __forceinline__ float4 ld_cg(const float4* p) { return __ldcg(p); }
 // sib[v] names v's sibling and side (>= 0: v is a left child), so a climb
 // reads both children without loading child[parent] first.
 #ifndef ASTER_BU_LEAVES
-#define ASTER_BU_LEAVES 256
+#define ASTER_BU_LEAVES 64
 #endif
 constexpr int BU_LEAVES = ASTER_BU_LEAVES;
 
@@ -516,7 +516,7 @@ __device__ __forceinline__ void bu_merge(const double4 cl, const double4 cr, con
     hi = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
 }
 
-__global__ void __launch_bounds__(BU_LEAVES, 4) k_bottom_up_local(
+__global__ void __launch_bounds__(BU_LEAVES, 1024 / BU_LEAVES) k_bottom_up_local(
     int64_t n, const int32_t* __restrict__ parent, const int32_t* __restrict__ sib, const int32_t* __restrict__ rlo,
     const int32_t* __restrict__ rhi, double4* __restrict__ node_cm, float4* __restrict__ bmin,
     float4* __restrict__ bmax, int32_t* __restrict__ front, unsigned int* __restrict__ nfront, int* __restrict__ err,
@@ -738,7 +738,7 @@ __global__ void __launch_bounds__(256) k_node_vel(int64_t n, const int32_t* __re
 // Child records of the internal nodes completed by the global phase of the
 // bottom-up merge (their arrival counters read 2; the block-local phase writes
 // the records of the nodes it completes and leaves their counters at 0).
-// Those nodes are sparse (~3% of the internal nodes at N = 2^20), so each block
+// Those nodes are sparse (~10% of the internal nodes at N = 2^20), so each block
 // first compacts the ones in its span of REC_SPAN counters into shared memory
 // and then gives them to consecutive threads: the latency-bound loads of the
 // children's data run in full warps instead of one lane per warp.
