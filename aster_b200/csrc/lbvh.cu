@@ -52,7 +52,7 @@ constexpr int MAX_CLIMB = 160;     // bottom-up level cap (tree depth <= 97 for 
 #define ASTER_WALK_MINBLOCKS 5
 #endif
 #ifndef ASTER_WALK_UNROLL
-#define ASTER_WALK_UNROLL 4
+#define ASTER_WALK_UNROLL 8
 #endif
 constexpr int WALK_WARPS = ASTER_WALK_WARPS;  // warps (groups in flight) per block
 constexpr int WALK_UNROLL = ASTER_WALK_UNROLL;
@@ -1153,7 +1153,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
                 float2 ax0 = make_float2(0.f, 0.f), ay0 = ax0, az0 = ax0;
                 if (two && lps == 1) {  // 49..64 bodies: both bodies of a lane share each list load
                     float2 ax1 = make_float2(0.f, 0.f), ay1 = ax1, az1 = ax1;
-#pragma unroll 2
+#pragma unroll 4
                     for (int q = 0; q < np; ++q) {
                         const float4 A = sm.lpa[warp][q], B = sm.lpb[warp][q];
                         interact2_f32<GUARD>(A, B, nb0x, nb0y, nb0z, eps2f2, ax0, ay0, az0);
