@@ -1170,7 +1170,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
                 sx0.add(ax0.x + ax0.y); sy0.add(ay0.x + ay0.y); sz0.add(az0.x + az0.y);
                 if (two) {
                     float2 ax1 = make_float2(0.f, 0.f), ay1 = ax1, az1 = ax1;
-#pragma unroll 2
+#pragma unroll 4
                     for (int q = sub; q < np; q += lps)
                         interact2_f32<GUARD>(sm.lpa[warp][q], sm.lpb[warp][q], nb1x, nb1y, nb1z, eps2f2, ax1, ay1, az1);
                     sx1.add(ax1.x + ax1.y); sy1.add(ay1.x + ay1.y); sz1.add(az1.x + az1.y);
