@@ -1179,7 +1179,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, PNL ? 4 : (MIXED ? ASTER_WALK
 #pragma unroll 4
                 for (int e = 0; e < cnt; ++e) interact_f64<GUARD>(sm.lcm[warp][e], c0, eps2, dx0, dy0, dz0);
                 if (two) {
-#pragma unroll 2
+#pragma unroll 4
                     for (int e = sub; e < cnt; e += lps) interact_f64<GUARD>(sm.lcm[warp][e], c1, eps2, dx1, dy1, dz1);
                 }
             }
