@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(BLOCK) k_adj_pair_mixed(int64_t n, const doubl
         __syncthreads();
 #pragma unroll 1
         for (int c0 = 0; c0 < NP; c0 += FOLD / 2) {
-#pragma unroll 2
+#pragma unroll 4
             for (int pp = c0; pp < c0 + FOLD / 2; ++pp) {
                 const float4 a = PA[pp], b = PB[pp], c = PC[pp], d = PD[pp], e = PE[pp];
                 const float2 mj = make_float2(b.z, b.w);
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(BLOCK) k_adj_pair_fp64(int64_t n, const double
         sx[threadIdx.x] = j < j1 ? xs[j] : make_double4(1e300, 1e300, 1e300, 0.0);
         sw[threadIdx.x] = j < j1 ? w[j] : make_double4(0, 0, 0, 0);
         __syncthreads();
-#pragma unroll 2
+#pragma unroll 4
         for (int jj = 0; jj < BLOCK; ++jj) {
             const double4 xj = sx[jj], wj = sw[jj];
 #pragma unroll

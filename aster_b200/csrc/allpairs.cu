@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_fp64(
         }
         __syncthreads();
         const int cnt = (int)min((int64_t)BLOCK, j1 - base);  // a partial last tile stops at its last source
-#pragma unroll 4
+#pragma unroll 8
         for (int q = 0; q < cnt; ++q) {
             const double4 pj = sp[q];
 #pragma unroll
@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(BLOCK) k_allpairs_mixed2(
 #pragma unroll 1
         for (int c0 = 0; c0 < npair; c0 += FOLD / 2) {
             if (npair == BLOCK / 2) {
-#pragma unroll 4
+#pragma unroll 8
                 for (int pq = c0; pq < c0 + FOLD / 2; ++pq) pair2(pq);
             } else {
 #pragma unroll 1
