@@ -50,6 +50,11 @@
 
 int aster_cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 
+// Generation of the device buffers: changes whenever any DevBuf is allocated
+// or freed, so that a cached graph (which holds buffer addresses) is only
+// replayed while every buffer it names still lives where it was captured.
+unsigned long long aster_devbuf_epoch();
+
 // Grow-only device buffer.
 struct DevBuf {
     void* ptr = nullptr;
@@ -84,6 +89,21 @@ struct EnsBufs {
 // Adjoint (reverse-mode) buffers.
 struct AdjBufs {
     DevBuf ckpt, segx, lx, lv, lm, w, target, part;
+};
+
+// An executable graph of one repeated step, kept across calls: replayed by
+// a later call whose key (parameters, sizes, buffer generation, timing on or
+// off) is the same, so that call captures and instantiates nothing.
+struct StepGraph {
+    std::vector<unsigned char> key;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    cudaGraphNode_t evnode[3] = {nullptr, nullptr, nullptr};  // the step's timing marks (re-pointed per launch)
+    // between calls the marks point here (the events of a call's timing die
+    // with the call; an executable graph must not keep naming them)
+    cudaEvent_t park = nullptr;
+    double inter = 0.0;                                         // host-side counts of one step
+    int64_t kernels = 0;
 };
 
 struct aster_ctx {
@@ -130,6 +150,9 @@ struct aster_ctx {
     // executable graphs of the last call's repeated steps; destroyed by the
     // next call's aster_begin (its work has finished by then) or at destroy
     std::vector<std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
+    // the tree KDK's middle step (kick-fused build + walk), kept across calls;
+    // a replaced one moves to `graphs`
+    StepGraph kdk_graph;
 };
 
 // Layout of ctx->red (4 KB of small device scalars).

@@ -5,6 +5,7 @@
 // std::vector<vec3> (AoS FP64) into OpenCL buffers; here AoS FP64 host arrays
 // are packed into 32-byte double4 records (x, y, z, m) and (vx, vy, vz, 0) so
 // that every body is one aligned 32-byte load.
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -20,10 +21,14 @@ int aster_cuda_fail(cudaError_t e, const char* what, const char* file, int line)
     return e == cudaErrorMemoryAllocation ? ASTER_ERR_OOM : ASTER_ERR_CUDA;
 }
 
+static std::atomic<unsigned long long> g_devbuf_epoch{0};
+unsigned long long aster_devbuf_epoch() { return g_devbuf_epoch.load(); }
+
 int DevBuf::ensure(size_t want) {
     if (want <= bytes && ptr) return ASTER_OK;
     release();
     size_t b = want < 256 ? 256 : want;
+    ++g_devbuf_epoch;
     cudaError_t e = cudaMalloc(&ptr, b);
     if (e != cudaSuccess) {
         ptr = nullptr;
@@ -36,7 +41,10 @@ int DevBuf::ensure(size_t want) {
 }
 
 void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        ++g_devbuf_epoch;
+        cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
 }
@@ -115,6 +123,9 @@ extern "C" int aster_ctx_destroy(aster_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     release_graphs(c);
+    if (c->kdk_graph.ge) cudaGraphExecDestroy(c->kdk_graph.ge);
+    if (c->kdk_graph.g) cudaGraphDestroy(c->kdk_graph.g);
+    if (c->kdk_graph.park) cudaEventDestroy(c->kdk_graph.park);
     DevBuf* bufs[] = {&c->pm, &c->vel, &c->acc, &c->phi, &c->plo, &c->vf, &c->scratch, &c->targets,
                       &c->stage, &c->red, &c->wh, &c->rec,
                       &c->tree.codes, &c->tree.codes_alt, &c->tree.sorted_codes, &c->tree.perm,

@@ -17,6 +17,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -280,6 +281,114 @@ static int repeat_steps(aster_ctx* c, int n, bool graph, F step, D done, R repla
 static int no_op() { return ASTER_OK; }
 static int no_replay(cudaGraph_t, cudaGraphExec_t) { return ASTER_OK; }
 
+// The key of a cached step graph: everything the captured launches depend on
+// besides the data in device memory (parameters, solver, precision, body
+// count, the addresses of the context's buffers through their generation,
+// whether the step carries timing marks).
+static std::vector<unsigned char> step_key(const aster_ctx* c, const aster_params* p, int solver, int precision,
+                                           bool timed) {
+    std::vector<unsigned char> k(sizeof(aster_params));
+    std::memcpy(k.data(), p, sizeof(aster_params));
+    const int64_t w[] = {solver, precision, timed ? 1 : 0, c->n, c->device, c->walk_stack_limit,
+                         (int64_t)aster_devbuf_epoch()};
+    const unsigned char* wb = reinterpret_cast<const unsigned char*>(w);
+    k.insert(k.end(), wb, wb + sizeof(w));
+    return k;
+}
+
+// Launches `count` more of the tree KDK's middle step from the context's
+// cached graph, capturing it first (one step, `middle`) when the cached one
+// does not match this call. The cached graph survives the call, so a later
+// call with the same key captures and instantiates nothing: its steps are
+// graph launches from the start, and a host thread held up for a few
+// milliseconds no longer leaves the GPU idle behind the capture. Without a
+// usable graph (capture refused) the steps run as plain launches.
+template <class F, class D, class P>
+static int middle_graph(aster_ctx* c, const aster_params* p, int solver, int precision, PhaseTimer* tm, int count,
+                        F middle, D done, P repoint, const int* last) {
+    StepGraph& sg = c->kdk_graph;
+    std::vector<unsigned char> key = step_key(c, p, solver, precision, tm != nullptr);
+    if (!(sg.ge && sg.key == key)) {
+        if (sg.ge) c->graphs.push_back({sg.g, sg.ge});  // may still be queued: destroyed by the next aster_begin
+        cudaEvent_t park = sg.park;
+        sg = StepGraph{};
+        sg.park = park;
+        if (!sg.park) ASTER_CUDA(cudaEventCreateWithFlags(&sg.park, cudaEventDisableTiming));
+        const double inter0 = c->stats.interactions;
+        const int64_t kern0 = c->stats.kernels;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const int st = middle();
+            const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            cudaGraphExec_t ge = nullptr;
+            if (st == ASTER_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess) {
+                sg.g = g;
+                sg.ge = ge;
+                sg.inter = c->stats.interactions - inter0;
+                sg.kernels = c->stats.kernels - kern0;
+                c->stats.interactions = inter0;  // counted per launch below
+                c->stats.kernels = kern0;
+                // every event-record node must be one of this step's marks (re-pointed
+                // before each launch) or a context event; otherwise keep it for this call only
+                bool keep = true;
+                size_t nn = 0;
+                ASTER_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+                std::vector<cudaGraphNode_t> nodes(nn);
+                ASTER_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+                for (cudaGraphNode_t nd : nodes) {
+                    cudaGraphNodeType ty;
+                    ASTER_CUDA(cudaGraphNodeGetType(nd, &ty));
+                    if (ty != cudaGraphNodeTypeEventRecord && ty != cudaGraphNodeTypeWaitEvent) continue;
+                    cudaEvent_t ev = nullptr;
+                    if (ty == cudaGraphNodeTypeEventRecord) ASTER_CUDA(cudaGraphEventRecordNodeGetEvent(nd, &ev));
+                    else ASTER_CUDA(cudaGraphEventWaitNodeGetEvent(nd, &ev));
+                    bool known = false;
+                    for (int k = 0; k < 3; ++k)
+                        if (tm && last[k] >= 0 && tm->ev[last[k]] == ev && ty == cudaGraphNodeTypeEventRecord) {
+                            sg.evnode[k] = nd;
+                            known = true;
+                        }
+                    for (int k = 0; k < 6; ++k)
+                        if (c->ev[k] == ev) known = true;
+                    keep = keep && known;
+                }
+                if (keep) sg.key = key;  // an empty key never matches: not reused by a later call
+            } else {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();  // the failed capture's error
+                if (st != ASTER_OK) return st;
+            }
+        } else {
+            cudaGetLastError();
+        }
+    }
+    int st = ASTER_OK;
+    for (int s = 0; s < count && st == ASTER_OK; ++s) {
+        bool untimed = false;
+        if (sg.ge && tm) st = repoint(sg.ge, sg.evnode, &untimed);
+        if (st != ASTER_OK) break;
+        if (!sg.ge || untimed) {  // plain launches (their marks, if any, recorded by done)
+            st = middle();
+            if (st == ASTER_OK) st = done();
+            continue;
+        }
+        const cudaError_t e = cudaGraphLaunch(sg.ge, c->stream);
+        if (e != cudaSuccess) st = aster_cuda_fail(e, "cudaGraphLaunch", __FILE__, __LINE__);
+        c->stats.interactions += sg.inter;
+        c->stats.kernels += sg.kernels;
+    }
+    // this call's timing events are destroyed when it returns: the marks of the
+    // kept graph point at its own event until the next launch re-points them
+    // (launches already enqueued keep the events they were launched with)
+    if (tm && sg.ge)
+        for (int k = 0; k < 3; ++k)
+            if (sg.evnode[k]) {
+                const cudaError_t e = cudaGraphExecEventRecordNodeSetEvent(sg.ge, sg.evnode[k], sg.park);
+                if (e != cudaSuccess && st == ASTER_OK) st = aster_cuda_fail(e, "park", __FILE__, __LINE__);
+            }
+    return st;
+}
+
 // Enqueues nsteps KDK steps (no synchronisation); marks/tm optional.
 static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precision, int nsteps, PhaseTimer* tm,
                     int (*marks)[3], int* nm) {
@@ -319,6 +428,33 @@ static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precisi
         }
         return ASTER_OK;
     };
+    // points the step's timing marks (event-record nodes en[]) at fresh events
+    // of this call before a launch of ge
+    // (*untimed: out of event slots, nothing re-pointed)
+    auto repoint = [&](cudaGraphExec_t ge, const cudaGraphNode_t* en, bool* untimed) -> int {
+        *untimed = false;
+        int m3[3] = {-1, -1, -1};
+        for (int k = 0; k < 3; ++k) {
+            if (!en[k]) continue;
+            // a mark that names the same event as an earlier one (all-pairs: no build span) shares it
+            int same = -1;
+            for (int q = 0; q < k; ++q)
+                if (en[q] == en[k]) same = q;
+            if (same >= 0) {
+                m3[k] = m3[same];
+                continue;
+            }
+            m3[k] = tm->fresh();
+            if (m3[k] < 0) {
+                *untimed = true;
+                return ASTER_OK;
+            }
+            ASTER_CUDA(cudaGraphExecEventRecordNodeSetEvent(ge, en[k], tm->ev[m3[k]]));
+        }
+        for (int k = 0; k < 3; ++k) marks[*nm][k] = m3[k];
+        ++*nm;
+        return ASTER_OK;
+    };
     auto replay = [&](cudaGraph_t g, cudaGraphExec_t ge) -> int {
         if (!tm) return ASTER_OK;
         if (!found) {  // the captured marks' event-record nodes (last[] names the captured events)
@@ -337,29 +473,18 @@ static int kdk_core(aster_ctx* c, const aster_params* p, int solver, int precisi
             }
             found = true;
         }
-        int m3[3] = {-1, -1, -1};
-        for (int k = 0; k < 3; ++k) {
-            if (!evnode[k]) continue;
-            // a mark that names the same event as an earlier one (all-pairs: no build span) shares it
-            int same = -1;
-            for (int q = 0; q < k; ++q)
-                if (evnode[q] == evnode[k]) same = q;
-            if (same >= 0) {
-                m3[k] = m3[same];
-                continue;
-            }
-            m3[k] = tm->fresh();
-            if (m3[k] < 0) return ASTER_OK;  // out of event slots: the step runs untimed
-            ASTER_CUDA(cudaGraphExecEventRecordNodeSetEvent(ge, evnode[k], tm->ev[m3[k]]));
-        }
-        for (int k = 0; k < 3; ++k) marks[*nm][k] = m3[k];
-        ++*nm;
-        return ASTER_OK;
+        bool untimed = false;  // out of event slots: the step runs untimed
+        return repoint(ge, evnode, &untimed);
     };
     if (fuse) {
         ASTER_TRY(first());
         ASTER_TRY(done());
-        ASTER_TRY(repeat_steps(c, nsteps - 2, true, middle, done, replay));
+        const int nmid = nsteps - 2;
+        if (nmid > 0) {
+            ASTER_TRY(middle());  // plain launches: whatever a step allocates is allocated now
+            ASTER_TRY(done());
+        }
+        if (nmid > 1) ASTER_TRY(middle_graph(c, p, solver, precision, tm, nmid - 1, middle, done, repoint, last));
         ASTER_TRY(final_step());
         ASTER_TRY(done());
     } else {

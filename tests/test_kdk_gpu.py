@@ -135,6 +135,41 @@ def test_tree_steps_fused_drift_equal_single_steps(ctx, prec, law):
         np.testing.assert_array_equal(a, b)
 
 
+def test_tree_kdk_graph_kept_across_calls(ctx):
+    """The middle steps of a multi-step tree run launch a graph that the
+    context keeps from an earlier call with the same parameters, body count
+    and buffers. A repeated run (which launches the kept graph) and the first
+    run both equal a fresh context's bit for bit; a run with another dt, and
+    one with more bodies (the buffers grow), capture anew and equal their own
+    fresh-context runs."""
+    from aster_b200.api import Context
+
+    def fresh(pos, vel, m, p):
+        with Context(0) as other:
+            other.upload(pos, vel, m)
+            other.kdk_steps(p, 6, SOLVER_LBVH, MIXED)
+            return other.download()
+
+    def run(pos, vel, m, p):
+        ctx.upload(pos, vel, m)
+        ctx.kdk_steps(p, 6, SOLVER_LBVH, MIXED)
+        return ctx.download()
+
+    pos, vel, m = gen.plummer(6000, 1031, masses="lognormal")
+    p = Params(G=1.0, eps2=0.005 ** 2, dt=5e-4, theta=0.5)
+    first, again = run(pos, vel, m, p), run(pos, vel, m, p)
+    ref = fresh(pos, vel, m, p)
+    for a, b, r in zip(first, again, ref):
+        np.testing.assert_array_equal(a, r)
+        np.testing.assert_array_equal(b, r)
+    p2 = Params(G=1.0, eps2=0.005 ** 2, dt=2.5e-4, theta=0.5)
+    for a, r in zip(run(pos, vel, m, p2), fresh(pos, vel, m, p2)):
+        np.testing.assert_array_equal(a, r)
+    pos3, vel3, m3 = gen.plummer(9000, 1032, masses="lognormal")
+    for a, r in zip(run(pos3, vel3, m3, p), fresh(pos3, vel3, m3, p)):
+        np.testing.assert_array_equal(a, r)
+
+
 def test_kdk_steps_host_equals_separate_calls(ctx):
     """aster_kdk_steps_host (one call, the positions' copy overlapping the last
     force evaluation) equals upload_acc + kdk_steps + download bit for bit."""
