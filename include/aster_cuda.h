@@ -173,7 +173,11 @@ int aster_lbvh_forces(aster_ctx* ctx, const aster_params* p, int precision,
 
 /* nsteps kick-drift-kick leapfrog steps of the resident state with one force
  * evaluation per step (the acceleration is cached across steps; the reference
- * update_leapfrog evaluates twice per step). solver: ASTER_SOLVER_*. */
+ * update_leapfrog evaluates twice per step). solver: ASTER_SOLVER_*. With
+ * the tree solver, the steps between the first and the last run as launches
+ * of one CUDA graph that the context keeps until it is destroyed: a later call
+ * with the same parameters, body count and device buffers launches it again
+ * instead of capturing a new one. */
 int aster_kdk_steps(aster_ctx* ctx, const aster_params* p, int solver, int precision,
                     int nsteps);
 
